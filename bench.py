@@ -1,0 +1,401 @@
+"""Benchmark: FDK backprojection throughput (GUPS) on one B200.
+
+Workload (the projector-pair throughput configuration): a 512^3 float32 volume
+at 0.5 mm from 720 projections over 360 deg of 1024x768 float32 pixels at
+0.388 mm, SID 1000 mm, SDD 1536 mm.  One step = one FDK backprojection of the
+whole stack into the volume (9.66e10 voxel-projection updates).  The metric is
+giga voxel-projection updates per second (GUPS).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Multi-GPU: replicas only (each rank backprojects its own stack; there is no
+data-path collective), value = all ranks' updates / max-over-ranks time.
+The reference arm times RTK's CPU FDK backprojector (the oracle's restatement
+with RTK's data types and loop order, oracle/rtk_oracle.c) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "backproj GUPS (FDK voxel-projection updates/s, 1e9)"
+UNIT = "GUPS"
+NX = NY = NZ = 512
+VOX = 0.5
+NU, NV, NP = 1024, 768, 720
+PIX = 0.388
+SID, SDD = 1000.0, 1536.0
+SEED = 20261203 + 1
+L1_BYTES_PER_UPDATE = 16  # four 4-byte taps of one bilinear interpolation
+WORKLOAD = {"workload": "FDK backprojection 512^3 @0.5mm <- 720 x 1024x768 @0.388mm, SID 1000, SDD 1536, 360 deg",
+            "volume": [NX, NY, NZ], "projections": [NU, NV, NP], "dtype_storage": "float32",
+            "l2_policy": "inputs larger than L2 (2.26 GB projection stack, 0.54 GB volume)"}
+
+
+def updates_per_step() -> float:
+    return float(NX) * NY * NZ * NP
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.out,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.out.close()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        mhz, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    mhz.append(float(parts[1]))
+                    mx = float(parts[2])
+                except ValueError:
+                    continue
+                for name, val in zip(names, parts[5:9]):
+                    if val.lower() == "active":
+                        reasons.add(name)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": mx, "samples": len(mhz),
+                "reasons": sorted(reasons)}
+
+
+def dist_setup(n_gpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def make_geometry():
+    import rtk_b200 as rtkb
+
+    return rtkb.geometry.circular(NP, SID, SDD)
+
+
+def make_projections(torch, g, gen):
+    """Seeded synthetic projections with the workload's shape: analytic line
+    integrals of 20 random ellipsoids when the phantom projector is available,
+    else seeded uniform values (the backprojector's cost does not depend on
+    the values)."""
+    import rtk_b200 as rtkb
+
+    pd = rtkb.make_desc((NU, NV, NP), (PIX, PIX, 1.0))
+    p = None
+    if hasattr(rtkb.ops, "project_ellipsoids"):
+        from tests import phantoms
+
+        ell = phantoms.random_ellipsoids(20, SEED)
+        p = rtkb.ops.project_ellipsoids(g, pd, ell)
+        kind = "analytic line integrals of 20 seeded random ellipsoids (semi-axes 5-80 mm)"
+    else:
+        p = torch.rand((NP, NV, NU), device="cuda", generator=gen)
+        kind = "seeded uniform random projections"
+    return pd, p, kind
+
+
+def smem_peak_gbs(torch, lib, stream) -> float:
+    """Measured shared-memory gather bandwidth (GB/s), best of 5."""
+    import ctypes as C
+
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    blocks, iters = sms * 8, 4096
+    sink = torch.zeros(blocks, device="cuda")
+    best = 0.0
+    for _ in range(6):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rc = lib.rtkb_probe_smem_gather(blocks, iters, C.c_void_p(sink.data_ptr()), C.c_void_p(stream.cuda_stream))
+        e1.record(stream)
+        e1.synchronize()
+        if rc != 0:
+            return float("nan")
+        t = e0.elapsed_time(e1) / 1e3
+        best = max(best, blocks * 256.0 * iters * 16 / t / 1e9)
+    return best
+
+
+def cpu_baseline_gups(g_oracle_factory, n_proj_sample: int, threads: int):
+    """RTK's CPU FDK backprojector (oracle restatement, FP32 data, FP64 coords)
+    on a bounded sample: the 512^3 volume from the first n_proj_sample projections."""
+    import numpy as np
+
+    from oracle import oracle as O
+
+    go = g_oracle_factory()
+    vo = O.image((NX, NY, NZ), (VOX,) * 3)
+    po = O.image((NU, NV, n_proj_sample), (PIX, PIX, 1.0))
+    rng = np.random.default_rng(SEED)
+    p = rng.random((n_proj_sample, NV, NU), dtype=np.float32)
+    vol = np.zeros((NZ, NY, NX), dtype=np.float32)
+    t0 = time.perf_counter()
+    O.fdk_backproject_f32_rtk(go, vo, po, p, vol, threads=threads)
+    dt = time.perf_counter() - t0
+    return float(NX) * NY * NZ * n_proj_sample / dt / 1e9, dt
+
+
+def oracle_geometry():
+    from oracle import oracle as O
+
+    go = O.Geometry()
+    for i in range(NP):
+        go.add_projection(SID, SDD, i * 360.0 / NP)
+    return go
+
+
+def run_reference(args, world, rank):
+    """--impl reference: RTK's CPU FDK backprojector on the host cores."""
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+
+    O.build()
+    threads = os.cpu_count() or 1
+    sample = 8  # projections per step: a bounded sample of the workload
+    for _ in range(args.warmup):
+        cpu_baseline_gups(oracle_geometry, sample, threads)
+    vals, tot = [], 0.0
+    for _ in range(args.steps):
+        v, dt = cpu_baseline_gups(oracle_geometry, sample, threads)
+        vals.append(v)
+        tot += dt
+    value = float(NX) * NY * NZ * sample * args.steps / tot / 1e9
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded uniform projections)", "config": WORKLOAD,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"512^3 volume from {sample} of the 720 projections per step"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def use_profile_case():
+    """256^3 at 1 mm from 360 of the 1024x768 projections: the same kernel on a
+    case small enough for multi-pass ncu captures (1.1 GB on the device)."""
+    global NX, NY, NZ, VOX, NP, WORKLOAD
+    NX = NY = NZ = 256
+    VOX = 1.0
+    NP = 360
+    WORKLOAD = dict(WORKLOAD, workload="profile case: FDK backprojection 256^3 @1mm <- 360 x 1024x768 @0.388mm",
+                    volume=[NX, NY, NZ], projections=[NU, NV, NP])
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="small case for ncu captures: 256^3 @1mm from 360 projections, device-timed region only")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.profile_case:
+        use_profile_case()
+    world, rank, local = dist_setup(args.gpus)
+    if args.impl == "reference":
+        rc = run_reference(args, world, rank)
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+        return rc
+
+    import torch
+
+    import rtk_b200 as rtkb
+    from rtk_b200 import build as rbuild
+
+    rbuild.build()
+    lib = rtkb.load()
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    gen = torch.Generator(device="cuda").manual_seed(SEED + rank)
+
+    g = make_geometry()
+    vd = rtkb.make_desc((NX, NY, NZ), (VOX,) * 3)
+    pd, proj, data_kind = make_projections(torch, g, gen)
+    zero = torch.zeros((NZ, NY, NX), device="cuda")
+    vol = torch.empty_like(zero)
+
+    def step():
+        rtkb.ops.fdk_backproject(g, vd, pd, proj, zero, out=vol, stream=stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if args.profile_case:
+        step()
+        torch.cuda.synchronize()
+        assert rtkb.ops.device_status(stream) == 0
+        print(json.dumps({"profile_case": WORKLOAD}), flush=True)
+        return 0
+
+    # ---- device-timed region: inputs resident in HBM ----
+    sampler = ClockSampler(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with sampler:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    t = max_over_ranks(e0.elapsed_time(e1) / 1e3, world)
+    clocks = sampler.summary()
+    assert rtkb.ops.device_status(stream) == 0
+    value = updates_per_step() * args.steps * world / t / 1e9
+    ms_per_step = t / args.steps * 1e3
+
+    # ---- end to end through the C ABI: pinned host in, host out ----
+    h_proj = torch.empty((NP, NV, NU), dtype=torch.float32, pin_memory=True)
+    h_proj.copy_(proj)
+    h_vol = torch.empty((NZ, NY, NX), dtype=torch.float32, pin_memory=True)
+    d_proj = torch.empty_like(proj)
+    d_zero = torch.zeros_like(zero)
+
+    def e2e_step():
+        d_proj.copy_(h_proj, non_blocking=True)
+        rtkb.ops.fdk_backproject(g, vd, pd, d_proj, d_zero, out=vol, stream=stream)
+        h_vol.copy_(vol, non_blocking=True)
+
+    for _ in range(2):
+        e2e_step()
+    torch.cuda.synchronize()
+    barrier(world)
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    f1.record(stream)
+    torch.cuda.synchronize()
+    te = max_over_ranks(f0.elapsed_time(f1) / 1e3, world)
+    e2e_value = updates_per_step() * args.steps * world / te / 1e9
+
+    # ---- roofline: L1/shared-memory gather bound ----
+    peak_smem = smem_peak_gbs(torch, lib, stream)
+    achieved = updates_per_step() * L1_BYTES_PER_UPDATE / (t / args.steps) / 1e9
+    pk = peaks()
+    hbm_bytes = (NX * NY * NZ * 4 * 2) + (NP * NV * NU * 4)
+    roofline = {"bound": "l1", "achieved": achieved, "peak": peak_smem, "unit": "GB/s",
+                "frac": achieved / peak_smem if peak_smem else None, "traffic": None,
+                "peak_source": "measured in this run: shared-memory bilinear-gather probe (rtkb_probe_smem_gather)",
+                "per_launch_updates": updates_per_step(), "bytes_per_update": L1_BYTES_PER_UPDATE,
+                "hbm": {"algorithmic_bytes_per_launch": hbm_bytes,
+                        "achieved_gbs": hbm_bytes / (t / args.steps) / 1e9,
+                        "peak_gbs": pk.get("hbm_gbs"), "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"}}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": f"synthetic: {data_kind}", "config": WORKLOAD,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h_proj.numel() * 4,
+                    "d2h_bytes_per_step": h_vol.numel() * 4,
+                    "path": "rtkb_fdk_backproject via ctypes, pinned host buffers, copies inside the timed region"},
+            "roofline": roofline, "clocks": clocks, "gpu_launches": args.steps,
+            "gpu_launches_note": "one rtkb backprojection kernel per step (plus one matrix upload copy)"}
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            threads = os.cpu_count() or 1
+            gups_probe, dt = cpu_baseline_gups(oracle_geometry, 2, threads)
+            n_s = int(max(2, min(64, 15.0 / max(dt / 2, 1e-3))))
+            gups, dt = cpu_baseline_gups(oracle_geometry, n_s, threads)
+            line["cpu_baseline"] = {"value": gups, "unit": UNIT, "cores": threads, "kind": "port",
+                                    "sample": f"512^3 volume from {n_s} of the 720 projections ({dt:.1f} s)"}
+        except Exception as ex:  # the baseline is reported, never the target
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                                    "sample": f"failed: {ex}"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,133 @@
+/*
+ * rtkb200.h -- C ABI of the B200-native RTK hot path (librtkb200.so).
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, returns an
+ * int status (RTKB_OK on success) and never throws.  The message of the last
+ * failure on the calling host thread is returned by rtkb_last_error().
+ *
+ * Buffers: all d_* arguments are caller-owned device pointers to float32
+ * images in ITK layout (row-major, x fastest: volume [z][y][x], projection
+ * stack [projection][v][u]).  Kernels are enqueued on the caller's stream
+ * (a cudaStream_t passed as void*, NULL = legacy default stream) and return
+ * without synchronising.  Calls on different streams are independent: there is
+ * no process-global __constant__ state, unlike the entry points they replace.
+ *
+ * Images are described by rtkb_image_desc: the largest-possible region
+ * (index, size), origin, spacing and direction, as ITK holds them.  Slice s of
+ * a projection stack is geometry projection index[2] + s, as in RTK filters
+ * whose input stack starts at a non-zero projection index.
+ *
+ * Reference interfaces replaced (paths in the RTK repository):
+ *   CUDA_reconstruct_conebeam   include/rtkCudaFDKBackProjectionImageFilter.hcu:22-29
+ *   CUDA_back_project           src/rtkCudaBackProjectionImageFilter.cu:125-135
+ *   CUDA_forward_project        include/rtkCudaForwardProjectionImageFilter.hcu:24-38
+ *   CUDA_ray_cast_back_project  src/rtkCudaRayCastBackProjectionImageFilter.cu:186-199
+ *   CUDA_weight_projection      src/rtkCudaFDKWeightProjectionFilter.cu:85-95
+ *   CUDA_parker_weight          src/rtkCudaParkerShortScanImageFilter.cu:106-118
+ *   CUDA_displaced_weight       src/rtkCudaDisplacedDetectorImageFilter.cu:132-185
+ *   CUDA_padding / CUDA_fft_convolution
+ *                               src/rtkCudaFFTProjectionsConvolutionImageFilter.cu:70-75,175-181
+ *   CUDA_conjugate_gradient     src/rtkCudaConjugateGradientImageFilter.cu:80-166
+ */
+#ifndef RTKB200_H
+#define RTKB200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define RTKB_OK 0
+#define RTKB_ERR_INVALID_ARGUMENT 1
+#define RTKB_ERR_CUDA 2
+#define RTKB_ERR_UNSUPPORTED 3
+#define RTKB_ERR_TIMEOUT 4
+#define RTKB_ERR_OUT_OF_MEMORY 5
+
+/* ---- image description (itk::ImageBase metadata) ---- */
+typedef struct rtkb_image_desc
+{
+  int    size[3];      /* largest-possible region size, x y z */
+  int    index[3];     /* largest-possible region start index */
+  double origin[3];    /* physical position of index (0,0,0) */
+  double spacing[3];   /* pixel spacing */
+  double direction[9]; /* row-major direction cosines */
+} rtkb_image_desc;
+
+/* ---- library ---- */
+/* Message of the last failure on this host thread ("" if none). */
+const char * rtkb_last_error(void);
+/* Library version string. */
+const char * rtkb_version(void);
+/* Waits for `stream`, then reads and clears the device-side status word that
+ * kernels set when a bounded wait gives up (RTKB_ERR_TIMEOUT) or an internal
+ * check fails.  *status receives 0 when no kernel reported a problem. */
+int rtkb_device_status(void * stream, int * status);
+
+/* ---- geometry: rtk::ThreeDCircularProjectionGeometry, FP64 ----
+ * src/rtkThreeDCircularProjectionGeometry.cxx:56-153 (AddProjection),
+ * :407-663 (getters).  Angles in degrees for add_projection, radians for
+ * add_projection_in_radians, as RTK. */
+typedef struct rtkb_geometry rtkb_geometry;
+rtkb_geometry * rtkb_geometry_new(void);
+void            rtkb_geometry_free(rtkb_geometry * g);
+int             rtkb_geometry_add_projection(rtkb_geometry * g, double sid, double sdd, double gantry_angle,
+                                             double proj_offset_x, double proj_offset_y, double out_of_plane_angle,
+                                             double in_plane_angle, double source_offset_x, double source_offset_y);
+int             rtkb_geometry_add_projection_in_radians(rtkb_geometry * g, double sid, double sdd,
+                                                        double gantry_angle, double proj_offset_x,
+                                                        double proj_offset_y, double out_of_plane_angle,
+                                                        double in_plane_angle, double source_offset_x,
+                                                        double source_offset_y);
+int             rtkb_geometry_number_of_projections(const rtkb_geometry * g);
+/* 3x4 projection matrix of projection i (GetMatrices()[i]), row-major */
+int             rtkb_geometry_get_matrix(const rtkb_geometry * g, int i, double out[12]);
+/* homogeneous source position (GetSourcePosition(i)) */
+int             rtkb_geometry_get_source_position(const rtkb_geometry * g, int i, double out[4]);
+/* GetProjectionCoordinatesToFixedSystemMatrix(i), row-major 4x4 */
+int             rtkb_geometry_get_projection_coordinates_to_fixed_system_matrix(const rtkb_geometry * g, int i,
+                                                                                double out[16]);
+/* which: 0 gantry, 1 source, 2 tilt, 3 out-of-plane, 4 in-plane angles (radians);
+ * 5 SID, 6 SDD, 7 projection offsets X, 8 Y, 9 source offsets X, 10 Y;
+ * 11 angular gaps of the source angles (GetAngularGaps(GetSourceAngles())) */
+int             rtkb_geometry_get_parameters(const rtkb_geometry * g, int which, double * out);
+double          rtkb_geometry_to_untilted_coordinate_at_isocenter(const rtkb_geometry * g, int i, double tilted);
+int             rtkb_geometry_set_radius_cylindrical_detector(rtkb_geometry * g, double radius);
+
+/* Volume-index -> projection-index matrices (3x4, row-major, untransposed) of
+ * stack slices first..first+n-1 as BackProjectionImageFilter builds them
+ * (include/rtkBackProjectionImageFilter.hxx:535-595), FDK-normalised when
+ * fdk != 0 (include/rtkFDKBackProjectionImageFilter.hxx:80-104).  modes[s]
+ * receives the path RTK takes: 1 optimised X, 2 optimised Y, 0 generic. */
+int rtkb_backprojection_matrices(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
+                                 int first, int n, int fdk, double * out_matrices, int * modes);
+
+/* ---- backprojection ----
+ * rtk::FDKBackProjectionImageFilter / rtk::BackProjectionImageFilter:
+ * d_vol_out = d_vol_in + sum over the stack of the (FDK-weighted) voxel-driven
+ * bilinear backprojection.  d_vol_in may equal d_vol_out (in place). */
+int rtkb_fdk_backproject(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
+                         const float * d_proj, const float * d_vol_in, float * d_vol_out, void * stream);
+int rtkb_voxel_backproject(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
+                           const float * d_proj, const float * d_vol_in, float * d_vol_out, void * stream);
+/* Matrix-level form mirroring CUDA_reconstruct_conebeam: n_proj FP64
+ * matrices (volume buffer index -> projection buffer index), modes as above,
+ * weighting 1 = FDK (1/w^2), 0 = none. */
+int rtkb_backproject_matrices(const int vol_size[3], const int proj_size[3], int n_proj, const double * matrices,
+                              const int * modes, int weighting, const float * d_proj, const float * d_vol_in,
+                              float * d_vol_out, void * stream);
+
+/* ---- measurement ----
+ * Shared-memory gather peak (no reference counterpart): n_blocks CTAs of 256
+ * threads each perform `iters` bilinear-footprint gathers (4 x 4 bytes) from
+ * shared memory without bank conflicts.  Bytes moved = n_blocks*256*iters*16;
+ * the caller times the launch.  d_sink: n_blocks floats, never written in
+ * practice (defeats dead-code elimination). */
+int rtkb_probe_smem_gather(int n_blocks, int iters, float * d_sink, void * stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

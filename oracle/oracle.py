@@ -1,0 +1,329 @@
+"""ctypes loader for the FP64 CPU oracle (oracle/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, ``__graft_entry__.smoke()`` and
+the CPU-baseline leg of ``bench.py`` as the checker.  The product package
+``rtk_b200`` never imports this module.
+
+Every array is float64 and C-contiguous; images use ITK's row-major x-fastest
+layout (volume [z][y][x], projection stack [projection][v][u]).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+
+
+class OrcImage(C.Structure):
+    _fields_ = [
+        ("size", C.c_int * 3),
+        ("index", C.c_int * 3),
+        ("origin", C.c_double * 3),
+        ("spacing", C.c_double * 3),
+        ("direction", C.c_double * 9),
+    ]
+
+
+class OrcRampParams(C.Structure):
+    _fields_ = [
+        ("hann_cut", C.c_double),
+        ("cosine_cut", C.c_double),
+        ("hamming", C.c_double),
+        ("ramlak_cut", C.c_double),
+        ("shepplogan_cut", C.c_double),
+        ("truncation_correction", C.c_double),
+        ("greatest_prime_factor", C.c_int),
+        ("zero_pad_factor", C.c_int),
+    ]
+
+
+def build() -> str:
+    """Compile liboracle.so with the recipe in oracle/Makefile."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        D = C.POINTER(C.c_double)
+        F = C.POINTER(C.c_float)
+        I = C.POINTER(C.c_int)
+        G = C.c_void_p
+        IM = C.POINTER(OrcImage)
+        sig = {
+            "orc_geometry_new": (G, []),
+            "orc_geometry_free": (None, [G]),
+            "orc_geometry_add_projection": (C.c_int, [G] + [C.c_double] * 9),
+            "orc_geometry_add_projection_rad": (C.c_int, [G] + [C.c_double] * 9),
+            "orc_geometry_size": (C.c_int, [G]),
+            "orc_geometry_matrix": (None, [G, C.c_int, D]),
+            "orc_geometry_source_position": (None, [G, C.c_int, D]),
+            "orc_geometry_proj_coords_to_fixed": (None, [G, C.c_int, D]),
+            "orc_geometry_parameters": (None, [G, C.c_int, D]),
+            "orc_geometry_source_angles": (None, [G, D]),
+            "orc_geometry_gantry_angles": (None, [G, D]),
+            "orc_geometry_tilt_angles": (None, [G, D]),
+            "orc_geometry_angular_gaps": (None, [G, D, D]),
+            "orc_geometry_angular_gaps_with_next": (None, [G, D, D]),
+            "orc_geometry_to_untilted": (C.c_double, [G, C.c_int, C.c_double]),
+            "orc_index_to_physical": (None, [IM, D]),
+            "orc_physical_to_index": (None, [IM, D]),
+            "orc_bp_matrix": (C.c_int, [G, IM, IM, C.c_int, C.c_int, D]),
+            "orc_backproject": (None, [G, IM, IM, D, D, D, C.c_int, C.c_int]),
+            "orc_joseph_forward": (None, [G, IM, D, IM, D, D, C.c_int]),
+            "orc_joseph_back": (None, [G, IM, D, D, IM, D]),
+            "orc_joseph_sample_count": (C.c_double, [G, IM, IM, C.c_int]),
+            "orc_fdk_weight": (None, [G, IM, D, D]),
+            "orc_parker_weight": (C.c_int, [G, IM, C.c_double, D, D]),
+            "orc_displaced_detector_region": (C.c_int, [G, IM, C.c_int, I, I, D, D]),
+            "orc_displaced_detector": (C.c_int, [G, IM, C.c_int, D, D]),
+            "orc_ramp_padded_size": (C.c_int, [C.c_int, C.POINTER(OrcRampParams)]),
+            "orc_ramp_kernel": (None, [C.c_int, C.c_double, C.POINTER(OrcRampParams), D]),
+            "orc_ramp_filter": (None, [IM, C.POINTER(OrcRampParams), D, D, C.c_int]),
+            "orc_cg_joseph": (None, [G, IM, IM, D, D, C.c_double, C.c_int, D, D, C.c_int]),
+            "orc_project_ellipsoids": (None, [G, IM, C.c_int, D, D, C.c_int]),
+            "orc_draw_ellipsoids": (None, [IM, C.c_int, D, D, C.c_int]),
+            "orc_fdk_backproject_f32_rtk": (C.c_int, [G, IM, IM, F, F, C.c_int]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def nthreads() -> int:
+    return max(1, os.cpu_count() or 1)
+
+
+def _d(a):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def image(size, spacing=(1.0, 1.0, 1.0), origin=None, index=(0, 0, 0), direction=None) -> OrcImage:
+    """ITK image description; origin defaults to centring the image on 0."""
+    im = OrcImage()
+    for a in range(3):
+        im.size[a] = int(size[a])
+        im.index[a] = int(index[a])
+        im.spacing[a] = float(spacing[a])
+        im.origin[a] = float(origin[a]) if origin is not None else -0.5 * (size[a] - 1) * spacing[a]
+    d = np.eye(3) if direction is None else np.asarray(direction, dtype=np.float64).reshape(3, 3)
+    for q in range(9):
+        im.direction[q] = float(d.flat[q])
+    return im
+
+
+def shape_of(im: OrcImage):
+    return (im.size[2], im.size[1], im.size[0])
+
+
+def index_to_physical(im: OrcImage):
+    m = np.zeros(16)
+    lib().orc_index_to_physical(C.byref(im), _d(m))
+    return m.reshape(4, 4)
+
+
+class Geometry:
+    """FP64 restatement of rtk::ThreeDCircularProjectionGeometry."""
+
+    def __init__(self):
+        self._g = lib().orc_geometry_new()
+
+    def __del__(self):
+        try:
+            if self._g:
+                lib().orc_geometry_free(self._g)
+                self._g = None
+        except Exception:
+            pass
+
+    def add_projection(self, sid, sdd, gantry_deg, pox=0.0, poy=0.0, oop_deg=0.0, ip_deg=0.0, sox=0.0, soy=0.0):
+        rc = lib().orc_geometry_add_projection(self._g, sid, sdd, gantry_deg, pox, poy, oop_deg, ip_deg, sox, soy)
+        if rc != 0:
+            raise ValueError("cannot mix parallel and divergent projections")
+
+    def __len__(self):
+        return lib().orc_geometry_size(self._g)
+
+    def matrix(self, i):
+        m = np.zeros(12)
+        lib().orc_geometry_matrix(self._g, i, _d(m))
+        return m.reshape(3, 4)
+
+    def source_position(self, i):
+        s = np.zeros(4)
+        lib().orc_geometry_source_position(self._g, i, _d(s))
+        return s
+
+    def proj_coords_to_fixed(self, i):
+        m = np.zeros(16)
+        lib().orc_geometry_proj_coords_to_fixed(self._g, i, _d(m))
+        return m.reshape(4, 4)
+
+    def _vec(self, fn):
+        out = np.zeros(len(self))
+        fn(self._g, _d(out))
+        return out
+
+    def source_angles(self):
+        return self._vec(lib().orc_geometry_source_angles)
+
+    def gantry_angles(self):
+        return self._vec(lib().orc_geometry_gantry_angles)
+
+    def tilt_angles(self):
+        return self._vec(lib().orc_geometry_tilt_angles)
+
+    def angular_gaps(self, angles):
+        a = np.ascontiguousarray(angles, dtype=np.float64)
+        out = np.zeros(len(self))
+        lib().orc_geometry_angular_gaps(self._g, _d(a), _d(out))
+        return out
+
+    def to_untilted(self, i, x):
+        return lib().orc_geometry_to_untilted(self._g, i, x)
+
+
+def bp_matrix(g: Geometry, vol: OrcImage, proj: OrcImage, i: int, fdk: bool):
+    m = np.zeros(12)
+    mode = lib().orc_bp_matrix(g._g, C.byref(vol), C.byref(proj), i, int(fdk), _d(m))
+    return m.reshape(3, 4), mode
+
+
+def backproject(g, vol, proj, proj_data, vol_in=None, fdk=True, threads=None):
+    p = np.ascontiguousarray(proj_data, dtype=np.float64)
+    vin = np.zeros(shape_of(vol)) if vol_in is None else np.ascontiguousarray(vol_in, dtype=np.float64)
+    out = np.empty(shape_of(vol))
+    lib().orc_backproject(g._g, C.byref(vol), C.byref(proj), _d(p), _d(vin), _d(out), int(fdk),
+                          threads or nthreads())
+    return out
+
+
+def joseph_forward(g, vol, vol_data, proj, proj_in=None, threads=None):
+    v = np.ascontiguousarray(vol_data, dtype=np.float64)
+    pin = np.zeros(shape_of(proj)) if proj_in is None else np.ascontiguousarray(proj_in, dtype=np.float64)
+    out = np.empty(shape_of(proj))
+    lib().orc_joseph_forward(g._g, C.byref(vol), _d(v), C.byref(proj), _d(pin), _d(out), threads or nthreads())
+    return out
+
+
+def joseph_back(g, vol, proj, proj_data, vol_in=None):
+    p = np.ascontiguousarray(proj_data, dtype=np.float64)
+    vin = np.zeros(shape_of(vol)) if vol_in is None else np.ascontiguousarray(vol_in, dtype=np.float64)
+    out = np.empty(shape_of(vol))
+    lib().orc_joseph_back(g._g, C.byref(vol), _d(vin), _d(out), C.byref(proj), _d(p))
+    return out
+
+
+def joseph_sample_count(g, vol, proj, threads=None) -> float:
+    return lib().orc_joseph_sample_count(g._g, C.byref(vol), C.byref(proj), threads or nthreads())
+
+
+def fdk_weight(g, proj, data):
+    d = np.ascontiguousarray(data, dtype=np.float64)
+    out = np.empty_like(d)
+    lib().orc_fdk_weight(g._g, C.byref(proj), _d(d), _d(out))
+    return out
+
+
+def parker_weight(g, proj, data, threshold=np.pi / 9):
+    d = np.ascontiguousarray(data, dtype=np.float64)
+    out = np.empty_like(d)
+    short = lib().orc_parker_weight(g._g, C.byref(proj), threshold, _d(d), _d(out))
+    return out, bool(short)
+
+
+def displaced_detector_region(g, proj, pad=True):
+    i0, s0 = C.c_int(), C.c_int()
+    inf, sup = C.c_double(), C.c_double()
+    st = lib().orc_displaced_detector_region(g._g, C.byref(proj), int(pad), C.byref(i0), C.byref(s0),
+                                             C.byref(inf), C.byref(sup))
+    return st, i0.value, s0.value, inf.value, sup.value
+
+
+def displaced_detector(g, proj, data, pad=True):
+    st, i0, s0, _, _ = displaced_detector_region(g, proj, pad)
+    if st < 0:
+        raise ValueError("Cannot account for detector displacement larger than 50% of panel size.")
+    d = np.ascontiguousarray(data, dtype=np.float64)
+    out = np.zeros((proj.size[2], proj.size[1], s0))
+    lib().orc_displaced_detector(g._g, C.byref(proj), int(pad), _d(d), _d(out))
+    return out, i0, s0
+
+
+def ramp_params(hann=0.0, cosine=0.0, hamming=0.0, ramlak=0.0, shepplogan=0.0, truncation=0.0, gpf=2, pad=2):
+    p = OrcRampParams()
+    p.hann_cut, p.cosine_cut, p.hamming = hann, cosine, hamming
+    p.ramlak_cut, p.shepplogan_cut, p.truncation_correction = ramlak, shepplogan, truncation
+    p.greatest_prime_factor, p.zero_pad_factor = gpf, pad
+    return p
+
+
+def ramp_padded_size(nu, params):
+    return lib().orc_ramp_padded_size(nu, C.byref(params))
+
+
+def ramp_kernel(padded, spacing, params):
+    k = np.zeros(padded // 2 + 1)
+    lib().orc_ramp_kernel(padded, spacing, C.byref(params), _d(k))
+    return k
+
+
+def ramp_filter(proj, data, params, threads=None):
+    d = np.ascontiguousarray(data, dtype=np.float64)
+    out = np.empty_like(d)
+    lib().orc_ramp_filter(C.byref(proj), C.byref(params), _d(d), _d(out), threads or nthreads())
+    return out
+
+
+def cg_joseph(g, vol, proj, proj_data, niter, x0=None, weights=None, tikhonov=0.0, threads=None):
+    p = np.ascontiguousarray(proj_data, dtype=np.float64)
+    w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+    x = np.zeros(shape_of(vol)) if x0 is None else np.array(x0, dtype=np.float64, copy=True, order="C")
+    res = np.zeros(niter + 1)
+    lib().orc_cg_joseph(g._g, C.byref(vol), C.byref(proj), _d(p), _d(w), tikhonov, niter, _d(x), _d(res),
+                        threads or nthreads())
+    return x, res
+
+
+def project_ellipsoids(g, proj, ell, threads=None):
+    e = np.ascontiguousarray(ell, dtype=np.float64).reshape(-1, 16)
+    out = np.empty(shape_of(proj))
+    lib().orc_project_ellipsoids(g._g, C.byref(proj), e.shape[0], _d(e), _d(out), threads or nthreads())
+    return out
+
+
+def draw_ellipsoids(vol, ell, threads=None):
+    e = np.ascontiguousarray(ell, dtype=np.float64).reshape(-1, 16)
+    out = np.empty(shape_of(vol))
+    lib().orc_draw_ellipsoids(C.byref(vol), e.shape[0], _d(e), _d(out), threads or nthreads())
+    return out
+
+
+def fdk_backproject_f32_rtk(g, vol, proj, proj_data_f32, vol_inout_f32, threads=None):
+    """RTK's CPU FDK backprojector with RTK's data types (the timed CPU baseline)."""
+    p = np.ascontiguousarray(proj_data_f32, dtype=np.float32)
+    assert vol_inout_f32.dtype == np.float32 and vol_inout_f32.flags.c_contiguous
+    rc = lib().orc_fdk_backproject_f32_rtk(g._g, C.byref(vol), C.byref(proj),
+                                           p.ctypes.data_as(C.POINTER(C.c_float)),
+                                           vol_inout_f32.ctypes.data_as(C.POINTER(C.c_float)),
+                                           threads or nthreads())
+    if rc != 0:
+        raise RuntimeError("CPU baseline needs the optimised-Y path (circular geometry)")

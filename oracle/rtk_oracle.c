@@ -1,0 +1,1668 @@
+/*
+ * rtk_oracle.c -- FP64 CPU restatement of RTK's hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker for the CUDA product, never part of
+ * it.  Every function restates the RTK 2.7.0 source cited in its comment
+ * (paths relative to the RTK repository).  All arithmetic is FP64, including
+ * image data, except orc_fdk_backproject_f32_rtk, which reproduces RTK's own
+ * CPU data types (FP32 data, FP64 coordinates) and is the timed CPU baseline.
+ *
+ * Parity status: partially pinned (see rtk_oracle.h).
+ */
+#include "rtk_oracle.h"
+
+#include <float.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#  include <omp.h>
+#endif
+
+#define ORC_PI 3.14159265358979323846
+
+/* ------------------------------------------------------------------------ */
+/* small matrix helpers (row-major)                                         */
+/* ------------------------------------------------------------------------ */
+static void
+mat_mul(const double * a, const double * b, double * c, int n, int k, int m)
+{
+  /* c (n x m) = a (n x k) * b (k x m) */
+  double t[64];
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < m; j++)
+    {
+      double s = 0.;
+      for (int l = 0; l < k; l++)
+        s += a[i * k + l] * b[l * m + j];
+      t[i * m + j] = s;
+    }
+  memcpy(c, t, sizeof(double) * n * m);
+}
+
+static void
+mat4_identity(double * m)
+{
+  memset(m, 0, 16 * sizeof(double));
+  m[0] = m[5] = m[10] = m[15] = 1.;
+}
+
+/* inverse of a 4x4 homogeneous affine matrix (last row 0 0 0 1) */
+static void
+affine4_inverse(const double * m, double * r)
+{
+  const double a = m[0], b = m[1], c = m[2], d = m[4], e = m[5], f = m[6], g = m[8], h = m[9], i = m[10];
+  const double A = e * i - f * h, B = -(d * i - f * g), C = d * h - e * g;
+  const double det = a * A + b * B + c * C;
+  const double id = 1. / det;
+  double       inv[9];
+  inv[0] = A * id;
+  inv[1] = -(b * i - c * h) * id;
+  inv[2] = (b * f - c * e) * id;
+  inv[3] = B * id;
+  inv[4] = (a * i - c * g) * id;
+  inv[5] = -(a * f - c * d) * id;
+  inv[6] = C * id;
+  inv[7] = -(a * h - b * g) * id;
+  inv[8] = (a * e - b * d) * id;
+  mat4_identity(r);
+  for (int row = 0; row < 3; row++)
+  {
+    for (int col = 0; col < 3; col++)
+      r[row * 4 + col] = inv[row * 3 + col];
+    r[row * 4 + 3] = -(inv[row * 3 + 0] * m[3] + inv[row * 3 + 1] * m[7] + inv[row * 3 + 2] * m[11]);
+  }
+}
+
+static double
+convert_0_2pi(double a)
+{
+  /* ThreeDCircularProjectionGeometry::ConvertAngleBetween0And2PIRadians,
+   * src/rtkThreeDCircularProjectionGeometry.cxx:40-44 */
+  return a - 2 * ORC_PI * floor(a / (2 * ORC_PI));
+}
+
+/* ------------------------------------------------------------------------ */
+/* geometry                                                                 */
+/* ------------------------------------------------------------------------ */
+struct orc_geometry
+{
+  int      n, cap;
+  double * par; /* 10 per projection: sid sdd ga pox poy oop ip sox soy srcangle */
+  double * rot; /* 16 */
+  double * mag; /* 12 */
+  double * srt; /* 16 */
+  double * prt; /* 9 */
+  double * mat; /* 12 */
+};
+
+enum
+{
+  P_SID,
+  P_SDD,
+  P_GA,
+  P_POX,
+  P_POY,
+  P_OOP,
+  P_IP,
+  P_SOX,
+  P_SOY,
+  P_SANG
+};
+
+orc_geometry *
+orc_geometry_new(void)
+{
+  orc_geometry * g = (orc_geometry *)calloc(1, sizeof(orc_geometry));
+  return g;
+}
+
+void
+orc_geometry_free(orc_geometry * g)
+{
+  if (!g)
+    return;
+  free(g->par);
+  free(g->rot);
+  free(g->mag);
+  free(g->srt);
+  free(g->prt);
+  free(g->mat);
+  free(g);
+}
+
+static void
+geometry_grow(orc_geometry * g)
+{
+  if (g->n < g->cap)
+    return;
+  g->cap = g->cap ? 2 * g->cap : 64;
+  g->par = (double *)realloc(g->par, sizeof(double) * 10 * g->cap);
+  g->rot = (double *)realloc(g->rot, sizeof(double) * 16 * g->cap);
+  g->mag = (double *)realloc(g->mag, sizeof(double) * 12 * g->cap);
+  g->srt = (double *)realloc(g->srt, sizeof(double) * 16 * g->cap);
+  g->prt = (double *)realloc(g->prt, sizeof(double) * 9 * g->cap);
+  g->mat = (double *)realloc(g->mat, sizeof(double) * 12 * g->cap);
+}
+
+/* ComputeRotationHomogeneousMatrix(angleX, angleY, angleZ):
+ * itk::CenteredEuler3DTransform in ZXY order, R = Rz * Rx * Ry
+ * (src/rtkThreeDCircularProjectionGeometry.cxx:536-549,
+ *  documentation/docs/Geometry.md:60-88) */
+static void
+rotation_zxy(double ax, double ay, double az, double * m)
+{
+  const double cx = cos(ax), sx = sin(ax), cy = cos(ay), sy = sin(ay), cz = cos(az), sz = sin(az);
+  const double Rx[9] = { 1, 0, 0, 0, cx, -sx, 0, sx, cx };
+  const double Ry[9] = { cy, 0, sy, 0, 1, 0, -sy, 0, cy };
+  const double Rz[9] = { cz, -sz, 0, sz, cz, 0, 0, 0, 1 };
+  double       t[9], r[9];
+  mat_mul(Rz, Rx, t, 3, 3, 3);
+  mat_mul(t, Ry, r, 3, 3, 3);
+  mat4_identity(m);
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++)
+      m[i * 4 + j] = r[i * 3 + j];
+}
+
+static void
+rotation_inverse(const double * rot, double * inv)
+{
+  /* GetRotationMatrices()[i].GetInverse(): the 3x3 block is orthonormal */
+  mat4_identity(inv);
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++)
+      inv[i * 4 + j] = rot[j * 4 + i];
+}
+
+int
+orc_geometry_add_projection_rad(orc_geometry * g, double sid, double sdd, double gantry, double pox, double poy,
+                                double oop, double ip, double sox, double soy)
+{
+  /* AddProjectionInRadians, src/rtkThreeDCircularProjectionGeometry.cxx:79-153 */
+  if (g->n > 0)
+  {
+    const double sdd0 = g->par[P_SDD];
+    if ((sdd == 0.) != (sdd0 == 0.))
+      return -1;
+  }
+  geometry_grow(g);
+  const int i = g->n;
+  double *  p = g->par + 10 * i;
+  p[P_SID] = sid;
+  p[P_SDD] = sdd;
+  p[P_GA] = convert_0_2pi(gantry);
+  p[P_POX] = pox;
+  p[P_POY] = poy;
+  p[P_OOP] = convert_0_2pi(oop);
+  p[P_IP] = convert_0_2pi(ip);
+  p[P_SOX] = sox;
+  p[P_SOY] = soy;
+
+  double * prt = g->prt + 9 * i;
+  memset(prt, 0, 9 * sizeof(double));
+  prt[0] = prt[4] = prt[8] = 1.;
+  prt[2] = sox - pox;
+  prt[5] = soy - poy;
+
+  /* ComputeProjectionMagnificationMatrix(-sdd, -sid), :573-582 */
+  double *     mag = g->mag + 12 * i;
+  const double msdd = -sdd, msid = -sid;
+  memset(mag, 0, 12 * sizeof(double));
+  mag[0] = mag[5] = (msdd == 0.) ? 1. : msdd;
+  mag[10] = (msdd == 0.) ? 0. : 1.;
+  mag[11] = (msdd == 0.) ? 1. : msid;
+
+  rotation_zxy(-oop, -gantry, -ip, g->rot + 16 * i);
+
+  double * srt = g->srt + 16 * i;
+  mat4_identity(srt);
+  srt[3] = -sox;
+  srt[7] = -soy;
+
+  double t1[12], t2[12];
+  mat_mul(prt, mag, t1, 3, 3, 4);
+  mat_mul(t1, srt, t2, 3, 4, 4);
+  mat_mul(t2, g->rot + 16 * i, g->mat + 12 * i, 3, 4, 4);
+  g->n++;
+
+  /* source angle, :133-144 */
+  double sph[4];
+  orc_geometry_source_position(g, i, sph);
+  sph[1] = 0.;
+  const double nrm = sqrt(sph[0] * sph[0] + sph[1] * sph[1] + sph[2] * sph[2]);
+  double       sp[3] = { sph[0] / nrm, sph[1] / nrm, sph[2] / nrm };
+  double       a = acos(sp[2]);
+  if (sp[0] > 0.)
+    a = 2. * ORC_PI - a;
+  p[P_SANG] = convert_0_2pi(a);
+  return 0;
+}
+
+int
+orc_geometry_add_projection(orc_geometry * g, double sid, double sdd, double ga, double pox, double poy, double oop,
+                            double ip, double sox, double soy)
+{
+  /* AddProjection, :56-77 */
+  const double d2r = atan(1.0) / 45.0;
+  return orc_geometry_add_projection_rad(g, sid, sdd, d2r * ga, pox, poy, d2r * oop, d2r * ip, sox, soy);
+}
+
+int
+orc_geometry_size(const orc_geometry * g)
+{
+  return g->n;
+}
+
+void
+orc_geometry_matrix(const orc_geometry * g, int i, double m[12])
+{
+  memcpy(m, g->mat + 12 * i, 12 * sizeof(double));
+}
+
+void
+orc_geometry_parameters(const orc_geometry * g, int i, double p[10])
+{
+  memcpy(p, g->par + 10 * i, 10 * sizeof(double));
+}
+
+void
+orc_geometry_source_position(const orc_geometry * g, int i, double s[4])
+{
+  /* GetSourcePosition, :597-608 */
+  const double * p = g->par + 10 * i;
+  double         inv[16];
+  rotation_inverse(g->rot + 16 * i, inv);
+  const double v[4] = { p[P_SOX], p[P_SOY], p[P_SID], 1. };
+  mat_mul(inv, v, s, 4, 4, 1);
+}
+
+void
+orc_geometry_proj_coords_to_fixed(const orc_geometry * g, int i, double m[16])
+{
+  /* GetProjectionCoordinatesToDetectorSystemMatrix + ...ToFixedSystemMatrix, :611-637 */
+  const double * p = g->par + 10 * i;
+  double         d[16], inv[16];
+  mat4_identity(d);
+  d[3] = p[P_POX];
+  d[7] = p[P_POY];
+  d[11] = (p[P_SDD] == 0.) ? -p[P_SID] : p[P_SID] - p[P_SDD];
+  d[10] = 0.;
+  rotation_inverse(g->rot + 16 * i, inv);
+  mat_mul(inv, d, m, 4, 4, 4);
+}
+
+void
+orc_geometry_source_angles(const orc_geometry * g, double * out)
+{
+  for (int i = 0; i < g->n; i++)
+    out[i] = g->par[10 * i + P_SANG];
+}
+
+void
+orc_geometry_gantry_angles(const orc_geometry * g, double * out)
+{
+  for (int i = 0; i < g->n; i++)
+    out[i] = g->par[10 * i + P_GA];
+}
+
+void
+orc_geometry_tilt_angles(const orc_geometry * g, double * out)
+{
+  /* GetTiltAngles, :407-418 */
+  for (int i = 0; i < g->n; i++)
+    out[i] = convert_0_2pi(-1. * g->par[10 * i + P_GA] - g->par[10 * i + P_SANG]);
+}
+
+typedef struct
+{
+  double a;
+  int    i;
+} angle_idx;
+
+static int
+cmp_angle(const void * x, const void * y)
+{
+  const angle_idx * p = (const angle_idx *)x;
+  const angle_idx * q = (const angle_idx *)y;
+  if (p->a < q->a)
+    return -1;
+  if (p->a > q->a)
+    return 1;
+  /* std::multimap keeps insertion order for equal keys */
+  return p->i - q->i;
+}
+
+static angle_idx *
+sorted_angles(const double * angles, int n)
+{
+  angle_idx * s = (angle_idx *)malloc(sizeof(angle_idx) * (n > 0 ? n : 1));
+  for (int i = 0; i < n; i++)
+  {
+    s[i].a = angles[i];
+    s[i].i = i;
+  }
+  qsort(s, n, sizeof(angle_idx), cmp_angle);
+  return s;
+}
+
+void
+orc_geometry_angular_gaps(const orc_geometry * g, const double * angles, double * out)
+{
+  /* GetAngularGaps, :478-533 */
+  const int n = g->n;
+  if (n == 1)
+    out[0] = 2 * ORC_PI;
+  if (n < 2)
+    return;
+  angle_idx * s = sorted_angles(angles, n);
+  out[s[0].i] = 0.5 * (s[1].a - s[n - 1].a + 2 * ORC_PI);
+  for (int k = 1; k < n - 1; k++)
+    out[s[k].i] = 0.5 * (s[k + 1].a - s[k - 1].a);
+  out[s[n - 1].i] = 0.5 * (s[0].a + 2 * ORC_PI - s[n - 2].a);
+  if (g->par[P_SDD] == 0.)
+  {
+    double mx = out[0];
+    for (int k = 1; k < n; k++)
+      if (out[k] > mx)
+        mx = out[k];
+    if (mx > ORC_PI / 2)
+      for (int k = 0; k < n; k++)
+      {
+        if (out[k] > ORC_PI / 2)
+          out[k] -= ORC_PI / 2;
+        out[k] *= 2.;
+      }
+  }
+  free(s);
+}
+
+void
+orc_geometry_angular_gaps_with_next(const orc_geometry * g, const double * angles, double * out)
+{
+  /* GetAngularGapsWithNext, :447-476 */
+  const int n = g->n;
+  if (n == 1)
+    out[0] = 2 * ORC_PI;
+  if (n < 2)
+    return;
+  angle_idx * s = sorted_angles(angles, n);
+  for (int k = 0; k < n - 1; k++)
+    out[s[k].i] = s[k + 1].a - s[k].a;
+  out[s[n - 1].i] = s[0].a + 2 * ORC_PI - s[n - 1].a;
+  free(s);
+}
+
+double
+orc_geometry_to_untilted(const orc_geometry * g, int i, double tilted)
+{
+  /* ToUntiltedCoordinateAtIsocenter, :641-663 */
+  const double * p = g->par + 10 * i;
+  const double   sid = p[P_SID], sdd = p[P_SDD], sx = p[P_SOX], px = p[P_POX];
+  const double   sidu = sqrt(sid * sid + sx * sx);
+  const double   l = (tilted + px - sx) * sid / sdd + sx;
+  const double   cosa = sx / sidu;
+  return l * fabs(sid) / (sidu - l * cosa);
+}
+
+/* ------------------------------------------------------------------------ */
+/* image matrices (include/rtkHomogeneousMatrix.h:38-81)                     */
+/* ------------------------------------------------------------------------ */
+void
+orc_index_to_physical(const orc_image * im, double m[16])
+{
+  mat4_identity(m);
+  for (int i = 0; i < 3; i++)
+  {
+    for (int j = 0; j < 3; j++)
+      m[i * 4 + j] = im->direction[i * 3 + j] * im->spacing[j];
+    m[i * 4 + 3] = im->origin[i];
+  }
+}
+
+void
+orc_physical_to_index(const orc_image * im, double m[16])
+{
+  double a[16];
+  orc_index_to_physical(im, a);
+  affine4_inverse(a, m);
+}
+
+static long
+npix(const orc_image * im)
+{
+  return (long)im->size[0] * im->size[1] * im->size[2];
+}
+
+/* ------------------------------------------------------------------------ */
+/* voxel-based and FDK backprojection                                       */
+/* ------------------------------------------------------------------------ */
+int
+orc_bp_matrix(const orc_geometry * g, const orc_image * vol, const orc_image * proj, int i, int fdk, double m[12])
+{
+  /* GetIndexToIndexProjectionMatrix, include/rtkBackProjectionImageFilter.hxx:535-595
+   * (untransposed: the transposition of :480-531 only changes memory layout) */
+  double vi2pp[16], t[12], volidx_to_projpp[12];
+  orc_index_to_physical(vol, vi2pp);
+  mat_mul(g->mag + 12 * i, g->srt + 16 * i, t, 3, 4, 4);
+  mat_mul(t, g->rot + 16 * i, t, 3, 4, 4);
+  mat_mul(t, vi2pp, volidx_to_projpp, 3, 4, 4);
+
+  double spp2i[16], mp[9], pp2pi[9];
+  orc_physical_to_index(proj, spp2i);
+  memset(mp, 0, sizeof(mp));
+  for (int r = 0; r < 2; r++)
+  {
+    mp[r * 3 + 2] = spp2i[r * 4 + 3];
+    for (int c = 0; c < 2; c++)
+      mp[r * 3 + c] = spp2i[r * 4 + c];
+  }
+  mp[8] = 1.;
+  mat_mul(mp, g->prt + 9 * i, pp2pi, 3, 3, 3);
+  mat_mul(pp2pi, volidx_to_projpp, m, 3, 3, 4);
+
+  if (fdk)
+  {
+    /* normalisation at the rotation centre,
+     * include/rtkFDKBackProjectionImageFilter.hxx:80-104 */
+    double vpp2i[16];
+    orc_physical_to_index(vol, vpp2i);
+    const double rc[3] = { vpp2i[3], vpp2i[7], vpp2i[11] };
+    double       persp = m[11];
+    for (int j = 0; j < 3; j++)
+      persp += m[8 + j] * rc[j];
+    for (int j = 0; j < 12; j++)
+      m[j] /= persp;
+  }
+  /* path selection on the transposed matrix, :106-116: transposed row 1 is
+   * the untransposed row 0 */
+  if (fabs(m[0]) < 1e-10 && fabs(m[8]) < 1e-10)
+    return 1;
+  if (fabs(m[1]) < 1e-10 && fabs(m[9]) < 1e-10)
+    return 2;
+  return 0;
+}
+
+static double
+interp_clamped(const double * p, int nu, int nv, double u, double v)
+{
+  /* itk::LinearInterpolateImageFunction on a 2-D image: clamp-to-edge bilinear */
+  double uc = u < 0. ? 0. : (u > nu - 1 ? nu - 1 : u);
+  double vc = v < 0. ? 0. : (v > nv - 1 ? nv - 1 : v);
+  int    iu = (int)floor(uc), iv = (int)floor(vc);
+  int    iu1 = iu + 1 < nu ? iu + 1 : nu - 1;
+  int    iv1 = iv + 1 < nv ? iv + 1 : nv - 1;
+  double fu = uc - iu, fv = vc - iv;
+  double a = p[(long)iv * nu + iu] + fu * (p[(long)iv * nu + iu1] - p[(long)iv * nu + iu]);
+  double b = p[(long)iv1 * nu + iu] + fu * (p[(long)iv1 * nu + iu1] - p[(long)iv1 * nu + iu]);
+  return a + fv * (b - a);
+}
+
+void
+orc_backproject(const orc_geometry * g, const orc_image * vol, const orc_image * proj, const double * proj_data,
+                const double * vol_in, double * vol_out, int fdk, int nthreads)
+{
+  /* BackProjectionImageFilter::DynamicThreadedGenerateData
+   * (include/rtkBackProjectionImageFilter.hxx:185-279) and
+   * FDKBackProjectionImageFilter::DynamicThreadedGenerateData
+   * (include/rtkFDKBackProjectionImageFilter.hxx:52-148) with their optimised
+   * paths (:152-306 and :352-475): u = (M0.x)/(M2.x), v = (M1.x)/(M2.x);
+   * optimised paths accept 0 <= floor(u) < Nu-1 and 0 <= floor(v) < Nv-1,
+   * the generic path accepts [-0.5, N-0.5) with clamp-to-edge interpolation;
+   * FDK weights each sample by (1/(M2.x))^2 after normalisation. */
+  const int  nx = vol->size[0], ny = vol->size[1], nz = vol->size[2];
+  const int  nu = proj->size[0], nv = proj->size[1], np = proj->size[2];
+  const long nvox = npix(vol);
+  if (vol_out != vol_in)
+    memcpy(vol_out, vol_in, sizeof(double) * nvox);
+  double * mats = (double *)malloc(sizeof(double) * 12 * (np > 0 ? np : 1));
+  int *    modes = (int *)malloc(sizeof(int) * (np > 0 ? np : 1));
+  for (int s = 0; s < np; s++)
+  {
+    modes[s] = orc_bp_matrix(g, vol, proj, proj->index[2] + s, fdk, mats + 12 * s);
+    double * m = mats + 12 * s;
+    if (modes[s] == 1)
+    {
+      m[0] = 0.;
+      m[8] = 0.;
+    }
+    else if (modes[s] == 2)
+    {
+      m[1] = 0.;
+      m[9] = 0.;
+    }
+  }
+  const double pi0 = proj->index[0], pi1 = proj->index[1];
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 1)
+  for (int k = 0; k < nz; k++)
+  {
+    for (int s = 0; s < np; s++)
+    {
+      const double * m = mats + 12 * s;
+      const double * p = proj_data + (long)s * nu * nv;
+      for (int j = 0; j < ny; j++)
+        for (int i = 0; i < nx; i++)
+        {
+          const double x = i + vol->index[0], y = j + vol->index[1], z = k + vol->index[2];
+          const double w = m[8] * x + m[9] * y + m[10] * z + m[11];
+          const double rw = 1. / w;
+          const double u = (m[0] * x + m[1] * y + m[2] * z + m[3]) * rw - pi0;
+          const double v = (m[4] * x + m[5] * y + m[6] * z + m[7]) * rw - pi1;
+          const long   o = ((long)k * ny + j) * nx + i;
+          const double wt = fdk ? rw * rw : 1.;
+          if (modes[s])
+          {
+            const int iu = (int)floor(u), iv = (int)floor(v);
+            if (iu >= 0 && iu < nu - 1 && iv >= 0 && iv < nv - 1)
+            {
+              const double fu = u - iu, fv = v - iv;
+              const double * q = p + (long)iv * nu + iu;
+              vol_out[o] += wt * ((1 - fv) * ((1 - fu) * q[0] + fu * q[1]) + fv * ((1 - fu) * q[nu] + fu * q[nu + 1]));
+            }
+          }
+          else if (u >= -0.5 && u < nu - 0.5 && v >= -0.5 && v < nv - 0.5)
+            vol_out[o] += wt * interp_clamped(p, nu, nv, u, v);
+        }
+    }
+  }
+  free(mats);
+  free(modes);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Joseph projector pair                                                    */
+/* ------------------------------------------------------------------------ */
+typedef struct
+{
+  double pix[3], dir[3];
+} ray_t;
+
+/* BoxShape::IsIntersectedByRay with identity direction, src/rtkBoxShape.cxx:47-97 */
+static int
+box_intersect(const double * bmin, const double * bmax, const double * org, const double * dir, double * tin,
+              double * tout)
+{
+  double inf = -DBL_MAX, sup = DBL_MAX;
+  for (int i = 0; i < 3; i++)
+  {
+    double mn = bmin[i], mx = bmax[i];
+    if (mn > mx)
+    {
+      double t = mn;
+      mn = mx;
+      mx = t;
+    }
+    if (dir[i] == 0. && (org[i] < mn || org[i] > mx))
+      return 0;
+    const double inv = 1 / dir[i];
+    double       t1 = (mn - org[i]) * inv, t2 = (mx - org[i]) * inv;
+    if (t1 > t2)
+    {
+      double t = t1;
+      t1 = t2;
+      t2 = t;
+    }
+    if (t1 > inf)
+      inf = t1;
+    if (t2 < sup)
+      sup = t2;
+    if (inf > sup)
+      return 0;
+    if (sup < 0.)
+      return 0;
+  }
+  *tin = inf;
+  *tout = sup;
+  return 1;
+}
+
+typedef struct
+{
+  double pix2vol[16]; /* projection index -> volume index (homogeneous) */
+  double src[3];      /* source in volume index coordinates */
+} joseph_proj_t;
+
+static void
+joseph_setup(const orc_geometry * g, const orc_image * vol, const orc_image * proj, int i, joseph_proj_t * jp)
+{
+  /* ProjectionsRegionConstIteratorRayBasedWithFlatPanel::NewProjection,
+   * include/rtkProjectionsRegionConstIteratorRayBasedWithFlatPanel.hxx:39-71 */
+  double vpp2i[16], p2f[16], pi2pp[16], t[16], s4[4], sv[4];
+  orc_physical_to_index(vol, vpp2i);
+  orc_geometry_proj_coords_to_fixed(g, i, p2f);
+  orc_index_to_physical(proj, pi2pp);
+  mat_mul(vpp2i, p2f, t, 4, 4, 4);
+  mat_mul(t, pi2pp, jp->pix2vol, 4, 4, 4);
+  orc_geometry_source_position(g, i, s4);
+  mat_mul(vpp2i, s4, sv, 4, 4, 1);
+  jp->src[0] = sv[0];
+  jp->src[1] = sv[1];
+  jp->src[2] = sv[2];
+}
+
+typedef struct
+{
+  int    main, dinf, dsup;
+  int    ns, fs;
+  double np_main, fp_main;
+  double residualB, residualE, stepx, stepy, curx, cury;
+  double stepmm_norm;
+  double minx, miny, maxx, maxy;
+  long   ox, oy, oz;
+} joseph_ray_t;
+
+/* Ray set-up shared by the forward and back projectors,
+ * include/rtkJosephForwardProjectionImageFilter.hxx:244-335 and
+ * include/rtkJosephBackProjectionImageFilter.hxx:127-201.
+ * forward != 0 selects the forward acceptance test.  Returns 1 if the ray is
+ * cast. */
+static int
+joseph_ray(const orc_image * vol, const joseph_proj_t * jp, double iu, double iv, double ik, int forward,
+           joseph_ray_t * r)
+{
+  double pix[3], dir[3], bmin[3], bmax[3];
+  for (int a = 0; a < 3; a++)
+    pix[a] = jp->pix2vol[a * 4 + 0] * iu + jp->pix2vol[a * 4 + 1] * iv + jp->pix2vol[a * 4 + 2] * ik +
+             jp->pix2vol[a * 4 + 3];
+  for (int a = 0; a < 3; a++)
+    dir[a] = -(pix[a] - jp->src[a]);
+  int mainDir = 0;
+  for (int a = 0; a < 3; a++)
+    if (fabs(dir[a]) > fabs(dir[mainDir]))
+      mainDir = a;
+  for (int a = 0; a < 3; a++)
+  {
+    bmin[a] = vol->index[a];
+    bmax[a] = vol->index[a] + vol->size[a] - 1;
+    bmax[a] *= 1. - DBL_EPSILON;
+  }
+  double infd = 0., supd = 0.;
+  int    hit = box_intersect(bmin, bmax, pix, dir, &infd, &supd);
+  if (forward)
+  {
+    if (infd < 0.)
+      infd = 0.;
+    if (supd > 1.)
+      supd = 1.;
+    if (!(hit && supd > 0. && infd <= 1. && supd > infd))
+      return 0;
+  }
+  else
+  {
+    if (!(hit && supd >= 0. && infd <= 1.))
+      return 0;
+    if (infd < 0.)
+      infd = 0.;
+    if (supd > 1.)
+      supd = 1.;
+  }
+  double np[3], fp[3];
+  for (int a = 0; a < 3; a++)
+  {
+    np[a] = pix[a] + infd * dir[a];
+    fp[a] = pix[a] + supd * dir[a];
+  }
+  r->main = mainDir;
+  r->ns = (int)rint(np[mainDir]);
+  r->fs = (int)rint(fp[mainDir]);
+  int dinf = (mainDir + 1) % 3, dsup = (mainDir + 2) % 3;
+  if (dinf > dsup)
+  {
+    int t = dinf;
+    dinf = dsup;
+    dsup = t;
+  }
+  r->dinf = dinf;
+  r->dsup = dsup;
+  r->minx = bmin[dinf];
+  r->miny = bmin[dsup];
+  r->maxx = bmax[dinf];
+  r->maxy = bmax[dsup];
+  const long offsets[3] = { 1, vol->size[0], (long)vol->size[0] * vol->size[1] };
+  r->ox = offsets[dinf];
+  r->oy = offsets[dsup];
+  r->oz = offsets[mainDir];
+  r->np_main = np[mainDir];
+  r->fp_main = fp[mainDir];
+  r->residualB = r->ns - np[mainDir];
+  r->residualE = fp[mainDir] - r->fs;
+  const double nrm = 1. / dir[mainDir];
+  r->stepx = dir[dinf] * nrm;
+  r->stepy = dir[dsup] * nrm;
+  if (np[mainDir] > fp[mainDir])
+  {
+    r->residualB *= -1;
+    r->residualE *= -1;
+    r->oz *= -1;
+    r->stepx *= -1;
+    r->stepy *= -1;
+  }
+  r->curx = np[dinf] + r->residualB * r->stepx;
+  r->cury = np[dsup] + r->residualB * r->stepy;
+  double smm[3];
+  smm[dinf] = vol->spacing[dinf] * r->stepx;
+  smm[dsup] = vol->spacing[dsup] * r->stepy;
+  smm[mainDir] = vol->spacing[mainDir];
+  r->stepmm_norm = sqrt(smm[0] * smm[0] + smm[1] * smm[1] + smm[2] * smm[2]);
+  return 1;
+}
+
+/* buffer offset of the absolute voxel index along one axis */
+static long
+clampl(long v, long lo, long hi)
+{
+  return v < lo ? lo : (v > hi ? hi : v);
+}
+
+/* Joseph bilinear (BilinearInterpolation / ...OnBorders, FP :443-543; BP
+ * :335-413).  Returns the four buffer offsets and weights of a sample at
+ * (x, y) in slice sl.  Indices are clamped into the buffer to guard rounding
+ * at the box faces (a no-op for the in-box samples RTK takes). */
+static void
+joseph_taps(const orc_image * vol, const joseph_ray_t * r, int sl, double x, double y, int border, long o[4],
+            double wgt[4])
+{
+  const int    ix = (int)floor(x), iy = (int)floor(y);
+  const double lx = x - ix, ly = y - iy, lxc = 1. - lx, lyc = 1. - ly;
+  const int    szx = vol->size[r->dinf], szy = vol->size[r->dsup];
+  const int    bx = vol->index[r->dinf], by = vol->index[r->dsup], bz = vol->index[r->main];
+  long         xi = ix, xs = ix + 1, yi = iy, ys = iy + 1;
+  if (border)
+  {
+    if (ix < r->minx)
+      xi = ix + 1;
+    if (iy < r->miny)
+      yi = iy + 1;
+    if (ix >= r->maxx)
+      xs = ix;
+    if (iy >= r->maxy)
+      ys = iy;
+  }
+  xi = clampl(xi - bx, 0, szx - 1);
+  xs = clampl(xs - bx, 0, szx - 1);
+  yi = clampl(yi - by, 0, szy - 1);
+  ys = clampl(ys - by, 0, szy - 1);
+  const long zo = (long)(sl - bz);
+  const long oz = labs(r->oz);
+  o[0] = zo * oz + xi * r->ox + yi * r->oy;
+  o[1] = zo * oz + xs * r->ox + yi * r->oy;
+  o[2] = zo * oz + xi * r->ox + ys * r->oy;
+  o[3] = zo * oz + xs * r->ox + ys * r->oy;
+  wgt[0] = lxc * lyc;
+  wgt[1] = lx * lyc;
+  wgt[2] = lxc * ly;
+  wgt[3] = lx * ly;
+}
+
+void
+orc_joseph_forward(const orc_geometry * g, const orc_image * vol, const double * vol_data, const orc_image * proj,
+                   const double * proj_in, double * proj_out, int nthreads)
+{
+  /* JosephForwardProjectionImageFilter::ThreadedGenerateData,
+   * include/rtkJosephForwardProjectionImageFilter.hxx:182-427 */
+  const int nu = proj->size[0], nv = proj->size[1], np = proj->size[2];
+  for (int s = 0; s < np; s++)
+  {
+    joseph_proj_t jp;
+    joseph_setup(g, vol, proj, proj->index[2] + s, &jp);
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 4)
+    for (int j = 0; j < nv; j++)
+      for (int i = 0; i < nu; i++)
+      {
+        const long   po = ((long)s * nv + j) * nu + i;
+        joseph_ray_t r;
+        if (!joseph_ray(vol, &jp, i + proj->index[0], j + proj->index[1], proj->index[2] + s, 1, &r))
+        {
+          proj_out[po] = proj_in[po];
+          continue;
+        }
+        const int dz = (r.np_main > r.fp_main) ? -1 : 1;
+        double    sum = 0.;
+        long      o[4];
+        double    w[4];
+        int       sl = r.ns;
+        double    x = r.curx, y = r.cury;
+        if (r.fs == r.ns)
+        {
+          joseph_taps(vol, &r, sl, x, y, 1, o, w);
+          sum += fabs(r.fp_main - r.np_main) *
+                 (w[0] * vol_data[o[0]] + w[2] * vol_data[o[2]] + w[1] * vol_data[o[1]] + w[3] * vol_data[o[3]]);
+        }
+        else
+        {
+          joseph_taps(vol, &r, sl, x, y, 1, o, w);
+          sum += (r.residualB + 0.5) *
+                 (w[0] * vol_data[o[0]] + w[2] * vol_data[o[2]] + w[1] * vol_data[o[1]] + w[3] * vol_data[o[3]]);
+          sl += dz;
+          x += r.stepx;
+          y += r.stepy;
+          const int nmid = abs(r.fs - r.ns) - 1;
+          for (int t = 0; t < nmid; t++)
+          {
+            joseph_taps(vol, &r, sl, x, y, 0, o, w);
+            sum += w[0] * vol_data[o[0]] + w[1] * vol_data[o[1]] + w[2] * vol_data[o[2]] + w[3] * vol_data[o[3]];
+            sl += dz;
+            x += r.stepx;
+            y += r.stepy;
+          }
+          joseph_taps(vol, &r, sl, x, y, 1, o, w);
+          sum += (r.residualE + 0.5) *
+                 (w[0] * vol_data[o[0]] + w[2] * vol_data[o[2]] + w[1] * vol_data[o[1]] + w[3] * vol_data[o[3]]);
+        }
+        proj_out[po] = proj_in[po] + sum * r.stepmm_norm;
+      }
+  }
+}
+
+void
+orc_joseph_back(const orc_geometry * g, const orc_image * vol, const double * vol_in, double * vol_out,
+                const orc_image * proj, const double * proj_data)
+{
+  /* JosephBackProjectionImageFilter::GenerateData,
+   * include/rtkJosephBackProjectionImageFilter.hxx:57-323 (single-threaded) */
+  const int nu = proj->size[0], nv = proj->size[1], np = proj->size[2];
+  if (vol_out != vol_in)
+    memcpy(vol_out, vol_in, sizeof(double) * npix(vol));
+  for (int s = 0; s < np; s++)
+  {
+    joseph_proj_t jp;
+    joseph_setup(g, vol, proj, proj->index[2] + s, &jp);
+    for (int j = 0; j < nv; j++)
+      for (int i = 0; i < nu; i++)
+      {
+        const double val = proj_data[((long)s * nv + j) * nu + i];
+        joseph_ray_t r;
+        if (!joseph_ray(vol, &jp, i + proj->index[0], j + proj->index[1], proj->index[2] + s, 0, &r))
+          continue;
+        const int    dz = (r.np_main > r.fp_main) ? -1 : 1;
+        long         o[4];
+        double       w[4];
+        int          sl = r.ns;
+        double       x = r.curx, y = r.cury;
+        const double c = val * r.stepmm_norm;
+        if (r.fs == r.ns)
+        {
+          joseph_taps(vol, &r, sl, x, y, 1, o, w);
+          const double f = c * fabs(r.fp_main - r.np_main);
+          for (int q = 0; q < 4; q++)
+            vol_out[o[q]] += f * w[q];
+        }
+        else
+        {
+          joseph_taps(vol, &r, sl, x, y, 1, o, w);
+          double f = c * (r.residualB + 0.5);
+          for (int q = 0; q < 4; q++)
+            vol_out[o[q]] += f * w[q];
+          sl += dz;
+          x += r.stepx;
+          y += r.stepy;
+          const int nmid = abs(r.fs - r.ns) - 1;
+          for (int t = 0; t < nmid; t++)
+          {
+            joseph_taps(vol, &r, sl, x, y, 0, o, w);
+            for (int q = 0; q < 4; q++)
+              vol_out[o[q]] += c * w[q];
+            sl += dz;
+            x += r.stepx;
+            y += r.stepy;
+          }
+          joseph_taps(vol, &r, sl, x, y, 1, o, w);
+          f = c * (r.residualE + 0.5);
+          for (int q = 0; q < 4; q++)
+            vol_out[o[q]] += f * w[q];
+        }
+      }
+  }
+}
+
+double
+orc_joseph_sample_count(const orc_geometry * g, const orc_image * vol, const orc_image * proj, int nthreads)
+{
+  const int nu = proj->size[0], nv = proj->size[1], np = proj->size[2];
+  double    total = 0.;
+  for (int s = 0; s < np; s++)
+  {
+    joseph_proj_t jp;
+    joseph_setup(g, vol, proj, proj->index[2] + s, &jp);
+    double acc = 0.;
+#pragma omp parallel for num_threads(nthreads) reduction(+ : acc) schedule(dynamic, 4)
+    for (int j = 0; j < nv; j++)
+      for (int i = 0; i < nu; i++)
+      {
+        joseph_ray_t r;
+        if (joseph_ray(vol, &jp, i + proj->index[0], j + proj->index[1], proj->index[2] + s, 1, &r))
+          acc += (r.fs == r.ns) ? 1. : (double)(abs(r.fs - r.ns) + 1);
+      }
+    total += acc;
+  }
+  return total;
+}
+
+/* ------------------------------------------------------------------------ */
+/* FDK weighting (include/rtkFDKWeightProjectionFilter.hxx:40-128)            */
+/* ------------------------------------------------------------------------ */
+void
+orc_fdk_weight(const orc_geometry * g, const orc_image * proj, const double * in, double * out)
+{
+  const int n = g->n;
+  double *  sang = (double *)malloc(sizeof(double) * (n > 0 ? n : 1));
+  double *  fac = (double *)malloc(sizeof(double) * (n > 0 ? n : 1));
+  double *  tilt = (double *)malloc(sizeof(double) * (n > 0 ? n : 1));
+  orc_geometry_source_angles(g, sang);
+  orc_geometry_angular_gaps(g, sang, fac);
+  orc_geometry_tilt_angles(g, tilt);
+  for (int k = 0; k < n; k++)
+  {
+    const double sdd = g->par[10 * k + P_SDD];
+    if (sdd == 0.)
+      fac[k] *= 0.5;
+    else
+    {
+      double sp[4];
+      orc_geometry_source_position(g, k, sp);
+      const double sid = g->par[10 * k + P_SID];
+      fac[k] *= fabs(sdd) / (2. * sid * sid);
+      fac[k] *= sqrt(sp[0] * sp[0] + sp[1] * sp[1] + sp[2] * sp[2]);
+    }
+  }
+  /* point base and increment from TransformIndexToPhysicalPoint */
+  double i2p[16], base[3], inc[3];
+  orc_index_to_physical(proj, i2p);
+  for (int a = 0; a < 3; a++)
+  {
+    base[a] = i2p[a * 4 + 3] + i2p[a * 4 + 0] * proj->index[0] + i2p[a * 4 + 1] * proj->index[1] +
+              i2p[a * 4 + 2] * proj->index[2];
+    inc[a] = i2p[a * 4 + 0] + i2p[a * 4 + 1] + i2p[a * 4 + 2];
+  }
+  const int nu = proj->size[0], nv = proj->size[1], np = proj->size[2];
+  for (int s = 0; s < np; s++)
+  {
+    const int      k = proj->index[2] + s;
+    const double * p = g->par + 10 * k;
+    const double   sdd = p[P_SDD];
+    const long     off = (long)s * nu * nv;
+    if (sdd != 0.)
+    {
+      double       py = base[1] + p[P_POY] - p[P_SOY];
+      const double cosa = cos(tilt[k]), sina = sin(tilt[k]), tana = tan(tilt[k]);
+      const double sid = p[P_SID], sdd2 = sdd * sdd, RD = sdd - sid;
+      const double numpart1 = sdd * (cosa + tana * sina);
+      const double sddtana = sdd * tana;
+      for (int j = 0; j < nv; j++, py += inc[1])
+      {
+        double       px = base[0] + p[P_POX] + tana * RD;
+        const double sdd2y2 = sdd2 + py * py;
+        for (int i = 0; i < nu; i++, px += inc[0])
+        {
+          const double denom = sqrt(sdd2y2 + pow(px - sddtana, 2.));
+          const double cosGamma = (numpart1 - px * sina) / denom;
+          out[off + (long)j * nu + i] = in[off + (long)j * nu + i] * fac[k] * cosGamma;
+        }
+      }
+    }
+    else
+      for (long q = 0; q < (long)nu * nv; q++)
+        out[off + q] = in[off + q] * fac[k];
+  }
+  free(sang);
+  free(fac);
+  free(tilt);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Parker short scan (include/rtkParkerShortScanImageFilter.hxx:41-209)      */
+/* ------------------------------------------------------------------------ */
+int
+orc_parker_weight(const orc_geometry * g, const orc_image * proj, double threshold, const double * in, double * out)
+{
+  const int  n = g->n;
+  const int  nu = proj->size[0], nv = proj->size[1], np = proj->size[2];
+  const long tot = npix(proj);
+  double *   ga = (double *)malloc(sizeof(double) * (n > 0 ? n : 1));
+  double *   gaps = (double *)malloc(sizeof(double) * (n > 0 ? n : 1));
+  orc_geometry_gantry_angles(g, ga);
+  orc_geometry_angular_gaps_with_next(g, ga, gaps);
+  int maxpos = 0;
+  for (int k = 1; k < n; k++)
+    if (gaps[k] > gaps[maxpos])
+      maxpos = k;
+  if (n < 1 || g->par[P_SDD] == 0. || gaps[maxpos] < threshold)
+  {
+    if (out != in)
+      memcpy(out, in, sizeof(double) * tot);
+    free(ga);
+    free(gaps);
+    return 0;
+  }
+  /* unique sorted angles (std::map keeps the first inserted index) */
+  angle_idx * s = sorted_angles(ga, n);
+  int         nu_ = 0;
+  for (int k = 0; k < n; k++)
+    if (nu_ == 0 || s[k].a != s[nu_ - 1].a)
+      s[nu_++] = s[k];
+  int last = 0;
+  for (int k = 0; k < nu_; k++)
+    if (s[k].a == ga[maxpos])
+      last = k;
+  const int first = (last + 1 == nu_) ? 0 : last + 1;
+  double    firstAngle = s[first].a, lastAngle = s[last].a;
+  if (lastAngle < firstAngle)
+    lastAngle += 2 * ORC_PI;
+  double delta = 0.5 * (lastAngle - firstAngle - ORC_PI);
+  delta = delta - 2 * ORC_PI * floor(delta / (2 * ORC_PI));
+  free(s);
+
+  for (int sl = 0; sl < np; sl++)
+  {
+    const int      k = proj->index[2] + sl;
+    const double * p = g->par + 10 * k;
+    const double   sox = p[P_SOX], sid = p[P_SID];
+    const double   invsid = 1. / sqrt(sid * sid + sox * sox);
+    double         beta = ga[k] - firstAngle;
+    if (beta < 0)
+      beta += 2 * ORC_PI;
+    for (int i = 0; i < nu; i++)
+    {
+      const double x = proj->origin[0] + proj->spacing[0] * (proj->index[0] + i);
+      const double l = orc_geometry_to_untilted(g, k, x);
+      const double alpha = atan(-1 * l * invsid);
+      double       w;
+      if (beta <= 2 * delta - 2 * alpha)
+        w = 2. * pow(sin((ORC_PI * beta) / (4 * (delta - alpha))), 2.);
+      else if (beta <= ORC_PI - 2 * alpha)
+        w = 2.;
+      else if (beta <= ORC_PI + 2 * delta)
+        w = 2. * pow(sin((ORC_PI * (ORC_PI + 2 * delta - beta)) / (4 * (delta + alpha))), 2.);
+      else
+        w = 0.;
+      for (int j = 0; j < nv; j++)
+      {
+        const long o = ((long)sl * nv + j) * nu + i;
+        out[o] = in[o] * w;
+      }
+    }
+  }
+  free(ga);
+  free(gaps);
+  return 1;
+}
+
+/* ------------------------------------------------------------------------ */
+/* displaced detector (include/rtkDisplacedDetectorImageFilter.hxx:83-323)   */
+/* ------------------------------------------------------------------------ */
+int
+orc_displaced_detector_region(const orc_geometry * g, const orc_image * proj, int pad, int * out_index0,
+                              int * out_size0, double * inf_corner, double * sup_corner)
+{
+  double i2p[16];
+  orc_index_to_physical(proj, i2p);
+  double inf = i2p[3] + i2p[0] * proj->index[0] + i2p[1] * proj->index[1] + i2p[2] * proj->index[2];
+  double sup = inf;
+  if (proj->spacing[0] < 0.)
+    inf += proj->spacing[0] * (proj->size[0] - 1);
+  else
+    sup += proj->spacing[0] * (proj->size[0] - 1);
+  double maxInf = -DBL_MAX, minSup = DBL_MAX;
+  for (int i = 0; i < g->n; i++)
+  {
+    const double a = orc_geometry_to_untilted(g, i, inf), b = orc_geometry_to_untilted(g, i, sup);
+    if (a > maxInf)
+      maxInf = a;
+    if (b < minSup)
+      minSup = b;
+  }
+  inf = maxInf;
+  sup = minSup;
+  *inf_corner = inf;
+  *sup_corner = sup;
+  *out_index0 = proj->index[0];
+  *out_size0 = proj->size[0];
+  if (inf > 0. || sup < 0.)
+    return -1;
+  if (fabs(inf + sup) < 0.1 * fabs(sup - inf))
+    return 0;
+  if (!pad)
+    return 1;
+  if (sup + inf > 0.)
+    *out_index0 = proj->index[0] - proj->size[0];
+  *out_size0 = 2 * proj->size[0];
+  return 1;
+}
+
+int
+orc_displaced_detector(const orc_geometry * g, const orc_image * proj, int pad, const double * in, double * out)
+{
+  int    oi0, os0;
+  double inf, sup;
+  int    st = orc_displaced_detector_region(g, proj, pad, &oi0, &os0, &inf, &sup);
+  if (st < 0)
+    return st;
+  const int nu = proj->size[0], nv = proj->size[1], np = proj->size[2];
+  if (st == 0)
+  {
+    memcpy(out, in, sizeof(double) * npix(proj));
+    return 0;
+  }
+  const double theta = (-inf < sup) ? -inf : sup;
+  const int    shift = proj->index[0] - oi0;
+  double *     w = (double *)malloc(sizeof(double) * nu);
+  for (int sl = 0; sl < np; sl++)
+  {
+    const int      k = proj->index[2] + sl;
+    const double * p = g->par + 10 * k;
+    const double   sx = p[P_SOX];
+    double         sid = p[P_SID];
+    sid = sqrt(sid * sid + sx * sx);
+    double invsid = 0., invden = 0.;
+    if (sid != 0.)
+    {
+      invsid = 1. / sid;
+      invden = 1. / (2. * atan(theta * invsid));
+    }
+    for (int i = 0; i < nu; i++)
+    {
+      const double x = proj->origin[0] + proj->spacing[0] * (proj->index[0] + i);
+      const double l = orc_geometry_to_untilted(g, k, x);
+      if (sup + inf > 0.)
+        w[i] = (l <= -theta) ? 0. : (l >= theta ? 2. : sin(ORC_PI * atan(l * invsid) * invden) + 1);
+      else
+        w[i] = (l <= -theta) ? 2. : (l >= theta ? 0. : 1 - sin(ORC_PI * atan(l * invsid) * invden));
+    }
+    for (int j = 0; j < nv; j++)
+    {
+      double *       orow = out + ((long)sl * nv + j) * os0;
+      const double * irow = in + ((long)sl * nv + j) * nu;
+      for (int i = 0; i < os0; i++)
+        orow[i] = 0.;
+      for (int i = 0; i < nu; i++)
+        orow[shift + i] = irow[i] * w[i];
+    }
+  }
+  free(w);
+  return 1;
+}
+
+/* ------------------------------------------------------------------------ */
+/* ramp filter                                                              */
+/* ------------------------------------------------------------------------ */
+static int
+is_prime(int n)
+{
+  int last = (int)sqrt((double)n);
+  for (int x = 2; x <= last; x++)
+    if (n % x == 0)
+      return 0;
+  return 1;
+}
+
+static int
+greatest_prime_factor(int n)
+{
+  /* FFTProjectionsConvolutionImageFilter::GreatestPrimeFactor, :322-333 */
+  int v = 2;
+  while (v <= n)
+    if (n % v == 0 && is_prime(v))
+      n /= v;
+    else
+      v += 1;
+  return v;
+}
+
+int
+orc_ramp_padded_size(int nu, const orc_ramp_params * p)
+{
+  /* GetPaddedImageRegion, include/rtkFFTProjectionsConvolutionImageFilter.hxx:280-306 */
+  int x = p->zero_pad_factor * nu;
+  while (greatest_prime_factor(x) > p->greatest_prime_factor)
+    x++;
+  return x;
+}
+
+/* complex DFT of length n in place (radix-2 when n is a power of two,
+ * direct O(n^2) otherwise); sign -1 forward, +1 inverse (unscaled) */
+static void
+dft(double * re, double * im, int n, int sign)
+{
+  if ((n & (n - 1)) == 0)
+  {
+    for (int i = 1, j = 0; i < n; i++)
+    {
+      int bit = n >> 1;
+      for (; j & bit; bit >>= 1)
+        j ^= bit;
+      j ^= bit;
+      if (i < j)
+      {
+        double t = re[i];
+        re[i] = re[j];
+        re[j] = t;
+        t = im[i];
+        im[i] = im[j];
+        im[j] = t;
+      }
+    }
+    for (int len = 2; len <= n; len <<= 1)
+    {
+      const double ang = sign * 2 * ORC_PI / len;
+      for (int i = 0; i < n; i += len)
+        for (int k = 0; k < len / 2; k++)
+        {
+          const double wr = cos(ang * k), wi = sin(ang * k);
+          const int    a = i + k, b = i + k + len / 2;
+          const double xr = re[b] * wr - im[b] * wi, xi = re[b] * wi + im[b] * wr;
+          re[b] = re[a] - xr;
+          im[b] = im[a] - xi;
+          re[a] += xr;
+          im[a] += xi;
+        }
+    }
+    return;
+  }
+  double * tr = (double *)malloc(sizeof(double) * n);
+  double * ti = (double *)malloc(sizeof(double) * n);
+  for (int k = 0; k < n; k++)
+  {
+    double sr = 0., si = 0.;
+    for (int t = 0; t < n; t++)
+    {
+      const double a = sign * 2 * ORC_PI * (double)(((long)k * t) % n) / n;
+      sr += re[t] * cos(a) - im[t] * sin(a);
+      si += re[t] * sin(a) + im[t] * cos(a);
+    }
+    tr[k] = sr;
+    ti[k] = si;
+  }
+  memcpy(re, tr, sizeof(double) * n);
+  memcpy(im, ti, sizeof(double) * n);
+  free(tr);
+  free(ti);
+}
+
+void
+orc_ramp_kernel(int padded, double spacing, const orc_ramp_params * p, double * kernel)
+{
+  /* FFTRampImageFilter::UpdateFFTProjectionsConvolutionKernel,
+   * include/rtkFFTRampImageFilter.hxx:47-178 (1-D kernel) */
+  double * re = (double *)calloc(padded, sizeof(double));
+  double * im = (double *)calloc(padded, sizeof(double));
+  re[0] = 1. / (4. * spacing);
+  for (int ix = 1, jx = padded - 1; ix < padded / 2; ix += 2, jx -= 2)
+  {
+    double v = ix * ORC_PI;
+    v = -1. / (v * v * spacing);
+    re[ix] = v;
+    re[jx] = v;
+  }
+  dft(re, im, padded, -1);
+  const int n = padded / 2 + 1;
+  for (int i = 0; i < n; i++)
+    kernel[i] = re[i];
+  int start_zero = n; /* index from which the kernel is zeroed */
+  if (p->hann_cut > 0.)
+  {
+    const int ncut = (int)floor(n * fmin(1.0, p->hann_cut) + 0.5);
+    for (int i = 0; i < ncut; i++)
+      kernel[i] *= 0.5 * (1 + cos(ORC_PI * i / ncut));
+    start_zero = ncut;
+  }
+  else if (p->cosine_cut > 0.)
+  {
+    const int ncut = (int)floor(n * fmin(1.0, p->cosine_cut) + 0.5);
+    for (int i = 0; i < ncut; i++)
+      kernel[i] *= cos(0.5 * ORC_PI * i / ncut);
+    start_zero = ncut;
+  }
+  else if (p->hamming > 0.)
+  {
+    const int ncut = (int)floor(n * fmin(1.0, p->hamming) + 0.5);
+    for (int i = 0; i < ncut; i++)
+      kernel[i] *= 0.54 + 0.46 * cos(ORC_PI * i / ncut);
+    start_zero = ncut;
+  }
+  else if (p->ramlak_cut > 0.)
+  {
+    start_zero = (int)floor(n * fmin(1.0, p->ramlak_cut) + 0.5);
+  }
+  else if (p->shepplogan_cut > 0.)
+  {
+    const int ncut = (int)floor(n * fmin(1.0, p->shepplogan_cut) + 0.5);
+    for (int i = 1; i < ncut; i++)
+    {
+      const double x = 0.5 * ORC_PI * i / ncut;
+      kernel[i] *= sin(x) / x;
+    }
+    start_zero = ncut < 1 ? 1 : ncut;
+  }
+  for (int i = start_zero; i < n; i++)
+    kernel[i] = 0.;
+  free(re);
+  free(im);
+}
+
+void
+orc_ramp_filter(const orc_image * proj, const orc_ramp_params * p, const double * in, double * out, int nthreads)
+{
+  /* FFTProjectionsConvolutionImageFilter::ThreadedGenerateData and
+   * PadInputImageRegion, include/rtkFFTProjectionsConvolutionImageFilter.hxx:121-276 */
+  const int nu = proj->size[0], nv = proj->size[1], np = proj->size[2];
+  const int padded = orc_ramp_padded_size(nu, p);
+  const int zeroext = (padded - nu) / 2;
+  int       next = (int)floor(p->truncation_correction * nu);
+  if (next > zeroext)
+    next = zeroext;
+  double * mw = (double *)malloc(sizeof(double) * (next + 1));
+  for (int i = 0; i < next + 1; i++)
+    mw[i] = pow(sin((next - i) * ORC_PI / (2 * next - 2)), 0.75);
+  double * K = (double *)malloc(sizeof(double) * (padded / 2 + 1));
+  orc_ramp_kernel(padded, proj->spacing[0], p, K);
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 8)
+  for (long row = 0; row < (long)nv * np; row++)
+  {
+    double *       re = (double *)calloc(padded, sizeof(double));
+    double *       im = (double *)calloc(padded, sizeof(double));
+    const double * r = in + row * nu;
+    /* padded buffer position q corresponds to input column q - zeroext */
+    for (int i = 0; i < nu; i++)
+      re[zeroext + i] = r[i];
+    if (next)
+    {
+      const double SA = r[1];
+      for (int b = 1; b <= next; b++)
+        re[zeroext - b] = mw[b] * (2.0 * SA - r[b]);
+      const double SE = r[nu - 1];
+      for (int b = 1; b <= next; b++)
+        re[zeroext + nu - 1 + b] = mw[b] * (2.0 * SE - r[nu - 1 - b]);
+    }
+    dft(re, im, padded, -1);
+    for (int f = 0; f < padded; f++)
+    {
+      const int    ff = f <= padded / 2 ? f : padded - f;
+      const double k = K[ff];
+      re[f] *= k;
+      im[f] *= k;
+    }
+    dft(re, im, padded, +1);
+    for (int i = 0; i < nu; i++)
+      out[row * nu + i] = re[zeroext + i] / padded;
+    free(re);
+    free(im);
+  }
+  free(K);
+  free(mw);
+}
+
+/* ------------------------------------------------------------------------ */
+/* conjugate gradient                                                       */
+/* ------------------------------------------------------------------------ */
+static void
+cg_apply_A(const orc_geometry * g, const orc_image * vol, const orc_image * proj, const double * weights,
+           double tikhonov, const double * x, double * out, double * ptmp, int nthreads)
+{
+  /* ReconstructionConjugateGradientOperator::GenerateData,
+   * include/rtkReconstructionConjugateGradientOperator.hxx:192-286 */
+  const long np = npix(proj), nvx = npix(vol);
+  memset(ptmp, 0, sizeof(double) * np);
+  orc_joseph_forward(g, vol, x, proj, ptmp, ptmp, nthreads);
+  if (weights)
+    for (long q = 0; q < np; q++)
+      ptmp[q] *= weights[q];
+  memset(out, 0, sizeof(double) * nvx);
+  orc_joseph_back(g, vol, out, out, proj, ptmp);
+  if (tikhonov != 0.)
+    for (long q = 0; q < nvx; q++)
+      out[q] += tikhonov * x[q];
+}
+
+void
+orc_cg_joseph(const orc_geometry * g, const orc_image * vol, const orc_image * proj, const double * proj_data,
+              const double * weights, double tikhonov, int niter, double * x, double * residuals, int nthreads)
+{
+  /* ConjugateGradientImageFilter::GenerateData,
+   * include/rtkConjugateGradientImageFilter.hxx:108-258, with FP64
+   * accumulators; b from ConjugateGradientConeBeamReconstructionFilter
+   * (include/rtkConjugateGradientConeBeamReconstructionFilter.hxx:223-244) */
+  const long np = npix(proj), nvx = npix(vol);
+  double *   ptmp = (double *)malloc(sizeof(double) * np);
+  double *   b = (double *)calloc(nvx, sizeof(double));
+  double *   R = (double *)malloc(sizeof(double) * nvx);
+  double *   P = (double *)malloc(sizeof(double) * nvx);
+  double *   AP = (double *)malloc(sizeof(double) * nvx);
+  for (long q = 0; q < np; q++)
+    ptmp[q] = proj_data[q] * (weights ? weights[q] : 1.);
+  orc_joseph_back(g, vol, b, b, proj, ptmp);
+  cg_apply_A(g, vol, proj, weights, tikhonov, x, AP, ptmp, nthreads);
+  for (long q = 0; q < nvx; q++)
+  {
+    R[q] = b[q] - AP[q];
+    P[q] = R[q];
+  }
+  const double eps = DBL_MIN;
+  double       rr = 0.;
+  for (long q = 0; q < nvx; q++)
+    rr += R[q] * R[q];
+  if (residuals)
+    residuals[0] = rr;
+  for (int it = 0; it < niter; it++)
+  {
+    cg_apply_A(g, vol, proj, weights, tikhonov, P, AP, ptmp, nthreads);
+    double num = 0., den = 0.;
+    for (long q = 0; q < nvx; q++)
+    {
+      num += R[q] * R[q];
+      den += P[q] * AP[q];
+    }
+    const double alpha = num / (den + eps);
+    for (long q = 0; q < nvx; q++)
+      x[q] += alpha * P[q];
+    den = num;
+    num = 0.;
+    for (long q = 0; q < nvx; q++)
+    {
+      R[q] -= alpha * AP[q];
+      num += R[q] * R[q];
+    }
+    const double beta = num / (den + eps);
+    for (long q = 0; q < nvx; q++)
+      P[q] = R[q] + beta * P[q];
+    if (residuals)
+      residuals[it + 1] = num;
+  }
+  free(ptmp);
+  free(b);
+  free(R);
+  free(P);
+  free(AP);
+}
+
+/* ------------------------------------------------------------------------ */
+/* phantoms                                                                 */
+/* ------------------------------------------------------------------------ */
+void
+orc_project_ellipsoids(const orc_geometry * g, const orc_image * proj, int n_ell, const double * ell,
+                       double * proj_out, int nthreads)
+{
+  /* analytic line integrals (RayConvexIntersectionImageFilter semantics,
+   * include/rtkRayConvexIntersectionImageFilter.hxx:57-84): for every pixel,
+   * sum over ellipsoids of density x chord length between source and pixel. */
+  const int nu = proj->size[0], nv = proj->size[1], np = proj->size[2];
+  double    pi2pp[16];
+  orc_index_to_physical(proj, pi2pp);
+  for (int s = 0; s < np; s++)
+  {
+    const int k = proj->index[2] + s;
+    double    p2f[16], T[16], src[4];
+    orc_geometry_proj_coords_to_fixed(g, k, p2f);
+    mat_mul(p2f, pi2pp, T, 4, 4, 4);
+    orc_geometry_source_position(g, k, src);
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 4)
+    for (int j = 0; j < nv; j++)
+      for (int i = 0; i < nu; i++)
+      {
+        const double ii = i + proj->index[0], jj = j + proj->index[1], kk = k;
+        double       pix[3], d[3];
+        for (int a = 0; a < 3; a++)
+        {
+          pix[a] = T[a * 4 + 0] * ii + T[a * 4 + 1] * jj + T[a * 4 + 2] * kk + T[a * 4 + 3];
+          d[a] = pix[a] - src[a];
+        }
+        const double len = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+        double       acc = 0.;
+        for (int e = 0; e < n_ell; e++)
+        {
+          const double * E = ell + 16 * e;
+          const double * R = E + 6;
+          double         o[3], dd[3], rel[3] = { src[0] - E[0], src[1] - E[1], src[2] - E[2] };
+          for (int a = 0; a < 3; a++)
+          {
+            /* local = R^T (world - c), scaled by 1/axis */
+            o[a] = (R[0 * 3 + a] * rel[0] + R[1 * 3 + a] * rel[1] + R[2 * 3 + a] * rel[2]) / E[3 + a];
+            dd[a] = (R[0 * 3 + a] * d[0] + R[1 * 3 + a] * d[1] + R[2 * 3 + a] * d[2]) / E[3 + a];
+          }
+          const double A = dd[0] * dd[0] + dd[1] * dd[1] + dd[2] * dd[2];
+          const double B = 2 * (o[0] * dd[0] + o[1] * dd[1] + o[2] * dd[2]);
+          const double C = o[0] * o[0] + o[1] * o[1] + o[2] * o[2] - 1.;
+          const double disc = B * B - 4 * A * C;
+          if (disc <= 0.)
+            continue;
+          const double sq = sqrt(disc);
+          double       t1 = (-B - sq) / (2 * A), t2 = (-B + sq) / (2 * A);
+          if (t1 < 0.)
+            t1 = 0.;
+          if (t2 > 1.)
+            t2 = 1.;
+          if (t2 > t1)
+            acc += E[15] * (t2 - t1) * len;
+        }
+        proj_out[((long)s * nv + j) * nu + i] = acc;
+      }
+  }
+}
+
+void
+orc_draw_ellipsoids(const orc_image * vol, int n_ell, const double * ell, double * vol_out, int nthreads)
+{
+  /* voxelised reference (DrawConvexImageFilter semantics,
+   * include/rtkDrawConvexImageFilter.hxx:54-57): density added where the voxel
+   * centre is inside */
+  const int nx = vol->size[0], ny = vol->size[1], nz = vol->size[2];
+  double    i2p[16];
+  orc_index_to_physical(vol, i2p);
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 1)
+  for (int k = 0; k < nz; k++)
+    for (int j = 0; j < ny; j++)
+      for (int i = 0; i < nx; i++)
+      {
+        const double x[3] = { i + vol->index[0], j + vol->index[1], k + vol->index[2] };
+        double       w[3];
+        for (int a = 0; a < 3; a++)
+          w[a] = i2p[a * 4 + 0] * x[0] + i2p[a * 4 + 1] * x[1] + i2p[a * 4 + 2] * x[2] + i2p[a * 4 + 3];
+        double acc = 0.;
+        for (int e = 0; e < n_ell; e++)
+        {
+          const double * E = ell + 16 * e;
+          const double * R = E + 6;
+          const double   rel[3] = { w[0] - E[0], w[1] - E[1], w[2] - E[2] };
+          double         q = 0.;
+          for (int a = 0; a < 3; a++)
+          {
+            const double l = (R[0 * 3 + a] * rel[0] + R[1 * 3 + a] * rel[1] + R[2 * 3 + a] * rel[2]) / E[3 + a];
+            q += l * l;
+          }
+          if (q <= 1.)
+            acc += E[15];
+        }
+        vol_out[((long)k * ny + j) * nx + i] = acc;
+      }
+}
+
+/* ------------------------------------------------------------------------ */
+/* timed CPU baseline: RTK's CPU FDK backprojector with RTK's data types     */
+/* ------------------------------------------------------------------------ */
+int
+orc_fdk_backproject_f32_rtk(const orc_geometry * g, const orc_image * vol, const orc_image * proj,
+                            const float * proj_data, float * vol_inout, int nthreads)
+{
+  /* FDKBackProjectionImageFilter::DynamicThreadedGenerateData with
+   * OptimizedBackprojectionY (include/rtkFDKBackProjectionImageFilter.hxx:52-148,
+   * 232-306), BackProjectionImageFilter::GetProjection transposing each
+   * projection per thread (include/rtkBackProjectionImageFilter.hxx:480-531).
+   * Returns -1 when a projection would take another path. */
+  const int nx = vol->size[0], ny = vol->size[1], nz = vol->size[2];
+  const int nu = proj->size[0], nv = proj->size[1], np = proj->size[2];
+  double *  mats = (double *)malloc(sizeof(double) * 12 * (np > 0 ? np : 1));
+  for (int s = 0; s < np; s++)
+    if (orc_bp_matrix(g, vol, proj, proj->index[2] + s, 1, mats + 12 * s) != 2)
+    {
+      free(mats);
+      return -1;
+    }
+  int bad = 0;
+#pragma omp parallel num_threads(nthreads)
+  {
+    int tid = 0, nt = 1;
+#ifdef _OPENMP
+    tid = omp_get_thread_num();
+    nt = omp_get_num_threads();
+#endif
+    const int k0 = (int)((long)nz * tid / nt), k1 = (int)((long)nz * (tid + 1) / nt);
+    float *   tp = (float *)malloc(sizeof(float) * (long)nu * nv);
+    if (!tp)
+    {
+#pragma omp atomic write
+      bad = 1;
+    }
+    else
+    {
+      for (int s = 0; s < np; s++)
+      {
+        /* transposed copy: tp[u][v] */
+        const float * pin = proj_data + (long)s * nu * nv;
+        for (int v = 0; v < nv; v++)
+          for (int u = 0; u < nu; u++)
+            tp[(long)u * nv + v] = pin[(long)v * nu + u];
+        /* transposed matrix: row0 = v-row, row1 = u-row */
+        const double * m = mats + 12 * s;
+        const double   t00 = m[4], t01 = m[5], t02 = m[6], t03 = m[7];
+        const double   t10 = m[0], t12 = m[2], t13 = m[3];
+        const double   t20 = m[8], t22 = m[10], t23 = m[11];
+        const int      psz0 = nv, psz1 = nu; /* transposed sizes */
+        const double   pidx0 = proj->index[1], pidx1 = proj->index[0];
+        for (int k = k0; k < k1; k++)
+        {
+          const int kk = k + vol->index[2];
+          for (int i = 0; i < nx; i++)
+          {
+            const int ii = i + vol->index[0];
+            int       jj = vol->index[1];
+            double    u = t00 * ii + t01 * jj + t02 * kk + t03;
+            double    v = t10 * ii + t12 * kk + t13;
+            double    w = t20 * ii + t22 * kk + t23;
+            w = 1 / w;
+            u = u * w - pidx0;
+            v = v * w - pidx1;
+            const double du = w * t01;
+            w *= w;
+            const int vi = (int)floor(v);
+            if (vi >= 0 && vi < psz1 - 1)
+            {
+              float * pv = vol_inout + ((long)k * ny) * nx + i;
+              for (int j = 0; j < ny; j++, pv += nx, u += du)
+              {
+                const int ui = (int)floor(u);
+                if (ui >= 0 && ui < psz0 - 1)
+                {
+                  const float * pp = tp + (long)vi * psz0 + ui;
+                  const double  v1 = v - vi, v2 = 1.0 - v1, u1 = u - ui, u2 = 1.0 - u1;
+                  *pv += w * (v2 * (u2 * pp[0] + u1 * pp[1]) + v1 * (u2 * pp[psz0] + u1 * pp[psz0 + 1]));
+                }
+              }
+            }
+          }
+        }
+      }
+      free(tp);
+    }
+  }
+  free(mats);
+  return bad ? -2 : 0;
+}

@@ -1,0 +1,101 @@
+"""ctypes binding of librtkb200.so (the C ABI declared in include/rtkb200.h).
+
+The library is built in-tree by ``rtk_b200.build``.  Loading fails loudly when
+it is missing: there is no CPU fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "librtkb200.so")
+HEADER_PATH = os.path.join(os.path.dirname(_PKG), "include", "rtkb200.h")
+
+RTKB_OK = 0
+RTKB_ERR_INVALID_ARGUMENT = 1
+RTKB_ERR_CUDA = 2
+RTKB_ERR_UNSUPPORTED = 3
+RTKB_ERR_TIMEOUT = 4
+RTKB_ERR_OUT_OF_MEMORY = 5
+
+
+class ImageDesc(C.Structure):
+    """rtkb_image_desc: itk::ImageBase metadata of a 3-D image."""
+
+    _fields_ = [
+        ("size", C.c_int * 3),
+        ("index", C.c_int * 3),
+        ("origin", C.c_double * 3),
+        ("spacing", C.c_double * 3),
+        ("direction", C.c_double * 9),
+    ]
+
+
+class RtkbError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"rtkb error {code}: {msg}")
+        self.code = code
+
+
+_D = C.POINTER(C.c_double)
+_I = C.POINTER(C.c_int)
+_F = C.POINTER(C.c_float)
+_V = C.c_void_p
+_G = C.c_void_p
+_IM = C.POINTER(ImageDesc)
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "rtkb_last_error": (C.c_char_p, []),
+    "rtkb_version": (C.c_char_p, []),
+    "rtkb_device_status": (C.c_int, [_V, _I]),
+    "rtkb_geometry_new": (_G, []),
+    "rtkb_geometry_free": (None, [_G]),
+    "rtkb_geometry_add_projection": (C.c_int, [_G] + [C.c_double] * 9),
+    "rtkb_geometry_add_projection_in_radians": (C.c_int, [_G] + [C.c_double] * 9),
+    "rtkb_geometry_number_of_projections": (C.c_int, [_G]),
+    "rtkb_geometry_get_matrix": (C.c_int, [_G, C.c_int, _D]),
+    "rtkb_geometry_get_source_position": (C.c_int, [_G, C.c_int, _D]),
+    "rtkb_geometry_get_projection_coordinates_to_fixed_system_matrix": (C.c_int, [_G, C.c_int, _D]),
+    "rtkb_geometry_get_parameters": (C.c_int, [_G, C.c_int, _D]),
+    "rtkb_geometry_to_untilted_coordinate_at_isocenter": (C.c_double, [_G, C.c_int, C.c_double]),
+    "rtkb_geometry_set_radius_cylindrical_detector": (C.c_int, [_G, C.c_double]),
+    "rtkb_backprojection_matrices": (C.c_int, [_G, _IM, _IM, C.c_int, C.c_int, C.c_int, _D, _I]),
+    "rtkb_fdk_backproject": (C.c_int, [_G, _IM, _IM, _V, _V, _V, _V]),
+    "rtkb_voxel_backproject": (C.c_int, [_G, _IM, _IM, _V, _V, _V, _V]),
+    "rtkb_backproject_matrices": (C.c_int, [_I, _I, C.c_int, _D, _I, C.c_int, _V, _V, _V, _V]),
+    "rtkb_probe_smem_gather": (C.c_int, [C.c_int, C.c_int, _V, _V]),
+}
+
+_lib = None
+
+
+def header_symbols() -> list[str]:
+    """Names of every function declared in include/rtkb200.h."""
+    txt = open(HEADER_PATH).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(rtkb_[a-z0-9_]+)\s*\(", txt)))
+
+
+def load(path: str = LIB_PATH):
+    """Load librtkb200.so and attach signatures; raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with `python -m rtk_b200.build` (no CPU fallback exists)")
+    L = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def check(code: int) -> None:
+    if code != RTKB_OK:
+        msg = load().rtkb_last_error()
+        raise RtkbError(code, msg.decode() if msg else "")

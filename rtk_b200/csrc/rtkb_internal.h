@@ -1,0 +1,91 @@
+// rtkb_internal.h -- shared host-side helpers of librtkb200 (not part of the ABI).
+#pragma once
+
+#include "rtkb200.h"
+
+#include <cmath>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+namespace rtkb
+{
+
+// ---- error reporting -------------------------------------------------------
+void         set_error(const std::string & msg);
+const char * g_last_error_cstr();
+void clear_error();
+int  fail(int code, const std::string & msg);
+int  cuda_fail(cudaError_t err, const char * what);
+
+#define RTKB_CUDA_TRY(expr)                                                                                            \
+  do                                                                                                                   \
+  {                                                                                                                    \
+    cudaError_t _e = (expr);                                                                                           \
+    if (_e != cudaSuccess)                                                                                             \
+      return ::rtkb::cuda_fail(_e, #expr);                                                                             \
+  } while (0)
+
+// ---- small FP64 matrix helpers (row-major) ----------------------------------
+struct Mat4
+{
+  double m[16];
+};
+
+void mat_mul(const double * a, const double * b, double * c, int n, int k, int m);
+void mat4_identity(double * m);
+bool affine4_inverse(const double * m, double * r);
+void index_to_physical(const rtkb_image_desc & im, double m[16]);
+bool physical_to_index(const rtkb_image_desc & im, double m[16]);
+bool desc_valid(const rtkb_image_desc * d, std::string & why);
+inline long long
+num_pixels(const rtkb_image_desc & d)
+{
+  return (long long)d.size[0] * d.size[1] * d.size[2];
+}
+
+// ---- geometry (rtk::ThreeDCircularProjectionGeometry) -----------------------
+struct Geometry
+{
+  struct Proj
+  {
+    double sid, sdd, gantry, pox, poy, oop, ip, sox, soy, source_angle;
+    double rot[16];  // 4x4 rotation (homogeneous)
+    double mag[12];  // 3x4 magnification
+    double srct[16]; // 4x4 source translation
+    double projt[9]; // 3x3 projection translation
+    double mat[12];  // 3x4 final projection matrix
+  };
+  std::vector<Proj> p;
+  double            radius_cylindrical = 0.;
+
+  int  add_projection_rad(double sid, double sdd, double ga, double pox, double poy, double oop, double ip,
+                          double sox, double soy);
+  void source_position(int i, double out[4]) const;
+  void proj_coords_to_fixed(int i, double out[16]) const;
+  void source_angles(std::vector<double> & out) const;
+  void gantry_angles(std::vector<double> & out) const;
+  void tilt_angles(std::vector<double> & out) const;
+  void angular_gaps(const std::vector<double> & angles, std::vector<double> & out) const;
+  void angular_gaps_with_next(const std::vector<double> & angles, std::vector<double> & out) const;
+  double to_untilted(int i, double tilted) const;
+};
+
+// Index-to-index backprojection matrix (volume index -> projection index),
+// untransposed; returns RTK's path (1 opt X, 2 opt Y, 0 generic).
+int bp_matrix(const Geometry & g, const rtkb_image_desc & vol, const rtkb_image_desc & proj, int i, bool fdk,
+              double m[12]);
+
+// Per-device library state: cached TMA encoder entry point.
+typedef int (*EncodeTiledFn)(void *, int, unsigned, void *, const unsigned long long *, const unsigned long long *,
+                             const unsigned *, const unsigned *, int, int, int, int);
+EncodeTiledFn tensor_map_encoder();
+
+} // namespace rtkb
+
+struct rtkb_geometry
+{
+  rtkb::Geometry g;
+};

@@ -119,6 +119,76 @@ int rtkb_backproject_matrices(const int vol_size[3], const int proj_size[3], int
                               const int * modes, int weighting, const float * d_proj, const float * d_vol_in,
                               float * d_vol_out, void * stream);
 
+/* ---- projection weighting and ramp filtering ----
+ * All take a projection stack description `proj` (slice s = geometry
+ * projection proj->index[2] + s) and float32 device buffers.  d_out may equal
+ * d_in except for the displaced-detector filter when it pads. */
+
+/* rtk::FDKWeightProjectionFilter (include/rtkFDKWeightProjectionFilter.hxx:40-128):
+ * angular-gap x ramp-scaling factor times cos(gamma), computed in FP64.
+ * Replaces CUDA_weight_projection. */
+int rtkb_fdk_weight(const rtkb_geometry * g, const rtkb_image_desc * proj, const float * d_in, float * d_out,
+                    void * stream);
+
+/* rtk::ParkerShortScanImageFilter (include/rtkParkerShortScanImageFilter.hxx:41-209);
+ * angular_gap_threshold in radians (RTK's default is pi/9).  *is_short_scan
+ * (may be NULL) receives 0 when the largest gap is below the threshold, in
+ * which case the projections are copied.  Replaces CUDA_parker_weight. */
+int rtkb_parker_short_scan(const rtkb_geometry * g, const rtkb_image_desc * proj, double angular_gap_threshold,
+                           const float * d_in, float * d_out, void * stream, int * is_short_scan);
+
+/* rtk::DisplacedDetectorImageFilter (include/rtkDisplacedDetectorImageFilter.hxx:83-323).
+ * _region computes the output image (x size doubled on the truncated side when
+ * pad_on_truncated_side and the detector is displaced) and *weighted; the
+ * filter writes that image.  Replaces CUDA_displaced_weight. */
+int rtkb_displaced_detector_region(const rtkb_geometry * g, const rtkb_image_desc * proj, int pad_on_truncated_side,
+                                   rtkb_image_desc * out, int * weighted);
+int rtkb_displaced_detector(const rtkb_geometry * g, const rtkb_image_desc * proj, int pad_on_truncated_side,
+                            const float * d_in, float * d_out, void * stream);
+
+/* Ramp filter parameters of rtk::FFTRampImageFilter (include/rtkFFTRampImageFilter.h)
+ * and rtk::FFTProjectionsConvolutionImageFilter: window cut frequencies (0 =
+ * off, first non-zero wins in this order), Ohnesorge truncation correction,
+ * greatest prime factor of the padded size (2 as in RTK built without FFTW;
+ * only 2 is accepted on the GPU) and zero-pad factor (2). */
+typedef struct rtkb_ramp_params
+{
+  double hann_cut;
+  double cosine_cut;
+  double hamming;
+  double ramlak_cut;
+  double shepplogan_cut;
+  double truncation_correction;
+  int    greatest_prime_factor;
+  int    zero_pad_factor;
+} rtkb_ramp_params;
+
+/* Padded FFT length for rows of nu pixels and, when kernel != NULL, the
+ * windowed frequency kernel (padded/2+1 FP64 values). */
+int rtkb_ramp_kernel(int nu, double spacing_u, const rtkb_ramp_params * params, int * padded, double * kernel);
+
+/* Row-wise ramp filtering: pad (and mirror), FFT, multiply, inverse FFT, crop
+ * -- a hand-written shared-memory FFT, two rows per complex transform.
+ * Replaces CUDA_padding + CUDA_fft_convolution + the crop filter. */
+int rtkb_ramp_filter(const rtkb_image_desc * proj, const rtkb_ramp_params * params, const float * d_in,
+                     float * d_out, void * stream);
+
+/* FDK projection preprocessing fused into one pass over the stack: displaced
+ * detector (optional), Parker short-scan weighting (optional), FDK weighting
+ * and ramp filtering.  `out` receives the filtered stack's description (the
+ * displaced detector may double its width); size d_out accordingly (query it
+ * with rtkb_displaced_detector_region when displaced != 0). */
+typedef struct rtkb_fdk_preprocess_params
+{
+  int              displaced_detector; /* 0 off, 1 on */
+  int              pad_on_truncated_side;
+  int              short_scan;          /* 0 off, 1 Parker weighting when the scan is short */
+  double           angular_gap_threshold;
+  rtkb_ramp_params ramp;
+} rtkb_fdk_preprocess_params;
+int rtkb_fdk_preprocess(const rtkb_geometry * g, const rtkb_image_desc * proj, const rtkb_fdk_preprocess_params * p,
+                        rtkb_image_desc * out, const float * d_in, float * d_out, void * stream);
+
 /* ---- measurement ----
  * Shared-memory gather peak (no reference counterpart): n_blocks CTAs of 256
  * threads each perform `iters` bilinear-footprint gathers (4 x 4 bytes) from

@@ -33,6 +33,33 @@ class ImageDesc(C.Structure):
     ]
 
 
+class RampParams(C.Structure):
+    """rtkb_ramp_params (rtk::FFTRampImageFilter settings)."""
+
+    _fields_ = [
+        ("hann_cut", C.c_double),
+        ("cosine_cut", C.c_double),
+        ("hamming", C.c_double),
+        ("ramlak_cut", C.c_double),
+        ("shepplogan_cut", C.c_double),
+        ("truncation_correction", C.c_double),
+        ("greatest_prime_factor", C.c_int),
+        ("zero_pad_factor", C.c_int),
+    ]
+
+
+class FdkPreprocessParams(C.Structure):
+    """rtkb_fdk_preprocess_params."""
+
+    _fields_ = [
+        ("displaced_detector", C.c_int),
+        ("pad_on_truncated_side", C.c_int),
+        ("short_scan", C.c_int),
+        ("angular_gap_threshold", C.c_double),
+        ("ramp", RampParams),
+    ]
+
+
 class RtkbError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"rtkb error {code}: {msg}")
@@ -67,6 +94,13 @@ SIGNATURES = {
     "rtkb_voxel_backproject": (C.c_int, [_G, _IM, _IM, _V, _V, _V, _V]),
     "rtkb_backproject_matrices": (C.c_int, [_I, _I, C.c_int, _D, _I, C.c_int, _V, _V, _V, _V]),
     "rtkb_probe_smem_gather": (C.c_int, [C.c_int, C.c_int, _V, _V]),
+    "rtkb_fdk_weight": (C.c_int, [_G, _IM, _V, _V, _V]),
+    "rtkb_parker_short_scan": (C.c_int, [_G, _IM, C.c_double, _V, _V, _V, _I]),
+    "rtkb_displaced_detector_region": (C.c_int, [_G, _IM, C.c_int, _IM, _I]),
+    "rtkb_displaced_detector": (C.c_int, [_G, _IM, C.c_int, _V, _V, _V]),
+    "rtkb_ramp_kernel": (C.c_int, [C.c_int, C.c_double, C.POINTER(RampParams), _I, _D]),
+    "rtkb_ramp_filter": (C.c_int, [_IM, C.POINTER(RampParams), _V, _V, _V]),
+    "rtkb_fdk_preprocess": (C.c_int, [_G, _IM, C.POINTER(FdkPreprocessParams), _IM, _V, _V, _V]),
 }
 
 _lib = None

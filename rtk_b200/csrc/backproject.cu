@@ -47,16 +47,32 @@ constexpr int kTZ = 16;
 constexpr int kConsumerWarps = 8;
 constexpr int kThreads = 32 * (kConsumerWarps + 1);
 constexpr int kStages = 4;
-constexpr int kHeaderBytes = 128;
+constexpr int kHeaderBytes = 256;
 
 struct __align__(16) StageHeader
 {
-  float4 a0;  // u numerator: A0x A0y A0z c0 (box-relative)
-  float4 a1;  // v numerator
-  float4 a2;  // w
-  float4 lim; // valid u range [x, y), valid v range [z, w) (box-relative)
-  int4   fl;  // flags, ub, vb, unused
+  float4 a0;    // u numerator: A0x A0y A0z c0 (box-relative)
+  float4 a1;    // v numerator
+  float4 a2;    // w
+  float4 lim;   // valid u range [x, y), valid v range [z, w) (box-relative)
+  int4   fl;    // flags, ub, vb, unused
+  double m[12]; // FP64 buffer-index matrix: boundary decisions and the slow path
 };
+static_assert(sizeof(StageHeader) <= kHeaderBytes, "stage header overflow");
+
+// Samples whose FP32 coordinate lies within kBand pixels of a detector bound
+// are accepted or rejected with FP64 arithmetic, so RTK's hard acceptance
+// test (0 <= floor(u) <= N-2) is decided as the FP64 CPU filters decide it.
+constexpr float kBand = 1e-3f;
+
+__device__ __forceinline__ bool
+accept_fp64(const double * m, int row, int X, int Y, int Z, int n)
+{
+  const double x = X, y = Y, z = Z;
+  const double rw = 1.0 / (m[8] * x + m[9] * y + m[10] * z + m[11]);
+  const double c = (m[row * 4 + 0] * x + m[row * 4 + 1] * y + m[row * 4 + 2] * z + m[row * 4 + 3]) * rw;
+  return c >= 0.0 && c < n - 1.0;
+}
 
 constexpr int kFlagFast = 1;
 constexpr int kFlagUInterior = 2;
@@ -134,7 +150,10 @@ bp_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const float * __restri
     // ------------------------------------------------------------- producer
     if (use_tma && lane == 0)
       prefetch_tensor_map(&tmap);
-    const int    x1 = min(x0 + kTX - 1, nx - 1), y1 = min(y0 + NYT - 1, ny - 1), z1 = min(z0 + kTZ - 1, nz - 1);
+    // Footprint of the whole tile, including voxels beyond a ragged volume
+    // edge: consumers compute (but never store) those y's, so their shared-
+    // memory taps must stay inside the box too.
+    const int    x1 = x0 + kTX - 1, y1 = y0 + NYT - 1, z1 = z0 + kTZ - 1;
     const int    c = lane & 7;
     const double X = (c & 1) ? x1 : x0, Y = (c & 2) ? y1 : y0, Z = (c & 4) ? z1 : z0;
     for (int p = 0; p < nproj; p++)
@@ -198,14 +217,9 @@ bp_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const float * __restri
           if (vmin - margin >= 0.0 && vmax + margin < nv - 1.0)
             flags |= kFlagVInterior;
         }
-        else
-        {
-          // slow path: consumers read the FP64 matrix from the box area
-          double * md = reinterpret_cast<double *>(box);
 #pragma unroll
-          for (int q = 0; q < 12; q++)
-            md[q] = m[q];
-        }
+        for (int q = 0; q < 12; q++)
+          h->m[q] = m[q];
         h->fl = make_int4(flags, ub, vb, 0);
       }
       if (fast && use_tma)
@@ -270,7 +284,13 @@ bp_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const float * __restri
         const float  v0 = fmaf(a1.x, fdx, fmaf(a1.z, fdz, a1.w)) * rw;
         const float  dv = a1.y * rw;
         const float  wt = FDKW ? rw * rw : 1.f;
-        const bool   uok = (fl.x & kFlagUInterior) || (u >= lim.x && u < lim.y);
+        bool         uok = true;
+        if (!(fl.x & kFlagUInterior))
+        {
+          uok = (u >= lim.x && u < lim.y);
+          if (fabsf(u - lim.x) < kBand || fabsf(u - lim.y) < kBand)
+            uok = accept_fp64(h->m, 0, X, y0, Z, nu); // u does not depend on y on this path
+        }
         if (uok)
         {
           const float   flu = floorf(u);
@@ -297,7 +317,10 @@ bp_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const float * __restri
             for (int j = 0; j < NYT; j++)
             {
               const float v = fmaf((float)j, dv, v0);
-              if (v >= lim.z && v < lim.w)
+              bool        vok = (v >= lim.z && v < lim.w);
+              if (fabsf(v - lim.z) < kBand || fabsf(v - lim.w) < kBand)
+                vok = accept_fp64(h->m, 1, X, y0 + j, Z, nv);
+              if (vok)
               {
                 const float   flv = floorf(v);
                 const float   fv = v - flv;
@@ -313,11 +336,10 @@ bp_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const float * __restri
       }
       else
       {
-        const double * md = reinterpret_cast<const double *>(box);
-        double         M[12];
+        double M[12];
 #pragma unroll
         for (int q = 0; q < 12; q++)
-          M[q] = md[q];
+          M[q] = h->m[q];
         slow_projection<NYT, FDKW>(M, proj, (long long)p * nu * nv, nu, nv, X, y0, Z, acc);
       }
     }
@@ -420,9 +442,9 @@ estimate_footprint(const std::vector<double> & mats, int nproj, int nx, int ny, 
           int       sign = 0;
           for (int c = 0; c < 8; c++)
           {
-            const double X = (c & 1) ? std::min(x0 + kTX - 1, nx - 1) : x0;
-            const double Y = (c & 2) ? std::min(y0 + nyt - 1, ny - 1) : y0;
-            const double Z = (c & 4) ? std::min(z0 + kTZ - 1, nz - 1) : z0;
+            const double X = (c & 1) ? x0 + kTX - 1 : x0;
+            const double Y = (c & 2) ? y0 + nyt - 1 : y0;
+            const double Z = (c & 4) ? z0 + kTZ - 1 : z0;
             const double w = m[8] * X + m[9] * Y + m[10] * Z + m[11];
             const int    sw = (w > 0.) ? 1 : ((w < 0.) ? -1 : 0);
             if (sw == 0 || (sign != 0 && sw != sign))

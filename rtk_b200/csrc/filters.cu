@@ -1,0 +1,557 @@
+// filters.cu -- projection-domain filters of the FDK pipeline on sm_100a.
+//
+// One pass over the projection stack applies, in RTK's order, the displaced-
+// detector weighting and padding (include/rtkDisplacedDetectorImageFilter.hxx),
+// the Parker short-scan weights (include/rtkParkerShortScanImageFilter.hxx),
+// the FDK cos(gamma) weighting (include/rtkFDKWeightProjectionFilter.hxx) and the
+// ramp filter (include/rtkFFTProjectionsConvolutionImageFilter.hxx:121-276 with
+// the kernel of include/rtkFFTRampImageFilter.hxx:47-178).
+//
+// The ramp filter is a hand-written shared-memory FFT: one CTA filters two
+// rows at once as the real and imaginary parts of one complex sequence (the
+// ramp kernel is real and even, so the two rows do not mix), zero-padded to
+// the power-of-two length RTK uses without FFTW.  Stockham radix-8 passes
+// (Govindaraju et al., SC08) with a final radix-4/2 pass; the inverse
+// transform is a forward transform of the conjugate.  Weights are computed in
+// FP64 (cos gamma) or from FP64 host tables (Parker, displaced detector); the
+// stack is read once and written once.
+#include "rtkb_filters.h"
+
+#include <cstring>
+
+namespace
+{
+
+constexpr int kMaxFFT = 8192;
+
+struct FilterArgs
+{
+  const float *  in;
+  float *        out;
+  const double * fdkp;  // kFdkWeightParams per projection, or null
+  const float *  colw;  // per (projection, output column) weight, or null
+  const float *  K;     // ramp kernel, N/2+1
+  const float2 * tw;    // twiddles e^{-2 pi i m/N}
+  const float *  mw;    // truncation mirror weights, next+1
+  int            nu_in, nu_out, nv, np, shift, N, next;
+};
+
+__device__ __forceinline__ float
+weighted_pixel(const FilterArgs & a, int s, int r, int c)
+{
+  const int ci = c - a.shift;
+  if (ci < 0 || ci >= a.nu_in)
+    return 0.f;
+  float v = __ldg(a.in + ((long long)s * a.nv + r) * a.nu_in + ci);
+  if (a.colw)
+    v *= __ldg(a.colw + (long long)s * a.nu_out + c);
+  if (a.fdkp)
+  {
+    const double * q = a.fdkp + (long long)s * rtkb::kFdkWeightParams;
+    double         w = q[0];
+    if (q[7] == 0.)
+    {
+      const double x = q[5] + c * q[8], y = q[6] + r * q[9];
+      const double dxs = x - q[3];
+      w *= (q[1] - x * q[2]) / sqrt(q[4] + y * y + dxs * dxs);
+    }
+    v = (float)(v * w);
+  }
+  return v;
+}
+
+__global__ void __launch_bounds__(256)
+weight_kernel(FilterArgs a)
+{
+  const long long n = (long long)a.nu_out * a.nv * a.np;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+  {
+    const int c = (int)(i % a.nu_out);
+    const int r = (int)((i / a.nu_out) % a.nv);
+    const int s = (int)(i / ((long long)a.nu_out * a.nv));
+    a.out[i] = weighted_pixel(a, s, r, c);
+  }
+}
+
+__device__ __forceinline__ float2
+cmul(float2 a, float2 b)
+{
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// d * e^{-2 pi i j / L} for the constant twiddles of a size-L (2, 4, 8) DFT
+__device__ __forceinline__ float2
+rot_const(float2 d, int j, int L)
+{
+  constexpr float c = 0.70710678118654752440f; // sqrt(1/2)
+  if (L == 2 || j == 0)
+    return d;
+  if (L == 4 || j == 2)
+    return make_float2(d.y, -d.x);
+  if (j == 1)
+    return make_float2(c * (d.x + d.y), c * (d.y - d.x));
+  return make_float2(c * (d.y - d.x), -c * (d.x + d.y));
+}
+
+// In-register forward DFT of size R (decimation in frequency), natural order out.
+template <int R>
+__device__ __forceinline__ void
+dft_reg(float2 (&v)[R])
+{
+#pragma unroll
+  for (int half = R / 2; half >= 1; half >>= 1)
+  {
+#pragma unroll
+    for (int i = 0; i < R; i += 2 * half)
+    {
+#pragma unroll
+      for (int j = 0; j < half; j++)
+      {
+        const float2 x = v[i + j], y = v[i + j + half];
+        v[i + j] = make_float2(x.x + y.x, x.y + y.y);
+        v[i + j + half] = rot_const(make_float2(x.x - y.x, x.y - y.y), j, 2 * half);
+      }
+    }
+  }
+  if (R == 4)
+  {
+    const float2 t = v[1];
+    v[1] = v[2];
+    v[2] = t;
+  }
+  else if (R == 8)
+  {
+    float2 t = v[1];
+    v[1] = v[4];
+    v[4] = t;
+    t = v[3];
+    v[3] = v[6];
+    v[6] = t;
+  }
+}
+
+// One Stockham pass: sub-transforms of length Ns become length Ns*R.
+template <int R>
+__device__ __forceinline__ void
+fft_pass(const float2 * __restrict__ src, float2 * __restrict__ dst, const float2 * __restrict__ tw, int N, int Ns)
+{
+  const int nb = N / R;
+  const int tstride = N / (Ns * R);
+  for (int j = threadIdx.x; j < nb; j += blockDim.x)
+  {
+    const int k = j & (Ns - 1);
+    float2    v[R];
+#pragma unroll
+    for (int r = 0; r < R; r++)
+      v[r] = src[j + r * nb];
+    if (Ns > 1)
+    {
+#pragma unroll
+      for (int r = 1; r < R; r++)
+        v[r] = cmul(v[r], __ldg(tw + k * r * tstride));
+    }
+    dft_reg<R>(v);
+    const int d = (j - k) * R + k;
+#pragma unroll
+    for (int r = 0; r < R; r++)
+      dst[d + r * Ns] = v[r];
+  }
+}
+
+// Full forward FFT of length N (power of two, >= 2); returns the buffer holding
+// the result (a or b).
+__device__ float2 *
+fft_forward(float2 * a, float2 * b, const float2 * tw, int N)
+{
+  float2 * src = a;
+  float2 * dst = b;
+  for (int Ns = 1; Ns < N;)
+  {
+    const int rem = N / Ns;
+    if (rem >= 8)
+    {
+      fft_pass<8>(src, dst, tw, N, Ns);
+      Ns *= 8;
+    }
+    else if (rem == 4)
+    {
+      fft_pass<4>(src, dst, tw, N, Ns);
+      Ns *= 4;
+    }
+    else
+    {
+      fft_pass<2>(src, dst, tw, N, Ns);
+      Ns *= 2;
+    }
+    __syncthreads();
+    float2 * t = src;
+    src = dst;
+    dst = t;
+  }
+  return src;
+}
+
+__global__ void
+ramp_fft_kernel(FilterArgs a)
+{
+  extern __shared__ float2 sbuf[];
+  float2 *  b0 = sbuf;
+  float2 *  b1 = sbuf + a.N;
+  const int rows = a.nv * a.np;
+  const int ra = 2 * blockIdx.x, rb = ra + 1;
+  const int N = a.N, nu = a.nu_out;
+  // load two weighted rows as one complex sequence, zero padded
+  for (int c = threadIdx.x; c < N; c += blockDim.x)
+  {
+    float x = 0.f, y = 0.f;
+    if (c < nu)
+    {
+      x = weighted_pixel(a, ra / a.nv, ra % a.nv, c);
+      if (rb < rows)
+        y = weighted_pixel(a, rb / a.nv, rb % a.nv, c);
+    }
+    b0[c] = make_float2(x, y);
+  }
+  __syncthreads();
+  if (a.next > 0)
+  {
+    // Ohnesorge mirror extrapolation (PadInputImageRegion :218-258): left
+    // values wrap to the end of the circular buffer.
+    const float2 SA = b0[1], SE = b0[nu - 1];
+    for (int bq = 1 + threadIdx.x; bq <= a.next; bq += blockDim.x)
+    {
+      const float  w = __ldg(a.mw + bq);
+      const float2 l = b0[bq], r = b0[nu - 1 - bq];
+      b0[N - bq] = make_float2(w * (2.f * SA.x - l.x), w * (2.f * SA.y - l.y));
+      b0[nu - 1 + bq] = make_float2(w * (2.f * SE.x - r.x), w * (2.f * SE.y - r.y));
+    }
+    __syncthreads();
+  }
+  float2 * X = fft_forward(b0, b1, a.tw, N);
+  float2 * other = (X == b0) ? b1 : b0;
+  // multiply by the real, even kernel and conjugate: the inverse transform is
+  // conj(FFT(conj(K X))) / N
+  for (int f = threadIdx.x; f < N; f += blockDim.x)
+  {
+    const float  k = __ldg(a.K + min(f, N - f));
+    const float2 z = X[f];
+    X[f] = make_float2(z.x * k, -z.y * k);
+  }
+  __syncthreads();
+  float2 *    W = fft_forward(X, other, a.tw, N);
+  const float inv = 1.f / (float)N;
+  for (int c = threadIdx.x; c < nu; c += blockDim.x)
+  {
+    const float2 z = W[c];
+    a.out[(long long)ra * nu + c] = z.x * inv;
+    if (rb < rows)
+      a.out[(long long)rb * nu + c] = -z.y * inv;
+  }
+}
+
+struct Options
+{
+  bool             displaced = false, pad = true, parker = false, fdk = false, ramp = false;
+  double           threshold = 3.14159265358979323846 / 9;
+  rtkb_ramp_params rp{};
+};
+
+template <typename T>
+static size_t
+append(std::vector<unsigned char> & blob, const std::vector<T> & v)
+{
+  size_t off = (blob.size() + 255) & ~size_t(255);
+  blob.resize(off + v.size() * sizeof(T));
+  if (!v.empty())
+    std::memcpy(blob.data() + off, v.data(), v.size() * sizeof(T));
+  return off;
+}
+
+int
+run_filters(const rtkb_geometry * g, const rtkb_image_desc * in, const Options & o, rtkb_image_desc * out_desc,
+            const float * d_in, float * d_out, cudaStream_t st, int * is_short)
+{
+  using namespace rtkb;
+  std::string why;
+  if (!g)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "Geometry has not been set.");
+  if (!desc_valid(in, why))
+    return fail(RTKB_ERR_INVALID_ARGUMENT, why);
+  const Geometry & G = g->g;
+  if (in->index[2] < 0 || (long long)in->index[2] + in->size[2] > (long long)G.p.size())
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "Mismatch between the number of projections and the geometry entries.");
+  if (o.displaced && (G.radius_cylindrical != 0. || (!G.p.empty() && G.p[0].sdd == 0.)))
+    return fail(RTKB_ERR_UNSUPPORTED, "Displaced detector cannot handle cylindrical detector or parallel geometry");
+
+  rtkb_image_desc    out = *in;
+  int                shift = 0;
+  std::vector<float> wd, wp, colw;
+  if (o.displaced)
+  {
+    DisplacedInfo info;
+    int           rc = displaced_region(G, *in, o.pad, info);
+    if (rc != RTKB_OK)
+      return rc;
+    if (info.weighted)
+    {
+      out = info.out;
+      shift = info.shift;
+      displaced_weights(G, *in, info, wd);
+    }
+  }
+  bool short_scan = false;
+  if (o.parker)
+    short_scan = parker_weights(G, out, o.threshold, wp);
+  if (is_short)
+    *is_short = short_scan ? 1 : 0;
+  if (out_desc)
+    *out_desc = out;
+  const int nu_in = in->size[0], nu_out = out.size[0], nv = in->size[1], np = in->size[2];
+  if (!d_in || !d_out)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "null buffer");
+  if (d_in == d_out && nu_out != nu_in)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "the padded displaced-detector output cannot be computed in place");
+  if (!wd.empty() || short_scan)
+  {
+    colw.assign((size_t)np * nu_out, 1.f);
+    for (int s = 0; s < np; s++)
+      for (int c = 0; c < nu_out; c++)
+      {
+        float       w = 1.f;
+        const int   ci = c - shift;
+        if (!wd.empty())
+          w *= (ci >= 0 && ci < nu_in) ? wd[(size_t)s * nu_in + ci] : 0.f;
+        if (short_scan)
+          w *= wp[(size_t)s * nu_out + c];
+        colw[(size_t)s * nu_out + c] = w;
+      }
+  }
+  std::vector<double> fdkp;
+  if (o.fdk)
+    fdk_weight_params(G, out, fdkp);
+
+  FilterArgs a{};
+  a.nu_in = nu_in;
+  a.nu_out = nu_out;
+  a.nv = nv;
+  a.np = np;
+  a.shift = shift;
+  std::vector<float> K, tw, mw;
+  if (o.ramp)
+  {
+    if (o.rp.greatest_prime_factor != 2 && o.rp.greatest_prime_factor != 0)
+      return fail(RTKB_ERR_UNSUPPORTED, "the GPU ramp filter pads to powers of two (greatest prime factor 2)");
+    const int N = ramp_padded_size(nu_out, o.rp);
+    if ((N & (N - 1)) != 0 || N > kMaxFFT || N < 2)
+      return fail(RTKB_ERR_UNSUPPORTED, "padded row length must be a power of two <= 8192");
+    std::vector<double> Kd;
+    ramp_kernel(N, out.spacing[0], o.rp, Kd);
+    K.assign(Kd.begin(), Kd.end());
+    twiddles(N, tw);
+    int next = (int)std::floor(o.rp.truncation_correction * nu_out);
+    next = std::min(next, (N - nu_out) / 2);
+    if (next == 1)
+      return fail(RTKB_ERR_INVALID_ARGUMENT, "truncation correction extent of one pixel is undefined");
+    if (next > 0)
+      truncation_mirror_weights(next, mw);
+    a.N = N;
+    a.next = next;
+  }
+  std::vector<unsigned char> blob;
+  const size_t               o_fdk = append(blob, fdkp), o_colw = append(blob, colw), o_K = append(blob, K),
+               o_tw = append(blob, tw), o_mw = append(blob, mw);
+  void * scratch = nullptr;
+  if (!blob.empty())
+    RTKB_CUDA_TRY(cudaMallocAsync(&scratch, blob.size(), st));
+  int rc = RTKB_OK;
+  do
+  {
+    if (scratch)
+    {
+      cudaError_t e = cudaMemcpyAsync(scratch, blob.data(), blob.size(), cudaMemcpyHostToDevice, st);
+      if (e != cudaSuccess)
+      {
+        rc = cuda_fail(e, "cudaMemcpyAsync");
+        break;
+      }
+    }
+    auto at = [&](size_t off, bool present) -> const void * {
+      return present ? static_cast<const void *>(static_cast<char *>(scratch) + off) : nullptr;
+    };
+    a.in = d_in;
+    a.out = d_out;
+    a.fdkp = static_cast<const double *>(at(o_fdk, !fdkp.empty()));
+    a.colw = static_cast<const float *>(at(o_colw, !colw.empty()));
+    a.K = static_cast<const float *>(at(o_K, !K.empty()));
+    a.tw = static_cast<const float2 *>(at(o_tw, !tw.empty()));
+    a.mw = static_cast<const float *>(at(o_mw, !mw.empty()));
+    if (o.ramp)
+    {
+      const long long pairs = ((long long)nv * np + 1) / 2;
+      const int       threads = std::min(512, std::max(64, a.N / 8));
+      const size_t    smem = 2 * (size_t)a.N * sizeof(float2);
+      cudaError_t     e = cudaFuncSetAttribute(ramp_fft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e == cudaSuccess && pairs > 0x7fffffffLL)
+        e = cudaErrorInvalidValue;
+      if (e == cudaSuccess)
+      {
+        ramp_fft_kernel<<<(unsigned)pairs, threads, smem, st>>>(a);
+        e = cudaGetLastError();
+      }
+      if (e != cudaSuccess)
+        rc = cuda_fail(e, "ramp_fft_kernel launch");
+    }
+    else
+    {
+      const long long n = (long long)nu_out * nv * np;
+      const long long blocks = std::min<long long>((n + 255) / 256, 148LL * 32);
+      weight_kernel<<<(unsigned)blocks, 256, 0, st>>>(a);
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess)
+        rc = cuda_fail(e, "weight_kernel launch");
+    }
+  } while (0);
+  if (scratch)
+  {
+    cudaError_t fe = cudaFreeAsync(scratch, st);
+    if (rc == RTKB_OK && fe != cudaSuccess)
+      rc = cuda_fail(fe, "cudaFreeAsync");
+  }
+  return rc;
+}
+
+template <typename F>
+int
+guarded(F && f)
+{
+  try
+  {
+    return f();
+  }
+  catch (...)
+  {
+    return rtkb::fail(RTKB_ERR_OUT_OF_MEMORY, "host allocation failed");
+  }
+}
+
+} // namespace
+
+extern "C" int
+rtkb_fdk_weight(const rtkb_geometry * g, const rtkb_image_desc * proj, const float * d_in, float * d_out,
+                void * stream)
+{
+  return guarded([&] {
+    Options o;
+    o.fdk = true;
+    return run_filters(g, proj, o, nullptr, d_in, d_out, static_cast<cudaStream_t>(stream), nullptr);
+  });
+}
+
+extern "C" int
+rtkb_parker_short_scan(const rtkb_geometry * g, const rtkb_image_desc * proj, double threshold, const float * d_in,
+                       float * d_out, void * stream, int * is_short_scan)
+{
+  return guarded([&] {
+    if (!std::isfinite(threshold))
+      return rtkb::fail(RTKB_ERR_INVALID_ARGUMENT, "invalid angular gap threshold");
+    Options o;
+    o.parker = true;
+    o.threshold = threshold;
+    return run_filters(g, proj, o, nullptr, d_in, d_out, static_cast<cudaStream_t>(stream), is_short_scan);
+  });
+}
+
+extern "C" int
+rtkb_displaced_detector_region(const rtkb_geometry * g, const rtkb_image_desc * proj, int pad, rtkb_image_desc * out,
+                               int * weighted)
+{
+  return guarded([&] {
+    std::string why;
+    if (!g || !out)
+      return rtkb::fail(RTKB_ERR_INVALID_ARGUMENT, "null argument");
+    if (!rtkb::desc_valid(proj, why))
+      return rtkb::fail(RTKB_ERR_INVALID_ARGUMENT, why);
+    rtkb::DisplacedInfo info;
+    int                 rc = rtkb::displaced_region(g->g, *proj, pad != 0, info);
+    if (rc != RTKB_OK)
+      return rc;
+    *out = info.weighted ? info.out : *proj;
+    if (weighted)
+      *weighted = info.weighted ? 1 : 0;
+    return RTKB_OK;
+  });
+}
+
+extern "C" int
+rtkb_displaced_detector(const rtkb_geometry * g, const rtkb_image_desc * proj, int pad, const float * d_in,
+                        float * d_out, void * stream)
+{
+  return guarded([&] {
+    Options o;
+    o.displaced = true;
+    o.pad = pad != 0;
+    return run_filters(g, proj, o, nullptr, d_in, d_out, static_cast<cudaStream_t>(stream), nullptr);
+  });
+}
+
+extern "C" int
+rtkb_ramp_kernel(int nu, double spacing, const rtkb_ramp_params * p, int * padded, double * kernel)
+{
+  return guarded([&] {
+    if (nu <= 0 || !p || !padded || !std::isfinite(spacing) || spacing == 0.)
+      return rtkb::fail(RTKB_ERR_INVALID_ARGUMENT, "invalid ramp kernel arguments");
+    const int N = rtkb::ramp_padded_size(nu, *p);
+    *padded = N;
+    if (kernel)
+    {
+      if ((N & (N - 1)) != 0)
+        return rtkb::fail(RTKB_ERR_UNSUPPORTED, "kernel evaluation needs a power-of-two padded size");
+      std::vector<double> K;
+      rtkb::ramp_kernel(N, spacing, *p, K);
+      std::copy(K.begin(), K.end(), kernel);
+    }
+    return RTKB_OK;
+  });
+}
+
+extern "C" int
+rtkb_ramp_filter(const rtkb_image_desc * proj, const rtkb_ramp_params * p, const float * d_in, float * d_out,
+                 void * stream)
+{
+  return guarded([&] {
+    if (!p)
+      return rtkb::fail(RTKB_ERR_INVALID_ARGUMENT, "null ramp parameters");
+    std::string why;
+    if (!rtkb::desc_valid(proj, why))
+      return rtkb::fail(RTKB_ERR_INVALID_ARGUMENT, why);
+    // the ramp needs no geometry: use a placeholder with enough projections
+    rtkb_geometry g;
+    const int     total = proj->index[2] + proj->size[2];
+    if (proj->index[2] < 0)
+      return rtkb::fail(RTKB_ERR_INVALID_ARGUMENT, "negative projection index");
+    g.g.p.resize(total);
+    Options o;
+    o.ramp = true;
+    o.rp = *p;
+    return run_filters(&g, proj, o, nullptr, d_in, d_out, static_cast<cudaStream_t>(stream), nullptr);
+  });
+}
+
+extern "C" int
+rtkb_fdk_preprocess(const rtkb_geometry * g, const rtkb_image_desc * proj, const rtkb_fdk_preprocess_params * p,
+                    rtkb_image_desc * out, const float * d_in, float * d_out, void * stream)
+{
+  return guarded([&] {
+    if (!p)
+      return rtkb::fail(RTKB_ERR_INVALID_ARGUMENT, "null preprocessing parameters");
+    Options o;
+    o.displaced = p->displaced_detector != 0;
+    o.pad = p->pad_on_truncated_side != 0;
+    o.parker = p->short_scan != 0;
+    o.threshold = p->angular_gap_threshold > 0. ? p->angular_gap_threshold : 3.14159265358979323846 / 9;
+    o.fdk = true;
+    o.ramp = true;
+    o.rp = p->ramp;
+    return run_filters(g, proj, o, out, d_in, d_out, static_cast<cudaStream_t>(stream), nullptr);
+  });
+}

@@ -1,0 +1,35 @@
+// rtkb_filters.h -- internal declarations of the projection-domain filters
+// (FDK weighting, Parker, displaced detector, ramp).
+#pragma once
+
+#include "rtkb_internal.h"
+
+namespace rtkb
+{
+
+// Per-projection FDK weighting parameters (FP64):
+// [0] factor, [1] numpart1, [2] sin(tilt), [3] sdd*tan(tilt), [4] sdd^2,
+// [5] x of column 0, [6] y of row 0, [7] parallel flag, [8] x step, [9] y step.
+constexpr int kFdkWeightParams = 10;
+void fdk_weight_params(const Geometry & g, const rtkb_image_desc & proj, std::vector<double> & out);
+
+// Parker weights per (projection, column); false when the scan is not short.
+bool parker_weights(const Geometry & g, const rtkb_image_desc & proj, double threshold, std::vector<float> & w);
+
+struct DisplacedInfo
+{
+  rtkb_image_desc out; // output image (x doubled on the truncated side when padded)
+  bool            weighted;
+  int             shift; // output column of input column 0
+  double          inf, sup;
+};
+int  displaced_region(const Geometry & g, const rtkb_image_desc & proj, bool pad, DisplacedInfo & info);
+void displaced_weights(const Geometry & g, const rtkb_image_desc & proj, const DisplacedInfo & info,
+                       std::vector<float> & w);
+
+int  ramp_padded_size(int nu, const rtkb_ramp_params & p);
+void ramp_kernel(int padded, double spacing, const rtkb_ramp_params & p, std::vector<double> & K);
+void twiddles(int n, std::vector<float> & tw);
+void truncation_mirror_weights(int next, std::vector<float> & mw);
+
+} // namespace rtkb

@@ -60,6 +60,100 @@ def voxel_backproject(geometry, vol_desc, proj_desc, proj, vol_in, out=None, str
     return _backproject(load().rtkb_voxel_backproject, geometry, vol_desc, proj_desc, proj, vol_in, out, stream)
 
 
+def ramp_params(hann=0.0, cosine=0.0, hamming=0.0, ramlak=0.0, shepplogan=0.0, truncation=0.0, gpf=2, pad=2):
+    from ._capi import RampParams
+
+    p = RampParams()
+    p.hann_cut, p.cosine_cut, p.hamming = hann, cosine, hamming
+    p.ramlak_cut, p.shepplogan_cut, p.truncation_correction = ramlak, shepplogan, truncation
+    p.greatest_prime_factor, p.zero_pad_factor = gpf, pad
+    return p
+
+
+def _unary(fn, desc, inp, out, out_shape=None):
+    torch = _torch()
+    _check_shape(inp, desc, "projections")
+    if out is None:
+        out = torch.empty(out_shape or tuple(inp.shape), device=inp.device, dtype=torch.float32)
+    return out
+
+
+def fdk_weight(geometry, proj_desc, proj, out=None, stream=None):
+    """rtk::FDKWeightProjectionFilter."""
+    out = _unary(None, proj_desc, proj, out)
+    check(load().rtkb_fdk_weight(geometry.handle, C.byref(proj_desc), _ptr(proj), _ptr(out), _stream(stream)))
+    return out
+
+
+def parker_short_scan(geometry, proj_desc, proj, threshold=3.141592653589793 / 9, out=None, stream=None):
+    """rtk::ParkerShortScanImageFilter; returns (out, is_short_scan)."""
+    out = _unary(None, proj_desc, proj, out)
+    short = C.c_int(0)
+    check(load().rtkb_parker_short_scan(geometry.handle, C.byref(proj_desc), threshold, _ptr(proj), _ptr(out),
+                                        _stream(stream), C.byref(short)))
+    return out, bool(short.value)
+
+
+def displaced_detector_region(geometry, proj_desc, pad=True):
+    from ._capi import ImageDesc
+
+    out = ImageDesc()
+    w = C.c_int(0)
+    check(load().rtkb_displaced_detector_region(geometry.handle, C.byref(proj_desc), int(pad), C.byref(out),
+                                                C.byref(w)))
+    return out, bool(w.value)
+
+
+def displaced_detector(geometry, proj_desc, proj, pad=True, stream=None):
+    """rtk::DisplacedDetectorImageFilter; returns (out, out_desc)."""
+    od, _ = displaced_detector_region(geometry, proj_desc, pad)
+    out = _unary(None, proj_desc, proj, None, shape_of(od))
+    check(load().rtkb_displaced_detector(geometry.handle, C.byref(proj_desc), int(pad), _ptr(proj), _ptr(out),
+                                         _stream(stream)))
+    return out, od
+
+
+def ramp_kernel(nu, spacing, params):
+    import numpy as np
+
+    padded = C.c_int(0)
+    check(load().rtkb_ramp_kernel(nu, spacing, C.byref(params), C.byref(padded), None))
+    k = np.zeros(padded.value // 2 + 1)
+    check(load().rtkb_ramp_kernel(nu, spacing, C.byref(params), C.byref(padded),
+                                  k.ctypes.data_as(C.POINTER(C.c_double))))
+    return padded.value, k
+
+
+def ramp_filter(proj_desc, proj, params=None, out=None, stream=None):
+    """rtk::FFTRampImageFilter (row-wise ramp filtering)."""
+    params = params or ramp_params()
+    out = _unary(None, proj_desc, proj, out)
+    check(load().rtkb_ramp_filter(C.byref(proj_desc), C.byref(params), _ptr(proj), _ptr(out), _stream(stream)))
+    return out
+
+
+def fdk_preprocess(geometry, proj_desc, proj, ramp=None, displaced=False, pad=True, short_scan=False,
+                   threshold=3.141592653589793 / 9, stream=None):
+    """Displaced detector + Parker + FDK weighting + ramp in one pass.
+    Returns (filtered stack, its description)."""
+    from ._capi import FdkPreprocessParams
+
+    p = FdkPreprocessParams()
+    p.displaced_detector, p.pad_on_truncated_side, p.short_scan = int(displaced), int(pad), int(short_scan)
+    p.angular_gap_threshold = threshold
+    p.ramp = ramp or ramp_params()
+    od = proj_desc
+    if displaced:
+        od, _ = displaced_detector_region(geometry, proj_desc, pad)
+    out = _unary(None, proj_desc, proj, None, shape_of(od))
+    from ._capi import ImageDesc
+
+    got = ImageDesc()
+    check(load().rtkb_fdk_preprocess(geometry.handle, C.byref(proj_desc), C.byref(p), C.byref(got), _ptr(proj),
+                                     _ptr(out), _stream(stream)))
+    return out, got
+
+
 def device_status(stream=None) -> int:
     """Synchronises the stream and returns (and clears) the kernels' status word."""
     st = C.c_int(0)

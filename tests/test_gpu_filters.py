@@ -1,0 +1,162 @@
+"""GPU parity of the projection-domain filters (FDK weighting, Parker short
+scan, displaced detector, ramp filter and their fused form) against the FP64
+oracle.  The irregular 4-projection geometry and the 1e-5 / 95 dB thresholds
+are those of RTK's CPU-vs-CUDA comparisons (test/rtkfdkprojweightcompcudatest.cxx:37-75,
+test/rtkshortscancompcudatest.cxx, test/rtkdisplaceddetectorcompcudatest.cxx)."""
+import numpy as np
+import pytest
+
+from tests import phantoms
+from tests.gpu_util import REL_L2_TOL, pair_geometry, pair_image, rel_l2, to_gpu, to_np
+
+pytestmark = pytest.mark.gpu
+
+IRREGULAR = [(600., 700., 0., 84., 35, 23, 15, 21, 26), (500., 800., 45., 21., 12, 16, 546, 14, 41),
+             (700., 900., 90., 68., 68, 54, 38, 35, 56), (900., 1000., 135., 48., 35, 84, 10, 84, 59)]
+
+
+def _sl_projections(oracle, go, po):
+    return oracle.project_ellipsoids(go, po, phantoms.shepp_logan(116.0))
+
+
+def _rtk_cuda_cpu_check(got, ref):
+    err, psnr, ok = phantoms.check_image_quality(got, ref, 1e-5, 95.0, 1.0)
+    assert ok, (err, psnr)
+
+
+def test_fdk_weight_irregular_geometry(rtkb, oracle):
+    gl, go = pair_geometry(rtkb, oracle, IRREGULAR)
+    pd, po = pair_image(rtkb, oracle, (128, 4, 4), (2.0, 2.0, 2.0), origin=(-127.0, -3.0, 0.0))
+    p = _sl_projections(oracle, go, po).astype(np.float32).astype(np.float64)
+    ref = oracle.fdk_weight(go, po, p)
+    got = to_np(rtkb.ops.fdk_weight(gl, pd, to_gpu(p)))
+    assert rel_l2(got, ref) < 1e-6
+    _rtk_cuda_cpu_check(got, ref)
+
+
+def test_fdk_weight_in_place_and_subset_index(rtkb, oracle):
+    params = [(1000.0, 1536.0, i * 3.0, 5.0, -4.0, 2.0, 1.0, 3.0, 1.0) for i in range(30)]
+    gl, go = pair_geometry(rtkb, oracle, params)
+    pd, po = pair_image(rtkb, oracle, (96, 40, 12), (0.8, 0.8, 1.0), index=(-3, 2, 10))
+    p = np.random.default_rng(1).uniform(0, 2, size=oracle.shape_of(po))
+    ref = oracle.fdk_weight(go, po, p)
+    t = to_gpu(p)
+    rtkb.ops.fdk_weight(gl, pd, t, out=t)
+    assert rel_l2(to_np(t), ref) < 1e-6
+
+
+def test_parker_short_scan(rtkb, oracle):
+    params = [(1000.0, 1536.0, i * 200.0 / 120, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0) for i in range(120)]
+    gl, go = pair_geometry(rtkb, oracle, params)
+    pd, po = pair_image(rtkb, oracle, (256, 8, 120), (1.0, 1.0, 1.0))
+    p = np.random.default_rng(2).uniform(0, 1, size=oracle.shape_of(po))
+    ref, short = oracle.parker_weight(go, po, p)
+    got, gshort = rtkb.ops.parker_short_scan(gl, pd, to_gpu(p))
+    assert short and gshort
+    assert rel_l2(to_np(got), ref) < 1e-6
+
+
+def test_parker_full_scan_is_a_copy(rtkb, oracle):
+    params = [(1000.0, 1536.0, i * 3.0) for i in range(120)]
+    gl, go = pair_geometry(rtkb, oracle, params)
+    pd, po = pair_image(rtkb, oracle, (64, 4, 120), (1.0, 1.0, 1.0))
+    p = np.random.default_rng(3).uniform(0, 1, size=oracle.shape_of(po)).astype(np.float32)
+    got, short = rtkb.ops.parker_short_scan(gl, pd, to_gpu(p))
+    assert not short
+    assert np.array_equal(to_np(got), p.astype(np.float64))
+
+
+def test_parker_irregular_like_rtkshortscancompcudatest(rtkb, oracle):
+    gl, go = pair_geometry(rtkb, oracle, IRREGULAR)
+    pd, po = pair_image(rtkb, oracle, (128, 4, 4), (2.0, 2.0, 2.0), origin=(-127.0, -3.0, 0.0))
+    p = _sl_projections(oracle, go, po).astype(np.float32).astype(np.float64)
+    ref, short = oracle.parker_weight(go, po, p)
+    got, gshort = rtkb.ops.parker_short_scan(gl, pd, to_gpu(p))
+    assert short == gshort
+    _rtk_cuda_cpu_check(to_np(got), ref)
+
+
+@pytest.mark.parametrize("offset", [80.0, -60.0])
+def test_displaced_detector(rtkb, oracle, offset):
+    params = [(1000.0, 1536.0, i * 6.0, offset, 0.0) for i in range(60)]
+    gl, go = pair_geometry(rtkb, oracle, params)
+    pd, po = pair_image(rtkb, oracle, (256, 6, 60), (0.8, 0.8, 1.0))
+    p = np.random.default_rng(4).uniform(0, 1, size=oracle.shape_of(po))
+    ref, i0, s0 = oracle.displaced_detector(go, po, p)
+    got, od = rtkb.ops.displaced_detector(gl, pd, to_gpu(p))
+    assert (od.index[0], od.size[0]) == (i0, s0)
+    assert rel_l2(to_np(got), ref) < 1e-6
+
+
+def test_displaced_irregular_like_rtkdisplaceddetectorcompcudatest(rtkb, oracle):
+    gl, go = pair_geometry(rtkb, oracle, IRREGULAR)
+    pd, po = pair_image(rtkb, oracle, (128, 4, 4), (2.0, 2.0, 2.0), origin=(-127.0, -3.0, 0.0))
+    p = _sl_projections(oracle, go, po).astype(np.float32).astype(np.float64)
+    ref, i0, s0 = oracle.displaced_detector(go, po, p)
+    got, od = rtkb.ops.displaced_detector(gl, pd, to_gpu(p))
+    assert (od.index[0], od.size[0]) == (i0, s0)
+    _rtk_cuda_cpu_check(to_np(got), ref)
+
+
+@pytest.mark.parametrize("nu,window", [(256, {}), (1024, {"hann": 1.0}), (300, {"hann": 0.8}),
+                                       (128, {"cosine": 0.7}), (512, {"hamming": 0.9}),
+                                       (200, {"ramlak": 0.6}), (256, {"shepplogan": 0.8}),
+                                       (256, {"truncation": 0.1}), (2048, {"hann": 0.5})])
+def test_ramp_filter(rtkb, oracle, nu, window):
+    pd, po = pair_image(rtkb, oracle, (nu, 7, 3), (0.5, 0.5, 1.0))
+    rng = np.random.default_rng(nu)
+    p = rng.uniform(0, 1, size=oracle.shape_of(po))
+    ref = oracle.ramp_filter(po, p, oracle.ramp_params(**window))
+    got = to_np(rtkb.ops.ramp_filter(pd, to_gpu(p), rtkb.ops.ramp_params(**window)))
+    assert rel_l2(got, ref) < REL_L2_TOL
+
+
+def test_ramp_kernel_matches_oracle(rtkb, oracle):
+    for nu, kw in ((256, {}), (1000, {"hann": 0.7}), (513, {"shepplogan": 1.0})):
+        n, k = rtkb.ops.ramp_kernel(nu, 0.388, rtkb.ops.ramp_params(**kw))
+        assert n == oracle.ramp_padded_size(nu, oracle.ramp_params(**kw))
+        np.testing.assert_allclose(k, oracle.ramp_kernel(n, 0.388, oracle.ramp_params(**kw)), rtol=1e-12,
+                                   atol=1e-12)
+
+
+@pytest.mark.parametrize("displaced,short", [(False, False), (True, False), (False, True), (True, True)])
+def test_fdk_preprocess_fused(rtkb, oracle, displaced, short):
+    arc = 220.0 if short else 360.0
+    params = [(1000.0, 1536.0, i * arc / 90, 60.0 if displaced else 0.0, 2.0) for i in range(90)]
+    gl, go = pair_geometry(rtkb, oracle, params)
+    pd, po = pair_image(rtkb, oracle, (200, 9, 90), (0.8, 0.8, 1.0))
+    p = np.random.default_rng(5).uniform(0, 1, size=oracle.shape_of(po))
+    q, qo = p, po
+    if displaced:
+        q, i0, s0 = oracle.displaced_detector(go, po, q)
+        qo = oracle.image((s0, 9, 90), (0.8, 0.8, 1.0), origin=tuple(po.origin), index=(i0, 0, 0))
+    if short:
+        q, _ = oracle.parker_weight(go, qo, q)
+    q = oracle.fdk_weight(go, qo, q)
+    ref = oracle.ramp_filter(qo, q, oracle.ramp_params(hann=0.9))
+    got, od = rtkb.ops.fdk_preprocess(gl, pd, to_gpu(p), rtkb.ops.ramp_params(hann=0.9), displaced=displaced,
+                                      short_scan=short)
+    assert (od.index[0], od.size[0]) == (qo.index[0], qo.size[0])
+    assert rel_l2(to_np(got), ref) < REL_L2_TOL
+
+
+def test_fdk_gpu_shepp_logan_like_rtkfdktest(rtkb, oracle):
+    """Full GPU FDK (fused preprocessing + backprojection) against the oracle
+    FDK, and against the phantom with rtkfdktest's thresholds."""
+    n = 180
+    params = [(600.0, 1200.0, i * 360.0 / n, 0, 0, 0, 0, 20, 15) for i in range(n)]
+    gl, go = pair_geometry(rtkb, oracle, params)
+    vd, vo = pair_image(rtkb, oracle, (128, 128, 128), (2.0,) * 3, origin=(-127.0,) * 3)
+    pd, po = pair_image(rtkb, oracle, (128, 128, n), (4.0,) * 3, origin=(-254.0,) * 3)
+    sl = phantoms.shepp_logan(116.0)
+    p = oracle.project_ellipsoids(go, po, sl).astype(np.float32).astype(np.float64)
+    ref_img = oracle.draw_ellipsoids(vo, sl)
+    filt = oracle.ramp_filter(po, oracle.fdk_weight(go, po, p), oracle.ramp_params())
+    ref = oracle.backproject(go, vo, po, filt, fdk=True)
+    import torch
+
+    f, _ = rtkb.ops.fdk_preprocess(gl, pd, to_gpu(p))
+    rec = to_np(rtkb.ops.fdk_backproject(gl, vd, pd, f, torch.zeros((128, 128, 128), device="cuda")))
+    assert rel_l2(rec, ref) < REL_L2_TOL
+    err, psnr, ok = phantoms.check_image_quality(rec * phantoms.fov_mask(go, vo, po), ref_img, 0.03, 26.0, 2.0)
+    assert ok, (err, psnr)

@@ -250,13 +250,13 @@ def run_reference(args, world, rank):
 
 
 def use_profile_case():
-    """256^3 at 1 mm from 360 of the 1024x768 projections: the same kernel on a
-    case small enough for multi-pass ncu captures (1.1 GB on the device)."""
-    global NX, NY, NZ, VOX, NP, WORKLOAD
+    """256^3 at 0.5 mm (the benchmark's voxel size, so the same tile
+    footprints and kernel configuration) from 360 of the 1024x768 projections:
+    small enough for multi-pass ncu captures (1.2 GB on the device)."""
+    global NX, NY, NZ, NP, WORKLOAD
     NX = NY = NZ = 256
-    VOX = 1.0
     NP = 360
-    WORKLOAD = dict(WORKLOAD, workload="profile case: FDK backprojection 256^3 @1mm <- 360 x 1024x768 @0.388mm",
+    WORKLOAD = dict(WORKLOAD, workload="profile case: FDK backprojection 256^3 @0.5mm <- 360 x 1024x768 @0.388mm",
                     volume=[NX, NY, NZ], projections=[NU, NV, NP])
 
 

@@ -119,6 +119,14 @@ int rtkb_backproject_matrices(const int vol_size[3], const int proj_size[3], int
                               const int * modes, int weighting, const float * d_proj, const float * d_vol_in,
                               float * d_vol_out, void * stream);
 
+/* Autotuner hook of the tiled backprojector (no reference counterpart):
+ * force >= 0 selects configuration `force` (box size, voxels per thread
+ * column, occupancy target) for later calls on this host thread, -1 restores
+ * the footprint heuristic.  *last_used receives the configuration of the last
+ * tiled launch on this thread (-1 if none), *count the number of
+ * configurations.  Either pointer may be NULL. */
+int rtkb_backproject_config(int force, int * last_used, int * count);
+
 /* ---- projection weighting and ramp filtering ----
  * All take a projection stack description `proj` (slice s = geometry
  * projection proj->index[2] + s) and float32 device buffers.  d_out may equal

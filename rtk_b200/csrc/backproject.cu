@@ -65,6 +65,14 @@ static_assert(sizeof(StageHeader) <= kHeaderBytes, "stage header overflow");
 // test (0 <= floor(u) <= N-2) is decided as the FP64 CPU filters decide it.
 constexpr float kBand = 1e-3f;
 
+__device__ __forceinline__ float
+rcp_approx(float x)
+{
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 __device__ __forceinline__ bool
 accept_fp64(const double * m, int row, int X, int Y, int Z, int n)
 {
@@ -88,36 +96,148 @@ struct Layout
   static constexpr int kTotal = kBars + 2 * kStages * 8;
 };
 
-// FP64 slow path for one projection: RTK's optimised-path arithmetic with
-// global-memory bilinear taps.
-template <int NYT, bool FDKW>
-__device__ __forceinline__ void
-slow_projection(const double * M, const float * __restrict__ proj, long long pofs, int nu, int nv, int X, int Y0,
-                int Z, float (&acc)[NYT])
+// FP64 slow path for one voxel and projection: RTK's optimised-path
+// arithmetic with global-memory bilinear taps.
+__device__ __forceinline__ float
+slow_voxel(const double * M, const float * __restrict__ proj, long long pofs, int nu, int nv, int X, int Y, int Z,
+           bool fdkw)
 {
-#pragma unroll
-  for (int j = 0; j < NYT; j++)
-  {
-    const double x = X, y = Y0 + j, z = Z;
-    const double w = M[8] * x + M[9] * y + M[10] * z + M[11];
-    const double rw = 1.0 / w;
-    const double u = (M[0] * x + M[1] * y + M[2] * z + M[3]) * rw;
-    const double v = (M[4] * x + M[5] * y + M[6] * z + M[7]) * rw;
-    if (u >= 0.0 && u < nu - 1.0 && v >= 0.0 && v < nv - 1.0)
-    {
-      const int       iu = (int)floor(u), iv = (int)floor(v);
-      const double    fu = u - iu, fv = v - iv;
-      const float *   q = proj + pofs + (long long)iv * nu + iu;
-      const double    a = (1 - fu) * __ldg(q) + fu * __ldg(q + 1);
-      const double    b = (1 - fu) * __ldg(q + nu) + fu * __ldg(q + nu + 1);
-      const double    val = (1 - fv) * a + fv * b;
-      acc[j] += (float)(FDKW ? rw * rw * val : val);
-    }
-  }
+  const double x = X, y = Y, z = Z;
+  const double w = M[8] * x + M[9] * y + M[10] * z + M[11];
+  const double rw = 1.0 / w;
+  const double u = (M[0] * x + M[1] * y + M[2] * z + M[3]) * rw;
+  const double v = (M[4] * x + M[5] * y + M[6] * z + M[7]) * rw;
+  if (!(u >= 0.0 && u < nu - 1.0 && v >= 0.0 && v < nv - 1.0))
+    return 0.f;
+  const int     iu = (int)floor(u), iv = (int)floor(v);
+  const double  fu = u - iu, fv = v - iv;
+  const float * q = proj + pofs + (long long)iv * nu + iu;
+  const double  a = (1 - fu) * __ldg(q) + fu * __ldg(q + 1);
+  const double  b = (1 - fu) * __ldg(q + nu) + fu * __ldg(q + nu + 1);
+  const double  val = (1 - fv) * a + fv * b;
+  return (float)(fdkw ? rw * rw * val : val);
 }
 
-template <int BW, int BH, int NYT, bool FDKW>
-__global__ void __launch_bounds__(kThreads, 1)
+// Producer warp: per projection, project the tile's corners, size the
+// footprint box, publish the tile-relative coefficients and start the TMA
+// load of the box.  Out of line: its FP64 registers stay off the consumers.
+template <int BW, int BH, int NYT>
+__device__ __noinline__ void
+bp_producer(const CUtensorMap * tmap, const float * __restrict__ proj, const double * __restrict__ mats, int nproj,
+            int nu, int nv, int x0, int y0, int z0, StageHeader * hdr, float * boxes, uint64_t * full,
+            uint64_t * empty, int use_tma)
+{
+  using L = Layout<BW, BH>;
+  const int lane = threadIdx.x & 31;
+  if (use_tma && lane == 0)
+    prefetch_tensor_map(tmap);
+  // Footprint of the whole tile, including voxels beyond a ragged volume
+  // edge: consumers compute (but never store) those y's, so their shared-
+  // memory taps must stay inside the box too.
+  const int    x1 = x0 + kTX - 1, y1 = y0 + NYT - 1, z1 = z0 + kTZ - 1;
+  const int    c = lane & 7;
+  const double X = (c & 1) ? x1 : x0, Y = (c & 2) ? y1 : y0, Z = (c & 4) ? z1 : z0;
+  for (int p = 0; p < nproj; p++)
+  {
+    const int s = p % kStages, k = p / kStages;
+    if (p >= kStages && !mbar_wait(&empty[s], (k - 1) & 1))
+      return;
+    const double * M = mats + 12 * (long long)p;
+    double         m[12];
+#pragma unroll
+    for (int q = 0; q < 12; q++)
+      m[q] = __ldg(M + q);
+    const double w = m[8] * X + m[9] * Y + m[10] * Z + m[11];
+    const double un = m[0] * X + m[1] * Y + m[2] * Z + m[3];
+    const double vn = m[4] * X + m[5] * Y + m[6] * Z + m[7];
+    // The box only needs the corners to ~1e-4 pixel: divide in FP32 (the
+    // numerators are FP64) and reduce in FP32.
+    const float rw = 1.0f / (float)w;
+    float       umin = (float)un * rw, umax = umin, vmin = (float)vn * rw, vmax = vmin;
+    int         wsign = (w > 0.0) ? 1 : ((w < 0.0) ? 2 : 3); // bit set: 1 positive, 2 negative
+#pragma unroll
+    for (int o = 1; o < 8; o <<= 1)
+    {
+      umin = fminf(umin, __shfl_xor_sync(0xffffffffu, umin, o));
+      umax = fmaxf(umax, __shfl_xor_sync(0xffffffffu, umax, o));
+      vmin = fminf(vmin, __shfl_xor_sync(0xffffffffu, vmin, o));
+      vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+      wsign |= __shfl_xor_sync(0xffffffffu, wsign, o);
+    }
+    // The tile's image is the hull of its projected corners only when w has
+    // one sign over the tile (no voxel at the source plane).  Matrices are
+    // finite (checked on the host), so a NaN or infinite u/v needs w == 0 at
+    // a corner, which fails the sign test.
+    const float margin = 0.05f;
+    bool        fast = (wsign == 1 || wsign == 2) && isfinite(umin) && isfinite(umax) && isfinite(vmin) &&
+               isfinite(vmax) && fabsf(umin) < 1e7f && fabsf(umax) < 1e7f && fabsf(vmin) < 1e7f && fabsf(vmax) < 1e7f;
+    int ub = 0, vb = 0;
+    if (fast)
+    {
+      ub = ((int)floorf(umin - margin)) & ~3;
+      vb = (int)floorf(vmin - margin);
+      fast = (umax + margin < (float)(ub + BW - 1)) && (vmax + margin < (float)(vb + BH - 1));
+    }
+    StageHeader * h = hdr + s;
+    float *       box = boxes + s * (BW * BH);
+    if (lane == 0)
+    {
+      int flags = 0;
+      if (fast)
+      {
+        const double wo = m[8] * x0 + m[9] * y0 + m[10] * z0 + m[11];
+        const double uo = m[0] * x0 + m[1] * y0 + m[2] * z0 + m[3];
+        const double vo = m[4] * x0 + m[5] * y0 + m[6] * z0 + m[7];
+        h->a0 = make_float4((float)(m[0] - ub * m[8]), (float)(m[1] - ub * m[9]), (float)(m[2] - ub * m[10]),
+                            (float)(uo - ub * wo));
+        h->a1 = make_float4((float)(m[4] - vb * m[8]), (float)(m[5] - vb * m[9]), (float)(m[6] - vb * m[10]),
+                            (float)(vo - vb * wo));
+        h->a2 = make_float4((float)m[8], (float)m[9], (float)m[10], (float)wo);
+        h->lim = make_float4((float)(-ub), (float)(nu - 1 - ub), (float)(-vb), (float)(nv - 1 - vb));
+        flags = kFlagFast;
+        if (umin - margin >= 0.0 && umax + margin < nu - 1.0)
+          flags |= kFlagUInterior;
+        if (vmin - margin >= 0.0 && vmax + margin < nv - 1.0)
+          flags |= kFlagVInterior;
+      }
+#pragma unroll
+      for (int q = 0; q < 12; q++)
+        h->m[q] = m[q];
+      h->fl = make_int4(flags, ub, vb, 0);
+    }
+    if (fast && use_tma)
+    {
+      if (lane == 0)
+      {
+        mbar_arrive_expect_tx(&full[s], (uint32_t)L::kBoxBytes);
+        tma_load_3d(box, tmap, ub, vb, p, &full[s]);
+      }
+    }
+    else
+    {
+      if (fast)
+      {
+        // plain-load fallback when the stack cannot be described to TMA
+        const long long pofs = (long long)p * nu * nv;
+        for (int e = lane; e < BW * BH; e += 32)
+        {
+          const int gu = ub + e % BW, gv = vb + e / BW;
+          box[e] = (gu >= 0 && gu < nu && gv >= 0 && gv < nv) ? __ldg(proj + pofs + (long long)gv * nu + gu) : 0.f;
+        }
+      }
+      __syncwarp();
+      if (lane == 0)
+        mbar_arrive(&full[s]);
+    }
+  }
+  // drain: wait for the last copies to land before the CTA may exit
+  for (int p = max(0, nproj - kStages); p < nproj; p++)
+    if (!mbar_wait(&full[p % kStages], (p / kStages) & 1))
+      return;
+}
+
+template <int BW, int BH, int NYT, int MINB, bool FDKW>
+__global__ void __launch_bounds__(kThreads, MINB)
 bp_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const float * __restrict__ proj,
                 const double * __restrict__ mats, int nproj, int nu, int nv, int nx, int ny, int nz, int ntx,
                 int ntz, const float * vol_in, float * vol_out, int use_tma)
@@ -147,118 +267,15 @@ bp_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const float * __restri
 
   if (warp == kConsumerWarps)
   {
-    // ------------------------------------------------------------- producer
-    if (use_tma && lane == 0)
-      prefetch_tensor_map(&tmap);
-    // Footprint of the whole tile, including voxels beyond a ragged volume
-    // edge: consumers compute (but never store) those y's, so their shared-
-    // memory taps must stay inside the box too.
-    const int    x1 = x0 + kTX - 1, y1 = y0 + NYT - 1, z1 = z0 + kTZ - 1;
-    const int    c = lane & 7;
-    const double X = (c & 1) ? x1 : x0, Y = (c & 2) ? y1 : y0, Z = (c & 4) ? z1 : z0;
-    for (int p = 0; p < nproj; p++)
-    {
-      const int s = p % kStages, k = p / kStages;
-      if (p >= kStages && !mbar_wait(&empty[s], (k - 1) & 1))
-        return;
-      const double * M = mats + 12 * (long long)p;
-      double         m[12];
-#pragma unroll
-      for (int q = 0; q < 12; q++)
-        m[q] = __ldg(M + q);
-      const double w = m[8] * X + m[9] * Y + m[10] * Z + m[11];
-      const double un = m[0] * X + m[1] * Y + m[2] * Z + m[3];
-      const double vn = m[4] * X + m[5] * Y + m[6] * Z + m[7];
-      const double rw = 1.0 / w;
-      double       umin = un * rw, umax = umin, vmin = vn * rw, vmax = vmin, wmin = w, wmax = w;
-#pragma unroll
-      for (int o = 1; o < 8; o <<= 1)
-      {
-        umin = fmin(umin, __shfl_xor_sync(0xffffffffu, umin, o));
-        umax = fmax(umax, __shfl_xor_sync(0xffffffffu, umax, o));
-        vmin = fmin(vmin, __shfl_xor_sync(0xffffffffu, vmin, o));
-        vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
-        wmin = fmin(wmin, __shfl_xor_sync(0xffffffffu, wmin, o));
-        wmax = fmax(wmax, __shfl_xor_sync(0xffffffffu, wmax, o));
-      }
-      // The tile's image is the hull of its projected corners only when w has
-      // one sign over the tile (no voxel at the source plane).  Matrices are
-      // finite (checked on the host), so a NaN or infinite u/v needs w == 0 at
-      // a corner, which fails the sign test.
-      const double margin = 0.05;
-      bool         fast = (wmin > 0.0 || wmax < 0.0) && isfinite(umin) && isfinite(umax) && isfinite(vmin) &&
-                  isfinite(vmax) && fabs(umin) < 1e7 && fabs(umax) < 1e7 && fabs(vmin) < 1e7 && fabs(vmax) < 1e7;
-      int ub = 0, vb = 0;
-      if (fast)
-      {
-        ub = ((int)floor(umin - margin)) & ~3;
-        vb = (int)floor(vmin - margin);
-        fast = (umax + margin < ub + BW - 1.0) && (vmax + margin < vb + BH - 1.0);
-      }
-      StageHeader * h = hdr + s;
-      float *       box = boxes + s * (BW * BH);
-      if (lane == 0)
-      {
-        int flags = 0;
-        if (fast)
-        {
-          const double wo = m[8] * x0 + m[9] * y0 + m[10] * z0 + m[11];
-          const double uo = m[0] * x0 + m[1] * y0 + m[2] * z0 + m[3];
-          const double vo = m[4] * x0 + m[5] * y0 + m[6] * z0 + m[7];
-          h->a0 = make_float4((float)(m[0] - ub * m[8]), (float)(m[1] - ub * m[9]), (float)(m[2] - ub * m[10]),
-                              (float)(uo - ub * wo));
-          h->a1 = make_float4((float)(m[4] - vb * m[8]), (float)(m[5] - vb * m[9]), (float)(m[6] - vb * m[10]),
-                              (float)(vo - vb * wo));
-          h->a2 = make_float4((float)m[8], (float)m[9], (float)m[10], (float)wo);
-          h->lim = make_float4((float)(-ub), (float)(nu - 1 - ub), (float)(-vb), (float)(nv - 1 - vb));
-          flags = kFlagFast;
-          if (umin - margin >= 0.0 && umax + margin < nu - 1.0)
-            flags |= kFlagUInterior;
-          if (vmin - margin >= 0.0 && vmax + margin < nv - 1.0)
-            flags |= kFlagVInterior;
-        }
-#pragma unroll
-        for (int q = 0; q < 12; q++)
-          h->m[q] = m[q];
-        h->fl = make_int4(flags, ub, vb, 0);
-      }
-      if (fast && use_tma)
-      {
-        if (lane == 0)
-        {
-          mbar_arrive_expect_tx(&full[s], (uint32_t)L::kBoxBytes);
-          tma_load_3d(box, &tmap, ub, vb, p, &full[s]);
-        }
-      }
-      else
-      {
-        if (fast)
-        {
-          // plain-load fallback when the stack cannot be described to TMA
-          const long long pofs = (long long)p * nu * nv;
-          for (int e = lane; e < BW * BH; e += 32)
-          {
-            const int gu = ub + e % BW, gv = vb + e / BW;
-            box[e] = (gu >= 0 && gu < nu && gv >= 0 && gv < nv) ? __ldg(proj + pofs + (long long)gv * nu + gu) : 0.f;
-          }
-        }
-        __syncwarp();
-        if (lane == 0)
-          mbar_arrive(&full[s]);
-      }
-    }
-    // drain: wait for the last copies to land before the CTA may exit
-    for (int p = max(0, nproj - kStages); p < nproj; p++)
-      if (!mbar_wait(&full[p % kStages], (p / kStages) & 1))
-        return;
+    bp_producer<BW, BH, NYT>(&tmap, proj, mats, nproj, nu, nv, x0, y0, z0, hdr, boxes, full, empty, use_tma);
     return;
   }
 
   // --------------------------------------------------------------- consumers
-  const int  t = threadIdx.x;
-  const int  dx = t % kTX, dz = t / kTX;
-  const int  X = x0 + dx, Z = z0 + dz;
-  const bool active = (X < nx) && (Z < nz);
+  const int   t = threadIdx.x;
+  const int   dx = t % kTX, dz = t / kTX;
+  const int   X = x0 + dx, Z = z0 + dz;
+  const bool  active = (X < nx) && (Z < nz);
   const float fdx = (float)dx, fdz = (float)dz;
   float       acc[NYT];
 #pragma unroll
@@ -277,9 +294,9 @@ bp_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const float * __restri
     {
       if (fl.x & kFlagFast)
       {
-        const float4 a0 = h->a0, a1 = h->a1, a2 = h->a2, lim = h->lim;
+        const float4 a0 = h->a0, a1 = h->a1, a2 = h->a2;
         const float  nw = fmaf(a2.x, fdx, fmaf(a2.z, fdz, a2.w));
-        const float  rw = __frcp_rn(nw);
+        const float  rw = rcp_approx(nw); // <= 1 ulp: ~1e-5 pixel at |u| <= 64
         const float  u = fmaf(a0.x, fdx, fmaf(a0.z, fdz, a0.w)) * rw;
         const float  v0 = fmaf(a1.x, fdx, fmaf(a1.z, fdz, a1.w)) * rw;
         const float  dv = a1.y * rw;
@@ -287,6 +304,7 @@ bp_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const float * __restri
         bool         uok = true;
         if (!(fl.x & kFlagUInterior))
         {
+          const float4 lim = h->lim;
           uok = (u >= lim.x && u < lim.y);
           if (fabsf(u - lim.x) < kBand || fabsf(u - lim.y) < kBand)
             uok = accept_fp64(h->m, 0, X, y0, Z, nu); // u does not depend on y on this path
@@ -313,6 +331,7 @@ bp_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const float * __restri
           }
           else
           {
+            const float4 lim = h->lim;
 #pragma unroll
             for (int j = 0; j < NYT; j++)
             {
@@ -336,11 +355,10 @@ bp_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const float * __restri
       }
       else
       {
-        double M[12];
+        const long long pofs = (long long)p * nu * nv;
 #pragma unroll
-        for (int q = 0; q < 12; q++)
-          M[q] = h->m[q];
-        slow_projection<NYT, FDKW>(M, proj, (long long)p * nu * nv, nu, nv, X, y0, Z, acc);
+        for (int j = 0; j < NYT; j++)
+          acc[j] += slow_voxel(h->m, proj, pofs, nu, nv, X, y0 + j, Z, FDKW);
       }
     }
     __syncwarp();
@@ -413,10 +431,19 @@ bp_generic_kernel(const float * __restrict__ proj, const double * __restrict__ m
   }
 }
 
-struct BoxConfig
+struct BpConfig
 {
-  int bw, bh;
+  int bw, bh, nyt, minb;
 };
+
+// Candidate (box width, box height, voxels per thread column, CTAs per SM the
+// register budget targets), in order of preference; the first whose box
+// holds the probed footprints is used unless the autotuner forces one.
+constexpr int           kNumBpConfigs = 6;
+static const BpConfig   kBpConfigs[kNumBpConfigs] = { { 64, 64, 16, 3 }, { 64, 64, 16, 2 }, { 64, 32, 8, 3 },
+                                                      { 64, 32, 8, 2 },  { 128, 64, 16, 1 }, { 128, 64, 8, 1 } };
+static thread_local int g_bp_forced_config = -1;
+static thread_local int g_bp_last_config = -1;
 
 // Largest detector footprint of a 16 x NYT x 16 tile, probed on the tiles at
 // the volume's corners (where magnification peaks) and its centre.
@@ -469,13 +496,13 @@ estimate_footprint(const std::vector<double> & mats, int nproj, int nx, int ny, 
   }
 }
 
-template <int BW, int BH, int NYT, bool FDKW>
+template <int BW, int BH, int NYT, int MINB, bool FDKW>
 static int
 launch_tiled(const CUtensorMap & tmap, bool use_tma, const float * d_proj, const double * d_mats, int nproj, int nu,
              int nv, int nx, int ny, int nz, const float * vin, float * vout, cudaStream_t st)
 {
   using L = Layout<BW, BH>;
-  auto kern = bp_tiled_kernel<BW, BH, NYT, FDKW>;
+  auto kern = bp_tiled_kernel<BW, BH, NYT, MINB, FDKW>;
   RTKB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kTotal));
   const int       ntx = (nx + kTX - 1) / kTX, nty = (ny + NYT - 1) / NYT, ntz = (nz + kTZ - 1) / kTZ;
   const long long nblocks = (long long)ntx * nty * ntz;
@@ -492,20 +519,25 @@ static int
 dispatch_tiled(int cfg, const CUtensorMap & tmap, bool use_tma, const float * d_proj, const double * d_mats,
                int nproj, int nu, int nv, int nx, int ny, int nz, const float * vin, float * vout, cudaStream_t st)
 {
+#define RTKB_BP_LAUNCH(BW, BH, NYT, MINB)                                                                              \
+  return launch_tiled<BW, BH, NYT, MINB, FDKW>(tmap, use_tma, d_proj, d_mats, nproj, nu, nv, nx, ny, nz, vin, vout, st)
   switch (cfg)
   {
     case 0:
-      return launch_tiled<64, 32, 8, FDKW>(tmap, use_tma, d_proj, d_mats, nproj, nu, nv, nx, ny, nz, vin, vout, st);
+      RTKB_BP_LAUNCH(64, 64, 16, 3);
     case 1:
-      return launch_tiled<64, 48, 8, FDKW>(tmap, use_tma, d_proj, d_mats, nproj, nu, nv, nx, ny, nz, vin, vout, st);
+      RTKB_BP_LAUNCH(64, 64, 16, 2);
     case 2:
-      return launch_tiled<128, 32, 8, FDKW>(tmap, use_tma, d_proj, d_mats, nproj, nu, nv, nx, ny, nz, vin, vout, st);
+      RTKB_BP_LAUNCH(64, 32, 8, 3);
+    case 3:
+      RTKB_BP_LAUNCH(64, 32, 8, 2);
+    case 4:
+      RTKB_BP_LAUNCH(128, 64, 16, 1);
     default:
-      return launch_tiled<128, 64, 8, FDKW>(tmap, use_tma, d_proj, d_mats, nproj, nu, nv, nx, ny, nz, vin, vout, st);
+      RTKB_BP_LAUNCH(128, 64, 8, 1);
   }
+#undef RTKB_BP_LAUNCH
 }
-
-static const BoxConfig kBoxConfigs[4] = { { 64, 32 }, { 64, 48 }, { 128, 32 }, { 128, 64 } };
 
 } // namespace
 
@@ -599,17 +631,24 @@ backproject_buffer(const int vol_size[3], const int proj_size[3], int nproj, con
         rc = cuda_fail(e, "bp_generic_kernel launch");
       break;
     }
-    // choose the smallest footprint box that fits the probed tiles
-    double fw, fh;
+    // first configuration whose box holds the footprints probed on the host
     std::vector<double> mv(mats, mats + 12 * (size_t)nproj);
-    estimate_footprint(mv, nproj, nx, ny, nz, 8, fw, fh);
-    int cfg = 3;
-    for (int c = 0; c < 4; c++)
-      if (fw + 3.2 < kBoxConfigs[c].bw - 1 && fh + 0.2 < kBoxConfigs[c].bh - 1)
+    double              fw8, fh8, fw16, fh16;
+    estimate_footprint(mv, nproj, nx, ny, nz, 8, fw8, fh8);
+    estimate_footprint(mv, nproj, nx, ny, nz, 16, fw16, fh16);
+    int cfg = kNumBpConfigs - 1;
+    for (int c = 0; c < kNumBpConfigs; c++)
+    {
+      const double fw = kBpConfigs[c].nyt == 16 ? fw16 : fw8, fh = kBpConfigs[c].nyt == 16 ? fh16 : fh8;
+      if (fw + 3.2 < kBpConfigs[c].bw - 1 && fh + 0.2 < kBpConfigs[c].bh - 1)
       {
         cfg = c;
         break;
       }
+    }
+    if (g_bp_forced_config >= 0)
+      cfg = g_bp_forced_config; // a box too small for some tiles only sends them to the FP64 path
+    g_bp_last_config = cfg;
     // TMA needs 16-byte aligned rows and base address
     CUtensorMap tmap;
     std::memset(&tmap, 0, sizeof(tmap));
@@ -621,7 +660,7 @@ backproject_buffer(const int vol_size[3], const int proj_size[3], int nproj, con
       const unsigned long long dims[3] = { (unsigned long long)nu, (unsigned long long)nv,
                                            (unsigned long long)np_total };
       const unsigned long long strides[2] = { (unsigned long long)nu * 4ULL, (unsigned long long)nu * nv * 4ULL };
-      const unsigned           box[3] = { (unsigned)kBoxConfigs[cfg].bw, (unsigned)kBoxConfigs[cfg].bh, 1u };
+      const unsigned           box[3] = { (unsigned)kBpConfigs[cfg].bw, (unsigned)kBpConfigs[cfg].bh, 1u };
       const unsigned           estr[3] = { 1u, 1u, 1u };
       const int r = enc(&tmap, (int)CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3u, const_cast<float *>(d_proj), dims, strides,
                         box, estr, (int)CU_TENSOR_MAP_INTERLEAVE_NONE, (int)CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -726,5 +765,18 @@ rtkb_device_status(void * stream, int * status)
                                         st));
   RTKB_CUDA_TRY(cudaStreamSynchronize(st));
   *status = (int)v;
+  return RTKB_OK;
+}
+
+extern "C" int
+rtkb_backproject_config(int force, int * last_used, int * count)
+{
+  if (force < -1 || force >= kNumBpConfigs)
+    return rtkb::fail(RTKB_ERR_INVALID_ARGUMENT, "backprojection configuration index out of range");
+  if (last_used)
+    *last_used = g_bp_last_config;
+  if (count)
+    *count = kNumBpConfigs;
+  g_bp_forced_config = force;
   return RTKB_OK;
 }

@@ -57,6 +57,7 @@ struct __align__(16) StageHeader
   float4 lim;   // valid u range [x, y), valid v range [z, w) (box-relative)
   int4   fl;    // flags, ub, vb, unused
   double m[12]; // FP64 buffer-index matrix: boundary decisions and the slow path
+  float  mf[12]; // FP32 copy: corner projection for the footprint box
 };
 static_assert(sizeof(StageHeader) <= kHeaderBytes, "stage header overflow");
 
@@ -73,7 +74,7 @@ rcp_approx(float x)
   return r;
 }
 
-__device__ __forceinline__ bool
+__device__ __noinline__ bool
 accept_fp64(const double * m, int row, int X, int Y, int Z, int n)
 {
   const double x = X, y = Y, z = Z;
@@ -85,6 +86,7 @@ accept_fp64(const double * m, int row, int X, int Y, int Z, int n)
 constexpr int kFlagFast = 1;
 constexpr int kFlagUInterior = 2;
 constexpr int kFlagVInterior = 4;
+constexpr int kFlagSkip = 8; // the whole tile projects off the detector
 
 template <int BW, int BH>
 struct Layout
@@ -97,8 +99,9 @@ struct Layout
 };
 
 // FP64 slow path for one voxel and projection: RTK's optimised-path
-// arithmetic with global-memory bilinear taps.
-__device__ __forceinline__ float
+// arithmetic with global-memory bilinear taps.  Out of line: the rare path's
+// FP64 registers stay off the hot loop.
+__device__ __noinline__ float
 slow_voxel(const double * M, const float * __restrict__ proj, long long pofs, int nu, int nv, int X, int Y, int Z,
            bool fdkw)
 {
@@ -120,9 +123,9 @@ slow_voxel(const double * M, const float * __restrict__ proj, long long pofs, in
 
 // Producer warp: per projection, project the tile's corners, size the
 // footprint box, publish the tile-relative coefficients and start the TMA
-// load of the box.  Out of line: its FP64 registers stay off the consumers.
+// load of the box.
 template <int BW, int BH, int NYT>
-__device__ __noinline__ void
+__device__ __forceinline__ void
 bp_producer(const CUtensorMap * tmap, const float * __restrict__ proj, const double * __restrict__ mats, int nproj,
             int nu, int nv, int x0, int y0, int z0, StageHeader * hdr, float * boxes, uint64_t * full,
             uint64_t * empty, int use_tma)
@@ -134,27 +137,36 @@ bp_producer(const CUtensorMap * tmap, const float * __restrict__ proj, const dou
   // Footprint of the whole tile, including voxels beyond a ragged volume
   // edge: consumers compute (but never store) those y's, so their shared-
   // memory taps must stay inside the box too.
-  const int    x1 = x0 + kTX - 1, y1 = y0 + NYT - 1, z1 = z0 + kTZ - 1;
-  const int    c = lane & 7;
-  const double X = (c & 1) ? x1 : x0, Y = (c & 2) ? y1 : y0, Z = (c & 4) ? z1 : z0;
+  const int   x1 = x0 + kTX - 1, y1 = y0 + NYT - 1, z1 = z0 + kTZ - 1;
+  const int   c = lane & 7;
+  const float X = (float)((c & 1) ? x1 : x0), Y = (float)((c & 2) ? y1 : y0), Z = (float)((c & 4) ? z1 : z0);
+  // Lanes 0-11 each carry one matrix entry, loaded one projection ahead; the
+  // matrix goes through the stage header (FP64 and an FP32 copy) so the warp
+  // reads it from shared memory instead of holding it in registers.
+  double mnext = (lane < 12 && nproj > 0) ? __ldg(mats + lane) : 0.0;
   for (int p = 0; p < nproj; p++)
   {
     const int s = p % kStages, k = p / kStages;
     if (p >= kStages && !mbar_wait(&empty[s], (k - 1) & 1))
       return;
-    const double * M = mats + 12 * (long long)p;
-    double         m[12];
-#pragma unroll
-    for (int q = 0; q < 12; q++)
-      m[q] = __ldg(M + q);
-    const double w = m[8] * X + m[9] * Y + m[10] * Z + m[11];
-    const double un = m[0] * X + m[1] * Y + m[2] * Z + m[3];
-    const double vn = m[4] * X + m[5] * Y + m[6] * Z + m[7];
-    // The box only needs the corners to ~1e-4 pixel: divide in FP32 (the
-    // numerators are FP64) and reduce in FP32.
-    const float rw = 1.0f / (float)w;
-    float       umin = (float)un * rw, umax = umin, vmin = (float)vn * rw, vmax = vmin;
-    int         wsign = (w > 0.0) ? 1 : ((w < 0.0) ? 2 : 3); // bit set: 1 positive, 2 negative
+    StageHeader * h = hdr + s;
+    if (lane < 12)
+    {
+      h->m[lane] = mnext;
+      h->mf[lane] = (float)mnext;
+    }
+    if (lane < 12 && p + 1 < nproj)
+      mnext = __ldg(mats + 12 * (long long)(p + 1) + lane);
+    __syncwarp();
+    // The box needs the corners to ~1e-4 pixel only: FP32 is enough.
+    const float * mf = h->mf;
+    const float   tw = mf[8] * X, ty = mf[9] * Y, tz = mf[10] * Z;
+    const float   w = tw + ty + tz + mf[11];
+    const float   wtol = 1e-4f * (fabsf(tw) + fabsf(ty) + fabsf(tz) + fabsf(mf[11]));
+    const float   rw = 1.0f / w;
+    float         umin = fmaf(mf[0], X, fmaf(mf[1], Y, fmaf(mf[2], Z, mf[3]))) * rw, umax = umin;
+    float         vmin = fmaf(mf[4], X, fmaf(mf[5], Y, fmaf(mf[6], Z, mf[7]))) * rw, vmax = vmin;
+    int           wsign = (w > wtol) ? 1 : ((w < -wtol) ? 2 : 3); // bits: 1 positive, 2 negative
 #pragma unroll
     for (int o = 1; o < 8; o <<= 1)
     {
@@ -166,7 +178,7 @@ bp_producer(const CUtensorMap * tmap, const float * __restrict__ proj, const dou
     }
     // The tile's image is the hull of its projected corners only when w has
     // one sign over the tile (no voxel at the source plane).  Matrices are
-    // finite (checked on the host), so a NaN or infinite u/v needs w == 0 at
+    // finite (checked on the host), so a NaN or infinite u/v needs w near 0 at
     // a corner, which fails the sign test.
     const float margin = 0.05f;
     bool        fast = (wsign == 1 || wsign == 2) && isfinite(umin) && isfinite(umax) && isfinite(vmin) &&
@@ -178,8 +190,14 @@ bp_producer(const CUtensorMap * tmap, const float * __restrict__ proj, const dou
       vb = (int)floorf(vmin - margin);
       fast = (umax + margin < (float)(ub + BW - 1)) && (vmax + margin < (float)(vb + BH - 1));
     }
-    StageHeader * h = hdr + s;
-    float *       box = boxes + s * (BW * BH);
+    // Every voxel of the tile fails RTK's acceptance test (0 <= u < nu-1,
+    // 0 <= v < nv-1) when its footprint lies beyond a detector edge.
+    const bool skip = fast && ((umax + margin < 0.f) || (umin - margin >= (float)(nu - 1)) ||
+                               (vmax + margin < 0.f) || (vmin - margin >= (float)(nv - 1)));
+    if (skip)
+      fast = false;
+    const double * m = h->m;
+    float * box = boxes + s * (BW * BH);
     if (lane == 0)
     {
       int flags = 0;
@@ -200,10 +218,7 @@ bp_producer(const CUtensorMap * tmap, const float * __restrict__ proj, const dou
         if (vmin - margin >= 0.0 && vmax + margin < nv - 1.0)
           flags |= kFlagVInterior;
       }
-#pragma unroll
-      for (int q = 0; q < 12; q++)
-        h->m[q] = m[q];
-      h->fl = make_int4(flags, ub, vb, 0);
+      h->fl = make_int4(skip ? kFlagSkip : flags, ub, vb, 0);
     }
     if (fast && use_tma)
     {
@@ -331,16 +346,29 @@ bp_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const float * __restri
           }
           else
           {
+            // Acceptance mask in FP32; voxels within kBand of a bound are
+            // re-decided in FP64 outside the unrolled loop.
             const float4 lim = h->lim;
+            unsigned     ok = 0, near = 0;
 #pragma unroll
             for (int j = 0; j < NYT; j++)
             {
               const float v = fmaf((float)j, dv, v0);
-              bool        vok = (v >= lim.z && v < lim.w);
-              if (fabsf(v - lim.z) < kBand || fabsf(v - lim.w) < kBand)
-                vok = accept_fp64(h->m, 1, X, y0 + j, Z, nv);
-              if (vok)
+              ok |= (v >= lim.z && v < lim.w) ? (1u << j) : 0u;
+              near |= (fabsf(v - lim.z) < kBand || fabsf(v - lim.w) < kBand) ? (1u << j) : 0u;
+            }
+            while (near)
+            {
+              const int j = __ffs(near) - 1;
+              near &= near - 1;
+              ok = accept_fp64(h->m, 1, X, y0 + j, Z, nv) ? (ok | (1u << j)) : (ok & ~(1u << j));
+            }
+#pragma unroll
+            for (int j = 0; j < NYT; j++)
+            {
+              if (ok & (1u << j))
               {
+                const float   v = fmaf((float)j, dv, v0);
                 const float   flv = floorf(v);
                 const float   fv = v - flv;
                 const float * q = col + (int)flv * BW;
@@ -353,7 +381,7 @@ bp_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const float * __restri
           }
         }
       }
-      else
+      else if (!(fl.x & kFlagSkip))
       {
         const long long pofs = (long long)p * nu * nv;
 #pragma unroll
@@ -440,8 +468,10 @@ struct BpConfig
 // register budget targets), in order of preference; the first whose box
 // holds the probed footprints is used unless the autotuner forces one.
 constexpr int           kNumBpConfigs = 6;
-static const BpConfig   kBpConfigs[kNumBpConfigs] = { { 64, 64, 16, 3 }, { 64, 64, 16, 2 }, { 64, 32, 8, 3 },
-                                                      { 64, 32, 8, 2 },  { 128, 64, 16, 1 }, { 128, 64, 8, 1 } };
+// Box widths of 68 and 132 floats put consecutive rows 4 banks apart, so taps
+// in the same column but different rows do not collide.
+static const BpConfig   kBpConfigs[kNumBpConfigs] = { { 68, 64, 16, 3 }, { 68, 64, 16, 2 }, { 68, 32, 8, 3 },
+                                                      { 68, 32, 8, 2 },  { 132, 64, 16, 1 }, { 132, 64, 8, 1 } };
 static thread_local int g_bp_forced_config = -1;
 static thread_local int g_bp_last_config = -1;
 
@@ -524,17 +554,17 @@ dispatch_tiled(int cfg, const CUtensorMap & tmap, bool use_tma, const float * d_
   switch (cfg)
   {
     case 0:
-      RTKB_BP_LAUNCH(64, 64, 16, 3);
+      RTKB_BP_LAUNCH(68, 64, 16, 3);
     case 1:
-      RTKB_BP_LAUNCH(64, 64, 16, 2);
+      RTKB_BP_LAUNCH(68, 64, 16, 2);
     case 2:
-      RTKB_BP_LAUNCH(64, 32, 8, 3);
+      RTKB_BP_LAUNCH(68, 32, 8, 3);
     case 3:
-      RTKB_BP_LAUNCH(64, 32, 8, 2);
+      RTKB_BP_LAUNCH(68, 32, 8, 2);
     case 4:
-      RTKB_BP_LAUNCH(128, 64, 16, 1);
+      RTKB_BP_LAUNCH(132, 64, 16, 1);
     default:
-      RTKB_BP_LAUNCH(128, 64, 8, 1);
+      RTKB_BP_LAUNCH(132, 64, 8, 1);
   }
 #undef RTKB_BP_LAUNCH
 }

@@ -119,6 +119,21 @@ int rtkb_backproject_matrices(const int vol_size[3], const int proj_size[3], int
                               const int * modes, int weighting, const float * d_proj, const float * d_vol_in,
                               float * d_vol_out, void * stream);
 
+/* ---- Joseph projector pair ----
+ * rtk::JosephForwardProjectionImageFilter
+ * (include/rtkJosephForwardProjectionImageFilter.hxx:182-427):
+ * d_proj_out = d_proj_in + line integrals of d_vol (one bilinear sample per
+ * main-direction slice, partial end weights, times the step length in mm).
+ * Replaces CUDA_forward_project.  d_proj_out may equal d_proj_in. */
+int rtkb_joseph_forward_project(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
+                                const float * d_vol, const float * d_proj_in, float * d_proj_out, void * stream);
+/* rtk::JosephBackProjectionImageFilter
+ * (include/rtkJosephBackProjectionImageFilter.hxx:57-323): the exact adjoint
+ * (bilinear splat), d_vol_out = d_vol_in + BP(d_proj).  Replaces
+ * CUDA_ray_cast_back_project.  d_vol_out may equal d_vol_in. */
+int rtkb_joseph_back_project(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
+                             const float * d_proj, const float * d_vol_in, float * d_vol_out, void * stream);
+
 /* Autotuner hook of the tiled backprojector (no reference counterpart):
  * force >= 0 selects configuration `force` (box size, voxels per thread
  * column, occupancy target) for later calls on this host thread, -1 restores

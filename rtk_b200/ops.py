@@ -60,6 +60,24 @@ def voxel_backproject(geometry, vol_desc, proj_desc, proj, vol_in, out=None, str
     return _backproject(load().rtkb_voxel_backproject, geometry, vol_desc, proj_desc, proj, vol_in, out, stream)
 
 
+def joseph_forward_project(geometry, vol_desc, proj_desc, vol, proj_in, out=None, stream=None):
+    """rtk::JosephForwardProjectionImageFilter: out = proj_in + Joseph line integrals of vol."""
+    torch = _torch()
+    _check_shape(vol, vol_desc, "volume")
+    _check_shape(proj_in, proj_desc, "projections")
+    if out is None:
+        out = torch.empty_like(proj_in)
+    _check_shape(out, proj_desc, "output")
+    check(load().rtkb_joseph_forward_project(geometry.handle, C.byref(vol_desc), C.byref(proj_desc), _ptr(vol),
+                                             _ptr(proj_in), _ptr(out), _stream(stream)))
+    return out
+
+
+def joseph_back_project(geometry, vol_desc, proj_desc, proj, vol_in, out=None, stream=None):
+    """rtk::JosephBackProjectionImageFilter: out = vol_in + Joseph backprojection of proj."""
+    return _backproject(load().rtkb_joseph_back_project, geometry, vol_desc, proj_desc, proj, vol_in, out, stream)
+
+
 def ramp_params(hann=0.0, cosine=0.0, hamming=0.0, ramlak=0.0, shepplogan=0.0, truncation=0.0, gpf=2, pad=2):
     from ._capi import RampParams
 

@@ -134,6 +134,41 @@ int rtkb_joseph_forward_project(const rtkb_geometry * g, const rtkb_image_desc *
 int rtkb_joseph_back_project(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
                              const float * d_proj, const float * d_vol_in, float * d_vol_out, void * stream);
 
+/* ---- conjugate gradient ----
+ * rtk::ConjugateGradientConeBeamReconstructionFilter
+ * (include/rtkConjugateGradientConeBeamReconstructionFilter.hxx:192-305) with
+ * rtk::ConjugateGradientImageFilter's iteration
+ * (include/rtkConjugateGradientImageFilter.hxx:108-258): normal equations
+ * A x = b, A = BP(W .* FP(.)) + tikhonov I with the Joseph pair, b = BP(W .* p),
+ * W = displaced-detector weights (no padding) of the input weights.  Vectors
+ * FP32; dot products, alpha and beta FP64, kept on the device.  Replaces
+ * CUDA_conjugate_gradient.
+ *
+ * A plan owns all device memory; one iteration is captured as a CUDA graph at
+ * start (on a private stream) and replayed by rtkb_cg_iterate. */
+typedef struct rtkb_cg_params
+{
+  double tikhonov;       /* Tikhonov weight (RTK's SetTikhonov), 0 = none */
+  int    use_cuda_graph; /* 1: replay a captured iteration graph */
+} rtkb_cg_params;
+typedef struct rtkb_cg rtkb_cg;
+int  rtkb_cg_create(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
+                    const rtkb_cg_params * params, rtkb_cg ** plan);
+/* Binds the iterate d_x (holds x0 on entry, updated in place) and computes
+ * r0 = b - A x0, p0 = r0.  d_weights may be NULL (all ones). */
+int  rtkb_cg_start(rtkb_cg * plan, const float * d_proj, const float * d_weights, int displaced_detector, float * d_x,
+                   void * stream);
+int  rtkb_cg_iterate(rtkb_cg * plan, int n, void * stream);
+/* Waits for `stream`; *rr = ||r_k||^2 of the normal equations, *rr0 = ||r_0||^2. */
+int  rtkb_cg_residual(rtkb_cg * plan, double * rr, double * rr0, int * iterations, void * stream);
+void rtkb_cg_destroy(rtkb_cg * plan);
+/* Whole reconstruction: at most max_iterations iterations, stopping early when
+ * ||r_k|| <= relative_residual * ||r_0|| (relative_residual <= 0: never). */
+int  rtkb_conjugate_gradient(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
+                             const rtkb_cg_params * params, const float * d_proj, const float * d_weights,
+                             int displaced_detector, float * d_x, int max_iterations, double relative_residual,
+                             int * iterations, double * final_relative_residual, void * stream);
+
 /* Autotuner hook of the tiled backprojector (no reference counterpart):
  * force >= 0 selects configuration `force` (box size, voxels per thread
  * column, occupancy target) for later calls on this host thread, -1 restores

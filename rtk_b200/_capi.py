@@ -136,3 +136,20 @@ def check(code: int) -> None:
     if code != RTKB_OK:
         msg = load().rtkb_last_error()
         raise RtkbError(code, msg.decode() if msg else "")
+
+
+class CgParams(C.Structure):
+    """rtkb_cg_params."""
+
+    _fields_ = [("tikhonov", C.c_double), ("use_cuda_graph", C.c_int)]
+
+
+SIGNATURES.update({
+    "rtkb_cg_create": (C.c_int, [_G, _IM, _IM, C.POINTER(CgParams), C.POINTER(C.c_void_p)]),
+    "rtkb_cg_start": (C.c_int, [_V, _V, _V, C.c_int, _V, _V]),
+    "rtkb_cg_iterate": (C.c_int, [_V, C.c_int, _V]),
+    "rtkb_cg_residual": (C.c_int, [_V, _D, _D, _I, _V]),
+    "rtkb_cg_destroy": (None, [_V]),
+    "rtkb_conjugate_gradient": (C.c_int, [_G, _IM, _IM, C.POINTER(CgParams), _V, _V, C.c_int, _V, C.c_int,
+                                          C.c_double, _I, _D, _V]),
+})

@@ -1,0 +1,467 @@
+// cg.cu -- conjugate-gradient cone-beam reconstruction on sm_100a.
+//
+// Restates rtk::ConjugateGradientConeBeamReconstructionFilter
+// (include/rtkConjugateGradientConeBeamReconstructionFilter.hxx:192-305),
+// rtk::ReconstructionConjugateGradientOperator
+// (include/rtkReconstructionConjugateGradientOperator.hxx:192-286) and
+// rtk::ConjugateGradientImageFilter::GenerateData
+// (include/rtkConjugateGradientImageFilter.hxx:108-258); replaces
+// CUDA_conjugate_gradient (src/rtkCudaConjugateGradientImageFilter.cu:80-166),
+// which calls cuBLAS with a handle per call and round-trips alpha and beta to
+// the host.
+//
+// A plan owns every device buffer, so one iteration allocates nothing and is
+// captured once as a CUDA graph.  Operator: A x = BP(W .* FP(x)) + tikhonov x
+// with the Joseph pair, W the displaced-detector weights of the input weights
+// (no padding).  Vectors are FP32; the dot products (deterministic two-pass
+// reductions), alpha and beta are FP64 and never leave the device.
+#include "rtkb_joseph.h"
+
+#include <cfloat>
+#include <cstring>
+
+struct rtkb_cg
+{
+  rtkb_geometry *          g = nullptr;  // private copy of the geometry
+  rtkb_image_desc          vol{}, proj{};
+  rtkb::JosephArgs         args{};
+  float                    tikhonov = 0.f;
+  bool                     use_graph = true;
+  long long                nvox = 0, npix = 0;
+  void *                   mem = nullptr; // one device allocation for everything below
+  rtkb::RayProj *          tab = nullptr;
+  float *                  W = nullptr; // weights (null: all ones)
+  float *                  tmp = nullptr;
+  float *                  R = nullptr;
+  float *                  P = nullptr;
+  float *                  AP = nullptr;
+  float *                  A = nullptr; // BP accumulator / FP transpose scratch
+  float *                  At = nullptr;
+  double *                 scal = nullptr; // rr, rr0, alpha, beta, pAp
+  double *                 partial = nullptr;
+  float *                  x = nullptr; // the iterate (caller's buffer)
+  cudaStream_t             cap = nullptr; // private stream the iteration graph is captured on
+  cudaGraph_t              graph = nullptr;
+  cudaGraphExec_t          exec = nullptr;
+  int                      iterations = 0;
+};
+
+namespace
+{
+
+constexpr int kRedBlocks = 148 * 4;
+constexpr int kRedThreads = 256;
+enum
+{
+  S_RR = 0,
+  S_RR0 = 1,
+  S_ALPHA = 2,
+  S_BETA = 3,
+  S_PAP = 4
+};
+
+__device__ __forceinline__ double
+block_sum(double v)
+{
+  __shared__ double sh[kRedThreads / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+    v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0)
+    sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double s = 0.;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < kRedThreads / 32; w++)
+      s += sh[w];
+  return s;
+}
+
+// partial[b] = sum over block b's fixed slice of a[i] * b[i] (FP64)
+__global__ void __launch_bounds__(kRedThreads)
+dot_partial_kernel(const float * __restrict__ a, const float * __restrict__ b, long long n, double * partial)
+{
+  double s = 0.;
+  for (long long i = blockIdx.x * (long long)kRedThreads + threadIdx.x; i < n; i += (long long)kRedBlocks * kRedThreads)
+    s = fma((double)a[i], (double)b[i], s);
+  s = block_sum(s);
+  if (threadIdx.x == 0)
+    partial[blockIdx.x] = s;
+}
+
+// x += alpha p; r -= alpha ap; partial of <r, r>
+__global__ void __launch_bounds__(kRedThreads)
+update_xr_kernel(float * __restrict__ x, float * __restrict__ r, const float * __restrict__ p,
+                 const float * __restrict__ ap, long long n, const double * __restrict__ scal, double * partial)
+{
+  const double alpha = scal[S_ALPHA];
+  const float  af = (float)alpha;
+  double       s = 0.;
+  for (long long i = blockIdx.x * (long long)kRedThreads + threadIdx.x; i < n; i += (long long)kRedBlocks * kRedThreads)
+  {
+    x[i] = fmaf(af, p[i], x[i]);
+    const float ri = fmaf(-af, ap[i], r[i]);
+    r[i] = ri;
+    s = fma((double)ri, (double)ri, s);
+  }
+  s = block_sum(s);
+  if (threadIdx.x == 0)
+    partial[blockIdx.x] = s;
+}
+
+__device__ __forceinline__ double
+sum_partials(const double * partial)
+{
+  // one warp, fixed order
+  double s = 0.;
+  for (int i = threadIdx.x; i < kRedBlocks; i += 32)
+    s += partial[i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+    s += __shfl_xor_sync(0xffffffffu, s, o);
+  return s;
+}
+
+// alpha = rr / (pAp + eps)
+__global__ void
+finalize_alpha_kernel(const double * partial, double * scal)
+{
+  const double pap = sum_partials(partial);
+  if (threadIdx.x == 0)
+  {
+    scal[S_PAP] = pap;
+    scal[S_ALPHA] = scal[S_RR] / (pap + DBL_MIN);
+  }
+}
+
+// beta = rr_new / (rr + eps); rr = rr_new
+__global__ void
+finalize_beta_kernel(const double * partial, double * scal)
+{
+  const double rr = sum_partials(partial);
+  if (threadIdx.x == 0)
+  {
+    scal[S_BETA] = rr / (scal[S_RR] + DBL_MIN);
+    scal[S_RR] = rr;
+  }
+}
+
+// rr = rr0 = sum of partials (start)
+__global__ void
+finalize_start_kernel(const double * partial, double * scal)
+{
+  const double rr = sum_partials(partial);
+  if (threadIdx.x == 0)
+  {
+    scal[S_RR] = rr;
+    scal[S_RR0] = rr;
+  }
+}
+
+// p = r + beta p
+__global__ void __launch_bounds__(256)
+update_p_kernel(float * __restrict__ p, const float * __restrict__ r, long long n, const double * __restrict__ scal)
+{
+  const float beta = (float)scal[S_BETA];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    p[i] = fmaf(beta, p[i], r[i]);
+}
+
+// r = r - ap; p = r (start: R0 = B - A x0)
+__global__ void __launch_bounds__(256)
+start_rp_kernel(float * __restrict__ r, float * __restrict__ p, const float * __restrict__ ap, long long n)
+{
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+  {
+    const float v = r[i] - ap[i];
+    r[i] = v;
+    p[i] = v;
+  }
+}
+
+// out = a .* b (b may be null: copy)
+__global__ void __launch_bounds__(256)
+mul_kernel(float * __restrict__ out, const float * __restrict__ a, const float * __restrict__ b, long long n)
+{
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = b ? a[i] * b[i] : a[i];
+}
+
+__global__ void __launch_bounds__(256)
+fill_kernel(float * __restrict__ out, float v, long long n)
+{
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = v;
+}
+
+unsigned
+grid_for(long long n)
+{
+  return (unsigned)std::min<long long>((n + 255) / 256, 148LL * 16);
+}
+
+// A P -> AP (uses tmp, A, At)
+cudaError_t
+apply_A(rtkb_cg * c, const float * in, float * out, cudaStream_t st)
+{
+  cudaError_t e = rtkb::joseph_forward_launch(c->args, in, c->A, nullptr, c->tmp, c->W, st);
+  if (e != cudaSuccess)
+    return e;
+  return rtkb::joseph_back_launch(c->args, c->tmp, c->A, c->At, nullptr, out, c->tikhonov != 0.f ? in : nullptr,
+                                  c->tikhonov, st);
+}
+
+cudaError_t
+enqueue_iteration(rtkb_cg * c, cudaStream_t st)
+{
+  cudaError_t e = apply_A(c, c->P, c->AP, st);
+  if (e != cudaSuccess)
+    return e;
+  dot_partial_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(c->P, c->AP, c->nvox, c->partial);
+  finalize_alpha_kernel<<<1, 32, 0, st>>>(c->partial, c->scal);
+  update_xr_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(c->x, c->R, c->P, c->AP, c->nvox, c->scal, c->partial);
+  finalize_beta_kernel<<<1, 32, 0, st>>>(c->partial, c->scal);
+  update_p_kernel<<<grid_for(c->nvox), 256, 0, st>>>(c->P, c->R, c->nvox, c->scal);
+  return cudaGetLastError();
+}
+
+void
+release(rtkb_cg * c)
+{
+  if (!c)
+    return;
+  if (c->exec)
+    cudaGraphExecDestroy(c->exec);
+  if (c->graph)
+    cudaGraphDestroy(c->graph);
+  if (c->mem)
+    cudaFree(c->mem);
+  if (c->cap)
+    cudaStreamDestroy(c->cap);
+  delete c->g;
+  delete c;
+}
+
+} // namespace
+
+extern "C" int
+rtkb_cg_create(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
+               const rtkb_cg_params * params, rtkb_cg ** out)
+{
+  using namespace rtkb;
+  if (!out)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "null plan pointer");
+  *out = nullptr;
+  int rc = joseph_check(g, vol, proj);
+  if (rc != RTKB_OK)
+    return rc;
+  rtkb_cg * c = nullptr;
+  try
+  {
+    c = new rtkb_cg();
+    c->g = new rtkb_geometry(*g);
+    c->vol = *vol;
+    c->proj = *proj;
+    c->tikhonov = params ? (float)params->tikhonov : 0.f;
+    c->use_graph = params ? params->use_cuda_graph != 0 : true;
+    c->nvox = num_pixels(*vol);
+    c->npix = num_pixels(*proj);
+    std::vector<RayProj> tab;
+    rc = joseph_tables(g->g, *vol, *proj, tab);
+    if (rc != RTKB_OK)
+    {
+      release(c);
+      return rc;
+    }
+    auto         up = [](size_t b) { return (b + 255) & ~size_t(255); };
+    const size_t tb = up(tab.size() * sizeof(RayProj)), pb = up((size_t)c->npix * 4), vb = up((size_t)c->nvox * 4);
+    const size_t sb = up(8 * sizeof(double)), rb = up(kRedBlocks * sizeof(double));
+    const size_t total = tb + 2 * pb + 5 * vb + sb + rb;
+    cudaError_t  e = cudaMalloc(&c->mem, total);
+    if (e == cudaSuccess && c->use_graph)
+      e = cudaStreamCreateWithFlags(&c->cap, cudaStreamNonBlocking);
+    if (e != cudaSuccess)
+    {
+      release(c);
+      return cuda_fail(e, "cudaMalloc (CG plan)");
+    }
+    char * m = static_cast<char *>(c->mem);
+    c->tab = reinterpret_cast<RayProj *>(m);
+    m += tb;
+    c->W = reinterpret_cast<float *>(m);
+    m += pb;
+    c->tmp = reinterpret_cast<float *>(m);
+    m += pb;
+    c->R = reinterpret_cast<float *>(m);
+    m += vb;
+    c->P = reinterpret_cast<float *>(m);
+    m += vb;
+    c->AP = reinterpret_cast<float *>(m);
+    m += vb;
+    c->A = reinterpret_cast<float *>(m);
+    m += vb;
+    c->At = reinterpret_cast<float *>(m);
+    m += vb;
+    c->scal = reinterpret_cast<double *>(m);
+    m += sb;
+    c->partial = reinterpret_cast<double *>(m);
+    e = cudaMemcpy(c->tab, tab.data(), tab.size() * sizeof(RayProj), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMemset(c->scal, 0, sb);
+    if (e != cudaSuccess)
+    {
+      release(c);
+      return cuda_fail(e, "CG plan upload");
+    }
+    joseph_args(c->args, *vol, *proj, c->tab);
+    *out = c;
+    return RTKB_OK;
+  }
+  catch (...)
+  {
+    release(c);
+    return fail(RTKB_ERR_OUT_OF_MEMORY, "host allocation failed");
+  }
+}
+
+extern "C" int
+rtkb_cg_start(rtkb_cg * c, const float * d_proj, const float * d_weights, int displaced_detector, float * d_x,
+              void * stream)
+{
+  using namespace rtkb;
+  if (!c || !d_proj || !d_x)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "null argument");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (c->exec)
+  {
+    cudaGraphExecDestroy(c->exec);
+    c->exec = nullptr;
+  }
+  if (c->graph)
+  {
+    cudaGraphDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  c->x = d_x;
+  c->iterations = 0;
+  // W = displaced-detector weights (no padding) of the input weights (ones by default)
+  const bool have_w = d_weights != nullptr;
+  if (displaced_detector)
+  {
+    if (!have_w)
+      fill_kernel<<<grid_for(c->npix), 256, 0, st>>>(c->tmp, 1.f, c->npix);
+    const int rc = rtkb_displaced_detector(c->g, &c->proj, 0, have_w ? d_weights : c->tmp, c->W, stream);
+    if (rc != RTKB_OK)
+      return rc;
+  }
+  else if (have_w)
+    RTKB_CUDA_TRY(cudaMemcpyAsync(c->W, d_weights, (size_t)c->npix * 4, cudaMemcpyDeviceToDevice, st));
+  else
+    fill_kernel<<<grid_for(c->npix), 256, 0, st>>>(c->W, 1.f, c->npix);
+  // R = B = BP(W .* p); AP = A x0; R -= AP; P = R
+  mul_kernel<<<grid_for(c->npix), 256, 0, st>>>(c->tmp, d_proj, c->W, c->npix);
+  cudaError_t e = joseph_back_launch(c->args, c->tmp, c->A, c->At, nullptr, c->R, nullptr, 0.f, st);
+  if (e == cudaSuccess)
+    e = apply_A(c, c->x, c->AP, st);
+  if (e != cudaSuccess)
+    return cuda_fail(e, "CG start");
+  start_rp_kernel<<<grid_for(c->nvox), 256, 0, st>>>(c->R, c->P, c->AP, c->nvox);
+  dot_partial_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(c->R, c->R, c->nvox, c->partial);
+  finalize_start_kernel<<<1, 32, 0, st>>>(c->partial, c->scal);
+  RTKB_CUDA_TRY(cudaGetLastError());
+  if (c->use_graph)
+  {
+    // capture one iteration once on the plan's private stream (the caller's
+    // may be the legacy default stream, which cannot be captured); later
+    // iterations replay it on the caller's stream
+    e = cudaStreamBeginCapture(c->cap, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess)
+    {
+      cudaError_t ei = enqueue_iteration(c, c->cap);
+      e = cudaStreamEndCapture(c->cap, &c->graph);
+      if (e == cudaSuccess)
+        e = ei;
+    }
+    if (e == cudaSuccess)
+      e = cudaGraphInstantiate(&c->exec, c->graph, 0);
+    if (e != cudaSuccess)
+      return cuda_fail(e, "CG graph capture");
+  }
+  return RTKB_OK;
+}
+
+extern "C" int
+rtkb_cg_iterate(rtkb_cg * c, int n, void * stream)
+{
+  using namespace rtkb;
+  if (!c || !c->x || n < 0)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "CG plan not started");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  for (int i = 0; i < n; i++)
+  {
+    cudaError_t e = c->exec ? cudaGraphLaunch(c->exec, st) : enqueue_iteration(c, st);
+    if (e != cudaSuccess)
+      return cuda_fail(e, "CG iteration");
+    c->iterations++;
+  }
+  return RTKB_OK;
+}
+
+extern "C" int
+rtkb_cg_residual(rtkb_cg * c, double * rr, double * rr0, int * iterations, void * stream)
+{
+  using namespace rtkb;
+  if (!c)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "null plan");
+  double       h[2] = { 0., 0. };
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  RTKB_CUDA_TRY(cudaMemcpyAsync(h, c->scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  RTKB_CUDA_TRY(cudaStreamSynchronize(st));
+  if (rr)
+    *rr = h[S_RR];
+  if (rr0)
+    *rr0 = h[S_RR0];
+  if (iterations)
+    *iterations = c->iterations;
+  return RTKB_OK;
+}
+
+extern "C" void
+rtkb_cg_destroy(rtkb_cg * c)
+{
+  release(c);
+}
+
+extern "C" int
+rtkb_conjugate_gradient(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
+                        const rtkb_cg_params * params, const float * d_proj, const float * d_weights,
+                        int displaced_detector, float * d_x, int max_iterations, double relative_residual,
+                        int * iterations, double * final_relative_residual, void * stream)
+{
+  using namespace rtkb;
+  rtkb_cg * c = nullptr;
+  int       rc = rtkb_cg_create(g, vol, proj, params, &c);
+  if (rc != RTKB_OK)
+    return rc;
+  rc = rtkb_cg_start(c, d_proj, d_weights, displaced_detector, d_x, stream);
+  double rr = 0., rr0 = 0.;
+  int    it = 0;
+  for (; rc == RTKB_OK && it < max_iterations; it++)
+  {
+    if (relative_residual > 0.)
+    {
+      rc = rtkb_cg_residual(c, &rr, &rr0, nullptr, stream);
+      if (rc != RTKB_OK || rr <= relative_residual * relative_residual * rr0)
+        break;
+    }
+    rc = rtkb_cg_iterate(c, 1, stream);
+  }
+  if (rc == RTKB_OK)
+    rc = rtkb_cg_residual(c, &rr, &rr0, nullptr, stream);
+  if (iterations)
+    *iterations = it;
+  if (final_relative_residual)
+    *final_relative_residual = rr0 > 0. ? std::sqrt(rr / rr0) : 0.;
+  rtkb_cg_destroy(c);
+  return rc;
+}

@@ -14,7 +14,7 @@
 // positions x0 + i*step (no accumulated drift).  Rays whose main direction is
 // x read (or scatter into) a z<->x transposed copy of the volume, so that
 // neighbouring rays touch neighbouring addresses for every main direction.
-#include "rtkb_internal.h"
+#include "rtkb_joseph.h"
 #include "rtkb_ptx.cuh"
 
 #include <cfloat>
@@ -22,24 +22,8 @@
 
 namespace
 {
-
-struct RayProj
-{
-  double pix2vol[12]; // rows 0-2 of the projection-index -> volume-index matrix
-  double src[3];      // source in volume index coordinates
-  double pad;
-};
-
-struct JosephArgs
-{
-  const RayProj * P;
-  int             nu, nv, np;
-  int             pidx0, pidx1, pidx2; // absolute index of buffer pixel (0, 0, 0)
-  int             n[3];                // volume size
-  int             vidx[3];             // volume region index
-  double          spacing[3];
-  double          bmin[3], bmax[3];
-};
+using rtkb::JosephArgs;
+using rtkb::RayProj;
 
 struct Ray
 {
@@ -229,7 +213,7 @@ border_taps(const JosephArgs & a, const Ray & r, const View & w, int sl, double 
 
 __global__ void __launch_bounds__(256)
 joseph_forward_kernel(JosephArgs a, const float * __restrict__ V, const float * __restrict__ Vt,
-                      const float * pin, float * pout)
+                      const float * pin, float * pout, const float * __restrict__ weights)
 {
   const int u = blockIdx.x * 32 + (threadIdx.x & 31);
   const int v = blockIdx.y * 8 + (threadIdx.x >> 5);
@@ -237,10 +221,12 @@ joseph_forward_kernel(JosephArgs a, const float * __restrict__ V, const float * 
   if (u >= a.nu || v >= a.nv)
     return;
   const long long po = ((long long)s * a.nv + v) * a.nu + u;
+  const float     base = pin ? pin[po] : 0.f;
+  const float     wgt = weights ? __ldg(weights + po) : 1.f;
   Ray             r;
   if (!setup_ray(a, a.P[s], u, v, s, true, r))
   {
-    pout[po] = pin[po];
+    pout[po] = weights ? base * wgt : base;
     return;
   }
   const View    w = view_for(a, r);
@@ -286,7 +272,8 @@ joseph_forward_kernel(JosephArgs a, const float * __restrict__ V, const float * 
     sum += (r.resE + 0.5) * (wt[0] * __ldg(vol + o[0]) + wt[2] * __ldg(vol + o[2]) + wt[1] * __ldg(vol + o[1]) +
                              wt[3] * __ldg(vol + o[3]));
   }
-  pout[po] = pin[po] + (float)(sum * r.norm);
+  const float val = base + (float)(sum * r.norm);
+  pout[po] = weights ? val * wgt : val;
 }
 
 __device__ __forceinline__ void
@@ -378,10 +365,11 @@ transpose_zx_kernel(const float * __restrict__ V, float * __restrict__ T, int nx
   }
 }
 
-// out[z][y][x] = in[z][y][x] + A[z][y][x] + At[x][y][z]
+// out[z][y][x] = in[z][y][x] + A[z][y][x] + At[x][y][z] (+ tau * x[z][y][x]);
+// in and x may be null.
 __global__ void __launch_bounds__(256)
 fold_transposed_kernel(const float * in, const float * __restrict__ A, const float * __restrict__ At, float * out,
-                       int nx, int ny, int nz)
+                       int nx, int ny, int nz, const float * __restrict__ xv, float tau)
 {
   __shared__ float tile[32][33];
   const int        y = blockIdx.y;
@@ -400,7 +388,12 @@ fold_transposed_kernel(const float * in, const float * __restrict__ A, const flo
     if (z < nz && x < nx)
     {
       const long long o = ((long long)z * ny + y) * nx + x;
-      out[o] = in[o] + A[o] + tile[tx][k];
+      float           r = A[o] + tile[tx][k];
+      if (in)
+        r += in[o];
+      if (xv)
+        r = fmaf(tau, xv[o], r);
+      out[o] = r;
     }
   }
 }
@@ -412,8 +405,8 @@ namespace rtkb
 
 // Per-projection ray set-up tables (ProjectionsRegionConstIteratorRayBasedWithFlatPanel::NewProjection,
 // include/rtkProjectionsRegionConstIteratorRayBasedWithFlatPanel.hxx:39-71).
-static int
-ray_tables(const Geometry & g, const rtkb_image_desc & vol, const rtkb_image_desc & proj, std::vector<RayProj> & out)
+int
+joseph_tables(const Geometry & g, const rtkb_image_desc & vol, const rtkb_image_desc & proj, std::vector<RayProj> & out)
 {
   double vpp2i[16], pi2pp[16];
   if (!physical_to_index(vol, vpp2i))
@@ -439,9 +432,10 @@ ray_tables(const Geometry & g, const rtkb_image_desc & vol, const rtkb_image_des
   return RTKB_OK;
 }
 
-static void
-fill_args(JosephArgs & a, const rtkb_image_desc & vol, const rtkb_image_desc & proj)
+void
+joseph_args(JosephArgs & a, const rtkb_image_desc & vol, const rtkb_image_desc & proj, const RayProj * d_tab)
 {
+  a.P = d_tab;
   a.nu = proj.size[0];
   a.nv = proj.size[1];
   a.np = proj.size[2];
@@ -458,9 +452,38 @@ fill_args(JosephArgs & a, const rtkb_image_desc & vol, const rtkb_image_desc & p
   }
 }
 
-static int
-joseph_common(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
-              std::vector<RayProj> & tab)
+cudaError_t
+joseph_forward_launch(const JosephArgs & a, const float * V, float * Vt, const float * pin, float * pout,
+                      const float * w, cudaStream_t st)
+{
+  const int  nx = a.n[0], ny = a.n[1], nz = a.n[2];
+  const dim3 tg((unsigned)(((nx + 31) / 32) * ((nz + 31) / 32)), (unsigned)ny);
+  transpose_zx_kernel<<<tg, 256, 0, st>>>(V, Vt, nx, ny, nz);
+  const dim3 grid((unsigned)((a.nu + 31) / 32), (unsigned)((a.nv + 7) / 8), (unsigned)a.np);
+  joseph_forward_kernel<<<grid, 256, 0, st>>>(a, V, Vt, pin, pout, w);
+  return cudaGetLastError();
+}
+
+cudaError_t
+joseph_back_launch(const JosephArgs & a, const float * proj, float * A, float * At, const float * vin, float * vout,
+                   const float * x, float tau, cudaStream_t st)
+{
+  const int       nx = a.n[0], ny = a.n[1], nz = a.n[2];
+  const long long nvox = (long long)nx * ny * nz;
+  cudaError_t     e = cudaMemsetAsync(A, 0, nvox * sizeof(float), st);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(At, 0, nvox * sizeof(float), st);
+  if (e != cudaSuccess)
+    return e;
+  const dim3 grid((unsigned)((a.nu + 31) / 32), (unsigned)((a.nv + 7) / 8), (unsigned)a.np);
+  joseph_back_kernel<<<grid, 256, 0, st>>>(a, proj, A, At);
+  const dim3 tg((unsigned)(((nx + 31) / 32) * ((nz + 31) / 32)), (unsigned)ny);
+  fold_transposed_kernel<<<tg, 256, 0, st>>>(vin, A, At, vout, nx, ny, nz, x, tau);
+  return cudaGetLastError();
+}
+
+int
+joseph_check(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj)
 {
   std::string why;
   if (!g)
@@ -473,7 +496,7 @@ joseph_common(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_i
     return fail(RTKB_ERR_INVALID_ARGUMENT, "Mismatch between the number of projections and the geometry entries.");
   if (proj->size[1] > 65535 * 8 || proj->size[2] > 65535 || vol->size[1] > 65535)
     return fail(RTKB_ERR_UNSUPPORTED, "image too large for one launch");
-  return ray_tables(g->g, *vol, *proj, tab);
+  return RTKB_OK;
 }
 
 } // namespace rtkb
@@ -485,32 +508,28 @@ rtkb_joseph_forward_project(const rtkb_geometry * g, const rtkb_image_desc * vol
   using namespace rtkb;
   try
   {
-    std::vector<RayProj> tab;
-    int                  rc = joseph_common(g, vol, proj, tab);
+    int rc = joseph_check(g, vol, proj);
     if (rc != RTKB_OK)
       return rc;
     if (!d_vol || !d_proj_in || !d_proj_out)
       return fail(RTKB_ERR_INVALID_ARGUMENT, "null buffer");
-    cudaStream_t    st = static_cast<cudaStream_t>(stream);
-    const long long nvox = num_pixels(*vol);
-    const size_t    tbytes = tab.size() * sizeof(RayProj);
-    const size_t    vbytes = (size_t)nvox * sizeof(float);
-    void *          scratch = nullptr;
-    RTKB_CUDA_TRY(cudaMallocAsync(&scratch, ((tbytes + 255) & ~size_t(255)) + vbytes, st));
+    std::vector<RayProj> tab;
+    rc = joseph_tables(g->g, *vol, *proj, tab);
+    if (rc != RTKB_OK)
+      return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t tbytes = (tab.size() * sizeof(RayProj) + 255) & ~size_t(255);
+    const size_t vbytes = (size_t)num_pixels(*vol) * sizeof(float);
+    void *       scratch = nullptr;
+    RTKB_CUDA_TRY(cudaMallocAsync(&scratch, tbytes + vbytes, st));
     RayProj *   d_tab = static_cast<RayProj *>(scratch);
-    float *     d_vt = reinterpret_cast<float *>(static_cast<char *>(scratch) + ((tbytes + 255) & ~size_t(255)));
-    cudaError_t e = cudaMemcpyAsync(d_tab, tab.data(), tbytes, cudaMemcpyHostToDevice, st);
+    float *     d_vt = reinterpret_cast<float *>(static_cast<char *>(scratch) + tbytes);
+    cudaError_t e = cudaMemcpyAsync(d_tab, tab.data(), tab.size() * sizeof(RayProj), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
     {
-      const int  nx = vol->size[0], ny = vol->size[1], nz = vol->size[2];
-      const dim3 tg((unsigned)(((nx + 31) / 32) * ((nz + 31) / 32)), (unsigned)ny);
-      transpose_zx_kernel<<<tg, 256, 0, st>>>(d_vol, d_vt, nx, ny, nz);
       JosephArgs a;
-      fill_args(a, *vol, *proj);
-      a.P = d_tab;
-      const dim3 grid((unsigned)((a.nu + 31) / 32), (unsigned)((a.nv + 7) / 8), (unsigned)a.np);
-      joseph_forward_kernel<<<grid, 256, 0, st>>>(a, d_vol, d_vt, d_proj_in, d_proj_out);
-      e = cudaGetLastError();
+      joseph_args(a, *vol, *proj, d_tab);
+      e = joseph_forward_launch(a, d_vol, d_vt, d_proj_in, d_proj_out, nullptr, st);
     }
     rc = (e == cudaSuccess) ? RTKB_OK : cuda_fail(e, "joseph forward");
     cudaError_t fe = cudaFreeAsync(scratch, st);
@@ -531,12 +550,15 @@ rtkb_joseph_back_project(const rtkb_geometry * g, const rtkb_image_desc * vol, c
   using namespace rtkb;
   try
   {
-    std::vector<RayProj> tab;
-    int                  rc = joseph_common(g, vol, proj, tab);
+    int rc = joseph_check(g, vol, proj);
     if (rc != RTKB_OK)
       return rc;
     if (!d_proj || !d_vol_in || !d_vol_out)
       return fail(RTKB_ERR_INVALID_ARGUMENT, "null buffer");
+    std::vector<RayProj> tab;
+    rc = joseph_tables(g->g, *vol, *proj, tab);
+    if (rc != RTKB_OK)
+      return rc;
     cudaStream_t    st = static_cast<cudaStream_t>(stream);
     const long long nvox = num_pixels(*vol);
     const size_t    tbytes = (tab.size() * sizeof(RayProj) + 255) & ~size_t(255);
@@ -545,21 +567,12 @@ rtkb_joseph_back_project(const rtkb_geometry * g, const rtkb_image_desc * vol, c
     RTKB_CUDA_TRY(cudaMallocAsync(&scratch, tbytes + 2 * vbytes, st));
     RayProj *   d_tab = static_cast<RayProj *>(scratch);
     float *     d_a = reinterpret_cast<float *>(static_cast<char *>(scratch) + tbytes);
-    float *     d_at = d_a + nvox;
     cudaError_t e = cudaMemcpyAsync(d_tab, tab.data(), tab.size() * sizeof(RayProj), cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess)
-      e = cudaMemsetAsync(d_a, 0, 2 * vbytes, st);
     if (e == cudaSuccess)
     {
       JosephArgs a;
-      fill_args(a, *vol, *proj);
-      a.P = d_tab;
-      const dim3 grid((unsigned)((a.nu + 31) / 32), (unsigned)((a.nv + 7) / 8), (unsigned)a.np);
-      joseph_back_kernel<<<grid, 256, 0, st>>>(a, d_proj, d_a, d_at);
-      const int  nx = vol->size[0], ny = vol->size[1], nz = vol->size[2];
-      const dim3 tg((unsigned)(((nx + 31) / 32) * ((nz + 31) / 32)), (unsigned)ny);
-      fold_transposed_kernel<<<tg, 256, 0, st>>>(d_vol_in, d_a, d_at, d_vol_out, nx, ny, nz);
-      e = cudaGetLastError();
+      joseph_args(a, *vol, *proj, d_tab);
+      e = joseph_back_launch(a, d_proj, d_a, d_a + nvox, d_vol_in, d_vol_out, nullptr, 0.f, st);
     }
     rc = (e == cudaSuccess) ? RTKB_OK : cuda_fail(e, "joseph back projection");
     cudaError_t fe = cudaFreeAsync(scratch, st);

@@ -1,0 +1,45 @@
+// rtkb_joseph.h -- internal interface of the Joseph projector pair, shared by
+// the C ABI entry points and the conjugate-gradient plan.
+#pragma once
+
+#include "rtkb_internal.h"
+
+namespace rtkb
+{
+
+struct RayProj
+{
+  double pix2vol[12]; // rows 0-2 of the projection-index -> volume-index matrix
+  double src[3];      // source in volume index coordinates
+  double pad;
+};
+
+struct JosephArgs
+{
+  const RayProj * P;
+  int             nu, nv, np;
+  int             pidx0, pidx1, pidx2; // absolute index of buffer pixel (0, 0, 0)
+  int             n[3];                // volume size
+  int             vidx[3];             // volume region index
+  double          spacing[3];
+  double          bmin[3], bmax[3];
+};
+
+
+// Per-projection ray tables of a stack (host side).
+int  joseph_tables(const Geometry & g, const rtkb_image_desc & vol, const rtkb_image_desc & proj,
+                   std::vector<RayProj> & out);
+void joseph_args(JosephArgs & a, const rtkb_image_desc & vol, const rtkb_image_desc & proj, const RayProj * d_tab);
+
+int joseph_check(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj);
+
+// Enqueue the forward projector: pout = w * (pin + FP(V)); pin, w may be null.
+// Vt: scratch of the volume's size (z<->x transposed copy).
+cudaError_t joseph_forward_launch(const JosephArgs & a, const float * V, float * Vt, const float * pin, float * pout,
+                                  const float * w, cudaStream_t st);
+// Enqueue the back projector: vout = vin + BP(proj) + tau * x; vin, x may be
+// null.  A, At: zero-initialised here, scratch of the volume's size each.
+cudaError_t joseph_back_launch(const JosephArgs & a, const float * proj, float * A, float * At, const float * vin,
+                               float * vout, const float * x, float tau, cudaStream_t st);
+
+} // namespace rtkb

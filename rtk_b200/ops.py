@@ -177,3 +177,67 @@ def device_status(stream=None) -> int:
     st = C.c_int(0)
     check(load().rtkb_device_status(_stream(stream), C.byref(st)))
     return st.value
+
+
+class ConjugateGradient:
+    """Plan of rtk::ConjugateGradientConeBeamReconstructionFilter (Joseph pair,
+    FP64 scalars on the device, one CUDA graph per iteration)."""
+
+    def __init__(self, geometry, vol_desc, proj_desc, tikhonov=0.0, use_cuda_graph=True):
+        from ._capi import CgParams
+
+        self._lib = load()
+        self.geometry = geometry
+        self.vol_desc, self.proj_desc = vol_desc, proj_desc
+        p = CgParams()
+        p.tikhonov, p.use_cuda_graph = tikhonov, int(use_cuda_graph)
+        h = C.c_void_p()
+        check(self._lib.rtkb_cg_create(geometry.handle, C.byref(vol_desc), C.byref(proj_desc), C.byref(p),
+                                       C.byref(h)))
+        self._h = h
+        self._keep = []
+
+    def start(self, proj, x, weights=None, displaced_detector=True, stream=None):
+        _check_shape(proj, self.proj_desc, "projections")
+        _check_shape(x, self.vol_desc, "volume")
+        if weights is not None:
+            _check_shape(weights, self.proj_desc, "weights")
+        self._keep = [proj, x, weights]
+        check(self._lib.rtkb_cg_start(self._h, _ptr(proj), _ptr(weights) if weights is not None else None,
+                                      int(displaced_detector), _ptr(x), _stream(stream)))
+        return self
+
+    def iterate(self, n=1, stream=None):
+        check(self._lib.rtkb_cg_iterate(self._h, int(n), _stream(stream)))
+
+    def residual(self, stream=None):
+        """(||r_k||^2, ||r_0||^2, k) -- synchronises the stream."""
+        rr, rr0, it = C.c_double(), C.c_double(), C.c_int()
+        check(self._lib.rtkb_cg_residual(self._h, C.byref(rr), C.byref(rr0), C.byref(it), _stream(stream)))
+        return rr.value, rr0.value, it.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.rtkb_cg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def conjugate_gradient(geometry, vol_desc, proj_desc, proj, x, niter, rel_residual=0.0, weights=None,
+                       displaced_detector=True, tikhonov=0.0, use_cuda_graph=True, stream=None):
+    """Whole CG reconstruction in place on x; returns (iterations, relative residual)."""
+    from ._capi import CgParams
+
+    p = CgParams()
+    p.tikhonov, p.use_cuda_graph = tikhonov, int(use_cuda_graph)
+    it, rel = C.c_int(), C.c_double()
+    check(load().rtkb_conjugate_gradient(geometry.handle, C.byref(vol_desc), C.byref(proj_desc), C.byref(p),
+                                         _ptr(proj), _ptr(weights) if weights is not None else None,
+                                         int(displaced_detector), _ptr(x), int(niter), float(rel_residual),
+                                         C.byref(it), C.byref(rel), _stream(stream)))
+    return it.value, rel.value

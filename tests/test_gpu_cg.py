@@ -1,0 +1,121 @@
+"""GPU conjugate gradient (rtkb_cg_*, rtkb_conjugate_gradient) against the
+FP64 oracle restating include/rtkConjugateGradientImageFilter.hxx with the
+Joseph operator of include/rtkReconstructionConjugateGradientOperator.hxx, and
+RTK's CG reconstruction test (test/rtkconjugategradientreconstructiontest.cxx:
+err/px < 0.08, PSNR > 23) on the GPU result."""
+import numpy as np
+import pytest
+
+from tests import phantoms
+from tests.gpu_util import pair_geometry, pair_image, rel_l2, to_gpu, to_np
+
+pytestmark = pytest.mark.gpu
+
+# CG iterates amplify rounding differences with every iteration; FP32 vectors
+# against FP64 stay within this bound over the iteration counts tested here.
+CG_TOL = 1e-4
+
+
+def _problem(rtkb, oracle, n=40, vsize=(32, 28, 30), offset=0.0, seed=0):
+    params = [(600.0, 900.0, i * 360.0 / n, offset, 0.0) for i in range(n)]
+    gl, go = pair_geometry(rtkb, oracle, params)
+    vd, vo = pair_image(rtkb, oracle, vsize, (8.0,) * 3)
+    pd, po = pair_image(rtkb, oracle, (56, 48, n), (8.0, 8.0, 1.0))
+    rng = np.random.default_rng(seed)
+    truth = rng.uniform(0.0, 1.0, size=oracle.shape_of(vo))
+    p = oracle.joseph_forward(go, vo, truth, po).astype(np.float32).astype(np.float64)
+    return gl, go, vd, vo, pd, po, p
+
+
+def test_cg_matches_oracle_iterates_and_residuals(rtkb, oracle):
+    gl, go, vd, vo, pd, po, p = _problem(rtkb, oracle)
+    niter = 6
+    ref_x, ref_res = oracle.cg_joseph(go, vo, po, p, niter)
+    import torch
+
+    x = torch.zeros(oracle.shape_of(vo), device="cuda")
+    cg = rtkb.ops.ConjugateGradient(gl, vd, pd)
+    cg.start(to_gpu(p), x, displaced_detector=False)
+    res = [cg.residual()[0]]
+    for _ in range(niter):
+        cg.iterate(1)
+        res.append(cg.residual()[0])
+    cg.close()
+    assert rel_l2(to_np(x), ref_x) < CG_TOL
+    np.testing.assert_allclose(res, ref_res, rtol=CG_TOL)
+    assert rtkb.ops.device_status() == 0
+
+
+def test_cg_graph_equals_eager(rtkb, oracle):
+    gl, go, vd, vo, pd, po, p = _problem(rtkb, oracle, seed=1)
+    import torch
+
+    outs = []
+    for graph in (True, False):
+        x = torch.zeros(oracle.shape_of(vo), device="cuda")
+        cg = rtkb.ops.ConjugateGradient(gl, vd, pd, use_cuda_graph=graph)
+        cg.start(to_gpu(p), x, displaced_detector=False)
+        cg.iterate(4)
+        outs.append((to_np(x), cg.residual()[0]))
+        cg.close()
+    # the Joseph back projector accumulates with atomics, so runs agree to FP32
+    # rounding rather than bitwise
+    assert rel_l2(outs[0][0], outs[1][0]) < 1e-5
+    assert abs(outs[0][1] / outs[1][1] - 1) < 1e-5
+
+
+def test_cg_tikhonov_weights_and_warm_start(rtkb, oracle):
+    gl, go, vd, vo, pd, po, p = _problem(rtkb, oracle, seed=2)
+    rng = np.random.default_rng(3)
+    w = rng.uniform(0.5, 2.0, size=p.shape).astype(np.float32).astype(np.float64)
+    x0 = rng.uniform(0.0, 0.5, size=oracle.shape_of(vo)).astype(np.float32).astype(np.float64)
+    ref_x, _ = oracle.cg_joseph(go, vo, po, p, 4, x0=x0, weights=w, tikhonov=0.3)
+    x = to_gpu(x0)
+    cg = rtkb.ops.ConjugateGradient(gl, vd, pd, tikhonov=0.3)
+    cg.start(to_gpu(p), x, weights=to_gpu(w), displaced_detector=False)
+    cg.iterate(4)
+    assert rel_l2(to_np(x), ref_x) < CG_TOL
+    cg.close()
+
+
+def test_cg_displaced_detector_weights(rtkb, oracle):
+    """W = displaced-detector weights of ones (RTK's default for CG)."""
+    gl, go, vd, vo, pd, po, p = _problem(rtkb, oracle, offset=60.0, seed=4)
+    ones = np.ones(p.shape)
+    wref, _, _ = oracle.displaced_detector(go, po, ones, pad=False)
+    ref_x, _ = oracle.cg_joseph(go, vo, po, p, 3, weights=wref)
+    import torch
+
+    x = torch.zeros(oracle.shape_of(vo), device="cuda")
+    it, rel = rtkb.ops.conjugate_gradient(gl, vd, pd, to_gpu(p), x, 3, displaced_detector=True)
+    assert it == 3 and 0 < rel < 1
+    assert rel_l2(to_np(x), ref_x) < CG_TOL
+
+
+def test_cg_early_stop_on_relative_residual(rtkb, oracle):
+    gl, go, vd, vo, pd, po, p = _problem(rtkb, oracle, seed=5)
+    import torch
+
+    x = torch.zeros(oracle.shape_of(vo), device="cuda")
+    it, rel = rtkb.ops.conjugate_gradient(gl, vd, pd, to_gpu(p), x, 200, rel_residual=1e-2,
+                                          displaced_detector=False)
+    assert rel <= 1e-2 and it < 200
+
+
+def test_cg_sphere_like_rtkconjugategradientreconstructiontest(rtkb, oracle):
+    """Sphere of radius 90 mm, 64^3 at 4 mm, 180 projections, 5 iterations
+    (RTK's test, Joseph back projector case)."""
+    n = 180
+    params = [(600.0, 1200.0, i * 360.0 / n) for i in range(n)]
+    gl, go = pair_geometry(rtkb, oracle, params)
+    vd, vo = pair_image(rtkb, oracle, (64, 64, 64), (4.0,) * 3, origin=(-126.0,) * 3)
+    pd, po = pair_image(rtkb, oracle, (64, 64, n), (8.0, 8.0, 1.0), origin=(-254.0, -254.0, 0.0))
+    sphere = phantoms.ellipsoid((0.0, 0.0, 0.0), (90.0, 90.0, 90.0), np.eye(3), 1.0)[None]
+    p = oracle.project_ellipsoids(go, po, sphere)
+    ref = oracle.draw_ellipsoids(vo, sphere)
+    import torch
+
+    x = torch.zeros((64, 64, 64), device="cuda")
+    rtkb.ops.conjugate_gradient(gl, vd, pd, to_gpu(p), x, 5, displaced_detector=True)
+    err, psnr, ok = phantoms.check_image_quality(to_np(x), ref, 0.08, 23.0, 2.0)
+    assert ok, (err, psnr)

@@ -112,6 +112,24 @@ int rtkb_fdk_backproject(const rtkb_geometry * g, const rtkb_image_desc * vol, c
                          const float * d_proj, const float * d_vol_in, float * d_vol_out, void * stream);
 int rtkb_voxel_backproject(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
                            const float * d_proj, const float * d_vol_in, float * d_vol_out, void * stream);
+/* rtkb_fdk_backproject without device allocations (no counterpart in the
+ * reference).  For callers that cannot allocate device memory during a
+ * reconstruction: an application whose device memory is reserved by its own
+ * allocator, or an on-line loop that must avoid cudaMalloc's implicit device
+ * synchronisation.  Same arguments and results as rtkb_fdk_backproject; its
+ * only scratch (the stack's FP64 matrices and path modes) is a file-scope
+ * device array sized for at most 2048 projections (about 200 KB, held by every
+ * GPU that loads the library until the process exits); larger stacks are
+ * rejected with RTKB_ERR_INVALID_ARGUMENT.  It calls no cudaMalloc, cudaFree
+ * or allocating library routine.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) with that device current;
+ * make that first call before any stream capture.  All calls share the array
+ * and it keeps the last call's contents: calls whose GPU work overlaps (other
+ * streams, other host threads) race on it and must be serialised by the
+ * caller. */
+int rtkb_fdk_backproject_static_scratch(const rtkb_geometry * g, const rtkb_image_desc * vol,
+                                        const rtkb_image_desc * proj, const float * d_proj, const float * d_vol_in,
+                                        float * d_vol_out, void * stream);
 /* Matrix-level form mirroring CUDA_reconstruct_conebeam: n_proj FP64
  * matrices (volume buffer index -> projection buffer index), modes as above,
  * weighting 1 = FDK (1/w^2), 0 = none. */

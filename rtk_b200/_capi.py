@@ -153,3 +153,7 @@ SIGNATURES.update({
     "rtkb_conjugate_gradient": (C.c_int, [_G, _IM, _IM, C.POINTER(CgParams), _V, _V, C.c_int, _V, C.c_int,
                                           C.c_double, _I, _D, _V]),
 })
+
+SIGNATURES.update({
+    "rtkb_fdk_backproject_static_scratch": (C.c_int, [_G, _IM, _IM, _V, _V, _V, _V]),
+})

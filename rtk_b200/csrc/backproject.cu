@@ -29,6 +29,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 
 namespace rtkb
 {
@@ -606,7 +607,8 @@ to_buffer_matrix(const rtkb_image_desc & vol, const rtkb_image_desc & proj, int 
 
 int
 backproject_buffer(const int vol_size[3], const int proj_size[3], int nproj, const double * mats, const int * modes,
-                   bool fdk, const float * d_proj, const float * d_vin, float * d_vout, cudaStream_t st)
+                   bool fdk, const float * d_proj, const float * d_vin, float * d_vout, cudaStream_t st,
+                   void * fixed_scratch = nullptr)
 {
   const int nx = vol_size[0], ny = vol_size[1], nz = vol_size[2];
   const int nu = proj_size[0], nv = proj_size[1];
@@ -630,10 +632,12 @@ backproject_buffer(const int vol_size[3], const int proj_size[3], int nproj, con
     if (modes[p] != 2)
       all_opt_y = false;
   }
-  // matrices and modes in one stream-ordered scratch allocation
+  // matrices and modes in one scratch block: the caller's when given, else a
+  // stream-ordered allocation
   const size_t mbytes = sizeof(double) * 12 * (size_t)nproj;
-  void *       scratch = nullptr;
-  RTKB_CUDA_TRY(cudaMallocAsync(&scratch, mbytes + sizeof(int) * nproj, st));
+  void *       scratch = fixed_scratch;
+  if (!scratch)
+    RTKB_CUDA_TRY(cudaMallocAsync(&scratch, mbytes + sizeof(int) * nproj, st));
   double * d_mats = static_cast<double *>(scratch);
   int *    d_modes = reinterpret_cast<int *>(static_cast<char *>(scratch) + mbytes);
   int      rc = RTKB_OK;
@@ -701,15 +705,19 @@ backproject_buffer(const int vol_size[3], const int proj_size[3], int nproj, con
              : dispatch_tiled<false>(cfg, tmap, use_tma, d_proj, d_mats, nproj, nu, nv, nx, ny, nz, d_vin, d_vout,
                                      st);
   } while (0);
-  cudaError_t fe = cudaFreeAsync(scratch, st);
-  if (rc == RTKB_OK && fe != cudaSuccess)
-    rc = cuda_fail(fe, "cudaFreeAsync");
+  if (!fixed_scratch)
+  {
+    cudaError_t fe = cudaFreeAsync(scratch, st);
+    if (rc == RTKB_OK && fe != cudaSuccess)
+      rc = cuda_fail(fe, "cudaFreeAsync");
+  }
   return rc;
 }
 
 static int
 backproject_geometry(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
-                     const float * d_proj, const float * d_vin, float * d_vout, void * stream, bool fdk)
+                     const float * d_proj, const float * d_vin, float * d_vout, void * stream, bool fdk,
+                     void * fixed_scratch = nullptr)
 {
   std::string why;
   if (!g)
@@ -731,7 +739,7 @@ backproject_geometry(const rtkb_geometry * g, const rtkb_image_desc * vol, const
     to_buffer_matrix(*vol, *proj, modes[s], m, mats.data() + 12 * s);
   }
   return backproject_buffer(vol->size, proj->size, nproj, mats.data(), modes.data(), fdk, d_proj, d_vin, d_vout,
-                            static_cast<cudaStream_t>(stream));
+                            static_cast<cudaStream_t>(stream), fixed_scratch);
 }
 
 } // namespace rtkb
@@ -809,4 +817,70 @@ rtkb_backproject_config(int force, int * last_used, int * count)
     *count = kNumBpConfigs;
   g_bp_forced_config = force;
   return RTKB_OK;
+}
+
+// ---- FDK backprojection without device allocations ----------------------------
+//
+// Some callers cannot allocate device memory while they reconstruct: an
+// application whose device memory is entirely reserved by its own allocator
+// (an image pipeline's GPU buffer pool, a framework's caching allocator at its
+// limit), or an on-line reconstruction loop that must not take cudaMalloc's
+// implicit device synchronisation.  rtkb_fdk_backproject_static_scratch serves
+// them: its only scratch (the FP64 projection matrices and path modes of the
+// stack) lives in the file-scope device array below, which every GPU that loads
+// this library holds from module load until the process exits.
+namespace
+{
+constexpr int kStaticMaxProjections = 2048;
+constexpr int kStaticBytesPerProjection = 12 * sizeof(double) + sizeof(int);
+static __device__ __align__(256) unsigned char g_bp_static_scratch[kStaticMaxProjections * kStaticBytesPerProjection];
+
+std::mutex g_static_mutex;
+void *     g_static_address[256] = {}; // per device ordinal
+
+// Device address of g_bp_static_scratch on the current device, looked up once
+// per device with that device current.  In host code the array's name is only
+// a stand-in for the symbol, never a device address.
+int
+static_scratch_address(void ** out)
+{
+  int dev = 0;
+  RTKB_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 256)
+    return rtkb::fail(RTKB_ERR_UNSUPPORTED, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_static_mutex);
+  if (!g_static_address[dev])
+  {
+    void *      p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_bp_static_scratch);
+    if (e != cudaSuccess)
+      return rtkb::cuda_fail(e, "cudaGetSymbolAddress(g_bp_static_scratch)");
+    g_static_address[dev] = p;
+  }
+  *out = g_static_address[dev];
+  return RTKB_OK;
+}
+} // namespace
+
+extern "C" int
+rtkb_fdk_backproject_static_scratch(const rtkb_geometry * g, const rtkb_image_desc * vol,
+                                    const rtkb_image_desc * proj, const float * d_proj, const float * d_vol_in,
+                                    float * d_vol_out, void * stream)
+{
+  if (proj && proj->size[2] > kStaticMaxProjections)
+    return rtkb::fail(RTKB_ERR_INVALID_ARGUMENT,
+                      "rtkb_fdk_backproject_static_scratch: the stack has more than 2048 projections, the size of "
+                      "its static scratch; split the stack or use rtkb_fdk_backproject");
+  try
+  {
+    void * scratch = nullptr;
+    int    rc = static_scratch_address(&scratch);
+    if (rc != RTKB_OK)
+      return rc;
+    return rtkb::backproject_geometry(g, vol, proj, d_proj, d_vol_in, d_vol_out, stream, true, scratch);
+  }
+  catch (...)
+  {
+    return rtkb::fail(RTKB_ERR_OUT_OF_MEMORY, "host allocation failed");
+  }
 }

@@ -241,3 +241,10 @@ def conjugate_gradient(geometry, vol_desc, proj_desc, proj, x, niter, rel_residu
                                          int(displaced_detector), _ptr(x), int(niter), float(rel_residual),
                                          C.byref(it), C.byref(rel), _stream(stream)))
     return it.value, rel.value
+
+
+def fdk_backproject_static_scratch(geometry, vol_desc, proj_desc, proj, vol_in, out=None, stream=None):
+    """rtkb_fdk_backproject_static_scratch: FDK backprojection that allocates no
+    device memory (stacks of at most 2048 projections; see include/rtkb200.h)."""
+    return _backproject(load().rtkb_fdk_backproject_static_scratch, geometry, vol_desc, proj_desc, proj, vol_in,
+                        out, stream)

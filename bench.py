@@ -153,23 +153,77 @@ def make_geometry():
 
 def make_projections(torch, g, gen):
     """Seeded synthetic projections with the workload's shape: analytic line
-    integrals of 20 random ellipsoids when the phantom projector is available,
-    else seeded uniform values (the backprojector's cost does not depend on
-    the values)."""
+    integrals (on the GPU, rtkb_project_ellipsoids) of 20 random ellipsoids with
+    semi-axes 5-80 mm, centres in a 200 mm sphere, random rotations and
+    densities 0.1-1 (no public dataset is named for this configuration)."""
     import rtk_b200 as rtkb
+    from tests import phantoms
 
     pd = rtkb.make_desc((NU, NV, NP), (PIX, PIX, 1.0))
-    p = None
-    if hasattr(rtkb.ops, "project_ellipsoids"):
-        from tests import phantoms
+    ell = phantoms.random_ellipsoids(20, SEED)
+    p = rtkb.ops.project_ellipsoids(g, pd, ell)
+    return pd, p, "analytic line integrals of 20 seeded random ellipsoids (semi-axes 5-80 mm)"
 
-        ell = phantoms.random_ellipsoids(20, SEED)
-        p = rtkb.ops.project_ellipsoids(g, pd, ell)
-        kind = "analytic line integrals of 20 seeded random ellipsoids (semi-axes 5-80 mm)"
-    else:
-        p = torch.rand((NP, NV, NU), device="cuda", generator=gen)
-        kind = "seeded uniform random projections"
-    return pd, p, kind
+
+def fdk_pipeline_ms(torch, rtkb, g, vd, pd, proj, stream, reps=3):
+    """Whole FDK (fused weighting + Hann ramp filter, then backprojection) on the
+    benchmark stack, device time per reconstruction."""
+    zero = torch.zeros(tuple(reversed(list(vd.size))), device="cuda")
+    ramp = rtkb.ops.ramp_params(hann=1.0)
+
+    def run():
+        f, fd = rtkb.ops.fdk_preprocess(g, pd, proj, ramp, stream=stream)
+        rtkb.ops.fdk_backproject(g, vd, fd, f, zero, out=zero, stream=stream)
+
+    run()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        run()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def cg_seconds_to_residual(torch, rtkb, stream, tol=1e-3, max_iter=300):
+    """CG configuration: 256^3 at 1 mm, 360 projections of 512x384 at 0.8 mm
+    (SID 1000, SDD 1536) of 20 seeded random ellipsoids with pre-log Poisson
+    noise at I0 = 5e4; Joseph pair, FP32 vectors, FP64 scalars, one CUDA graph
+    per iteration.  Seconds until the normal-equation residual falls to
+    tol * ||r_0||, device time from the start of CG to convergence."""
+    from tests import phantoms
+
+    n = 360
+    g = rtkb.geometry.circular(n, SID, SDD)
+    vd = rtkb.make_desc((256, 256, 256), (1.0, 1.0, 1.0))
+    pd = rtkb.make_desc((512, 384, n), (0.8, 0.8, 1.0))
+    ell = phantoms.random_ellipsoids(20, SEED + 2, centre_radius=60.0, axis_range=(5.0, 60.0))
+    ell[:, 15] *= 0.02  # attenuation in 1/mm: densities 0.002-0.02
+    clean = rtkb.ops.project_ellipsoids(g, pd, ell, stream=stream)
+    i0 = 5e4
+    gen = torch.Generator(device="cuda").manual_seed(SEED + 3)
+    counts = torch.poisson(i0 * torch.exp(-clean), generator=gen).clamp_(min=1.0)
+    p = (-torch.log(counts / i0)).contiguous()
+    x = torch.zeros((256, 256, 256), device="cuda")
+    cg = rtkb.ops.ConjugateGradient(g, vd, pd)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    cg.start(p, x, stream=stream)
+    rr, rr0, it = cg.residual(stream)
+    while rr > tol * tol * rr0 and it < max_iter:
+        cg.iterate(1, stream)
+        rr, rr0, it = cg.residual(stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    secs = e0.elapsed_time(e1) / 1e3
+    cg.close()
+    return {"seconds_to_rel_residual_1e-3": secs if rr <= tol * tol * rr0 else None, "iterations": it,
+            "relative_residual": (rr / rr0) ** 0.5, "seconds_per_iteration": secs / max(it, 1),
+            "config": "256^3 @1mm <- 360 x 512x384 @0.8mm, SID 1000, SDD 1536, 20 random ellipsoids, "
+                      "Poisson I0=5e4, Joseph pair, FP32 vectors / FP64 scalars, CUDA graph per iteration",
+            "learned_pcg": None}
 
 
 def smem_peak_gbs(torch, lib, stream) -> float:
@@ -267,6 +321,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra-legs", action="store_true",
+                    help="skip the FDK pipeline and CG seconds-to-residual legs")
     ap.add_argument("--profile-case", action="store_true",
                     help="small case for ncu captures: 256^3 @1mm from 360 projections, device-timed region only")
     args = ap.parse_args()
@@ -377,6 +433,9 @@ def main():
             "roofline": roofline, "clocks": clocks, "gpu_launches": args.steps,
             "gpu_launches_note": "one rtkb backprojection kernel per step (plus one matrix upload copy)"}
 
+    if world == 1 and not args.no_extra_legs:
+        line["fdk_pipeline_ms"] = fdk_pipeline_ms(torch, rtkb, g, vd, pd, proj, stream)
+        line["cg"] = cg_seconds_to_residual(torch, rtkb, stream)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             threads = os.cpu_count() or 1

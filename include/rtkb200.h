@@ -265,6 +265,15 @@ typedef struct rtkb_fdk_preprocess_params
 int rtkb_fdk_preprocess(const rtkb_geometry * g, const rtkb_image_desc * proj, const rtkb_fdk_preprocess_params * p,
                         rtkb_image_desc * out, const float * d_in, float * d_out, void * stream);
 
+/* ---- phantoms ----
+ * Analytic line integrals of ellipsoids (rtk::ProjectGeometricPhantomImageFilter
+ * semantics, include/rtkRayConvexIntersectionImageFilter.hxx:57-84): d_out =
+ * sum over ellipsoids of density x length of the source-to-pixel segment inside
+ * it.  Each ellipsoid is 16 doubles: centre (3), semi-axes (3), rotation
+ * (3x3 row-major, local -> world), density.  FP64 arithmetic. */
+int rtkb_project_ellipsoids(const rtkb_geometry * g, const rtkb_image_desc * proj, int n_ellipsoids,
+                            const double * ellipsoids, float * d_out, void * stream);
+
 /* ---- measurement ----
  * Shared-memory gather peak (no reference counterpart): n_blocks CTAs of 256
  * threads each perform `iters` bilinear-footprint gathers (4 x 4 bytes) from

@@ -157,3 +157,7 @@ SIGNATURES.update({
 SIGNATURES.update({
     "rtkb_fdk_backproject_static_scratch": (C.c_int, [_G, _IM, _IM, _V, _V, _V, _V]),
 })
+
+SIGNATURES.update({
+    "rtkb_project_ellipsoids": (C.c_int, [_G, _IM, C.c_int, _D, _V, _V]),
+})

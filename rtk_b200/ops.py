@@ -248,3 +248,18 @@ def fdk_backproject_static_scratch(geometry, vol_desc, proj_desc, proj, vol_in, 
     device memory (stacks of at most 2048 projections; see include/rtkb200.h)."""
     return _backproject(load().rtkb_fdk_backproject_static_scratch, geometry, vol_desc, proj_desc, proj, vol_in,
                         out, stream)
+
+
+def project_ellipsoids(geometry, proj_desc, ellipsoids, out=None, stream=None):
+    """Analytic projections of ellipsoids (16 doubles each: centre, semi-axes,
+    rotation local->world row-major, density) onto the described stack."""
+    import numpy as np
+
+    torch = _torch()
+    e = np.ascontiguousarray(ellipsoids, dtype=np.float64).reshape(-1, 16)
+    if out is None:
+        out = torch.empty(shape_of(proj_desc), device="cuda", dtype=torch.float32)
+    _check_shape(out, proj_desc, "output")
+    check(load().rtkb_project_ellipsoids(geometry.handle, C.byref(proj_desc), e.shape[0],
+                                         e.ctypes.data_as(C.POINTER(C.c_double)), _ptr(out), _stream(stream)))
+    return out

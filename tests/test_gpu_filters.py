@@ -160,3 +160,13 @@ def test_fdk_gpu_shepp_logan_like_rtkfdktest(rtkb, oracle):
     assert rel_l2(rec, ref) < REL_L2_TOL
     err, psnr, ok = phantoms.check_image_quality(rec * phantoms.fov_mask(go, vo, po), ref_img, 0.03, 26.0, 2.0)
     assert ok, (err, psnr)
+
+
+def test_project_ellipsoids_matches_oracle(rtkb, oracle):
+    params = [(1000.0, 1536.0, i * 12.0, 5.0, -3.0, 2.0, 1.0, 4.0, 2.0) for i in range(30)]
+    gl, go = pair_geometry(rtkb, oracle, params)
+    pd, po = pair_image(rtkb, oracle, (160, 120, 30), (1.5, 1.5, 1.0), index=(-3, 2, 0))
+    ell = np.concatenate([phantoms.random_ellipsoids(12, 3, centre_radius=40.0), phantoms.shepp_logan(60.0)])
+    ref = oracle.project_ellipsoids(go, po, ell)
+    got = to_np(rtkb.ops.project_ellipsoids(gl, pd, ell))
+    assert rel_l2(got, ref) < 1e-6

@@ -37,6 +37,9 @@ PIX = 0.388
 SID, SDD = 1000.0, 1536.0
 SEED = 20261203 + 1
 L1_BYTES_PER_UPDATE = 16  # four 4-byte taps of one bilinear interpolation
+# DRAM bytes (read + write) of one backprojection launch of this workload, from the 1-pass ncu capture
+# summarised in profiles/bp_tiled_kernel_512cube_720proj_traffic.md (126.56 GB read + 0.656 GB written).
+BP_LAUNCH_DRAM_BYTES = 126.56e9 + 0.656e9
 WORKLOAD = {"workload": "FDK backprojection 512^3 @0.5mm <- 720 x 1024x768 @0.388mm, SID 1000, SDD 1536, 360 deg",
             "volume": [NX, NY, NZ], "projections": [NU, NV, NP], "dtype_storage": "float32",
             "l2_policy": "inputs larger than L2 (2.26 GB projection stack, 0.54 GB volume)"}
@@ -417,7 +420,9 @@ def main():
     pk = peaks()
     hbm_bytes = (NX * NY * NZ * 4 * 2) + (NP * NV * NU * 4)
     roofline = {"bound": "l1", "achieved": achieved, "peak": peak_smem, "unit": "GB/s",
-                "frac": achieved / peak_smem if peak_smem else None, "traffic": None,
+                "frac": achieved / peak_smem if peak_smem else None,
+                "traffic": BP_LAUNCH_DRAM_BYTES if NX == 512 else None,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one full-size launch",
                 "peak_source": "measured in this run: shared-memory bilinear-gather probe (rtkb_probe_smem_gather)",
                 "per_launch_updates": updates_per_step(), "bytes_per_update": L1_BYTES_PER_UPDATE,
                 "hbm": {"algorithmic_bytes_per_launch": hbm_bytes,

@@ -189,12 +189,16 @@ def fdk_pipeline_ms(torch, rtkb, g, vd, pd, proj, stream, reps=3):
     return e0.elapsed_time(e1) / reps
 
 
-def cg_seconds_to_residual(torch, rtkb, stream, tol=1e-3, max_iter=300):
+def cg_seconds_to_residual(torch, rtkb, stream, tol=1e-3, max_iter=300, learned_pcg=True):
     """CG configuration: 256^3 at 1 mm, 360 projections of 512x384 at 0.8 mm
     (SID 1000, SDD 1536) of 20 seeded random ellipsoids with pre-log Poisson
     noise at I0 = 5e4; Joseph pair, FP32 vectors, FP64 scalars, one CUDA graph
     per iteration.  Seconds until the normal-equation residual falls to
-    tol * ||r_0||, device time from the start of CG to convergence."""
+    tol * ||r_0||, device time from the start of CG to convergence.  The
+    learned-PCG leg trains the U-Net preconditioner on the same geometry
+    (training pairs from the plan's own normal operator, hand-written
+    forward/backward kernels, Adam) and solves the same problem with
+    flexible PCG; training time is reported separately."""
     from tests import phantoms
 
     n = 360
@@ -208,25 +212,58 @@ def cg_seconds_to_residual(torch, rtkb, stream, tol=1e-3, max_iter=300):
     gen = torch.Generator(device="cuda").manual_seed(SEED + 3)
     counts = torch.poisson(i0 * torch.exp(-clean), generator=gen).clamp_(min=1.0)
     p = (-torch.log(counts / i0)).contiguous()
-    x = torch.zeros((256, 256, 256), device="cuda")
-    cg = rtkb.ops.ConjugateGradient(g, vd, pd)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    cg.start(p, x, stream=stream)
-    rr, rr0, it = cg.residual(stream)
-    while rr > tol * tol * rr0 and it < max_iter:
-        cg.iterate(1, stream)
+
+    def solve(net):
+        x = torch.zeros((256, 256, 256), device="cuda")
+        cg = rtkb.ops.ConjugateGradient(g, vd, pd)
+        if net is not None:
+            cg.set_preconditioner(net, history=8)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        cg.start(p, x, stream=stream)
         rr, rr0, it = cg.residual(stream)
-    e1.record(stream)
+        while rr > tol * tol * rr0 and it < max_iter:
+            cg.iterate(1, stream)
+            rr, rr0, it = cg.residual(stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        secs = e0.elapsed_time(e1) / 1e3
+        status = cg.preconditioner_status()
+        cg.close()
+        return (secs if rr <= tol * tol * rr0 else None), it, (rr / rr0) ** 0.5, secs / max(it, 1), status, x
+
+    secs, it, rel, per_it, _, x_cg = solve(None)
+    out = {"seconds_to_rel_residual_1e-3": secs, "iterations": it, "relative_residual": rel,
+           "seconds_per_iteration": per_it,
+           "config": "256^3 @1mm <- 360 x 512x384 @0.8mm, SID 1000, SDD 1536, 20 random ellipsoids, "
+                     "Poisson I0=5e4, Joseph pair, FP32 vectors / FP64 scalars, CUDA graph per iteration",
+           "learned_pcg": None}
+    if not learned_pcg:
+        return out
+    from rtk_b200 import learned
+
+    plan = rtkb.ops.ConjugateGradient(g, vd, pd)
+    t0 = time.perf_counter()
+    rs, es, _ = learned.make_training_pairs(plan, 32, seed=SEED + 5)
     torch.cuda.synchronize()
-    secs = e0.elapsed_time(e1) / 1e3
-    cg.close()
-    return {"seconds_to_rel_residual_1e-3": secs if rr <= tol * tol * rr0 else None, "iterations": it,
-            "relative_residual": (rr / rr0) ** 0.5, "seconds_per_iteration": secs / max(it, 1),
-            "config": "256^3 @1mm <- 360 x 512x384 @0.8mm, SID 1000, SDD 1536, 20 random ellipsoids, "
-                      "Poisson I0=5e4, Joseph pair, FP32 vectors / FP64 scalars, CUDA graph per iteration",
-            "learned_pcg": None}
+    t_pairs = time.perf_counter() - t0
+    net = learned.UNet(seed=1)
+    hist, t_train = learned.train(net, rs, es, steps=3000, batch=4, crop=64, lr=2e-3, lr_final=2e-4, log_every=500)
+    del rs, es
+    plan.close()
+    psecs, pit, prel, pper, (active, fb), x_pcg = solve(net)
+    net.close()
+    diff = float((x_pcg - x_cg).double().norm() / x_cg.double().norm())
+    out["learned_pcg"] = {
+        "seconds_to_rel_residual_1e-3": psecs, "iterations": pit, "relative_residual": prel,
+        "seconds_per_iteration": pper, "speedup_vs_cg": (secs / psecs) if (secs and psecs) else None,
+        "fallback_to_cg_at_iteration": fb if fb >= 0 else None, "rel_diff_to_cg_solution": diff,
+        "training": {"pairs": 32, "pairs_seconds": t_pairs, "steps": 3000, "batch": 4, "crop": 64,
+                     "train_seconds": t_train, "final_loss": hist[-1][1] if hist else None},
+        "method": "flexible PCG, history 8, 3-level 3D U-Net 16/32/64 (BF16 mma.sync convolutions, FP32 "
+                  "accumulation), fallback to plain CG after 2 non-improving iterations"}
+    return out
 
 
 def smem_peak_gbs(torch, lib, stream) -> float:

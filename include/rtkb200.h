@@ -176,6 +176,12 @@ int  rtkb_cg_create(const rtkb_geometry * g, const rtkb_image_desc * vol, const 
  * r0 = b - A x0, p0 = r0.  d_weights may be NULL (all ones). */
 int  rtkb_cg_start(rtkb_cg * plan, const float * d_proj, const float * d_weights, int displaced_detector, float * d_x,
                    void * stream);
+/* As rtkb_cg_start, but for a given normal-equation right-hand side d_b
+ * (a volume) instead of b = BP(W .* p); W keeps its current value (1 unless a
+ * previous rtkb_cg_start set it).  No reference counterpart: used to run CG on
+ * synthetic problems A x = b whose solution is known (training data of the
+ * learned preconditioner). */
+int  rtkb_cg_start_rhs(rtkb_cg * plan, const float * d_b, float * d_x, void * stream);
 int  rtkb_cg_iterate(rtkb_cg * plan, int n, void * stream);
 /* Waits for `stream`; *rr = ||r_k||^2 of the normal equations, *rr0 = ||r_0||^2. */
 int  rtkb_cg_residual(rtkb_cg * plan, double * rr, double * rr0, int * iterations, void * stream);
@@ -186,6 +192,56 @@ int  rtkb_conjugate_gradient(const rtkb_geometry * g, const rtkb_image_desc * vo
                              const rtkb_cg_params * params, const float * d_proj, const float * d_weights,
                              int displaced_detector, float * d_x, int max_iterations, double relative_residual,
                              int * iterations, double * final_relative_residual, void * stream);
+/* d_out = A d_in with the plan's operator (weights W = 1 until rtkb_cg_start
+ * sets them).  Used to generate (A e, e) training pairs for the learned
+ * preconditioner.  No reference counterpart (RTK's operator is internal to
+ * rtk::ReconstructionConjugateGradientOperator). */
+int  rtkb_cg_apply_operator(rtkb_cg * plan, const float * d_in, float * d_out, void * stream);
+
+/* ---- learned preconditioner (no reference counterpart) ----
+ * A 3-level 3D U-Net (16/32/64 channels, 3x3x3 convolutions, ReLU, no biases,
+ * average pooling, nearest up-sampling, concatenated skips, 1x1x1 output),
+ * BF16 weights and activations with FP32 accumulation on the tensor cores,
+ * FP32 master weights and Adam.  Volumes are float32 [batch][z][y][x] whose
+ * sizes are multiples of 4.  Parameters (host order): for each of the ten 3x3x3
+ * layers W[tap][c_in][c_out] with tap = (kz*3+ky)*3+kx (cross-correlation,
+ * zero padding 1), then the 16 output weights. */
+typedef struct rtkb_unet rtkb_unet;
+int       rtkb_unet_create(unsigned long long seed, rtkb_unet ** net); /* He-normal initialisation */
+long long rtkb_unet_num_parameters(const rtkb_unet * net);
+int       rtkb_unet_get_parameters(const rtkb_unet * net, float * host, long long n);
+int       rtkb_unet_set_parameters(rtkb_unet * net, const float * host, long long n); /* resets Adam */
+/* Gradients of the last rtkb_unet_train_step (mean squared error). */
+int       rtkb_unet_get_gradients(const rtkb_unet * net, float * host, long long n);
+/* Sizes the activation workspace (allocates; call outside stream capture). */
+int       rtkb_unet_reserve(rtkb_unet * net, int batch, int nx, int ny, int nz);
+/* d_out = s N(d_in / s) with s = rms(d_in) when normalize, else N(d_in). */
+int       rtkb_unet_forward(rtkb_unet * net, int batch, int nx, int ny, int nz, const float * d_in, float * d_out,
+                            int normalize, void * stream);
+/* One step on the mean squared error between N(d_in) and d_target (no
+ * normalisation) over the voxels at least loss_margin voxels inside every face
+ * of each volume (crops see their surroundings as zeros, so their borders
+ * cannot be fitted): gradients always, an Adam update when `update`; *loss (if
+ * not NULL, synchronises) = mean squared error before the update. */
+int       rtkb_unet_train_step(rtkb_unet * net, int batch, int nx, int ny, int nz, const float * d_in,
+                               const float * d_target, int loss_margin, double learning_rate, int update,
+                               double * loss, void * stream);
+void      rtkb_unet_destroy(rtkb_unet * net);
+
+/* Flexible PCG: with a network set (before rtkb_cg_start; NULL removes it) each
+ * iteration preconditions the residual, z = s N(r / s), steps with
+ * alpha = <p,r>/<p,Ap> and A-orthogonalises the next direction against the
+ * last `history` (1..16) directions, p = z - sum_j <z,Ap_j>/<p_j,Ap_j> p_j
+ * (truncated flexible CG; history 1 is the Polak-Ribiere flexible CG).  It
+ * keeps 2 x history extra volumes on the device.  rtkb_cg_iterate reads the
+ * normal-equation residual after every preconditioned iteration and continues
+ * as plain CG from the current iterate (p = r) once ||r|| has not improved on
+ * its best value for two consecutive iterations.  The network must outlive the
+ * plan; volume sizes must be multiples of 4. */
+int  rtkb_cg_set_preconditioner(rtkb_cg * plan, rtkb_unet * net, int history);
+/* *active: 1 while the network is in use; *fallback_iteration: iteration at
+ * which plain CG took over (-1: never). */
+int  rtkb_cg_preconditioner_status(const rtkb_cg * plan, int * active, int * fallback_iteration);
 
 /* Autotuner hook of the tiled backprojector (no reference counterpart):
  * force >= 0 selects configuration `force` (box size, voxels per thread

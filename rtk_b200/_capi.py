@@ -161,3 +161,20 @@ SIGNATURES.update({
 SIGNATURES.update({
     "rtkb_project_ellipsoids": (C.c_int, [_G, _IM, C.c_int, _D, _V, _V]),
 })
+
+SIGNATURES.update({
+    "rtkb_cg_apply_operator": (C.c_int, [_V, _V, _V, _V]),
+    "rtkb_cg_start_rhs": (C.c_int, [_V, _V, _V, _V]),
+    "rtkb_cg_set_preconditioner": (C.c_int, [_V, _V, C.c_int]),
+    "rtkb_cg_preconditioner_status": (C.c_int, [_V, _I, _I]),
+    "rtkb_unet_create": (C.c_int, [C.c_ulonglong, C.POINTER(C.c_void_p)]),
+    "rtkb_unet_num_parameters": (C.c_longlong, [_V]),
+    "rtkb_unet_get_parameters": (C.c_int, [_V, _F, C.c_longlong]),
+    "rtkb_unet_set_parameters": (C.c_int, [_V, _F, C.c_longlong]),
+    "rtkb_unet_get_gradients": (C.c_int, [_V, _F, C.c_longlong]),
+    "rtkb_unet_reserve": (C.c_int, [_V, C.c_int, C.c_int, C.c_int, C.c_int]),
+    "rtkb_unet_forward": (C.c_int, [_V, C.c_int, C.c_int, C.c_int, C.c_int, _V, _V, C.c_int, _V]),
+    "rtkb_unet_train_step": (C.c_int, [_V, C.c_int, C.c_int, C.c_int, C.c_int, _V, _V, C.c_int, C.c_double,
+                                       C.c_int, _D, _V]),
+    "rtkb_unet_destroy": (None, [_V]),
+})

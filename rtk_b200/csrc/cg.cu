@@ -44,7 +44,29 @@ struct rtkb_cg
   cudaGraph_t              graph = nullptr;
   cudaGraphExec_t          exec = nullptr;
   int                      iterations = 0;
+  // flexible PCG with a learned preconditioner (optional)
+  rtkb_unet *              net = nullptr;
+  void *                   pmem = nullptr; // Z and the second partial-sum buffer
+  float *                  Z = nullptr;
+  double *                 partial2 = nullptr;
+  int                      m = 0;              // directions kept for re-orthogonalisation
+  float *                  Ph = nullptr;       // m previous directions
+  float *                  APh = nullptr;      // A times each of them
+  double *                 hist = nullptr;     // [m] <p_j, A p_j>, [m] beta_j, [1] slot counter
+  double *                 mpartial = nullptr; // [m][kRedBlocks] partial dot products
+  bool                     pcg_active = false;
+  int                      fallback_iteration = -1;
+  double                   rr_best = 0.;
+  int                      stall = 0;
+  cudaGraph_t              graph_p = nullptr;
+  cudaGraphExec_t          exec_p = nullptr;
 };
+
+namespace rtkb
+{
+cudaError_t unet_apply(rtkb_unet * u, const float * in, float * out, cudaStream_t st);
+bool        unet_reserved_for(const rtkb_unet * u, int nx, int ny, int nz);
+} // namespace rtkb
 
 namespace
 {
@@ -59,6 +81,9 @@ enum
   S_BETA = 3,
   S_PAP = 4
 };
+// Flexible PCG patience: fall back to plain CG when ||r|| has not improved on
+// its best value for this many consecutive iterations.
+constexpr int kPcgPatience = 2;
 
 __device__ __forceinline__ double
 block_sum(double v)
@@ -194,6 +219,136 @@ fill_kernel(float * __restrict__ out, float v, long long n)
     out[i] = v;
 }
 
+// partial[b] = <a1, b1>, partial2[b] = <a2, b2> over block b's slice (FP64)
+__global__ void __launch_bounds__(kRedThreads)
+dot2_partial_kernel(const float * __restrict__ a1, const float * __restrict__ b1, const float * __restrict__ a2,
+                    const float * __restrict__ b2, long long n, double * partial, double * partial2)
+{
+  double s1 = 0., s2 = 0.;
+  for (long long i = blockIdx.x * (long long)kRedThreads + threadIdx.x; i < n; i += (long long)kRedBlocks * kRedThreads)
+  {
+    s1 = fma((double)a1[i], (double)b1[i], s1);
+    s2 = fma((double)a2[i], (double)b2[i], s2);
+  }
+  s1 = block_sum(s1);
+  __syncthreads();
+  s2 = block_sum(s2);
+  if (threadIdx.x == 0)
+  {
+    partial[blockIdx.x] = s1;
+    partial2[blockIdx.x] = s2;
+  }
+}
+
+// flexible PCG: alpha = <p, r> / (<p, Ap> + eps)
+__global__ void
+finalize_alpha_pcg_kernel(const double * partial, const double * partial2, double * scal)
+{
+  const double pap = sum_partials(partial);
+  const double pr = sum_partials(partial2);
+  if (threadIdx.x == 0)
+  {
+    scal[S_PAP] = pap;
+    scal[S_ALPHA] = pr / (pap + DBL_MIN);
+  }
+}
+
+// rr = <r, r> (no beta: the PCG direction update comes after the preconditioner)
+__global__ void
+finalize_rr_kernel(const double * partial, double * scal)
+{
+  const double rr = sum_partials(partial);
+  if (threadIdx.x == 0)
+    scal[S_RR] = rr;
+}
+
+// Truncated flexible CG keeps the last m directions p_j, A p_j and <p_j, A p_j>
+// in a ring; slot = counter mod m.  Store the current direction there.
+constexpr int kMaxHistory = 16;
+__global__ void __launch_bounds__(256)
+store_direction_kernel(const float * __restrict__ p, const float * __restrict__ ap, float * __restrict__ ph,
+                       float * __restrict__ aph, long long n, int m, const double * __restrict__ scal,
+                       double * __restrict__ hist)
+{
+  const int slot = (int)hist[2 * m] % m;
+  float *   dp = ph + (size_t)slot * n;
+  float *   dap = aph + (size_t)slot * n;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+  {
+    dp[i] = p[i];
+    dap[i] = ap[i];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0)
+    hist[slot] = scal[S_PAP];
+}
+
+__global__ void
+advance_slot_kernel(double * hist, int m)
+{
+  if (threadIdx.x == 0 && blockIdx.x == 0)
+    hist[2 * m] += 1.;
+}
+
+// mpartial[j][b] = <z, A p_j> over block b's slice, j < m (FP64)
+__global__ void __launch_bounds__(kRedThreads)
+multi_dot_kernel(const float * __restrict__ z, const float * __restrict__ aph, long long n, int m,
+                 double * __restrict__ mpartial)
+{
+  double s[kMaxHistory];
+#pragma unroll
+  for (int j = 0; j < kMaxHistory; j++)
+    s[j] = 0.;
+  for (long long i = blockIdx.x * (long long)kRedThreads + threadIdx.x; i < n; i += (long long)kRedBlocks * kRedThreads)
+  {
+    const double zi = z[i];
+#pragma unroll
+    for (int j = 0; j < kMaxHistory; j++)
+      if (j < m)
+        s[j] = fma(zi, (double)aph[(size_t)j * n + i], s[j]);
+  }
+#pragma unroll 1
+  for (int j = 0; j < m; j++)
+  {
+    const double t = block_sum(s[j]);
+    if (threadIdx.x == 0)
+      mpartial[(size_t)j * kRedBlocks + blockIdx.x] = t;
+    __syncthreads();
+  }
+}
+
+// beta_j = -<z, A p_j> / <p_j, A p_j> (0 for empty slots): A-orthogonalises the
+// new direction against the kept ones (Notay's truncated flexible CG)
+__global__ void
+finalize_betas_kernel(const double * __restrict__ mpartial, int m, double * __restrict__ hist)
+{
+  for (int j = 0; j < m; j++)
+  {
+    const double zap = sum_partials(mpartial + (size_t)j * kRedBlocks);
+    if (threadIdx.x == 0)
+      hist[m + j] = hist[j] > 0. ? -zap / hist[j] : 0.;
+  }
+}
+
+// p = z + sum_j beta_j p_j
+__global__ void __launch_bounds__(256)
+update_p_multi_kernel(float * __restrict__ p, const float * __restrict__ z, const float * __restrict__ ph, long long n,
+                      int m, const double * __restrict__ hist)
+{
+  float b[kMaxHistory];
+#pragma unroll
+  for (int j = 0; j < kMaxHistory; j++)
+    b[j] = j < m ? (float)hist[m + j] : 0.f;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+  {
+    float v = z[i];
+#pragma unroll
+    for (int j = 0; j < kMaxHistory; j++)
+      if (j < m)
+        v = fmaf(b[j], ph[(size_t)j * n + i], v);
+    p[i] = v;
+  }
+}
+
 unsigned
 grid_for(long long n)
 {
@@ -225,15 +380,72 @@ enqueue_iteration(rtkb_cg * c, cudaStream_t st)
   return cudaGetLastError();
 }
 
+// One truncated flexible-PCG iteration: Ap; alpha = <p,r>/<p,Ap>;
+// x += alpha p; r -= alpha Ap; keep (p, Ap, <p,Ap>); z = M(r);
+// p = z - sum_j <z,Ap_j>/<p_j,Ap_j> p_j over the kept directions.
+cudaError_t
+enqueue_pcg_iteration(rtkb_cg * c, cudaStream_t st)
+{
+  cudaError_t e = apply_A(c, c->P, c->AP, st);
+  if (e != cudaSuccess)
+    return e;
+  dot2_partial_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(c->P, c->AP, c->P, c->R, c->nvox, c->partial, c->partial2);
+  finalize_alpha_pcg_kernel<<<1, 32, 0, st>>>(c->partial, c->partial2, c->scal);
+  update_xr_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(c->x, c->R, c->P, c->AP, c->nvox, c->scal, c->partial);
+  finalize_rr_kernel<<<1, 32, 0, st>>>(c->partial, c->scal);
+  store_direction_kernel<<<grid_for(c->nvox), 256, 0, st>>>(c->P, c->AP, c->Ph, c->APh, c->nvox, c->m, c->scal,
+                                                             c->hist);
+  advance_slot_kernel<<<1, 32, 0, st>>>(c->hist, c->m);
+  e = rtkb::unet_apply(c->net, c->R, c->Z, st);
+  if (e != cudaSuccess)
+    return e;
+  multi_dot_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(c->Z, c->APh, c->nvox, c->m, c->mpartial);
+  finalize_betas_kernel<<<1, 32, 0, st>>>(c->mpartial, c->m, c->hist);
+  update_p_multi_kernel<<<grid_for(c->nvox), 256, 0, st>>>(c->P, c->Z, c->Ph, c->nvox, c->m, c->hist);
+  return cudaGetLastError();
+}
+
+cudaError_t
+capture(rtkb_cg * c, bool pcg, cudaGraph_t * graph, cudaGraphExec_t * exec)
+{
+  cudaError_t e = cudaStreamBeginCapture(c->cap, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess)
+  {
+    cudaError_t ei = pcg ? enqueue_pcg_iteration(c, c->cap) : enqueue_iteration(c, c->cap);
+    e = cudaStreamEndCapture(c->cap, graph);
+    if (e == cudaSuccess)
+      e = ei;
+  }
+  if (e == cudaSuccess)
+    e = cudaGraphInstantiate(exec, *graph, 0);
+  return e;
+}
+
+void
+drop_graphs(rtkb_cg * c)
+{
+  if (c->exec)
+    cudaGraphExecDestroy(c->exec);
+  if (c->graph)
+    cudaGraphDestroy(c->graph);
+  if (c->exec_p)
+    cudaGraphExecDestroy(c->exec_p);
+  if (c->graph_p)
+    cudaGraphDestroy(c->graph_p);
+  c->exec = nullptr;
+  c->graph = nullptr;
+  c->exec_p = nullptr;
+  c->graph_p = nullptr;
+}
+
 void
 release(rtkb_cg * c)
 {
   if (!c)
     return;
-  if (c->exec)
-    cudaGraphExecDestroy(c->exec);
-  if (c->graph)
-    cudaGraphDestroy(c->graph);
+  drop_graphs(c);
+  if (c->pmem)
+    cudaFree(c->pmem);
   if (c->mem)
     cudaFree(c->mem);
   if (c->cap)
@@ -308,6 +520,11 @@ rtkb_cg_create(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_
     e = cudaMemcpy(c->tab, tab.data(), tab.size() * sizeof(RayProj), cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
       e = cudaMemset(c->scal, 0, sb);
+    if (e == cudaSuccess)
+    {
+      fill_kernel<<<grid_for(c->npix), 256>>>(c->W, 1.f, c->npix); // W = 1 until rtkb_cg_start sets it
+      e = cudaDeviceSynchronize();
+    }
     if (e != cudaSuccess)
     {
       release(c);
@@ -324,6 +541,59 @@ rtkb_cg_create(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_
   }
 }
 
+namespace
+{
+// Shared tail of the two starts: R holds b on entry; R = b - A x0, P = R (or
+// M(R) with a preconditioner), rr; then the iteration graphs are captured.
+int
+start_from_rhs(rtkb_cg * c, cudaStream_t st)
+{
+  using namespace rtkb;
+  cudaError_t e = apply_A(c, c->x, c->AP, st);
+  if (e != cudaSuccess)
+    return cuda_fail(e, "CG start");
+  start_rp_kernel<<<grid_for(c->nvox), 256, 0, st>>>(c->R, c->P, c->AP, c->nvox);
+  dot_partial_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(c->R, c->R, c->nvox, c->partial);
+  finalize_start_kernel<<<1, 32, 0, st>>>(c->partial, c->scal);
+  RTKB_CUDA_TRY(cudaGetLastError());
+  if (c->pcg_active)
+  {
+    // empty direction history; z0 = M(r0), p0 = z0 (run eagerly once, before any capture)
+    RTKB_CUDA_TRY(cudaMemsetAsync(c->hist, 0, (2 * c->m + 1) * sizeof(double), st));
+    RTKB_CUDA_TRY(unet_apply(c->net, c->R, c->Z, st));
+    mul_kernel<<<grid_for(c->nvox), 256, 0, st>>>(c->P, c->Z, nullptr, c->nvox);
+    RTKB_CUDA_TRY(cudaGetLastError());
+    double h[2] = { 0., 0. };
+    RTKB_CUDA_TRY(cudaMemcpyAsync(h, c->scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    RTKB_CUDA_TRY(cudaStreamSynchronize(st));
+    c->rr_best = h[S_RR];
+  }
+  if (c->use_graph)
+  {
+    // capture one iteration once on the plan's private stream (the caller's
+    // may be the legacy default stream, which cannot be captured); later
+    // iterations replay it on the caller's stream
+    e = capture(c, false, &c->graph, &c->exec);
+    if (e == cudaSuccess && c->pcg_active)
+      e = capture(c, true, &c->graph_p, &c->exec_p);
+    if (e != cudaSuccess)
+      return cuda_fail(e, "CG graph capture");
+  }
+  return RTKB_OK;
+}
+
+void
+reset_run(rtkb_cg * c, float * d_x)
+{
+  drop_graphs(c);
+  c->x = d_x;
+  c->iterations = 0;
+  c->pcg_active = c->net != nullptr;
+  c->fallback_iteration = -1;
+  c->stall = 0;
+}
+} // namespace
+
 extern "C" int
 rtkb_cg_start(rtkb_cg * c, const float * d_proj, const float * d_weights, int displaced_detector, float * d_x,
               void * stream)
@@ -332,18 +602,7 @@ rtkb_cg_start(rtkb_cg * c, const float * d_proj, const float * d_weights, int di
   if (!c || !d_proj || !d_x)
     return fail(RTKB_ERR_INVALID_ARGUMENT, "null argument");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (c->exec)
-  {
-    cudaGraphExecDestroy(c->exec);
-    c->exec = nullptr;
-  }
-  if (c->graph)
-  {
-    cudaGraphDestroy(c->graph);
-    c->graph = nullptr;
-  }
-  c->x = d_x;
-  c->iterations = 0;
+  reset_run(c, d_x);
   // W = displaced-detector weights (no padding) of the input weights (ones by default)
   const bool have_w = d_weights != nullptr;
   if (displaced_detector)
@@ -358,36 +617,24 @@ rtkb_cg_start(rtkb_cg * c, const float * d_proj, const float * d_weights, int di
     RTKB_CUDA_TRY(cudaMemcpyAsync(c->W, d_weights, (size_t)c->npix * 4, cudaMemcpyDeviceToDevice, st));
   else
     fill_kernel<<<grid_for(c->npix), 256, 0, st>>>(c->W, 1.f, c->npix);
-  // R = B = BP(W .* p); AP = A x0; R -= AP; P = R
+  // R = B = BP(W .* p)
   mul_kernel<<<grid_for(c->npix), 256, 0, st>>>(c->tmp, d_proj, c->W, c->npix);
-  cudaError_t e = joseph_back_launch(c->args, c->tmp, c->A, c->At, nullptr, c->R, nullptr, 0.f, st);
-  if (e == cudaSuccess)
-    e = apply_A(c, c->x, c->AP, st);
+  const cudaError_t e = joseph_back_launch(c->args, c->tmp, c->A, c->At, nullptr, c->R, nullptr, 0.f, st);
   if (e != cudaSuccess)
     return cuda_fail(e, "CG start");
-  start_rp_kernel<<<grid_for(c->nvox), 256, 0, st>>>(c->R, c->P, c->AP, c->nvox);
-  dot_partial_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(c->R, c->R, c->nvox, c->partial);
-  finalize_start_kernel<<<1, 32, 0, st>>>(c->partial, c->scal);
-  RTKB_CUDA_TRY(cudaGetLastError());
-  if (c->use_graph)
-  {
-    // capture one iteration once on the plan's private stream (the caller's
-    // may be the legacy default stream, which cannot be captured); later
-    // iterations replay it on the caller's stream
-    e = cudaStreamBeginCapture(c->cap, cudaStreamCaptureModeThreadLocal);
-    if (e == cudaSuccess)
-    {
-      cudaError_t ei = enqueue_iteration(c, c->cap);
-      e = cudaStreamEndCapture(c->cap, &c->graph);
-      if (e == cudaSuccess)
-        e = ei;
-    }
-    if (e == cudaSuccess)
-      e = cudaGraphInstantiate(&c->exec, c->graph, 0);
-    if (e != cudaSuccess)
-      return cuda_fail(e, "CG graph capture");
-  }
-  return RTKB_OK;
+  return start_from_rhs(c, st);
+}
+
+extern "C" int
+rtkb_cg_start_rhs(rtkb_cg * c, const float * d_b, float * d_x, void * stream)
+{
+  using namespace rtkb;
+  if (!c || !d_b || !d_x)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "null argument");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  reset_run(c, d_x);
+  RTKB_CUDA_TRY(cudaMemcpyAsync(c->R, d_b, (size_t)c->nvox * 4, cudaMemcpyDeviceToDevice, st));
+  return start_from_rhs(c, st);
 }
 
 extern "C" int
@@ -399,6 +646,31 @@ rtkb_cg_iterate(rtkb_cg * c, int n, void * stream)
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   for (int i = 0; i < n; i++)
   {
+    if (c->pcg_active)
+    {
+      cudaError_t e = c->exec_p ? cudaGraphLaunch(c->exec_p, st) : enqueue_pcg_iteration(c, st);
+      if (e != cudaSuccess)
+        return cuda_fail(e, "PCG iteration");
+      c->iterations++;
+      // the true normal-equation residual judges the preconditioner: when
+      // ||r|| stops improving, continue as plain CG from the current iterate
+      double rr = 0.;
+      RTKB_CUDA_TRY(cudaMemcpyAsync(&rr, c->scal + S_RR, sizeof(double), cudaMemcpyDeviceToHost, st));
+      RTKB_CUDA_TRY(cudaStreamSynchronize(st));
+      if (rr < c->rr_best)
+      {
+        c->rr_best = rr;
+        c->stall = 0;
+      }
+      else if (++c->stall >= kPcgPatience)
+      {
+        c->pcg_active = false;
+        c->fallback_iteration = c->iterations;
+        mul_kernel<<<grid_for(c->nvox), 256, 0, st>>>(c->P, c->R, nullptr, c->nvox); // restart: p = r
+        RTKB_CUDA_TRY(cudaGetLastError());
+      }
+      continue;
+    }
     cudaError_t e = c->exec ? cudaGraphLaunch(c->exec, st) : enqueue_iteration(c, st);
     if (e != cudaSuccess)
       return cuda_fail(e, "CG iteration");
@@ -464,4 +736,76 @@ rtkb_conjugate_gradient(const rtkb_geometry * g, const rtkb_image_desc * vol, co
     *final_relative_residual = rr0 > 0. ? std::sqrt(rr / rr0) : 0.;
   rtkb_cg_destroy(c);
   return rc;
+}
+
+extern "C" int
+rtkb_cg_set_preconditioner(rtkb_cg * c, rtkb_unet * net, int history)
+{
+  using namespace rtkb;
+  if (!c)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "null plan");
+  if (net && (history < 1 || history > kMaxHistory))
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "history must be in 1..16");
+  drop_graphs(c);
+  c->x = nullptr; // must be started again
+  c->net = nullptr;
+  c->pcg_active = false;
+  if (!net)
+    return RTKB_OK;
+  const int nx = c->vol.size[0], ny = c->vol.size[1], nz = c->vol.size[2];
+  int       rc = rtkb_unet_reserve(net, 1, nx, ny, nz);
+  if (rc != RTKB_OK)
+    return rc;
+  if (c->pmem && c->m != history)
+  {
+    cudaFree(c->pmem);
+    c->pmem = nullptr;
+  }
+  if (!c->pmem)
+  {
+    const size_t vb = ((size_t)c->nvox * 4 + 255) & ~size_t(255);
+    const size_t rb = kRedBlocks * sizeof(double);
+    const size_t total = vb * (1 + 2 * (size_t)history) + rb * (1 + history) + (2 * history + 1) * sizeof(double);
+    RTKB_CUDA_TRY(cudaMalloc(&c->pmem, total));
+    char * m = static_cast<char *>(c->pmem);
+    c->Z = reinterpret_cast<float *>(m);
+    m += vb;
+    c->Ph = reinterpret_cast<float *>(m);
+    m += vb * history;
+    c->APh = reinterpret_cast<float *>(m);
+    m += vb * history;
+    c->partial2 = reinterpret_cast<double *>(m);
+    m += rb;
+    c->mpartial = reinterpret_cast<double *>(m);
+    m += rb * history;
+    c->hist = reinterpret_cast<double *>(m);
+    c->m = history;
+    // zero so that never-written slots contribute nothing (beta_j = 0, 0 * p_j)
+    RTKB_CUDA_TRY(cudaMemset(c->Ph, 0, 2 * vb * history));
+  }
+  c->net = net;
+  return RTKB_OK;
+}
+
+extern "C" int
+rtkb_cg_preconditioner_status(const rtkb_cg * c, int * active, int * fallback_iteration)
+{
+  using namespace rtkb;
+  if (!c)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "null plan");
+  if (active)
+    *active = c->pcg_active ? 1 : 0;
+  if (fallback_iteration)
+    *fallback_iteration = c->fallback_iteration;
+  return RTKB_OK;
+}
+
+extern "C" int
+rtkb_cg_apply_operator(rtkb_cg * c, const float * d_in, float * d_out, void * stream)
+{
+  using namespace rtkb;
+  if (!c || !d_in || !d_out || d_in == d_out)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "null or aliased argument");
+  const cudaError_t e = apply_A(c, d_in, d_out, static_cast<cudaStream_t>(stream));
+  return e == cudaSuccess ? RTKB_OK : cuda_fail(e, "normal operator");
 }

@@ -207,8 +207,37 @@ class ConjugateGradient:
                                       int(displaced_detector), _ptr(x), _stream(stream)))
         return self
 
+    def start_rhs(self, b, x, stream=None):
+        """Start CG on A x = b for a given right-hand side volume b."""
+        _check_shape(b, self.vol_desc, "right-hand side")
+        _check_shape(x, self.vol_desc, "volume")
+        self._keep = [b, x]
+        check(self._lib.rtkb_cg_start_rhs(self._h, _ptr(b), _ptr(x), _stream(stream)))
+        return self
+
     def iterate(self, n=1, stream=None):
         check(self._lib.rtkb_cg_iterate(self._h, int(n), _stream(stream)))
+
+    def set_preconditioner(self, net, history=8):
+        """Flexible PCG with a learned preconditioner (a rtk_b200.learned.UNet;
+        None removes it), re-orthogonalising against `history` directions.
+        Call before start()."""
+        self._net = net
+        check(self._lib.rtkb_cg_set_preconditioner(self._h, net.handle if net is not None else None,
+                                                   int(history)))
+
+    def preconditioner_status(self):
+        """(network still in use, iteration at which plain CG took over or -1)."""
+        a, f = C.c_int(), C.c_int()
+        check(self._lib.rtkb_cg_preconditioner_status(self._h, C.byref(a), C.byref(f)))
+        return bool(a.value), f.value
+
+    def apply_operator(self, x, out, stream=None):
+        """out = A x (normal operator of the plan; W = 1 before start())."""
+        _check_shape(x, self.vol_desc, "volume")
+        _check_shape(out, self.vol_desc, "volume")
+        check(self._lib.rtkb_cg_apply_operator(self._h, _ptr(x), _ptr(out), _stream(stream)))
+        return out
 
     def residual(self, stream=None):
         """(||r_k||^2, ||r_0||^2, k) -- synchronises the stream."""

@@ -189,6 +189,57 @@ def fdk_pipeline_ms(torch, rtkb, g, vd, pd, proj, stream, reps=3):
     return e0.elapsed_time(e1) / reps
 
 
+def draw_ellipsoids(torch, vd, ell):
+    """Voxelised ellipsoids (rtk::DrawEllipsoidImageFilter semantics: a voxel
+    whose centre lies inside adds the density) on a volume description with
+    identity direction: synthetic input of the forward-projection leg."""
+    nx, ny, nz = vd.size
+    ax = [vd.origin[a] + vd.spacing[a] * torch.arange(vd.size[a], device="cuda", dtype=torch.float64) for a in range(3)]
+    out = torch.zeros((nz, ny, nx), device="cuda", dtype=torch.float32)
+    for e in ell:
+        c, semi, R, dens = e[0:3], e[3:6], e[6:15].reshape(3, 3), e[15]
+        acc = 0.0
+        for k in range(3):  # local coordinate k = (R^T (p - c))_k / semi_k
+            col = R[:, k]
+            lk = ((ax[0] - c[0])[None, None, :] * col[0] + (ax[1] - c[1])[None, :, None] * col[1] +
+                  (ax[2] - c[2])[:, None, None] * col[2]) / semi[k]
+            acc = acc + lk * lk
+        out += float(dens) * (acc <= 1.0).float()
+    return out
+
+
+def joseph_forward_leg(torch, rtkb, lib, stream, reps=2):
+    """Joseph forward projection of the projector-pair configuration: a 512^3
+    volume at 0.5 mm holding the 20 seeded random ellipsoids, projected onto
+    720 x 1024x768 at 0.388 mm.  Ray samples per second (device time, inputs
+    resident) with the L1 roofline: one bilinear sample gathers 4 taps x 4 B."""
+    from tests import phantoms
+
+    g = make_geometry()
+    vd = rtkb.make_desc((NX, NY, NZ), (VOX, VOX, VOX))
+    pd = rtkb.make_desc((NU, NV, NP), (PIX, PIX, 1.0))
+    vol = draw_ellipsoids(torch, vd, phantoms.random_ellipsoids(20, SEED))
+    zero = torch.zeros((NP, NV, NU), device="cuda")
+    out = torch.empty_like(zero)
+    n = rtkb.ops.joseph_sample_count(g, vd, pd, stream=stream)
+    rtkb.ops.joseph_forward_project(g, vd, pd, vol, zero, out=out, stream=stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        rtkb.ops.joseph_forward_project(g, vd, pd, vol, zero, out=out, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3 / reps
+    peak = smem_peak_gbs(torch, lib, stream)
+    achieved = n * 16 / t / 1e9
+    return {"workload": "Joseph forward projection 512^3 @0.5mm -> 720 x 1024x768 @0.388mm, 20 random ellipsoids",
+            "samples_per_launch": n, "ms_per_launch": t * 1e3, "gsamples_per_s": n / t / 1e9,
+            "roofline": {"bound": "l1", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "bytes_per_sample": 16,
+                         "peak_source": "shared-memory bilinear-gather probe (the taps are L1-cached global loads)"}}
+
+
 def cg_seconds_to_residual(torch, rtkb, stream, tol=1e-3, max_iter=300, learned_pcg=True):
     """CG configuration: 256^3 at 1 mm, 360 projections of 512x384 at 0.8 mm
     (SID 1000, SDD 1536) of 20 seeded random ellipsoids with pre-log Poisson
@@ -223,19 +274,23 @@ def cg_seconds_to_residual(torch, rtkb, stream, tol=1e-3, max_iter=300, learned_
         e0.record(stream)
         cg.start(p, x, stream=stream)
         rr, rr0, it = cg.residual(stream)
+        hist = [1.0]
         while rr > tol * tol * rr0 and it < max_iter:
             cg.iterate(1, stream)
             rr, rr0, it = cg.residual(stream)
+            hist.append(round((rr / rr0) ** 0.5, 6))
         e1.record(stream)
         torch.cuda.synchronize()
         secs = e0.elapsed_time(e1) / 1e3
         status = cg.preconditioner_status()
         cg.close()
+        solve.hist = hist
         return (secs if rr <= tol * tol * rr0 else None), it, (rr / rr0) ** 0.5, secs / max(it, 1), status, x
 
     secs, it, rel, per_it, _, x_cg = solve(None)
+    cg_hist = solve.hist
     out = {"seconds_to_rel_residual_1e-3": secs, "iterations": it, "relative_residual": rel,
-           "seconds_per_iteration": per_it,
+           "seconds_per_iteration": per_it, "residual_history": cg_hist,
            "config": "256^3 @1mm <- 360 x 512x384 @0.8mm, SID 1000, SDD 1536, 20 random ellipsoids, "
                      "Poisson I0=5e4, Joseph pair, FP32 vectors / FP64 scalars, CUDA graph per iteration",
            "learned_pcg": None}
@@ -259,6 +314,7 @@ def cg_seconds_to_residual(torch, rtkb, stream, tol=1e-3, max_iter=300, learned_
         "seconds_to_rel_residual_1e-3": psecs, "iterations": pit, "relative_residual": prel,
         "seconds_per_iteration": pper, "speedup_vs_cg": (secs / psecs) if (secs and psecs) else None,
         "fallback_to_cg_at_iteration": fb if fb >= 0 else None, "rel_diff_to_cg_solution": diff,
+        "residual_history": solve.hist,
         "training": {"pairs": 32, "pairs_seconds": t_pairs, "steps": 3000, "batch": 4, "crop": 64,
                      "train_seconds": t_train, "final_loss": hist[-1][1] if hist else None},
         "method": "flexible PCG, history 8, 3-level 3D U-Net 16/32/64 (BF16 mma.sync convolutions, FP32 "
@@ -477,6 +533,8 @@ def main():
 
     if world == 1 and not args.no_extra_legs:
         line["fdk_pipeline_ms"] = fdk_pipeline_ms(torch, rtkb, g, vd, pd, proj, stream)
+        del proj
+        line["joseph_forward"] = joseph_forward_leg(torch, rtkb, lib, stream)
         line["cg"] = cg_seconds_to_residual(torch, rtkb, stream)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:

@@ -152,6 +152,12 @@ int rtkb_joseph_forward_project(const rtkb_geometry * g, const rtkb_image_desc *
 int rtkb_joseph_back_project(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
                              const float * d_proj, const float * d_vol_in, float * d_vol_out, void * stream);
 
+/* Number of bilinear samples rtkb_joseph_forward_project takes for these
+ * images (the algorithmic work of the ray-cast throughput figure); waits for
+ * `stream`.  No reference counterpart (RTK's tests count ray-box lengths). */
+int rtkb_joseph_sample_count(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
+                             double * count, void * stream);
+
 /* ---- conjugate gradient ----
  * rtk::ConjugateGradientConeBeamReconstructionFilter
  * (include/rtkConjugateGradientConeBeamReconstructionFilter.hxx:192-305) with

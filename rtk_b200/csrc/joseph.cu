@@ -398,6 +398,26 @@ fold_transposed_kernel(const float * in, const float * __restrict__ A, const flo
   }
 }
 
+// Number of bilinear samples the forward projector takes per launch: one per
+// main-direction slice between the rounded entry and exit slices (|fs-ns|+1),
+// one for rays that enter and leave within one slice.
+__global__ void __launch_bounds__(256)
+joseph_count_kernel(JosephArgs a, unsigned long long * total)
+{
+  const int          u = blockIdx.x * 32 + (threadIdx.x & 31);
+  const int          v = blockIdx.y * 8 + (threadIdx.x >> 5);
+  const int          s = blockIdx.z;
+  unsigned long long c = 0;
+  Ray                r;
+  if (u < a.nu && v < a.nv && setup_ray(a, a.P[s], u, v, s, true, r))
+    c = (unsigned long long)(abs(r.fs - r.ns) + 1);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+    c += __shfl_xor_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0 && c)
+    atomicAdd(total, c);
+}
+
 } // namespace
 
 namespace rtkb
@@ -578,6 +598,57 @@ rtkb_joseph_back_project(const rtkb_geometry * g, const rtkb_image_desc * vol, c
     cudaError_t fe = cudaFreeAsync(scratch, st);
     if (rc == RTKB_OK && fe != cudaSuccess)
       rc = cuda_fail(fe, "cudaFreeAsync");
+    return rc;
+  }
+  catch (...)
+  {
+    return fail(RTKB_ERR_OUT_OF_MEMORY, "host allocation failed");
+  }
+}
+
+extern "C" int
+rtkb_joseph_sample_count(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
+                         double * count, void * stream)
+{
+  using namespace rtkb;
+  try
+  {
+    int rc = joseph_check(g, vol, proj);
+    if (rc != RTKB_OK)
+      return rc;
+    if (!count)
+      return fail(RTKB_ERR_INVALID_ARGUMENT, "null count");
+    std::vector<RayProj> tab;
+    rc = joseph_tables(g->g, *vol, *proj, tab);
+    if (rc != RTKB_OK)
+      return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t tbytes = (tab.size() * sizeof(RayProj) + 255) & ~size_t(255);
+    void *       scratch = nullptr;
+    RTKB_CUDA_TRY(cudaMallocAsync(&scratch, tbytes + sizeof(unsigned long long), st));
+    RayProj *            d_tab = static_cast<RayProj *>(scratch);
+    unsigned long long * d_n = reinterpret_cast<unsigned long long *>(static_cast<char *>(scratch) + tbytes);
+    unsigned long long   h = 0;
+    cudaError_t e = cudaMemcpyAsync(d_tab, tab.data(), tab.size() * sizeof(RayProj), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+      e = cudaMemsetAsync(d_n, 0, sizeof(unsigned long long), st);
+    if (e == cudaSuccess)
+    {
+      JosephArgs a;
+      joseph_args(a, *vol, *proj, d_tab);
+      const dim3 grid((unsigned)((a.nu + 31) / 32), (unsigned)((a.nv + 7) / 8), (unsigned)a.np);
+      joseph_count_kernel<<<grid, 256, 0, st>>>(a, d_n);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(&h, d_n, sizeof(h), cudaMemcpyDeviceToHost, st);
+    rc = (e == cudaSuccess) ? RTKB_OK : cuda_fail(e, "joseph sample count");
+    cudaError_t fe = cudaFreeAsync(scratch, st);
+    if (fe == cudaSuccess)
+      fe = cudaStreamSynchronize(st);
+    if (rc == RTKB_OK && fe != cudaSuccess)
+      rc = cuda_fail(fe, "joseph sample count");
+    *count = (double)h;
     return rc;
   }
   catch (...)

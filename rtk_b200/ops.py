@@ -78,6 +78,14 @@ def joseph_back_project(geometry, vol_desc, proj_desc, proj, vol_in, out=None, s
     return _backproject(load().rtkb_joseph_back_project, geometry, vol_desc, proj_desc, proj, vol_in, out, stream)
 
 
+def joseph_sample_count(geometry, vol_desc, proj_desc, stream=None) -> float:
+    """Bilinear samples one Joseph forward projection takes (synchronises)."""
+    n = C.c_double()
+    check(load().rtkb_joseph_sample_count(geometry.handle, C.byref(vol_desc), C.byref(proj_desc), C.byref(n),
+                                          _stream(stream)))
+    return n.value
+
+
 def ramp_params(hann=0.0, cosine=0.0, hamming=0.0, ramlak=0.0, shepplogan=0.0, truncation=0.0, gpf=2, pad=2):
     from ._capi import RampParams
 

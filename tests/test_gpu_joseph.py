@@ -112,3 +112,12 @@ def test_joseph_cg_size_projection_subset(rtkb, oracle):
         got = to_np(rtkb.ops.joseph_forward_project(gl, vd, pd, to_gpu(vol), torch.zeros((2, 384, 512),
                                                                                           device="cuda")))
         assert rel_l2(got, ref) < REL_L2_TOL
+
+
+@pytest.mark.parametrize("geom", sorted(GEOMS))
+def test_joseph_sample_count_matches_oracle(rtkb, oracle, geom):
+    """rtkb_joseph_sample_count (the work unit of the ray-cast throughput
+    figure) equals the oracle's count from the same FP64 ray set-up."""
+    gl, go, vd, vo, pd, po, vol, pr = _case(rtkb, oracle, GEOMS[geom](30), (40, 36, 44), (4.0, 4.5, 3.5),
+                                            (72, 64, 30), (5.0, 5.0, 1.0), vindex=(2, -3, 1), pindex=(-4, 3, 0))
+    assert rtkb.ops.joseph_sample_count(gl, vd, pd) == oracle.joseph_sample_count(go, vo, po)

@@ -399,6 +399,51 @@ def run_reference(args, world, rank):
     return 0
 
 
+def profile_cg():
+    """CG configuration kernels, each launched a few times outside any graph
+    (targets for ncu --set full captures; prints a JSON line of device times)."""
+    import torch
+
+    import rtk_b200 as rtkb
+    from rtk_b200 import learned
+    from tests import phantoms
+
+    rtkb.load()
+    n = 360
+    g = rtkb.geometry.circular(n, SID, SDD)
+    vd = rtkb.make_desc((256, 256, 256), (1.0, 1.0, 1.0))
+    pd = rtkb.make_desc((512, 384, n), (0.8, 0.8, 1.0))
+    ell = phantoms.random_ellipsoids(20, SEED + 2, centre_radius=60.0, axis_range=(5.0, 60.0))
+    ell[:, 15] *= 0.02
+    p = rtkb.ops.project_ellipsoids(g, pd, ell)
+    x = torch.zeros((256, 256, 256), device="cuda")
+    cg = rtkb.ops.ConjugateGradient(g, vd, pd, use_cuda_graph=False)
+    cg.start(p, x)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    cg.iterate(2)
+    e1.record()
+    torch.cuda.synchronize()
+    t_it = e0.elapsed_time(e1) / 2
+    cg.close()
+    net = learned.UNet(seed=1)
+    r = torch.randn((256, 256, 256), device="cuda")
+    z = net.forward(r)
+    torch.cuda.synchronize()
+    e0.record()
+    net.forward(r, z)
+    e1.record()
+    torch.cuda.synchronize()
+    t_fwd = e0.elapsed_time(e1)
+    xb = torch.randn((4, 64, 64, 64), device="cuda")
+    net.train_step(xb, xb, lr=1e-3, margin=16)
+    net.close()
+    print(json.dumps({"profile_cg": {"cg_iteration_ms": t_it, "unet_forward_ms_256": t_fwd,
+                                     "workload": "256^3 @1mm <- 360 x 512x384 @0.8mm"}}), flush=True)
+    return 0
+
+
 def use_profile_case():
     """256^3 at 0.5 mm (the benchmark's voxel size, so the same tile
     footprints and kernel configuration) from 360 of the 1024x768 projections:
@@ -419,9 +464,14 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra-legs", action="store_true",
                     help="skip the FDK pipeline and CG seconds-to-residual legs")
+    ap.add_argument("--profile-cg", action="store_true",
+                    help="run the CG configuration's kernels once each for ncu captures (256^3, 360 x 512x384): CG "
+                         "start + 2 eager iterations, one U-Net forward on the volume, one training step on 4 x 64^3")
     ap.add_argument("--profile-case", action="store_true",
                     help="small case for ncu captures: 256^3 @1mm from 360 projections, device-timed region only")
     args = ap.parse_args()
+    if args.profile_cg:
+        return profile_cg()
     args.warmup = max(args.warmup, 3)
     if args.profile_case:
         use_profile_case()

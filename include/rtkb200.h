@@ -112,6 +112,16 @@ int rtkb_fdk_backproject(const rtkb_geometry * g, const rtkb_image_desc * vol, c
                          const float * d_proj, const float * d_vol_in, float * d_vol_out, void * stream);
 int rtkb_voxel_backproject(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
                            const float * d_proj, const float * d_vol_in, float * d_vol_out, void * stream);
+/* BF16 storage variant (no counterpart in the reference, whose stacks are
+ * float): the same backprojections from a bfloat16 projection stack
+ * (d_proj_bf16, same layout; RTK's arithmetic with FP32 interpolation and
+ * accumulation, FP32 volume).  Halves the stack's memory and bandwidth. */
+int rtkb_fdk_backproject_bf16(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
+                              const void * d_proj_bf16, const float * d_vol_in, float * d_vol_out, void * stream);
+int rtkb_voxel_backproject_bf16(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
+                                const void * d_proj_bf16, const float * d_vol_in, float * d_vol_out, void * stream);
+/* d_out[i] = bfloat16(d_in[i]), round to nearest even, i < n. */
+int rtkb_convert_to_bf16(const float * d_in, void * d_out, long long n, void * stream);
 /* rtkb_fdk_backproject without device allocations (no counterpart in the
  * reference).  For callers that cannot allocate device memory during a
  * reconstruction: an application whose device memory is reserved by its own

@@ -166,6 +166,9 @@ SIGNATURES.update({
     "rtkb_cg_apply_operator": (C.c_int, [_V, _V, _V, _V]),
     "rtkb_cg_start_rhs": (C.c_int, [_V, _V, _V, _V]),
     "rtkb_joseph_sample_count": (C.c_int, [_G, _IM, _IM, _D, _V]),
+    "rtkb_fdk_backproject_bf16": (C.c_int, [_G, _IM, _IM, _V, _V, _V, _V]),
+    "rtkb_voxel_backproject_bf16": (C.c_int, [_G, _IM, _IM, _V, _V, _V, _V]),
+    "rtkb_convert_to_bf16": (C.c_int, [_V, _V, C.c_longlong, _V]),
     "rtkb_cg_set_preconditioner": (C.c_int, [_V, _V, C.c_int]),
     "rtkb_cg_preconditioner_status": (C.c_int, [_V, _I, _I]),
     "rtkb_unet_create": (C.c_int, [C.c_ulonglong, C.POINTER(C.c_void_p)]),

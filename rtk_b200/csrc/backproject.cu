@@ -27,6 +27,8 @@
 #include "rtkb_internal.h"
 #include "rtkb_ptx.cuh"
 
+#include <cuda_bf16.h>
+
 #include <algorithm>
 #include <cstring>
 #include <mutex>
@@ -75,6 +77,48 @@ rcp_approx(float x)
   return r;
 }
 
+// Stored projection element: float32, or bfloat16 (BF16 storage variant;
+// interpolation and accumulation stay FP32).
+template <typename T>
+__device__ __forceinline__ float
+tap(const T * p)
+{
+  return *p;
+}
+template <>
+__device__ __forceinline__ float
+tap<__nv_bfloat16>(const __nv_bfloat16 * p)
+{
+  return __uint_as_float((unsigned)*reinterpret_cast<const unsigned short *>(p) << 16);
+}
+template <typename T>
+__device__ __forceinline__ float
+gtap(const T * p)
+{
+  return __ldg(p);
+}
+template <>
+__device__ __forceinline__ float
+gtap<__nv_bfloat16>(const __nv_bfloat16 * p)
+{
+  return __uint_as_float((unsigned)__ldg(reinterpret_cast<const unsigned short *>(p)) << 16);
+}
+template <typename T>
+__device__ __forceinline__ T
+zero_elem()
+{
+  return T(0);
+}
+template <>
+__device__ __forceinline__ __nv_bfloat16
+zero_elem<__nv_bfloat16>()
+{
+  return __ushort_as_bfloat16((unsigned short)0);
+}
+// TMA boxes must start at x * sizeof(T) = 0 mod 16
+template <typename T>
+constexpr int kAlignElems = 16 / (int)sizeof(T);
+
 __device__ __noinline__ bool
 accept_fp64(const double * m, int row, int X, int Y, int Z, int n)
 {
@@ -89,10 +133,10 @@ constexpr int kFlagUInterior = 2;
 constexpr int kFlagVInterior = 4;
 constexpr int kFlagSkip = 8; // the whole tile projects off the detector
 
-template <int BW, int BH>
+template <int BW, int BH, typename T = float>
 struct Layout
 {
-  static constexpr int kBoxBytes = BW * BH * 4;
+  static constexpr int kBoxBytes = BW * BH * (int)sizeof(T);
   static constexpr int kHeaders = 0;
   static constexpr int kBoxes = kStages * kHeaderBytes;
   static constexpr int kBars = kBoxes + kStages * kBoxBytes;
@@ -102,8 +146,9 @@ struct Layout
 // FP64 slow path for one voxel and projection: RTK's optimised-path
 // arithmetic with global-memory bilinear taps.  Out of line: the rare path's
 // FP64 registers stay off the hot loop.
+template <typename T>
 __device__ __noinline__ float
-slow_voxel(const double * M, const float * __restrict__ proj, long long pofs, int nu, int nv, int X, int Y, int Z,
+slow_voxel(const double * M, const T * __restrict__ proj, long long pofs, int nu, int nv, int X, int Y, int Z,
            bool fdkw)
 {
   const double x = X, y = Y, z = Z;
@@ -115,9 +160,9 @@ slow_voxel(const double * M, const float * __restrict__ proj, long long pofs, in
     return 0.f;
   const int     iu = (int)floor(u), iv = (int)floor(v);
   const double  fu = u - iu, fv = v - iv;
-  const float * q = proj + pofs + (long long)iv * nu + iu;
-  const double  a = (1 - fu) * __ldg(q) + fu * __ldg(q + 1);
-  const double  b = (1 - fu) * __ldg(q + nu) + fu * __ldg(q + nu + 1);
+  const T *     q = proj + pofs + (long long)iv * nu + iu;
+  const double  a = (1 - fu) * gtap(q) + fu * gtap(q + 1);
+  const double  b = (1 - fu) * gtap(q + nu) + fu * gtap(q + nu + 1);
   const double  val = (1 - fv) * a + fv * b;
   return (float)(fdkw ? rw * rw * val : val);
 }
@@ -125,13 +170,13 @@ slow_voxel(const double * M, const float * __restrict__ proj, long long pofs, in
 // Producer warp: per projection, project the tile's corners, size the
 // footprint box, publish the tile-relative coefficients and start the TMA
 // load of the box.
-template <int BW, int BH, int NYT>
+template <int BW, int BH, int NYT, typename T>
 __device__ __forceinline__ void
-bp_producer(const CUtensorMap * tmap, const float * __restrict__ proj, const double * __restrict__ mats, int nproj,
-            int nu, int nv, int x0, int y0, int z0, StageHeader * hdr, float * boxes, uint64_t * full,
+bp_producer(const CUtensorMap * tmap, const T * __restrict__ proj, const double * __restrict__ mats, int nproj,
+            int nu, int nv, int x0, int y0, int z0, StageHeader * hdr, T * boxes, uint64_t * full,
             uint64_t * empty, int use_tma)
 {
-  using L = Layout<BW, BH>;
+  using L = Layout<BW, BH, T>;
   const int lane = threadIdx.x & 31;
   if (use_tma && lane == 0)
     prefetch_tensor_map(tmap);
@@ -187,7 +232,7 @@ bp_producer(const CUtensorMap * tmap, const float * __restrict__ proj, const dou
     int ub = 0, vb = 0;
     if (fast)
     {
-      ub = ((int)floorf(umin - margin)) & ~3;
+      ub = ((int)floorf(umin - margin)) & ~(kAlignElems<T> - 1);
       vb = (int)floorf(vmin - margin);
       fast = (umax + margin < (float)(ub + BW - 1)) && (vmax + margin < (float)(vb + BH - 1));
     }
@@ -198,7 +243,7 @@ bp_producer(const CUtensorMap * tmap, const float * __restrict__ proj, const dou
     if (skip)
       fast = false;
     const double * m = h->m;
-    float * box = boxes + s * (BW * BH);
+    T *      box = boxes + s * (BW * BH);
     if (lane == 0)
     {
       int flags = 0;
@@ -238,7 +283,7 @@ bp_producer(const CUtensorMap * tmap, const float * __restrict__ proj, const dou
         for (int e = lane; e < BW * BH; e += 32)
         {
           const int gu = ub + e % BW, gv = vb + e / BW;
-          box[e] = (gu >= 0 && gu < nu && gv >= 0 && gv < nv) ? __ldg(proj + pofs + (long long)gv * nu + gu) : 0.f;
+          box[e] = (gu >= 0 && gu < nu && gv >= 0 && gv < nv) ? proj[pofs + (long long)gv * nu + gu] : zero_elem<T>();
         }
       }
       __syncwarp();
@@ -252,16 +297,16 @@ bp_producer(const CUtensorMap * tmap, const float * __restrict__ proj, const dou
       return;
 }
 
-template <int BW, int BH, int NYT, int MINB, bool FDKW>
+template <int BW, int BH, int NYT, int MINB, bool FDKW, typename T = float>
 __global__ void __launch_bounds__(kThreads, MINB)
-bp_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const float * __restrict__ proj,
+bp_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const T * __restrict__ proj,
                 const double * __restrict__ mats, int nproj, int nu, int nv, int nx, int ny, int nz, int ntx,
                 int ntz, const float * vol_in, float * vol_out, int use_tma)
 {
-  using L = Layout<BW, BH>;
+  using L = Layout<BW, BH, T>;
   extern __shared__ __align__(1024) unsigned char smem[];
   StageHeader * hdr = reinterpret_cast<StageHeader *>(smem + L::kHeaders);
-  float *       boxes = reinterpret_cast<float *>(smem + L::kBoxes);
+  T *           boxes = reinterpret_cast<T *>(smem + L::kBoxes);
   uint64_t *    full = reinterpret_cast<uint64_t *>(smem + L::kBars);
   uint64_t *    empty = full + kStages;
 
@@ -283,7 +328,7 @@ bp_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const float * __restri
 
   if (warp == kConsumerWarps)
   {
-    bp_producer<BW, BH, NYT>(&tmap, proj, mats, nproj, nu, nv, x0, y0, z0, hdr, boxes, full, empty, use_tma);
+    bp_producer<BW, BH, NYT, T>(&tmap, proj, mats, nproj, nu, nv, x0, y0, z0, hdr, boxes, full, empty, use_tma);
     return;
   }
 
@@ -304,7 +349,7 @@ bp_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const float * __restri
     if (!mbar_wait(&full[s], k & 1))
       return;
     const StageHeader * h = hdr + s;
-    const float *       box = boxes + s * (BW * BH);
+    const T *           box = boxes + s * (BW * BH);
     const int4          fl = h->fl;
     if (active)
     {
@@ -329,7 +374,7 @@ bp_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const float * __restri
         {
           const float   flu = floorf(u);
           const float   fu = u - flu;
-          const float * col = box + (int)flu;
+          const T *     col = box + (int)flu;
           if (fl.x & kFlagVInterior)
           {
 #pragma unroll
@@ -338,8 +383,8 @@ bp_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const float * __restri
               const float   v = fmaf((float)j, dv, v0);
               const float   flv = floorf(v);
               const float   fv = v - flv;
-              const float * q = col + (int)flv * BW;
-              const float   p00 = q[0], p01 = q[1], p10 = q[BW], p11 = q[BW + 1];
+              const T *     q = col + (int)flv * BW;
+              const float   p00 = tap(q), p01 = tap(q + 1), p10 = tap(q + BW), p11 = tap(q + BW + 1);
               const float   r0 = fmaf(fu, p01 - p00, p00);
               const float   r1 = fmaf(fu, p11 - p10, p10);
               acc[j] = fmaf(wt, fmaf(fv, r1 - r0, r0), acc[j]);
@@ -372,8 +417,8 @@ bp_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const float * __restri
                 const float   v = fmaf((float)j, dv, v0);
                 const float   flv = floorf(v);
                 const float   fv = v - flv;
-                const float * q = col + (int)flv * BW;
-                const float   p00 = q[0], p01 = q[1], p10 = q[BW], p11 = q[BW + 1];
+                const T *     q = col + (int)flv * BW;
+                const float   p00 = tap(q), p01 = tap(q + 1), p10 = tap(q + BW), p11 = tap(q + BW + 1);
                 const float   r0 = fmaf(fu, p01 - p00, p00);
                 const float   r1 = fmaf(fu, p11 - p10, p10);
                 acc[j] = fmaf(wt, fmaf(fv, r1 - r0, r0), acc[j]);
@@ -413,9 +458,9 @@ bp_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const float * __restri
 // Generic path (any geometry): one thread per voxel, FP64 arithmetic, RTK's
 // optimised-path bounds for modes 1/2 and itk::LinearInterpolateImageFunction
 // semantics (clamp-to-edge, accepted range [-0.5, N-0.5)) for mode 0.
-template <bool FDKW>
+template <bool FDKW, typename T = float>
 __global__ void __launch_bounds__(256)
-bp_generic_kernel(const float * __restrict__ proj, const double * __restrict__ mats, const int * __restrict__ modes,
+bp_generic_kernel(const T * __restrict__ proj, const double * __restrict__ mats, const int * __restrict__ modes,
                   int nproj, int nu, int nv, int nx, int ny, int nz, const float * vol_in, float * vol_out)
 {
   const long long n = (long long)nx * ny * nz;
@@ -432,7 +477,7 @@ bp_generic_kernel(const float * __restrict__ proj, const double * __restrict__ m
       const double   rw = 1.0 / w;
       const double   u = (__ldg(M + 0) * x + __ldg(M + 1) * y + __ldg(M + 2) * z + __ldg(M + 3)) * rw;
       const double   v = (__ldg(M + 4) * x + __ldg(M + 5) * y + __ldg(M + 6) * z + __ldg(M + 7)) * rw;
-      const float *  P = proj + (long long)p * nu * nv;
+      const T *      P = proj + (long long)p * nu * nv;
       const double   wt = FDKW ? rw * rw : 1.0;
       if (__ldg(modes + p))
       {
@@ -440,9 +485,9 @@ bp_generic_kernel(const float * __restrict__ proj, const double * __restrict__ m
         {
           const int     iu = (int)floor(u), iv = (int)floor(v);
           const double  fu = u - iu, fv = v - iv;
-          const float * q = P + (long long)iv * nu + iu;
-          acc += wt * ((1 - fv) * ((1 - fu) * __ldg(q) + fu * __ldg(q + 1)) +
-                       fv * ((1 - fu) * __ldg(q + nu) + fu * __ldg(q + nu + 1)));
+          const T *     q = P + (long long)iv * nu + iu;
+          acc += wt * ((1 - fv) * ((1 - fu) * gtap(q) + fu * gtap(q + 1)) +
+                       fv * ((1 - fu) * gtap(q + nu) + fu * gtap(q + nu + 1)));
         }
       }
       else if (u >= -0.5 && u < nu - 0.5 && v >= -0.5 && v < nv - 0.5)
@@ -451,8 +496,8 @@ bp_generic_kernel(const float * __restrict__ proj, const double * __restrict__ m
         const int    iu = (int)floor(uc), iv = (int)floor(vc);
         const int    iu1 = min(iu + 1, nu - 1), iv1 = min(iv + 1, nv - 1);
         const double fu = uc - iu, fv = vc - iv;
-        const double a = (1 - fu) * __ldg(P + (long long)iv * nu + iu) + fu * __ldg(P + (long long)iv * nu + iu1);
-        const double b = (1 - fu) * __ldg(P + (long long)iv1 * nu + iu) + fu * __ldg(P + (long long)iv1 * nu + iu1);
+        const double a = (1 - fu) * gtap(P + (long long)iv * nu + iu) + fu * gtap(P + (long long)iv * nu + iu1);
+        const double b = (1 - fu) * gtap(P + (long long)iv1 * nu + iu) + fu * gtap(P + (long long)iv1 * nu + iu1);
         acc += wt * ((1 - fv) * a + fv * b);
       }
     }
@@ -473,6 +518,10 @@ constexpr int           kNumBpConfigs = 6;
 // in the same column but different rows do not collide.
 static const BpConfig   kBpConfigs[kNumBpConfigs] = { { 68, 64, 16, 3 }, { 68, 64, 16, 2 }, { 68, 32, 8, 3 },
                                                       { 68, 32, 8, 2 },  { 132, 64, 16, 1 }, { 132, 64, 8, 1 } };
+// BF16 boxes: widths are multiples of 8 elements (16-byte TMA rows); 72 and
+// 136 elements are 36 and 68 words, again 4 banks per row.
+static const BpConfig   kBpConfigsBf16[kNumBpConfigs] = { { 72, 64, 16, 3 }, { 72, 64, 16, 2 }, { 72, 32, 8, 3 },
+                                                          { 72, 32, 8, 2 },  { 136, 64, 16, 1 }, { 136, 64, 8, 1 } };
 static thread_local int g_bp_forced_config = -1;
 static thread_local int g_bp_last_config = -1;
 
@@ -527,13 +576,13 @@ estimate_footprint(const std::vector<double> & mats, int nproj, int nx, int ny, 
   }
 }
 
-template <int BW, int BH, int NYT, int MINB, bool FDKW>
+template <int BW, int BH, int NYT, int MINB, bool FDKW, typename T>
 static int
-launch_tiled(const CUtensorMap & tmap, bool use_tma, const float * d_proj, const double * d_mats, int nproj, int nu,
+launch_tiled(const CUtensorMap & tmap, bool use_tma, const T * d_proj, const double * d_mats, int nproj, int nu,
              int nv, int nx, int ny, int nz, const float * vin, float * vout, cudaStream_t st)
 {
-  using L = Layout<BW, BH>;
-  auto kern = bp_tiled_kernel<BW, BH, NYT, MINB, FDKW>;
+  using L = Layout<BW, BH, T>;
+  auto kern = bp_tiled_kernel<BW, BH, NYT, MINB, FDKW, T>;
   RTKB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kTotal));
   const int       ntx = (nx + kTX - 1) / kTX, nty = (ny + NYT - 1) / NYT, ntz = (nz + kTZ - 1) / kTZ;
   const long long nblocks = (long long)ntx * nty * ntz;
@@ -551,7 +600,8 @@ dispatch_tiled(int cfg, const CUtensorMap & tmap, bool use_tma, const float * d_
                int nproj, int nu, int nv, int nx, int ny, int nz, const float * vin, float * vout, cudaStream_t st)
 {
 #define RTKB_BP_LAUNCH(BW, BH, NYT, MINB)                                                                              \
-  return launch_tiled<BW, BH, NYT, MINB, FDKW>(tmap, use_tma, d_proj, d_mats, nproj, nu, nv, nx, ny, nz, vin, vout, st)
+  return launch_tiled<BW, BH, NYT, MINB, FDKW, float>(tmap, use_tma, d_proj, d_mats, nproj, nu, nv, nx, ny, nz, vin,   \
+                                                      vout, st)
   switch (cfg)
   {
     case 0:
@@ -568,6 +618,40 @@ dispatch_tiled(int cfg, const CUtensorMap & tmap, bool use_tma, const float * d_
       RTKB_BP_LAUNCH(132, 64, 8, 1);
   }
 #undef RTKB_BP_LAUNCH
+}
+
+template <bool FDKW>
+static int
+dispatch_tiled(int cfg, const CUtensorMap & tmap, bool use_tma, const __nv_bfloat16 * d_proj, const double * d_mats,
+               int nproj, int nu, int nv, int nx, int ny, int nz, const float * vin, float * vout, cudaStream_t st)
+{
+#define RTKB_BP_LAUNCH(BW, BH, NYT, MINB)                                                                              \
+  return launch_tiled<BW, BH, NYT, MINB, FDKW, __nv_bfloat16>(tmap, use_tma, d_proj, d_mats, nproj, nu, nv, nx, ny, nz, \
+                                                              vin, vout, st)
+  switch (cfg)
+  {
+    case 0:
+      RTKB_BP_LAUNCH(72, 64, 16, 3);
+    case 1:
+      RTKB_BP_LAUNCH(72, 64, 16, 2);
+    case 2:
+      RTKB_BP_LAUNCH(72, 32, 8, 3);
+    case 3:
+      RTKB_BP_LAUNCH(72, 32, 8, 2);
+    case 4:
+      RTKB_BP_LAUNCH(136, 64, 16, 1);
+    default:
+      RTKB_BP_LAUNCH(136, 64, 8, 1);
+  }
+#undef RTKB_BP_LAUNCH
+}
+
+// FP32 -> BF16 (round to nearest even), two elements per thread
+__global__ void __launch_bounds__(256)
+to_bf16_kernel(const float * __restrict__ in, __nv_bfloat16 * __restrict__ out, long long n)
+{
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = __float2bfloat16_rn(in[i]);
 }
 
 } // namespace
@@ -605,11 +689,15 @@ to_buffer_matrix(const rtkb_image_desc & vol, const rtkb_image_desc & proj, int 
   std::memcpy(out, m, sizeof(m));
 }
 
+template <typename T>
 int
 backproject_buffer(const int vol_size[3], const int proj_size[3], int nproj, const double * mats, const int * modes,
-                   bool fdk, const float * d_proj, const float * d_vin, float * d_vout, cudaStream_t st,
+                   bool fdk, const T * d_proj, const float * d_vin, float * d_vout, cudaStream_t st,
                    void * fixed_scratch = nullptr)
 {
+  constexpr bool    kBf16 = sizeof(T) == 2;
+  const BpConfig *  configs = kBf16 ? kBpConfigsBf16 : kBpConfigs;
+  constexpr double  kSlack = kAlignElems<T> - 1 + 0.2; // box origin rounding + margins
   const int nx = vol_size[0], ny = vol_size[1], nz = vol_size[2];
   const int nu = proj_size[0], nv = proj_size[1];
   if (nx <= 0 || ny <= 0 || nz <= 0 || nu <= 0 || nv <= 0 || nproj < 0 || proj_size[2] < nproj)
@@ -655,11 +743,11 @@ backproject_buffer(const int vol_size[3], const int proj_size[3], int nproj, con
     {
       const long long blocks = std::min<long long>((nvox + 255) / 256, 148LL * 64);
       if (fdk)
-        bp_generic_kernel<true><<<(unsigned)blocks, 256, 0, st>>>(d_proj, d_mats, d_modes, nproj, nu, nv, nx, ny, nz,
-                                                                  d_vin, d_vout);
+        bp_generic_kernel<true, T><<<(unsigned)blocks, 256, 0, st>>>(d_proj, d_mats, d_modes, nproj, nu, nv, nx, ny,
+                                                                     nz, d_vin, d_vout);
       else
-        bp_generic_kernel<false><<<(unsigned)blocks, 256, 0, st>>>(d_proj, d_mats, d_modes, nproj, nu, nv, nx, ny,
-                                                                   nz, d_vin, d_vout);
+        bp_generic_kernel<false, T><<<(unsigned)blocks, 256, 0, st>>>(d_proj, d_mats, d_modes, nproj, nu, nv, nx, ny,
+                                                                      nz, d_vin, d_vout);
       e = cudaGetLastError();
       if (e != cudaSuccess)
         rc = cuda_fail(e, "bp_generic_kernel launch");
@@ -673,8 +761,8 @@ backproject_buffer(const int vol_size[3], const int proj_size[3], int nproj, con
     int cfg = kNumBpConfigs - 1;
     for (int c = 0; c < kNumBpConfigs; c++)
     {
-      const double fw = kBpConfigs[c].nyt == 16 ? fw16 : fw8, fh = kBpConfigs[c].nyt == 16 ? fh16 : fh8;
-      if (fw + 3.2 < kBpConfigs[c].bw - 1 && fh + 0.2 < kBpConfigs[c].bh - 1)
+      const double fw = configs[c].nyt == 16 ? fw16 : fw8, fh = configs[c].nyt == 16 ? fh16 : fh8;
+      if (fw + kSlack < configs[c].bw - 1 && fh + 0.2 < configs[c].bh - 1)
       {
         cfg = c;
         break;
@@ -689,14 +777,17 @@ backproject_buffer(const int vol_size[3], const int proj_size[3], int nproj, con
     bool              use_tma = false;
     EncodeTiledFn     enc = tensor_map_encoder();
     const long long   np_total = proj_size[2];
-    if (enc && (nu % 4) == 0 && (reinterpret_cast<uintptr_t>(d_proj) % 16) == 0 && np_total <= 0x7fffffffLL)
+    const unsigned long long esz = sizeof(T);
+    if (enc && ((unsigned long long)nu * esz) % 16 == 0 && (reinterpret_cast<uintptr_t>(d_proj) % 16) == 0 &&
+        np_total <= 0x7fffffffLL)
     {
       const unsigned long long dims[3] = { (unsigned long long)nu, (unsigned long long)nv,
                                            (unsigned long long)np_total };
-      const unsigned long long strides[2] = { (unsigned long long)nu * 4ULL, (unsigned long long)nu * nv * 4ULL };
-      const unsigned           box[3] = { (unsigned)kBpConfigs[cfg].bw, (unsigned)kBpConfigs[cfg].bh, 1u };
+      const unsigned long long strides[2] = { (unsigned long long)nu * esz, (unsigned long long)nu * nv * esz };
+      const unsigned           box[3] = { (unsigned)configs[cfg].bw, (unsigned)configs[cfg].bh, 1u };
       const unsigned           estr[3] = { 1u, 1u, 1u };
-      const int r = enc(&tmap, (int)CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3u, const_cast<float *>(d_proj), dims, strides,
+      const int r = enc(&tmap, kBf16 ? (int)CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : (int)CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                        3u, const_cast<T *>(d_proj), dims, strides,
                         box, estr, (int)CU_TENSOR_MAP_INTERLEAVE_NONE, (int)CU_TENSOR_MAP_SWIZZLE_NONE,
                         (int)CU_TENSOR_MAP_L2_PROMOTION_L2_128B, (int)CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
       use_tma = (r == 0);
@@ -714,9 +805,10 @@ backproject_buffer(const int vol_size[3], const int proj_size[3], int nproj, con
   return rc;
 }
 
+template <typename T>
 static int
 backproject_geometry(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
-                     const float * d_proj, const float * d_vin, float * d_vout, void * stream, bool fdk,
+                     const T * d_proj, const float * d_vin, float * d_vout, void * stream, bool fdk,
                      void * fixed_scratch = nullptr)
 {
   std::string why;
@@ -770,6 +862,50 @@ rtkb_voxel_backproject(const rtkb_geometry * g, const rtkb_image_desc * vol, con
   {
     return rtkb::fail(RTKB_ERR_OUT_OF_MEMORY, "host allocation failed");
   }
+}
+
+extern "C" int
+rtkb_fdk_backproject_bf16(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
+                          const void * d_proj_bf16, const float * d_vol_in, float * d_vol_out, void * stream)
+{
+  try
+  {
+    return rtkb::backproject_geometry(g, vol, proj, static_cast<const __nv_bfloat16 *>(d_proj_bf16), d_vol_in,
+                                      d_vol_out, stream, true);
+  }
+  catch (...)
+  {
+    return rtkb::fail(RTKB_ERR_OUT_OF_MEMORY, "host allocation failed");
+  }
+}
+
+extern "C" int
+rtkb_voxel_backproject_bf16(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
+                            const void * d_proj_bf16, const float * d_vol_in, float * d_vol_out, void * stream)
+{
+  try
+  {
+    return rtkb::backproject_geometry(g, vol, proj, static_cast<const __nv_bfloat16 *>(d_proj_bf16), d_vol_in,
+                                      d_vol_out, stream, false);
+  }
+  catch (...)
+  {
+    return rtkb::fail(RTKB_ERR_OUT_OF_MEMORY, "host allocation failed");
+  }
+}
+
+extern "C" int
+rtkb_convert_to_bf16(const float * d_in, void * d_out, long long n, void * stream)
+{
+  if ((!d_in || !d_out) && n > 0)
+    return rtkb::fail(RTKB_ERR_INVALID_ARGUMENT, "null buffer");
+  if (n <= 0)
+    return RTKB_OK;
+  const long long blocks = std::min<long long>((n + 255) / 256, 148LL * 32);
+  to_bf16_kernel<<<(unsigned)blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+    d_in, static_cast<__nv_bfloat16 *>(d_out), n);
+  RTKB_CUDA_TRY(cudaGetLastError());
+  return RTKB_OK;
 }
 
 extern "C" int

@@ -38,26 +38,60 @@ def _check_shape(t, desc, what):
         raise ValueError(f"{what}: shape {tuple(t.shape)} does not match description {shape_of(desc)}")
 
 
-def _backproject(fn, geometry, vol_desc, proj_desc, proj, vol_in, out, stream):
+def _ptr_bf16(t):
+    torch = _torch()
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError("expected a CUDA tensor (there is no CPU path)")
+    if t.dtype != torch.bfloat16 or not t.is_contiguous():
+        raise TypeError("expected a contiguous bfloat16 tensor")
+    return C.c_void_p(t.data_ptr())
+
+
+def _backproject(fn, geometry, vol_desc, proj_desc, proj, vol_in, out, stream, fn_bf16=None):
+    """Backprojection from a float32 stack, or from a bfloat16 stack (BF16
+    storage variant) when proj.dtype is torch.bfloat16."""
     torch = _torch()
     _check_shape(proj, proj_desc, "projections")
     _check_shape(vol_in, vol_desc, "volume")
     if out is None:
         out = torch.empty_like(vol_in)
     _check_shape(out, vol_desc, "output")
-    check(fn(geometry.handle, C.byref(vol_desc), C.byref(proj_desc), _ptr(proj), _ptr(vol_in), _ptr(out),
-             _stream(stream)))
+    if proj.dtype == torch.bfloat16:
+        if fn_bf16 is None:
+            raise TypeError("this projector has no bfloat16 variant")
+        fn, pp = fn_bf16, _ptr_bf16(proj)
+    else:
+        pp = _ptr(proj)
+    check(fn(geometry.handle, C.byref(vol_desc), C.byref(proj_desc), pp, _ptr(vol_in), _ptr(out), _stream(stream)))
+    return out
+
+
+def to_bf16(x, out=None, stream=None):
+    """bfloat16 copy of a float32 CUDA tensor (round to nearest even), by the
+    library's own kernel."""
+    torch = _torch()
+    if out is None:
+        out = torch.empty(x.shape, dtype=torch.bfloat16, device=x.device)
+    if out.shape != x.shape:
+        raise ValueError("shape mismatch")
+    check(load().rtkb_convert_to_bf16(_ptr(x), _ptr_bf16(out), x.numel(), _stream(stream)))
     return out
 
 
 def fdk_backproject(geometry, vol_desc, proj_desc, proj, vol_in, out=None, stream=None):
-    """rtk::FDKBackProjectionImageFilter: out = vol_in + FDK backprojection."""
-    return _backproject(load().rtkb_fdk_backproject, geometry, vol_desc, proj_desc, proj, vol_in, out, stream)
+    """rtk::FDKBackProjectionImageFilter: out = vol_in + FDK backprojection
+    (proj float32, or bfloat16 for the BF16 storage variant)."""
+    L = load()
+    return _backproject(L.rtkb_fdk_backproject, geometry, vol_desc, proj_desc, proj, vol_in, out, stream,
+                        L.rtkb_fdk_backproject_bf16)
 
 
 def voxel_backproject(geometry, vol_desc, proj_desc, proj, vol_in, out=None, stream=None):
-    """rtk::BackProjectionImageFilter (voxel-based): out = vol_in + backprojection."""
-    return _backproject(load().rtkb_voxel_backproject, geometry, vol_desc, proj_desc, proj, vol_in, out, stream)
+    """rtk::BackProjectionImageFilter (voxel-based): out = vol_in + backprojection
+    (proj float32, or bfloat16 for the BF16 storage variant)."""
+    L = load()
+    return _backproject(L.rtkb_voxel_backproject, geometry, vol_desc, proj_desc, proj, vol_in, out, stream,
+                        L.rtkb_voxel_backproject_bf16)
 
 
 def joseph_forward_project(geometry, vol_desc, proj_desc, vol, proj_in, out=None, stream=None):

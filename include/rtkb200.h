@@ -112,6 +112,48 @@ int rtkb_fdk_backproject(const rtkb_geometry * g, const rtkb_image_desc * vol, c
                          const float * d_proj, const float * d_vol_in, float * d_vol_out, void * stream);
 int rtkb_voxel_backproject(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
                            const float * d_proj, const float * d_vol_in, float * d_vol_out, void * stream);
+/* Batched backprojection (no counterpart in the reference): many independent
+ * problems of uneven sizes in one persistent launch -- CTAs take (problem,
+ * tile) work items from a shared queue until it is empty.  Each problem is a
+ * full rtkb_fdk_backproject / rtkb_voxel_backproject call (its own geometry,
+ * descriptions and buffers, float32 stacks).  config: backprojector
+ * configuration (0..count-1 of rtkb_backproject_config) for the whole batch,
+ * -1 for the first one whose box holds every problem's footprint;
+ * *used_config (may be NULL) receives it.  Problems on RTK's generic path
+ * (tilted detectors, rotated volumes) run as separate launches.  These one-shot
+ * calls prepare, execute and release a batch and wait for `stream`. */
+typedef struct rtkb_bp_problem
+{
+  const rtkb_geometry * geometry;
+  rtkb_image_desc       vol, proj;
+  const float *         d_proj;
+  const float *         d_vol_in;
+  float *               d_vol_out;
+} rtkb_bp_problem;
+int rtkb_fdk_backproject_batch(const rtkb_bp_problem * problems, int n, int config, int * used_config, void * stream);
+int rtkb_voxel_backproject_batch(const rtkb_bp_problem * problems, int n, int config, int * used_config,
+                                 void * stream);
+/* Prepared batch: the host work (matrices, footprints, TMA descriptors,
+ * device tables) done once; each execute is one persistent launch on
+ * `stream` (asynchronous).  The problems' buffers must stay valid while the
+ * batch is used.  rtkb_bp_batch_config returns the configuration it runs. */
+typedef struct rtkb_bp_batch rtkb_bp_batch;
+int  rtkb_bp_batch_create(const rtkb_bp_problem * problems, int n, int fdk, int config, rtkb_bp_batch ** batch);
+int  rtkb_bp_batch_execute(rtkb_bp_batch * batch, void * stream);
+int  rtkb_bp_batch_config(const rtkb_bp_batch * batch);
+void rtkb_bp_batch_destroy(rtkb_bp_batch * batch);
+/* Autotuner: times every backprojector configuration on this batch (a
+ * prepared batch per configuration, one warm-up and `repeats` timed executes
+ * each, CUDA events on `stream`) and returns
+ * the fastest in *best_config (its time in *best_ms, every configuration's in
+ * config_ms[count] when not NULL).  With n == 1 it times the single-problem
+ * path (rtkb_fdk_backproject / rtkb_voxel_backproject with the configuration
+ * forced), whose calls then take the result through rtkb_backproject_config.  Writes the problems' outputs, which must
+ * not alias their inputs.  Use the result as `config` of the batch calls or
+ * with rtkb_backproject_config for single calls. */
+int rtkb_backproject_autotune(const rtkb_bp_problem * problems, int n, int fdk, int repeats, int * best_config,
+                              double * best_ms, double * config_ms, void * stream);
+
 /* BF16 storage variant (no counterpart in the reference, whose stacks are
  * float): the same backprojections from a bfloat16 projection stack
  * (d_proj_bf16, same layout; RTK's arithmetic with FP32 interpolation and

@@ -182,3 +182,21 @@ SIGNATURES.update({
                                        C.c_int, _D, _V]),
     "rtkb_unet_destroy": (None, [_V]),
 })
+
+
+class BpProblem(C.Structure):
+    """rtkb_bp_problem."""
+
+    _fields_ = [("geometry", C.c_void_p), ("vol", ImageDesc), ("proj", ImageDesc), ("d_proj", C.c_void_p),
+                ("d_vol_in", C.c_void_p), ("d_vol_out", C.c_void_p)]
+
+
+SIGNATURES.update({
+    "rtkb_fdk_backproject_batch": (C.c_int, [C.POINTER(BpProblem), C.c_int, C.c_int, _I, _V]),
+    "rtkb_voxel_backproject_batch": (C.c_int, [C.POINTER(BpProblem), C.c_int, C.c_int, _I, _V]),
+    "rtkb_backproject_autotune": (C.c_int, [C.POINTER(BpProblem), C.c_int, C.c_int, C.c_int, _I, _D, _D, _V]),
+    "rtkb_bp_batch_create": (C.c_int, [C.POINTER(BpProblem), C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "rtkb_bp_batch_execute": (C.c_int, [_V, _V]),
+    "rtkb_bp_batch_config": (C.c_int, [_V]),
+    "rtkb_bp_batch_destroy": (None, [_V]),
+})

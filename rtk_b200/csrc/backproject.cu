@@ -39,6 +39,7 @@ namespace dev
 {
 __device__ unsigned int g_device_status = 0;
 }
+struct BatchProblemHandle; // device-side problem table of a prepared batch
 } // namespace rtkb
 
 namespace
@@ -170,11 +171,14 @@ slow_voxel(const double * M, const T * __restrict__ proj, long long pofs, int nu
 // Producer warp: per projection, project the tile's corners, size the
 // footprint box, publish the tile-relative coefficients and start the TMA
 // load of the box.
+// gbase: projections this CTA's ring has already carried (persistent
+// kernels continue the stage index and barrier parity across tiles).
+// Returns false when a bounded wait gave up.
 template <int BW, int BH, int NYT, typename T>
-__device__ __forceinline__ void
+__device__ __forceinline__ bool
 bp_producer(const CUtensorMap * tmap, const T * __restrict__ proj, const double * __restrict__ mats, int nproj,
             int nu, int nv, int x0, int y0, int z0, StageHeader * hdr, T * boxes, uint64_t * full,
-            uint64_t * empty, int use_tma)
+            uint64_t * empty, int use_tma, unsigned gbase = 0)
 {
   using L = Layout<BW, BH, T>;
   const int lane = threadIdx.x & 31;
@@ -192,9 +196,11 @@ bp_producer(const CUtensorMap * tmap, const T * __restrict__ proj, const double 
   double mnext = (lane < 12 && nproj > 0) ? __ldg(mats + lane) : 0.0;
   for (int p = 0; p < nproj; p++)
   {
-    const int s = p % kStages, k = p / kStages;
-    if (p >= kStages && !mbar_wait(&empty[s], (k - 1) & 1))
-      return;
+    const unsigned gp = gbase + (unsigned)p;
+    const int      s = (int)(gp % kStages);
+    const unsigned k = gp / kStages;
+    if (gp >= (unsigned)kStages && !mbar_wait(&empty[s], (k - 1) & 1))
+      return false;
     StageHeader * h = hdr + s;
     if (lane < 12)
     {
@@ -293,45 +299,23 @@ bp_producer(const CUtensorMap * tmap, const T * __restrict__ proj, const double 
   }
   // drain: wait for the last copies to land before the CTA may exit
   for (int p = max(0, nproj - kStages); p < nproj; p++)
-    if (!mbar_wait(&full[p % kStages], (p / kStages) & 1))
-      return;
+  {
+    const unsigned gp = gbase + (unsigned)p;
+    if (!mbar_wait(&full[gp % kStages], (gp / kStages) & 1))
+      return false;
+  }
+  return true;
 }
 
-template <int BW, int BH, int NYT, int MINB, bool FDKW, typename T = float>
-__global__ void __launch_bounds__(kThreads, MINB)
-bp_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const T * __restrict__ proj,
-                const double * __restrict__ mats, int nproj, int nu, int nv, int nx, int ny, int nz, int ntx,
-                int ntz, const float * vol_in, float * vol_out, int use_tma)
+// Consumer warps: thread (x, z) of the tile accumulates its y-column over the
+// stack and adds it to the volume.  Returns false when a bounded wait gave up.
+template <int BW, int BH, int NYT, bool FDKW, typename T>
+__device__ __forceinline__ bool
+bp_consumer(const T * __restrict__ proj, int nproj, int nu, int nv, int nx, int ny, int nz, int x0, int y0, int z0,
+            const StageHeader * hdr, const T * boxes, uint64_t * full, uint64_t * empty, const float * vol_in,
+            float * vol_out, unsigned gbase = 0)
 {
-  using L = Layout<BW, BH, T>;
-  extern __shared__ __align__(1024) unsigned char smem[];
-  StageHeader * hdr = reinterpret_cast<StageHeader *>(smem + L::kHeaders);
-  T *           boxes = reinterpret_cast<T *>(smem + L::kBoxes);
-  uint64_t *    full = reinterpret_cast<uint64_t *>(smem + L::kBars);
-  uint64_t *    empty = full + kStages;
-
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int b = blockIdx.x;
-  const int tx = b % ntx, tz = (b / ntx) % ntz, ty = b / (ntx * ntz);
-  const int x0 = tx * kTX, y0 = ty * NYT, z0 = tz * kTZ;
-
-  if (threadIdx.x == 0)
-  {
-    for (int s = 0; s < kStages; s++)
-    {
-      mbar_init(&full[s], 1);
-      mbar_init(&empty[s], kConsumerWarps);
-    }
-    fence_barrier_init();
-  }
-  __syncthreads();
-
-  if (warp == kConsumerWarps)
-  {
-    bp_producer<BW, BH, NYT, T>(&tmap, proj, mats, nproj, nu, nv, x0, y0, z0, hdr, boxes, full, empty, use_tma);
-    return;
-  }
-
+  const int lane = threadIdx.x & 31;
   // --------------------------------------------------------------- consumers
   const int   t = threadIdx.x;
   const int   dx = t % kTX, dz = t / kTX;
@@ -345,9 +329,10 @@ bp_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const T * __restrict__
 
   for (int p = 0; p < nproj; p++)
   {
-    const int s = p % kStages, k = p / kStages;
-    if (!mbar_wait(&full[s], k & 1))
-      return;
+    const unsigned gp = gbase + (unsigned)p;
+    const int      s = (int)(gp % kStages);
+    if (!mbar_wait(&full[s], (gp / kStages) & 1))
+      return false;
     const StageHeader * h = hdr + s;
     const T *           box = boxes + s * (BW * BH);
     const int4          fl = h->fl;
@@ -453,6 +438,132 @@ bp_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const T * __restrict__
       }
     }
   }
+  return true;
+}
+
+template <int BW, int BH, int NYT, int MINB, bool FDKW, typename T = float>
+__global__ void __launch_bounds__(kThreads, MINB)
+bp_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const T * __restrict__ proj,
+                const double * __restrict__ mats, int nproj, int nu, int nv, int nx, int ny, int nz, int ntx,
+                int ntz, const float * vol_in, float * vol_out, int use_tma)
+{
+  using L = Layout<BW, BH, T>;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  StageHeader * hdr = reinterpret_cast<StageHeader *>(smem + L::kHeaders);
+  T *           boxes = reinterpret_cast<T *>(smem + L::kBoxes);
+  uint64_t *    full = reinterpret_cast<uint64_t *>(smem + L::kBars);
+  uint64_t *    empty = full + kStages;
+
+  const int warp = threadIdx.x >> 5;
+  const int b = blockIdx.x;
+  const int tx = b % ntx, tz = (b / ntx) % ntz, ty = b / (ntx * ntz);
+  const int x0 = tx * kTX, y0 = ty * NYT, z0 = tz * kTZ;
+
+  if (threadIdx.x == 0)
+  {
+    for (int s = 0; s < kStages; s++)
+    {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kConsumerWarps);
+    }
+    fence_barrier_init();
+  }
+  __syncthreads();
+
+  if (warp == kConsumerWarps)
+  {
+    bp_producer<BW, BH, NYT, T>(&tmap, proj, mats, nproj, nu, nv, x0, y0, z0, hdr, boxes, full, empty, use_tma);
+    return;
+  }
+
+  bp_consumer<BW, BH, NYT, FDKW, T>(proj, nproj, nu, nv, nx, ny, nz, x0, y0, z0, hdr, boxes, full, empty, vol_in,
+                                    vol_out);
+}
+
+constexpr int kBatchSmemExtra = 1024 + 16; // base alignment slack + work item + abort flag
+
+// One problem of a persistent batched launch: its own TMA descriptor (in
+// global memory), matrices, sizes and volumes; tile_begin = index of its
+// first work item in the batch's queue.
+struct __align__(64) BatchProblem
+{
+  CUtensorMap    tmap;
+  const float *  proj;
+  const double * mats;
+  const float *  vin;
+  float *        vout;
+  long long      tile_begin;
+  int            nproj, nu, nv, nx, ny, nz, ntx, ntz, use_tma, pad;
+};
+
+// Persistent batched backprojection: every CTA takes (problem, tile) work
+// items from a global counter until the queue is empty, so many problems of
+// uneven sizes share one launch without tail effects per problem.  The
+// stage ring continues across items (gbase), so no barrier is re-armed; a
+// bounded wait that gives up raises a CTA-wide abort at the next item.
+template <int BW, int BH, int NYT, int MINB, bool FDKW>
+__global__ void __launch_bounds__(kThreads, MINB)
+bp_batch_kernel(const BatchProblem * __restrict__ probs, int nprob, long long nitems,
+                unsigned long long * __restrict__ counter)
+{
+  using L = Layout<BW, BH, float>;
+  // No static shared variables here: they would shift the dynamic region and
+  // break the 128-byte alignment TMA needs for its destination boxes.  The
+  // base is aligned explicitly (the launch adds kBatchSmemExtra bytes).
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char * smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+  StageHeader *   hdr = reinterpret_cast<StageHeader *>(smem + L::kHeaders);
+  float *         boxes = reinterpret_cast<float *>(smem + L::kBoxes);
+  uint64_t *      full = reinterpret_cast<uint64_t *>(smem + L::kBars);
+  uint64_t *      empty = full + kStages;
+  long long &     item_sh = *reinterpret_cast<long long *>(smem + L::kTotal);
+  int &           abort_sh = *reinterpret_cast<int *>(smem + L::kTotal + 8);
+  const int       warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0)
+  {
+    for (int s = 0; s < kStages; s++)
+    {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kConsumerWarps);
+    }
+    fence_barrier_init();
+    abort_sh = 0;
+  }
+  unsigned gbase = 0;
+  for (;;)
+  {
+    __syncthreads();
+    if (threadIdx.x == 0)
+      item_sh = (long long)atomicAdd(counter, 1ULL);
+    __syncthreads();
+    const long long item = item_sh;
+    if (item >= nitems || abort_sh)
+      break;
+    int lo = 0, hi = nprob - 1;
+    while (lo < hi)
+    {
+      const int mid = (lo + hi + 1) >> 1;
+      if (probs[mid].tile_begin <= item)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    const BatchProblem & P = probs[lo];
+    const long long      local = item - P.tile_begin;
+    const int            tx = (int)(local % P.ntx), tz = (int)((local / P.ntx) % P.ntz),
+               ty = (int)(local / ((long long)P.ntx * P.ntz));
+    const int x0 = tx * kTX, y0 = ty * NYT, z0 = tz * kTZ;
+    bool      ok;
+    if (warp == kConsumerWarps)
+      ok = bp_producer<BW, BH, NYT, float>(&P.tmap, P.proj, P.mats, P.nproj, P.nu, P.nv, x0, y0, z0, hdr, boxes, full,
+                                           empty, P.use_tma, gbase);
+    else
+      ok = bp_consumer<BW, BH, NYT, FDKW, float>(P.proj, P.nproj, P.nu, P.nv, P.nx, P.ny, P.nz, x0, y0, z0, hdr, boxes,
+                                                 full, empty, P.vin, P.vout, gbase);
+    if (!ok)
+      abort_sh = 1;
+    gbase += (unsigned)P.nproj;
+  }
 }
 
 // Generic path (any geometry): one thread per voxel, FP64 arithmetic, RTK's
@@ -536,7 +647,11 @@ estimate_footprint(const std::vector<double> & mats, int nproj, int nx, int ny, 
   const int tiles_x[3] = { 0, std::max(0, (nx - 1) / kTX * kTX), std::max(0, (nx / 2) / kTX * kTX) };
   const int tiles_y[3] = { 0, std::max(0, (ny - 1) / nyt * nyt), std::max(0, (ny / 2) / nyt * nyt) };
   const int tiles_z[3] = { 0, std::max(0, (nz - 1) / kTZ * kTZ), std::max(0, (nz / 2) / kTZ * kTZ) };
-  for (int p = 0; p < nproj; p++)
+  // footprints vary smoothly with the projection: probe about 64 of them
+  // (the estimate only picks the box size; tiles that do not fit take the
+  // FP64 path, so it never affects results)
+  const int step = std::max(1, nproj / 64);
+  for (int p = 0; p < nproj; p += step)
   {
     const double * m = mats.data() + 12 * p;
     for (int a = 0; a < 3; a++)
@@ -644,6 +759,46 @@ dispatch_tiled(int cfg, const CUtensorMap & tmap, bool use_tma, const __nv_bfloa
       RTKB_BP_LAUNCH(136, 64, 8, 1);
   }
 #undef RTKB_BP_LAUNCH
+}
+
+template <int BW, int BH, int NYT, int MINB, bool FDKW>
+static int
+launch_batch(const BatchProblem * d_probs, int nprob, long long nitems, unsigned long long * d_counter, cudaStream_t st)
+{
+  using L = Layout<BW, BH, float>;
+  auto      kern = bp_batch_kernel<BW, BH, NYT, MINB, FDKW>;
+  const int smem = L::kTotal + kBatchSmemExtra;
+  RTKB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  int dev = 0, sms = 0, per_sm = 0;
+  RTKB_CUDA_TRY(cudaGetDevice(&dev));
+  RTKB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  RTKB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem));
+  const long long grid = std::max<long long>(1, std::min<long long>(nitems, (long long)sms * std::max(per_sm, 1)));
+  kern<<<(unsigned)grid, kThreads, smem, st>>>(d_probs, nprob, nitems, d_counter);
+  RTKB_CUDA_TRY(cudaGetLastError());
+  return RTKB_OK;
+}
+
+template <bool FDKW>
+static int
+dispatch_batch(int cfg, const BatchProblem * d_probs, int nprob, long long nitems, unsigned long long * d_counter,
+               cudaStream_t st)
+{
+  switch (cfg)
+  {
+    case 0:
+      return launch_batch<68, 64, 16, 3, FDKW>(d_probs, nprob, nitems, d_counter, st);
+    case 1:
+      return launch_batch<68, 64, 16, 2, FDKW>(d_probs, nprob, nitems, d_counter, st);
+    case 2:
+      return launch_batch<68, 32, 8, 3, FDKW>(d_probs, nprob, nitems, d_counter, st);
+    case 3:
+      return launch_batch<68, 32, 8, 2, FDKW>(d_probs, nprob, nitems, d_counter, st);
+    case 4:
+      return launch_batch<132, 64, 16, 1, FDKW>(d_probs, nprob, nitems, d_counter, st);
+    default:
+      return launch_batch<132, 64, 8, 1, FDKW>(d_probs, nprob, nitems, d_counter, st);
+  }
 }
 
 // FP32 -> BF16 (round to nearest even), two elements per thread
@@ -836,6 +991,240 @@ backproject_geometry(const rtkb_geometry * g, const rtkb_image_desc * vol, const
 
 } // namespace rtkb
 
+// A prepared batch: device tables (problem descriptors with their TMA maps,
+// matrices, work counter) built once on the host; executing it is one
+// counter reset and one persistent launch (plus separate launches for the
+// problems on RTK's generic path).
+struct rtkb_bp_batch
+{
+  bool                       fdk = true;
+  int                        cfg = 0;
+  int                        nbatch = 0;
+  long long                  items = 0;
+  void *                     mem = nullptr;
+  rtkb::BatchProblemHandle * probs = nullptr; // device array (opaque on the host side)
+  unsigned long long *       counter = nullptr;
+  struct Generic
+  {
+    rtkb_bp_problem     p;
+    std::vector<double> mats;
+    std::vector<int>    modes;
+  };
+  std::vector<Generic> generic;
+};
+
+namespace rtkb
+{
+
+static void
+release_batch(rtkb_bp_batch * b)
+{
+  if (!b)
+    return;
+  if (b->mem)
+    cudaFree(b->mem);
+  delete b;
+}
+
+static int
+create_batch(const rtkb_bp_problem * probs, int n, bool fdk, int cfg, rtkb_bp_batch ** out)
+{
+  if (!out)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "null batch pointer");
+  *out = nullptr;
+  if (n < 0 || (n > 0 && !probs))
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "null problem list");
+  if (cfg >= kNumBpConfigs)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "configuration out of range");
+  rtkb_bp_batch * B = new rtkb_bp_batch();
+  B->fdk = fdk;
+  struct Host
+  {
+    int                 idx;
+    std::vector<double> mats;
+  };
+  std::vector<Host> batch;
+  double            fw8 = 0., fh8 = 0., fw16 = 0., fh16 = 0.;
+  for (int i = 0; i < n; i++)
+  {
+    const rtkb_bp_problem & P = probs[i];
+    std::string             why;
+    int                     rc = RTKB_OK;
+    if (!P.geometry)
+      rc = fail(RTKB_ERR_INVALID_ARGUMENT, "Geometry has not been set.");
+    else if (!desc_valid(&P.vol, why) || !desc_valid(&P.proj, why))
+      rc = fail(RTKB_ERR_INVALID_ARGUMENT, why);
+    else if (P.geometry->g.radius_cylindrical != 0.)
+      rc = fail(RTKB_ERR_UNSUPPORTED, "Voxel-based FDK back projector can currently not handle cylindrical detectors");
+    else if (P.proj.index[2] < 0 || (long long)P.proj.index[2] + P.proj.size[2] > (long long)P.geometry->g.p.size())
+      rc = fail(RTKB_ERR_INVALID_ARGUMENT, "Mismatch between the number of projections and the geometry entries.");
+    else if (!P.d_vol_in || !P.d_vol_out || (P.proj.size[2] > 0 && !P.d_proj))
+      rc = fail(RTKB_ERR_INVALID_ARGUMENT, "null buffer");
+    if (rc != RTKB_OK)
+    {
+      release_batch(B);
+      return rc;
+    }
+    const int           np = P.proj.size[2];
+    std::vector<double> mats(12 * (size_t)np);
+    std::vector<int>    modes(np);
+    bool                opt_y = true;
+    for (int sidx = 0; sidx < np; sidx++)
+    {
+      double m[12];
+      modes[sidx] = bp_matrix(P.geometry->g, P.vol, P.proj, P.proj.index[2] + sidx, fdk, m);
+      to_buffer_matrix(P.vol, P.proj, modes[sidx], m, mats.data() + 12 * sidx);
+      for (int q = 0; q < 12; q++)
+        if (!std::isfinite(mats[12 * sidx + q]))
+        {
+          release_batch(B);
+          return fail(RTKB_ERR_INVALID_ARGUMENT, "non-finite projection matrix");
+        }
+      opt_y = opt_y && modes[sidx] == 2;
+    }
+    if (!opt_y || np == 0)
+    {
+      B->generic.push_back(rtkb_bp_batch::Generic{ P, std::move(mats), std::move(modes) });
+      continue;
+    }
+    double a, b, c, d;
+    estimate_footprint(mats, np, P.vol.size[0], P.vol.size[1], P.vol.size[2], 8, a, b);
+    estimate_footprint(mats, np, P.vol.size[0], P.vol.size[1], P.vol.size[2], 16, c, d);
+    fw8 = std::max(fw8, a);
+    fh8 = std::max(fh8, b);
+    fw16 = std::max(fw16, c);
+    fh16 = std::max(fh16, d);
+    batch.push_back(Host{ i, std::move(mats) });
+  }
+  if (cfg < 0)
+  {
+    cfg = kNumBpConfigs - 1;
+    for (int c = 0; c < kNumBpConfigs; c++)
+    {
+      const double fw = kBpConfigs[c].nyt == 16 ? fw16 : fw8, fh = kBpConfigs[c].nyt == 16 ? fh16 : fh8;
+      if (fw + 3.2 < kBpConfigs[c].bw - 1 && fh + 0.2 < kBpConfigs[c].bh - 1)
+      {
+        cfg = c;
+        break;
+      }
+    }
+  }
+  B->cfg = cfg;
+  B->nbatch = (int)batch.size();
+  if (batch.empty())
+  {
+    *out = B;
+    return RTKB_OK;
+  }
+  const BpConfig            C = kBpConfigs[cfg];
+  std::vector<BatchProblem> hp(batch.size());
+  size_t                    nmats = 0;
+  for (const Host & h : batch)
+    nmats += h.mats.size();
+  const size_t pbytes = (hp.size() * sizeof(BatchProblem) + 255) & ~size_t(255);
+  const size_t mbytes = (nmats * sizeof(double) + 255) & ~size_t(255);
+  cudaError_t  e = cudaMalloc(&B->mem, pbytes + mbytes + 256);
+  if (e != cudaSuccess)
+  {
+    release_batch(B);
+    return cuda_fail(e, "cudaMalloc (batch tables)");
+  }
+  BatchProblem * d_probs = static_cast<BatchProblem *>(B->mem);
+  double *       d_mats = reinterpret_cast<double *>(static_cast<char *>(B->mem) + pbytes);
+  B->probs = reinterpret_cast<BatchProblemHandle *>(d_probs);
+  B->counter = reinterpret_cast<unsigned long long *>(static_cast<char *>(B->mem) + pbytes + mbytes);
+  std::vector<double> allm;
+  allm.reserve(nmats);
+  long long     items = 0;
+  EncodeTiledFn enc = tensor_map_encoder();
+  for (size_t k = 0; k < batch.size(); k++)
+  {
+    const rtkb_bp_problem & P = probs[batch[k].idx];
+    BatchProblem &          Q = hp[k];
+    std::memset(&Q, 0, sizeof(Q));
+    Q.proj = P.d_proj;
+    Q.mats = d_mats + allm.size();
+    allm.insert(allm.end(), batch[k].mats.begin(), batch[k].mats.end());
+    Q.vin = P.d_vol_in;
+    Q.vout = P.d_vol_out;
+    Q.nproj = P.proj.size[2];
+    Q.nu = P.proj.size[0];
+    Q.nv = P.proj.size[1];
+    Q.nx = P.vol.size[0];
+    Q.ny = P.vol.size[1];
+    Q.nz = P.vol.size[2];
+    Q.ntx = (Q.nx + kTX - 1) / kTX;
+    Q.ntz = (Q.nz + kTZ - 1) / kTZ;
+    const int nty = (Q.ny + C.nyt - 1) / C.nyt;
+    Q.tile_begin = items;
+    items += (long long)Q.ntx * nty * Q.ntz;
+    Q.use_tma = 0;
+    if (enc && (Q.nu % 4) == 0 && (reinterpret_cast<uintptr_t>(P.d_proj) % 16) == 0)
+    {
+      const unsigned long long dims[3] = { (unsigned long long)Q.nu, (unsigned long long)Q.nv,
+                                           (unsigned long long)Q.nproj };
+      const unsigned long long strides[2] = { (unsigned long long)Q.nu * 4ULL, (unsigned long long)Q.nu * Q.nv * 4ULL };
+      const unsigned           box[3] = { (unsigned)C.bw, (unsigned)C.bh, 1u };
+      const unsigned           estr[3] = { 1u, 1u, 1u };
+      const int r = enc(&Q.tmap, (int)CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3u, const_cast<float *>(P.d_proj), dims, strides,
+                        box, estr, (int)CU_TENSOR_MAP_INTERLEAVE_NONE, (int)CU_TENSOR_MAP_SWIZZLE_NONE,
+                        (int)CU_TENSOR_MAP_L2_PROMOTION_L2_128B, (int)CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      Q.use_tma = (r == 0) ? 1 : 0;
+    }
+  }
+  B->items = items;
+  e = cudaMemcpy(d_probs, hp.data(), hp.size() * sizeof(BatchProblem), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(d_mats, allm.data(), allm.size() * sizeof(double), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess)
+  {
+    release_batch(B);
+    return cuda_fail(e, "batch upload");
+  }
+  *out = B;
+  return RTKB_OK;
+}
+
+static int
+execute_batch(rtkb_bp_batch * B, cudaStream_t st)
+{
+  if (!B)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "null batch");
+  for (rtkb_bp_batch::Generic & G : B->generic)
+  {
+    const int rc = backproject_buffer(G.p.vol.size, G.p.proj.size, G.p.proj.size[2], G.mats.data(), G.modes.data(),
+                                      B->fdk, G.p.d_proj, G.p.d_vol_in, G.p.d_vol_out, st);
+    if (rc != RTKB_OK)
+      return rc;
+  }
+  if (B->nbatch == 0)
+    return RTKB_OK;
+  RTKB_CUDA_TRY(cudaMemsetAsync(B->counter, 0, sizeof(unsigned long long), st));
+  const BatchProblem * d_probs = reinterpret_cast<const BatchProblem *>(B->probs);
+  return B->fdk ? dispatch_batch<true>(B->cfg, d_probs, B->nbatch, B->items, B->counter, st)
+                : dispatch_batch<false>(B->cfg, d_probs, B->nbatch, B->items, B->counter, st);
+}
+
+static int
+backproject_batch(const rtkb_bp_problem * probs, int n, bool fdk, int cfg, int * used_config, cudaStream_t st)
+{
+  rtkb_bp_batch * B = nullptr;
+  int             rc = create_batch(probs, n, fdk, cfg, &B);
+  if (rc != RTKB_OK)
+    return rc;
+  if (used_config)
+    *used_config = B->cfg;
+  rc = execute_batch(B, st);
+  // the tables are freed only once the launch that reads them has finished
+  const cudaError_t e = cudaStreamSynchronize(st);
+  if (rc == RTKB_OK && e != cudaSuccess)
+    rc = cuda_fail(e, "batch backprojection");
+  release_batch(B);
+  return rc;
+}
+
+} // namespace rtkb
+
 extern "C" int
 rtkb_fdk_backproject(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
                      const float * d_proj, const float * d_vol_in, float * d_vol_out, void * stream)
@@ -892,6 +1281,132 @@ rtkb_voxel_backproject_bf16(const rtkb_geometry * g, const rtkb_image_desc * vol
   {
     return rtkb::fail(RTKB_ERR_OUT_OF_MEMORY, "host allocation failed");
   }
+}
+
+extern "C" int
+rtkb_fdk_backproject_batch(const rtkb_bp_problem * problems, int n, int config, int * used_config, void * stream)
+{
+  try
+  {
+    return rtkb::backproject_batch(problems, n, true, config, used_config, static_cast<cudaStream_t>(stream));
+  }
+  catch (...)
+  {
+    return rtkb::fail(RTKB_ERR_OUT_OF_MEMORY, "host allocation failed");
+  }
+}
+
+extern "C" int
+rtkb_voxel_backproject_batch(const rtkb_bp_problem * problems, int n, int config, int * used_config, void * stream)
+{
+  try
+  {
+    return rtkb::backproject_batch(problems, n, false, config, used_config, static_cast<cudaStream_t>(stream));
+  }
+  catch (...)
+  {
+    return rtkb::fail(RTKB_ERR_OUT_OF_MEMORY, "host allocation failed");
+  }
+}
+
+extern "C" int
+rtkb_bp_batch_create(const rtkb_bp_problem * problems, int n, int fdk, int config, rtkb_bp_batch ** batch)
+{
+  try
+  {
+    return rtkb::create_batch(problems, n, fdk != 0, config, batch);
+  }
+  catch (...)
+  {
+    return rtkb::fail(RTKB_ERR_OUT_OF_MEMORY, "host allocation failed");
+  }
+}
+
+extern "C" int
+rtkb_bp_batch_execute(rtkb_bp_batch * batch, void * stream)
+{
+  return rtkb::execute_batch(batch, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int
+rtkb_bp_batch_config(const rtkb_bp_batch * batch)
+{
+  return batch ? batch->cfg : -1;
+}
+
+extern "C" void
+rtkb_bp_batch_destroy(rtkb_bp_batch * batch)
+{
+  rtkb::release_batch(batch);
+}
+
+extern "C" int
+rtkb_backproject_autotune(const rtkb_bp_problem * problems, int n, int fdk, int repeats, int * best_config,
+                          double * best_ms, double * config_ms, void * stream)
+{
+  using namespace rtkb;
+  if (!problems || n <= 0 || !best_config)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "null argument");
+  for (int i = 0; i < n; i++)
+    if (problems[i].d_vol_in == problems[i].d_vol_out)
+      return fail(RTKB_ERR_INVALID_ARGUMENT, "autotuning runs the batch repeatedly: d_vol_out must not alias d_vol_in");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaEvent_t  e0 = nullptr, e1 = nullptr;
+  RTKB_CUDA_TRY(cudaEventCreate(&e0));
+  RTKB_CUDA_TRY(cudaEventCreate(&e1));
+  int    best = -1, rc = RTKB_OK;
+  double best_t = 1e300;
+  const int saved_force = g_bp_forced_config;
+  for (int c = 0; c < kNumBpConfigs && rc == RTKB_OK; c++)
+  {
+    // one problem: time the single-problem kernel its own calls run (with the
+    // configuration forced); several: a prepared persistent batch
+    rtkb_bp_batch * B = nullptr;
+    if (n > 1)
+    {
+      rc = create_batch(problems, n, fdk != 0, c, &B);
+      if (rc != RTKB_OK)
+        break;
+    }
+    g_bp_forced_config = c;
+    const rtkb_bp_problem & P0 = problems[0];
+    auto run = [&]() {
+      return n > 1 ? execute_batch(B, st)
+                   : backproject_geometry(P0.geometry, &P0.vol, &P0.proj, P0.d_proj, P0.d_vol_in, P0.d_vol_out, stream,
+                                          fdk != 0);
+    };
+    rc = run(); // warm-up
+    cudaError_t e = cudaEventRecord(e0, st);
+    for (int r = 0; r < std::max(repeats, 1) && rc == RTKB_OK && e == cudaSuccess; r++)
+      rc = run();
+    if (e == cudaSuccess)
+      e = cudaEventRecord(e1, st);
+    if (e == cudaSuccess)
+      e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (e == cudaSuccess)
+      e = cudaEventElapsedTime(&ms, e0, e1);
+    if (e != cudaSuccess && rc == RTKB_OK)
+      rc = cuda_fail(e, "autotune timing");
+    release_batch(B);
+    g_bp_forced_config = saved_force;
+    const double t = ms / std::max(repeats, 1);
+    if (config_ms)
+      config_ms[c] = t;
+    if (rc == RTKB_OK && t < best_t)
+    {
+      best_t = t;
+      best = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc != RTKB_OK)
+    return rc;
+  *best_config = best;
+  if (best_ms)
+    *best_ms = best_t;
+  return RTKB_OK;
 }
 
 extern "C" int

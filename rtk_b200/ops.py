@@ -334,3 +334,86 @@ def project_ellipsoids(geometry, proj_desc, ellipsoids, out=None, stream=None):
     check(load().rtkb_project_ellipsoids(geometry.handle, C.byref(proj_desc), e.shape[0],
                                          e.ctypes.data_as(C.POINTER(C.c_double)), _ptr(out), _stream(stream)))
     return out
+
+
+def _problem_array(problems):
+    from ._capi import BpProblem
+
+    torch = _torch()
+    arr = (BpProblem * len(problems))()
+    keep = []
+    for k, (geometry, vol_desc, proj_desc, proj, vol_in, out) in enumerate(problems):
+        _check_shape(proj, proj_desc, "projections")
+        _check_shape(vol_in, vol_desc, "volume")
+        _check_shape(out, vol_desc, "output")
+        arr[k].geometry = geometry.handle
+        arr[k].vol = vol_desc
+        arr[k].proj = proj_desc
+        arr[k].d_proj = _ptr(proj).value
+        arr[k].d_vol_in = _ptr(vol_in).value
+        arr[k].d_vol_out = _ptr(out).value
+        keep.append((proj, vol_in, out))
+    return arr, keep
+
+
+def backproject_batch(problems, fdk=True, config=-1, stream=None):
+    """Batched FDK (or voxel) backprojection of independent problems in one
+    persistent launch.  problems: [(geometry, vol_desc, proj_desc, proj,
+    vol_in, out)], float32 CUDA tensors.  Returns the configuration used."""
+    arr, _ = _problem_array(problems)
+    used = C.c_int(-1)
+    L = load()
+    fn = L.rtkb_fdk_backproject_batch if fdk else L.rtkb_voxel_backproject_batch
+    check(fn(arr, len(problems), int(config), C.byref(used), _stream(stream)))
+    return used.value
+
+
+def backproject_autotune(problems, fdk=True, repeats=2, stream=None):
+    """The project's autotuner: times every backprojector configuration on the
+    batch and returns (best configuration, its ms, [ms per configuration])."""
+    arr, _ = _problem_array(problems)
+    times = (C.c_double * 16)(*([-1.0] * 16))  # one entry per configuration (fewer than 16)
+    best, best_ms = C.c_int(), C.c_double()
+    check(load().rtkb_backproject_autotune(arr, len(problems), int(fdk), int(repeats), C.byref(best),
+                                           C.byref(best_ms), times, _stream(stream)))
+    return best.value, best_ms.value, [t for t in times if t >= 0.0]
+
+
+class BackprojectionBatch:
+    """Prepared batch (rtkb_bp_batch_*): host work done once, each execute()
+    is one persistent launch over all problems.  The tensors of `problems`
+    are kept alive with the batch."""
+
+    def __init__(self, problems, fdk=True, config=-1):
+        self._lib = load()
+        arr, self._keep = _problem_array(problems)
+        h = C.c_void_p()
+        check(self._lib.rtkb_bp_batch_create(arr, len(problems), int(fdk), int(config), C.byref(h)))
+        self._h = h
+        self.config = self._lib.rtkb_bp_batch_config(h)
+
+    def execute(self, stream=None):
+        check(self._lib.rtkb_bp_batch_execute(self._h, _stream(stream)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            torch = _torch()
+            torch.cuda.synchronize()
+            self._lib.rtkb_bp_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def backproject_config(force=-1):
+    """Autotuner hook of the tiled backprojector (rtkb_backproject_config):
+    force >= 0 selects that configuration for later calls on this host thread,
+    -1 restores the footprint heuristic.  Returns (configuration of the last
+    tiled launch on this thread or -1, number of configurations)."""
+    last, count = C.c_int(), C.c_int()
+    check(load().rtkb_backproject_config(int(force), C.byref(last), C.byref(count)))
+    return last.value, count.value

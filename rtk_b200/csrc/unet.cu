@@ -31,6 +31,7 @@
 // concatenation of the decoder inputs are folded into the halo loader, the
 // ReLU-derivative mask into the data-gradient epilogue.
 #include "rtkb_internal.h"
+#include "rtkb_ptx.cuh"
 
 #include <cuda_bf16.h>
 
@@ -270,6 +271,224 @@ conv_fwd_kernel(ConvIn in, const bf16 * __restrict__ wpack, Dims d, bf16 * __res
       }
     }
   }
+}
+
+// ---- forward / data-gradient convolution on the 5th-generation tensor cores ------------------------
+// tcgen05.mma (kind::f16: BF16 x BF16 -> FP32 in tensor memory), operands in
+// shared memory described by matrix descriptors (K-major, no swizzle).  A CTA
+// (one warpgroup) owns an 8 (x) x 16 (y) x 4 (z) output tile: four M = 128
+// accumulators (one per z-slice, 8 x-voxels x 16 y-rows), N = output channels.
+// Per 16-channel input chunk the 10 x 18 x 6 halo is stored as
+// [k-half][voxel][8 channels], so the A operand of tap (dz, dy, dx) and slice
+// z is a descriptor starting at that tap's first halo voxel with 8-row groups
+// one halo row (10 voxels = 160 bytes) apart; weights are packed as
+// [tap][k-half][c_out][8 c_in].  One thread issues the 27 x 4 MMAs of a chunk
+// and commits them to an mbarrier; the epilogue reads the accumulators with
+// tcgen05.ld, applies ReLU or the gradient mask and stores BF16.
+constexpr int kCX = 8, kCY = 16, kCZ = 4;                   // output tile
+constexpr int kCHX = kCX + 2, kCHY = kCY + 2, kCHZ = kCZ + 2; // halo
+constexpr int kCHalo = kCHX * kCHY * kCHZ;                   // 1080 voxels
+constexpr int kCHaloBytes = kCHalo * 32;
+
+struct TcDims
+{
+  int nx, ny, nz, batch, tx, ty, tz;
+};
+
+TcDims
+make_tc_dims(int nx, int ny, int nz, int batch)
+{
+  TcDims d{ nx, ny, nz, batch, (nx + kCX - 1) / kCX, (ny + kCY - 1) / kCY, (nz + kCZ - 1) / kCZ };
+  return d;
+}
+
+__device__ __forceinline__ uint64_t
+umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+{
+  // start address, leading and stride byte offsets (all >> 4), version 1 (sm_100), no swizzle
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+template <int N>
+__device__ __forceinline__ constexpr uint32_t
+umma_idesc_bf16()
+{
+  // FP32 accumulator, BF16 A and B, both K-major, N >> 3, M = 128 >> 4
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+
+__device__ __forceinline__ void
+umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accumulate)
+{
+  asm volatile("{\n\t.reg .pred p;\n\t"
+               "setp.ne.b32 p, %4, 0;\n\t"
+               "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+               :
+               : "r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void
+umma_commit(uint64_t * bar)
+{
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+               ::"r"(rtkb::dev::smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void
+tmem_ld16(uint32_t taddr, uint32_t (&r)[16])
+{
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                 "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                 "=r"(r[15])
+               : "r"(taddr));
+}
+
+template <int N>
+__global__ void __launch_bounds__(128, 1)
+conv_fwd_tc_kernel(ConvIn in, const bf16 * __restrict__ wpack, TcDims d, bf16 * __restrict__ out,
+                   const bf16 * __restrict__ mask, int relu)
+{
+  constexpr int      kCols = (kCZ * N <= 32) ? 32 : (kCZ * N <= 64) ? 64 : (kCZ * N <= 128) ? 128 : (kCZ * N <= 256) ? 256 : 512;
+  constexpr uint32_t kIdesc = umma_idesc_bf16<N>();
+  extern __shared__ __align__(128) char smem[];
+  char *             halo = smem;                              // [2][kCHalo][16 B]
+  char *             wsm = smem + kCHaloBytes;                 // [27][2][N][16 B]
+  uint64_t *         bar = reinterpret_cast<uint64_t *>(wsm + 27 * 2 * N * 16);
+  uint32_t *         tmem_slot = reinterpret_cast<uint32_t *>(bar + 1);
+  const int          warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  long long          tile = blockIdx.x;
+  const int          tx = (int)(tile % d.tx);
+  tile /= d.tx;
+  const int ty = (int)(tile % d.ty);
+  tile /= d.ty;
+  const int tz = (int)(tile % d.tz);
+  const int n = (int)(tile / d.tz);
+  const int x0 = tx * kCX, y0 = ty * kCY, z0 = tz * kCZ;
+
+  if (warp == 0)
+  {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(rtkb::dev::smem_u32(tmem_slot)),
+                 "r"((uint32_t)kCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (threadIdx.x == 0)
+  {
+    rtkb::dev::mbar_init(bar, 1);
+    rtkb::dev::fence_barrier_init();
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = *tmem_slot;
+  const int      nchunks = (in.ca + in.cb) / 16;
+  const uint32_t halo_s = rtkb::dev::smem_u32(halo), w_s = rtkb::dev::smem_u32(wsm);
+  bool           ok = true;
+
+  for (int chunk = 0; chunk < nchunks && ok; chunk++)
+  {
+    // halo chunk: 16 channels of the 10 x 18 x 6 neighbourhood, [k-half][voxel][16 B], zero outside
+    {
+      const bool   from_a = chunk * 16 < in.ca;
+      const int    cs = from_a ? in.ca : in.cb;
+      const int    c0 = from_a ? chunk * 16 : chunk * 16 - in.ca;
+      const bf16 * src = from_a ? in.a : in.b;
+      const bool   half = from_a && in.a_half;
+      const int    snx = half ? d.nx >> 1 : d.nx, sny = half ? d.ny >> 1 : d.ny, snz = half ? d.nz >> 1 : d.nz;
+      for (int i = threadIdx.x; i < kCHalo * 2; i += 128)
+      {
+        const int hv = i >> 1, h = i & 1;
+        const int hx = hv % kCHX, hy = (hv / kCHX) % kCHY, hz = hv / (kCHX * kCHY);
+        const int gx = x0 - 1 + hx, gy = y0 - 1 + hy, gz = z0 - 1 + hz;
+        uint4     v = make_uint4(0u, 0u, 0u, 0u);
+        if (gx >= 0 && gx < d.nx && gy >= 0 && gy < d.ny && gz >= 0 && gz < d.nz)
+        {
+          const int sx = half ? gx >> 1 : gx, sy = half ? gy >> 1 : gy, sz = half ? gz >> 1 : gz;
+          v = *reinterpret_cast<const uint4 *>(src + ((((long long)n * snz + sz) * sny + sy) * snx + sx) * cs + c0 + h * 8);
+        }
+        *reinterpret_cast<uint4 *>(halo + (h * kCHalo + hv) * 16) = v;
+      }
+      const uint4 * wsrc = reinterpret_cast<const uint4 *>(wpack + (size_t)chunk * 27 * 2 * N * 8);
+      uint4 *       wdst = reinterpret_cast<uint4 *>(wsm);
+      for (int i = threadIdx.x; i < 27 * 2 * N; i += 128)
+        wdst[i] = wsrc[i];
+    }
+    // make the generic-proxy stores visible to the tensor cores, then issue
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+      asm volatile("tcgen05.fence::after_thread_sync;");
+#pragma unroll 1
+      for (int t = 0; t < 27; t++)
+      {
+        const int      dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
+        const uint64_t db = umma_desc(w_s + (uint32_t)(t * 2 * N * 16), (uint32_t)(N * 16), 128u);
+#pragma unroll
+        for (int zl = 0; zl < kCZ; zl++)
+        {
+          const int      hv0 = ((zl + dz) * kCHY + dy) * kCHX + dx;
+          const uint64_t da = umma_desc(halo_s + (uint32_t)(hv0 * 16), (uint32_t)(kCHalo * 16), (uint32_t)(kCHX * 16));
+          umma_bf16(tmem + (uint32_t)(zl * N), da, db, kIdesc, (chunk > 0 || t > 0) ? 1u : 0u);
+        }
+      }
+      umma_commit(bar);
+    }
+    // the MMAs read shared memory asynchronously: wait before it is overwritten
+    // (a wait that gave up stops every thread: the loop stays CTA-uniform)
+    ok = __syncthreads_and(rtkb::dev::mbar_wait(bar, (uint32_t)(chunk & 1)) ? 1 : 0) != 0;
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;");
+
+  // epilogue: warp w reads TMEM lanes 32w..32w+31 = output rows m (x = m % 8, y = m / 8)
+  if (ok)
+  {
+    const int m = warp * 32 + lane;
+    const int x = x0 + (m & 7), y = y0 + (m >> 3);
+#pragma unroll 1
+    for (int zl = 0; zl < kCZ; zl++)
+    {
+      const int  z = z0 + zl;
+      const bool inside = x < d.nx && y < d.ny && z < d.nz;
+      const long long vbase = ((((long long)n * d.nz + z) * d.ny + y) * d.nx + x) * N;
+#pragma unroll
+      for (int cb = 0; cb < N; cb += 16)
+      {
+        uint32_t r[16];
+        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(zl * N + cb), r);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (!inside)
+          continue;
+        unsigned o[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++)
+        {
+          float v0 = __uint_as_float(r[2 * q]), v1 = __uint_as_float(r[2 * q + 1]);
+          if (relu)
+          {
+            v0 = fmaxf(v0, 0.f);
+            v1 = fmaxf(v1, 0.f);
+          }
+          if (mask)
+          {
+            const float2 mk = unpack_bf16x2(*reinterpret_cast<const unsigned *>(mask + vbase + cb + 2 * q));
+            v0 = mk.x > 0.f ? v0 : 0.f;
+            v1 = mk.y > 0.f ? v1 : 0.f;
+          }
+          o[q] = pack_bf16x2(v0, v1);
+        }
+        uint4 * dst = reinterpret_cast<uint4 *>(out + vbase + cb);
+        dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
+        dst[1] = make_uint4(o[4], o[5], o[6], o[7]);
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)kCols));
 }
 
 // ---- weight gradient --------------------------------------------------------------------------------
@@ -679,25 +898,24 @@ skip_grad_kernel(const bf16 * __restrict__ cat, int ccat, int ca, const bf16 * _
 }
 
 // ---- weights: packing, Adam ------------------------------------------------------------------------------
-// Forward pack: wp[c][t][co][slot], slot = ((ci%16)/8 ^ (co>>2)&1)*8 + ci%8.
-// Data-gradient pack (input channels = co, output channels = ci, taps
-// mirrored): wd[c'][t][ci][slot], value W[26 - t][ci][co], c' = co / 16,
-// slot = ((co%16)/8 ^ (ci>>2)&1)*8 + co%8.
+// Forward pack for the tensor-core kernel: wf[c][t][h][co][8] = W[t][16c + 8h + j][co]
+// (input chunk c, k-half h, j < 8).  Data-gradient pack (input channels = co,
+// output channels = ci, taps mirrored): wd[c'][t][h][ci][8] = W[26 - t][ci][16c' + 8h + j].
 __global__ void
 pack_kernel(const float * __restrict__ W, int cin, int cout, bf16 * __restrict__ wf, bf16 * __restrict__ wd)
 {
   const int n = 27 * cin * cout;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
   {
-    const int co = i % cout, ci = (i / cout) % cin, t = i / (cout * cin);
+    const int  co = i % cout, ci = (i / cout) % cin, t = i / (cout * cin);
     const bf16 w = __float2bfloat16_rn(W[i]);
     {
-      const int c = ci >> 4, k = ci & 15, slot = (((k >> 3) ^ ((co >> 2) & 1)) << 3) | (k & 7);
-      wf[(((size_t)c * 27 + t) * cout + co) * 16 + slot] = w;
+      const int c = ci >> 4, h = (ci >> 3) & 1, j = ci & 7;
+      wf[((((size_t)c * 27 + t) * 2 + h) * cout + co) * 8 + j] = w;
     }
     {
-      const int c = co >> 4, k = co & 15, slot = (((k >> 3) ^ ((ci >> 2) & 1)) << 3) | (k & 7);
-      wd[(((size_t)c * 27 + (26 - t)) * cin + ci) * 16 + slot] = w;
+      const int c = co >> 4, h = (co >> 3) & 1, j = co & 7;
+      wd[((((size_t)c * 27 + (26 - t)) * 2 + h) * cin + ci) * 8 + j] = w;
     }
   }
 }
@@ -780,20 +998,21 @@ layer_params(int l)
   return l == 10 ? 16 : 27LL * kLayers[l].cin * kLayers[l].cout;
 }
 
-template <int NT>
+template <int N>
 void
-conv_fwd_launch(const ConvIn & in, const bf16 * wp, const Dims & d, bf16 * out, const bf16 * mask, int relu,
-                cudaStream_t st)
+conv_fwd_tc_launch(const ConvIn & in, const bf16 * wp, const Dims & d0, bf16 * out, const bf16 * mask, int relu,
+                   cudaStream_t st)
 {
-  const int smem = kHaloBytes + 27 * NT * 8 * 32;
+  const int smem = kCHaloBytes + 27 * 2 * N * 16 + 16;
   static bool configured = false; // attribute set once per process (same value on every device)
   if (!configured)
   {
-    cudaFuncSetAttribute(conv_fwd_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(conv_fwd_tc_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     configured = true;
   }
+  const TcDims    d = make_tc_dims(d0.nx, d0.ny, d0.nz, d0.batch);
   const long long tiles = (long long)d.tx * d.ty * d.tz * d.batch;
-  conv_fwd_kernel<NT><<<(unsigned)tiles, kThreads, smem, st>>>(in, wp, d, out, mask, relu);
+  conv_fwd_tc_kernel<N><<<(unsigned)tiles, 128, smem, st>>>(in, wp, d, out, mask, relu);
 }
 
 template <int NT>
@@ -819,11 +1038,11 @@ conv_fwd(int cout, const ConvIn & in, const bf16 * wp, const Dims & d, bf16 * ou
 {
   switch (cout)
   {
-  case 16: conv_fwd_launch<2>(in, wp, d, out, mask, relu, st); break;
-  case 32: conv_fwd_launch<4>(in, wp, d, out, mask, relu, st); break;
-  case 48: conv_fwd_launch<6>(in, wp, d, out, mask, relu, st); break;
-  case 64: conv_fwd_launch<8>(in, wp, d, out, mask, relu, st); break;
-  default: conv_fwd_launch<12>(in, wp, d, out, mask, relu, st); break;
+  case 16: conv_fwd_tc_launch<16>(in, wp, d, out, mask, relu, st); break;
+  case 32: conv_fwd_tc_launch<32>(in, wp, d, out, mask, relu, st); break;
+  case 48: conv_fwd_tc_launch<48>(in, wp, d, out, mask, relu, st); break;
+  case 64: conv_fwd_tc_launch<64>(in, wp, d, out, mask, relu, st); break;
+  default: conv_fwd_tc_launch<96>(in, wp, d, out, mask, relu, st); break;
   }
 }
 

@@ -25,11 +25,13 @@
 // correlation as torch.nn.functional.conv3d with padding 1) and repacked to
 // BF16 after every update.
 //
-// Tensor-core kernels use mma.sync m16n8k16 (BF16 in, FP32 accumulate) with
-// ldmatrix gathers: implicit GEMM with M = voxels of a 16x4x4 output tile,
-// N = output channels, K = 27 taps x 16-channel input chunks.  Up-sampling and
-// concatenation of the decoder inputs are folded into the halo loader, the
-// ReLU-derivative mask into the data-gradient epilogue.
+// The forward and data-gradient convolutions run on tcgen05 (implicit GEMM:
+// M = voxels of an 8x16x4 output tile as four M = 128 accumulators in tensor
+// memory, N = output channels, K = 27 taps x 16-channel input chunks, operands
+// from shared-memory descriptors); the weight gradient uses mma.sync m16n8k16
+// with ldmatrix gathers.  Up-sampling and concatenation of the decoder inputs
+// are folded into the halo loaders, the ReLU-derivative mask into the
+// data-gradient epilogue.
 #include "rtkb_internal.h"
 #include "rtkb_ptx.cuh"
 
@@ -55,14 +57,6 @@ __device__ __forceinline__ unsigned
 smem_u32(const void * p)
 {
   return static_cast<unsigned>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void
-ldsm_x4(unsigned addr, unsigned & r0, unsigned & r1, unsigned & r2, unsigned & r3)
-{
-  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
-               : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
-               : "r"(addr));
 }
 
 __device__ __forceinline__ void
@@ -160,116 +154,6 @@ load_halo(char * halo, const ConvIn & in, const Dims & d, int n, int x0, int y0,
       v = *reinterpret_cast<const uint4 *>(src + off);
     }
     *reinterpret_cast<uint4 *>(halo + hv * 32 + ((h ^ ((hv >> 2) & 1)) << 4)) = v;
-  }
-}
-
-// ---- forward / data-gradient convolution ------------------------------------------------------------
-// out[v][co] = act( sum_t sum_ci in[v + t - 1][ci] * W[t][ci][co] ), co < 8*NT.
-// Weights arrive packed per 16-channel input chunk: [chunk][27][co][16] BF16
-// with the 16-byte halves swapped when bit 2 of co is set.  mask (optional):
-// out *= (mask > 0) (the ReLU derivative of the layer that produced the
-// gradient); relu: out = max(out, 0).
-template <int NT>
-__global__ void __launch_bounds__(kThreads, NT > 8 ? 1 : 2)
-conv_fwd_kernel(ConvIn in, const bf16 * __restrict__ wpack, Dims d, bf16 * __restrict__ out,
-                const bf16 * __restrict__ mask, int relu)
-{
-  constexpr int COUT = NT * 8;
-  extern __shared__ __align__(128) char smem[];
-  char *        halo = smem;
-  char *        wsm = smem + kHaloBytes;
-  const int     lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int           n, x0, y0, z0;
-  tile_origin(d, blockIdx.x, n, x0, y0, z0);
-  const int nchunks = (in.ca + in.cb) / 16;
-
-  float acc[2][NT][4];
-#pragma unroll
-  for (int m = 0; m < 2; m++)
-#pragma unroll
-    for (int j = 0; j < NT; j++)
-#pragma unroll
-      for (int k = 0; k < 4; k++)
-        acc[m][j][k] = 0.f;
-
-  // lane roles in ldmatrix: A rows (voxels along x) and halves, B rows (co)
-  const int a_row = (lane & 7) + ((lane >> 3) & 1) * 8, a_half = lane >> 4;
-  const int b_co = (lane & 7) + (lane >> 4) * 8, b_half = (lane >> 3) & 1;
-  const unsigned halo_s = smem_u32(halo), w_s = smem_u32(wsm);
-
-  for (int chunk = 0; chunk < nchunks; chunk++)
-  {
-    __syncthreads();
-    load_halo(halo, in, d, n, x0, y0, z0, chunk);
-    {
-      const uint4 * src = reinterpret_cast<const uint4 *>(wpack + (size_t)chunk * 27 * COUT * 16);
-      uint4 *       dst = reinterpret_cast<uint4 *>(wsm);
-      for (int i = threadIdx.x; i < 27 * COUT * 2; i += kThreads)
-        dst[i] = src[i];
-    }
-    __syncthreads();
-#pragma unroll 1
-    for (int t = 0; t < 27; t++)
-    {
-      const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
-      unsigned  a[2][4];
-#pragma unroll
-      for (int m = 0; m < 2; m++)
-      {
-        const int q = warp * 2 + m, zl = q >> 2, yl = q & 3;
-        const int hv = ((zl + dz) * kHY + (yl + dy)) * kHX + dx + a_row;
-        ldsm_x4(halo_s + hv * 32 + ((a_half ^ ((hv >> 2) & 1)) << 4), a[m][0], a[m][1], a[m][2], a[m][3]);
-      }
-#pragma unroll
-      for (int jp = 0; jp < NT / 2; jp++)
-      {
-        const int co = jp * 16 + b_co;
-        unsigned  b0, b1, b2, b3;
-        ldsm_x4(w_s + (t * COUT + co) * 32 + ((b_half ^ ((co >> 2) & 1)) << 4), b0, b1, b2, b3);
-#pragma unroll
-        for (int m = 0; m < 2; m++)
-        {
-          mma_bf16(acc[m][2 * jp], a[m][0], a[m][1], a[m][2], a[m][3], b0, b1);
-          mma_bf16(acc[m][2 * jp + 1], a[m][0], a[m][1], a[m][2], a[m][3], b2, b3);
-        }
-      }
-    }
-  }
-
-  // epilogue: c0,c1 at (row lane/4, co 2*(lane%4)), c2,c3 at row + 8
-#pragma unroll
-  for (int m = 0; m < 2; m++)
-  {
-    const int q = warp * 2 + m, zl = q >> 2, yl = q & 3;
-    const int y = y0 + yl, z = z0 + zl;
-    if (y >= d.ny || z >= d.nz)
-      continue;
-#pragma unroll
-    for (int hr = 0; hr < 2; hr++)
-    {
-      const int x = x0 + (lane >> 2) + hr * 8;
-      if (x >= d.nx)
-        continue;
-      const long long vbase = ((((long long)n * d.nz + z) * d.ny + y) * d.nx + x) * COUT;
-#pragma unroll
-      for (int j = 0; j < NT; j++)
-      {
-        const int co = j * 8 + (lane & 3) * 2;
-        float     v0 = acc[m][j][hr * 2], v1 = acc[m][j][hr * 2 + 1];
-        if (relu)
-        {
-          v0 = fmaxf(v0, 0.f);
-          v1 = fmaxf(v1, 0.f);
-        }
-        if (mask)
-        {
-          const float2 mk = unpack_bf16x2(*reinterpret_cast<const unsigned *>(mask + vbase + co));
-          v0 = mk.x > 0.f ? v0 : 0.f;
-          v1 = mk.y > 0.f ? v1 : 0.f;
-        }
-        *reinterpret_cast<unsigned *>(out + vbase + co) = pack_bf16x2(v0, v1);
-      }
-    }
   }
 }
 

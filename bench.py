@@ -528,6 +528,30 @@ def profile_cg():
     return 0
 
 
+def profile_fdk():
+    """FDK preprocessing of the projector-pair stack (720 x 1024x768), twice:
+    target of ncu captures of the fused weighting + ramp-filter kernel."""
+    import torch
+
+    import rtk_b200 as rtkb
+
+    rtkb.load()
+    g = make_geometry()
+    pd = rtkb.make_desc((NU, NV, NP), (PIX, PIX, 1.0))
+    p = torch.rand((NP, NV, NU), device="cuda", generator=torch.Generator(device="cuda").manual_seed(SEED))
+    rp = rtkb.ops.ramp_params(hann=1.0)
+    rtkb.ops.fdk_preprocess(g, pd, p, rp)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    rtkb.ops.fdk_preprocess(g, pd, p, rp)
+    e1.record()
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_fdk": {"preprocess_ms": e0.elapsed_time(e1),
+                                      "workload": "weights + Hann ramp of 720 x 768 rows of 1024 (padded 2048)"}}))
+    return 0
+
+
 def use_profile_case():
     """256^3 at 0.5 mm (the benchmark's voxel size, so the same tile
     footprints and kernel configuration) from 360 of the 1024x768 projections:
@@ -551,11 +575,15 @@ def main():
     ap.add_argument("--profile-cg", action="store_true",
                     help="run the CG configuration's kernels once each for ncu captures (256^3, 360 x 512x384): CG "
                          "start + 2 eager iterations, one U-Net forward on the volume, one training step on 4 x 64^3")
+    ap.add_argument("--profile-fdk", action="store_true",
+                    help="FDK preprocessing (weights + Hann ramp filter) of the 720 x 1024x768 stack, twice, for ncu")
     ap.add_argument("--profile-case", action="store_true",
                     help="small case for ncu captures: 256^3 @1mm from 360 projections, device-timed region only")
     args = ap.parse_args()
     if args.profile_cg:
         return profile_cg()
+    if args.profile_fdk:
+        return profile_fdk()
     args.warmup = max(args.warmup, 3)
     if args.profile_case:
         use_profile_case()

@@ -36,8 +36,41 @@ struct FilterArgs
   int            nu_in, nu_out, nv, np, shift, N, next;
 };
 
+// Per-row part of the weights: FDK cos(gamma) terms for row r of projection s
+// (include/rtkFDKWeightProjectionFilter.hxx:67-128; parameters from the FP64
+// host table), evaluated per pixel in FP32 (relative error ~1e-7).
+struct RowWeight
+{
+  float f, num1, sina, sddtana, e, xc0, dxc;
+  int   mode; // 0: none, 1: constant (parallel), 2: cos(gamma)
+};
+
+__device__ __forceinline__ RowWeight
+row_weight(const FilterArgs & a, int s, int r)
+{
+  RowWeight w{ 1.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0 };
+  if (!a.fdkp)
+    return w;
+  const double * q = a.fdkp + (long long)s * rtkb::kFdkWeightParams;
+  w.f = (float)q[0];
+  if (q[7] != 0.)
+  {
+    w.mode = 1;
+    return w;
+  }
+  const double y = q[6] + r * q[9];
+  w.mode = 2;
+  w.num1 = (float)q[1];
+  w.sina = (float)q[2];
+  w.sddtana = (float)q[3];
+  w.e = (float)(q[4] + y * y);
+  w.xc0 = (float)q[5];
+  w.dxc = (float)q[8];
+  return w;
+}
+
 __device__ __forceinline__ float
-weighted_pixel(const FilterArgs & a, int s, int r, int c)
+weighted_pixel(const FilterArgs & a, const RowWeight & w, int s, int r, int c)
 {
   const int ci = c - a.shift;
   if (ci < 0 || ci >= a.nu_in)
@@ -45,32 +78,33 @@ weighted_pixel(const FilterArgs & a, int s, int r, int c)
   float v = __ldg(a.in + ((long long)s * a.nv + r) * a.nu_in + ci);
   if (a.colw)
     v *= __ldg(a.colw + (long long)s * a.nu_out + c);
-  if (a.fdkp)
+  if (w.mode == 1)
+    v *= w.f;
+  else if (w.mode == 2)
   {
-    const double * q = a.fdkp + (long long)s * rtkb::kFdkWeightParams;
-    double         w = q[0];
-    if (q[7] == 0.)
-    {
-      const double x = q[5] + c * q[8], y = q[6] + r * q[9];
-      const double dxs = x - q[3];
-      w *= (q[1] - x * q[2]) / sqrt(q[4] + y * y + dxs * dxs);
-    }
-    v = (float)(v * w);
+    const float x = fmaf((float)c, w.dxc, w.xc0), dxs = x - w.sddtana;
+    v *= w.f * (w.num1 - x * w.sina) * rsqrtf(fmaf(dxs, dxs, w.e));
   }
   return v;
 }
 
+// grid: (column blocks, rows, projections)
 __global__ void __launch_bounds__(256)
 weight_kernel(FilterArgs a)
 {
-  const long long n = (long long)a.nu_out * a.nv * a.np;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-  {
-    const int c = (int)(i % a.nu_out);
-    const int r = (int)((i / a.nu_out) % a.nv);
-    const int s = (int)(i / ((long long)a.nu_out * a.nv));
-    a.out[i] = weighted_pixel(a, s, r, c);
-  }
+  const int       r = blockIdx.y, s = blockIdx.z;
+  const RowWeight w = row_weight(a, s, r);
+  float *         o = a.out + ((long long)s * a.nv + r) * a.nu_out;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < a.nu_out; c += gridDim.x * blockDim.x)
+    o[c] = weighted_pixel(a, w, s, r, c);
+}
+
+// Shared-memory index with one pad element after every 8: the stride-R writes
+// of the early Stockham passes (R = 8, 4) then spread over all banks.
+__device__ __forceinline__ int
+pidx(int x)
+{
+  return x + (x >> 3);
 }
 
 __device__ __forceinline__ float2
@@ -143,7 +177,7 @@ fft_pass(const float2 * __restrict__ src, float2 * __restrict__ dst, const float
     float2    v[R];
 #pragma unroll
     for (int r = 0; r < R; r++)
-      v[r] = src[j + r * nb];
+      v[r] = src[pidx(j + r * nb)];
     if (Ns > 1)
     {
 #pragma unroll
@@ -154,7 +188,7 @@ fft_pass(const float2 * __restrict__ src, float2 * __restrict__ dst, const float
     const int d = (j - k) * R + k;
 #pragma unroll
     for (int r = 0; r < R; r++)
-      dst[d + r * Ns] = v[r];
+      dst[pidx(d + r * Ns)] = v[r];
   }
 }
 
@@ -196,34 +230,37 @@ ramp_fft_kernel(FilterArgs a)
 {
   extern __shared__ float2 sbuf[];
   float2 *  b0 = sbuf;
-  float2 *  b1 = sbuf + a.N;
+  float2 *  b1 = sbuf + pidx(a.N);
   const int rows = a.nv * a.np;
   const int ra = 2 * blockIdx.x, rb = ra + 1;
   const int N = a.N, nu = a.nu_out;
   // load two weighted rows as one complex sequence, zero padded
+  const int       sa = ra / a.nv, rra = ra % a.nv, sb = rb / a.nv, rrb = rb % a.nv;
+  const RowWeight wa = row_weight(a, sa, rra);
+  const RowWeight wb = rb < rows ? row_weight(a, sb, rrb) : wa;
   for (int c = threadIdx.x; c < N; c += blockDim.x)
   {
     float x = 0.f, y = 0.f;
     if (c < nu)
     {
-      x = weighted_pixel(a, ra / a.nv, ra % a.nv, c);
+      x = weighted_pixel(a, wa, sa, rra, c);
       if (rb < rows)
-        y = weighted_pixel(a, rb / a.nv, rb % a.nv, c);
+        y = weighted_pixel(a, wb, sb, rrb, c);
     }
-    b0[c] = make_float2(x, y);
+    b0[pidx(c)] = make_float2(x, y);
   }
   __syncthreads();
   if (a.next > 0)
   {
     // Ohnesorge mirror extrapolation (PadInputImageRegion :218-258): left
     // values wrap to the end of the circular buffer.
-    const float2 SA = b0[1], SE = b0[nu - 1];
+    const float2 SA = b0[pidx(1)], SE = b0[pidx(nu - 1)];
     for (int bq = 1 + threadIdx.x; bq <= a.next; bq += blockDim.x)
     {
       const float  w = __ldg(a.mw + bq);
-      const float2 l = b0[bq], r = b0[nu - 1 - bq];
-      b0[N - bq] = make_float2(w * (2.f * SA.x - l.x), w * (2.f * SA.y - l.y));
-      b0[nu - 1 + bq] = make_float2(w * (2.f * SE.x - r.x), w * (2.f * SE.y - r.y));
+      const float2 l = b0[pidx(bq)], r = b0[pidx(nu - 1 - bq)];
+      b0[pidx(N - bq)] = make_float2(w * (2.f * SA.x - l.x), w * (2.f * SA.y - l.y));
+      b0[pidx(nu - 1 + bq)] = make_float2(w * (2.f * SE.x - r.x), w * (2.f * SE.y - r.y));
     }
     __syncthreads();
   }
@@ -234,15 +271,15 @@ ramp_fft_kernel(FilterArgs a)
   for (int f = threadIdx.x; f < N; f += blockDim.x)
   {
     const float  k = __ldg(a.K + min(f, N - f));
-    const float2 z = X[f];
-    X[f] = make_float2(z.x * k, -z.y * k);
+    const float2 z = X[pidx(f)];
+    X[pidx(f)] = make_float2(z.x * k, -z.y * k);
   }
   __syncthreads();
   float2 *    W = fft_forward(X, other, a.tw, N);
   const float inv = 1.f / (float)N;
   for (int c = threadIdx.x; c < nu; c += blockDim.x)
   {
-    const float2 z = W[c];
+    const float2 z = W[pidx(c)];
     a.out[(long long)ra * nu + c] = z.x * inv;
     if (rb < rows)
       a.out[(long long)rb * nu + c] = -z.y * inv;
@@ -311,6 +348,8 @@ run_filters(const rtkb_geometry * g, const rtkb_image_desc * in, const Options &
     return fail(RTKB_ERR_INVALID_ARGUMENT, "null buffer");
   if (d_in == d_out && nu_out != nu_in)
     return fail(RTKB_ERR_INVALID_ARGUMENT, "the padded displaced-detector output cannot be computed in place");
+  if (nv > 65535 || np > 65535)
+    return fail(RTKB_ERR_UNSUPPORTED, "projection stacks of more than 65535 rows or projections per call");
   if (!wd.empty() || short_scan)
   {
     colw.assign((size_t)np * nu_out, 1.f);
@@ -389,7 +428,7 @@ run_filters(const rtkb_geometry * g, const rtkb_image_desc * in, const Options &
     {
       const long long pairs = ((long long)nv * np + 1) / 2;
       const int       threads = std::min(512, std::max(64, a.N / 8));
-      const size_t    smem = 2 * (size_t)a.N * sizeof(float2);
+      const size_t    smem = 2 * (size_t)(a.N + a.N / 8) * sizeof(float2);
       cudaError_t     e = cudaFuncSetAttribute(ramp_fft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       if (e == cudaSuccess && pairs > 0x7fffffffLL)
         e = cudaErrorInvalidValue;
@@ -403,9 +442,8 @@ run_filters(const rtkb_geometry * g, const rtkb_image_desc * in, const Options &
     }
     else
     {
-      const long long n = (long long)nu_out * nv * np;
-      const long long blocks = std::min<long long>((n + 255) / 256, 148LL * 32);
-      weight_kernel<<<(unsigned)blocks, 256, 0, st>>>(a);
+      const dim3 grid((unsigned)((nu_out + 255) / 256), (unsigned)nv, (unsigned)np);
+      weight_kernel<<<grid, 256, 0, st>>>(a);
       cudaError_t e = cudaGetLastError();
       if (e != cudaSuccess)
         rc = cuda_fail(e, "weight_kernel launch");

@@ -99,12 +99,12 @@ weight_kernel(FilterArgs a)
     o[c] = weighted_pixel(a, w, s, r, c);
 }
 
-// Shared-memory index with one pad element after every 8: the stride-R writes
-// of the early Stockham passes (R = 8, 4) then spread over all banks.
-__device__ __forceinline__ int
+// Shared-memory index with one pad element after every 16: the stride-16
+// writes of the first radix-16 Stockham pass then spread over all banks.
+__host__ __device__ __forceinline__ int
 pidx(int x)
 {
-  return x + (x >> 3);
+  return x + (x >> 4);
 }
 
 __device__ __forceinline__ float2
@@ -164,13 +164,73 @@ dft_reg(float2 (&v)[R])
   }
 }
 
-// One Stockham pass: sub-transforms of length Ns become length Ns*R.
+// In-register forward DFT of size 16 (radix-2 decimation in frequency with the
+// W16^j = e^{-2 pi i j/16} constants, then the 4-bit reversal).
+__device__ __forceinline__ void
+dft16(float2 (&v)[16])
+{
+  constexpr float c[8] = { 1.f, 0.92387953251128675613f, 0.70710678118654752440f, 0.38268343236508977173f,
+                           0.f, -0.38268343236508977173f, -0.70710678118654752440f, -0.92387953251128675613f };
+  constexpr float sn[8] = { 0.f, 0.38268343236508977173f, 0.70710678118654752440f, 0.92387953251128675613f,
+                            1.f, 0.92387953251128675613f, 0.70710678118654752440f, 0.38268343236508977173f };
+#pragma unroll
+  for (int j = 0; j < 8; j++)
+  {
+    const float2 x = v[j], y = v[j + 8];
+    const float2 d = make_float2(x.x - y.x, x.y - y.y);
+    v[j] = make_float2(x.x + y.x, x.y + y.y);
+    v[j + 8] = make_float2(d.x * c[j] + d.y * sn[j], d.y * c[j] - d.x * sn[j]); // d * W16^j
+  }
+#pragma unroll
+  for (int half = 4; half >= 1; half >>= 1)
+  {
+#pragma unroll
+    for (int i = 0; i < 16; i += 2 * half)
+    {
+#pragma unroll
+      for (int j = 0; j < half; j++)
+      {
+        const float2 x = v[i + j], y = v[i + j + half];
+        v[i + j] = make_float2(x.x + y.x, x.y + y.y);
+        v[i + j + half] = rot_const(make_float2(x.x - y.x, x.y - y.y), j, 2 * half);
+      }
+    }
+  }
+  float2 t[16];
+#pragma unroll
+  for (int k = 0; k < 16; k++)
+    t[k] = v[((k & 1) << 3) | ((k & 2) << 1) | ((k & 4) >> 1) | ((k & 8) >> 3)];
+#pragma unroll
+  for (int k = 0; k < 16; k++)
+    v[k] = t[k];
+}
+
 template <int R>
 __device__ __forceinline__ void
-fft_pass(const float2 * __restrict__ src, float2 * __restrict__ dst, const float2 * __restrict__ tw, int N, int Ns)
+dft_any(float2 (&v)[R])
+{
+  if constexpr (R == 16)
+    dft16(v);
+  else
+    dft_reg<R>(v);
+}
+
+// Twiddle rows of one pass: powers 1, 2, 4, 8 (those below R) of
+// w = e^{-2 pi i k / (Ns R)}, each row Ns entries long (k = 0..Ns-1).
+template <int R>
+__host__ __device__ constexpr int
+twiddle_rows()
+{
+  return R == 16 ? 4 : R == 8 ? 3 : R == 4 ? 2 : 1;
+}
+
+// One Stockham pass in shared memory (padded indices): sub-transforms of
+// length Ns become length Ns*R.  twp: this pass's twiddle rows.
+template <int R>
+__device__ __forceinline__ void
+fft_pass(const float2 * __restrict__ src, float2 * __restrict__ dst, const float2 * __restrict__ twp, int N, int Ns)
 {
   const int nb = N / R;
-  const int tstride = N / (Ns * R);
   for (int j = threadIdx.x; j < nb; j += blockDim.x)
   {
     const int k = j & (Ns - 1);
@@ -180,11 +240,33 @@ fft_pass(const float2 * __restrict__ src, float2 * __restrict__ dst, const float
       v[r] = src[pidx(j + r * nb)];
     if (Ns > 1)
     {
+      // w^r from the tabulated w, w^2, w^4, w^8 with at most three products
+      float2 t[R];
+      t[1] = twp[k];
+      if constexpr (R > 2)
+      {
+        t[2] = twp[Ns + k];
+        t[3] = cmul(t[2], t[1]);
+      }
+      if constexpr (R > 4)
+      {
+        t[4] = twp[2 * Ns + k];
+        t[5] = cmul(t[4], t[1]);
+        t[6] = cmul(t[4], t[2]);
+        t[7] = cmul(t[4], t[3]);
+      }
+      if constexpr (R > 8)
+      {
+        t[8] = twp[3 * Ns + k];
+#pragma unroll
+        for (int q = 1; q < 8; q++)
+          t[8 + q] = cmul(t[8], t[q]);
+      }
 #pragma unroll
       for (int r = 1; r < R; r++)
-        v[r] = cmul(v[r], __ldg(tw + k * r * tstride));
+        v[r] = cmul(v[r], t[r]);
     }
-    dft_reg<R>(v);
+    dft_any<R>(v);
     const int d = (j - k) * R + k;
 #pragma unroll
     for (int r = 0; r < R; r++)
@@ -192,29 +274,39 @@ fft_pass(const float2 * __restrict__ src, float2 * __restrict__ dst, const float
   }
 }
 
-// Full forward FFT of length N (power of two, >= 2); returns the buffer holding
-// the result (a or b).
+// Forward FFT of length N (power of two, >= 2): radix-16 passes, then one
+// radix-8/4/2 pass; returns the buffer holding the result (a or b).
 __device__ float2 *
 fft_forward(float2 * a, float2 * b, const float2 * tw, int N)
 {
   float2 * src = a;
   float2 * dst = b;
+  int      off = 0;
   for (int Ns = 1; Ns < N;)
   {
     const int rem = N / Ns;
-    if (rem >= 8)
+    if (rem >= 16)
     {
-      fft_pass<8>(src, dst, tw, N, Ns);
+      fft_pass<16>(src, dst, tw + off, N, Ns);
+      off += Ns > 1 ? twiddle_rows<16>() * Ns : 0;
+      Ns *= 16;
+    }
+    else if (rem == 8)
+    {
+      fft_pass<8>(src, dst, tw + off, N, Ns);
+      off += Ns > 1 ? twiddle_rows<8>() * Ns : 0;
       Ns *= 8;
     }
     else if (rem == 4)
     {
-      fft_pass<4>(src, dst, tw, N, Ns);
+      fft_pass<4>(src, dst, tw + off, N, Ns);
+      off += Ns > 1 ? twiddle_rows<4>() * Ns : 0;
       Ns *= 4;
     }
     else
     {
-      fft_pass<2>(src, dst, tw, N, Ns);
+      fft_pass<2>(src, dst, tw + off, N, Ns);
+      off += Ns > 1 ? twiddle_rows<2>() * Ns : 0;
       Ns *= 2;
     }
     __syncthreads();
@@ -225,64 +317,104 @@ fft_forward(float2 * a, float2 * b, const float2 * tw, int N)
   return src;
 }
 
-__global__ void
-ramp_fft_kernel(FilterArgs a)
+// Ramp filter of the stack, persistent: each CTA loads the pass twiddles and
+// the ramp kernel into shared memory once, then filters row pairs (two real
+// rows as one complex sequence) until the stack is done.
+__global__ void __launch_bounds__(512)
+ramp_fft_kernel(FilterArgs a, int tw_len)
 {
   extern __shared__ float2 sbuf[];
+  const int N = a.N, P = pidx(N), nu = a.nu_out;
   float2 *  b0 = sbuf;
-  float2 *  b1 = sbuf + pidx(a.N);
-  const int rows = a.nv * a.np;
-  const int ra = 2 * blockIdx.x, rb = ra + 1;
-  const int N = a.N, nu = a.nu_out;
-  // load two weighted rows as one complex sequence, zero padded
-  const int       sa = ra / a.nv, rra = ra % a.nv, sb = rb / a.nv, rrb = rb % a.nv;
-  const RowWeight wa = row_weight(a, sa, rra);
-  const RowWeight wb = rb < rows ? row_weight(a, sb, rrb) : wa;
-  for (int c = threadIdx.x; c < N; c += blockDim.x)
+  float2 *  b1 = sbuf + P;
+  float2 *  tws = sbuf + 2 * P;
+  float *   Ks = reinterpret_cast<float *>(tws + tw_len);
+  for (int i = threadIdx.x; i < tw_len; i += blockDim.x)
+    tws[i] = a.tw[i];
+  for (int i = threadIdx.x; i <= N / 2; i += blockDim.x)
+    Ks[i] = a.K[i];
+  const long long rows = (long long)a.nv * a.np, pairs = (rows + 1) / 2;
+  const float     inv = 1.f / (float)N;
+  for (long long pr = blockIdx.x; pr < pairs; pr += gridDim.x)
   {
-    float x = 0.f, y = 0.f;
-    if (c < nu)
+    const long long ra = 2 * pr, rb = ra + 1;
+    const bool      hb = rb < rows;
+    const int       sa = (int)(ra / a.nv), rra = (int)(ra % a.nv);
+    const int       sb = hb ? (int)(rb / a.nv) : sa, rrb = hb ? (int)(rb % a.nv) : rra;
+    const RowWeight wa = row_weight(a, sa, rra);
+    const RowWeight wb = row_weight(a, sb, rrb);
+    __syncthreads(); // the previous pair's results have been stored
+    for (int c = threadIdx.x; c < N; c += blockDim.x)
     {
-      x = weighted_pixel(a, wa, sa, rra, c);
-      if (rb < rows)
-        y = weighted_pixel(a, wb, sb, rrb, c);
-    }
-    b0[pidx(c)] = make_float2(x, y);
-  }
-  __syncthreads();
-  if (a.next > 0)
-  {
-    // Ohnesorge mirror extrapolation (PadInputImageRegion :218-258): left
-    // values wrap to the end of the circular buffer.
-    const float2 SA = b0[pidx(1)], SE = b0[pidx(nu - 1)];
-    for (int bq = 1 + threadIdx.x; bq <= a.next; bq += blockDim.x)
-    {
-      const float  w = __ldg(a.mw + bq);
-      const float2 l = b0[pidx(bq)], r = b0[pidx(nu - 1 - bq)];
-      b0[pidx(N - bq)] = make_float2(w * (2.f * SA.x - l.x), w * (2.f * SA.y - l.y));
-      b0[pidx(nu - 1 + bq)] = make_float2(w * (2.f * SE.x - r.x), w * (2.f * SE.y - r.y));
+      float x = 0.f, y = 0.f;
+      if (c < nu)
+      {
+        x = weighted_pixel(a, wa, sa, rra, c);
+        if (hb)
+          y = weighted_pixel(a, wb, sb, rrb, c);
+      }
+      b0[pidx(c)] = make_float2(x, y);
     }
     __syncthreads();
+    if (a.next > 0)
+    {
+      // Ohnesorge mirror extrapolation (PadInputImageRegion :218-258): left
+      // values wrap to the end of the circular buffer.
+      const float2 SA = b0[pidx(1)], SE = b0[pidx(nu - 1)];
+      for (int bq = 1 + threadIdx.x; bq <= a.next; bq += blockDim.x)
+      {
+        const float  w = __ldg(a.mw + bq);
+        const float2 l = b0[pidx(bq)], r = b0[pidx(nu - 1 - bq)];
+        b0[pidx(N - bq)] = make_float2(w * (2.f * SA.x - l.x), w * (2.f * SA.y - l.y));
+        b0[pidx(nu - 1 + bq)] = make_float2(w * (2.f * SE.x - r.x), w * (2.f * SE.y - r.y));
+      }
+      __syncthreads();
+    }
+    float2 * X = fft_forward(b0, b1, tws, N);
+    float2 * other = (X == b0) ? b1 : b0;
+    // multiply by the real, even kernel and conjugate: the inverse transform is
+    // conj(FFT(conj(K X))) / N
+    for (int f = threadIdx.x; f < N; f += blockDim.x)
+    {
+      const float  k = Ks[min(f, N - f)];
+      const float2 z = X[pidx(f)];
+      X[pidx(f)] = make_float2(z.x * k, -z.y * k);
+    }
+    __syncthreads();
+    float2 * W = fft_forward(X, other, tws, N);
+    for (int c = threadIdx.x; c < nu; c += blockDim.x)
+    {
+      const float2 z = W[pidx(c)];
+      a.out[ra * nu + c] = z.x * inv;
+      if (hb)
+        a.out[rb * nu + c] = -z.y * inv;
+    }
   }
-  float2 * X = fft_forward(b0, b1, a.tw, N);
-  float2 * other = (X == b0) ? b1 : b0;
-  // multiply by the real, even kernel and conjugate: the inverse transform is
-  // conj(FFT(conj(K X))) / N
-  for (int f = threadIdx.x; f < N; f += blockDim.x)
+}
+
+// Twiddle rows of every pass of a length-N transform, in pass order, FP64
+// values stored as float2 (see fft_pass).
+static void
+pass_twiddles(int N, std::vector<float> & tw)
+{
+  tw.clear();
+  for (int Ns = 1; Ns < N;)
   {
-    const float  k = __ldg(a.K + min(f, N - f));
-    const float2 z = X[pidx(f)];
-    X[pidx(f)] = make_float2(z.x * k, -z.y * k);
-  }
-  __syncthreads();
-  float2 *    W = fft_forward(X, other, a.tw, N);
-  const float inv = 1.f / (float)N;
-  for (int c = threadIdx.x; c < nu; c += blockDim.x)
-  {
-    const float2 z = W[pidx(c)];
-    a.out[(long long)ra * nu + c] = z.x * inv;
-    if (rb < rows)
-      a.out[(long long)rb * nu + c] = -z.y * inv;
+    const int rem = N / Ns;
+    const int R = rem >= 16 ? 16 : rem;
+    const int nrows = R == 16 ? 4 : R == 8 ? 3 : R == 4 ? 2 : 1;
+    if (Ns > 1)
+      for (int row = 0; row < nrows; row++)
+      {
+        const int pw = 1 << row;
+        for (int k = 0; k < Ns; k++)
+        {
+          const double ang = -2. * 3.14159265358979323846 * (double)pw * (double)k / ((double)Ns * R);
+          tw.push_back((float)std::cos(ang));
+          tw.push_back((float)std::sin(ang));
+        }
+      }
+    Ns *= R;
   }
 }
 
@@ -386,7 +518,7 @@ run_filters(const rtkb_geometry * g, const rtkb_image_desc * in, const Options &
     std::vector<double> Kd;
     ramp_kernel(N, out.spacing[0], o.rp, Kd);
     K.assign(Kd.begin(), Kd.end());
-    twiddles(N, tw);
+    pass_twiddles(N, tw);
     int next = (int)std::floor(o.rp.truncation_correction * nu_out);
     next = std::min(next, (N - nu_out) / 2);
     if (next == 1)
@@ -427,14 +559,21 @@ run_filters(const rtkb_geometry * g, const rtkb_image_desc * in, const Options &
     if (o.ramp)
     {
       const long long pairs = ((long long)nv * np + 1) / 2;
-      const int       threads = std::min(512, std::max(64, a.N / 8));
-      const size_t    smem = 2 * (size_t)(a.N + a.N / 8) * sizeof(float2);
+      const int       threads = std::min(512, std::max(64, a.N / 16));
+      const int       tw_len = (int)(tw.size() / 2);
+      const size_t    smem = (2 * (size_t)pidx(a.N) + tw_len) * sizeof(float2) + ((size_t)a.N / 2 + 1) * sizeof(float);
       cudaError_t     e = cudaFuncSetAttribute(ramp_fft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e == cudaSuccess && pairs > 0x7fffffffLL)
-        e = cudaErrorInvalidValue;
+      int             dev = 0, sms = 0, per_sm = 0;
       if (e == cudaSuccess)
+        e = cudaGetDevice(&dev);
+      if (e == cudaSuccess)
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ramp_fft_kernel, threads, smem);
+      if (e == cudaSuccess && pairs > 0)
       {
-        ramp_fft_kernel<<<(unsigned)pairs, threads, smem, st>>>(a);
+        const long long grid = std::min<long long>(pairs, (long long)sms * std::max(per_sm, 1));
+        ramp_fft_kernel<<<(unsigned)grid, threads, smem, st>>>(a, tw_len);
         e = cudaGetLastError();
       }
       if (e != cudaSuccess)

@@ -70,12 +70,15 @@ row_weight(const FilterArgs & a, int s, int r)
 }
 
 __device__ __forceinline__ float
-weighted_pixel(const FilterArgs & a, const RowWeight & w, int s, int r, int c)
+raw_pixel(const FilterArgs & a, int s, int r, int c)
 {
   const int ci = c - a.shift;
-  if (ci < 0 || ci >= a.nu_in)
-    return 0.f;
-  float v = __ldg(a.in + ((long long)s * a.nv + r) * a.nu_in + ci);
+  return (ci >= 0 && ci < a.nu_in) ? __ldg(a.in + ((long long)s * a.nv + r) * a.nu_in + ci) : 0.f;
+}
+
+__device__ __forceinline__ float
+apply_weights(const FilterArgs & a, const RowWeight & w, int s, int c, float v)
+{
   if (a.colw)
     v *= __ldg(a.colw + (long long)s * a.nu_out + c);
   if (w.mode == 1)
@@ -86,6 +89,12 @@ weighted_pixel(const FilterArgs & a, const RowWeight & w, int s, int r, int c)
     v *= w.f * (w.num1 - x * w.sina) * rsqrtf(fmaf(dxs, dxs, w.e));
   }
   return v;
+}
+
+__device__ __forceinline__ float
+weighted_pixel(const FilterArgs & a, const RowWeight & w, int s, int r, int c)
+{
+  return apply_weights(a, w, s, c, raw_pixel(a, s, r, c));
 }
 
 // grid: (column blocks, rows, projections)
@@ -335,6 +344,25 @@ ramp_fft_kernel(FilterArgs a, int tw_len)
     Ks[i] = a.K[i];
   const long long rows = (long long)a.nv * a.np, pairs = (rows + 1) / 2;
   const float     inv = 1.f / (float)N;
+  // the next pair's raw pixels are prefetched into registers while the
+  // current pair is transformed (columns threadIdx.x + i * blockDim.x;
+  // blockDim.x >= N / 16, so 16 columns per thread cover the row)
+  float pa[16], pb[16];
+  auto  prefetch = [&](long long pr) {
+    const long long ra = 2 * pr, rb = ra + 1;
+    const int       sa = (int)(ra / a.nv), rra = (int)(ra % a.nv);
+    const bool      hb = rb < rows;
+    const int       sb = hb ? (int)(rb / a.nv) : sa, rrb = hb ? (int)(rb % a.nv) : rra;
+#pragma unroll
+    for (int i = 0; i < 16; i++)
+    {
+      const int c = threadIdx.x + i * blockDim.x;
+      pa[i] = (c < nu) ? raw_pixel(a, sa, rra, c) : 0.f;
+      pb[i] = (c < nu && hb) ? raw_pixel(a, sb, rrb, c) : 0.f;
+    }
+  };
+  if (blockIdx.x < pairs)
+    prefetch(blockIdx.x);
   for (long long pr = blockIdx.x; pr < pairs; pr += gridDim.x)
   {
     const long long ra = 2 * pr, rb = ra + 1;
@@ -344,17 +372,19 @@ ramp_fft_kernel(FilterArgs a, int tw_len)
     const RowWeight wa = row_weight(a, sa, rra);
     const RowWeight wb = row_weight(a, sb, rrb);
     __syncthreads(); // the previous pair's results have been stored
-    for (int c = threadIdx.x; c < N; c += blockDim.x)
+#pragma unroll
+    for (int i = 0; i < 16; i++)
     {
-      float x = 0.f, y = 0.f;
-      if (c < nu)
+      const int c = threadIdx.x + i * blockDim.x;
+      if (c < N)
       {
-        x = weighted_pixel(a, wa, sa, rra, c);
-        if (hb)
-          y = weighted_pixel(a, wb, sb, rrb, c);
+        const float x = (c < nu) ? apply_weights(a, wa, sa, c, pa[i]) : 0.f;
+        const float y = (c < nu && hb) ? apply_weights(a, wb, sb, c, pb[i]) : 0.f;
+        b0[pidx(c)] = make_float2(x, y);
       }
-      b0[pidx(c)] = make_float2(x, y);
     }
+    if (pr + gridDim.x < pairs)
+      prefetch(pr + gridDim.x);
     __syncthreads();
     if (a.next > 0)
     {

@@ -7,14 +7,18 @@
 // ramp filter (include/rtkFFTProjectionsConvolutionImageFilter.hxx:121-276 with
 // the kernel of include/rtkFFTRampImageFilter.hxx:47-178).
 //
-// The ramp filter is a hand-written shared-memory FFT: one CTA filters two
-// rows at once as the real and imaginary parts of one complex sequence (the
-// ramp kernel is real and even, so the two rows do not mix), zero-padded to
-// the power-of-two length RTK uses without FFTW.  Stockham radix-8 passes
-// (Govindaraju et al., SC08) with a final radix-4/2 pass; the inverse
-// transform is a forward transform of the conjugate.  Weights are computed in
-// FP64 (cos gamma) or from FP64 host tables (Parker, displaced detector); the
-// stack is read once and written once.
+// The ramp filter is a hand-written shared-memory FFT, compiled per padded
+// length N: two real rows are filtered at once as the real and imaginary
+// parts of one complex sequence (the ramp kernel is real and even, so the rows
+// do not mix), zero-padded to the power-of-two length RTK uses without FFTW.
+// Stockham radix-16 passes (Govindaraju et al., SC08) with a final radix-8/4/2
+// pass, twiddle powers from per-pass tables built in FP64 on the host, padded
+// shared-memory indices; the inverse transform is a forward transform of the
+// conjugate.  CTAs are persistent: the twiddles and the ramp kernel are loaded
+// into shared memory once, and the next row pair is prefetched into registers
+// while the current one is transformed.  FDK cos(gamma) weights come from
+// FP64 per-row terms evaluated per pixel in FP32, Parker and displaced-detector
+// weights from FP64 host tables; the stack is read once and written once.
 #include "rtkb_filters.h"
 
 #include <cstring>
@@ -110,7 +114,7 @@ weight_kernel(FilterArgs a)
 
 // Shared-memory index with one pad element after every 16: the stride-16
 // writes of the first radix-16 Stockham pass then spread over all banks.
-__host__ __device__ __forceinline__ int
+__host__ __device__ __forceinline__ constexpr int
 pidx(int x)
 {
   return x + (x >> 4);
@@ -233,23 +237,26 @@ twiddle_rows()
   return R == 16 ? 4 : R == 8 ? 3 : R == 4 ? 2 : 1;
 }
 
-// One Stockham pass in shared memory (padded indices): sub-transforms of
-// length Ns become length Ns*R.  twp: this pass's twiddle rows.
-template <int R>
+// Compile-time version of the pass chain for a fixed N: every stride, radix
+// and loop trip is a constant, so index arithmetic folds into immediates.
+template <int N, int T, int Ns, int R>
 __device__ __forceinline__ void
-fft_pass(const float2 * __restrict__ src, float2 * __restrict__ dst, const float2 * __restrict__ twp, int N, int Ns)
+fft_pass_c(const float2 * __restrict__ src, float2 * __restrict__ dst, const float2 * __restrict__ twp)
 {
-  const int nb = N / R;
-  for (int j = threadIdx.x; j < nb; j += blockDim.x)
+  constexpr int nb = N / R;
+#pragma unroll
+  for (int jj = 0; jj < (nb + T - 1) / T; jj++)
   {
+    const int j = threadIdx.x + jj * T;
+    if (nb % T != 0 && j >= nb)
+      break;
     const int k = j & (Ns - 1);
     float2    v[R];
 #pragma unroll
     for (int r = 0; r < R; r++)
       v[r] = src[pidx(j + r * nb)];
-    if (Ns > 1)
+    if constexpr (Ns > 1)
     {
-      // w^r from the tabulated w, w^2, w^4, w^8 with at most three products
       float2 t[R];
       t[1] = twp[k];
       if constexpr (R > 2)
@@ -283,57 +290,33 @@ fft_pass(const float2 * __restrict__ src, float2 * __restrict__ dst, const float
   }
 }
 
-// Forward FFT of length N (power of two, >= 2): radix-16 passes, then one
-// radix-8/4/2 pass; returns the buffer holding the result (a or b).
-__device__ float2 *
-fft_forward(float2 * a, float2 * b, const float2 * tw, int N)
+template <int N, int T, int Ns>
+__device__ __forceinline__ float2 *
+fft_chain(float2 * src, float2 * dst, const float2 * tw)
 {
-  float2 * src = a;
-  float2 * dst = b;
-  int      off = 0;
-  for (int Ns = 1; Ns < N;)
+  if constexpr (Ns >= N)
+    return src;
+  else
   {
-    const int rem = N / Ns;
-    if (rem >= 16)
-    {
-      fft_pass<16>(src, dst, tw + off, N, Ns);
-      off += Ns > 1 ? twiddle_rows<16>() * Ns : 0;
-      Ns *= 16;
-    }
-    else if (rem == 8)
-    {
-      fft_pass<8>(src, dst, tw + off, N, Ns);
-      off += Ns > 1 ? twiddle_rows<8>() * Ns : 0;
-      Ns *= 8;
-    }
-    else if (rem == 4)
-    {
-      fft_pass<4>(src, dst, tw + off, N, Ns);
-      off += Ns > 1 ? twiddle_rows<4>() * Ns : 0;
-      Ns *= 4;
-    }
-    else
-    {
-      fft_pass<2>(src, dst, tw + off, N, Ns);
-      off += Ns > 1 ? twiddle_rows<2>() * Ns : 0;
-      Ns *= 2;
-    }
+    constexpr int R = (N / Ns >= 16) ? 16 : N / Ns;
+    fft_pass_c<N, T, Ns, R>(src, dst, tw);
     __syncthreads();
-    float2 * t = src;
-    src = dst;
-    dst = t;
+    return fft_chain<N, T, Ns * R>(dst, src, tw + (Ns > 1 ? twiddle_rows<R>() * Ns : 0));
   }
-  return src;
 }
 
 // Ramp filter of the stack, persistent: each CTA loads the pass twiddles and
 // the ramp kernel into shared memory once, then filters row pairs (two real
 // rows as one complex sequence) until the stack is done.
-__global__ void __launch_bounds__(512)
+// 128 registers per thread at most: (threads x 128) x (512 / threads) = 64 K
+template <int N>
+__global__ void __launch_bounds__(N / 16 > 64 ? N / 16 : 64, 512 / (N / 16 > 64 ? N / 16 : 64))
 ramp_fft_kernel(FilterArgs a, int tw_len)
 {
+  constexpr int T = N / 16 > 64 ? N / 16 : 64; // threads; 16 columns per thread cover the row
+  constexpr int P = pidx(N);
   extern __shared__ float2 sbuf[];
-  const int N = a.N, P = pidx(N), nu = a.nu_out;
+  const int nu = a.nu_out;
   float2 *  b0 = sbuf;
   float2 *  b1 = sbuf + P;
   float2 *  tws = sbuf + 2 * P;
@@ -356,7 +339,7 @@ ramp_fft_kernel(FilterArgs a, int tw_len)
 #pragma unroll
     for (int i = 0; i < 16; i++)
     {
-      const int c = threadIdx.x + i * blockDim.x;
+      const int c = threadIdx.x + i * T;
       pa[i] = (c < nu) ? raw_pixel(a, sa, rra, c) : 0.f;
       pb[i] = (c < nu && hb) ? raw_pixel(a, sb, rrb, c) : 0.f;
     }
@@ -375,7 +358,7 @@ ramp_fft_kernel(FilterArgs a, int tw_len)
 #pragma unroll
     for (int i = 0; i < 16; i++)
     {
-      const int c = threadIdx.x + i * blockDim.x;
+      const int c = threadIdx.x + i * T;
       if (c < N)
       {
         const float x = (c < nu) ? apply_weights(a, wa, sa, c, pa[i]) : 0.f;
@@ -400,7 +383,7 @@ ramp_fft_kernel(FilterArgs a, int tw_len)
       }
       __syncthreads();
     }
-    float2 * X = fft_forward(b0, b1, tws, N);
+    float2 * X = fft_chain<N, T, 1>(b0, b1, tws);
     float2 * other = (X == b0) ? b1 : b0;
     // multiply by the real, even kernel and conjugate: the inverse transform is
     // conj(FFT(conj(K X))) / N
@@ -411,7 +394,7 @@ ramp_fft_kernel(FilterArgs a, int tw_len)
       X[pidx(f)] = make_float2(z.x * k, -z.y * k);
     }
     __syncthreads();
-    float2 * W = fft_forward(X, other, tws, N);
+    float2 * W = fft_chain<N, T, 1>(X, other, tws);
     for (int c = threadIdx.x; c < nu; c += blockDim.x)
     {
       const float2 z = W[pidx(c)];
@@ -446,6 +429,29 @@ pass_twiddles(int N, std::vector<float> & tw)
       }
     Ns *= R;
   }
+}
+
+template <int N>
+static cudaError_t
+launch_ramp(const FilterArgs & a, int tw_len, long long pairs, cudaStream_t st)
+{
+  constexpr int threads = N / 16 > 64 ? N / 16 : 64;
+  const size_t  smem = (2 * (size_t)pidx(N) + tw_len) * sizeof(float2) + ((size_t)N / 2 + 1) * sizeof(float);
+  cudaError_t   e = cudaFuncSetAttribute(ramp_fft_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int           dev = 0, sms = 0, per_sm = 0;
+  if (e == cudaSuccess)
+    e = cudaGetDevice(&dev);
+  if (e == cudaSuccess)
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ramp_fft_kernel<N>, threads, smem);
+  if (e == cudaSuccess && pairs > 0)
+  {
+    const long long grid = std::min<long long>(pairs, (long long)sms * std::max(per_sm, 1));
+    ramp_fft_kernel<N><<<(unsigned)grid, threads, smem, st>>>(a, tw_len);
+    e = cudaGetLastError();
+  }
+  return e;
 }
 
 struct Options
@@ -589,22 +595,23 @@ run_filters(const rtkb_geometry * g, const rtkb_image_desc * in, const Options &
     if (o.ramp)
     {
       const long long pairs = ((long long)nv * np + 1) / 2;
-      const int       threads = std::min(512, std::max(64, a.N / 16));
-      const int       tw_len = (int)(tw.size() / 2);
-      const size_t    smem = (2 * (size_t)pidx(a.N) + tw_len) * sizeof(float2) + ((size_t)a.N / 2 + 1) * sizeof(float);
-      cudaError_t     e = cudaFuncSetAttribute(ramp_fft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      int             dev = 0, sms = 0, per_sm = 0;
-      if (e == cudaSuccess)
-        e = cudaGetDevice(&dev);
-      if (e == cudaSuccess)
-        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-      if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ramp_fft_kernel, threads, smem);
-      if (e == cudaSuccess && pairs > 0)
+      const int    tw_len = (int)(tw.size() / 2);
+      cudaError_t  e = cudaSuccess;
+      switch (a.N)
       {
-        const long long grid = std::min<long long>(pairs, (long long)sms * std::max(per_sm, 1));
-        ramp_fft_kernel<<<(unsigned)grid, threads, smem, st>>>(a, tw_len);
-        e = cudaGetLastError();
+        case 2: e = launch_ramp<2>(a, tw_len, pairs, st); break;
+        case 4: e = launch_ramp<4>(a, tw_len, pairs, st); break;
+        case 8: e = launch_ramp<8>(a, tw_len, pairs, st); break;
+        case 16: e = launch_ramp<16>(a, tw_len, pairs, st); break;
+        case 32: e = launch_ramp<32>(a, tw_len, pairs, st); break;
+        case 64: e = launch_ramp<64>(a, tw_len, pairs, st); break;
+        case 128: e = launch_ramp<128>(a, tw_len, pairs, st); break;
+        case 256: e = launch_ramp<256>(a, tw_len, pairs, st); break;
+        case 512: e = launch_ramp<512>(a, tw_len, pairs, st); break;
+        case 1024: e = launch_ramp<1024>(a, tw_len, pairs, st); break;
+        case 2048: e = launch_ramp<2048>(a, tw_len, pairs, st); break;
+        case 4096: e = launch_ramp<4096>(a, tw_len, pairs, st); break;
+        default: e = launch_ramp<8192>(a, tw_len, pairs, st); break;
       }
       if (e != cudaSuccess)
         rc = cuda_fail(e, "ramp_fft_kernel launch");

@@ -138,9 +138,14 @@ template <int BW, int BH, typename T = float>
 struct Layout
 {
   static constexpr int kBoxBytes = BW * BH * (int)sizeof(T);
+  // TMA writes its boxes to 128-byte aligned shared memory: the ring's stride
+  // is the box rounded up to 128 bytes
+  static constexpr int kBoxStride = (kBoxBytes + 127) / 128 * 128;
+  static constexpr int kBoxStrideElems = kBoxStride / (int)sizeof(T);
   static constexpr int kHeaders = 0;
   static constexpr int kBoxes = kStages * kHeaderBytes;
-  static constexpr int kBars = kBoxes + kStages * kBoxBytes;
+  static constexpr int kBars = kBoxes + kStages * kBoxStride;
+  static_assert(kBoxes % 128 == 0 && kBoxStride % 128 == 0, "TMA box destinations must be 128-byte aligned");
   static constexpr int kTotal = kBars + 2 * kStages * 8;
 };
 
@@ -249,7 +254,7 @@ bp_producer(const CUtensorMap * tmap, const T * __restrict__ proj, const double 
     if (skip)
       fast = false;
     const double * m = h->m;
-    T *      box = boxes + s * (BW * BH);
+    T *      box = boxes + s * L::kBoxStrideElems;
     if (lane == 0)
     {
       int flags = 0;
@@ -334,7 +339,7 @@ bp_consumer(const T * __restrict__ proj, int nproj, int nu, int nv, int nx, int 
     if (!mbar_wait(&full[s], (gp / kStages) & 1))
       return false;
     const StageHeader * h = hdr + s;
-    const T *           box = boxes + s * (BW * BH);
+    const T *           box = boxes + s * Layout<BW, BH, T>::kBoxStrideElems;
     const int4          fl = h->fl;
     if (active)
     {
@@ -626,13 +631,16 @@ struct BpConfig
 // holds the probed footprints is used unless the autotuner forces one.
 constexpr int           kNumBpConfigs = 6;
 // Box widths of 68 and 132 floats put consecutive rows 4 banks apart, so taps
-// in the same column but different rows do not collide.
-static const BpConfig   kBpConfigs[kNumBpConfigs] = { { 68, 64, 16, 3 }, { 68, 64, 16, 2 }, { 68, 32, 8, 3 },
-                                                      { 68, 32, 8, 2 },  { 132, 64, 16, 1 }, { 132, 64, 8, 1 } };
+// in the same column but different rows do not collide.  24-voxel columns at
+// 2 CTAs per SM amortise each column's per-projection set-up over more voxels
+// (fastest on 512^3 x 720); their 72-row box holds the corner tiles' footprints.
+static const BpConfig   kBpConfigs[kNumBpConfigs] = { { 68, 72, 24, 2 }, { 68, 64, 16, 3 }, { 68, 64, 16, 2 },
+                                                      { 68, 32, 8, 3 },  { 132, 64, 16, 1 }, { 132, 64, 8, 1 } };
 // BF16 boxes: widths are multiples of 8 elements (16-byte TMA rows); 72 and
-// 136 elements are 36 and 68 words, again 4 banks per row.
-static const BpConfig   kBpConfigsBf16[kNumBpConfigs] = { { 72, 64, 16, 3 }, { 72, 64, 16, 2 }, { 72, 32, 8, 3 },
-                                                          { 72, 32, 8, 2 },  { 136, 64, 16, 1 }, { 136, 64, 8, 1 } };
+// 136 elements are 36 and 68 words, again 4 banks per row.  16-voxel columns
+// at 3 CTAs per SM come first here (faster than 24 with BF16 taps).
+static const BpConfig   kBpConfigsBf16[kNumBpConfigs] = { { 72, 64, 16, 3 }, { 72, 72, 24, 2 }, { 72, 64, 16, 2 },
+                                                          { 72, 32, 8, 3 },  { 136, 64, 16, 1 }, { 136, 64, 8, 1 } };
 static thread_local int g_bp_forced_config = -1;
 static thread_local int g_bp_last_config = -1;
 
@@ -720,13 +728,13 @@ dispatch_tiled(int cfg, const CUtensorMap & tmap, bool use_tma, const float * d_
   switch (cfg)
   {
     case 0:
-      RTKB_BP_LAUNCH(68, 64, 16, 3);
+      RTKB_BP_LAUNCH(68, 72, 24, 2);
     case 1:
-      RTKB_BP_LAUNCH(68, 64, 16, 2);
+      RTKB_BP_LAUNCH(68, 64, 16, 3);
     case 2:
-      RTKB_BP_LAUNCH(68, 32, 8, 3);
+      RTKB_BP_LAUNCH(68, 64, 16, 2);
     case 3:
-      RTKB_BP_LAUNCH(68, 32, 8, 2);
+      RTKB_BP_LAUNCH(68, 32, 8, 3);
     case 4:
       RTKB_BP_LAUNCH(132, 64, 16, 1);
     default:
@@ -748,11 +756,11 @@ dispatch_tiled(int cfg, const CUtensorMap & tmap, bool use_tma, const __nv_bfloa
     case 0:
       RTKB_BP_LAUNCH(72, 64, 16, 3);
     case 1:
-      RTKB_BP_LAUNCH(72, 64, 16, 2);
+      RTKB_BP_LAUNCH(72, 72, 24, 2);
     case 2:
-      RTKB_BP_LAUNCH(72, 32, 8, 3);
+      RTKB_BP_LAUNCH(72, 64, 16, 2);
     case 3:
-      RTKB_BP_LAUNCH(72, 32, 8, 2);
+      RTKB_BP_LAUNCH(72, 32, 8, 3);
     case 4:
       RTKB_BP_LAUNCH(136, 64, 16, 1);
     default:
@@ -787,13 +795,13 @@ dispatch_batch(int cfg, const BatchProblem * d_probs, int nprob, long long nitem
   switch (cfg)
   {
     case 0:
-      return launch_batch<68, 64, 16, 3, FDKW>(d_probs, nprob, nitems, d_counter, st);
+      return launch_batch<68, 72, 24, 2, FDKW>(d_probs, nprob, nitems, d_counter, st);
     case 1:
-      return launch_batch<68, 64, 16, 2, FDKW>(d_probs, nprob, nitems, d_counter, st);
+      return launch_batch<68, 64, 16, 3, FDKW>(d_probs, nprob, nitems, d_counter, st);
     case 2:
-      return launch_batch<68, 32, 8, 3, FDKW>(d_probs, nprob, nitems, d_counter, st);
+      return launch_batch<68, 64, 16, 2, FDKW>(d_probs, nprob, nitems, d_counter, st);
     case 3:
-      return launch_batch<68, 32, 8, 2, FDKW>(d_probs, nprob, nitems, d_counter, st);
+      return launch_batch<68, 32, 8, 3, FDKW>(d_probs, nprob, nitems, d_counter, st);
     case 4:
       return launch_batch<132, 64, 16, 1, FDKW>(d_probs, nprob, nitems, d_counter, st);
     default:
@@ -910,14 +918,14 @@ backproject_buffer(const int vol_size[3], const int proj_size[3], int nproj, con
     }
     // first configuration whose box holds the footprints probed on the host
     std::vector<double> mv(mats, mats + 12 * (size_t)nproj);
-    double              fw8, fh8, fw16, fh16;
-    estimate_footprint(mv, nproj, nx, ny, nz, 8, fw8, fh8);
-    estimate_footprint(mv, nproj, nx, ny, nz, 16, fw16, fh16);
+    double              fw[3], fh[3]; // columns of 8, 16, 24 voxels
+    for (int q = 0; q < 3; q++)
+      estimate_footprint(mv, nproj, nx, ny, nz, 8 * (q + 1), fw[q], fh[q]);
     int cfg = kNumBpConfigs - 1;
     for (int c = 0; c < kNumBpConfigs; c++)
     {
-      const double fw = configs[c].nyt == 16 ? fw16 : fw8, fh = configs[c].nyt == 16 ? fh16 : fh8;
-      if (fw + kSlack < configs[c].bw - 1 && fh + 0.2 < configs[c].bh - 1)
+      const int q = configs[c].nyt / 8 - 1;
+      if (fw[q] + kSlack < configs[c].bw - 1 && fh[q] + 0.2 < configs[c].bh - 1)
       {
         cfg = c;
         break;
@@ -1044,7 +1052,7 @@ create_batch(const rtkb_bp_problem * probs, int n, bool fdk, int cfg, rtkb_bp_ba
     std::vector<double> mats;
   };
   std::vector<Host> batch;
-  double            fw8 = 0., fh8 = 0., fw16 = 0., fh16 = 0.;
+  double            fw[3] = { 0., 0., 0. }, fh[3] = { 0., 0., 0. }; // columns of 8, 16, 24 voxels
   for (int i = 0; i < n; i++)
   {
     const rtkb_bp_problem & P = probs[i];
@@ -1087,13 +1095,13 @@ create_batch(const rtkb_bp_problem * probs, int n, bool fdk, int cfg, rtkb_bp_ba
       B->generic.push_back(rtkb_bp_batch::Generic{ P, std::move(mats), std::move(modes) });
       continue;
     }
-    double a, b, c, d;
-    estimate_footprint(mats, np, P.vol.size[0], P.vol.size[1], P.vol.size[2], 8, a, b);
-    estimate_footprint(mats, np, P.vol.size[0], P.vol.size[1], P.vol.size[2], 16, c, d);
-    fw8 = std::max(fw8, a);
-    fh8 = std::max(fh8, b);
-    fw16 = std::max(fw16, c);
-    fh16 = std::max(fh16, d);
+    for (int q = 0; q < 3; q++)
+    {
+      double a, b;
+      estimate_footprint(mats, np, P.vol.size[0], P.vol.size[1], P.vol.size[2], 8 * (q + 1), a, b);
+      fw[q] = std::max(fw[q], a);
+      fh[q] = std::max(fh[q], b);
+    }
     batch.push_back(Host{ i, std::move(mats) });
   }
   if (cfg < 0)
@@ -1101,8 +1109,8 @@ create_batch(const rtkb_bp_problem * probs, int n, bool fdk, int cfg, rtkb_bp_ba
     cfg = kNumBpConfigs - 1;
     for (int c = 0; c < kNumBpConfigs; c++)
     {
-      const double fw = kBpConfigs[c].nyt == 16 ? fw16 : fw8, fh = kBpConfigs[c].nyt == 16 ? fh16 : fh8;
-      if (fw + 3.2 < kBpConfigs[c].bw - 1 && fh + 0.2 < kBpConfigs[c].bh - 1)
+      const int q = kBpConfigs[c].nyt / 8 - 1;
+      if (fw[q] + 3.2 < kBpConfigs[c].bw - 1 && fh[q] + 0.2 < kBpConfigs[c].bh - 1)
       {
         cfg = c;
         break;

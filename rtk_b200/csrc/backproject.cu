@@ -323,14 +323,20 @@ bp_consumer(const T * __restrict__ proj, int nproj, int nu, int nv, int nx, int 
   const int lane = threadIdx.x & 31;
   // --------------------------------------------------------------- consumers
   const int   t = threadIdx.x;
-  const int   dx = t % kTX, dz = t / kTX;
+  // warp w covers x in [8 (w % 2), +8) and z in [4 (w / 2), +4): 8 x 4
+  // voxels whose taps span few detector columns (see the box widths below)
+  const int   dx = (lane & 7) + 8 * ((t >> 5) & 1), dz = (lane >> 3) + 4 * (t >> 6);
   const int   X = x0 + dx, Z = z0 + dz;
   const bool  active = (X < nx) && (Z < nz);
   const float fdx = (float)dx, fdz = (float)dz;
-  float       acc[NYT];
+  static_assert(NYT % 2 == 0, "voxel columns are processed in pairs");
+  // Accumulators of voxels 2k and 2k+1 share a register pair, so the
+  // interior loop runs on sm_100's packed FP32 instructions (FFMA2).
+  float2      acc2[NYT / 2];
 #pragma unroll
-  for (int j = 0; j < NYT; j++)
-    acc[j] = 0.f;
+  for (int k = 0; k < NYT / 2; k++)
+    acc2[k] = make_float2(0.f, 0.f);
+#define BP_ACC(j) (((j) & 1) ? acc2[(j) >> 1].y : acc2[(j) >> 1].x)
 
   for (int p = 0; p < nproj; p++)
   {
@@ -367,17 +373,25 @@ bp_consumer(const T * __restrict__ proj, int nproj, int nu, int nv, int nx, int 
           const T *     col = box + (int)flu;
           if (fl.x & kFlagVInterior)
           {
+            // Voxels j and j+1 per step on packed FP32 instructions: the
+            // same operations and roundings as one voxel at a time, with
+            // b - a written as fma(-1, a, b), so the sums are bit-identical.
+            const float2 fu2 = make_float2(fu, fu), wt2 = make_float2(wt, wt);
+            const float2 m1 = make_float2(-1.f, -1.f);
 #pragma unroll
-            for (int j = 0; j < NYT; j++)
+            for (int j = 0; j < NYT; j += 2)
             {
-              const float   v = fmaf((float)j, dv, v0);
-              const float   flv = floorf(v);
-              const float   fv = v - flv;
-              const T *     q = col + (int)flv * BW;
-              const float   p00 = tap(q), p01 = tap(q + 1), p10 = tap(q + BW), p11 = tap(q + BW + 1);
-              const float   r0 = fmaf(fu, p01 - p00, p00);
-              const float   r1 = fmaf(fu, p11 - p10, p10);
-              acc[j] = fmaf(wt, fmaf(fv, r1 - r0, r0), acc[j]);
+              const float2 v = make_float2(fmaf((float)j, dv, v0), fmaf((float)(j + 1), dv, v0));
+              const float2 fl = make_float2(floorf(v.x), floorf(v.y));
+              const float2 fv = __ffma2_rn(m1, fl, v);
+              const T *    qa = col + (int)fl.x * BW;
+              const T *    qb = col + (int)fl.y * BW;
+              const float2 p00 = make_float2(tap(qa), tap(qb)), p01 = make_float2(tap(qa + 1), tap(qb + 1));
+              const float2 p10 = make_float2(tap(qa + BW), tap(qb + BW));
+              const float2 p11 = make_float2(tap(qa + BW + 1), tap(qb + BW + 1));
+              const float2 r0 = __ffma2_rn(fu2, __ffma2_rn(m1, p00, p01), p00);
+              const float2 r1 = __ffma2_rn(fu2, __ffma2_rn(m1, p10, p11), p10);
+              acc2[j >> 1] = __ffma2_rn(wt2, __ffma2_rn(fv, __ffma2_rn(m1, r0, r1), r0), acc2[j >> 1]);
             }
           }
           else
@@ -411,7 +425,7 @@ bp_consumer(const T * __restrict__ proj, int nproj, int nu, int nv, int nx, int 
                 const float   p00 = tap(q), p01 = tap(q + 1), p10 = tap(q + BW), p11 = tap(q + BW + 1);
                 const float   r0 = fmaf(fu, p01 - p00, p00);
                 const float   r1 = fmaf(fu, p11 - p10, p10);
-                acc[j] = fmaf(wt, fmaf(fv, r1 - r0, r0), acc[j]);
+                BP_ACC(j) = fmaf(wt, fmaf(fv, r1 - r0, r0), BP_ACC(j));
               }
             }
           }
@@ -422,7 +436,7 @@ bp_consumer(const T * __restrict__ proj, int nproj, int nu, int nv, int nx, int 
         const long long pofs = (long long)p * nu * nv;
 #pragma unroll
         for (int j = 0; j < NYT; j++)
-          acc[j] += slow_voxel(h->m, proj, pofs, nu, nv, X, y0 + j, Z, FDKW);
+          BP_ACC(j) += slow_voxel(h->m, proj, pofs, nu, nv, X, y0 + j, Z, FDKW);
       }
     }
     __syncwarp();
@@ -439,12 +453,13 @@ bp_consumer(const T * __restrict__ proj, int nproj, int nu, int nv, int nx, int 
       if (Y < ny)
       {
         const long long o = ((long long)Z * ny + Y) * nx + X;
-        vol_out[o] = vol_in[o] + acc[j];
+        vol_out[o] = vol_in[o] + BP_ACC(j);
       }
     }
   }
   return true;
 }
+#undef BP_ACC
 
 template <int BW, int BH, int NYT, int MINB, bool FDKW, typename T = float>
 __global__ void __launch_bounds__(kThreads, MINB)
@@ -630,17 +645,20 @@ struct BpConfig
 // register budget targets), in order of preference; the first whose box
 // holds the probed footprints is used unless the autotuner forces one.
 constexpr int           kNumBpConfigs = 6;
-// Box widths of 68 and 132 floats put consecutive rows 4 banks apart, so taps
-// in the same column but different rows do not collide.  24-voxel columns at
-// 2 CTAs per SM amortise each column's per-projection set-up over more voxels
-// (fastest on 512^3 x 720); their 72-row box holds the corner tiles' footprints.
-static const BpConfig   kBpConfigs[kNumBpConfigs] = { { 68, 72, 24, 2 }, { 68, 64, 16, 3 }, { 68, 64, 16, 2 },
-                                                      { 68, 32, 8, 3 },  { 132, 64, 16, 1 }, { 132, 64, 8, 1 } };
-// BF16 boxes: widths are multiples of 8 elements (16-byte TMA rows); 72 and
-// 136 elements are 36 and 68 words, again 4 banks per row.  16-voxel columns
-// at 3 CTAs per SM come first here (faster than 24 with BF16 taps).
-static const BpConfig   kBpConfigsBf16[kNumBpConfigs] = { { 72, 64, 16, 3 }, { 72, 72, 24, 2 }, { 72, 64, 16, 2 },
-                                                          { 72, 32, 8, 3 },  { 136, 64, 16, 1 }, { 136, 64, 8, 1 } };
+// Box rows are 16 (mod 32) words long: a warp covers 8 x 4 voxels, whose taps
+// span at most ~16 columns, so when its lanes straddle two detector rows the
+// second row's taps fall in the other half of the banks (rows 4 banks apart
+// cost 25 % extra shared-memory wavefronts in conflicts).  16-voxel columns at
+// 3 CTAs per SM with a 48-row box come first (fastest on 512^3 x 720); 24-voxel
+// columns at 2 CTAs per SM amortise each column's set-up over more voxels;
+// the rest hold taller and wider footprints.
+static const BpConfig   kBpConfigs[kNumBpConfigs] = { { 80, 48, 16, 3 }, { 80, 72, 24, 2 }, { 80, 72, 16, 2 },
+                                                      { 80, 32, 8, 3 }, { 112, 48, 8, 2 }, { 144, 64, 8, 1 } };
+// BF16 boxes: widths are multiples of 8 elements (16-byte TMA rows); 96 and
+// 160 elements are 48 and 80 words, again 16 (mod 32); same order as the FP32
+// table.
+static const BpConfig   kBpConfigsBf16[kNumBpConfigs] = { { 96, 48, 16, 3 }, { 96, 72, 24, 2 }, { 96, 72, 16, 2 },
+                                                          { 96, 32, 8, 3 }, { 160, 48, 8, 2 }, { 160, 64, 8, 1 } };
 static thread_local int g_bp_forced_config = -1;
 static thread_local int g_bp_last_config = -1;
 
@@ -728,17 +746,17 @@ dispatch_tiled(int cfg, const CUtensorMap & tmap, bool use_tma, const float * d_
   switch (cfg)
   {
     case 0:
-      RTKB_BP_LAUNCH(68, 72, 24, 2);
+      RTKB_BP_LAUNCH(80, 48, 16, 3);
     case 1:
-      RTKB_BP_LAUNCH(68, 64, 16, 3);
+      RTKB_BP_LAUNCH(80, 72, 24, 2);
     case 2:
-      RTKB_BP_LAUNCH(68, 64, 16, 2);
+      RTKB_BP_LAUNCH(80, 72, 16, 2);
     case 3:
-      RTKB_BP_LAUNCH(68, 32, 8, 3);
+      RTKB_BP_LAUNCH(80, 32, 8, 3);
     case 4:
-      RTKB_BP_LAUNCH(132, 64, 16, 1);
+      RTKB_BP_LAUNCH(112, 48, 8, 2);
     default:
-      RTKB_BP_LAUNCH(132, 64, 8, 1);
+      RTKB_BP_LAUNCH(144, 64, 8, 1);
   }
 #undef RTKB_BP_LAUNCH
 }
@@ -754,17 +772,17 @@ dispatch_tiled(int cfg, const CUtensorMap & tmap, bool use_tma, const __nv_bfloa
   switch (cfg)
   {
     case 0:
-      RTKB_BP_LAUNCH(72, 64, 16, 3);
+      RTKB_BP_LAUNCH(96, 48, 16, 3);
     case 1:
-      RTKB_BP_LAUNCH(72, 72, 24, 2);
+      RTKB_BP_LAUNCH(96, 72, 24, 2);
     case 2:
-      RTKB_BP_LAUNCH(72, 64, 16, 2);
+      RTKB_BP_LAUNCH(96, 72, 16, 2);
     case 3:
-      RTKB_BP_LAUNCH(72, 32, 8, 3);
+      RTKB_BP_LAUNCH(96, 32, 8, 3);
     case 4:
-      RTKB_BP_LAUNCH(136, 64, 16, 1);
+      RTKB_BP_LAUNCH(160, 48, 8, 2);
     default:
-      RTKB_BP_LAUNCH(136, 64, 8, 1);
+      RTKB_BP_LAUNCH(160, 64, 8, 1);
   }
 #undef RTKB_BP_LAUNCH
 }
@@ -795,17 +813,17 @@ dispatch_batch(int cfg, const BatchProblem * d_probs, int nprob, long long nitem
   switch (cfg)
   {
     case 0:
-      return launch_batch<68, 72, 24, 2, FDKW>(d_probs, nprob, nitems, d_counter, st);
+      return launch_batch<80, 48, 16, 3, FDKW>(d_probs, nprob, nitems, d_counter, st);
     case 1:
-      return launch_batch<68, 64, 16, 3, FDKW>(d_probs, nprob, nitems, d_counter, st);
+      return launch_batch<80, 72, 24, 2, FDKW>(d_probs, nprob, nitems, d_counter, st);
     case 2:
-      return launch_batch<68, 64, 16, 2, FDKW>(d_probs, nprob, nitems, d_counter, st);
+      return launch_batch<80, 72, 16, 2, FDKW>(d_probs, nprob, nitems, d_counter, st);
     case 3:
-      return launch_batch<68, 32, 8, 3, FDKW>(d_probs, nprob, nitems, d_counter, st);
+      return launch_batch<80, 32, 8, 3, FDKW>(d_probs, nprob, nitems, d_counter, st);
     case 4:
-      return launch_batch<132, 64, 16, 1, FDKW>(d_probs, nprob, nitems, d_counter, st);
+      return launch_batch<112, 48, 8, 2, FDKW>(d_probs, nprob, nitems, d_counter, st);
     default:
-      return launch_batch<132, 64, 8, 1, FDKW>(d_probs, nprob, nitems, d_counter, st);
+      return launch_batch<144, 64, 8, 1, FDKW>(d_probs, nprob, nitems, d_counter, st);
   }
 }
 

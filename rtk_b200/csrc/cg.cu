@@ -36,6 +36,7 @@ struct rtkb_cg
   float *                  P = nullptr;
   float *                  AP = nullptr;
   float *                  A = nullptr; // BP accumulator / FP transpose scratch
+  void *                   fps = nullptr; // forward projector scratch (transposed and quad copies)
   float *                  At = nullptr;
   double *                 scal = nullptr; // rr, rr0, alpha, beta, pAp
   double *                 partial = nullptr;
@@ -359,7 +360,7 @@ grid_for(long long n)
 cudaError_t
 apply_A(rtkb_cg * c, const float * in, float * out, cudaStream_t st)
 {
-  cudaError_t e = rtkb::joseph_forward_launch(c->args, in, c->A, nullptr, c->tmp, c->W, st);
+  cudaError_t e = rtkb::joseph_forward_launch(c->args, in, c->fps, nullptr, c->tmp, c->W, st);
   if (e != cudaSuccess)
     return e;
   return rtkb::joseph_back_launch(c->args, c->tmp, c->A, c->At, nullptr, out, c->tikhonov != 0.f ? in : nullptr,
@@ -488,7 +489,8 @@ rtkb_cg_create(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_
     auto         up = [](size_t b) { return (b + 255) & ~size_t(255); };
     const size_t tb = up(tab.size() * sizeof(RayProj)), pb = up((size_t)c->npix * 4), vb = up((size_t)c->nvox * 4);
     const size_t sb = up(8 * sizeof(double)), rb = up(kRedBlocks * sizeof(double));
-    const size_t total = tb + 2 * pb + 5 * vb + sb + rb;
+    const size_t fb = up(joseph_forward_scratch_bytes(c->nvox));
+    const size_t total = tb + 2 * pb + 5 * vb + sb + rb + fb;
     cudaError_t  e = cudaMalloc(&c->mem, total);
     if (e == cudaSuccess && c->use_graph)
       e = cudaStreamCreateWithFlags(&c->cap, cudaStreamNonBlocking);
@@ -517,6 +519,8 @@ rtkb_cg_create(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_
     c->scal = reinterpret_cast<double *>(m);
     m += sb;
     c->partial = reinterpret_cast<double *>(m);
+    m += rb;
+    c->fps = m;
     e = cudaMemcpy(c->tab, tab.data(), tab.size() * sizeof(RayProj), cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
       e = cudaMemset(c->scal, 0, sb);

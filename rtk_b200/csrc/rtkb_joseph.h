@@ -34,9 +34,11 @@ void joseph_args(JosephArgs & a, const rtkb_image_desc & vol, const rtkb_image_d
 int joseph_check(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj);
 
 // Enqueue the forward projector: pout = w * (pin + FP(V)); pin, w may be null.
-// Vt: scratch of the volume's size (z<->x transposed copy).
-cudaError_t joseph_forward_launch(const JosephArgs & a, const float * V, float * Vt, const float * pin, float * pout,
-                                  const float * w, cudaStream_t st);
+// scratch: joseph_forward_scratch_bytes(voxels) bytes, 256-byte aligned (the
+// z<->x transposed copy and the two quad-expanded copies of the volume).
+size_t      joseph_forward_scratch_bytes(long long nvox);
+cudaError_t joseph_forward_launch(const JosephArgs & a, const float * V, void * scratch, const float * pin,
+                                  float * pout, const float * w, cudaStream_t st);
 // Enqueue the back projector: vout = vin + BP(proj) + tau * x; vin, x may be
 // null.  A, At: zero-initialised here, scratch of the volume's size each.
 cudaError_t joseph_back_launch(const JosephArgs & a, const float * proj, float * A, float * At, const float * vin,

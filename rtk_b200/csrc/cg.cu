@@ -35,9 +35,7 @@ struct rtkb_cg
   float *                  R = nullptr;
   float *                  P = nullptr;
   float *                  AP = nullptr;
-  float *                  A = nullptr; // BP accumulator / FP transpose scratch
-  void *                   fps = nullptr; // forward projector scratch (transposed and quad copies)
-  float *                  At = nullptr;
+  void *                   scratch = nullptr; // projector scratch (copies and accumulators of the volume)
   double *                 scal = nullptr; // rr, rr0, alpha, beta, pAp
   double *                 partial = nullptr;
   float *                  x = nullptr; // the iterate (caller's buffer)
@@ -360,10 +358,10 @@ grid_for(long long n)
 cudaError_t
 apply_A(rtkb_cg * c, const float * in, float * out, cudaStream_t st)
 {
-  cudaError_t e = rtkb::joseph_forward_launch(c->args, in, c->fps, nullptr, c->tmp, c->W, st);
+  cudaError_t e = rtkb::joseph_forward_launch(c->args, in, c->scratch, nullptr, c->tmp, c->W, st);
   if (e != cudaSuccess)
     return e;
-  return rtkb::joseph_back_launch(c->args, c->tmp, c->A, c->At, nullptr, out, c->tikhonov != 0.f ? in : nullptr,
+  return rtkb::joseph_back_launch(c->args, c->tmp, c->scratch, nullptr, out, c->tikhonov != 0.f ? in : nullptr,
                                   c->tikhonov, st);
 }
 
@@ -489,8 +487,8 @@ rtkb_cg_create(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_
     auto         up = [](size_t b) { return (b + 255) & ~size_t(255); };
     const size_t tb = up(tab.size() * sizeof(RayProj)), pb = up((size_t)c->npix * 4), vb = up((size_t)c->nvox * 4);
     const size_t sb = up(8 * sizeof(double)), rb = up(kRedBlocks * sizeof(double));
-    const size_t fb = up(joseph_forward_scratch_bytes(c->nvox));
-    const size_t total = tb + 2 * pb + 5 * vb + sb + rb + fb;
+    const size_t fb = up(std::max(joseph_forward_scratch_bytes(c->nvox), joseph_back_scratch_bytes(c->nvox)));
+    const size_t total = tb + 2 * pb + 3 * vb + sb + rb + fb;
     cudaError_t  e = cudaMalloc(&c->mem, total);
     if (e == cudaSuccess && c->use_graph)
       e = cudaStreamCreateWithFlags(&c->cap, cudaStreamNonBlocking);
@@ -512,15 +510,11 @@ rtkb_cg_create(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_
     m += vb;
     c->AP = reinterpret_cast<float *>(m);
     m += vb;
-    c->A = reinterpret_cast<float *>(m);
-    m += vb;
-    c->At = reinterpret_cast<float *>(m);
-    m += vb;
     c->scal = reinterpret_cast<double *>(m);
     m += sb;
     c->partial = reinterpret_cast<double *>(m);
     m += rb;
-    c->fps = m;
+    c->scratch = m;
     e = cudaMemcpy(c->tab, tab.data(), tab.size() * sizeof(RayProj), cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
       e = cudaMemset(c->scal, 0, sb);
@@ -623,7 +617,7 @@ rtkb_cg_start(rtkb_cg * c, const float * d_proj, const float * d_weights, int di
     fill_kernel<<<grid_for(c->npix), 256, 0, st>>>(c->W, 1.f, c->npix);
   // R = B = BP(W .* p)
   mul_kernel<<<grid_for(c->npix), 256, 0, st>>>(c->tmp, d_proj, c->W, c->npix);
-  const cudaError_t e = joseph_back_launch(c->args, c->tmp, c->A, c->At, nullptr, c->R, nullptr, 0.f, st);
+  const cudaError_t e = joseph_back_launch(c->args, c->tmp, c->scratch, nullptr, c->R, nullptr, 0.f, st);
   if (e != cudaSuccess)
     return cuda_fail(e, "CG start");
   return start_from_rhs(c, st);

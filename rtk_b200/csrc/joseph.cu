@@ -7,14 +7,12 @@
 // marchers behind CUDA_forward_project and CUDA_ray_cast_back_project, which
 // use fixed-step trilinear texture sampling instead of Joseph's scheme.
 //
-// One thread per detector pixel.  The forward projector's grid runs every
+// One thread per detector pixel.  Both projectors' grids run every
 // projection of a band of 8 detector rows before the next band (blockIdx.y =
 // projection, blockIdx.z = row band): detector rows run along the volume's y
-// axis, so the blocks in flight read one y-slab of the volume, which stays in
-// L2 across projections (its quad copies are 4x the volume).  The back
-// projector keeps projection-major order (blockIdx.z = projection): with
-// many projections in flight over one slab, their reductions queue on the
-// same L2 lines (1.4x slower on 256^3 x 360).  The ray set-up
+// axis, so the blocks in flight touch one y-slab of the volume, which stays
+// in L2 across projections (the quad copies and quad accumulators are 4x the
+// volume).  The ray set-up
 // (pixel and source in volume index coordinates, main direction, box
 // clipping, rint() slice bounds, residual weights) is FP64 exactly as RTK
 // computes it; the two border steps
@@ -340,12 +338,28 @@ red_add(float * p, float v)
   asm volatile("red.global.add.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
 }
 
-__global__ void __launch_bounds__(256)
-joseph_back_kernel(JosephArgs a, const float * __restrict__ proj, float * A, float * At)
+__device__ __forceinline__ void
+red_add4(float4 * p, float4 v)
+{
+  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w)
+               : "memory");
+}
+
+// Back projector: the border steps splat into the scalar accumulators A (or
+// At, transposed); the middle steps of main-z (main-x) rays add their four
+// weights with one 16-byte vector reduction into the quad accumulator QAN
+// (QAT), laid out as the forward projector's quad copies: element e collects
+// the contributions to (f(a,b), f(a,b+1), f(a+1,b), f(a+1,b+1)) of the 2 x 2
+// neighbourhood at e.  The fold kernel adds each voxel's four quad entries.
+// Rays with main direction y keep four scalar reductions into A.  64
+// registers (4 CTAs per SM) keep more reductions in flight.
+template <typename Off>
+__global__ void __launch_bounds__(256, 4)
+joseph_back_kernel(JosephArgs a, const float * __restrict__ proj, float * A, float * At, float4 * QAN, float4 * QAT)
 {
   const int u = blockIdx.x * 32 + (threadIdx.x & 31);
-  const int v = blockIdx.y * 8 + (threadIdx.x >> 5);
-  const int s = blockIdx.z;
+  const int v = blockIdx.z * 8 + (threadIdx.x >> 5);
+  const int s = blockIdx.y;
   if (u >= a.nu || v >= a.nv)
     return;
   const float val = __ldg(proj + ((long long)s * a.nv + v) * a.nu + u);
@@ -371,33 +385,55 @@ joseph_back_kernel(JosephArgs a, const float * __restrict__ proj, float * A, flo
 #pragma unroll
   for (int q = 0; q < 4; q++)
     red_add(vol + o[q], (float)(f * wt[q]));
-  const int       nmid = abs(r.fs - r.ns) - 1;
-  const float     x0 = (float)(r.curx + r.stepx - w.bx), y0 = (float)(r.cury + r.stepy - w.by);
-  const float     sx = (float)r.stepx, sy = (float)r.stepy, cf = (float)c;
-  const int       xmax = max(w.nxp - 2, 0), ymax = max(w.nyp - 2, 0);
-  const long long ox1 = (w.nxp > 1) ? w.ox : 0, oy1 = (w.nyp > 1) ? w.oy : 0;
-  float *         slice = vol + (long long)(r.ns + r.dz - w.bz) * w.oz;
-  const long long dslice = r.dz * w.oz;
-  for (int i = 0; i < nmid; i++, slice += dslice)
-  {
-    const float x = fmaf((float)i, sx, x0), y = fmaf((float)i, sy, y0);
-    int         ix = (int)floorf(x), iy = (int)floorf(y);
-    ix = min(max(ix, 0), xmax);
-    iy = min(max(iy, 0), ymax);
-    const float lx = x - ix, ly = y - iy;
-    float *     q = slice + ix * w.ox + iy * w.oy;
-    const float cy0 = cf * (1.f - ly), cy1 = cf * ly;
-    red_add(q, cy0 * (1.f - lx));
-    red_add(q + ox1, cy0 * lx);
-    red_add(q + oy1, cy1 * (1.f - lx));
-    red_add(q + ox1 + oy1, cy1 * lx);
-  }
+  const int nmid = abs(r.fs - r.ns) - 1;
+  // the last border step goes first, so the FP64 ray state is dead in the loop
   const int last = r.ns + r.dz * (nmid + 1);
   border_taps(a, r, w, last, r.curx + (nmid + 1) * r.stepx, r.cury + (nmid + 1) * r.stepy, o, wt);
   f = c * (r.resE + 0.5);
 #pragma unroll
   for (int q = 0; q < 4; q++)
     red_add(vol + o[q], (float)(f * wt[q]));
+  const float     x0 = (float)(r.curx + r.stepx - w.bx), y0 = (float)(r.cury + r.stepy - w.by);
+  const float     sx = (float)r.stepx, sy = (float)r.stepy, cf = (float)c;
+  const int       xmax = max(w.nxp - 2, 0), ymax = max(w.nyp - 2, 0);
+  const Off       ox = (Off)w.ox, oy = (Off)w.oy;
+  const long long first = (long long)(r.ns + r.dz - w.bz) * w.oz, dslice = r.dz * w.oz;
+  if (r.main != 1)
+  {
+    // one-voxel in-plane axes: the "+1" neighbour is the voxel itself
+    const bool ca = w.nxp == 1, cb = w.nyp == 1;
+    float4 *   slice = (w.transposed ? QAT : QAN) + first;
+    for (int i = 0; i < nmid; i++, slice += dslice)
+    {
+      const float x = fmaf((float)i, sx, x0), y = fmaf((float)i, sy, y0);
+      const int   ix = min(max((int)floorf(x), 0), xmax), iy = min(max((int)floorf(y), 0), ymax);
+      const float lx = x - ix, ly = y - iy;
+      const float cy0 = cf * (1.f - ly), cy1 = cf * ly;
+      float4      q = make_float4(cy0 * (1.f - lx), cy1 * (1.f - lx), cy0 * lx, cy1 * lx);
+      if (ca)
+        q = make_float4(q.x + q.z, q.y + q.w, 0.f, 0.f);
+      if (cb)
+        q = make_float4(q.x + q.y, 0.f, q.z + q.w, 0.f);
+      red_add4(slice + ((Off)ix * ox + (Off)iy * oy), q);
+    }
+  }
+  else
+  {
+    const Off ox1 = (w.nxp > 1) ? ox : 0, oy1 = (w.nyp > 1) ? oy : 0;
+    float *   slice = vol + first;
+    for (int i = 0; i < nmid; i++, slice += dslice)
+    {
+      const float x = fmaf((float)i, sx, x0), y = fmaf((float)i, sy, y0);
+      const int   ix = min(max((int)floorf(x), 0), xmax), iy = min(max((int)floorf(y), 0), ymax);
+      const float lx = x - ix, ly = y - iy;
+      float *     q = slice + ((Off)ix * ox + (Off)iy * oy);
+      const float cy0 = cf * (1.f - ly), cy1 = cf * ly;
+      red_add(q, cy0 * (1.f - lx));
+      red_add(q + ox1, cy0 * lx);
+      red_add(q + oy1, cy1 * (1.f - lx));
+      red_add(q + ox1 + oy1, cy1 * lx);
+    }
+  }
 }
 
 // T[x][y][z] = V[z][y][x] (32x32 shared-memory tiles in the x-z plane)
@@ -426,8 +462,9 @@ transpose_zx_kernel(const float * __restrict__ V, float * __restrict__ T, int nx
 // out[z][y][x] = in[z][y][x] + A[z][y][x] + At[x][y][z] (+ tau * x[z][y][x]);
 // in and x may be null.
 __global__ void __launch_bounds__(256)
-fold_transposed_kernel(const float * in, const float * __restrict__ A, const float * __restrict__ At, float * out,
-                       int nx, int ny, int nz, const float * __restrict__ xv, float tau)
+fold_transposed_kernel(const float * in, const float * __restrict__ A, const float * __restrict__ At,
+                       const float4 * __restrict__ QAN, const float4 * __restrict__ QAT, float * out, int nx, int ny,
+                       int nz, const float * __restrict__ xv, float tau)
 {
   __shared__ float tile[32][33];
   const int        y = blockIdx.y;
@@ -437,7 +474,20 @@ fold_transposed_kernel(const float * in, const float * __restrict__ A, const flo
   {
     const int x = x0 + k, z = z0 + tx;
     if (x < nx && z < nz)
-      tile[k][tx] = At[((long long)x * ny + y) * nz + z];
+    {
+      // transposed quads: a = y (stride nz), b = z (stride 1)
+      const long long t = ((long long)x * ny + y) * nz + z;
+      float           r = At[t] + QAT[t].x;
+      if (z > 0)
+        r += QAT[t - 1].y;
+      if (y > 0)
+      {
+        r += QAT[t - nz].z;
+        if (z > 0)
+          r += QAT[t - nz - 1].w;
+      }
+      tile[k][tx] = r;
+    }
   }
   __syncthreads();
   for (int k = ty; k < 32; k += 8)
@@ -445,8 +495,18 @@ fold_transposed_kernel(const float * in, const float * __restrict__ A, const flo
     const int z = z0 + k, x = x0 + tx;
     if (z < nz && x < nx)
     {
+      // natural quads: a = x (stride 1), b = y (stride nx)
       const long long o = ((long long)z * ny + y) * nx + x;
-      float           r = A[o] + tile[tx][k];
+      float           r = A[o] + QAN[o].x;
+      if (y > 0)
+        r += QAN[o - nx].y;
+      if (x > 0)
+      {
+        r += QAN[o - 1].z;
+        if (y > 0)
+          r += QAN[o - nx - 1].w;
+      }
+      r += tile[tx][k];
       if (in)
         r += in[o];
       if (xv)
@@ -559,21 +619,34 @@ joseph_forward_launch(const JosephArgs & a, const float * V, void * scratch, con
   return cudaGetLastError();
 }
 
+size_t
+joseph_back_scratch_bytes(long long nvox)
+{
+  return 2 * (((size_t)nvox * sizeof(float) + 255) / 256 * 256) + 2 * (size_t)nvox * sizeof(float4);
+}
+
 cudaError_t
-joseph_back_launch(const JosephArgs & a, const float * proj, float * A, float * At, const float * vin, float * vout,
+joseph_back_launch(const JosephArgs & a, const float * proj, void * scratch, const float * vin, float * vout,
                    const float * x, float tau, cudaStream_t st)
 {
   const int       nx = a.n[0], ny = a.n[1], nz = a.n[2];
   const long long nvox = (long long)nx * ny * nz;
-  cudaError_t     e = cudaMemsetAsync(A, 0, nvox * sizeof(float), st);
-  if (e == cudaSuccess)
-    e = cudaMemsetAsync(At, 0, nvox * sizeof(float), st);
+  const size_t    vb = ((size_t)nvox * sizeof(float) + 255) / 256 * 256;
+  char *          m = static_cast<char *>(scratch);
+  float *         A = reinterpret_cast<float *>(m);
+  float *         At = reinterpret_cast<float *>(m + vb);
+  float4 *        QAN = reinterpret_cast<float4 *>(m + 2 * vb);
+  float4 *        QAT = QAN + nvox;
+  cudaError_t     e = cudaMemsetAsync(scratch, 0, joseph_back_scratch_bytes(nvox), st);
   if (e != cudaSuccess)
     return e;
-  const dim3 grid((unsigned)((a.nu + 31) / 32), (unsigned)((a.nv + 7) / 8), (unsigned)a.np);
-  joseph_back_kernel<<<grid, 256, 0, st>>>(a, proj, A, At);
+  const dim3 grid((unsigned)((a.nu + 31) / 32), (unsigned)a.np, (unsigned)((a.nv + 7) / 8));
+  if (nvox < (1ll << 31))
+    joseph_back_kernel<int><<<grid, 256, 0, st>>>(a, proj, A, At, QAN, QAT);
+  else
+    joseph_back_kernel<long long><<<grid, 256, 0, st>>>(a, proj, A, At, QAN, QAT);
   const dim3 tg((unsigned)(((nx + 31) / 32) * ((nz + 31) / 32)), (unsigned)ny);
-  fold_transposed_kernel<<<tg, 256, 0, st>>>(vin, A, At, vout, nx, ny, nz, x, tau);
+  fold_transposed_kernel<<<tg, 256, 0, st>>>(vin, A, At, QAN, QAT, vout, nx, ny, nz, x, tau);
   return cudaGetLastError();
 }
 
@@ -656,17 +729,16 @@ rtkb_joseph_back_project(const rtkb_geometry * g, const rtkb_image_desc * vol, c
     cudaStream_t    st = static_cast<cudaStream_t>(stream);
     const long long nvox = num_pixels(*vol);
     const size_t    tbytes = (tab.size() * sizeof(RayProj) + 255) & ~size_t(255);
-    const size_t    vbytes = (size_t)nvox * sizeof(float);
     void *          scratch = nullptr;
-    RTKB_CUDA_TRY(cudaMallocAsync(&scratch, tbytes + 2 * vbytes, st));
+    RTKB_CUDA_TRY(cudaMallocAsync(&scratch, tbytes + joseph_back_scratch_bytes(nvox), st));
     RayProj *   d_tab = static_cast<RayProj *>(scratch);
-    float *     d_a = reinterpret_cast<float *>(static_cast<char *>(scratch) + tbytes);
+    void *      d_a = static_cast<char *>(scratch) + tbytes;
     cudaError_t e = cudaMemcpyAsync(d_tab, tab.data(), tab.size() * sizeof(RayProj), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
     {
       JosephArgs a;
       joseph_args(a, *vol, *proj, d_tab);
-      e = joseph_back_launch(a, d_proj, d_a, d_a + nvox, d_vol_in, d_vol_out, nullptr, 0.f, st);
+      e = joseph_back_launch(a, d_proj, d_a, d_vol_in, d_vol_out, nullptr, 0.f, st);
     }
     rc = (e == cudaSuccess) ? RTKB_OK : cuda_fail(e, "joseph back projection");
     cudaError_t fe = cudaFreeAsync(scratch, st);

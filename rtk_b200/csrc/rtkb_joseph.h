@@ -40,8 +40,11 @@ size_t      joseph_forward_scratch_bytes(long long nvox);
 cudaError_t joseph_forward_launch(const JosephArgs & a, const float * V, void * scratch, const float * pin,
                                   float * pout, const float * w, cudaStream_t st);
 // Enqueue the back projector: vout = vin + BP(proj) + tau * x; vin, x may be
-// null.  A, At: zero-initialised here, scratch of the volume's size each.
-cudaError_t joseph_back_launch(const JosephArgs & a, const float * proj, float * A, float * At, const float * vin,
+// null.  scratch: joseph_back_scratch_bytes(voxels) bytes, 256-byte aligned,
+// zeroed here (scalar and quad accumulators, natural and transposed); at
+// least joseph_forward_scratch_bytes, so one buffer serves both projectors.
+size_t      joseph_back_scratch_bytes(long long nvox);
+cudaError_t joseph_back_launch(const JosephArgs & a, const float * proj, void * scratch, const float * vin,
                                float * vout, const float * x, float tau, cudaStream_t st);
 
 } // namespace rtkb

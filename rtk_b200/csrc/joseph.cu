@@ -414,7 +414,21 @@ joseph_back_kernel(JosephArgs a, const float * __restrict__ proj, float * A, flo
         q = make_float4(q.x + q.z, q.y + q.w, 0.f, 0.f);
       if (cb)
         q = make_float4(q.x + q.y, 0.f, q.z + q.w, 0.f);
-      red_add4(slice + ((Off)ix * ox + (Off)iy * oy), q);
+      float4 *       dst = slice + ((Off)ix * ox + (Off)iy * oy);
+      // lanes 2k and 2k+1 (neighbouring pixels of one row) often hit the same
+      // quad: the even lane then adds both, the odd lane sends nothing
+      const unsigned act = __activemask();
+      const int      lane = threadIdx.x & 31;
+      const bool     pa = (act >> (lane ^ 1)) & 1u;
+      const unsigned long long pk = __shfl_xor_sync(act, (unsigned long long)dst, 1);
+      const float4   pq = make_float4(__shfl_xor_sync(act, q.x, 1), __shfl_xor_sync(act, q.y, 1),
+                                      __shfl_xor_sync(act, q.z, 1), __shfl_xor_sync(act, q.w, 1));
+      const bool     same = pa && pk == (unsigned long long)dst;
+      if (same && (lane & 1))
+        continue;
+      if (same)
+        q = make_float4(q.x + pq.x, q.y + pq.y, q.z + pq.z, q.w + pq.w);
+      red_add4(dst, q);
     }
   }
   else

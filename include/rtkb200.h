@@ -112,6 +112,21 @@ int rtkb_fdk_backproject(const rtkb_geometry * g, const rtkb_image_desc * vol, c
                          const float * d_proj, const float * d_vol_in, float * d_vol_out, void * stream);
 int rtkb_voxel_backproject(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
                            const float * d_proj, const float * d_vol_in, float * d_vol_out, void * stream);
+/* rtk::FDKBackProjectionImageFilter on host buffers, as RTK's CUDA pipeline
+ * runs it from CPU images: the stack is streamed to the device in subsets of
+ * `chunk` projections (include/rtkFDKConeBeamReconstructionFilter.hxx:116-157;
+ * chunk <= 0: an eighth of the stack), each copied on an internal stream into
+ * one of two device staging buffers while the previous one is backprojected
+ * into a device copy of the volume; the last chunk is backprojected in four
+ * z-slabs, each copied back while the next is computed (the host<->device
+ * transfers ITK's CudaDataManager makes around
+ * rtkCudaFDKBackProjectionImageFilter.cxx:34-125, overlapped).  h_vol_in may
+ * be NULL (zero volume).  Asynchronous on `stream`
+ * like cudaMemcpyAsync: h_vol_out is written when the stream reaches the end
+ * of this work.  Pinned host buffers give full copy bandwidth and overlap. */
+int rtkb_fdk_backproject_host(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
+                              const float * h_proj, const float * h_vol_in, float * h_vol_out, int chunk,
+                              void * stream);
 /* Batched backprojection (no counterpart in the reference): many independent
  * problems of uneven sizes in one persistent launch -- CTAs take (problem,
  * tile) work items from a shared queue until it is empty.  Each problem is a

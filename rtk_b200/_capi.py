@@ -91,6 +91,7 @@ SIGNATURES = {
     "rtkb_geometry_set_radius_cylindrical_detector": (C.c_int, [_G, C.c_double]),
     "rtkb_backprojection_matrices": (C.c_int, [_G, _IM, _IM, C.c_int, C.c_int, C.c_int, _D, _I]),
     "rtkb_fdk_backproject": (C.c_int, [_G, _IM, _IM, _V, _V, _V, _V]),
+    "rtkb_fdk_backproject_host": (C.c_int, [_G, _IM, _IM, _V, _V, _V, C.c_int, _V]),
     "rtkb_voxel_backproject": (C.c_int, [_G, _IM, _IM, _V, _V, _V, _V]),
     "rtkb_backproject_matrices": (C.c_int, [_I, _I, C.c_int, _D, _I, C.c_int, _V, _V, _V, _V]),
     "rtkb_probe_smem_gather": (C.c_int, [C.c_int, C.c_int, _V, _V]),

@@ -1265,6 +1265,182 @@ rtkb_fdk_backproject(const rtkb_geometry * g, const rtkb_image_desc * vol, const
   }
 }
 
+// Host-buffer FDK backprojection: the stack streams through two device
+// staging buffers in chunks (RTK's projection subsets,
+// include/rtkFDKConeBeamReconstructionFilter.hxx:116-157), each copied on an
+// internal stream while the previous chunk is backprojected in place into a
+// device copy of the volume on the caller's stream; the last chunk runs slab
+// by slab in z, each slab copied back while the next is backprojected.
+namespace rtkb
+{
+static int
+fdk_backproject_host(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
+                     const float * h_proj, const float * h_vol_in, float * h_vol_out, int chunk, cudaStream_t st)
+{
+  std::string why;
+  if (!g)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "Geometry has not been set.");
+  if (!desc_valid(vol, why) || !desc_valid(proj, why))
+    return fail(RTKB_ERR_INVALID_ARGUMENT, why);
+  const int       nproj = proj->size[2];
+  const long long per = (long long)proj->size[0] * proj->size[1];
+  const long long slice = (long long)vol->size[0] * vol->size[1];
+  const int       nz = vol->size[2];
+  const long long nvox = slice * nz;
+  if (!h_vol_out || (nproj > 0 && !h_proj))
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "null buffer");
+  if (proj->index[2] < 0 || (long long)proj->index[2] + nproj > (long long)g->g.p.size())
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "Mismatch between the number of projections and the geometry entries.");
+  if (chunk <= 0)
+    chunk = std::max(1, (nproj + 7) / 8);
+  chunk = std::max(1, std::min(chunk, std::max(nproj, 1)));
+  const int nchunks = (nproj + chunk - 1) / chunk;
+  // the last chunk runs as kSlabs z-slabs (multiples of 16 slices), each slab
+  // copied back while the next one is backprojected
+  constexpr int kSlabs = 4;
+  int           zb[kSlabs + 1];
+  int           nslab = 0;
+  zb[0] = 0;
+  for (int q = 1; q <= kSlabs; q++)
+  {
+    const int z = (q == kSlabs) ? nz : std::min(nz, (int)((long long)nz * q / kSlabs / 16 * 16));
+    if (z > zb[nslab])
+      zb[++nslab] = z;
+  }
+  if (nchunks == 0)
+    nslab = 1, zb[1] = nz;
+  const size_t vbytes = ((size_t)nvox * sizeof(float) + 255) / 256 * 256;
+  const size_t sbytes = ((size_t)chunk * per * sizeof(float) + 255) / 256 * 256;
+  const int    nstage = std::min(nchunks, 2);
+  constexpr int kEvents = 6 + kSlabs; // allocation, chunk copied (2), stage free (2), copies done, slab done
+  cudaStream_t  cs = nullptr;
+  cudaEvent_t   ev[kEvents] = {};
+  void *        mem = nullptr;
+  int           rc = RTKB_OK;
+  RTKB_CUDA_TRY(cudaMallocAsync(&mem, vbytes + nstage * sbytes, st));
+  do
+  {
+    cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    for (int i = 0; i < kEvents && e == cudaSuccess; i++)
+      e = cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming);
+    if (e != cudaSuccess)
+    {
+      rc = cuda_fail(e, "stream/event creation");
+      break;
+    }
+    float * d_vol = static_cast<float *>(mem);
+    float * stage[2] = { reinterpret_cast<float *>(static_cast<char *>(mem) + vbytes),
+                         reinterpret_cast<float *>(static_cast<char *>(mem) + vbytes + sbytes) };
+    // the copy stream may touch the allocation once the caller's stream has
+    // made it (stream-ordered allocation)
+    e = cudaEventRecord(ev[0], st);
+    if (e == cudaSuccess)
+      e = cudaStreamWaitEvent(cs, ev[0], 0);
+    if (e == cudaSuccess)
+      e = h_vol_in ? cudaMemcpyAsync(d_vol, h_vol_in, (size_t)nvox * sizeof(float), cudaMemcpyHostToDevice, st)
+                   : cudaMemsetAsync(d_vol, 0, (size_t)nvox * sizeof(float), st);
+    if (e != cudaSuccess)
+    {
+      rc = cuda_fail(e, "volume initialisation");
+      break;
+    }
+    for (int k = 0; k < nchunks && rc == RTKB_OK; k++)
+    {
+      const int b = k & 1;
+      const int first = k * chunk, nk = std::min(chunk, nproj - first);
+      if (k >= 2)
+        e = cudaStreamWaitEvent(cs, ev[3 + b], 0); // the backprojection of chunk k-2 is done with stage b
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(stage[b], h_proj + (size_t)first * per, (size_t)nk * per * sizeof(float),
+                            cudaMemcpyHostToDevice, cs);
+      if (e == cudaSuccess)
+        e = cudaEventRecord(ev[1 + b], cs);
+      if (e == cudaSuccess)
+        e = cudaStreamWaitEvent(st, ev[1 + b], 0);
+      if (e != cudaSuccess)
+      {
+        rc = cuda_fail(e, "chunk copy");
+        break;
+      }
+      rtkb_image_desc sub = *proj;
+      sub.size[2] = nk;
+      sub.index[2] = proj->index[2] + first;
+      if (k < nchunks - 1)
+      {
+        rc = backproject_geometry(g, vol, &sub, static_cast<const float *>(stage[b]), d_vol, d_vol, st, true);
+        if (rc == RTKB_OK && (e = cudaEventRecord(ev[3 + b], st)) != cudaSuccess)
+          rc = cuda_fail(e, "cudaEventRecord");
+        continue;
+      }
+      for (int q = 0; q < nslab && rc == RTKB_OK; q++)
+      {
+        // slab q of the volume: a region with its z index offset, as RTK
+        // backprojects a requested region
+        rtkb_image_desc vs = *vol;
+        vs.size[2] = zb[q + 1] - zb[q];
+        vs.index[2] = vol->index[2] + zb[q];
+        float * d_slab = d_vol + (size_t)zb[q] * slice;
+        rc = backproject_geometry(g, &vs, &sub, static_cast<const float *>(stage[b]), d_slab, d_slab, st, true);
+        if (rc != RTKB_OK)
+          break;
+        e = cudaEventRecord(ev[6 + q], st);
+        if (e == cudaSuccess)
+          e = cudaStreamWaitEvent(cs, ev[6 + q], 0);
+        if (e == cudaSuccess)
+          e = cudaMemcpyAsync(h_vol_out + (size_t)zb[q] * slice, d_slab, (size_t)vs.size[2] * slice * sizeof(float),
+                              cudaMemcpyDeviceToHost, cs);
+        if (e != cudaSuccess)
+          rc = cuda_fail(e, "slab copy");
+      }
+    }
+    if (rc != RTKB_OK)
+      break;
+    if (nchunks == 0)
+      e = cudaMemcpyAsync(h_vol_out, d_vol, (size_t)nvox * sizeof(float), cudaMemcpyDeviceToHost, st);
+    else
+    {
+      // the caller's stream completes after the last slab's copy
+      e = cudaEventRecord(ev[5], cs);
+      if (e == cudaSuccess)
+        e = cudaStreamWaitEvent(st, ev[5], 0);
+    }
+    if (e != cudaSuccess)
+      rc = cuda_fail(e, "volume copy");
+  } while (0);
+  if (rc != RTKB_OK && cs)
+  {
+    // join whatever the copy stream has enqueued before the buffers are freed
+    if (cudaEventRecord(ev[5], cs) == cudaSuccess)
+      cudaStreamWaitEvent(st, ev[5], 0);
+  }
+  // events and the copy stream are released once their work completes
+  for (int i = 0; i < kEvents; i++)
+    if (ev[i])
+      cudaEventDestroy(ev[i]);
+  if (cs)
+    cudaStreamDestroy(cs);
+  cudaError_t fe = cudaFreeAsync(mem, st);
+  if (rc == RTKB_OK && fe != cudaSuccess)
+    rc = cuda_fail(fe, "cudaFreeAsync");
+  return rc;
+}
+} // namespace rtkb
+
+extern "C" int
+rtkb_fdk_backproject_host(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
+                          const float * h_proj, const float * h_vol_in, float * h_vol_out, int chunk, void * stream)
+{
+  try
+  {
+    return rtkb::fdk_backproject_host(g, vol, proj, h_proj, h_vol_in, h_vol_out, chunk,
+                                      static_cast<cudaStream_t>(stream));
+  }
+  catch (...)
+  {
+    return rtkb::fail(RTKB_ERR_OUT_OF_MEMORY, "host allocation failed");
+  }
+}
+
 extern "C" int
 rtkb_voxel_backproject(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
                        const float * d_proj, const float * d_vol_in, float * d_vol_out, void * stream)

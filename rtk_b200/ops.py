@@ -314,6 +314,37 @@ def conjugate_gradient(geometry, vol_desc, proj_desc, proj, x, niter, rel_residu
     return it.value, rel.value
 
 
+def _host_ptr(t, what):
+    torch = _torch()
+    if not isinstance(t, torch.Tensor) or t.is_cuda:
+        raise TypeError(f"{what}: expected a host (CPU) tensor")
+    if t.dtype != torch.float32 or not t.is_contiguous():
+        raise TypeError(f"{what}: expected a contiguous float32 tensor")
+    return C.c_void_p(t.data_ptr())
+
+
+def fdk_backproject_host(geometry, vol_desc, proj_desc, proj, vol_in=None, out=None, chunk=0, stream=None):
+    """rtkb_fdk_backproject_host: FDK backprojection of a host (CPU) stack into a
+    host volume, the stack streamed to the GPU in chunks of `chunk`
+    projections (0: an eighth of the stack) whose copies overlap the
+    backprojection of the previous chunk; the volume comes back slab by slab
+    while the last chunk is backprojected.  vol_in None means a zero volume.
+    Asynchronous on `stream`: synchronise it before reading `out`.  Pinned
+    tensors (pin_memory=True) give full copy bandwidth and overlap."""
+    torch = _torch()
+    _check_shape(proj, proj_desc, "projections")
+    if vol_in is not None:
+        _check_shape(vol_in, vol_desc, "volume")
+    if out is None:
+        out = torch.empty(shape_of(vol_desc), dtype=torch.float32, pin_memory=True)
+    _check_shape(out, vol_desc, "output")
+    vin = _host_ptr(vol_in, "volume") if vol_in is not None else None
+    check(load().rtkb_fdk_backproject_host(geometry.handle, C.byref(vol_desc), C.byref(proj_desc),
+                                           _host_ptr(proj, "projections"), vin, _host_ptr(out, "output"),
+                                           int(chunk), _stream(stream)))
+    return out
+
+
 def fdk_backproject_static_scratch(geometry, vol_desc, proj_desc, proj, vol_in, out=None, stream=None):
     """rtkb_fdk_backproject_static_scratch: FDK backprojection that allocates no
     device memory (stacks of at most 2048 projections; see include/rtkb200.h)."""

@@ -139,3 +139,42 @@ def test_fdk_bp_full_size_c2_region_and_linearity(rtkb, oracle):
     lin = torch.linalg.vector_norm(v12 - (0.5 * v1 + 2.0 * v2)) / torch.linalg.vector_norm(v12)
     assert lin.item() < 1e-5
     assert rtkb.ops.device_status() == 0
+
+
+@pytest.mark.parametrize("chunk,vol_init", [(0, False), (7, True), (1000, True), (1, False)])
+def test_fdk_bp_host_buffers_streamed_in_chunks(rtkb, oracle, chunk, vol_init):
+    """rtkb_fdk_backproject_host: host stack and volume, the stack streamed in
+    chunks (ragged last chunk with 7, one chunk with 1000, one projection per
+    chunk with 1), projection indices offset as in a subset of a longer scan."""
+    import torch
+
+    params = _circular(50, 1000.0, 1536.0, pox=12.0)
+    gl, go = pair_geometry(rtkb, oracle, params)
+    vd, vo = pair_image(rtkb, oracle, (40, 36, 44), (2.5,) * 3, index=(2, -3, 1))
+    pd, po = pair_image(rtkb, oracle, (160, 120, 45), (1.0,) * 3, index=(-80, 0, 3))
+    rng = np.random.default_rng(11 + chunk)
+    p = rng.uniform(-1.0, 1.0, size=oracle.shape_of(po)).astype(np.float32).astype(np.float64)
+    v0 = (rng.uniform(-1.0, 1.0, size=oracle.shape_of(vo)) if vol_init else np.zeros(oracle.shape_of(vo)))
+    v0 = v0.astype(np.float32).astype(np.float64)
+    ref = oracle.backproject(go, vo, po, p, v0, fdk=True)
+    hp = torch.from_numpy(p.astype(np.float32)).pin_memory()
+    hv = torch.from_numpy(v0.astype(np.float32)).pin_memory() if vol_init else None
+    out = rtkb.ops.fdk_backproject_host(gl, vd, pd, hp, hv, chunk=chunk)
+    torch.cuda.synchronize()
+    assert rtkb.ops.device_status() == 0
+    got = out.numpy().astype(np.float64)
+    dev = to_np(rtkb.ops.fdk_backproject(gl, vd, pd, to_gpu(p), to_gpu(v0)))
+    assert rel_l2(got, ref) < REL_L2_TOL, rel_l2(got, ref)
+    # chunking only regroups the FP32 sums per voxel: the running volume is
+    # rounded to FP32 once per chunk (45 times with chunk=1, ~1.7e-6)
+    assert rel_l2(got, dev) < 5e-6, rel_l2(got, dev)
+
+
+def test_fdk_bp_host_rejects_device_tensors(rtkb, oracle):
+    import torch
+
+    gl, go = pair_geometry(rtkb, oracle, _circular(4, 1000.0, 1500.0))
+    vd, vo = pair_image(rtkb, oracle, (8, 8, 8), (1.0,) * 3)
+    pd, po = pair_image(rtkb, oracle, (16, 16, 4), (1.0,) * 3)
+    with pytest.raises(TypeError):
+        rtkb.ops.fdk_backproject_host(gl, vd, pd, torch.zeros((4, 16, 16), device="cuda"))

@@ -348,9 +348,9 @@ def cg_seconds_to_residual(torch, rtkb, stream, tol=1e-3, max_iter=300, learned_
     counts = torch.poisson(i0 * torch.exp(-clean), generator=gen).clamp_(min=1.0)
     p = (-torch.log(counts / i0)).contiguous()
 
-    def solve(net):
+    def solve(net, storage="fp32", max_it=max_iter):
         x = torch.zeros((256, 256, 256), device="cuda")
-        cg = rtkb.ops.ConjugateGradient(g, vd, pd)
+        cg = rtkb.ops.ConjugateGradient(g, vd, pd, storage=storage)
         if net is not None:
             cg.set_preconditioner(net, history=8)
         torch.cuda.synchronize()
@@ -359,7 +359,7 @@ def cg_seconds_to_residual(torch, rtkb, stream, tol=1e-3, max_iter=300, learned_
         cg.start(p, x, stream=stream)
         rr, rr0, it = cg.residual(stream)
         hist = [1.0]
-        while rr > tol * tol * rr0 and it < max_iter:
+        while rr > tol * tol * rr0 and it < max_it:
             cg.iterate(1, stream)
             rr, rr0, it = cg.residual(stream)
             hist.append(round((rr / rr0) ** 0.5, 6))
@@ -378,6 +378,37 @@ def cg_seconds_to_residual(torch, rtkb, stream, tol=1e-3, max_iter=300, learned_
            "config": "256^3 @1mm <- 360 x 512x384 @0.8mm, SID 1000, SDD 1536, 20 random ellipsoids, "
                      "Poisson I0=5e4, Joseph pair, FP32 vectors / FP64 scalars, CUDA graph per iteration",
            "learned_pcg": None}
+
+    # precision study: 30 iterations in one graph replay loop per storage
+    # variant (FP32, or BF16 r, p, A p and projection temporary), and each
+    # variant's seconds to the residual target
+    def fixed(storage, niter=30):
+        x = torch.zeros((256, 256, 256), device="cuda")
+        cg = rtkb.ops.ConjugateGradient(g, vd, pd, storage=storage)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        cg.start(p, x, stream=stream)
+        cg.iterate(niter, stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        rr, rr0, it = cg.residual(stream)
+        cg.close()
+        return e0.elapsed_time(e1) / 1e3, (rr / rr0) ** 0.5, x
+
+    study = {"iterations": 30}
+    t32, r32, x32 = fixed("fp32")
+    t16, r16, x16 = fixed("bf16")
+    bsecs, bit, brel, bper, _, _ = solve(None, storage="bf16", max_it=100)
+    study["fp32"] = {"seconds": t32, "relative_residual": r32}
+    study["bf16"] = {"seconds": t16, "relative_residual": r16,
+                     "rel_diff_to_fp32": float((x16 - x32).double().norm() / x32.double().norm()),
+                     "seconds_to_rel_residual_1e-3": bsecs, "iterations_to_1e-3": bit if bsecs else None,
+                     "residual_history": solve.hist}
+    study["oracle_error"] = ("per-variant error against the FP64 oracle's CG: "
+                             "tests/test_gpu_cg.py::test_cg_bf16_storage_precision_against_oracle")
+    del x32, x16
+    out["precision_study"] = study
     if not learned_pcg:
         return out
     from rtk_b200 import learned

@@ -241,6 +241,10 @@ typedef struct rtkb_cg_params
 {
   double tikhonov;       /* Tikhonov weight (RTK's SetTikhonov), 0 = none */
   int    use_cuda_graph; /* 1: replay a captured iteration graph */
+  int    storage;        /* 0: FP32; 1: BF16 storage of the normal-equation vectors (r, p, A p) and of the
+                            projection-domain temporary, FP32 arithmetic and FP64 dots, alpha and beta
+                            (no counterpart in the reference; the iterate stays in the caller's FP32
+                            buffer; no learned preconditioner) */
 } rtkb_cg_params;
 typedef struct rtkb_cg rtkb_cg;
 int  rtkb_cg_create(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,

@@ -15,6 +15,7 @@
 // with the Joseph pair, W the displaced-detector weights of the input weights
 // (no padding).  Vectors are FP32; the dot products (deterministic two-pass
 // reductions), alpha and beta are FP64 and never leave the device.
+#include "rtkb_elem.cuh"
 #include "rtkb_joseph.h"
 
 #include <cfloat>
@@ -27,12 +28,13 @@ struct rtkb_cg
   rtkb::JosephArgs         args{};
   float                    tikhonov = 0.f;
   bool                     use_graph = true;
+  bool                     bf16 = false; // R, P, AP and tmp stored as bfloat16 (FP32 arithmetic)
   long long                nvox = 0, npix = 0;
   void *                   mem = nullptr; // one device allocation for everything below
   rtkb::RayProj *          tab = nullptr;
   float *                  W = nullptr; // weights (null: all ones)
   float *                  tmp = nullptr;
-  float *                  R = nullptr;
+  float *                  R = nullptr; // R, P, AP hold bfloat16 values in a BF16 plan
   float *                  P = nullptr;
   float *                  AP = nullptr;
   void *                   scratch = nullptr; // projector scratch (copies and accumulators of the volume)
@@ -69,6 +71,9 @@ bool        unet_reserved_for(const rtkb_unet * u, int nx, int ny, int nz);
 
 namespace
 {
+using rtkb::Elem;
+using rtkb::ld_elem;
+using rtkb::st_elem;
 
 constexpr int kRedBlocks = 148 * 4;
 constexpr int kRedThreads = 256;
@@ -102,30 +107,32 @@ block_sum(double v)
 }
 
 // partial[b] = sum over block b's fixed slice of a[i] * b[i] (FP64)
+template <typename S>
 __global__ void __launch_bounds__(kRedThreads)
-dot_partial_kernel(const float * __restrict__ a, const float * __restrict__ b, long long n, double * partial)
+dot_partial_kernel(const S * __restrict__ a, const S * __restrict__ b, long long n, double * partial)
 {
   double s = 0.;
   for (long long i = blockIdx.x * (long long)kRedThreads + threadIdx.x; i < n; i += (long long)kRedBlocks * kRedThreads)
-    s = fma((double)a[i], (double)b[i], s);
+    s = fma((double)ld_elem(a, i), (double)ld_elem(b, i), s);
   s = block_sum(s);
   if (threadIdx.x == 0)
     partial[blockIdx.x] = s;
 }
 
-// x += alpha p; r -= alpha ap; partial of <r, r>
+// x += alpha p; r -= alpha ap; partial of <r, r> (of r as stored)
+template <typename S>
 __global__ void __launch_bounds__(kRedThreads)
-update_xr_kernel(float * __restrict__ x, float * __restrict__ r, const float * __restrict__ p,
-                 const float * __restrict__ ap, long long n, const double * __restrict__ scal, double * partial)
+update_xr_kernel(float * __restrict__ x, S * __restrict__ r, const S * __restrict__ p, const S * __restrict__ ap,
+                 long long n, const double * __restrict__ scal, double * partial)
 {
   const double alpha = scal[S_ALPHA];
   const float  af = (float)alpha;
   double       s = 0.;
   for (long long i = blockIdx.x * (long long)kRedThreads + threadIdx.x; i < n; i += (long long)kRedBlocks * kRedThreads)
   {
-    x[i] = fmaf(af, p[i], x[i]);
-    const float ri = fmaf(-af, ap[i], r[i]);
-    r[i] = ri;
+    x[i] = fmaf(af, ld_elem(p, i), x[i]);
+    st_elem(r, i, fmaf(-af, ld_elem(ap, i), ld_elem(r, i)));
+    const float ri = ld_elem(r, i);
     s = fma((double)ri, (double)ri, s);
   }
   s = block_sum(s);
@@ -183,32 +190,35 @@ finalize_start_kernel(const double * partial, double * scal)
 }
 
 // p = r + beta p
+template <typename S>
 __global__ void __launch_bounds__(256)
-update_p_kernel(float * __restrict__ p, const float * __restrict__ r, long long n, const double * __restrict__ scal)
+update_p_kernel(S * __restrict__ p, const S * __restrict__ r, long long n, const double * __restrict__ scal)
 {
   const float beta = (float)scal[S_BETA];
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    p[i] = fmaf(beta, p[i], r[i]);
+    st_elem(p, i, fmaf(beta, ld_elem(p, i), ld_elem(r, i)));
 }
 
 // r = r - ap; p = r (start: R0 = B - A x0)
+template <typename S>
 __global__ void __launch_bounds__(256)
-start_rp_kernel(float * __restrict__ r, float * __restrict__ p, const float * __restrict__ ap, long long n)
+start_rp_kernel(S * __restrict__ r, S * __restrict__ p, const S * __restrict__ ap, long long n)
 {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
   {
-    const float v = r[i] - ap[i];
-    r[i] = v;
-    p[i] = v;
+    const float v = ld_elem(r, i) - ld_elem(ap, i);
+    st_elem(r, i, v);
+    st_elem(p, i, v);
   }
 }
 
-// out = a .* b (b may be null: copy)
+// out = a .* b (b may be null: copy), stored as TO
+template <typename TO>
 __global__ void __launch_bounds__(256)
-mul_kernel(float * __restrict__ out, const float * __restrict__ a, const float * __restrict__ b, long long n)
+mul_kernel(TO * __restrict__ out, const float * __restrict__ a, const float * __restrict__ b, long long n)
 {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    out[i] = b ? a[i] * b[i] : a[i];
+    st_elem(out, i, b ? a[i] * b[i] : a[i]);
 }
 
 __global__ void __launch_bounds__(256)
@@ -354,29 +364,53 @@ grid_for(long long n)
   return (unsigned)std::min<long long>((n + 255) / 256, 148LL * 16);
 }
 
-// A P -> AP (uses tmp, A, At)
-cudaError_t
-apply_A(rtkb_cg * c, const float * in, float * out, cudaStream_t st)
+Elem
+storage(const rtkb_cg * c)
 {
-  cudaError_t e = rtkb::joseph_forward_launch(c->args, in, c->scratch, nullptr, c->tmp, c->W, st);
+  return c->bf16 ? Elem::BF16 : Elem::F32;
+}
+
+template <typename S>
+S *
+as(float * p)
+{
+  return reinterpret_cast<S *>(p);
+}
+
+// out = A in (uses tmp and the projector scratch); in and out have storage
+// ie and oe, tmp the plan's storage
+cudaError_t
+apply_A(rtkb_cg * c, const void * in, Elem ie, void * out, Elem oe, cudaStream_t st)
+{
+  cudaError_t e = rtkb::joseph_forward_launch(c->args, in, ie, c->scratch, nullptr, c->tmp, storage(c), c->W, st);
   if (e != cudaSuccess)
     return e;
-  return rtkb::joseph_back_launch(c->args, c->tmp, c->scratch, nullptr, out, c->tikhonov != 0.f ? in : nullptr,
-                                  c->tikhonov, st);
+  return rtkb::joseph_back_launch(c->args, c->tmp, storage(c), c->scratch, nullptr, out, oe,
+                                  c->tikhonov != 0.f ? in : nullptr, ie, c->tikhonov, st);
+}
+
+template <typename S>
+cudaError_t
+enqueue_iteration_t(rtkb_cg * c, cudaStream_t st)
+{
+  S *         P = as<S>(c->P);
+  S *         AP = as<S>(c->AP);
+  S *         R = as<S>(c->R);
+  cudaError_t e = apply_A(c, P, storage(c), AP, storage(c), st);
+  if (e != cudaSuccess)
+    return e;
+  dot_partial_kernel<S><<<kRedBlocks, kRedThreads, 0, st>>>(P, AP, c->nvox, c->partial);
+  finalize_alpha_kernel<<<1, 32, 0, st>>>(c->partial, c->scal);
+  update_xr_kernel<S><<<kRedBlocks, kRedThreads, 0, st>>>(c->x, R, P, AP, c->nvox, c->scal, c->partial);
+  finalize_beta_kernel<<<1, 32, 0, st>>>(c->partial, c->scal);
+  update_p_kernel<S><<<grid_for(c->nvox), 256, 0, st>>>(P, R, c->nvox, c->scal);
+  return cudaGetLastError();
 }
 
 cudaError_t
 enqueue_iteration(rtkb_cg * c, cudaStream_t st)
 {
-  cudaError_t e = apply_A(c, c->P, c->AP, st);
-  if (e != cudaSuccess)
-    return e;
-  dot_partial_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(c->P, c->AP, c->nvox, c->partial);
-  finalize_alpha_kernel<<<1, 32, 0, st>>>(c->partial, c->scal);
-  update_xr_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(c->x, c->R, c->P, c->AP, c->nvox, c->scal, c->partial);
-  finalize_beta_kernel<<<1, 32, 0, st>>>(c->partial, c->scal);
-  update_p_kernel<<<grid_for(c->nvox), 256, 0, st>>>(c->P, c->R, c->nvox, c->scal);
-  return cudaGetLastError();
+  return c->bf16 ? enqueue_iteration_t<__nv_bfloat16>(c, st) : enqueue_iteration_t<float>(c, st);
 }
 
 // One truncated flexible-PCG iteration: Ap; alpha = <p,r>/<p,Ap>;
@@ -385,12 +419,12 @@ enqueue_iteration(rtkb_cg * c, cudaStream_t st)
 cudaError_t
 enqueue_pcg_iteration(rtkb_cg * c, cudaStream_t st)
 {
-  cudaError_t e = apply_A(c, c->P, c->AP, st);
+  cudaError_t e = apply_A(c, c->P, Elem::F32, c->AP, Elem::F32, st);
   if (e != cudaSuccess)
     return e;
   dot2_partial_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(c->P, c->AP, c->P, c->R, c->nvox, c->partial, c->partial2);
   finalize_alpha_pcg_kernel<<<1, 32, 0, st>>>(c->partial, c->partial2, c->scal);
-  update_xr_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(c->x, c->R, c->P, c->AP, c->nvox, c->scal, c->partial);
+  update_xr_kernel<float><<<kRedBlocks, kRedThreads, 0, st>>>(c->x, c->R, c->P, c->AP, c->nvox, c->scal, c->partial);
   finalize_rr_kernel<<<1, 32, 0, st>>>(c->partial, c->scal);
   store_direction_kernel<<<grid_for(c->nvox), 256, 0, st>>>(c->P, c->AP, c->Ph, c->APh, c->nvox, c->m, c->scal,
                                                              c->hist);
@@ -475,6 +509,7 @@ rtkb_cg_create(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_
     c->proj = *proj;
     c->tikhonov = params ? (float)params->tikhonov : 0.f;
     c->use_graph = params ? params->use_cuda_graph != 0 : true;
+    c->bf16 = params ? params->storage == 1 : false;
     c->nvox = num_pixels(*vol);
     c->npix = num_pixels(*proj);
     std::vector<RayProj> tab;
@@ -547,11 +582,20 @@ int
 start_from_rhs(rtkb_cg * c, cudaStream_t st)
 {
   using namespace rtkb;
-  cudaError_t e = apply_A(c, c->x, c->AP, st);
+  cudaError_t e = apply_A(c, c->x, Elem::F32, c->AP, storage(c), st);
   if (e != cudaSuccess)
     return cuda_fail(e, "CG start");
-  start_rp_kernel<<<grid_for(c->nvox), 256, 0, st>>>(c->R, c->P, c->AP, c->nvox);
-  dot_partial_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(c->R, c->R, c->nvox, c->partial);
+  if (c->bf16)
+  {
+    using B = __nv_bfloat16;
+    start_rp_kernel<B><<<grid_for(c->nvox), 256, 0, st>>>(as<B>(c->R), as<B>(c->P), as<B>(c->AP), c->nvox);
+    dot_partial_kernel<B><<<kRedBlocks, kRedThreads, 0, st>>>(as<B>(c->R), as<B>(c->R), c->nvox, c->partial);
+  }
+  else
+  {
+    start_rp_kernel<float><<<grid_for(c->nvox), 256, 0, st>>>(c->R, c->P, c->AP, c->nvox);
+    dot_partial_kernel<float><<<kRedBlocks, kRedThreads, 0, st>>>(c->R, c->R, c->nvox, c->partial);
+  }
   finalize_start_kernel<<<1, 32, 0, st>>>(c->partial, c->scal);
   RTKB_CUDA_TRY(cudaGetLastError());
   if (c->pcg_active)
@@ -559,7 +603,7 @@ start_from_rhs(rtkb_cg * c, cudaStream_t st)
     // empty direction history; z0 = M(r0), p0 = z0 (run eagerly once, before any capture)
     RTKB_CUDA_TRY(cudaMemsetAsync(c->hist, 0, (2 * c->m + 1) * sizeof(double), st));
     RTKB_CUDA_TRY(unet_apply(c->net, c->R, c->Z, st));
-    mul_kernel<<<grid_for(c->nvox), 256, 0, st>>>(c->P, c->Z, nullptr, c->nvox);
+    mul_kernel<float><<<grid_for(c->nvox), 256, 0, st>>>(c->P, c->Z, nullptr, c->nvox);
     RTKB_CUDA_TRY(cudaGetLastError());
     double h[2] = { 0., 0. };
     RTKB_CUDA_TRY(cudaMemcpyAsync(h, c->scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -615,9 +659,13 @@ rtkb_cg_start(rtkb_cg * c, const float * d_proj, const float * d_weights, int di
     RTKB_CUDA_TRY(cudaMemcpyAsync(c->W, d_weights, (size_t)c->npix * 4, cudaMemcpyDeviceToDevice, st));
   else
     fill_kernel<<<grid_for(c->npix), 256, 0, st>>>(c->W, 1.f, c->npix);
-  // R = B = BP(W .* p)
-  mul_kernel<<<grid_for(c->npix), 256, 0, st>>>(c->tmp, d_proj, c->W, c->npix);
-  const cudaError_t e = joseph_back_launch(c->args, c->tmp, c->scratch, nullptr, c->R, nullptr, 0.f, st);
+  // R = B = BP(W .* p), tmp and R in the plan's storage
+  if (c->bf16)
+    mul_kernel<__nv_bfloat16><<<grid_for(c->npix), 256, 0, st>>>(as<__nv_bfloat16>(c->tmp), d_proj, c->W, c->npix);
+  else
+    mul_kernel<float><<<grid_for(c->npix), 256, 0, st>>>(c->tmp, d_proj, c->W, c->npix);
+  const cudaError_t e = joseph_back_launch(c->args, c->tmp, storage(c), c->scratch, nullptr, c->R, storage(c), nullptr,
+                                           Elem::F32, 0.f, st);
   if (e != cudaSuccess)
     return cuda_fail(e, "CG start");
   return start_from_rhs(c, st);
@@ -631,7 +679,11 @@ rtkb_cg_start_rhs(rtkb_cg * c, const float * d_b, float * d_x, void * stream)
     return fail(RTKB_ERR_INVALID_ARGUMENT, "null argument");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   reset_run(c, d_x);
-  RTKB_CUDA_TRY(cudaMemcpyAsync(c->R, d_b, (size_t)c->nvox * 4, cudaMemcpyDeviceToDevice, st));
+  if (c->bf16)
+    mul_kernel<__nv_bfloat16><<<grid_for(c->nvox), 256, 0, st>>>(as<__nv_bfloat16>(c->R), d_b, nullptr, c->nvox);
+  else
+    RTKB_CUDA_TRY(cudaMemcpyAsync(c->R, d_b, (size_t)c->nvox * 4, cudaMemcpyDeviceToDevice, st));
+  RTKB_CUDA_TRY(cudaGetLastError());
   return start_from_rhs(c, st);
 }
 
@@ -664,7 +716,7 @@ rtkb_cg_iterate(rtkb_cg * c, int n, void * stream)
       {
         c->pcg_active = false;
         c->fallback_iteration = c->iterations;
-        mul_kernel<<<grid_for(c->nvox), 256, 0, st>>>(c->P, c->R, nullptr, c->nvox); // restart: p = r
+        mul_kernel<float><<<grid_for(c->nvox), 256, 0, st>>>(c->P, c->R, nullptr, c->nvox); // restart: p = r
         RTKB_CUDA_TRY(cudaGetLastError());
       }
       continue;
@@ -744,6 +796,8 @@ rtkb_cg_set_preconditioner(rtkb_cg * c, rtkb_unet * net, int history)
     return fail(RTKB_ERR_INVALID_ARGUMENT, "null plan");
   if (net && (history < 1 || history > kMaxHistory))
     return fail(RTKB_ERR_INVALID_ARGUMENT, "history must be in 1..16");
+  if (net && c->bf16)
+    return fail(RTKB_ERR_UNSUPPORTED, "the learned preconditioner runs on FP32 plans only");
   drop_graphs(c);
   c->x = nullptr; // must be started again
   c->net = nullptr;
@@ -804,6 +858,6 @@ rtkb_cg_apply_operator(rtkb_cg * c, const float * d_in, float * d_out, void * st
   using namespace rtkb;
   if (!c || !d_in || !d_out || d_in == d_out)
     return fail(RTKB_ERR_INVALID_ARGUMENT, "null or aliased argument");
-  const cudaError_t e = apply_A(c, d_in, d_out, static_cast<cudaStream_t>(stream));
+  const cudaError_t e = apply_A(c, d_in, Elem::F32, d_out, Elem::F32, static_cast<cudaStream_t>(stream));
   return e == cudaSuccess ? RTKB_OK : cuda_fail(e, "normal operator");
 }

@@ -20,6 +20,7 @@
 // positions x0 + i*step (no accumulated drift).  Rays whose main direction is
 // x read (or scatter into) a z<->x transposed copy of the volume, so that
 // neighbouring rays touch neighbouring addresses for every main direction.
+#include "rtkb_elem.cuh"
 #include "rtkb_joseph.h"
 #include "rtkb_ptx.cuh"
 
@@ -30,6 +31,8 @@
 namespace
 {
 using rtkb::JosephArgs;
+using rtkb::ld_elem;
+using rtkb::st_elem;
 using rtkb::RayProj;
 
 struct Ray
@@ -231,11 +234,11 @@ border_taps(const JosephArgs & a, const Ray & r, const View & w, int sl, double 
 // 64 registers give 4 CTAs per SM: the loop is bound by gather latency, and
 // the FP64 ray state is dead before it starts (the last border step is taken
 // first; the sums are still added in ray order).
-template <typename Off>
+template <typename Off, typename TP>
 __global__ void __launch_bounds__(256, 4)
 joseph_forward_kernel(JosephArgs a, const float * __restrict__ V, const float * __restrict__ Vt,
-                      const float4 * __restrict__ QN, const float4 * __restrict__ QT, const float * pin,
-                      float * pout, const float * __restrict__ weights)
+                      const float4 * __restrict__ QN, const float4 * __restrict__ QT, const TP * pin, TP * pout,
+                      const float * __restrict__ weights)
 {
   const int u = blockIdx.x * 32 + (threadIdx.x & 31);
   const int v = blockIdx.z * 8 + (threadIdx.x >> 5);
@@ -246,8 +249,8 @@ joseph_forward_kernel(JosephArgs a, const float * __restrict__ V, const float * 
   Ray             r;
   if (!setup_ray(a, a.P[s], u, v, s, true, r))
   {
-    const float base = pin ? pin[po] : 0.f;
-    pout[po] = weights ? base * __ldg(weights + po) : base;
+    const float base = pin ? ld_elem(pin, po) : 0.f;
+    st_elem(pout, po, weights ? base * __ldg(weights + po) : base);
     return;
   }
   const View    w = view_for(a, r);
@@ -312,9 +315,9 @@ joseph_forward_kernel(JosephArgs a, const float * __restrict__ V, const float * 
     sum += acc;
     sum += lastv;
   }
-  const float base = pin ? pin[po] : 0.f;
+  const float base = pin ? ld_elem(pin, po) : 0.f;
   const float val = base + (float)(sum * r.norm);
-  pout[po] = weights ? val * __ldg(weights + po) : val;
+  st_elem(pout, po, weights ? val * __ldg(weights + po) : val);
 }
 
 // Quads of a volume laid out [k][m][f] (f fastest): element e = (k m_n + m)
@@ -353,16 +356,16 @@ red_add4(float4 * p, float4 v)
 // neighbourhood at e.  The fold kernel adds each voxel's four quad entries.
 // Rays with main direction y keep four scalar reductions into A.  64
 // registers (4 CTAs per SM) keep more reductions in flight.
-template <typename Off>
+template <typename Off, typename TP>
 __global__ void __launch_bounds__(256, 4)
-joseph_back_kernel(JosephArgs a, const float * __restrict__ proj, float * A, float * At, float4 * QAN, float4 * QAT)
+joseph_back_kernel(JosephArgs a, const TP * __restrict__ proj, float * A, float * At, float4 * QAN, float4 * QAT)
 {
   const int u = blockIdx.x * 32 + (threadIdx.x & 31);
   const int v = blockIdx.z * 8 + (threadIdx.x >> 5);
   const int s = blockIdx.y;
   if (u >= a.nu || v >= a.nv)
     return;
-  const float val = __ldg(proj + ((long long)s * a.nv + v) * a.nu + u);
+  const float val = ld_elem(proj, ((long long)s * a.nv + v) * a.nu + u);
   Ray         r;
   if (!setup_ray(a, a.P[s], u, v, s, false, r))
     return;
@@ -475,10 +478,11 @@ transpose_zx_kernel(const float * __restrict__ V, float * __restrict__ T, int nx
 
 // out[z][y][x] = in[z][y][x] + A[z][y][x] + At[x][y][z] (+ tau * x[z][y][x]);
 // in and x may be null.
+template <typename TV, typename TX>
 __global__ void __launch_bounds__(256)
-fold_transposed_kernel(const float * in, const float * __restrict__ A, const float * __restrict__ At,
-                       const float4 * __restrict__ QAN, const float4 * __restrict__ QAT, float * out, int nx, int ny,
-                       int nz, const float * __restrict__ xv, float tau)
+fold_transposed_kernel(const TV * in, const float * __restrict__ A, const float * __restrict__ At,
+                       const float4 * __restrict__ QAN, const float4 * __restrict__ QAT, TV * out, int nx, int ny,
+                       int nz, const TX * __restrict__ xv, float tau)
 {
   __shared__ float tile[32][33];
   const int        y = blockIdx.y;
@@ -522,10 +526,10 @@ fold_transposed_kernel(const float * in, const float * __restrict__ A, const flo
       }
       r += tile[tx][k];
       if (in)
-        r += in[o];
+        r += ld_elem(in, o);
       if (xv)
-        r = fmaf(tau, xv[o], r);
-      out[o] = r;
+        r = fmaf(tau, ld_elem(xv, o), r);
+      st_elem(out, o, r);
     }
   }
 }
@@ -604,22 +608,39 @@ joseph_args(JosephArgs & a, const rtkb_image_desc & vol, const rtkb_image_desc &
   }
 }
 
+// Scratch of both projectors (one buffer serves both): two volume-sized
+// float regions and two quad regions.  Forward: z<->x transposed copy, FP32
+// copy of a BF16 volume, natural and transposed quad copies.  Back: natural
+// and transposed scalar accumulators, natural and transposed quad
+// accumulators.
 size_t
 joseph_forward_scratch_bytes(long long nvox)
 {
-  return ((size_t)nvox * sizeof(float) + 255) / 256 * 256 + 2 * (size_t)nvox * sizeof(float4);
+  return 2 * (((size_t)nvox * sizeof(float) + 255) / 256 * 256) + 2 * (size_t)nvox * sizeof(float4);
 }
 
+size_t
+joseph_back_scratch_bytes(long long nvox)
+{
+  return joseph_forward_scratch_bytes(nvox);
+}
+
+namespace
+{
+__global__ void __launch_bounds__(256)
+widen_kernel(const __nv_bfloat16 * __restrict__ in, float * __restrict__ out, long long n)
+{
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = __bfloat162float(in[i]);
+}
+
+template <typename TP>
 cudaError_t
-joseph_forward_launch(const JosephArgs & a, const float * V, void * scratch, const float * pin, float * pout,
-                      const float * w, cudaStream_t st)
+forward_launch(const JosephArgs & a, const float * V, float * Vt, float4 * QN, float4 * QT, const TP * pin, TP * pout,
+               const float * w, cudaStream_t st)
 {
   const int       nx = a.n[0], ny = a.n[1], nz = a.n[2];
   const long long nvox = (long long)nx * ny * nz;
-  float *         Vt = static_cast<float *>(scratch);
-  float4 *        QN = reinterpret_cast<float4 *>(static_cast<char *>(scratch) +
-                                                  ((size_t)nvox * sizeof(float) + 255) / 256 * 256);
-  float4 *        QT = QN + nvox;
   const dim3      tg((unsigned)(((nx + 31) / 32) * ((nz + 31) / 32)), (unsigned)ny);
   transpose_zx_kernel<<<tg, 256, 0, st>>>(V, Vt, nx, ny, nz);
   const unsigned qg = (unsigned)std::min<long long>((nvox + 255) / 256, 148LL * 32);
@@ -627,21 +648,16 @@ joseph_forward_launch(const JosephArgs & a, const float * V, void * scratch, con
   quad_kernel<<<qg, 256, 0, st>>>(Vt, QT, nz, ny, nvox, false); // a = y, b = z
   const dim3 grid((unsigned)((a.nu + 31) / 32), (unsigned)a.np, (unsigned)((a.nv + 7) / 8));
   if (nvox < (1ll << 31))
-    joseph_forward_kernel<int><<<grid, 256, 0, st>>>(a, V, Vt, QN, QT, pin, pout, w);
+    joseph_forward_kernel<int, TP><<<grid, 256, 0, st>>>(a, V, Vt, QN, QT, pin, pout, w);
   else
-    joseph_forward_kernel<long long><<<grid, 256, 0, st>>>(a, V, Vt, QN, QT, pin, pout, w);
+    joseph_forward_kernel<long long, TP><<<grid, 256, 0, st>>>(a, V, Vt, QN, QT, pin, pout, w);
   return cudaGetLastError();
 }
 
-size_t
-joseph_back_scratch_bytes(long long nvox)
-{
-  return 2 * (((size_t)nvox * sizeof(float) + 255) / 256 * 256) + 2 * (size_t)nvox * sizeof(float4);
-}
-
+template <typename TP, typename TV, typename TX>
 cudaError_t
-joseph_back_launch(const JosephArgs & a, const float * proj, void * scratch, const float * vin, float * vout,
-                   const float * x, float tau, cudaStream_t st)
+back_launch(const JosephArgs & a, const TP * proj, void * scratch, const TV * vin, TV * vout, const TX * x, float tau,
+            cudaStream_t st)
 {
   const int       nx = a.n[0], ny = a.n[1], nz = a.n[2];
   const long long nvox = (long long)nx * ny * nz;
@@ -656,12 +672,72 @@ joseph_back_launch(const JosephArgs & a, const float * proj, void * scratch, con
     return e;
   const dim3 grid((unsigned)((a.nu + 31) / 32), (unsigned)a.np, (unsigned)((a.nv + 7) / 8));
   if (nvox < (1ll << 31))
-    joseph_back_kernel<int><<<grid, 256, 0, st>>>(a, proj, A, At, QAN, QAT);
+    joseph_back_kernel<int, TP><<<grid, 256, 0, st>>>(a, proj, A, At, QAN, QAT);
   else
-    joseph_back_kernel<long long><<<grid, 256, 0, st>>>(a, proj, A, At, QAN, QAT);
+    joseph_back_kernel<long long, TP><<<grid, 256, 0, st>>>(a, proj, A, At, QAN, QAT);
   const dim3 tg((unsigned)(((nx + 31) / 32) * ((nz + 31) / 32)), (unsigned)ny);
-  fold_transposed_kernel<<<tg, 256, 0, st>>>(vin, A, At, QAN, QAT, vout, nx, ny, nz, x, tau);
+  fold_transposed_kernel<TV, TX><<<tg, 256, 0, st>>>(vin, A, At, QAN, QAT, vout, nx, ny, nz, x, tau);
   return cudaGetLastError();
+}
+} // namespace
+
+cudaError_t
+joseph_forward_launch(const JosephArgs & a, const void * V, Elem ve, void * scratch, const void * pin, void * pout,
+                      Elem pe, const float * w, cudaStream_t st)
+{
+  const long long nvox = (long long)a.n[0] * a.n[1] * a.n[2];
+  const size_t    vb = ((size_t)nvox * sizeof(float) + 255) / 256 * 256;
+  char *          m = static_cast<char *>(scratch);
+  float *         Vt = reinterpret_cast<float *>(m);
+  float4 *        QN = reinterpret_cast<float4 *>(m + 2 * vb);
+  float4 *        QT = QN + nvox;
+  const float *   V32 = static_cast<const float *>(V);
+  if (ve == Elem::BF16)
+  {
+    float * w32 = reinterpret_cast<float *>(m + vb);
+    widen_kernel<<<(unsigned)std::min<long long>((nvox + 255) / 256, 148LL * 32), 256, 0, st>>>(
+      static_cast<const __nv_bfloat16 *>(V), w32, nvox);
+    V32 = w32;
+  }
+  if (pe == Elem::BF16)
+    return forward_launch(a, V32, Vt, QN, QT, static_cast<const __nv_bfloat16 *>(pin),
+                          static_cast<__nv_bfloat16 *>(pout), w, st);
+  return forward_launch(a, V32, Vt, QN, QT, static_cast<const float *>(pin), static_cast<float *>(pout), w, st);
+}
+
+namespace
+{
+template <typename TP, typename TV>
+cudaError_t
+back_x(const JosephArgs & a, const TP * proj, void * scratch, const void * vin, void * vout, const void * x, Elem xe,
+       float tau, cudaStream_t st)
+{
+  const TV * vi = static_cast<const TV *>(vin);
+  TV *       vo = static_cast<TV *>(vout);
+  if (xe == Elem::BF16)
+    return back_launch(a, proj, scratch, vi, vo, static_cast<const __nv_bfloat16 *>(x), tau, st);
+  return back_launch(a, proj, scratch, vi, vo, static_cast<const float *>(x), tau, st);
+}
+
+template <typename TP>
+cudaError_t
+back_v(const JosephArgs & a, const void * proj, void * scratch, const void * vin, void * vout, Elem ve, const void * x,
+       Elem xe, float tau, cudaStream_t st)
+{
+  const TP * p = static_cast<const TP *>(proj);
+  if (ve == Elem::BF16)
+    return back_x<TP, __nv_bfloat16>(a, p, scratch, vin, vout, x, xe, tau, st);
+  return back_x<TP, float>(a, p, scratch, vin, vout, x, xe, tau, st);
+}
+} // namespace
+
+cudaError_t
+joseph_back_launch(const JosephArgs & a, const void * proj, Elem pe, void * scratch, const void * vin, void * vout,
+                   Elem ve, const void * x, Elem xe, float tau, cudaStream_t st)
+{
+  if (pe == Elem::BF16)
+    return back_v<__nv_bfloat16>(a, proj, scratch, vin, vout, ve, x, xe, tau, st);
+  return back_v<float>(a, proj, scratch, vin, vout, ve, x, xe, tau, st);
 }
 
 int

@@ -33,18 +33,40 @@ void joseph_args(JosephArgs & a, const rtkb_image_desc & vol, const rtkb_image_d
 
 int joseph_check(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj);
 
+// Storage type of a volume or projection stack (arithmetic is FP32 either way).
+enum class Elem
+{
+  F32,
+  BF16
+};
+
+// Scratch of either projector: joseph_forward_scratch_bytes(voxels) bytes,
+// 256-byte aligned (equal to joseph_back_scratch_bytes, so one buffer serves
+// both): transposed, widened and quad-expanded copies of the volume for the
+// forward projector, scalar and quad accumulators for the back projector.
+size_t joseph_forward_scratch_bytes(long long nvox);
+size_t joseph_back_scratch_bytes(long long nvox);
+
 // Enqueue the forward projector: pout = w * (pin + FP(V)); pin, w may be null.
-// scratch: joseph_forward_scratch_bytes(voxels) bytes, 256-byte aligned (the
-// z<->x transposed copy and the two quad-expanded copies of the volume).
-size_t      joseph_forward_scratch_bytes(long long nvox);
-cudaError_t joseph_forward_launch(const JosephArgs & a, const float * V, void * scratch, const float * pin,
-                                  float * pout, const float * w, cudaStream_t st);
+// V has storage ve, pin and pout storage pe.
+cudaError_t joseph_forward_launch(const JosephArgs & a, const void * V, Elem ve, void * scratch, const void * pin,
+                                  void * pout, Elem pe, const float * w, cudaStream_t st);
+inline cudaError_t
+joseph_forward_launch(const JosephArgs & a, const float * V, void * scratch, const float * pin, float * pout,
+                      const float * w, cudaStream_t st)
+{
+  return joseph_forward_launch(a, V, Elem::F32, scratch, pin, pout, Elem::F32, w, st);
+}
 // Enqueue the back projector: vout = vin + BP(proj) + tau * x; vin, x may be
-// null.  scratch: joseph_back_scratch_bytes(voxels) bytes, 256-byte aligned,
-// zeroed here (scalar and quad accumulators, natural and transposed); at
-// least joseph_forward_scratch_bytes, so one buffer serves both projectors.
-size_t      joseph_back_scratch_bytes(long long nvox);
-cudaError_t joseph_back_launch(const JosephArgs & a, const float * proj, void * scratch, const float * vin,
-                               float * vout, const float * x, float tau, cudaStream_t st);
+// null.  proj has storage pe, vin and vout storage ve, x storage xe.  Zeroes
+// its accumulators in the scratch.
+cudaError_t joseph_back_launch(const JosephArgs & a, const void * proj, Elem pe, void * scratch, const void * vin,
+                               void * vout, Elem ve, const void * x, Elem xe, float tau, cudaStream_t st);
+inline cudaError_t
+joseph_back_launch(const JosephArgs & a, const float * proj, void * scratch, const float * vin, float * vout,
+                   const float * x, float tau, cudaStream_t st)
+{
+  return joseph_back_launch(a, proj, Elem::F32, scratch, vin, vout, Elem::F32, x, Elem::F32, tau, st);
+}
 
 } // namespace rtkb

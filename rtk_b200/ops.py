@@ -221,18 +221,27 @@ def device_status(stream=None) -> int:
     return st.value
 
 
+def _storage_code(storage):
+    codes = {"fp32": 0, "bf16": 1}
+    if storage not in codes:
+        raise ValueError(f"storage must be one of {sorted(codes)}")
+    return codes[storage]
+
+
 class ConjugateGradient:
     """Plan of rtk::ConjugateGradientConeBeamReconstructionFilter (Joseph pair,
-    FP64 scalars on the device, one CUDA graph per iteration)."""
+    FP64 scalars on the device, one CUDA graph per iteration).  storage="bf16"
+    stores the normal-equation vectors and the projection-domain temporary
+    as bfloat16 (FP32 arithmetic, FP64 dots and step sizes)."""
 
-    def __init__(self, geometry, vol_desc, proj_desc, tikhonov=0.0, use_cuda_graph=True):
+    def __init__(self, geometry, vol_desc, proj_desc, tikhonov=0.0, use_cuda_graph=True, storage="fp32"):
         from ._capi import CgParams
 
         self._lib = load()
         self.geometry = geometry
         self.vol_desc, self.proj_desc = vol_desc, proj_desc
         p = CgParams()
-        p.tikhonov, p.use_cuda_graph = tikhonov, int(use_cuda_graph)
+        p.tikhonov, p.use_cuda_graph, p.storage = tikhonov, int(use_cuda_graph), _storage_code(storage)
         h = C.c_void_p()
         check(self._lib.rtkb_cg_create(geometry.handle, C.byref(vol_desc), C.byref(proj_desc), C.byref(p),
                                        C.byref(h)))
@@ -300,12 +309,12 @@ class ConjugateGradient:
 
 
 def conjugate_gradient(geometry, vol_desc, proj_desc, proj, x, niter, rel_residual=0.0, weights=None,
-                       displaced_detector=True, tikhonov=0.0, use_cuda_graph=True, stream=None):
+                       displaced_detector=True, tikhonov=0.0, use_cuda_graph=True, stream=None, storage="fp32"):
     """Whole CG reconstruction in place on x; returns (iterations, relative residual)."""
     from ._capi import CgParams
 
     p = CgParams()
-    p.tikhonov, p.use_cuda_graph = tikhonov, int(use_cuda_graph)
+    p.tikhonov, p.use_cuda_graph, p.storage = tikhonov, int(use_cuda_graph), _storage_code(storage)
     it, rel = C.c_int(), C.c_double()
     check(load().rtkb_conjugate_gradient(geometry.handle, C.byref(vol_desc), C.byref(proj_desc), C.byref(p),
                                          _ptr(proj), _ptr(weights) if weights is not None else None,

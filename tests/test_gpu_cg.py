@@ -119,3 +119,66 @@ def test_cg_sphere_like_rtkconjugategradientreconstructiontest(rtkb, oracle):
     rtkb.ops.conjugate_gradient(gl, vd, pd, to_gpu(p), x, 5, displaced_detector=True)
     err, psnr, ok = phantoms.check_image_quality(to_np(x), ref, 0.08, 23.0, 2.0)
     assert ok, (err, psnr)
+
+
+# BF16 storage of r, p, A p and the projection temporary rounds each stored
+# value to 8 significant bits (relative 2^-9).  CG in reduced precision loses
+# the conjugacy of its directions, so its iterates drift from the exact ones
+# faster than the rounding itself (4.6e-2 after 6 iterations on this problem,
+# while the residual still falls as fast as in FP32).
+BF16_CG_TOL = 0.1
+
+
+def test_cg_bf16_storage_precision_against_oracle(rtkb, oracle):
+    """Precision study of the storage variants: FP32 and BF16 plans against
+    the FP64 oracle's CG on the same problem, graph and eager BF16 alike."""
+    import torch
+
+    gl, go, vd, vo, pd, po, p = _problem(rtkb, oracle, seed=3)
+    niter = 6
+    ref_x, ref_res = oracle.cg_joseph(go, vo, po, p, niter)
+    errs = {}
+    for storage, graph in (("fp32", True), ("bf16", True), ("bf16", False)):
+        x = torch.zeros(oracle.shape_of(vo), device="cuda")
+        cg = rtkb.ops.ConjugateGradient(gl, vd, pd, storage=storage, use_cuda_graph=graph)
+        cg.start(to_gpu(p), x, displaced_detector=False)
+        res = [cg.residual()[0]]
+        for _ in range(niter):
+            cg.iterate(1)
+            res.append(cg.residual()[0])
+        cg.close()
+        assert rtkb.ops.device_status() == 0
+        assert res[-1] < 0.1 * res[0], res
+        errs[(storage, graph)] = rel_l2(to_np(x), ref_x)
+        errs[(storage, graph, "residual")] = res[-1] / res[0]
+    assert errs[("fp32", True)] < CG_TOL, errs
+    # the BF16 plan's residual falls within a factor 2 of the FP32 plan's
+    assert errs[("bf16", True, "residual")] < 2 * errs[("fp32", True, "residual")], errs
+    # BF16 storage really rounds (error well above FP32's) and stays bounded
+    for graph in (True, False):
+        assert 10 * errs[("fp32", True)] < errs[("bf16", graph)] < BF16_CG_TOL, errs
+
+
+def test_cg_bf16_operator_and_preconditioner_refusal(rtkb, oracle):
+    """The BF16 plan's operator rounds only its projection temporary; the
+    learned preconditioner is refused (FP32 plans only)."""
+    import torch
+
+    from rtk_b200.learned import UNet
+
+    gl, go, vd, vo, pd, po, p = _problem(rtkb, oracle, seed=4)
+    rng = np.random.default_rng(4)
+    e = to_gpu(rng.uniform(-1.0, 1.0, size=oracle.shape_of(vo)))
+    outs = []
+    for storage in ("fp32", "bf16"):
+        cg = rtkb.ops.ConjugateGradient(gl, vd, pd, storage=storage)
+        out = torch.empty_like(e)
+        cg.apply_operator(e, out)
+        outs.append(to_np(out))
+        if storage == "bf16":
+            with pytest.raises(Exception):
+                cg.set_preconditioner(UNet(seed=0))
+        cg.close()
+    d = rel_l2(outs[1], outs[0])
+    assert 1e-5 < d < 1e-2, d
+    assert rtkb.ops.device_status() == 0

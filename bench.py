@@ -321,7 +321,61 @@ def batch_leg(torch, rtkb, stream, n=64, reps=3):
             "one_launch_per_problem_ms": t_seq,
             "one_launch_per_problem_gups": updates / (t_seq / 1e3) / 1e9, "autotuned_config": best,
             "autotune_ms_per_config": [round(t, 3) for t in times],
-            "note": "FDK backprojection part of the batched configuration; the 10-iteration CG part is not batched"}
+            "note": "FDK backprojection part of the batched configuration; its CG part is the batched_cg entry"}
+
+
+def batch_cg_leg(torch, rtkb, stream, n=64, niter=10):
+    """CG half of the batched configuration: n seeded problems (volumes
+    64^3-256^3, 90-360 projections, detectors 128^2-512^2, SID 800-1200 mm),
+    niter CG iterations each with the Joseph pair.  Batched: one CUDA graph
+    launch runs every problem's iterations, each problem on its own branch;
+    against the same plans iterated one problem after another."""
+    import numpy as np
+
+    from rtk_b200._capi import check
+
+    rng = np.random.default_rng(SEED + 8)
+    probs = []
+    samples = 0.0
+    for _ in range(n):
+        nv_ = int(rng.integers(64, 257))
+        npj = int(rng.integers(90, 361))
+        nu = int(rng.integers(32, 129)) * 4
+        nvd = int(rng.integers(128, 513))
+        sid = float(rng.uniform(800, 1200))
+        g = rtkb.geometry.circular(npj, sid, 1.5 * sid)
+        vsp = min(1.0, 0.9 * nu / (nv_ * 1.5))
+        vd = rtkb.make_desc((nv_, nv_, nv_), (vsp,) * 3)
+        pd = rtkb.make_desc((nu, nvd, npj), (1.0, 1.0, 1.0))
+        probs.append((g, vd, pd, torch.rand((npj, nvd, nu), device="cuda"),
+                      torch.zeros((nv_, nv_, nv_), device="cuda"), None, False))
+    batch = rtkb.ops.ConjugateGradientBatch(probs)
+    batch.start(stream)
+    batch.iterate(niter, stream)  # capture and a first replay
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    batch.iterate(niter, stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_batch = e0.elapsed_time(e1)
+    lib = rtkb.load()
+    e0.record(stream)
+    for i in range(n):
+        plan = lib.rtkb_cg_batch_plan(batch._h, i)
+        check(lib.rtkb_cg_iterate(plan, niter, stream.cuda_stream))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_seq = e0.elapsed_time(e1)
+    assert rtkb.ops.device_status(stream) == 0
+    batch.close()
+    del probs
+    return {"workload": f"{n} CG problems x {niter} iterations (Joseph pair), volumes 64^3-256^3, 90-360 "
+                        "projections, detectors 128^2-512^2, SID 800-1200 mm (seeded)",
+            "batched_graph_ms": t_batch, "one_problem_after_another_ms": t_seq,
+            "speedup": t_seq / t_batch if t_batch else None,
+            "note": "one CUDA graph launch with a branch per problem; the Joseph pair is not a persistent "
+                    "multi-problem kernel"}
 
 
 def cg_seconds_to_residual(torch, rtkb, stream, tol=1e-3, max_iter=300, learned_pcg=True):
@@ -740,6 +794,7 @@ def main():
         del proj
         line["joseph_forward"] = joseph_forward_leg(torch, rtkb, lib, stream)
         line["batched"] = batch_leg(torch, rtkb, stream)
+        line["batched_cg"] = batch_cg_leg(torch, rtkb, stream)
         line["cg"] = cg_seconds_to_residual(torch, rtkb, stream)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:

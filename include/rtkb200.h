@@ -269,6 +269,29 @@ int  rtkb_conjugate_gradient(const rtkb_geometry * g, const rtkb_image_desc * vo
                              const rtkb_cg_params * params, const float * d_proj, const float * d_weights,
                              int displaced_detector, float * d_x, int max_iterations, double relative_residual,
                              int * iterations, double * final_relative_residual, void * stream);
+/* Batched CG (no counterpart in the reference): many independent problems of
+ * uneven sizes, each a full rtkb_cg_start problem (own geometry,
+ * descriptions, stack, weights and iterate).  rtkb_cg_batch_iterate runs
+ * `niter` iterations of every problem as ONE CUDA graph launch: the graph,
+ * captured on the first call for a given niter, holds each problem's
+ * iterations on its own branch, so the problems' kernels run concurrently.
+ * rtkb_cg_batch_plan returns problem i's plan for rtkb_cg_residual. */
+typedef struct rtkb_cg_batch_problem
+{
+  const rtkb_geometry * geometry;
+  rtkb_image_desc       vol, proj;
+  const float *         d_proj;
+  const float *         d_weights; /* may be NULL */
+  int                   displaced_detector;
+  float *               d_x; /* x0 on entry, the iterate afterwards */
+} rtkb_cg_batch_problem;
+typedef struct rtkb_cg_batch rtkb_cg_batch;
+int       rtkb_cg_batch_create(const rtkb_cg_batch_problem * problems, int n, const rtkb_cg_params * params,
+                               rtkb_cg_batch ** batch);
+int       rtkb_cg_batch_start(rtkb_cg_batch * batch, const rtkb_cg_batch_problem * problems, void * stream);
+int       rtkb_cg_batch_iterate(rtkb_cg_batch * batch, int niter, void * stream);
+rtkb_cg * rtkb_cg_batch_plan(rtkb_cg_batch * batch, int i);
+void      rtkb_cg_batch_destroy(rtkb_cg_batch * batch);
 /* d_out = A d_in with the plan's operator (weights W = 1 until rtkb_cg_start
  * sets them).  Used to generate (A e, e) training pairs for the learned
  * preconditioner.  No reference counterpart (RTK's operator is internal to

@@ -159,6 +159,22 @@ SIGNATURES.update({
     "rtkb_fdk_backproject_static_scratch": (C.c_int, [_G, _IM, _IM, _V, _V, _V, _V]),
 })
 
+class CgBatchProblem(C.Structure):
+    """rtkb_cg_batch_problem."""
+
+    _fields_ = [("geometry", C.c_void_p), ("vol", ImageDesc), ("proj", ImageDesc), ("d_proj", C.c_void_p),
+                ("d_weights", C.c_void_p), ("displaced_detector", C.c_int), ("d_x", C.c_void_p)]
+
+
+SIGNATURES.update({
+    "rtkb_cg_batch_create": (C.c_int, [C.POINTER(CgBatchProblem), C.c_int, C.POINTER(CgParams),
+                                       C.POINTER(C.c_void_p)]),
+    "rtkb_cg_batch_start": (C.c_int, [_V, C.POINTER(CgBatchProblem), _V]),
+    "rtkb_cg_batch_iterate": (C.c_int, [_V, C.c_int, _V]),
+    "rtkb_cg_batch_plan": (C.c_void_p, [_V, C.c_int]),
+    "rtkb_cg_batch_destroy": (None, [_V]),
+})
+
 SIGNATURES.update({
     "rtkb_project_ellipsoids": (C.c_int, [_G, _IM, C.c_int, _D, _V, _V]),
 })

@@ -20,6 +20,7 @@
 
 #include <cfloat>
 #include <cstring>
+#include <vector>
 
 struct rtkb_cg
 {
@@ -860,4 +861,205 @@ rtkb_cg_apply_operator(rtkb_cg * c, const float * d_in, float * d_out, void * st
     return fail(RTKB_ERR_INVALID_ARGUMENT, "null or aliased argument");
   const cudaError_t e = apply_A(c, d_in, Elem::F32, d_out, Elem::F32, static_cast<cudaStream_t>(stream));
   return e == cudaSuccess ? RTKB_OK : cuda_fail(e, "normal operator");
+}
+
+// ---------------------------------------------------------------- batched CG
+// Many independent CG problems (the batched configuration's 10-iteration CG
+// half): one plan per problem, eager (no per-plan graph), and ONE CUDA graph
+// holding every problem's iterations, each problem's chain on its own forked
+// capture stream.  A replay is a single launch; the problems' kernels run
+// concurrently wherever their grids leave the GPU room.
+struct rtkb_cg_batch
+{
+  std::vector<rtkb_cg *>    plans;
+  std::vector<cudaStream_t> streams; // capture branches
+  std::vector<cudaEvent_t>  joins;
+  cudaEvent_t               fork = nullptr;
+  cudaStream_t              cap = nullptr;
+  cudaGraph_t               graph = nullptr;
+  cudaGraphExec_t           exec = nullptr;
+  int                       graph_iterations = 0; // iterations per problem in the captured graph
+  bool                      started = false;
+};
+
+namespace
+{
+void
+drop_batch_graph(rtkb_cg_batch * b)
+{
+  if (b->exec)
+    cudaGraphExecDestroy(b->exec);
+  if (b->graph)
+    cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+  b->graph_iterations = 0;
+}
+
+void
+release_batch(rtkb_cg_batch * b)
+{
+  if (!b)
+    return;
+  drop_batch_graph(b);
+  for (rtkb_cg * c : b->plans)
+    release(c);
+  for (cudaStream_t s : b->streams)
+    cudaStreamDestroy(s);
+  for (cudaEvent_t e : b->joins)
+    cudaEventDestroy(e);
+  if (b->fork)
+    cudaEventDestroy(b->fork);
+  if (b->cap)
+    cudaStreamDestroy(b->cap);
+  delete b;
+}
+
+// capture niter iterations of every plan: fork from the capture stream, one
+// branch per plan, join back
+cudaError_t
+capture_batch(rtkb_cg_batch * b, int niter)
+{
+  cudaError_t e = cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess)
+    return e;
+  cudaError_t ei = cudaEventRecord(b->fork, b->cap);
+  for (size_t i = 0; i < b->plans.size() && ei == cudaSuccess; i++)
+  {
+    ei = cudaStreamWaitEvent(b->streams[i], b->fork, 0);
+    for (int k = 0; k < niter && ei == cudaSuccess; k++)
+      ei = enqueue_iteration(b->plans[i], b->streams[i]);
+    if (ei == cudaSuccess)
+      ei = cudaEventRecord(b->joins[i], b->streams[i]);
+    if (ei == cudaSuccess)
+      ei = cudaStreamWaitEvent(b->cap, b->joins[i], 0);
+  }
+  e = cudaStreamEndCapture(b->cap, &b->graph);
+  if (e == cudaSuccess)
+    e = ei;
+  if (e == cudaSuccess)
+    e = cudaGraphInstantiate(&b->exec, b->graph, 0);
+  if (e == cudaSuccess)
+    b->graph_iterations = niter;
+  return e;
+}
+} // namespace
+
+extern "C" int
+rtkb_cg_batch_create(const rtkb_cg_batch_problem * problems, int n, const rtkb_cg_params * params,
+                     rtkb_cg_batch ** out)
+{
+  using namespace rtkb;
+  if (!out || !problems || n <= 0)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "null argument or empty batch");
+  *out = nullptr;
+  rtkb_cg_params p = params ? *params : rtkb_cg_params{ 0., 1, 0 };
+  p.use_cuda_graph = 0; // the batch captures all plans in one graph
+  rtkb_cg_batch * b = nullptr;
+  try
+  {
+    b = new rtkb_cg_batch();
+    for (int i = 0; i < n; i++)
+    {
+      const rtkb_cg_batch_problem & q = problems[i];
+      if (!q.d_proj || !q.d_x)
+      {
+        release_batch(b);
+        return fail(RTKB_ERR_INVALID_ARGUMENT, "null buffer in batch problem");
+      }
+      rtkb_cg * c = nullptr;
+      const int rc = rtkb_cg_create(q.geometry, &q.vol, &q.proj, &p, &c);
+      if (rc != RTKB_OK)
+      {
+        release_batch(b);
+        return rc;
+      }
+      b->plans.push_back(c);
+      cudaStream_t s = nullptr;
+      cudaEvent_t  ev = nullptr;
+      cudaError_t  e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+      if (e == cudaSuccess)
+        b->streams.push_back(s);
+      if (e == cudaSuccess)
+        e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+      if (e == cudaSuccess)
+        b->joins.push_back(ev);
+      if (e != cudaSuccess)
+      {
+        release_batch(b);
+        return cuda_fail(e, "batch streams");
+      }
+    }
+    cudaError_t e = cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking);
+    if (e == cudaSuccess)
+      e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+    if (e != cudaSuccess)
+    {
+      release_batch(b);
+      return cuda_fail(e, "batch streams");
+    }
+  }
+  catch (...)
+  {
+    release_batch(b);
+    return fail(RTKB_ERR_OUT_OF_MEMORY, "host allocation failed");
+  }
+  *out = b;
+  return RTKB_OK;
+}
+
+extern "C" int
+rtkb_cg_batch_start(rtkb_cg_batch * b, const rtkb_cg_batch_problem * problems, void * stream)
+{
+  using namespace rtkb;
+  if (!b || !problems)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "null argument");
+  drop_batch_graph(b);
+  for (size_t i = 0; i < b->plans.size(); i++)
+  {
+    const rtkb_cg_batch_problem & q = problems[i];
+    const int rc = rtkb_cg_start(b->plans[i], q.d_proj, q.d_weights, q.displaced_detector, q.d_x, stream);
+    if (rc != RTKB_OK)
+      return rc;
+  }
+  b->started = true;
+  return RTKB_OK;
+}
+
+extern "C" int
+rtkb_cg_batch_iterate(rtkb_cg_batch * b, int niter, void * stream)
+{
+  using namespace rtkb;
+  if (!b || !b->started || niter < 0)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "batch not started");
+  if (niter == 0)
+    return RTKB_OK;
+  if (b->graph_iterations != niter)
+  {
+    drop_batch_graph(b);
+    const cudaError_t e = capture_batch(b, niter);
+    if (e != cudaSuccess)
+    {
+      drop_batch_graph(b);
+      return cuda_fail(e, "batched CG graph capture");
+    }
+  }
+  RTKB_CUDA_TRY(cudaGraphLaunch(b->exec, static_cast<cudaStream_t>(stream)));
+  for (rtkb_cg * c : b->plans)
+    c->iterations += niter;
+  return RTKB_OK;
+}
+
+extern "C" rtkb_cg *
+rtkb_cg_batch_plan(rtkb_cg_batch * b, int i)
+{
+  if (!b || i < 0 || i >= (int)b->plans.size())
+    return nullptr;
+  return b->plans[i];
+}
+
+extern "C" void
+rtkb_cg_batch_destroy(rtkb_cg_batch * b)
+{
+  release_batch(b);
 }

@@ -308,6 +308,66 @@ class ConjugateGradient:
             pass
 
 
+class ConjugateGradientBatch:
+    """Batched CG (rtkb_cg_batch_*): many independent problems, each a tuple
+    (geometry, vol_desc, proj_desc, proj, x[, weights[, displaced_detector]]);
+    iterate(n) runs n iterations of every problem as one CUDA graph launch."""
+
+    def __init__(self, problems, tikhonov=0.0, storage="fp32"):
+        from ._capi import CgBatchProblem, CgParams
+
+        self._lib = load()
+        arr = (CgBatchProblem * len(problems))()
+        self._keep = list(problems)
+        for i, prob in enumerate(problems):
+            g, vd, pd, proj, x = prob[:5]
+            w = prob[5] if len(prob) > 5 else None
+            dd = prob[6] if len(prob) > 6 else True
+            _check_shape(proj, pd, "projections")
+            _check_shape(x, vd, "volume")
+            if w is not None:
+                _check_shape(w, pd, "weights")
+            q = arr[i]
+            q.geometry, q.vol, q.proj = g.handle, vd, pd
+            q.d_proj, q.d_x = _ptr(proj).value, _ptr(x).value
+            q.d_weights = _ptr(w).value if w is not None else None
+            q.displaced_detector = int(dd)
+        self._arr = arr
+        p = CgParams()
+        p.tikhonov, p.use_cuda_graph, p.storage = tikhonov, 0, _storage_code(storage)
+        h = C.c_void_p()
+        check(self._lib.rtkb_cg_batch_create(arr, len(problems), C.byref(p), C.byref(h)))
+        self._h = h
+        self.n = len(problems)
+
+    def start(self, stream=None):
+        check(self._lib.rtkb_cg_batch_start(self._h, self._arr, _stream(stream)))
+
+    def iterate(self, n, stream=None):
+        check(self._lib.rtkb_cg_batch_iterate(self._h, int(n), _stream(stream)))
+
+    def residual(self, i, stream=None):
+        """(||r_k||^2, ||r_0||^2, k) of problem i -- synchronises the stream."""
+        plan = self._lib.rtkb_cg_batch_plan(self._h, int(i))
+        if not plan:
+            raise IndexError(i)
+        rr, rr0, it = C.c_double(), C.c_double(), C.c_int()
+        check(self._lib.rtkb_cg_residual(C.c_void_p(plan), C.byref(rr), C.byref(rr0), C.byref(it), _stream(stream)))
+        return rr.value, rr0.value, it.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _torch().cuda.synchronize()
+            self._lib.rtkb_cg_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def conjugate_gradient(geometry, vol_desc, proj_desc, proj, x, niter, rel_residual=0.0, weights=None,
                        displaced_detector=True, tikhonov=0.0, use_cuda_graph=True, stream=None, storage="fp32"):
     """Whole CG reconstruction in place on x; returns (iterations, relative residual)."""

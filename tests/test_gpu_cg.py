@@ -182,3 +182,48 @@ def test_cg_bf16_operator_and_preconditioner_refusal(rtkb, oracle):
     d = rel_l2(outs[1], outs[0])
     assert 1e-5 < d < 1e-2, d
     assert rtkb.ops.device_status() == 0
+
+
+def test_cg_batch_matches_single_plans_and_oracle(rtkb, oracle):
+    """Batched CG (rtkb_cg_batch_*): six uneven problems iterated as one graph
+    launch (replayed twice) agree with separate plans and, for one problem,
+    with the FP64 oracle's CG."""
+    import torch
+
+    rng = np.random.default_rng(7)
+    probs, cases = [], []
+    for i in range(6):
+        n = int(rng.integers(16, 33))
+        nv = int(rng.integers(18, 33))
+        vsize = (nv, nv - 2, nv + 1)
+        psize = (int(rng.integers(10, 17)) * 4, int(rng.integers(30, 49)), n)
+        sid = float(rng.uniform(500.0, 700.0))
+        gl, go = pair_geometry(rtkb, oracle, [(sid, 1.5 * sid, k * 360.0 / n, 0.0, 0.0) for k in range(n)])
+        vd, vo = pair_image(rtkb, oracle, vsize, (8.0,) * 3)
+        pd, po = pair_image(rtkb, oracle, psize, (8.0, 8.0, 1.0))
+        truth = rng.uniform(0.0, 1.0, size=oracle.shape_of(vo))
+        p = oracle.joseph_forward(go, vo, truth, po).astype(np.float32).astype(np.float64)
+        x = torch.zeros(oracle.shape_of(vo), device="cuda")
+        probs.append((gl, vd, pd, to_gpu(p), x, None, False))
+        cases.append((gl, go, vd, vo, pd, po, p))
+    batch = rtkb.ops.ConjugateGradientBatch(probs)
+    batch.start()
+    batch.iterate(3)
+    batch.iterate(3)  # replay of the same graph
+    res = [batch.residual(i) for i in range(len(probs))]
+    assert rtkb.ops.device_status() == 0
+    for i, (gl, go, vd, vo, pd, po, p) in enumerate(cases):
+        assert res[i][2] == 6
+        x1 = torch.zeros(oracle.shape_of(vo), device="cuda")
+        cg = rtkb.ops.ConjugateGradient(gl, vd, pd)
+        cg.start(to_gpu(p), x1, displaced_detector=False)
+        cg.iterate(6)
+        rr1 = cg.residual()[0]
+        cg.close()
+        # same kernels; only the order of the back projector's FP32 reductions differs
+        assert rel_l2(to_np(probs[i][4]), to_np(x1)) < 1e-5
+        np.testing.assert_allclose(res[i][0], rr1, rtol=1e-4)
+    gl, go, vd, vo, pd, po, p = cases[0]
+    ref_x, _ = oracle.cg_joseph(go, vo, po, p, 6)
+    assert rel_l2(to_np(probs[0][4]), ref_x) < CG_TOL
+    batch.close()

@@ -38,8 +38,8 @@ SID, SDD = 1000.0, 1536.0
 SEED = 20261203 + 1
 L1_BYTES_PER_UPDATE = 16  # four 4-byte taps of one bilinear interpolation
 # DRAM bytes (read + write) of one backprojection launch of this workload, from the 1-pass ncu capture
-# summarised in profiles/bp_tiled_kernel_512cube_720proj_traffic.md (71.90 GB read + 0.657 GB written).
-BP_LAUNCH_DRAM_BYTES = 71.90e9 + 0.6567e9
+# summarised in profiles/bp_tiled_kernel_512cube_720proj_traffic.md (69.86 GB read + 0.651 GB written).
+BP_LAUNCH_DRAM_BYTES = 69.86e9 + 0.6506e9
 WORKLOAD = {"workload": "FDK backprojection 512^3 @0.5mm <- 720 x 1024x768 @0.388mm, SID 1000, SDD 1536, 360 deg",
             "volume": [NX, NY, NZ], "projections": [NU, NV, NP], "dtype_storage": "float32",
             "l2_policy": "inputs larger than L2 (2.26 GB projection stack, 0.54 GB volume)"}

@@ -385,16 +385,30 @@ bp_consumer(const T * __restrict__ proj, int nproj, int nu, int nv, int nx, int 
             for (int j = 0; j < NYT; j += 2)
             {
               const float2 v = make_float2(fmaf((float)j, dv, v0), fmaf((float)(j + 1), dv, v0));
-              // floor(v) and its integer without the conversion unit: for
-              // |v| < 2^22, v + 1.5 * 2^23 lies in [2^23, 2^24), where floats
-              // are spaced 1, so rounding the sum toward zero gives floor(v) +
-              // 1.5 * 2^23 exactly, and its low mantissa bits floor(v) + 2^22.
-              // Bit-identical to floorf and (int)floorf; v stays inside the
-              // box here.
-              const float2 tb = __fadd2_rz(v, make_float2(kFloorBias, kFloorBias));
-              const float2 fv = __ffma2_rn(m1, __fadd2_rn(tb, make_float2(-kFloorBias, -kFloorBias)), v);
-              const T *    qa = col + (__float_as_int(tb.x) - kFloorBiasBits) * BW;
-              const T *    qb = col + (__float_as_int(tb.y) - kFloorBiasBits) * BW;
+              float2 fv;
+              const T * qa;
+              const T * qb;
+              if constexpr (sizeof(T) == 4)
+              {
+                // floor(v) and its integer without the conversion unit: for
+                // |v| < 2^22, v + 1.5 * 2^23 lies in [2^23, 2^24), where floats
+                // are spaced 1, so rounding the sum toward zero gives floor(v)
+                // + 1.5 * 2^23 exactly, and its low mantissa bits floor(v) +
+                // 2^22.  Bit-identical to floorf and (int)floorf; v stays
+                // inside the box here.  (Slower with BF16 taps, whose
+                // widening already keeps the integer pipes busy.)
+                const float2 tb = __fadd2_rz(v, make_float2(kFloorBias, kFloorBias));
+                fv = __ffma2_rn(m1, __fadd2_rn(tb, make_float2(-kFloorBias, -kFloorBias)), v);
+                qa = col + (__float_as_int(tb.x) - kFloorBiasBits) * BW;
+                qb = col + (__float_as_int(tb.y) - kFloorBiasBits) * BW;
+              }
+              else
+              {
+                const float2 fl = make_float2(floorf(v.x), floorf(v.y));
+                fv = __ffma2_rn(m1, fl, v);
+                qa = col + (int)fl.x * BW;
+                qb = col + (int)fl.y * BW;
+              }
               const float2 p00 = make_float2(tap(qa), tap(qb)), p01 = make_float2(tap(qa + 1), tap(qb + 1));
               const float2 p10 = make_float2(tap(qa + BW), tap(qb + BW));
               const float2 p11 = make_float2(tap(qa + BW + 1), tap(qb + BW + 1));

@@ -882,12 +882,31 @@ layer_params(int l)
   return l == 10 ? 16 : 27LL * kLayers[l].cin * kLayers[l].cout;
 }
 
+// Dynamic shared memory for a tcgen05 kernel that holds `cols` TMEM columns:
+// at least `need`, and enough that the CTAs one SM can hold never ask for more
+// than the SM's 512 columns (tcgen05.alloc would otherwise wait for another
+// CTA to release its columns).
+int
+tmem_bounded_smem(int need, int cols)
+{
+  constexpr int kSmemPerSm = 228 * 1024, kReservedPerCta = 1024;
+  const int     max_ctas = 512 / cols;
+  const int     floor_bytes = kSmemPerSm / (max_ctas + 1) - kReservedPerCta + 16;
+  return std::max(need, floor_bytes);
+}
+
+constexpr int
+tmem_cols(int n)
+{
+  return (n <= 32) ? 32 : (n <= 64) ? 64 : (n <= 128) ? 128 : (n <= 256) ? 256 : 512;
+}
+
 template <int N>
 void
 conv_fwd_tc_launch(const ConvIn & in, const bf16 * wp, const Dims & d0, bf16 * out, const bf16 * mask, int relu,
                    cudaStream_t st)
 {
-  const int smem = kCHaloBytes + 27 * 2 * N * 16 + 16;
+  const int smem = tmem_bounded_smem(kCHaloBytes + 27 * 2 * N * 16 + 16, tmem_cols(kCZ * N));
   static bool configured = false; // attribute set once per process (same value on every device)
   if (!configured)
   {

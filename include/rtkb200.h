@@ -117,8 +117,9 @@ int rtkb_voxel_backproject(const rtkb_geometry * g, const rtkb_image_desc * vol,
  * `chunk` projections (include/rtkFDKConeBeamReconstructionFilter.hxx:116-157;
  * chunk <= 0: an eighth of the stack), each copied on an internal stream into
  * one of two device staging buffers while the previous one is backprojected
- * into a device copy of the volume; the last chunk is backprojected in four
- * z-slabs, each copied back while the next is computed (the host<->device
+ * into a device copy of the volume (the first chunk, whose copy nothing
+ * overlaps, is a quarter of the others); the last chunk is backprojected in
+ * eight z-slabs, each copied back while the next is computed (the host<->device
  * transfers ITK's CudaDataManager makes around
  * rtkCudaFDKBackProjectionImageFilter.cxx:34-125, overlapped).  h_vol_in may
  * be NULL (zero volume).  Asynchronous on `stream`

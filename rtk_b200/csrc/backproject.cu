@@ -1317,10 +1317,14 @@ fdk_backproject_host(const rtkb_geometry * g, const rtkb_image_desc * vol, const
   if (chunk <= 0)
     chunk = std::max(1, (nproj + 7) / 8);
   chunk = std::max(1, std::min(chunk, std::max(nproj, 1)));
-  const int nchunks = (nproj + chunk - 1) / chunk;
+  // chunk k covers projections [start(k), start(k + 1)): the first chunk is a
+  // quarter of the others, since its copy is the only one nothing overlaps
+  const int first_chunk = std::max(1, chunk / 4);
+  auto      start = [&](int k) { return k == 0 ? 0 : std::min(nproj, first_chunk + (k - 1) * chunk); };
+  const int nchunks = nproj == 0 ? 0 : 1 + (std::max(0, nproj - first_chunk) + chunk - 1) / chunk;
   // the last chunk runs as kSlabs z-slabs (multiples of 16 slices), each slab
   // copied back while the next one is backprojected
-  constexpr int kSlabs = 4;
+  constexpr int kSlabs = 8;
   int           zb[kSlabs + 1];
   int           nslab = 0;
   zb[0] = 0;
@@ -1370,7 +1374,7 @@ fdk_backproject_host(const rtkb_geometry * g, const rtkb_image_desc * vol, const
     for (int k = 0; k < nchunks && rc == RTKB_OK; k++)
     {
       const int b = k & 1;
-      const int first = k * chunk, nk = std::min(chunk, nproj - first);
+      const int first = start(k), nk = start(k + 1) - first;
       if (k >= 2)
         e = cudaStreamWaitEvent(cs, ev[3 + b], 0); // the backprojection of chunk k-2 is done with stage b
       if (e == cudaSuccess)

@@ -396,8 +396,9 @@ def fdk_backproject_host(geometry, vol_desc, proj_desc, proj, vol_in=None, out=N
     """rtkb_fdk_backproject_host: FDK backprojection of a host (CPU) stack into a
     host volume, the stack streamed to the GPU in chunks of `chunk`
     projections (0: an eighth of the stack) whose copies overlap the
-    backprojection of the previous chunk; the volume comes back slab by slab
-    while the last chunk is backprojected.  vol_in None means a zero volume.
+    backprojection of the previous chunk (the first chunk is a quarter of the
+    others); the volume comes back slab by slab while the last chunk is
+    backprojected.  vol_in None means a zero volume.
     Asynchronous on `stream`: synchronise it before reading `out`.  Pinned
     tensors (pin_memory=True) give full copy bandwidth and overlap."""
     torch = _torch()

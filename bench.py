@@ -115,6 +115,8 @@ class ClockSampler:
 
 
 def dist_setup(n_gpus: int):
+    """One process per GPU (NCCL); without a GPU (the CPU tests of the
+    multi-process path) the same plumbing runs over gloo."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -124,9 +126,12 @@ def dist_setup(n_gpus: int):
         import torch
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
     return world, rank, local
 
 
@@ -136,7 +141,8 @@ def max_over_ranks(x: float, world: int) -> float:
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], device="cuda", dtype=torch.float64)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], device=dev, dtype=torch.float64)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 

@@ -91,8 +91,21 @@ int             rtkb_geometry_get_projection_coordinates_to_fixed_system_matrix(
                                                                                 double out[16]);
 /* which: 0 gantry, 1 source, 2 tilt, 3 out-of-plane, 4 in-plane angles (radians);
  * 5 SID, 6 SDD, 7 projection offsets X, 8 Y, 9 source offsets X, 10 Y;
- * 11 angular gaps of the source angles (GetAngularGaps(GetSourceAngles())) */
+ * 11 angular gaps of the source angles (GetAngularGaps(GetSourceAngles()));
+ * 12-15 collimation U inf, U sup, V inf, V sup (DBL_MAX: unbounded) */
 int             rtkb_geometry_get_parameters(const rtkb_geometry * g, int which, double * out);
+/* SetCollimationOfLastProjection */
+int             rtkb_geometry_set_collimation_of_last_projection(rtkb_geometry * g, double uinf, double usup,
+                                                                 double vinf, double vsup);
+/* rtk::ThreeDCircularProjectionGeometryXMLFileReader / rtk::ReadGeometry
+ * (src/rtkThreeDCircularProjectionGeometryXMLFileReader.cxx): *out receives a
+ * new geometry (free with rtkb_geometry_free); versions 3 and 2; a stored
+ * matrix that differs from the recomputed one by more than 0.001 is an error.
+ * rtk::ThreeDCircularProjectionGeometryXMLFileWriter
+ * (src/rtkThreeDCircularProjectionGeometryXMLFileWriter.cxx): version 3, 15
+ * significant digits, parameters equal over all projections written once. */
+int             rtkb_geometry_read_xml(const char * filename, rtkb_geometry ** out);
+int             rtkb_geometry_write_xml(const rtkb_geometry * g, const char * filename);
 double          rtkb_geometry_to_untilted_coordinate_at_isocenter(const rtkb_geometry * g, int i, double tilted);
 int             rtkb_geometry_set_radius_cylindrical_detector(rtkb_geometry * g, double radius);
 

@@ -159,6 +159,13 @@ SIGNATURES.update({
     "rtkb_fdk_backproject_static_scratch": (C.c_int, [_G, _IM, _IM, _V, _V, _V, _V]),
 })
 
+SIGNATURES.update({
+    "rtkb_geometry_set_collimation_of_last_projection": (C.c_int, [_G, C.c_double, C.c_double, C.c_double,
+                                                                   C.c_double]),
+    "rtkb_geometry_read_xml": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
+    "rtkb_geometry_write_xml": (C.c_int, [_G, C.c_char_p]),
+})
+
 class CgBatchProblem(C.Structure):
     """rtkb_cg_batch_problem."""
 

@@ -225,6 +225,7 @@ Geometry::add_projection_rad(double sid, double sdd, double ga, double pox, doub
   q.ip = convert_0_2pi(ip);
   q.sox = sox;
   q.soy = soy;
+  q.coll_uinf = q.coll_usup = q.coll_vinf = q.coll_vsup = DBL_MAX; // RTK's default: no collimation
 
   std::memset(q.projt, 0, sizeof(q.projt));
   q.projt[0] = q.projt[4] = q.projt[8] = 1.;
@@ -573,13 +574,14 @@ rtkb_geometry_get_parameters(const rtkb_geometry * g, int which, double * out)
       break;
     }
     default:
-      if (which < 3 || which > 10)
+      if (which < 3 || which > 15 || which == 11)
         return fail(RTKB_ERR_INVALID_ARGUMENT, "unknown geometry parameter selector");
       v.resize(P.size());
       for (size_t i = 0; i < P.size(); i++)
       {
         const auto & q = P[i];
-        const double vals[8] = { q.oop, q.ip, q.sid, q.sdd, q.pox, q.poy, q.sox, q.soy };
+        const double vals[13] = { q.oop, q.ip,  q.sid, q.sdd,       q.pox,       q.poy,      q.sox,
+                                  q.soy, 0.,    q.coll_uinf, q.coll_usup, q.coll_vinf, q.coll_vsup };
         v[i] = vals[which - 3];
       }
   }
@@ -593,6 +595,21 @@ rtkb_geometry_to_untilted_coordinate_at_isocenter(const rtkb_geometry * g, int i
   if (!proj_ok(g, i))
     return NAN;
   return g->g.to_untilted(i, tilted);
+}
+
+extern "C" int
+rtkb_geometry_set_collimation_of_last_projection(rtkb_geometry * g, double uinf, double usup, double vinf,
+                                                 double vsup)
+{
+  // SetCollimationOfLastProjection, src/rtkThreeDCircularProjectionGeometry.cxx
+  if (!g || g->g.p.empty())
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "geometry has no projection");
+  auto & q = g->g.p.back();
+  q.coll_uinf = uinf;
+  q.coll_usup = usup;
+  q.coll_vinf = vinf;
+  q.coll_vsup = vsup;
+  return RTKB_OK;
 }
 
 extern "C" int

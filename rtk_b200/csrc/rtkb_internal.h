@@ -52,6 +52,7 @@ struct Geometry
   struct Proj
   {
     double sid, sdd, gantry, pox, poy, oop, ip, sox, soy, source_angle;
+    double coll_uinf, coll_usup, coll_vinf, coll_vsup; // collimation (unbounded: DBL_MAX)
     double rot[16];  // 4x4 rotation (homogeneous)
     double mag[12];  // 3x4 magnification
     double srct[16]; // 4x4 source translation

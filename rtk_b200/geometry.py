@@ -53,6 +53,9 @@ class ThreeDCircularProjectionGeometry:
     def SetRadiusCylindricalDetector(self, r):  # noqa: N802
         check(self._lib.rtkb_geometry_set_radius_cylindrical_detector(self._g, r))
 
+    def SetCollimationOfLastProjection(self, uinf, usup, vinf, vsup):  # noqa: N802
+        check(self._lib.rtkb_geometry_set_collimation_of_last_projection(self._g, uinf, usup, vinf, vsup))
+
     # ---- getters ----
     def __len__(self):
         return self._lib.rtkb_geometry_number_of_projections(self._g)
@@ -120,8 +123,35 @@ class ThreeDCircularProjectionGeometry:
     def GetAngularGapsOfSourceAngles(self):  # noqa: N802
         return self._param(11)
 
+    def GetCollimationUInf(self):  # noqa: N802
+        return self._param(12)
+
+    def GetCollimationUSup(self):  # noqa: N802
+        return self._param(13)
+
+    def GetCollimationVInf(self):  # noqa: N802
+        return self._param(14)
+
+    def GetCollimationVSup(self):  # noqa: N802
+        return self._param(15)
+
     def ToUntiltedCoordinateAtIsocenter(self, i, tilted):  # noqa: N802
         return self._lib.rtkb_geometry_to_untilted_coordinate_at_isocenter(self._g, i, tilted)
+
+
+def read_geometry(filename) -> ThreeDCircularProjectionGeometry:
+    """rtk::ReadGeometry: a geometry from an RTK XML geometry file."""
+    g = ThreeDCircularProjectionGeometry.__new__(ThreeDCircularProjectionGeometry)
+    g._lib = load()
+    h = C.c_void_p()
+    check(g._lib.rtkb_geometry_read_xml(str(filename).encode(), C.byref(h)))
+    g._g = h.value
+    return g
+
+
+def write_geometry(geometry, filename) -> None:
+    """rtk::ThreeDCircularProjectionGeometryXMLFileWriter: write an RTK XML geometry file."""
+    check(geometry._lib.rtkb_geometry_write_xml(geometry.handle, str(filename).encode()))
 
 
 def circular(n_proj, sid, sdd, arc_deg=360.0, first_deg=0.0, **kw) -> ThreeDCircularProjectionGeometry:

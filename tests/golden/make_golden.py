@@ -2,7 +2,7 @@
 
 geometry_kat.json: the two projections and 3x4 matrices published in RTK's
 documentation/docs/Geometry.md (XML example, SID 1000 / SDD 1536), parsed from
-the document itself.
+the document itself.  geometry_example.xml: that XML example verbatim.
 
 Run inside the development container (the reference tree is not available
 where the tests run):  python tests/golden/make_golden.py /path/to/RTK
@@ -31,13 +31,24 @@ def parse_geometry_md(path: str) -> dict:
     return {"source": "documentation/docs/Geometry.md", "sid": sid, "sdd": sdd, "projections": projs}
 
 
+def geometry_md_xml(path: str) -> str:
+    """The XML example of the document, verbatim (a file the geometry reader
+    must accept: version 3, global SID/SDD/radius, per-projection matrices)."""
+    txt = open(path).read()
+    return re.search(r"(<\?xml.*?</RTKThreeDCircularGeometry>)", txt, flags=re.S).group(1) + "\n"
+
+
 def main():
     ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     here = os.path.dirname(os.path.abspath(__file__))
-    kat = parse_geometry_md(os.path.join(ref, "documentation", "docs", "Geometry.md"))
+    md = os.path.join(ref, "documentation", "docs", "Geometry.md")
+    kat = parse_geometry_md(md)
     with open(os.path.join(here, "geometry_kat.json"), "w") as f:
         json.dump(kat, f, indent=1)
     print("wrote geometry_kat.json with", len(kat["projections"]), "projections")
+    with open(os.path.join(here, "geometry_example.xml"), "w") as f:
+        f.write(geometry_md_xml(md))
+    print("wrote geometry_example.xml")
 
 
 if __name__ == "__main__":

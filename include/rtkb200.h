@@ -109,6 +109,17 @@ int             rtkb_geometry_write_xml(const rtkb_geometry * g, const char * fi
 double          rtkb_geometry_to_untilted_coordinate_at_isocenter(const rtkb_geometry * g, int i, double tilted);
 int             rtkb_geometry_set_radius_cylindrical_detector(rtkb_geometry * g, double radius);
 
+/* ---- image files ----
+ * MetaImage (.mha: header and data in one file; .mhd: data in a .raw/.zraw
+ * beside it), the format RTK's applications read and write through ITK's
+ * MetaImageIO.  Read: fills *desc (index 0, origin = the file's Offset) and,
+ * when data is not NULL, converts the voxels (float, double, 8/16/32-bit
+ * integers, either byte order, zlib-compressed or not) to float32 in data
+ * (x fastest; capacity in voxels).  Write: float32, zlib-compressed when
+ * compress != 0; Offset = the physical position of the region's first voxel. */
+int rtkb_image_read_mha(const char * filename, rtkb_image_desc * desc, float * data, long long capacity);
+int rtkb_image_write_mha(const char * filename, const rtkb_image_desc * desc, const float * data, int compress);
+
 /* Volume-index -> projection-index matrices (3x4, row-major, untransposed) of
  * stack slices first..first+n-1 as BackProjectionImageFilter builds them
  * (include/rtkBackProjectionImageFilter.hxx:535-595), FDK-normalised when

@@ -164,6 +164,8 @@ SIGNATURES.update({
                                                                    C.c_double]),
     "rtkb_geometry_read_xml": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
     "rtkb_geometry_write_xml": (C.c_int, [_G, C.c_char_p]),
+    "rtkb_image_read_mha": (C.c_int, [C.c_char_p, _IM, _V, C.c_longlong]),
+    "rtkb_image_write_mha": (C.c_int, [C.c_char_p, _IM, _V, C.c_int]),
 })
 
 class CgBatchProblem(C.Structure):

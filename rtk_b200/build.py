@@ -42,7 +42,7 @@ def build(verbose: bool = False, extra: list[str] | None = None) -> str:
     cmd = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-rdc=true", "-ccbin", host_cc,
            "-Xcompiler", "-fPIC,-O3", "-Xptxas", "-warn-spills", "--expt-relaxed-constexpr",
            "-I", os.path.join(ROOT, "include"), "-I", os.path.join(PKG, "csrc"),
-           "-shared", "-o", LIB + ".tmp", *srcs, "-lcudart_static", "-ldl", "-lrt", "-lpthread"]
+           "-shared", "-o", LIB + ".tmp", *srcs, "-lcudart_static", "-ldl", "-lrt", "-lpthread", "-lz"]
     if extra:
         cmd[1:1] = extra
     if verbose:

@@ -3,7 +3,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from ._capi import ImageDesc
+from ._capi import ImageDesc, check, load
 
 
 def make_desc(size, spacing=(1.0, 1.0, 1.0), origin=None, index=(0, 0, 0), direction=None) -> ImageDesc:
@@ -44,3 +44,30 @@ class Image:
 
     def GetOrigin(self):  # noqa: N802
         return tuple(self.desc.origin)
+
+
+def read_image(filename):
+    """A MetaImage file (.mha / .mhd, any scalar element type) as (float32
+    numpy array of shape (z, y, x), ImageDesc), as itk::ImageFileReader with
+    MetaImageIO gives it to RTK."""
+    import ctypes as C
+
+    lib = load()
+    d = ImageDesc()
+    check(lib.rtkb_image_read_mha(str(filename).encode(), C.byref(d), None, 0))
+    a = np.empty(shape_of(d), dtype=np.float32)
+    check(lib.rtkb_image_read_mha(str(filename).encode(), C.byref(d), a.ctypes.data_as(C.c_void_p), a.size))
+    return a, d
+
+
+def write_image(filename, data, desc: ImageDesc, compress=False) -> None:
+    """Write a float32 image (numpy array or torch tensor, shape (z, y, x)) as a
+    MetaImage file (.mha, or .mhd with its .raw / .zraw beside it)."""
+    import ctypes as C
+
+    a = data.detach().cpu().numpy() if hasattr(data, "detach") else np.asarray(data)
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    if a.shape != shape_of(desc):
+        raise ValueError(f"data shape {a.shape} does not match size {shape_of(desc)}")
+    check(load().rtkb_image_write_mha(str(filename).encode(), C.byref(desc), a.ctypes.data_as(C.c_void_p),
+                                      int(compress)))

@@ -270,7 +270,13 @@ typedef struct rtkb_cg_params
                             projection-domain temporary, FP32 arithmetic and FP64 dots, alpha and beta
                             (no counterpart in the reference; the iterate stays in the caller's FP32
                             buffer; no learned preconditioner) */
+  double gamma;          /* Laplacian regularisation weight (RTK's SetGamma): A x += gamma * (-Laplacian(x)) */
 } rtkb_cg_params;
+/* rtk::LaplacianImageFilter / CudaLaplacianImageFilter (include/rtkLaplacianImageFilter.hxx;
+ * src/rtkCudaLaplacianImageFilter.cu): d_out = Laplacian(d_in), the
+ * backward-difference divergence of the forward-difference gradient with a
+ * zero-flux Neumann boundary, spacing-scaled. */
+int  rtkb_laplacian(const rtkb_image_desc * vol, const float * d_in, float * d_out, void * stream);
 typedef struct rtkb_cg rtkb_cg;
 int  rtkb_cg_create(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
                     const rtkb_cg_params * params, rtkb_cg ** plan);

@@ -92,7 +92,8 @@ def lib():
             "orc_ramp_padded_size": (C.c_int, [C.c_int, C.POINTER(OrcRampParams)]),
             "orc_ramp_kernel": (None, [C.c_int, C.c_double, C.POINTER(OrcRampParams), D]),
             "orc_ramp_filter": (None, [IM, C.POINTER(OrcRampParams), D, D, C.c_int]),
-            "orc_cg_joseph": (None, [G, IM, IM, D, D, C.c_double, C.c_int, D, D, C.c_int]),
+            "orc_cg_joseph": (None, [G, IM, IM, D, D, C.c_double, C.c_double, C.c_int, D, D, C.c_int]),
+            "orc_laplacian": (None, [IM, D, D]),
             "orc_project_ellipsoids": (None, [G, IM, C.c_int, D, D, C.c_int]),
             "orc_draw_ellipsoids": (None, [IM, C.c_int, D, D, C.c_int]),
             "orc_fdk_backproject_f32_rtk": (C.c_int, [G, IM, IM, F, F, C.c_int]),
@@ -293,12 +294,19 @@ def ramp_filter(proj, data, params, threads=None):
     return out
 
 
-def cg_joseph(g, vol, proj, proj_data, niter, x0=None, weights=None, tikhonov=0.0, threads=None):
+def laplacian(vol, x):
+    d = np.ascontiguousarray(x, dtype=np.float64)
+    out = np.empty_like(d)
+    lib().orc_laplacian(C.byref(vol), _d(d), _d(out))
+    return out
+
+
+def cg_joseph(g, vol, proj, proj_data, niter, x0=None, weights=None, tikhonov=0.0, gamma=0.0, threads=None):
     p = np.ascontiguousarray(proj_data, dtype=np.float64)
     w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
     x = np.zeros(shape_of(vol)) if x0 is None else np.array(x0, dtype=np.float64, copy=True, order="C")
     res = np.zeros(niter + 1)
-    lib().orc_cg_joseph(g._g, C.byref(vol), C.byref(proj), _d(p), _d(w), tikhonov, niter, _d(x), _d(res),
+    lib().orc_cg_joseph(g._g, C.byref(vol), C.byref(proj), _d(p), _d(w), tikhonov, gamma, niter, _d(x), _d(res),
                         threads or nthreads())
     return x, res
 

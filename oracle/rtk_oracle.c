@@ -1394,12 +1394,46 @@ orc_ramp_filter(const orc_image * proj, const orc_ramp_params * p, const double 
 /* ------------------------------------------------------------------------ */
 /* conjugate gradient                                                       */
 /* ------------------------------------------------------------------------ */
+void
+orc_laplacian(const orc_image * vol, const double * x, double * out)
+{
+  /* LaplacianImageFilter (include/rtkLaplacianImageFilter.hxx): the
+   * backward-difference divergence (include/rtkBackwardDifferenceDivergenceImageFilter.hxx,
+   * zero before the first index, the last gradient subtracted at the last
+   * index) of the forward-difference gradient
+   * (include/rtkForwardDifferenceGradientImageFilter.hxx, zero-flux Neumann
+   * boundary), both scaled by 1/spacing: per axis, the sum over the existing
+   * neighbours of (x_nb - x_i) / spacing^2. */
+  const int nx = vol->size[0], ny = vol->size[1], nz = vol->size[2];
+  const double w[3] = { 1. / (vol->spacing[0] * vol->spacing[0]), 1. / (vol->spacing[1] * vol->spacing[1]),
+                        1. / (vol->spacing[2] * vol->spacing[2]) };
+  const long st[3] = { 1, nx, (long)nx * ny };
+  const int  n[3] = { nx, ny, nz };
+  for (int z = 0; z < nz; z++)
+    for (int y = 0; y < ny; y++)
+      for (int xx = 0; xx < nx; xx++)
+      {
+        const long i = ((long)z * ny + y) * nx + xx;
+        const int  c[3] = { xx, y, z };
+        double     l = 0.;
+        for (int a = 0; a < 3; a++)
+        {
+          if (c[a] + 1 < n[a])
+            l += (x[i + st[a]] - x[i]) * w[a];
+          if (c[a] > 0)
+            l += (x[i - st[a]] - x[i]) * w[a];
+        }
+        out[i] = l;
+      }
+}
+
 static void
 cg_apply_A(const orc_geometry * g, const orc_image * vol, const orc_image * proj, const double * weights,
-           double tikhonov, const double * x, double * out, double * ptmp, int nthreads)
+           double tikhonov, double gamma, const double * x, double * out, double * ptmp, int nthreads)
 {
   /* ReconstructionConjugateGradientOperator::GenerateData,
-   * include/rtkReconstructionConjugateGradientOperator.hxx:192-286 */
+   * include/rtkReconstructionConjugateGradientOperator.hxx:192-311:
+   * BP(W .* FP(x)), then + gamma * (-Laplacian(x)), then + tikhonov * x */
   const long np = npix(proj), nvx = npix(vol);
   memset(ptmp, 0, sizeof(double) * np);
   orc_joseph_forward(g, vol, x, proj, ptmp, ptmp, nthreads);
@@ -1408,6 +1442,14 @@ cg_apply_A(const orc_geometry * g, const orc_image * vol, const orc_image * proj
       ptmp[q] *= weights[q];
   memset(out, 0, sizeof(double) * nvx);
   orc_joseph_back(g, vol, out, out, proj, ptmp);
+  if (gamma != 0.)
+  {
+    double * lap = (double *)malloc(sizeof(double) * nvx);
+    orc_laplacian(vol, x, lap);
+    for (long q = 0; q < nvx; q++)
+      out[q] += -gamma * lap[q];
+    free(lap);
+  }
   if (tikhonov != 0.)
     for (long q = 0; q < nvx; q++)
       out[q] += tikhonov * x[q];
@@ -1415,7 +1457,8 @@ cg_apply_A(const orc_geometry * g, const orc_image * vol, const orc_image * proj
 
 void
 orc_cg_joseph(const orc_geometry * g, const orc_image * vol, const orc_image * proj, const double * proj_data,
-              const double * weights, double tikhonov, int niter, double * x, double * residuals, int nthreads)
+              const double * weights, double tikhonov, double gamma, int niter, double * x, double * residuals,
+              int nthreads)
 {
   /* ConjugateGradientImageFilter::GenerateData,
    * include/rtkConjugateGradientImageFilter.hxx:108-258, with FP64
@@ -1430,7 +1473,7 @@ orc_cg_joseph(const orc_geometry * g, const orc_image * vol, const orc_image * p
   for (long q = 0; q < np; q++)
     ptmp[q] = proj_data[q] * (weights ? weights[q] : 1.);
   orc_joseph_back(g, vol, b, b, proj, ptmp);
-  cg_apply_A(g, vol, proj, weights, tikhonov, x, AP, ptmp, nthreads);
+  cg_apply_A(g, vol, proj, weights, tikhonov, gamma, x, AP, ptmp, nthreads);
   for (long q = 0; q < nvx; q++)
   {
     R[q] = b[q] - AP[q];
@@ -1444,7 +1487,7 @@ orc_cg_joseph(const orc_geometry * g, const orc_image * vol, const orc_image * p
     residuals[0] = rr;
   for (int it = 0; it < niter; it++)
   {
-    cg_apply_A(g, vol, proj, weights, tikhonov, P, AP, ptmp, nthreads);
+    cg_apply_A(g, vol, proj, weights, tikhonov, gamma, P, AP, ptmp, nthreads);
     double num = 0., den = 0.;
     for (long q = 0; q < nvx; q++)
     {

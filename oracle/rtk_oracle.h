@@ -120,7 +120,10 @@ void orc_ramp_filter(const orc_image * proj, const orc_ramp_params * p, const do
  * Runs niter iterations from x (in/out).  residuals[k] = ||r_k||^2 for
  * k = 0..niter (may be NULL).  weights may be NULL (all ones). */
 void orc_cg_joseph(const orc_geometry * g, const orc_image * vol, const orc_image * proj, const double * proj_data,
-                   const double * weights, double tikhonov, int niter, double * x, double * residuals, int nthreads);
+                   const double * weights, double tikhonov, double gamma, int niter, double * x, double * residuals,
+                   int nthreads);
+/* RTK's LaplacianImageFilter (Neumann boundary, spacing-scaled): out = Laplacian(x) */
+void orc_laplacian(const orc_image * vol, const double * x, double * out);
 
 /* ---- phantoms (test input generators; src/rtkQuadricShape.cxx semantics) ---- */
 /* ellipsoids: per ellipsoid 16 doubles: cx cy cz, ax ay az, R (3x3 row-major, local->world), density */

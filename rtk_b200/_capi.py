@@ -142,7 +142,7 @@ def check(code: int) -> None:
 class CgParams(C.Structure):
     """rtkb_cg_params."""
 
-    _fields_ = [("tikhonov", C.c_double), ("use_cuda_graph", C.c_int), ("storage", C.c_int)]
+    _fields_ = [("tikhonov", C.c_double), ("use_cuda_graph", C.c_int), ("storage", C.c_int), ("gamma", C.c_double)]
 
 
 SIGNATURES.update({
@@ -165,6 +165,7 @@ SIGNATURES.update({
     "rtkb_geometry_read_xml": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
     "rtkb_geometry_write_xml": (C.c_int, [_G, C.c_char_p]),
     "rtkb_image_read_mha": (C.c_int, [C.c_char_p, _IM, _V, C.c_longlong]),
+    "rtkb_laplacian": (C.c_int, [_IM, _V, _V, _V]),
     "rtkb_image_write_mha": (C.c_int, [C.c_char_p, _IM, _V, C.c_int]),
 })
 

@@ -28,6 +28,7 @@ struct rtkb_cg
   rtkb_image_desc          vol{}, proj{};
   rtkb::JosephArgs         args{};
   float                    tikhonov = 0.f;
+  float                    gamma = 0.f; // Laplacian regularisation weight (RTK's SetGamma)
   bool                     use_graph = true;
   bool                     bf16 = false; // R, P, AP and tmp stored as bfloat16 (FP32 arithmetic)
   long long                nvox = 0, npix = 0;
@@ -365,6 +366,50 @@ grid_for(long long n)
   return (unsigned)std::min<long long>((n + 255) / 256, 148LL * 16);
 }
 
+// RTK's LaplacianImageFilter (include/rtkLaplacianImageFilter.hxx: backward-
+// difference divergence of the forward-difference gradient, zero-flux
+// Neumann boundary, spacing-scaled): per axis, the sum over the existing
+// neighbours of (x_nb - x_i) * w_axis with w = 1 / spacing^2.
+// out = scale * Laplacian(x), or out += scale * Laplacian(x) when add.
+template <typename TI, typename TO>
+__global__ void __launch_bounds__(256)
+laplacian_kernel(const TI * __restrict__ x, TO * out, int nx, int ny, int nz, float wx, float wy, float wz,
+                 float scale, bool add)
+{
+  const long long n = (long long)nx * ny * nz, sxy = (long long)nx * ny;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+  {
+    const int   ix = (int)(i % nx), iy = (int)((i / nx) % ny), iz = (int)(i / sxy);
+    const float c = ld_elem(x, i);
+    float       lx = 0.f, ly = 0.f, lz = 0.f;
+    if (ix + 1 < nx)
+      lx += ld_elem(x, i + 1) - c;
+    if (ix > 0)
+      lx += ld_elem(x, i - 1) - c;
+    if (iy + 1 < ny)
+      ly += ld_elem(x, i + nx) - c;
+    if (iy > 0)
+      ly += ld_elem(x, i - nx) - c;
+    if (iz + 1 < nz)
+      lz += ld_elem(x, i + sxy) - c;
+    if (iz > 0)
+      lz += ld_elem(x, i - sxy) - c;
+    const float l = fmaf(lx, wx, fmaf(ly, wy, lz * wz));
+    st_elem(out, i, add ? fmaf(scale, l, ld_elem(out, i)) : scale * l);
+  }
+}
+
+template <typename TI, typename TO>
+cudaError_t
+laplacian_launch(const rtkb_image_desc & v, const TI * x, TO * out, float scale, bool add, cudaStream_t st)
+{
+  const long long n = (long long)v.size[0] * v.size[1] * v.size[2];
+  laplacian_kernel<TI, TO><<<(unsigned)std::min<long long>((n + 255) / 256, 148LL * 16), 256, 0, st>>>(
+    x, out, v.size[0], v.size[1], v.size[2], (float)(1. / (v.spacing[0] * v.spacing[0])),
+    (float)(1. / (v.spacing[1] * v.spacing[1])), (float)(1. / (v.spacing[2] * v.spacing[2])), scale, add);
+  return cudaGetLastError();
+}
+
 Elem
 storage(const rtkb_cg * c)
 {
@@ -386,8 +431,17 @@ apply_A(rtkb_cg * c, const void * in, Elem ie, void * out, Elem oe, cudaStream_t
   cudaError_t e = rtkb::joseph_forward_launch(c->args, in, ie, c->scratch, nullptr, c->tmp, storage(c), c->W, st);
   if (e != cudaSuccess)
     return e;
-  return rtkb::joseph_back_launch(c->args, c->tmp, storage(c), c->scratch, nullptr, out, oe,
-                                  c->tikhonov != 0.f ? in : nullptr, ie, c->tikhonov, st);
+  e = rtkb::joseph_back_launch(c->args, c->tmp, storage(c), c->scratch, nullptr, out, oe,
+                               c->tikhonov != 0.f ? in : nullptr, ie, c->tikhonov, st);
+  if (e != cudaSuccess || c->gamma == 0.f)
+    return e;
+  // + gamma * (-Laplacian(in)) (ReconstructionConjugateGradientOperator, include/rtkReconstructionConjugateGradientOperator.hxx:294-311)
+  using B = __nv_bfloat16;
+  if (ie == Elem::BF16)
+    return oe == Elem::BF16 ? laplacian_launch(c->vol, static_cast<const B *>(in), static_cast<B *>(out), -c->gamma, true, st)
+                            : laplacian_launch(c->vol, static_cast<const B *>(in), static_cast<float *>(out), -c->gamma, true, st);
+  return oe == Elem::BF16 ? laplacian_launch(c->vol, static_cast<const float *>(in), static_cast<B *>(out), -c->gamma, true, st)
+                          : laplacian_launch(c->vol, static_cast<const float *>(in), static_cast<float *>(out), -c->gamma, true, st);
 }
 
 template <typename S>
@@ -509,6 +563,7 @@ rtkb_cg_create(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_
     c->vol = *vol;
     c->proj = *proj;
     c->tikhonov = params ? (float)params->tikhonov : 0.f;
+    c->gamma = params ? (float)params->gamma : 0.f;
     c->use_graph = params ? params->use_cuda_graph != 0 : true;
     c->bf16 = params ? params->storage == 1 : false;
     c->nvox = num_pixels(*vol);
@@ -1062,4 +1117,17 @@ extern "C" void
 rtkb_cg_batch_destroy(rtkb_cg_batch * b)
 {
   release_batch(b);
+}
+
+extern "C" int
+rtkb_laplacian(const rtkb_image_desc * vol, const float * d_in, float * d_out, void * stream)
+{
+  using namespace rtkb;
+  std::string why;
+  if (!vol || !d_in || !d_out || d_in == d_out)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "null or aliased argument");
+  if (!desc_valid(vol, why))
+    return fail(RTKB_ERR_INVALID_ARGUMENT, why);
+  const cudaError_t e = laplacian_launch(*vol, d_in, d_out, 1.f, false, static_cast<cudaStream_t>(stream));
+  return e == cudaSuccess ? RTKB_OK : cuda_fail(e, "laplacian");
 }

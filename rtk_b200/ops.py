@@ -221,6 +221,17 @@ def device_status(stream=None) -> int:
     return st.value
 
 
+def laplacian(vol_desc, x, out=None, stream=None):
+    """rtk::LaplacianImageFilter (CudaLaplacianImageFilter): out = Laplacian(x)
+    with a zero-flux Neumann boundary, spacing-scaled."""
+    _check_shape(x, vol_desc, "volume")
+    if out is None:
+        out = _torch().empty_like(x)
+    _check_shape(out, vol_desc, "output")
+    check(load().rtkb_laplacian(C.byref(vol_desc), _ptr(x), _ptr(out), _stream(stream)))
+    return out
+
+
 def _storage_code(storage):
     codes = {"fp32": 0, "bf16": 1}
     if storage not in codes:
@@ -234,7 +245,8 @@ class ConjugateGradient:
     stores the normal-equation vectors and the projection-domain temporary
     as bfloat16 (FP32 arithmetic, FP64 dots and step sizes)."""
 
-    def __init__(self, geometry, vol_desc, proj_desc, tikhonov=0.0, use_cuda_graph=True, storage="fp32"):
+    def __init__(self, geometry, vol_desc, proj_desc, tikhonov=0.0, use_cuda_graph=True, storage="fp32",
+                 gamma=0.0):
         from ._capi import CgParams
 
         self._lib = load()
@@ -242,6 +254,7 @@ class ConjugateGradient:
         self.vol_desc, self.proj_desc = vol_desc, proj_desc
         p = CgParams()
         p.tikhonov, p.use_cuda_graph, p.storage = tikhonov, int(use_cuda_graph), _storage_code(storage)
+        p.gamma = gamma
         h = C.c_void_p()
         check(self._lib.rtkb_cg_create(geometry.handle, C.byref(vol_desc), C.byref(proj_desc), C.byref(p),
                                        C.byref(h)))
@@ -313,7 +326,7 @@ class ConjugateGradientBatch:
     (geometry, vol_desc, proj_desc, proj, x[, weights[, displaced_detector]]);
     iterate(n) runs n iterations of every problem as one CUDA graph launch."""
 
-    def __init__(self, problems, tikhonov=0.0, storage="fp32"):
+    def __init__(self, problems, tikhonov=0.0, storage="fp32", gamma=0.0):
         from ._capi import CgBatchProblem, CgParams
 
         self._lib = load()
@@ -334,7 +347,7 @@ class ConjugateGradientBatch:
             q.displaced_detector = int(dd)
         self._arr = arr
         p = CgParams()
-        p.tikhonov, p.use_cuda_graph, p.storage = tikhonov, 0, _storage_code(storage)
+        p.tikhonov, p.use_cuda_graph, p.storage, p.gamma = tikhonov, 0, _storage_code(storage), gamma
         h = C.c_void_p()
         check(self._lib.rtkb_cg_batch_create(arr, len(problems), C.byref(p), C.byref(h)))
         self._h = h
@@ -369,12 +382,14 @@ class ConjugateGradientBatch:
 
 
 def conjugate_gradient(geometry, vol_desc, proj_desc, proj, x, niter, rel_residual=0.0, weights=None,
-                       displaced_detector=True, tikhonov=0.0, use_cuda_graph=True, stream=None, storage="fp32"):
+                       displaced_detector=True, tikhonov=0.0, use_cuda_graph=True, stream=None, storage="fp32",
+                       gamma=0.0):
     """Whole CG reconstruction in place on x; returns (iterations, relative residual)."""
     from ._capi import CgParams
 
     p = CgParams()
     p.tikhonov, p.use_cuda_graph, p.storage = tikhonov, int(use_cuda_graph), _storage_code(storage)
+    p.gamma = gamma
     it, rel = C.c_int(), C.c_double()
     check(load().rtkb_conjugate_gradient(geometry.handle, C.byref(vol_desc), C.byref(proj_desc), C.byref(p),
                                          _ptr(proj), _ptr(weights) if weights is not None else None,

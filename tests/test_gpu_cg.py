@@ -227,3 +227,45 @@ def test_cg_batch_matches_single_plans_and_oracle(rtkb, oracle):
     ref_x, _ = oracle.cg_joseph(go, vo, po, p, 6)
     assert rel_l2(to_np(probs[0][4]), ref_x) < CG_TOL
     batch.close()
+
+
+def test_laplacian_matches_oracle(rtkb, oracle):
+    """rtkb_laplacian against RTK's LaplacianImageFilter restated (Neumann
+    boundary, anisotropic spacing, a one-voxel axis)."""
+    rng = np.random.default_rng(9)
+    for size, sp in (((17, 12, 9), (1.0, 2.5, 0.7)), ((8, 1, 5), (2.0, 1.0, 3.0))):
+        vd, vo = pair_image(rtkb, oracle, size, sp)
+        x = rng.uniform(-1.0, 1.0, size=oracle.shape_of(vo)).astype(np.float32).astype(np.float64)
+        got = to_np(rtkb.ops.laplacian(vd, to_gpu(x)))
+        ref = oracle.laplacian(vo, x)
+        assert rel_l2(got, ref) < 1e-6, rel_l2(got, ref)
+
+
+def test_cg_laplacian_regularisation_matches_oracle(rtkb, oracle):
+    """CG with RTK's gamma (Laplacian) and Tikhonov terms, graph and eager,
+    against the FP64 oracle's CG with the same operator."""
+    import torch
+
+    gl, go, vd, vo, pd, po, p = _problem(rtkb, oracle, seed=6)
+    # gamma large enough to matter: the regulariser half the size of A^T A on a random volume
+    xr = to_gpu(np.random.default_rng(6).uniform(-1.0, 1.0, size=oracle.shape_of(vo)))
+    plan = rtkb.ops.ConjugateGradient(gl, vd, pd)
+    ax = plan.apply_operator(xr, torch.empty_like(xr))
+    plan.close()
+    gamma = 0.5 * float(ax.norm() / rtkb.ops.laplacian(vd, xr).norm())
+    ref_x, ref_res = oracle.cg_joseph(go, vo, po, p, 5, tikhonov=0.3, gamma=gamma)
+    for graph in (True, False):
+        x = torch.zeros(oracle.shape_of(vo), device="cuda")
+        cg = rtkb.ops.ConjugateGradient(gl, vd, pd, tikhonov=0.3, gamma=gamma, use_cuda_graph=graph)
+        cg.start(to_gpu(p), x, displaced_detector=False)
+        res = [cg.residual()[0]]
+        for _ in range(5):
+            cg.iterate(1)
+            res.append(cg.residual()[0])
+        cg.close()
+        assert rel_l2(to_np(x), ref_x) < CG_TOL
+        np.testing.assert_allclose(res, ref_res, rtol=CG_TOL)
+    # the regulariser changes the solution
+    plain, _ = oracle.cg_joseph(go, vo, po, p, 5, tikhonov=0.3)
+    assert rel_l2(plain, ref_x) > 1e-3
+    assert rtkb.ops.device_status() == 0

@@ -384,6 +384,37 @@ def batch_cg_leg(torch, rtkb, stream, n=64, niter=10):
                     "multi-problem kernel"}
 
 
+def sart_leg(torch, rtkb, stream, niter=1):
+    """SART (RTK's defaults: lambda 0.3, one projection per subset, Joseph
+    forward and voxel-based back projection) on the CG configuration's problem:
+    256^3 at 1 mm from 360 projections of 512x384 at 0.8 mm, seeded order."""
+    from tests import phantoms
+
+    n = 360
+    g = rtkb.geometry.circular(n, SID, SDD)
+    vd = rtkb.make_desc((256, 256, 256), (1.0, 1.0, 1.0))
+    pd = rtkb.make_desc((512, 384, n), (0.8, 0.8, 1.0))
+    ell = phantoms.random_ellipsoids(20, SEED + 2, centre_radius=60.0, axis_range=(5.0, 60.0))
+    ell[:, 15] *= 0.02
+    p = rtkb.ops.project_ellipsoids(g, pd, ell, stream=stream)
+    x = torch.zeros((256, 256, 256), device="cuda")
+    rtkb.ops.sart(g, vd, pd, p, x, niter=1, seed=1, stream=stream)  # warm-up (allocations, host tables)
+    x.zero_()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    rtkb.ops.sart(g, vd, pd, p, x, niter=niter, seed=1, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    fp = rtkb.ops.joseph_forward_project(g, vd, pd, x, torch.zeros_like(p), stream=stream)
+    misfit = float((fp - p).double().norm() / p.double().norm())
+    return {"workload": "SART, 256^3 @1mm <- 360 x 512x384 @0.8mm, lambda 0.3, 1 projection per subset",
+            "iterations": niter, "seconds_per_iteration_device": e0.elapsed_time(e1) / 1e3 / niter,
+            "seconds_per_iteration_wall": wall / niter, "relative_projection_misfit_after": misfit}
+
+
 def cg_seconds_to_residual(torch, rtkb, stream, tol=1e-3, max_iter=300, learned_pcg=True):
     """CG configuration: 256^3 at 1 mm, 360 projections of 512x384 at 0.8 mm
     (SID 1000, SDD 1536) of 20 seeded random ellipsoids with pre-log Poisson
@@ -802,6 +833,7 @@ def main():
         line["joseph_forward"] = joseph_forward_leg(torch, rtkb, lib, stream)
         line["batched"] = batch_leg(torch, rtkb, stream)
         line["batched_cg"] = batch_cg_leg(torch, rtkb, stream)
+        line["sart"] = sart_leg(torch, rtkb, stream)
         line["cg"] = cg_seconds_to_residual(torch, rtkb, stream)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:

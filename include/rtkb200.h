@@ -323,6 +323,33 @@ int       rtkb_cg_batch_start(rtkb_cg_batch * batch, const rtkb_cg_batch_problem
 int       rtkb_cg_batch_iterate(rtkb_cg_batch * batch, int niter, void * stream);
 rtkb_cg * rtkb_cg_batch_plan(rtkb_cg_batch * batch, int i);
 void      rtkb_cg_batch_destroy(rtkb_cg_batch * batch);
+/* rtk::RayBoxIntersectionImageFilter with BoxShape::SetBoxFromImage(volume,
+ * false) (include/rtkRayConvexIntersectionImageFilter.hxx:57-84,
+ * src/rtkBoxShape.cxx): per pixel, the length (mm) of the source-to-pixel ray
+ * inside the box from the volume's origin to origin + D (spacing x (size-1)). */
+int rtkb_ray_box_lengths(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
+                         float * d_out, void * stream);
+/* rtk::SARTConeBeamReconstructionFilter (include/rtkSARTConeBeamReconstructionFilter.hxx)
+ * with the Joseph forward and voxel-based back projectors, in place on d_x.
+ * order: the processing order (np projection positions in the stack, a
+ * permutation) or NULL for a Fisher-Yates shuffle driven by SplitMix64(seed)
+ * (RTK shuffles with std::default_random_engine, whose sequence the standard
+ * leaves to the implementation).  Defaults in RTK: niter 3, lambda 0.3, no
+ * positivity, 1 projection per subset, displaced-detector filter on,
+ * division threshold 1e-5. */
+typedef struct rtkb_sart_params
+{
+  int                niter;
+  double             lambda;
+  int                positivity;
+  int                projections_per_subset;
+  int                disable_displaced_detector;
+  double             division_threshold;
+  const int *        order;
+  unsigned long long seed;
+} rtkb_sart_params;
+int rtkb_sart(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj, const float * d_proj,
+              float * d_x, const rtkb_sart_params * params, void * stream);
 /* d_out = A d_in with the plan's operator (weights W = 1 until rtkb_cg_start
  * sets them).  Used to generate (A e, e) training pairs for the learned
  * preconditioner.  No reference counterpart (RTK's operator is internal to

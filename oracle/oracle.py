@@ -94,6 +94,9 @@ def lib():
             "orc_ramp_filter": (None, [IM, C.POINTER(OrcRampParams), D, D, C.c_int]),
             "orc_cg_joseph": (None, [G, IM, IM, D, D, C.c_double, C.c_double, C.c_int, D, D, C.c_int]),
             "orc_laplacian": (None, [IM, D, D]),
+            "orc_ray_box": (None, [G, IM, IM, D, C.c_int]),
+            "orc_sart": (None, [G, IM, IM, D, D, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_double,
+                                C.POINTER(C.c_int), C.c_int]),
             "orc_project_ellipsoids": (None, [G, IM, C.c_int, D, D, C.c_int]),
             "orc_draw_ellipsoids": (None, [IM, C.c_int, D, D, C.c_int]),
             "orc_fdk_backproject_f32_rtk": (C.c_int, [G, IM, IM, F, F, C.c_int]),
@@ -299,6 +302,23 @@ def laplacian(vol, x):
     out = np.empty_like(d)
     lib().orc_laplacian(C.byref(vol), _d(d), _d(out))
     return out
+
+
+def ray_box(g, vol, proj, threads=None):
+    out = np.empty(shape_of(proj))
+    lib().orc_ray_box(g._g, C.byref(vol), C.byref(proj), _d(out), threads or nthreads())
+    return out
+
+
+def sart(g, vol, proj, proj_data, niter, order, x0=None, lam=0.3, positivity=False, subset=1,
+         displaced_detector=True, threshold=1e-5, threads=None):
+    p = np.ascontiguousarray(proj_data, dtype=np.float64)
+    x = np.zeros(shape_of(vol)) if x0 is None else np.array(x0, dtype=np.float64, copy=True, order="C")
+    o = np.ascontiguousarray(order, dtype=np.int32)
+    lib().orc_sart(g._g, C.byref(vol), C.byref(proj), _d(p), _d(x), int(niter), float(lam), int(positivity),
+                   int(subset), int(displaced_detector), float(threshold),
+                   o.ctypes.data_as(C.POINTER(C.c_int)), threads or nthreads())
+    return x
 
 
 def cg_joseph(g, vol, proj, proj_data, niter, x0=None, weights=None, tikhonov=0.0, gamma=0.0, threads=None):

@@ -1709,3 +1709,161 @@ orc_fdk_backproject_f32_rtk(const orc_geometry * g, const orc_image * vol, const
   free(mats);
   return bad ? -2 : 0;
 }
+
+/* ------------------------------------------------------------------------ */
+/* SART: SARTConeBeamReconstructionFilter (include/rtkSARTConeBeamReconstructionFilter.hxx) */
+
+void
+orc_ray_box(const orc_geometry * g, const orc_image * vol, const orc_image * proj, double * out, int nthreads)
+{
+  /* RayBoxIntersectionImageFilter: RayConvexIntersectionImageFilter
+   * (include/rtkRayConvexIntersectionImageFilter.hxx:57-84) with density 1
+   * and the BoxShape of BoxShape::SetBoxFromImage(volume, false)
+   * (src/rtkBoxShape.cxx:141-160: from the origin to origin + D (spacing x
+   * (size - 1))), intersected as BoxShape::IsIntersectedByRay
+   * (src/rtkBoxShape.cxx:47-97) along the normalised source-to-pixel
+   * direction: out = supDist - infDist in mm, 0 without intersection. */
+  const int nu = proj->size[0], nv = proj->size[1], np = proj->size[2];
+  const double * D = vol->direction;
+  double         bmin[3], bmax[3], ext[3];
+  for (int a = 0; a < 3; a++)
+    ext[a] = vol->spacing[a] * (vol->size[a] - 1);
+  for (int r = 0; r < 3; r++)
+  {
+    bmin[r] = vol->origin[r];
+    bmax[r] = vol->origin[r] + D[3 * r + 0] * ext[0] + D[3 * r + 1] * ext[1] + D[3 * r + 2] * ext[2];
+  }
+  double mn[3], mx[3];
+  for (int a = 0; a < 3; a++) /* D^T applied to the corners */
+  {
+    mn[a] = D[0 * 3 + a] * bmin[0] + D[1 * 3 + a] * bmin[1] + D[2 * 3 + a] * bmin[2];
+    mx[a] = D[0 * 3 + a] * bmax[0] + D[1 * 3 + a] * bmax[1] + D[2 * 3 + a] * bmax[2];
+    if (mn[a] > mx[a])
+    {
+      const double t = mn[a];
+      mn[a] = mx[a];
+      mx[a] = t;
+    }
+  }
+  double pi2pp[16];
+  orc_index_to_physical(proj, pi2pp);
+  for (int s = 0; s < np; s++)
+  {
+    const int k = proj->index[2] + s;
+    double    p2f[16], T[16], src[4];
+    orc_geometry_proj_coords_to_fixed(g, k, p2f);
+    mat_mul(p2f, pi2pp, T, 4, 4, 4);
+    orc_geometry_source_position(g, k, src);
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 4)
+    for (int j = 0; j < nv; j++)
+      for (int i = 0; i < nu; i++)
+      {
+        const double ii = i + proj->index[0], jj = j + proj->index[1], kk = k;
+        double       d[3];
+        for (int a = 0; a < 3; a++)
+          d[a] = T[a * 4 + 0] * ii + T[a * 4 + 1] * jj + T[a * 4 + 2] * kk + T[a * 4 + 3] - src[a];
+        const double len = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+        double       org[3], dir[3];
+        for (int a = 0; a < 3; a++)
+        {
+          org[a] = D[0 * 3 + a] * src[0] + D[1 * 3 + a] * src[1] + D[2 * 3 + a] * src[2];
+          dir[a] = (D[0 * 3 + a] * d[0] + D[1 * 3 + a] * d[1] + D[2 * 3 + a] * d[2]) / len;
+        }
+        double inf = -DBL_MAX, sup = DBL_MAX;
+        int    hit = 1;
+        for (int a = 0; a < 3 && hit; a++)
+        {
+          if (dir[a] == 0. && (org[a] < mn[a] || org[a] > mx[a]))
+          {
+            hit = 0;
+            break;
+          }
+          const double inv = 1. / dir[a];
+          double       t1 = (mn[a] - org[a]) * inv, t2 = (mx[a] - org[a]) * inv;
+          if (t1 > t2)
+          {
+            const double t = t1;
+            t1 = t2;
+            t2 = t;
+          }
+          inf = fmax(t1, inf);
+          sup = fmin(t2, sup);
+          if (inf > sup || sup < 0.)
+            hit = 0;
+        }
+        out[((long)s * nv + j) * nu + i] = hit ? sup - inf : 0.;
+      }
+  }
+}
+
+void
+orc_sart(const orc_geometry * g, const orc_image * vol, const orc_image * proj, const double * proj_data, double * x,
+         int niter, double lambda, int positivity, int projections_per_subset, int displaced_detector,
+         double threshold, const int * order, int nthreads)
+{
+  /* SARTConeBeamReconstructionFilter::GenerateData (include/rtkSARTConeBeamReconstructionFilter.hxx):
+   * for each projection s in `order`: e = lambda (p_s - JosephFP_s(x)),
+   * divided (or zeroed below threshold) by the ray-box length, displaced-
+   * detector weighted (no padding), voxel-based back projected into B, and
+   * ones back projected into N; after every `projections_per_subset`
+   * projections (and after the last one) x += B / N (or 0 below threshold),
+   * then x = max(x, 0) with positivity. */
+  const long per = (long)proj->size[0] * proj->size[1], nvx = npix(vol);
+  const int  np = proj->size[2];
+  double *   rb = (double *)malloc(sizeof(double) * per * np);
+  double *   fp = (double *)malloc(sizeof(double) * per);
+  double *   e = (double *)malloc(sizeof(double) * per);
+  double *   e2 = (double *)malloc(sizeof(double) * per);
+  double *   ones = (double *)malloc(sizeof(double) * per);
+  double *   B = (double *)calloc(nvx, sizeof(double));
+  double *   N = (double *)calloc(nvx, sizeof(double));
+  orc_ray_box(g, vol, proj, rb, nthreads);
+  for (long q = 0; q < per; q++)
+    ones[q] = 1.;
+  for (int it = 0; it < niter; it++)
+  {
+    int count = 0;
+    for (int i = 0; i < np; i++)
+    {
+      const int  s = order[i];
+      orc_image  p1 = *proj;
+      p1.size[2] = 1;
+      p1.index[2] = proj->index[2] + s;
+      memset(fp, 0, sizeof(double) * per);
+      orc_joseph_forward(g, vol, x, &p1, fp, fp, nthreads);
+      for (long q = 0; q < per; q++)
+      {
+        const double den = rb[(long)s * per + q];
+        e[q] = den < threshold ? 0. : lambda * (proj_data[(long)s * per + q] - fp[q]) / den;
+      }
+      if (displaced_detector)
+        orc_displaced_detector(g, &p1, 0, e, e2);
+      else
+        memcpy(e2, e, sizeof(double) * per);
+      if (count == 0)
+      {
+        memset(B, 0, sizeof(double) * nvx);
+        memset(N, 0, sizeof(double) * nvx);
+      }
+      orc_backproject(g, vol, &p1, e2, B, B, 0, nthreads);
+      orc_backproject(g, vol, &p1, ones, N, N, 0, nthreads);
+      if (++count == projections_per_subset || i == np - 1)
+      {
+        for (long v = 0; v < nvx; v++)
+        {
+          x[v] += N[v] < threshold ? 0. : B[v] / N[v];
+          if (positivity && x[v] < 0.)
+            x[v] = 0.;
+        }
+        count = 0;
+      }
+    }
+  }
+  free(rb);
+  free(fp);
+  free(e);
+  free(e2);
+  free(ones);
+  free(B);
+  free(N);
+}

@@ -122,6 +122,12 @@ void orc_ramp_filter(const orc_image * proj, const orc_ramp_params * p, const do
 void orc_cg_joseph(const orc_geometry * g, const orc_image * vol, const orc_image * proj, const double * proj_data,
                    const double * weights, double tikhonov, double gamma, int niter, double * x, double * residuals,
                    int nthreads);
+/* RayBoxIntersectionImageFilter with SetBoxFromImage(vol, false): per-pixel length (mm) of the ray in the box */
+void orc_ray_box(const orc_geometry * g, const orc_image * vol, const orc_image * proj, double * out, int nthreads);
+/* SARTConeBeamReconstructionFilter with the Joseph forward and voxel-based back projectors, in place on x */
+void orc_sart(const orc_geometry * g, const orc_image * vol, const orc_image * proj, const double * proj_data, double * x,
+              int niter, double lambda, int positivity, int projections_per_subset, int displaced_detector,
+              double threshold, const int * order, int nthreads);
 /* RTK's LaplacianImageFilter (Neumann boundary, spacing-scaled): out = Laplacian(x) */
 void orc_laplacian(const orc_image * vol, const double * x, double * out);
 

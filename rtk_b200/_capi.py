@@ -166,6 +166,8 @@ SIGNATURES.update({
     "rtkb_geometry_write_xml": (C.c_int, [_G, C.c_char_p]),
     "rtkb_image_read_mha": (C.c_int, [C.c_char_p, _IM, _V, C.c_longlong]),
     "rtkb_laplacian": (C.c_int, [_IM, _V, _V, _V]),
+    "rtkb_ray_box_lengths": (C.c_int, [_G, _IM, _IM, _V, _V]),
+    "rtkb_sart": (C.c_int, [_G, _IM, _IM, _V, _V, C.c_void_p, _V]),
     "rtkb_image_write_mha": (C.c_int, [C.c_char_p, _IM, _V, C.c_int]),
 })
 
@@ -227,3 +229,11 @@ SIGNATURES.update({
     "rtkb_bp_batch_config": (C.c_int, [_V]),
     "rtkb_bp_batch_destroy": (None, [_V]),
 })
+
+
+class SartParams(C.Structure):
+    """rtkb_sart_params."""
+
+    _fields_ = [("niter", C.c_int), ("lam", C.c_double), ("positivity", C.c_int),
+                ("projections_per_subset", C.c_int), ("disable_displaced_detector", C.c_int),
+                ("division_threshold", C.c_double), ("order", C.POINTER(C.c_int)), ("seed", C.c_ulonglong)]

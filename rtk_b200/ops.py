@@ -232,6 +232,43 @@ def laplacian(vol_desc, x, out=None, stream=None):
     return out
 
 
+def ray_box_lengths(geometry, vol_desc, proj_desc, out=None, stream=None):
+    """rtk::RayBoxIntersectionImageFilter (box of the volume, SetBoxFromImage(vol,
+    false)): per-pixel ray length in mm."""
+    if out is None:
+        out = _torch().empty(shape_of(proj_desc), device="cuda", dtype=_torch().float32)
+    _check_shape(out, proj_desc, "output")
+    check(load().rtkb_ray_box_lengths(geometry.handle, C.byref(vol_desc), C.byref(proj_desc), _ptr(out),
+                                      _stream(stream)))
+    return out
+
+
+def sart(geometry, vol_desc, proj_desc, proj, x, niter=3, lam=0.3, positivity=False, subset=1,
+         displaced_detector=True, threshold=1e-5, order=None, seed=0, stream=None):
+    """rtk::SARTConeBeamReconstructionFilter (Joseph forward, voxel-based back
+    projection), in place on x; order: processing order of the stack's
+    projections (a permutation), or None for a seeded shuffle."""
+    import numpy as np
+
+    from ._capi import SartParams
+
+    _check_shape(proj, proj_desc, "projections")
+    _check_shape(x, vol_desc, "volume")
+    p = SartParams()
+    p.niter, p.lam, p.positivity = int(niter), float(lam), int(positivity)
+    p.projections_per_subset, p.disable_displaced_detector = int(subset), int(not displaced_detector)
+    p.division_threshold, p.seed = float(threshold), int(seed)
+    keep = None
+    if order is not None:
+        keep = np.ascontiguousarray(order, dtype=np.int32)
+        if keep.size != proj_desc.size[2]:
+            raise ValueError("order must list every projection of the stack")
+        p.order = keep.ctypes.data_as(C.POINTER(C.c_int))
+    check(load().rtkb_sart(geometry.handle, C.byref(vol_desc), C.byref(proj_desc), _ptr(proj), _ptr(x), C.byref(p),
+                           _stream(stream)))
+    return x
+
+
 def _storage_code(storage):
     codes = {"fp32": 0, "bf16": 1}
     if storage not in codes:

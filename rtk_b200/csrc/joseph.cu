@@ -234,7 +234,7 @@ border_taps(const JosephArgs & a, const Ray & r, const View & w, int sl, double 
 // 64 registers give 4 CTAs per SM: the loop is bound by gather latency, and
 // the FP64 ray state is dead before it starts (the last border step is taken
 // first; the sums are still added in ray order).
-template <typename Off, typename TP>
+template <typename Off, typename TP, bool kQuads>
 __global__ void __launch_bounds__(256, 4)
 joseph_forward_kernel(JosephArgs a, const float * __restrict__ V, const float * __restrict__ Vt,
                       const float4 * __restrict__ QN, const float4 * __restrict__ QT, const TP * pin, TP * pout,
@@ -282,7 +282,7 @@ joseph_forward_kernel(JosephArgs a, const float * __restrict__ V, const float * 
     const long long first = (long long)(r.ns + r.dz - w.bz) * w.oz, dslice = r.dz * w.oz;
     const float2    m1 = make_float2(-1.f, -1.f);
     float           acc = 0.f;
-    if (r.main != 1)
+    if (kQuads && r.main != 1)
     {
       const float4 * slice = (w.transposed ? QT : QN) + first;
       for (int i = 0; i < nmid; i++, slice += dslice)
@@ -634,6 +634,11 @@ widen_kernel(const __nv_bfloat16 * __restrict__ in, float * __restrict__ out, lo
     out[i] = __bfloat162float(in[i]);
 }
 
+// The quad copies cost two passes over 5x the volume's bytes: they pay off
+// over a stack, not for one or two projections (SART's subsets), which take
+// the four-tap loop directly.
+constexpr int kQuadMinProjections = 4;
+
 template <typename TP>
 cudaError_t
 forward_launch(const JosephArgs & a, const float * V, float * Vt, float4 * QN, float4 * QT, const TP * pin, TP * pout,
@@ -641,16 +646,25 @@ forward_launch(const JosephArgs & a, const float * V, float * Vt, float4 * QN, f
 {
   const int       nx = a.n[0], ny = a.n[1], nz = a.n[2];
   const long long nvox = (long long)nx * ny * nz;
+  const bool      quads = a.np >= kQuadMinProjections;
   const dim3      tg((unsigned)(((nx + 31) / 32) * ((nz + 31) / 32)), (unsigned)ny);
   transpose_zx_kernel<<<tg, 256, 0, st>>>(V, Vt, nx, ny, nz);
-  const unsigned qg = (unsigned)std::min<long long>((nvox + 255) / 256, 148LL * 32);
-  quad_kernel<<<qg, 256, 0, st>>>(V, QN, nx, ny, nvox, true);  // a = x, b = y
-  quad_kernel<<<qg, 256, 0, st>>>(Vt, QT, nz, ny, nvox, false); // a = y, b = z
+  if (quads)
+  {
+    const unsigned qg = (unsigned)std::min<long long>((nvox + 255) / 256, 148LL * 32);
+    quad_kernel<<<qg, 256, 0, st>>>(V, QN, nx, ny, nvox, true);  // a = x, b = y
+    quad_kernel<<<qg, 256, 0, st>>>(Vt, QT, nz, ny, nvox, false); // a = y, b = z
+  }
   const dim3 grid((unsigned)((a.nu + 31) / 32), (unsigned)a.np, (unsigned)((a.nv + 7) / 8));
-  if (nvox < (1ll << 31))
-    joseph_forward_kernel<int, TP><<<grid, 256, 0, st>>>(a, V, Vt, QN, QT, pin, pout, w);
+  const bool small = nvox < (1ll << 31);
+  if (quads && small)
+    joseph_forward_kernel<int, TP, true><<<grid, 256, 0, st>>>(a, V, Vt, QN, QT, pin, pout, w);
+  else if (quads)
+    joseph_forward_kernel<long long, TP, true><<<grid, 256, 0, st>>>(a, V, Vt, QN, QT, pin, pout, w);
+  else if (small)
+    joseph_forward_kernel<int, TP, false><<<grid, 256, 0, st>>>(a, V, Vt, QN, QT, pin, pout, w);
   else
-    joseph_forward_kernel<long long, TP><<<grid, 256, 0, st>>>(a, V, Vt, QN, QT, pin, pout, w);
+    joseph_forward_kernel<long long, TP, false><<<grid, 256, 0, st>>>(a, V, Vt, QN, QT, pin, pout, w);
   return cudaGetLastError();
 }
 

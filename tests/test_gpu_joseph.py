@@ -121,3 +121,15 @@ def test_joseph_sample_count_matches_oracle(rtkb, oracle, geom):
     gl, go, vd, vo, pd, po, vol, pr = _case(rtkb, oracle, GEOMS[geom](30), (40, 36, 44), (4.0, 4.5, 3.5),
                                             (72, 64, 30), (5.0, 5.0, 1.0), vindex=(2, -3, 1), pindex=(-4, 3, 0))
     assert rtkb.ops.joseph_sample_count(gl, vd, pd) == oracle.joseph_sample_count(go, vo, po)
+
+
+def test_joseph_forward_short_stack_without_quads(rtkb, oracle):
+    """Stacks of fewer than four projections (SART's subsets) take the four-tap
+    loop without the quad copies: main-z (0 deg) and main-x (95 deg) rays."""
+    params = [(700.0, 1100.0, 0.0, 6.0, -3.0), (700.0, 1100.0, 95.0, 6.0, -3.0)]
+    gl, go, vd, vo, pd, po, vol, pr = _case(rtkb, oracle, params, (40, 32, 36), (4.0,) * 3, (72, 60, 2),
+                                            (3.0, 3.0, 1.0))
+    ref = oracle.joseph_forward(go, vo, vol, po, pr)
+    got = to_np(rtkb.ops.joseph_forward_project(gl, vd, pd, to_gpu(vol), to_gpu(pr)))
+    assert rtkb.ops.device_status() == 0
+    assert rel_l2(got, ref) < REL_L2_TOL, rel_l2(got, ref)

@@ -415,6 +415,43 @@ def sart_leg(torch, rtkb, stream, niter=1):
             "seconds_per_iteration_wall": wall / niter, "relative_projection_misfit_after": misfit}
 
 
+def osem_leg(torch, rtkb, stream, niter=3, subset=10):
+    """OSEM (RTK's default niter 3 and back projector, voxel-based; 10
+    projections per subset as in RTK's OSEM test; Joseph forward projection)
+    on the CG configuration's problem: 256^3 at 1 mm from 360 projections of
+    512x384 at 0.8 mm, seeded order, from a constant volume of 0.01.  Timed
+    without (beta 0, ML-EM updates) and with De Pierro's term (beta 0.01)."""
+    from tests import phantoms
+
+    n = 360
+    g = rtkb.geometry.circular(n, SID, SDD)
+    vd = rtkb.make_desc((256, 256, 256), (1.0, 1.0, 1.0))
+    pd = rtkb.make_desc((512, 384, n), (0.8, 0.8, 1.0))
+    ell = phantoms.random_ellipsoids(20, SEED + 2, centre_radius=60.0, axis_range=(5.0, 60.0))
+    ell[:, 15] *= 0.02
+    p = rtkb.ops.project_ellipsoids(g, pd, ell, stream=stream)
+    x = torch.full((256, 256, 256), 0.01, device="cuda")
+    for beta in (0.0, 0.01):  # warm-up of both update kernels (allocations, host tables, module loading)
+        rtkb.ops.osem(g, vd, pd, p, x, niter=2, subset=subset, beta=beta, seed=1, stream=stream)
+    out = {"workload": f"OSEM, 256^3 @1mm <- 360 x 512x384 @0.8mm, {subset} projections per subset, "
+                       "Joseph forward / voxel-based back projection", "iterations": niter}
+    for beta in (0.0, 0.01):
+        x.fill_(0.01)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rtkb.ops.osem(g, vd, pd, p, x, niter=niter, subset=subset, beta=beta, seed=1, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        fp = rtkb.ops.joseph_forward_project(g, vd, pd, x, torch.zeros_like(p), stream=stream)
+        misfit = float((fp - p).double().norm() / p.double().norm())
+        out[f"beta_{beta:g}"] = {"seconds_device": e0.elapsed_time(e1) / 1e3, "seconds_wall": wall,
+                                 "relative_projection_misfit_after": misfit}
+    return out
+
+
 def cg_seconds_to_residual(torch, rtkb, stream, tol=1e-3, max_iter=300, learned_pcg=True):
     """CG configuration: 256^3 at 1 mm, 360 projections of 512x384 at 0.8 mm
     (SID 1000, SDD 1536) of 20 seeded random ellipsoids with pre-log Poisson
@@ -834,6 +871,7 @@ def main():
         line["batched"] = batch_leg(torch, rtkb, stream)
         line["batched_cg"] = batch_cg_leg(torch, rtkb, stream)
         line["sart"] = sart_leg(torch, rtkb, stream)
+        line["osem"] = osem_leg(torch, rtkb, stream)
         line["cg"] = cg_seconds_to_residual(torch, rtkb, stream)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:

@@ -350,6 +350,39 @@ typedef struct rtkb_sart_params
 } rtkb_sart_params;
 int rtkb_sart(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj, const float * d_proj,
               float * d_x, const rtkb_sart_params * params, void * stream);
+/* rtk::OSEMConeBeamReconstructionFilter
+ * (include/rtkOSEMConeBeamReconstructionFilter.hxx:84-273) with the Joseph
+ * forward projector and the voxel-based (BP_VOXELBASED, RTK's default) or
+ * Joseph (BP_JOSEPH) back projector, in place on d_x.  Per subset:
+ * x = (x BP(p / FP(x))) / R with De Pierro's factor R
+ * (rtk::DePierroRegularizationImageFilter; R = BP(1) when beta = 0); both
+ * divisions are itk::DivideOrZeroOutImageFilter's (threshold 1e-5, constants 1
+ * and 0).  order / seed as for SART.  store_normalization keeps BP(1) of each
+ * subset on the device after the first iteration (RTK's
+ * StoreNormalizationImages; the result is the same either way).  Defaults in
+ * RTK: niter 3, 1 projection per subset, beta 0, normalisation stored. */
+#define RTKB_OSEM_BP_VOXEL 0
+#define RTKB_OSEM_BP_JOSEPH 1
+typedef struct rtkb_osem_params
+{
+  int                niter;
+  int                projections_per_subset;
+  double             beta;
+  int                store_normalization;
+  int                backprojector;
+  const int *        order;
+  unsigned long long seed;
+} rtkb_osem_params;
+int rtkb_osem(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj, const float * d_proj,
+              float * d_x, const rtkb_osem_params * params, void * stream);
+/* rtk::DePierroRegularizationImageFilter
+ * (include/rtkDePierroRegularizationImageFilter.hxx:26-131): d_out =
+ * (A + sqrt(A^2 + 8 beta 26 d_update)) / 2, A = d_norm - beta K(d_xk), K the
+ * 3x3x3 neighbourhood sum (26 at the centre, 1 elsewhere, zero outside the
+ * image).  d_norm NULL: a volume of ones (the filter's default normalisation).
+ * d_out may alias d_update or d_norm, and d_xk only when beta = 0. */
+int rtkb_de_pierro_regularization(const rtkb_image_desc * vol, const float * d_xk, const float * d_update,
+                                  const float * d_norm, double beta, float * d_out, void * stream);
 /* d_out = A d_in with the plan's operator (weights W = 1 until rtkb_cg_start
  * sets them).  Used to generate (A e, e) training pairs for the learned
  * preconditioner.  No reference counterpart (RTK's operator is internal to

@@ -97,6 +97,8 @@ def lib():
             "orc_ray_box": (None, [G, IM, IM, D, C.c_int]),
             "orc_sart": (None, [G, IM, IM, D, D, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_double,
                                 C.POINTER(C.c_int), C.c_int]),
+            "orc_de_pierro": (None, [IM, D, D, D, C.c_double, D]),
+            "orc_osem": (None, [G, IM, IM, D, D, C.c_int, C.c_int, C.c_double, C.c_int, C.POINTER(C.c_int), C.c_int]),
             "orc_project_ellipsoids": (None, [G, IM, C.c_int, D, D, C.c_int]),
             "orc_draw_ellipsoids": (None, [IM, C.c_int, D, D, C.c_int]),
             "orc_fdk_backproject_f32_rtk": (C.c_int, [G, IM, IM, F, F, C.c_int]),
@@ -318,6 +320,26 @@ def sart(g, vol, proj, proj_data, niter, order, x0=None, lam=0.3, positivity=Fal
     lib().orc_sart(g._g, C.byref(vol), C.byref(proj), _d(p), _d(x), int(niter), float(lam), int(positivity),
                    int(subset), int(displaced_detector), float(threshold),
                    o.ctypes.data_as(C.POINTER(C.c_int)), threads or nthreads())
+    return x
+
+
+def de_pierro(vol, xk, update, norm, beta):
+    """DePierroRegularizationImageFilter; norm None = a volume of ones."""
+    a = np.ascontiguousarray(xk, dtype=np.float64)
+    u = np.ascontiguousarray(update, dtype=np.float64)
+    n = None if norm is None else np.ascontiguousarray(norm, dtype=np.float64)
+    out = np.empty(shape_of(vol))
+    lib().orc_de_pierro(C.byref(vol), _d(a), _d(u), _d(n), float(beta), _d(out))
+    return out
+
+
+def osem(g, vol, proj, proj_data, niter, order, x0, subset=1, beta=0.0, joseph_bp=False, threads=None):
+    """OSEMConeBeamReconstructionFilter (Joseph forward projector; voxel-based or Joseph back projector)."""
+    p = np.ascontiguousarray(proj_data, dtype=np.float64)
+    x = np.array(x0, dtype=np.float64, copy=True, order="C")
+    o = np.ascontiguousarray(order, dtype=np.int32)
+    lib().orc_osem(g._g, C.byref(vol), C.byref(proj), _d(p), _d(x), int(niter), int(subset), float(beta),
+                   int(joseph_bp), o.ctypes.data_as(C.POINTER(C.c_int)), threads or nthreads())
     return x
 
 

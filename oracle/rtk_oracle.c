@@ -1867,3 +1867,104 @@ orc_sart(const orc_geometry * g, const orc_image * vol, const orc_image * proj, 
   free(B);
   free(N);
 }
+
+void
+orc_de_pierro(const orc_image * vol, const double * xk, const double * update, const double * norm, double beta,
+              double * out)
+{
+  /* DePierroRegularizationImageFilter (include/rtkDePierroRegularizationImageFilter.hxx:26-131):
+   * K = 3x3x3 neighbourhood inner product with weight 3^3 - 1 = 26 at the
+   * centre and 1 elsewhere, zero outside the image (ConstantBoundaryCondition);
+   * A = norm - beta K(xk) (norm = 1 when absent); B = 4 * 2 * beta * 26 * update;
+   * out = (A + sqrt(A^2 + B)) / 2. */
+  const long nx = vol->size[0], ny = vol->size[1], nz = vol->size[2];
+  for (long z = 0; z < nz; z++)
+    for (long y = 0; y < ny; y++)
+      for (long x = 0; x < nx; x++)
+      {
+        const long i = (z * ny + y) * nx + x;
+        double     k = 0.;
+        for (long dz = -1; dz <= 1; dz++)
+          for (long dy = -1; dy <= 1; dy++)
+            for (long dx = -1; dx <= 1; dx++)
+            {
+              const long zz = z + dz, yy = y + dy, xx = x + dx;
+              if (zz < 0 || zz >= nz || yy < 0 || yy >= ny || xx < 0 || xx >= nx)
+                continue;
+              k += ((dx | dy | dz) == 0 ? 26. : 1.) * xk[(zz * ny + yy) * nx + xx];
+            }
+        const double a = (norm ? norm[i] : 1.) - beta * k;
+        const double b = 4. * 2. * beta * 26. * update[i];
+        out[i] = (a + sqrt(a * a + b)) / 2.;
+      }
+}
+
+void
+orc_osem(const orc_geometry * g, const orc_image * vol, const orc_image * proj, const double * proj_data, double * x,
+         int niter, int projections_per_subset, double beta, int joseph_bp, const int * order, int nthreads)
+{
+  /* OSEMConeBeamReconstructionFilter::GenerateData
+   * (include/rtkOSEMConeBeamReconstructionFilter.hxx:161-273): for each
+   * projection s in `order`, r = p_s / JosephFP_s(x) (1 where
+   * |FP| < 1e-5: DivideOrZeroOutImageFilter with constant 1), back projected
+   * (voxel-based, or Joseph with joseph_bp) into B, ones back projected into N;
+   * after every `projections_per_subset` projections (and after the last one)
+   * M = B x, R = DePierro(x, M, N) and x = M / R (0 where |R| < 1e-5).  The
+   * normalisation images are recomputed every iteration; storing them, as RTK
+   * does by default, gives the same values. */
+  const long per = (long)proj->size[0] * proj->size[1], nvx = npix(vol);
+  const int  np = proj->size[2];
+  double *   fp = (double *)malloc(sizeof(double) * per);
+  double *   ones = (double *)malloc(sizeof(double) * per);
+  double *   B = (double *)calloc(nvx, sizeof(double));
+  double *   N = (double *)calloc(nvx, sizeof(double));
+  double *   M = (double *)malloc(sizeof(double) * nvx);
+  double *   R = (double *)malloc(sizeof(double) * nvx);
+  for (long q = 0; q < per; q++)
+    ones[q] = 1.;
+  for (int it = 0; it < niter; it++)
+  {
+    int count = 0;
+    for (int i = 0; i < np; i++)
+    {
+      const int s = order[i];
+      orc_image p1 = *proj;
+      p1.size[2] = 1;
+      p1.index[2] = proj->index[2] + s;
+      memset(fp, 0, sizeof(double) * per);
+      orc_joseph_forward(g, vol, x, &p1, fp, fp, nthreads);
+      for (long q = 0; q < per; q++)
+        fp[q] = fabs(fp[q]) < 1e-5 ? 1. : proj_data[(long)s * per + q] / fp[q];
+      if (count == 0)
+      {
+        memset(B, 0, sizeof(double) * nvx);
+        memset(N, 0, sizeof(double) * nvx);
+      }
+      if (joseph_bp)
+      {
+        orc_joseph_back(g, vol, B, B, &p1, fp);
+        orc_joseph_back(g, vol, N, N, &p1, ones);
+      }
+      else
+      {
+        orc_backproject(g, vol, &p1, fp, B, B, 0, nthreads);
+        orc_backproject(g, vol, &p1, ones, N, N, 0, nthreads);
+      }
+      if (++count == projections_per_subset || i == np - 1)
+      {
+        for (long v = 0; v < nvx; v++)
+          M[v] = B[v] * x[v];
+        orc_de_pierro(vol, x, M, N, beta, R);
+        for (long v = 0; v < nvx; v++)
+          x[v] = fabs(R[v]) < 1e-5 ? 0. : M[v] / R[v];
+        count = 0;
+      }
+    }
+  }
+  free(fp);
+  free(ones);
+  free(B);
+  free(N);
+  free(M);
+  free(R);
+}

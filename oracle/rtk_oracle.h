@@ -128,6 +128,14 @@ void orc_ray_box(const orc_geometry * g, const orc_image * vol, const orc_image 
 void orc_sart(const orc_geometry * g, const orc_image * vol, const orc_image * proj, const double * proj_data, double * x,
               int niter, double lambda, int positivity, int projections_per_subset, int displaced_detector,
               double threshold, const int * order, int nthreads);
+/* DePierroRegularizationImageFilter: out = (A + sqrt(A^2 + 8 beta 26 update)) / 2,
+ * A = norm - beta K(xk), K the 26-neighbour sum plus 26 xk (zero outside); norm may be NULL (ones) */
+void orc_de_pierro(const orc_image * vol, const double * xk, const double * update, const double * norm, double beta,
+                   double * out);
+/* OSEMConeBeamReconstructionFilter with the Joseph forward projector and the voxel-based (joseph_bp = 0) or Joseph
+ * back projector, in place on x */
+void orc_osem(const orc_geometry * g, const orc_image * vol, const orc_image * proj, const double * proj_data, double * x,
+              int niter, int projections_per_subset, double beta, int joseph_bp, const int * order, int nthreads);
 /* RTK's LaplacianImageFilter (Neumann boundary, spacing-scaled): out = Laplacian(x) */
 void orc_laplacian(const orc_image * vol, const double * x, double * out);
 

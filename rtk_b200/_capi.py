@@ -168,6 +168,8 @@ SIGNATURES.update({
     "rtkb_laplacian": (C.c_int, [_IM, _V, _V, _V]),
     "rtkb_ray_box_lengths": (C.c_int, [_G, _IM, _IM, _V, _V]),
     "rtkb_sart": (C.c_int, [_G, _IM, _IM, _V, _V, C.c_void_p, _V]),
+    "rtkb_osem": (C.c_int, [_G, _IM, _IM, _V, _V, C.c_void_p, _V]),
+    "rtkb_de_pierro_regularization": (C.c_int, [_IM, _V, _V, _V, C.c_double, _V, _V]),
     "rtkb_image_write_mha": (C.c_int, [C.c_char_p, _IM, _V, C.c_int]),
 })
 
@@ -237,3 +239,11 @@ class SartParams(C.Structure):
     _fields_ = [("niter", C.c_int), ("lam", C.c_double), ("positivity", C.c_int),
                 ("projections_per_subset", C.c_int), ("disable_displaced_detector", C.c_int),
                 ("division_threshold", C.c_double), ("order", C.POINTER(C.c_int)), ("seed", C.c_ulonglong)]
+
+
+class OsemParams(C.Structure):
+    """rtkb_osem_params."""
+
+    _fields_ = [("niter", C.c_int), ("projections_per_subset", C.c_int), ("beta", C.c_double),
+                ("store_normalization", C.c_int), ("backprojector", C.c_int), ("order", C.POINTER(C.c_int)),
+                ("seed", C.c_ulonglong)]

@@ -84,6 +84,10 @@ typedef int (*EncodeTiledFn)(void *, int, unsigned, void *, const unsigned long 
                              const unsigned *, const unsigned *, int, int, int, int);
 EncodeTiledFn tensor_map_encoder();
 
+// Projection processing order of the iterative solvers when the caller gives
+// none: 0..n-1 shuffled by Fisher-Yates driven by SplitMix64(seed).
+void seeded_order(int n, unsigned long long seed, std::vector<int> & order);
+
 } // namespace rtkb
 
 struct rtkb_geometry

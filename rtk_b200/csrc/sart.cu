@@ -127,25 +127,6 @@ grid_of(long long n)
   return (unsigned)std::min<long long>((n + 255) / 256, 148LL * 16);
 }
 
-// SplitMix64 (Steele, Lea and Flood 2014) driving a Fisher-Yates shuffle
-void
-seeded_order(int n, unsigned long long seed, std::vector<int> & order)
-{
-  order.resize(n);
-  std::iota(order.begin(), order.end(), 0);
-  uint64_t state = seed;
-  auto     next = [&]() {
-    uint64_t z = (state += 0x9E3779B97F4A7C15ull);
-    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-    return z ^ (z >> 31);
-  };
-  for (int i = n - 1; i > 0; i--)
-  {
-    const int j = (int)(next() % (uint64_t)(i + 1));
-    std::swap(order[i], order[j]);
-  }
-}
 
 int
 ray_box_lengths(const rtkb_geometry * g, const rtkb_image_desc & vol, const rtkb_image_desc & proj, float * d_out,
@@ -202,6 +183,29 @@ ray_box_lengths(const rtkb_geometry * g, const rtkb_image_desc & vol, const rtkb
   return rc;
 }
 } // namespace
+
+namespace rtkb
+{
+// SplitMix64 (Steele, Lea and Flood 2014) driving a Fisher-Yates shuffle
+void
+seeded_order(int n, unsigned long long seed, std::vector<int> & order)
+{
+  order.resize(n);
+  std::iota(order.begin(), order.end(), 0);
+  uint64_t state = seed;
+  auto     next = [&]() {
+    uint64_t z = (state += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+  };
+  for (int i = n - 1; i > 0; i--)
+  {
+    const int j = (int)(next() % (uint64_t)(i + 1));
+    std::swap(order[i], order[j]);
+  }
+}
+} // namespace rtkb
 
 extern "C" int
 rtkb_ray_box_lengths(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj, float * d_out,

@@ -269,6 +269,51 @@ def sart(geometry, vol_desc, proj_desc, proj, x, niter=3, lam=0.3, positivity=Fa
     return x
 
 
+def osem(geometry, vol_desc, proj_desc, proj, x, niter=3, subset=1, beta=0.0, store_normalization=True,
+         backprojector="voxel", order=None, seed=0, stream=None):
+    """rtk::OSEMConeBeamReconstructionFilter (Joseph forward projection;
+    backprojector "voxel", RTK's default, or "joseph") with De Pierro's
+    regularisation weight beta, in place on x; order: processing order of
+    the stack's projections (a permutation), or None for a seeded shuffle."""
+    import numpy as np
+
+    from ._capi import OsemParams
+
+    codes = {"voxel": 0, "joseph": 1}
+    if backprojector not in codes:
+        raise ValueError(f"backprojector must be one of {sorted(codes)}")
+    _check_shape(proj, proj_desc, "projections")
+    _check_shape(x, vol_desc, "volume")
+    p = OsemParams()
+    p.niter, p.projections_per_subset, p.beta = int(niter), int(subset), float(beta)
+    p.store_normalization, p.backprojector, p.seed = int(store_normalization), codes[backprojector], int(seed)
+    keep = None
+    if order is not None:
+        keep = np.ascontiguousarray(order, dtype=np.int32)
+        if keep.size != proj_desc.size[2]:
+            raise ValueError("order must list every projection of the stack")
+        p.order = keep.ctypes.data_as(C.POINTER(C.c_int))
+    check(load().rtkb_osem(geometry.handle, C.byref(vol_desc), C.byref(proj_desc), _ptr(proj), _ptr(x), C.byref(p),
+                           _stream(stream)))
+    return x
+
+
+def de_pierro_regularization(vol_desc, xk, update, norm=None, beta=0.01, out=None, stream=None):
+    """rtk::DePierroRegularizationImageFilter: inputs x_k, the ML-EM update and
+    the normalisation volume (None: ones); returns the regularisation factor."""
+    _check_shape(xk, vol_desc, "x_k")
+    _check_shape(update, vol_desc, "update")
+    if norm is not None:
+        _check_shape(norm, vol_desc, "normalisation")
+    if out is None:
+        out = _torch().empty_like(xk)
+    _check_shape(out, vol_desc, "output")
+    check(load().rtkb_de_pierro_regularization(C.byref(vol_desc), _ptr(xk), _ptr(update),
+                                               None if norm is None else _ptr(norm), float(beta), _ptr(out),
+                                               _stream(stream)))
+    return out
+
+
 def _storage_code(storage):
     codes = {"fp32": 0, "bf16": 1}
     if storage not in codes:

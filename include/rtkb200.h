@@ -65,6 +65,15 @@ const char * rtkb_version(void);
  * kernels set when a bounded wait gives up (RTKB_ERR_TIMEOUT) or an internal
  * check fails.  *status receives 0 when no kernel reported a problem. */
 int rtkb_device_status(void * stream, int * status);
+/* Temporary device memory of every entry point comes from one stream-ordered
+ * memory pool per device that the library owns; memory freed there stays
+ * reserved for later calls (the caller's default pool is not touched).
+ * rtkb_trim_memory_pool returns the unused part to the driver (*reserved_after,
+ * may be NULL: bytes still reserved, those of work not yet finished in stream
+ * order); rtkb_memory_pool_reserved reads the reserved size.  Current device.
+ * No reference counterpart (ITK's CUDA images allocate per image). */
+int rtkb_trim_memory_pool(long long * reserved_after);
+int rtkb_memory_pool_reserved(long long * reserved);
 
 /* ---- geometry: rtk::ThreeDCircularProjectionGeometry, FP64 ----
  * src/rtkThreeDCircularProjectionGeometry.cxx:56-153 (AddProjection),

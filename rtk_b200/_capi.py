@@ -169,6 +169,8 @@ SIGNATURES.update({
     "rtkb_ray_box_lengths": (C.c_int, [_G, _IM, _IM, _V, _V]),
     "rtkb_sart": (C.c_int, [_G, _IM, _IM, _V, _V, C.c_void_p, _V]),
     "rtkb_osem": (C.c_int, [_G, _IM, _IM, _V, _V, C.c_void_p, _V]),
+    "rtkb_trim_memory_pool": (C.c_int, [C.POINTER(C.c_longlong)]),
+    "rtkb_memory_pool_reserved": (C.c_int, [C.POINTER(C.c_longlong)]),
     "rtkb_de_pierro_regularization": (C.c_int, [_IM, _V, _V, _V, C.c_double, _V, _V]),
     "rtkb_image_write_mha": (C.c_int, [C.c_char_p, _IM, _V, C.c_int]),
 })

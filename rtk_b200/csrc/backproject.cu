@@ -929,7 +929,7 @@ backproject_buffer(const int vol_size[3], const int proj_size[3], int nproj, con
   const size_t mbytes = sizeof(double) * 12 * (size_t)nproj;
   void *       scratch = fixed_scratch;
   if (!scratch)
-    RTKB_CUDA_TRY(cudaMallocAsync(&scratch, mbytes + sizeof(int) * nproj, st));
+    RTKB_CUDA_TRY(rtkb::scratch_malloc(&scratch, mbytes + sizeof(int) * nproj, st));
   double * d_mats = static_cast<double *>(scratch);
   int *    d_modes = reinterpret_cast<int *>(static_cast<char *>(scratch) + mbytes);
   int      rc = RTKB_OK;
@@ -1002,7 +1002,7 @@ backproject_buffer(const int vol_size[3], const int proj_size[3], int nproj, con
   } while (0);
   if (!fixed_scratch)
   {
-    cudaError_t fe = cudaFreeAsync(scratch, st);
+    cudaError_t fe = rtkb::scratch_free(scratch, st);
     if (rc == RTKB_OK && fe != cudaSuccess)
       rc = cuda_fail(fe, "cudaFreeAsync");
   }
@@ -1344,7 +1344,7 @@ fdk_backproject_host(const rtkb_geometry * g, const rtkb_image_desc * vol, const
   cudaEvent_t   ev[kEvents] = {};
   void *        mem = nullptr;
   int           rc = RTKB_OK;
-  RTKB_CUDA_TRY(cudaMallocAsync(&mem, vbytes + nstage * sbytes, st));
+  RTKB_CUDA_TRY(rtkb::scratch_malloc(&mem, vbytes + nstage * sbytes, st));
   do
   {
     cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
@@ -1446,7 +1446,7 @@ fdk_backproject_host(const rtkb_geometry * g, const rtkb_image_desc * vol, const
       cudaEventDestroy(ev[i]);
   if (cs)
     cudaStreamDestroy(cs);
-  cudaError_t fe = cudaFreeAsync(mem, st);
+  cudaError_t fe = rtkb::scratch_free(mem, st);
   if (rc == RTKB_OK && fe != cudaSuccess)
     rc = cuda_fail(fe, "cudaFreeAsync");
   return rc;

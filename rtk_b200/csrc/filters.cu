@@ -569,7 +569,7 @@ run_filters(const rtkb_geometry * g, const rtkb_image_desc * in, const Options &
                o_tw = append(blob, tw), o_mw = append(blob, mw);
   void * scratch = nullptr;
   if (!blob.empty())
-    RTKB_CUDA_TRY(cudaMallocAsync(&scratch, blob.size(), st));
+    RTKB_CUDA_TRY(rtkb::scratch_malloc(&scratch, blob.size(), st));
   int rc = RTKB_OK;
   do
   {
@@ -627,7 +627,7 @@ run_filters(const rtkb_geometry * g, const rtkb_image_desc * in, const Options &
   } while (0);
   if (scratch)
   {
-    cudaError_t fe = cudaFreeAsync(scratch, st);
+    cudaError_t fe = rtkb::scratch_free(scratch, st);
     if (rc == RTKB_OK && fe != cudaSuccess)
       rc = cuda_fail(fe, "cudaFreeAsync");
   }

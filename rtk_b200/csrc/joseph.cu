@@ -792,7 +792,7 @@ rtkb_joseph_forward_project(const rtkb_geometry * g, const rtkb_image_desc * vol
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const size_t tbytes = (tab.size() * sizeof(RayProj) + 255) & ~size_t(255);
     void *       scratch = nullptr;
-    RTKB_CUDA_TRY(cudaMallocAsync(&scratch, tbytes + joseph_forward_scratch_bytes(num_pixels(*vol)), st));
+    RTKB_CUDA_TRY(rtkb::scratch_malloc(&scratch, tbytes + joseph_forward_scratch_bytes(num_pixels(*vol)), st));
     RayProj *   d_tab = static_cast<RayProj *>(scratch);
     void *      d_vt = static_cast<char *>(scratch) + tbytes;
     cudaError_t e = cudaMemcpyAsync(d_tab, tab.data(), tab.size() * sizeof(RayProj), cudaMemcpyHostToDevice, st);
@@ -803,7 +803,7 @@ rtkb_joseph_forward_project(const rtkb_geometry * g, const rtkb_image_desc * vol
       e = joseph_forward_launch(a, d_vol, d_vt, d_proj_in, d_proj_out, nullptr, st);
     }
     rc = (e == cudaSuccess) ? RTKB_OK : cuda_fail(e, "joseph forward");
-    cudaError_t fe = cudaFreeAsync(scratch, st);
+    cudaError_t fe = rtkb::scratch_free(scratch, st);
     if (rc == RTKB_OK && fe != cudaSuccess)
       rc = cuda_fail(fe, "cudaFreeAsync");
     return rc;
@@ -834,7 +834,7 @@ rtkb_joseph_back_project(const rtkb_geometry * g, const rtkb_image_desc * vol, c
     const long long nvox = num_pixels(*vol);
     const size_t    tbytes = (tab.size() * sizeof(RayProj) + 255) & ~size_t(255);
     void *          scratch = nullptr;
-    RTKB_CUDA_TRY(cudaMallocAsync(&scratch, tbytes + joseph_back_scratch_bytes(nvox), st));
+    RTKB_CUDA_TRY(rtkb::scratch_malloc(&scratch, tbytes + joseph_back_scratch_bytes(nvox), st));
     RayProj *   d_tab = static_cast<RayProj *>(scratch);
     void *      d_a = static_cast<char *>(scratch) + tbytes;
     cudaError_t e = cudaMemcpyAsync(d_tab, tab.data(), tab.size() * sizeof(RayProj), cudaMemcpyHostToDevice, st);
@@ -845,7 +845,7 @@ rtkb_joseph_back_project(const rtkb_geometry * g, const rtkb_image_desc * vol, c
       e = joseph_back_launch(a, d_proj, d_a, d_vol_in, d_vol_out, nullptr, 0.f, st);
     }
     rc = (e == cudaSuccess) ? RTKB_OK : cuda_fail(e, "joseph back projection");
-    cudaError_t fe = cudaFreeAsync(scratch, st);
+    cudaError_t fe = rtkb::scratch_free(scratch, st);
     if (rc == RTKB_OK && fe != cudaSuccess)
       rc = cuda_fail(fe, "cudaFreeAsync");
     return rc;
@@ -875,7 +875,7 @@ rtkb_joseph_sample_count(const rtkb_geometry * g, const rtkb_image_desc * vol, c
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const size_t tbytes = (tab.size() * sizeof(RayProj) + 255) & ~size_t(255);
     void *       scratch = nullptr;
-    RTKB_CUDA_TRY(cudaMallocAsync(&scratch, tbytes + sizeof(unsigned long long), st));
+    RTKB_CUDA_TRY(rtkb::scratch_malloc(&scratch, tbytes + sizeof(unsigned long long), st));
     RayProj *            d_tab = static_cast<RayProj *>(scratch);
     unsigned long long * d_n = reinterpret_cast<unsigned long long *>(static_cast<char *>(scratch) + tbytes);
     unsigned long long   h = 0;
@@ -893,7 +893,7 @@ rtkb_joseph_sample_count(const rtkb_geometry * g, const rtkb_image_desc * vol, c
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(&h, d_n, sizeof(h), cudaMemcpyDeviceToHost, st);
     rc = (e == cudaSuccess) ? RTKB_OK : cuda_fail(e, "joseph sample count");
-    cudaError_t fe = cudaFreeAsync(scratch, st);
+    cudaError_t fe = rtkb::scratch_free(scratch, st);
     if (fe == cudaSuccess)
       fe = cudaStreamSynchronize(st);
     if (rc == RTKB_OK && fe != cudaSuccess)

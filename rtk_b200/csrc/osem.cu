@@ -68,33 +68,35 @@ osem_ratio_kernel(const float * __restrict__ p, float * __restrict__ fp, long lo
   }
 }
 
-// De Pierro's regularisation factor R at voxel i, in the operation order of
-// rtk::DePierroRegularizationImageFilter: the 27-tap neighbourhood inner
-// product in double (itk::NeighborhoodOperatorImageFilter's real type for a
-// float image), rounded to float, times beta; A = N - that; B = M times
+// De Pierro's regularisation factor R at voxel (ix, iy, iz), in the operation
+// order of rtk::DePierroRegularizationImageFilter: the 27-tap neighbourhood
+// inner product in double (itk::NeighborhoodOperatorImageFilter's real type
+// for a float image), rounded to float, times beta; A = N - that; B = M times
 // float(8 beta 26); R = (A + sqrt(A A + B)) / 2 in float.
 template <bool kStencil>
 __device__ __forceinline__ float
-de_pierro_factor(const float * __restrict__ x, long long i, int nx, int ny, int nz, float n, float m, float beta,
-                 float c2)
+de_pierro_factor(const float * __restrict__ x, int ix, int iy, int iz, int nx, int ny, int nz, float n, float m,
+                 float beta, float c2)
 {
   float a = n;
   if (kStencil)
   {
     const long long sxy = (long long)nx * ny;
-    const int       ix = (int)(i % nx), iy = (int)((i / nx) % ny), iz = (int)(i / sxy);
     double          s = 0.;
+#pragma unroll
     for (int dz = -1; dz <= 1; dz++)
     {
       const int z = iz + dz;
       if (z < 0 || z >= nz)
         continue;
+#pragma unroll
       for (int dy = -1; dy <= 1; dy++)
       {
         const int y = iy + dy;
         if (y < 0 || y >= ny)
           continue;
         const float * row = x + (long long)z * sxy + (long long)y * nx;
+#pragma unroll
         for (int dx = -1; dx <= 1; dx++)
         {
           const int xx = ix + dx;
@@ -111,18 +113,33 @@ de_pierro_factor(const float * __restrict__ x, long long i, int nx, int ny, int 
   return (a + sqrtf(a * a + b)) / 2.f;
 }
 
+// Voxel rows: threads along x, blocks over (x tiles, y, z), striding over y and
+// z beyond the grid's limits.
+#define FOR_EACH_VOXEL(nx, ny, nz)                                                                                    \
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x;                                                               \
+  if (ix < nx)                                                                                                        \
+    for (int iz = blockIdx.z; iz < nz; iz += gridDim.z)                                                               \
+      for (int iy = blockIdx.y; iy < ny; iy += gridDim.y)
+
+dim3
+voxel_grid(const rtkb_image_desc & v)
+{
+  return dim3((unsigned)((v.size[0] + 127) / 128), (unsigned)std::min(v.size[1], 65535),
+              (unsigned)std::min(v.size[2], 65535));
+}
+
 // OSEM update: x_out = DivideOrZeroOut(B x, R).  x_out may equal x when the
 // neighbourhood term is off (beta = 0).
 template <bool kStencil>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(128)
 osem_update_kernel(const float * x, const float * __restrict__ B, const float * __restrict__ N, float * x_out,
                    int nx, int ny, int nz, float beta, float c2)
 {
-  const long long n = (long long)nx * ny * nz;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+  FOR_EACH_VOXEL(nx, ny, nz)
   {
-    const float m = B[i] * x[i];
-    const float r = de_pierro_factor<kStencil>(x, i, nx, ny, nz, N[i], m, beta, c2);
+    const long long i = ((long long)iz * ny + iy) * nx + ix;
+    const float     m = B[i] * x[i];
+    const float     r = de_pierro_factor<kStencil>(x, ix, iy, iz, nx, ny, nz, N[i], m, beta, c2);
     x_out[i] = fabsf(r) < kDivideThreshold ? 0.f : m / r;
   }
 }
@@ -130,13 +147,15 @@ osem_update_kernel(const float * x, const float * __restrict__ B, const float * 
 // rtk::DePierroRegularizationImageFilter alone: out = R(x_k, update, norm);
 // norm == nullptr stands for the default normalisation volume of ones.
 template <bool kStencil>
-__global__ void __launch_bounds__(256)
-de_pierro_kernel(const float * __restrict__ xk, const float * __restrict__ upd, const float * __restrict__ norm,
-                 float * __restrict__ out, int nx, int ny, int nz, float beta, float c2)
+__global__ void __launch_bounds__(128)
+de_pierro_kernel(const float * __restrict__ xk, const float * upd, const float * norm, float * out, int nx, int ny,
+                 int nz, float beta, float c2)
 {
-  const long long n = (long long)nx * ny * nz;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    out[i] = de_pierro_factor<kStencil>(xk, i, nx, ny, nz, norm ? norm[i] : 1.f, upd[i], beta, c2);
+  FOR_EACH_VOXEL(nx, ny, nz)
+  {
+    const long long i = ((long long)iz * ny + iy) * nx + ix;
+    out[i] = de_pierro_factor<kStencil>(xk, ix, iy, iz, nx, ny, nz, norm ? norm[i] : 1.f, upd[i], beta, c2);
+  }
 }
 
 bool
@@ -182,11 +201,11 @@ rtkb_de_pierro_regularization(const rtkb_image_desc * vol, const float * d_xk, c
     return RTKB_OK;
   const float fb = (float)beta, c2 = (float)(4. * 2. * beta * 26.);
   if (beta != 0.)
-    de_pierro_kernel<true><<<grid_for(n), 256, 0, st>>>(d_xk, d_update, d_norm, d_out, vol->size[0], vol->size[1],
-                                                         vol->size[2], fb, c2);
+    de_pierro_kernel<true><<<voxel_grid(*vol), 128, 0, st>>>(d_xk, d_update, d_norm, d_out, vol->size[0],
+                                                              vol->size[1], vol->size[2], fb, c2);
   else
-    de_pierro_kernel<false><<<grid_for(n), 256, 0, st>>>(d_xk, d_update, d_norm, d_out, vol->size[0], vol->size[1],
-                                                          vol->size[2], fb, c2);
+    de_pierro_kernel<false><<<voxel_grid(*vol), 128, 0, st>>>(d_xk, d_update, d_norm, d_out, vol->size[0],
+                                                               vol->size[1], vol->size[2], fb, c2);
   cudaError_t ce = cudaGetLastError();
   return ce == cudaSuccess ? RTKB_OK : cuda_fail(ce, "De Pierro regularisation");
 }
@@ -237,15 +256,15 @@ rtkb_osem(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image
     const size_t stack_b = gathered ? up256((size_t)per * np * 4) : 0;
     const size_t total = stack_b + 2 * gb + vb /*B*/ + (store ? 0 : vb) /*N*/ + (stencil ? vb : 0) /*x ping-pong*/;
     void *       mem = nullptr;
-    RTKB_CUDA_TRY(cudaMallocAsync(&mem, total, st));
+    RTKB_CUDA_TRY(rtkb::scratch_malloc(&mem, total, st));
     void * norms = nullptr;
     if (store)
     {
-      cudaError_t ce = cudaMallocAsync(&norms, vb * (size_t)nsub, st);
+      cudaError_t ce = rtkb::scratch_malloc(&norms, vb * (size_t)nsub, st);
       if (ce != cudaSuccess)
       {
         cudaGetLastError();
-        cudaFreeAsync(mem, st);
+        rtkb::scratch_free(mem, st);
         return fail(RTKB_ERR_OUT_OF_MEMORY, "no room for " + std::to_string(nsub) +
                                                 " stored normalisation volumes; set store_normalization to 0");
       }
@@ -345,19 +364,19 @@ rtkb_osem(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image
         if (stencil)
         {
           float * xo = (x == d_x) ? xalt : d_x;
-          osem_update_kernel<true><<<grid_for(nvox), 256, 0, st>>>(x, B, N, xo, nx, ny, nz, fb, c2);
+          osem_update_kernel<true><<<voxel_grid(*vol), 128, 0, st>>>(x, B, N, xo, nx, ny, nz, fb, c2);
           x = xo;
         }
         else
-          osem_update_kernel<false><<<grid_for(nvox), 256, 0, st>>>(x, B, N, x, nx, ny, nz, fb, c2);
+          osem_update_kernel<false><<<voxel_grid(*vol), 128, 0, st>>>(x, B, N, x, nx, ny, nz, fb, c2);
         cuda_step(cudaGetLastError(), "OSEM update");
       }
     if (rc == RTKB_OK && x != d_x)
       cuda_step(cudaMemcpyAsync(d_x, x, (size_t)nvox * 4, cudaMemcpyDeviceToDevice, st), "cudaMemcpyAsync");
-    cudaError_t fe = cudaFreeAsync(mem, st);
+    cudaError_t fe = rtkb::scratch_free(mem, st);
     if (norms)
     {
-      cudaError_t fe2 = cudaFreeAsync(norms, st);
+      cudaError_t fe2 = rtkb::scratch_free(norms, st);
       if (fe == cudaSuccess)
         fe = fe2;
     }

@@ -116,7 +116,7 @@ rtkb_project_ellipsoids(const rtkb_geometry * g, const rtkb_image_desc * proj, i
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const size_t tb = (tab.size() * sizeof(PixProj) + 255) & ~size_t(255), eb = ell.size() * sizeof(Ell);
     void *       scratch = nullptr;
-    RTKB_CUDA_TRY(cudaMallocAsync(&scratch, tb + eb, st));
+    RTKB_CUDA_TRY(rtkb::scratch_malloc(&scratch, tb + eb, st));
     PixProj *   d_tab = static_cast<PixProj *>(scratch);
     Ell *       d_ell = reinterpret_cast<Ell *>(static_cast<char *>(scratch) + tb);
     cudaError_t e = cudaMemcpyAsync(d_tab, tab.data(), tab.size() * sizeof(PixProj), cudaMemcpyHostToDevice, st);
@@ -131,7 +131,7 @@ rtkb_project_ellipsoids(const rtkb_geometry * g, const rtkb_image_desc * proj, i
       e = cudaGetLastError();
     }
     int         rc = (e == cudaSuccess) ? RTKB_OK : cuda_fail(e, "project ellipsoids");
-    cudaError_t fe = cudaFreeAsync(scratch, st);
+    cudaError_t fe = rtkb::scratch_free(scratch, st);
     if (rc == RTKB_OK && fe != cudaSuccess)
       rc = cuda_fail(fe, "cudaFreeAsync");
     return rc;

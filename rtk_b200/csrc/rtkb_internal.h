@@ -84,6 +84,17 @@ typedef int (*EncodeTiledFn)(void *, int, unsigned, void *, const unsigned long 
                              const unsigned *, const unsigned *, int, int, int, int);
 EncodeTiledFn tensor_map_encoder();
 
+// Stream-ordered scratch from the library's own per-device memory pool (kept
+// reserved between calls; rtkb_trim_memory_pool returns it).
+cudaError_t scratch_malloc(void ** p, size_t bytes, cudaStream_t st);
+template <class T>
+cudaError_t
+scratch_malloc(T ** p, size_t bytes, cudaStream_t st)
+{
+  return scratch_malloc(reinterpret_cast<void **>(p), bytes, st);
+}
+cudaError_t scratch_free(void * p, cudaStream_t st);
+
 // Projection processing order of the iterative solvers when the caller gives
 // none: 0..n-1 shuffled by Fisher-Yates driven by SplitMix64(seed).
 void seeded_order(int n, unsigned long long seed, std::vector<int> & order);

@@ -167,7 +167,7 @@ ray_box_lengths(const rtkb_geometry * g, const rtkb_image_desc & vol, const rtkb
       std::swap(b.mn[a], b.mx[a]);
   }
   void * d_tab = nullptr;
-  RTKB_CUDA_TRY(cudaMallocAsync(&d_tab, tab.size() * sizeof(RayTab), st));
+  RTKB_CUDA_TRY(rtkb::scratch_malloc(&d_tab, tab.size() * sizeof(RayTab), st));
   cudaError_t e = cudaMemcpyAsync(d_tab, tab.data(), tab.size() * sizeof(RayTab), cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess)
   {
@@ -177,7 +177,7 @@ ray_box_lengths(const rtkb_geometry * g, const rtkb_image_desc & vol, const rtkb
     e = cudaGetLastError();
   }
   int         rc = (e == cudaSuccess) ? RTKB_OK : cuda_fail(e, "ray-box lengths");
-  cudaError_t fe = cudaFreeAsync(d_tab, st);
+  cudaError_t fe = rtkb::scratch_free(d_tab, st);
   if (rc == RTKB_OK && fe != cudaSuccess)
     rc = cuda_fail(fe, "cudaFreeAsync");
   return rc;
@@ -267,7 +267,7 @@ rtkb_sart(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image
     const size_t    vb = ((size_t)nvox * 4 + 255) & ~size_t(255), pb = ((size_t)per * 4 + 255) & ~size_t(255);
     const size_t    rbb = ((size_t)per * np * 4 + 255) & ~size_t(255);
     void *          mem = nullptr;
-    RTKB_CUDA_TRY(cudaMallocAsync(&mem, 2 * vb + rbb + 4 * pb, st));
+    RTKB_CUDA_TRY(rtkb::scratch_malloc(&mem, 2 * vb + rbb + 4 * pb, st));
     char *  m = static_cast<char *>(mem);
     float * B = reinterpret_cast<float *>(m);
     float * N = reinterpret_cast<float *>(m + vb);
@@ -341,7 +341,7 @@ rtkb_sart(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image
         }
       }
     }
-    cudaError_t fe = cudaFreeAsync(mem, st);
+    cudaError_t fe = rtkb::scratch_free(mem, st);
     if (rc == RTKB_OK && fe != cudaSuccess)
       rc = cuda_fail(fe, "cudaFreeAsync");
     return rc;

@@ -214,6 +214,21 @@ def fdk_preprocess(geometry, proj_desc, proj, ramp=None, displaced=False, pad=Tr
     return out, got
 
 
+def trim_memory_pool() -> int:
+    """Return the library's unused reserved scratch memory (current device) to
+    the driver; returns the bytes still reserved."""
+    n = C.c_longlong()
+    check(load().rtkb_trim_memory_pool(C.byref(n)))
+    return n.value
+
+
+def memory_pool_reserved() -> int:
+    """Bytes the library's scratch pool holds on the current device."""
+    n = C.c_longlong()
+    check(load().rtkb_memory_pool_reserved(C.byref(n)))
+    return n.value
+
+
 def device_status(stream=None) -> int:
     """Synchronises the stream and returns (and clears) the kernels' status word."""
     st = C.c_int(0)

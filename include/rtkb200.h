@@ -384,6 +384,48 @@ typedef struct rtkb_osem_params
 } rtkb_osem_params;
 int rtkb_osem(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj, const float * d_proj,
               float * d_x, const rtkb_osem_params * params, void * stream);
+/* rtk::RegularizedConjugateGradientConeBeamReconstructionFilter
+ * (include/rtkRegularizedConjugateGradientConeBeamReconstructionFilter.hxx:171-296)
+ * with the Joseph pair: main_loop_iterations times, CG restarted from the
+ * current volume for cg_iterations iterations (the plan of rtkb_cg_create with
+ * tikhonov and gamma; weights W = displaced-detector weighting of d_weights,
+ * NULL = ones, unless disable_displaced_detector), then positivity
+ * (ThresholdBelow(0) -> 0), TV denoising (rtkb_tv_denoising_bpdq with gamma_tv,
+ * tv_iterations, tv_dimensions) and soft thresholding of the image
+ * (sgn(x) max(|x| - soft_threshold, 0)), each when enabled.  In place on d_x;
+ * waits for `stream` before returning.  Defaults in RTK: 10 main iterations,
+ * 4 CG iterations, positivity and TV on (gamma_tv 5e-5, 10 iterations, all
+ * dimensions), soft threshold off (0.001).  RTK's wavelets denoising step
+ * (Daubechies) and support mask are not provided. */
+typedef struct rtkb_regularized_cg_params
+{
+  int         main_loop_iterations;
+  int         cg_iterations;
+  double      tikhonov;
+  double      gamma;
+  int         positivity;
+  int         tv;
+  double      gamma_tv;
+  int         tv_iterations;
+  const int * tv_dimensions; /* 3 flags (x, y, z); NULL: all */
+  int         soft_threshold_on_image;
+  double      soft_threshold;
+  int         disable_displaced_detector;
+} rtkb_regularized_cg_params;
+int rtkb_regularized_cg(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
+                        const float * d_proj, const float * d_weights, float * d_x,
+                        const rtkb_regularized_cg_params * params, void * stream);
+/* rtk::TotalVariationDenoisingBPDQImageFilter
+ * (include/rtkTotalVariationDenoisingBPDQImageFilter.hxx,
+ * include/rtkDenoisingBPDQImageFilter.hxx:60-148): niter >= 1 iterations of
+ * basis pursuit dequantisation with threshold gamma over the dimensions whose
+ * flag is set (NULL: all).  d_out may equal d_in. */
+int rtkb_tv_denoising_bpdq(const rtkb_image_desc * vol, const float * d_in, float * d_out, double gamma, int niter,
+                           const int dims_processed[3], void * stream);
+/* rtk::TotalVariationImageFilter (include/rtkTotalVariationImageFilter.hxx):
+ * *tv = sum over voxels of the forward-difference gradient norm (zero-flux
+ * Neumann, spacing-scaled); waits for `stream`. */
+int rtkb_total_variation(const rtkb_image_desc * vol, const float * d_in, double * tv, void * stream);
 /* rtk::DePierroRegularizationImageFilter
  * (include/rtkDePierroRegularizationImageFilter.hxx:26-131): d_out =
  * (A + sqrt(A^2 + 8 beta 26 d_update)) / 2, A = d_norm - beta K(d_xk), K the

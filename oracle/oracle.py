@@ -98,6 +98,10 @@ def lib():
             "orc_sart": (None, [G, IM, IM, D, D, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_double,
                                 C.POINTER(C.c_int), C.c_int]),
             "orc_de_pierro": (None, [IM, D, D, D, C.c_double, D]),
+            "orc_tv_denoising_bpdq": (None, [IM, D, D, C.c_double, C.c_int, C.POINTER(C.c_int)]),
+            "orc_total_variation": (C.c_double, [IM, D]),
+            "orc_regularized_cg": (None, [G, IM, IM, D, D, D, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int,
+                                          C.c_int, C.c_double, C.c_int, C.POINTER(C.c_int), C.c_int, C.c_double, C.c_int]),
             "orc_osem": (None, [G, IM, IM, D, D, C.c_int, C.c_int, C.c_double, C.c_int, C.POINTER(C.c_int), C.c_int]),
             "orc_project_ellipsoids": (None, [G, IM, C.c_int, D, D, C.c_int]),
             "orc_draw_ellipsoids": (None, [IM, C.c_int, D, D, C.c_int]),
@@ -340,6 +344,37 @@ def osem(g, vol, proj, proj_data, niter, order, x0, subset=1, beta=0.0, joseph_b
     o = np.ascontiguousarray(order, dtype=np.int32)
     lib().orc_osem(g._g, C.byref(vol), C.byref(proj), _d(p), _d(x), int(niter), int(subset), float(beta),
                    int(joseph_bp), o.ctypes.data_as(C.POINTER(C.c_int)), threads or nthreads())
+    return x
+
+
+def _dims(dims):
+    return (C.c_int * 3)(*[int(bool(d)) for d in dims])
+
+
+def tv_denoising_bpdq(vol, f, gamma, niter, dims=(True, True, True)):
+    """TotalVariationDenoisingBPDQImageFilter."""
+    a = np.ascontiguousarray(f, dtype=np.float64)
+    out = np.empty(shape_of(vol))
+    lib().orc_tv_denoising_bpdq(C.byref(vol), _d(a), _d(out), float(gamma), int(niter), _dims(dims))
+    return out
+
+
+def total_variation(vol, x):
+    """TotalVariationImageFilter."""
+    return lib().orc_total_variation(C.byref(vol), _d(np.ascontiguousarray(x, dtype=np.float64)))
+
+
+def regularized_cg(g, vol, proj, proj_data, x0, main_iterations=10, cg_iterations=4, weights=None, tikhonov=0.0,
+                   gamma=0.0, positivity=True, tv=True, gamma_tv=5e-5, tv_iterations=10, tv_dims=(True, True, True),
+                   soft_threshold=False, soft_threshold_value=1e-3, threads=None):
+    """RegularizedConjugateGradientConeBeamReconstructionFilter (Joseph pair)."""
+    p = np.ascontiguousarray(proj_data, dtype=np.float64)
+    w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+    x = np.array(x0, dtype=np.float64, copy=True, order="C")
+    lib().orc_regularized_cg(g._g, C.byref(vol), C.byref(proj), _d(p), _d(w), _d(x), int(main_iterations),
+                             int(cg_iterations), float(tikhonov), float(gamma), int(positivity), int(tv),
+                             float(gamma_tv), int(tv_iterations), _dims(tv_dims), int(soft_threshold),
+                             float(soft_threshold_value), threads or nthreads())
     return x
 
 

@@ -1968,3 +1968,180 @@ orc_osem(const orc_geometry * g, const orc_image * vol, const orc_image * proj, 
   free(M);
   free(R);
 }
+
+/* ------------------------------------------------------------------------ */
+/* total variation and the regularised conjugate gradient                   */
+/* ------------------------------------------------------------------------ */
+static double
+tv_div(const orc_image * vol, const double * z, const int * dk, int nd, long x, long y, long zz)
+{
+  /* BackwardDifferenceDivergenceImageFilter::DynamicThreadedGenerateData
+   * (include/rtkBackwardDifferenceDivergenceImageFilter.hxx): per processed
+   * dimension (packed component j, dimension dk[j]), (z_j(i) - z_j(i - e))/s
+   * with zero outside (ConstantBoundaryCondition); AfterThreadedGenerateData
+   * then subtracts z_j(i)/s on the last slice along dk[j] -- for the single
+   * voxel at which its iterators start (all other coordinates 0), as coded. */
+  const long n[3] = { vol->size[0], vol->size[1], vol->size[2] }, c[3] = { x, y, zz };
+  const long nvx = n[0] * n[1] * n[2], i = (zz * n[1] + y) * n[0] + x;
+  const long stride[3] = { 1, n[0], n[0] * n[1] };
+  double     div = 0.;
+  for (int j = 0; j < nd; j++)
+  {
+    const int    k = dk[j];
+    const double inv = 1. / vol->spacing[k];
+    const double here = z[(long)j * nvx + i];
+    const double prev = c[k] > 0 ? z[(long)j * nvx + i - stride[k]] : 0.;
+    div += (here - prev) * inv;
+  }
+  for (int j = 0; j < nd; j++)
+  {
+    const int k = dk[j];
+    int       first = 1;
+    for (int d = 0; d < 3; d++)
+      if (d != k && c[d] != 0)
+        first = 0;
+    if (first && c[k] == n[k] - 1)
+      div -= z[(long)j * nvx + i] / vol->spacing[k];
+  }
+  return div;
+}
+
+static void
+tv_grad_threshold(const orc_image * vol, const double * w, double * z, const int * dk, int nd, double gamma,
+                  int subtract)
+{
+  /* z_j = P_gamma(z_j - grad_j w) (subtract) or P_gamma(grad_j w): the
+   * forward-difference gradient with a zero-flux Neumann boundary
+   * (ForwardDifferenceGradientImageFilter, spacing-scaled) and
+   * MagnitudeThresholdImageFilter (vectors longer than gamma scaled back to
+   * gamma, others unchanged) */
+  const long n[3] = { vol->size[0], vol->size[1], vol->size[2] };
+  const long nvx = n[0] * n[1] * n[2], stride[3] = { 1, n[0], n[0] * n[1] };
+  for (long zz = 0; zz < n[2]; zz++)
+    for (long y = 0; y < n[1]; y++)
+      for (long x = 0; x < n[0]; x++)
+      {
+        const long c[3] = { x, y, zz }, i = (zz * n[1] + y) * n[0] + x;
+        double     v[3] = { 0., 0., 0. }, nn = 0.;
+        for (int j = 0; j < nd; j++)
+        {
+          const int    k = dk[j];
+          const double g = c[k] < n[k] - 1 ? (w[i + stride[k]] - w[i]) / vol->spacing[k] : 0.;
+          v[j] = subtract ? z[(long)j * nvx + i] - g : g;
+          nn += v[j] * v[j];
+        }
+        nn = sqrt(nn);
+        for (int j = 0; j < nd; j++)
+          z[(long)j * nvx + i] = nn > gamma ? gamma * v[j] / nn : v[j];
+      }
+}
+
+void
+orc_tv_denoising_bpdq(const orc_image * vol, const double * f, double * out, double gamma, int niter,
+                      const int dims[3])
+{
+  /* TotalVariationDenoisingBPDQImageFilter / DenoisingBPDQImageFilter
+   * (include/rtkDenoisingBPDQImageFilter.hxx:60-148): beta = 0.9 minSpacing
+   * / 2^d (d processed dimensions; minSpacing starts from spacing[0], then the
+   * minimum over the processed ones); iteration 0: z = P(grad(beta f));
+   * iterations 1..niter-1: z = P(z - grad(beta minSpacing (f - div z)));
+   * out = f - div z. */
+  const long nvx = npix(vol);
+  int        dk[3], nd = 0;
+  double     minsp = vol->spacing[0];
+  for (int d = 0; d < 3; d++)
+    if (dims[d])
+    {
+      dk[nd++] = d;
+      if (vol->spacing[d] < minsp)
+        minsp = vol->spacing[d];
+    }
+  const double beta = 1. / pow(2., nd) * 0.9 * minsp;
+  double *     z = (double *)calloc((size_t)(nd > 0 ? nd : 1) * nvx, sizeof(double));
+  double *     w = (double *)malloc(sizeof(double) * nvx);
+  for (long i = 0; i < nvx; i++)
+    w[i] = beta * f[i];
+  tv_grad_threshold(vol, w, z, dk, nd, gamma, 0);
+  const long n0 = vol->size[0], n1 = vol->size[1], n2 = vol->size[2];
+  for (int it = 1; it < niter; it++)
+  {
+    for (long zz = 0; zz < n2; zz++)
+      for (long y = 0; y < n1; y++)
+        for (long x = 0; x < n0; x++)
+        {
+          const long i = (zz * n1 + y) * n0 + x;
+          w[i] = beta * minsp * (f[i] - tv_div(vol, z, dk, nd, x, y, zz));
+        }
+    tv_grad_threshold(vol, w, z, dk, nd, gamma, 1);
+  }
+  for (long zz = 0; zz < n2; zz++)
+    for (long y = 0; y < n1; y++)
+      for (long x = 0; x < n0; x++)
+      {
+        const long i = (zz * n1 + y) * n0 + x;
+        w[i] = f[i] - tv_div(vol, z, dk, nd, x, y, zz);
+      }
+  memcpy(out, w, sizeof(double) * nvx);
+  free(z);
+  free(w);
+}
+
+double
+orc_total_variation(const orc_image * vol, const double * x)
+{
+  /* TotalVariationImageFilter::ThreadedGenerateData
+   * (include/rtkTotalVariationImageFilter.hxx): sum over voxels of the norm of
+   * the forward-difference gradient (zero-flux Neumann, spacing-scaled) */
+  const long n[3] = { vol->size[0], vol->size[1], vol->size[2] }, stride[3] = { 1, n[0], n[0] * n[1] };
+  double     tv = 0.;
+  for (long zz = 0; zz < n[2]; zz++)
+    for (long y = 0; y < n[1]; y++)
+      for (long xx = 0; xx < n[0]; xx++)
+      {
+        const long c[3] = { xx, y, zz }, i = (zz * n[1] + y) * n[0] + xx;
+        double     s = 0.;
+        for (int d = 0; d < 3; d++)
+        {
+          const double g = c[d] < n[d] - 1 ? (x[i + stride[d]] - x[i]) / vol->spacing[d] : 0.;
+          s += g * g;
+        }
+        tv += sqrt(s);
+      }
+  return tv;
+}
+
+void
+orc_regularized_cg(const orc_geometry * g, const orc_image * vol, const orc_image * proj, const double * proj_data,
+                   const double * weights, double * x, int main_iterations, int cg_iterations, double tikhonov,
+                   double gamma, int positivity, int tv, double gamma_tv, int tv_iterations, const int tv_dims[3],
+                   int soft_threshold, double soft_threshold_value, int nthreads)
+{
+  /* RegularizedConjugateGradientConeBeamReconstructionFilter::GenerateData
+   * (include/rtkRegularizedConjugateGradientConeBeamReconstructionFilter.hxx:
+   * 250-296): main_iterations x (CG restarted from the current volume for
+   * cg_iterations iterations, then ThresholdBelow(0) -> 0, TV denoising (BPDQ),
+   * soft thresholding sgn(x) max(|x| - t, 0)).  weights: the CG's W (the
+   * displaced-detector weighting already applied), NULL for ones. */
+  const long nvx = npix(vol);
+  double *   t = (double *)malloc(sizeof(double) * nvx);
+  for (int m = 0; m < main_iterations; m++)
+  {
+    orc_cg_joseph(g, vol, proj, proj_data, weights, tikhonov, gamma, cg_iterations, x, NULL, nthreads);
+    if (positivity)
+      for (long i = 0; i < nvx; i++)
+        if (x[i] < 0.)
+          x[i] = 0.;
+    if (tv)
+    {
+      orc_tv_denoising_bpdq(vol, x, t, gamma_tv, tv_iterations, tv_dims);
+      memcpy(x, t, sizeof(double) * nvx);
+    }
+    if (soft_threshold)
+      for (long i = 0; i < nvx; i++)
+      {
+        const double a = fabs(x[i]) - soft_threshold_value;
+        x[i] = a > 0. ? (x[i] > 0. ? a : (x[i] < 0. ? -a : 0.)) : 0.;
+      }
+  }
+  free(t);
+}

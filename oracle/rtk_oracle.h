@@ -136,6 +136,17 @@ void orc_de_pierro(const orc_image * vol, const double * xk, const double * upda
  * back projector, in place on x */
 void orc_osem(const orc_geometry * g, const orc_image * vol, const orc_image * proj, const double * proj_data, double * x,
               int niter, int projections_per_subset, double beta, int joseph_bp, const int * order, int nthreads);
+/* TotalVariationDenoisingBPDQImageFilter: niter >= 1 iterations, dims: processed dimensions (0/1) */
+void orc_tv_denoising_bpdq(const orc_image * vol, const double * f, double * out, double gamma, int niter,
+                           const int dims[3]);
+/* TotalVariationImageFilter: sum of forward-difference gradient norms */
+double orc_total_variation(const orc_image * vol, const double * x);
+/* RegularizedConjugateGradientConeBeamReconstructionFilter with the Joseph pair (CG, positivity, TV, soft
+ * threshold on the image), in place on x; weights = the CG's W or NULL */
+void orc_regularized_cg(const orc_geometry * g, const orc_image * vol, const orc_image * proj, const double * proj_data,
+                        const double * weights, double * x, int main_iterations, int cg_iterations, double tikhonov,
+                        double gamma, int positivity, int tv, double gamma_tv, int tv_iterations, const int tv_dims[3],
+                        int soft_threshold, double soft_threshold_value, int nthreads);
 /* RTK's LaplacianImageFilter (Neumann boundary, spacing-scaled): out = Laplacian(x) */
 void orc_laplacian(const orc_image * vol, const double * x, double * out);
 

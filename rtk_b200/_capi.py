@@ -169,6 +169,9 @@ SIGNATURES.update({
     "rtkb_ray_box_lengths": (C.c_int, [_G, _IM, _IM, _V, _V]),
     "rtkb_sart": (C.c_int, [_G, _IM, _IM, _V, _V, C.c_void_p, _V]),
     "rtkb_osem": (C.c_int, [_G, _IM, _IM, _V, _V, C.c_void_p, _V]),
+    "rtkb_regularized_cg": (C.c_int, [_G, _IM, _IM, _V, _V, _V, C.c_void_p, _V]),
+    "rtkb_tv_denoising_bpdq": (C.c_int, [_IM, _V, _V, C.c_double, C.c_int, C.POINTER(C.c_int), _V]),
+    "rtkb_total_variation": (C.c_int, [_IM, _V, C.POINTER(C.c_double), _V]),
     "rtkb_trim_memory_pool": (C.c_int, [C.POINTER(C.c_longlong)]),
     "rtkb_memory_pool_reserved": (C.c_int, [C.POINTER(C.c_longlong)]),
     "rtkb_de_pierro_regularization": (C.c_int, [_IM, _V, _V, _V, C.c_double, _V, _V]),
@@ -249,3 +252,13 @@ class OsemParams(C.Structure):
     _fields_ = [("niter", C.c_int), ("projections_per_subset", C.c_int), ("beta", C.c_double),
                 ("store_normalization", C.c_int), ("backprojector", C.c_int), ("order", C.POINTER(C.c_int)),
                 ("seed", C.c_ulonglong)]
+
+
+class RegularizedCgParams(C.Structure):
+    """rtkb_regularized_cg_params."""
+
+    _fields_ = [("main_loop_iterations", C.c_int), ("cg_iterations", C.c_int), ("tikhonov", C.c_double),
+                ("gamma", C.c_double), ("positivity", C.c_int), ("tv", C.c_int), ("gamma_tv", C.c_double),
+                ("tv_iterations", C.c_int), ("tv_dimensions", C.POINTER(C.c_int)),
+                ("soft_threshold_on_image", C.c_int), ("soft_threshold", C.c_double),
+                ("disable_displaced_detector", C.c_int)]

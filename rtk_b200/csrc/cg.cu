@@ -692,6 +692,51 @@ reset_run(rtkb_cg * c, float * d_x)
 }
 } // namespace
 
+namespace
+{
+// W = displaced-detector weights (no padding) of the input weights (ones by
+// default), then out = BP(W .* p) in the storage type oe.
+int
+weights_and_rhs(rtkb_cg * c, const float * d_proj, const float * d_weights, int displaced_detector, void * out,
+                rtkb::Elem oe, cudaStream_t st)
+{
+  using namespace rtkb;
+  const bool have_w = d_weights != nullptr;
+  if (displaced_detector)
+  {
+    if (!have_w)
+      fill_kernel<<<grid_for(c->npix), 256, 0, st>>>(c->tmp, 1.f, c->npix);
+    const int rc = rtkb_displaced_detector(c->g, &c->proj, 0, have_w ? d_weights : c->tmp, c->W, st);
+    if (rc != RTKB_OK)
+      return rc;
+  }
+  else if (have_w)
+    RTKB_CUDA_TRY(cudaMemcpyAsync(c->W, d_weights, (size_t)c->npix * 4, cudaMemcpyDeviceToDevice, st));
+  else
+    fill_kernel<<<grid_for(c->npix), 256, 0, st>>>(c->W, 1.f, c->npix);
+  // tmp = W .* p in the plan's storage
+  if (c->bf16)
+    mul_kernel<__nv_bfloat16><<<grid_for(c->npix), 256, 0, st>>>(as<__nv_bfloat16>(c->tmp), d_proj, c->W, c->npix);
+  else
+    mul_kernel<float><<<grid_for(c->npix), 256, 0, st>>>(c->tmp, d_proj, c->W, c->npix);
+  const cudaError_t e =
+    joseph_back_launch(c->args, c->tmp, storage(c), c->scratch, nullptr, out, oe, nullptr, Elem::F32, 0.f, st);
+  return e == cudaSuccess ? RTKB_OK : cuda_fail(e, "CG right-hand side");
+}
+} // namespace
+
+namespace rtkb
+{
+int
+cg_rhs(rtkb_cg * c, const float * d_proj, const float * d_weights, int displaced_detector, float * d_b,
+       cudaStream_t st)
+{
+  if (!c || !d_proj || !d_b)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "null argument");
+  return weights_and_rhs(c, d_proj, d_weights, displaced_detector, d_b, Elem::F32, st);
+}
+} // namespace rtkb
+
 extern "C" int
 rtkb_cg_start(rtkb_cg * c, const float * d_proj, const float * d_weights, int displaced_detector, float * d_x,
               void * stream)
@@ -701,29 +746,10 @@ rtkb_cg_start(rtkb_cg * c, const float * d_proj, const float * d_weights, int di
     return fail(RTKB_ERR_INVALID_ARGUMENT, "null argument");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   reset_run(c, d_x);
-  // W = displaced-detector weights (no padding) of the input weights (ones by default)
-  const bool have_w = d_weights != nullptr;
-  if (displaced_detector)
-  {
-    if (!have_w)
-      fill_kernel<<<grid_for(c->npix), 256, 0, st>>>(c->tmp, 1.f, c->npix);
-    const int rc = rtkb_displaced_detector(c->g, &c->proj, 0, have_w ? d_weights : c->tmp, c->W, stream);
-    if (rc != RTKB_OK)
-      return rc;
-  }
-  else if (have_w)
-    RTKB_CUDA_TRY(cudaMemcpyAsync(c->W, d_weights, (size_t)c->npix * 4, cudaMemcpyDeviceToDevice, st));
-  else
-    fill_kernel<<<grid_for(c->npix), 256, 0, st>>>(c->W, 1.f, c->npix);
-  // R = B = BP(W .* p), tmp and R in the plan's storage
-  if (c->bf16)
-    mul_kernel<__nv_bfloat16><<<grid_for(c->npix), 256, 0, st>>>(as<__nv_bfloat16>(c->tmp), d_proj, c->W, c->npix);
-  else
-    mul_kernel<float><<<grid_for(c->npix), 256, 0, st>>>(c->tmp, d_proj, c->W, c->npix);
-  const cudaError_t e = joseph_back_launch(c->args, c->tmp, storage(c), c->scratch, nullptr, c->R, storage(c), nullptr,
-                                           Elem::F32, 0.f, st);
-  if (e != cudaSuccess)
-    return cuda_fail(e, "CG start");
+  // R = b = BP(W .* p)
+  const int rc = weights_and_rhs(c, d_proj, d_weights, displaced_detector, c->R, storage(c), st);
+  if (rc != RTKB_OK)
+    return rc;
   return start_from_rhs(c, st);
 }
 

@@ -95,6 +95,12 @@ scratch_malloc(T ** p, size_t bytes, cudaStream_t st)
 }
 cudaError_t scratch_free(void * p, cudaStream_t st);
 
+// The conjugate-gradient plan's weights W (displaced-detector weighting of
+// d_weights, ones when NULL) and right-hand side d_b = BP(W .* d_proj), FP32;
+// rtkb_cg_start_rhs(plan, d_b, ...) then restarts from any volume with them.
+int cg_rhs(rtkb_cg * c, const float * d_proj, const float * d_weights, int displaced_detector, float * d_b,
+           cudaStream_t st);
+
 // Projection processing order of the iterative solvers when the caller gives
 // none: 0..n-1 shuffled by Fisher-Yates driven by SplitMix64(seed).
 void seeded_order(int n, unsigned long long seed, std::vector<int> & order);

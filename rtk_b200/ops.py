@@ -329,6 +329,55 @@ def de_pierro_regularization(vol_desc, xk, update, norm=None, beta=0.01, out=Non
     return out
 
 
+def _dims3(dims):
+    return (C.c_int * 3)(*[int(bool(d)) for d in dims])
+
+
+def regularized_cg(geometry, vol_desc, proj_desc, proj, x, weights=None, main_loop_iterations=10, cg_iterations=4,
+                   tikhonov=0.0, gamma=0.0, positivity=True, tv=True, gamma_tv=5e-5, tv_iterations=10,
+                   tv_dimensions=(True, True, True), soft_threshold_on_image=False, soft_threshold=1e-3,
+                   displaced_detector=True, stream=None):
+    """rtk::RegularizedConjugateGradientConeBeamReconstructionFilter (Joseph
+    pair; CG, positivity, TV denoising, soft threshold), in place on x."""
+    from ._capi import RegularizedCgParams
+
+    _check_shape(proj, proj_desc, "projections")
+    _check_shape(x, vol_desc, "volume")
+    if weights is not None:
+        _check_shape(weights, proj_desc, "weights")
+    p = RegularizedCgParams()
+    p.main_loop_iterations, p.cg_iterations = int(main_loop_iterations), int(cg_iterations)
+    p.tikhonov, p.gamma, p.positivity, p.tv = float(tikhonov), float(gamma), int(positivity), int(tv)
+    p.gamma_tv, p.tv_iterations = float(gamma_tv), int(tv_iterations)
+    dims = _dims3(tv_dimensions)
+    p.tv_dimensions = C.cast(dims, C.POINTER(C.c_int))
+    p.soft_threshold_on_image, p.soft_threshold = int(soft_threshold_on_image), float(soft_threshold)
+    p.disable_displaced_detector = int(not displaced_detector)
+    check(load().rtkb_regularized_cg(geometry.handle, C.byref(vol_desc), C.byref(proj_desc), _ptr(proj),
+                                     None if weights is None else _ptr(weights), _ptr(x), C.byref(p),
+                                     _stream(stream)))
+    return x
+
+
+def tv_denoising_bpdq(vol_desc, x, gamma, niter, dimensions=(True, True, True), out=None, stream=None):
+    """rtk::TotalVariationDenoisingBPDQImageFilter (out may be x)."""
+    _check_shape(x, vol_desc, "volume")
+    if out is None:
+        out = _torch().empty_like(x)
+    _check_shape(out, vol_desc, "output")
+    check(load().rtkb_tv_denoising_bpdq(C.byref(vol_desc), _ptr(x), _ptr(out), float(gamma), int(niter),
+                                        _dims3(dimensions), _stream(stream)))
+    return out
+
+
+def total_variation(vol_desc, x, stream=None) -> float:
+    """rtk::TotalVariationImageFilter (waits for the stream)."""
+    _check_shape(x, vol_desc, "volume")
+    v = C.c_double()
+    check(load().rtkb_total_variation(C.byref(vol_desc), _ptr(x), C.byref(v), _stream(stream)))
+    return v.value
+
+
 def _storage_code(storage):
     codes = {"fp32": 0, "bf16": 1}
     if storage not in codes:

@@ -452,6 +452,57 @@ def osem_leg(torch, rtkb, stream, niter=3, subset=10):
     return out
 
 
+def regularized_cg_leg(torch, rtkb, stream, main_iterations=3):
+    """Regularised CG with RTK's defaults (4 CG iterations per main iteration,
+    positivity, TV denoising gamma 5e-5 x 10 BPDQ iterations) on the CG
+    configuration's problem (noise-free projections), 3 main iterations; and
+    the TV denoiser alone on the 256^3 volume against the HBM roofline: one
+    BPDQ run of n iterations must move (28 n + 8) bytes per voxel (first
+    iteration: f in, the three-component dual field z out; each later one:
+    f and z in, z out; final pass: f and z in, the volume out)."""
+    from tests import phantoms
+
+    n = 360
+    g = rtkb.geometry.circular(n, SID, SDD)
+    vd = rtkb.make_desc((256, 256, 256), (1.0, 1.0, 1.0))
+    pd = rtkb.make_desc((512, 384, n), (0.8, 0.8, 1.0))
+    ell = phantoms.random_ellipsoids(20, SEED + 2, centre_radius=60.0, axis_range=(5.0, 60.0))
+    ell[:, 15] *= 0.02
+    p = rtkb.ops.project_ellipsoids(g, pd, ell, stream=stream)
+    x = torch.zeros((256, 256, 256), device="cuda")
+    rtkb.ops.regularized_cg(g, vd, pd, p, x, main_loop_iterations=1, stream=stream)  # warm-up
+    x.zero_()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    rtkb.ops.regularized_cg(g, vd, pd, p, x, main_loop_iterations=main_iterations, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    total = e0.elapsed_time(e1) / 1e3
+    niter, reps = 10, 10
+    out = torch.empty_like(x)
+    rtkb.ops.tv_denoising_bpdq(vd, x, 5e-5, niter, out=out, stream=stream)
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(reps):
+        rtkb.ops.tv_denoising_bpdq(vd, x, 5e-5, niter, out=out, stream=stream)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    tv_s = t0.elapsed_time(t1) / 1e3 / reps
+    tv_bytes = (28 * niter + 8) * 256 ** 3
+    hbm = peaks().get("hbm_gbs")
+    return {"workload": "regularised CG, 256^3 @1mm <- 360 x 512x384 @0.8mm, 4 CG iterations + positivity + "
+                        "TV (gamma 5e-5, 10 BPDQ iterations) per main iteration",
+            "main_iterations": main_iterations, "seconds_device": total,
+            "seconds_per_main_iteration": total / main_iterations,
+            "tv_denoising": {"volume": [256, 256, 256], "iterations": niter, "ms": tv_s * 1e3,
+                             "roofline": {"bound": "hbm", "algorithmic_bytes": tv_bytes,
+                                          "achieved_gbs": tv_bytes / tv_s / 1e9, "peak_gbs": hbm,
+                                          "frac": (tv_bytes / tv_s / 1e9) / hbm if hbm else None,
+                                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"}}}
+
+
 def cg_seconds_to_residual(torch, rtkb, stream, tol=1e-3, max_iter=300, learned_pcg=True):
     """CG configuration: 256^3 at 1 mm, 360 projections of 512x384 at 0.8 mm
     (SID 1000, SDD 1536) of 20 seeded random ellipsoids with pre-log Poisson
@@ -872,6 +923,7 @@ def main():
         line["batched_cg"] = batch_cg_leg(torch, rtkb, stream)
         line["sart"] = sart_leg(torch, rtkb, stream)
         line["osem"] = osem_leg(torch, rtkb, stream)
+        line["regularized_cg"] = regularized_cg_leg(torch, rtkb, stream)
         line["cg"] = cg_seconds_to_residual(torch, rtkb, stream)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:

@@ -26,9 +26,14 @@
 // that slice, gives the same values.
 //
 // Layout: the dual field z is one float plane per processed dimension (SoA,
-// coalesced along x); each BPDQ iteration is two passes over the volume, the
-// divergence/subtract/scale pass and the gradient/subtract/threshold pass,
-// 48 bytes per voxel of HBM traffic.
+// coalesced along x), ping-ponged between two buffers.  Each BPDQ iteration
+// after the first is ONE pass: a thread recomputes w = beta' (f - div z) at
+// its voxel and at its forward neighbours from cached loads of f and z (the
+// same float operations in the same order as a separate pass would do), so an
+// iteration moves 28 bytes per voxel of HBM traffic (f and z in, z out).
+// RTK's default, all three dimensions processed, has kernels of its own with
+// the directions fixed at compile time and 32-bit offsets where the volume
+// allows (the generic kernels spend most of their time on index arithmetic).
 #include "rtkb200.h"
 #include "rtkb_internal.h"
 
@@ -67,66 +72,232 @@ stride_of(const TvDims & t, int k)
   return k == 0 ? 1LL : (k == 1 ? (long long)t.n[0] : (long long)t.n[0] * t.n[1]);
 }
 
-// z_j = P_gamma(z_j - grad_j w) (kSubtract) or P_gamma(grad_j w), with w read
-// as scale * src (scale = beta in iteration 0, where src is f; 1 afterwards).
-template <bool kSubtract>
+// coordinate and size along dimension k (selects: no local-memory arrays)
+__device__ __forceinline__ int
+coord_of(int x, int y, int z, int k)
+{
+  return k == 0 ? x : (k == 1 ? y : z);
+}
+
+__device__ __forceinline__ int
+size_of(const TvDims & t, int k)
+{
+  return k == 0 ? t.n[0] : (k == 1 ? t.n[1] : t.n[2]);
+}
+
+// div z at voxel i: backward differences, zero before the first voxel, z_k
+// dropped on the last slice along k.
+__device__ __forceinline__ float
+div_at(const float * __restrict__ Z, const TvDims & t, int x, int y, int z, long long i, long long nvox)
+{
+  float div = 0.f;
+#pragma unroll
+  for (int j = 0; j < 3; j++)
+  {
+    if (j >= t.nd)
+      break;
+    const int   k = t.dk[j], ck = coord_of(x, y, z, k);
+    const float here = ck < size_of(t, k) - 1 ? Z[j * nvox + i] : 0.f;
+    const float prev = ck > 0 ? Z[j * nvox + i - stride_of(t, k)] : 0.f;
+    div += (here - prev) * t.inv_s[j];
+  }
+  return div;
+}
+
+// P_gamma: vectors longer than gamma scaled back to gamma
+__device__ __forceinline__ void
+clip3(float & a, float & b, float & c, float gamma)
+{
+  const float norm = sqrtf(a * a + b * b + c * c);
+  if (norm > gamma)
+  {
+    a = gamma * a / norm;
+    b = gamma * b / norm;
+    c = gamma * c / norm;
+  }
+}
+
+// Iteration 0 (generic dimensions): z = P_gamma(grad(beta f)).
 __global__ void __launch_bounds__(128)
-tv_gradient_kernel(const float * __restrict__ src, float scale, float * __restrict__ Z, TvDims t, float gamma)
+tv_first_kernel(const float * __restrict__ f, float beta, float * __restrict__ Z, TvDims t, float gamma)
 {
   const long long nvox = (long long)t.n[0] * t.n[1] * t.n[2];
   FOR_EACH_ROW_VOXEL(t.n)
   {
     const long long i = ((long long)iz * t.n[1] + iy) * t.n[0] + ix;
-    const int       c[3] = { ix, iy, iz };
-    const float     w0 = src[i] * scale;
+    const float     w0 = f[i] * beta;
     float           v[3] = { 0.f, 0.f, 0.f };
-    double          nn = 0.;
 #pragma unroll
     for (int j = 0; j < 3; j++)
     {
       if (j >= t.nd)
         break;
       const int k = t.dk[j];
-      const float g = c[k] < t.n[k] - 1 ? (src[i + stride_of(t, k)] * scale - w0) * t.inv_s[j] : 0.f;
-      v[j] = kSubtract ? Z[j * nvox + i] - g : g;
-      nn += (double)v[j] * v[j];
+      v[j] = coord_of(ix, iy, iz, k) < size_of(t, k) - 1 ? (f[i + stride_of(t, k)] * beta - w0) * t.inv_s[j] : 0.f;
     }
-    const double norm = sqrt(nn);
-    const bool   clip = norm > (double)gamma;
+    clip3(v[0], v[1], v[2], gamma);
 #pragma unroll
     for (int j = 0; j < 3; j++)
-    {
-      if (j >= t.nd)
-        break;
-      Z[j * nvox + i] = clip ? gamma * v[j] / (float)norm : v[j];
-    }
+      if (j < t.nd)
+        Z[j * nvox + i] = v[j];
   }
 }
 
-// out = f - div z (kFinal) or scale (f - div z).  out may alias f.
-template <bool kFinal>
+// Iterations 1..n-1 (generic dimensions), fused: Zout = P_gamma(Zin - grad w),
+// w = beta1 (f - div Zin) evaluated at the voxel and at each forward neighbour.
 __global__ void __launch_bounds__(128)
-tv_divergence_kernel(const float * f, const float * __restrict__ Z, float * out, TvDims t, float scale)
+tv_iterate_kernel(const float * __restrict__ f, const float * __restrict__ Zin, float * __restrict__ Zout, TvDims t,
+                  float beta1, float gamma)
 {
   const long long nvox = (long long)t.n[0] * t.n[1] * t.n[2];
   FOR_EACH_ROW_VOXEL(t.n)
   {
     const long long i = ((long long)iz * t.n[1] + iy) * t.n[0] + ix;
-    const int       c[3] = { ix, iy, iz };
-    float           div = 0.f;
+    const float     w0 = (f[i] - div_at(Zin, t, ix, iy, iz, i, nvox)) * beta1;
+    float           v[3] = { 0.f, 0.f, 0.f };
 #pragma unroll
     for (int j = 0; j < 3; j++)
     {
       if (j >= t.nd)
         break;
-      const int   k = t.dk[j];
-      const float here = c[k] < t.n[k] - 1 ? Z[j * nvox + i] : 0.f;
-      const float prev = c[k] > 0 ? Z[j * nvox + i - stride_of(t, k)] : 0.f;
-      div += (here - prev) * t.inv_s[j];
+      const int k = t.dk[j];
+      float     g = 0.f;
+      if (coord_of(ix, iy, iz, k) < size_of(t, k) - 1)
+      {
+        const long long i1 = i + stride_of(t, k);
+        const float     w1 =
+          (f[i1] - div_at(Zin, t, ix + (k == 0), iy + (k == 1), iz + (k == 2), i1, nvox)) * beta1;
+        g = (w1 - w0) * t.inv_s[j];
+      }
+      v[j] = Zin[j * nvox + i] - g;
     }
-    const float u = f[i] - div;
-    out[i] = kFinal ? u : u * scale;
+    clip3(v[0], v[1], v[2], gamma);
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+      if (j < t.nd)
+        Zout[j * nvox + i] = v[j];
   }
+}
+
+// out = f - div z (generic dimensions).  out may alias f.
+__global__ void __launch_bounds__(128)
+tv_final_kernel(const float * f, const float * __restrict__ Z, float * out, TvDims t)
+{
+  const long long nvox = (long long)t.n[0] * t.n[1] * t.n[2];
+  FOR_EACH_ROW_VOXEL(t.n)
+  {
+    const long long i = ((long long)iz * t.n[1] + iy) * t.n[0] + ix;
+    out[i] = f[i] - div_at(Z, t, ix, iy, iz, i, nvox);
+  }
+}
+
+// ---- all three dimensions processed (RTK's default) ----
+template <typename Off>
+struct Vol3
+{
+  int   n[3];
+  Off   sy, sz; // strides of y and z
+  float isx, isy, isz;
+};
+
+template <typename Off>
+__device__ __forceinline__ float
+div3(const float * __restrict__ zx, const float * __restrict__ zy, const float * __restrict__ zz, const Vol3<Off> & v,
+     int x, int y, int z, Off p)
+{
+  float r = ((x < v.n[0] - 1 ? zx[p] : 0.f) - (x > 0 ? zx[p - 1] : 0.f)) * v.isx;
+  r += ((y < v.n[1] - 1 ? zy[p] : 0.f) - (y > 0 ? zy[p - v.sy] : 0.f)) * v.isy;
+  r += ((z < v.n[2] - 1 ? zz[p] : 0.f) - (z > 0 ? zz[p - v.sz] : 0.f)) * v.isz;
+  return r;
+}
+
+template <typename Off>
+__global__ void __launch_bounds__(128)
+tv3_first_kernel(const float * __restrict__ f, float beta, float * __restrict__ Z, Vol3<Off> v, float gamma)
+{
+  const Off nvox = v.sz * v.n[2];
+  float *   zx = Z;
+  float *   zy = Z + nvox;
+  float *   zz = Z + 2 * nvox;
+  FOR_EACH_ROW_VOXEL(v.n)
+  {
+    const Off   p = (Off)iz * v.sz + (Off)iy * v.sy + ix;
+    const float w0 = f[p] * beta;
+    float       a = ix < v.n[0] - 1 ? (f[p + 1] * beta - w0) * v.isx : 0.f;
+    float       b = iy < v.n[1] - 1 ? (f[p + v.sy] * beta - w0) * v.isy : 0.f;
+    float       c = iz < v.n[2] - 1 ? (f[p + v.sz] * beta - w0) * v.isz : 0.f;
+    clip3(a, b, c, gamma);
+    zx[p] = a;
+    zy[p] = b;
+    zz[p] = c;
+  }
+}
+
+template <typename Off>
+__global__ void __launch_bounds__(128)
+tv3_iterate_kernel(const float * __restrict__ f, const float * __restrict__ Zin, float * __restrict__ Zout,
+                   Vol3<Off> v, float beta1, float gamma)
+{
+  const Off     nvox = v.sz * v.n[2];
+  const float * zx = Zin;
+  const float * zy = Zin + nvox;
+  const float * zz = Zin + 2 * nvox;
+  FOR_EACH_ROW_VOXEL(v.n)
+  {
+    const Off   p = (Off)iz * v.sz + (Off)iy * v.sy + ix;
+    const float w0 = (f[p] - div3(zx, zy, zz, v, ix, iy, iz, p)) * beta1;
+    float       a = zx[p], b = zy[p], c = zz[p];
+    if (ix < v.n[0] - 1)
+      a -= ((f[p + 1] - div3(zx, zy, zz, v, ix + 1, iy, iz, p + 1)) * beta1 - w0) * v.isx;
+    if (iy < v.n[1] - 1)
+      b -= ((f[p + v.sy] - div3(zx, zy, zz, v, ix, iy + 1, iz, p + v.sy)) * beta1 - w0) * v.isy;
+    if (iz < v.n[2] - 1)
+      c -= ((f[p + v.sz] - div3(zx, zy, zz, v, ix, iy, iz + 1, p + v.sz)) * beta1 - w0) * v.isz;
+    clip3(a, b, c, gamma);
+    Zout[p] = a;
+    Zout[nvox + p] = b;
+    Zout[2 * nvox + p] = c;
+  }
+}
+
+template <typename Off>
+__global__ void __launch_bounds__(128)
+tv3_final_kernel(const float * f, const float * __restrict__ Z, float * out, Vol3<Off> v)
+{
+  const Off     nvox = v.sz * v.n[2];
+  const float * zx = Z;
+  const float * zy = Z + nvox;
+  const float * zz = Z + 2 * nvox;
+  FOR_EACH_ROW_VOXEL(v.n)
+  {
+    const Off p = (Off)iz * v.sz + (Off)iy * v.sy + ix;
+    out[p] = f[p] - div3(zx, zy, zz, v, ix, iy, iz, p);
+  }
+}
+
+template <typename Off>
+void
+tv3_run(const rtkb_image_desc & vd, const TvDims & t, const float * f, float * out, int niter, float b0, float b1,
+        float g, float * Z, dim3 grid, cudaStream_t st)
+{
+  Vol3<Off> v;
+  for (int d = 0; d < 3; d++)
+    v.n[d] = vd.size[d];
+  v.sy = (Off)vd.size[0];
+  v.sz = (Off)vd.size[0] * vd.size[1];
+  v.isx = t.inv_s[0];
+  v.isy = t.inv_s[1];
+  v.isz = t.inv_s[2];
+  const long long nvox = (long long)vd.size[0] * vd.size[1] * vd.size[2];
+  float *         za = Z;
+  float *         zb = Z + 3 * nvox;
+  tv3_first_kernel<Off><<<grid, 128, 0, st>>>(f, b0, za, v, g);
+  for (int it = 1; it < niter; it++)
+  {
+    tv3_iterate_kernel<Off><<<grid, 128, 0, st>>>(f, za, zb, v, b1, g);
+    std::swap(za, zb);
+  }
+  tv3_final_kernel<Off><<<grid, 128, 0, st>>>(f, za, out, v);
 }
 
 // x = max(x, 0) (ThresholdBelow(0), outside value 0) and / or
@@ -217,10 +388,11 @@ tv_dims(const rtkb_image_desc & v, const int * dims, TvDims & t, double & min_sp
   return true;
 }
 
-// BPDQ TV denoising of f into out (out may equal f); Z: nd * nvox floats, w: nvox floats.
+// BPDQ TV denoising of f into out (out may equal f); Z: two buffers of three
+// planes of nvox floats.
 cudaError_t
 tv_bpdq(const rtkb_image_desc & v, const float * f, float * out, double gamma, int niter, const int * dims, float * Z,
-        float * w, cudaStream_t st)
+        cudaStream_t st)
 {
   TvDims t;
   double minsp = 0.;
@@ -231,13 +403,23 @@ tv_bpdq(const rtkb_image_desc & v, const float * f, float * out, double gamma, i
   const dim3      grid = row_grid(v);
   if (t.nd == 0)
     return f == out ? cudaSuccess : cudaMemcpyAsync(out, f, (size_t)nvox * 4, cudaMemcpyDeviceToDevice, st);
-  tv_gradient_kernel<false><<<grid, 128, 0, st>>>(f, b0, Z, t, g);
+  if (t.nd == 3)
+  {
+    if (nvox < (1LL << 31) - (1LL << 20))
+      tv3_run<int>(v, t, f, out, niter, b0, b1, g, Z, grid, st);
+    else
+      tv3_run<long long>(v, t, f, out, niter, b0, b1, g, Z, grid, st);
+    return cudaGetLastError();
+  }
+  float * za = Z;
+  float * zb = Z + 3 * nvox;
+  tv_first_kernel<<<grid, 128, 0, st>>>(f, b0, za, t, g);
   for (int it = 1; it < niter; it++)
   {
-    tv_divergence_kernel<false><<<grid, 128, 0, st>>>(f, Z, w, t, b1);
-    tv_gradient_kernel<true><<<grid, 128, 0, st>>>(w, 1.f, Z, t, g);
+    tv_iterate_kernel<<<grid, 128, 0, st>>>(f, za, zb, t, b1, g);
+    std::swap(za, zb);
   }
-  tv_divergence_kernel<true><<<grid, 128, 0, st>>>(f, Z, out, t, 1.f);
+  tv_final_kernel<<<grid, 128, 0, st>>>(f, za, out, t);
   return cudaGetLastError();
 }
 
@@ -267,10 +449,8 @@ rtkb_tv_denoising_bpdq(const rtkb_image_desc * vol, const float * d_in, float * 
     return RTKB_OK;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   void *       mem = nullptr;
-  RTKB_CUDA_TRY(scratch_malloc(&mem, 4 * up256((size_t)nvox * 4), st));
-  float *     Z = static_cast<float *>(mem);
-  float *     w = reinterpret_cast<float *>(static_cast<char *>(mem) + 3 * up256((size_t)nvox * 4));
-  cudaError_t e = tv_bpdq(*vol, d_in, d_out, gamma, niter, dims, Z, w, st);
+  RTKB_CUDA_TRY(scratch_malloc(&mem, (size_t)6 * nvox * 4, st));
+  cudaError_t e = tv_bpdq(*vol, d_in, d_out, gamma, niter, dims, static_cast<float *>(mem), st);
   cudaError_t fe = scratch_free(mem, st);
   if (e != cudaSuccess)
     return cuda_fail(e, "TV denoising");
@@ -338,7 +518,7 @@ rtkb_regularized_cg(const rtkb_geometry * g, const rtkb_image_desc * vol, const 
     return rc;
   const size_t vb = up256((size_t)nvox * 4);
   void *       mem = nullptr;
-  cudaError_t  e = scratch_malloc(&mem, (prm->tv ? 5 : 1) * vb, st);
+  cudaError_t  e = scratch_malloc(&mem, vb + (prm->tv ? (size_t)6 * nvox * 4 : 0), st);
   if (e != cudaSuccess)
   {
     rtkb_cg_destroy(plan);
@@ -346,7 +526,6 @@ rtkb_regularized_cg(const rtkb_geometry * g, const rtkb_image_desc * vol, const 
   }
   float *   b = static_cast<float *>(mem);
   float *   Z = prm->tv ? reinterpret_cast<float *>(static_cast<char *>(mem) + vb) : nullptr;
-  float *   w = prm->tv ? reinterpret_cast<float *>(static_cast<char *>(mem) + 4 * vb) : nullptr;
   const int all[3] = { 1, 1, 1 };
   int       dims[3];
   for (int d = 0; d < 3; d++)
@@ -366,7 +545,7 @@ rtkb_regularized_cg(const rtkb_geometry * g, const rtkb_image_desc * vol, const 
       if ((e = cudaGetLastError()) != cudaSuccess)
         rc = cuda_fail(e, "positivity");
     }
-    if (rc == RTKB_OK && prm->tv && (e = tv_bpdq(*vol, d_x, d_x, prm->gamma_tv, prm->tv_iterations, dims, Z, w, st)) !=
+    if (rc == RTKB_OK && prm->tv && (e = tv_bpdq(*vol, d_x, d_x, prm->gamma_tv, prm->tv_iterations, dims, Z, st)) !=
                                       cudaSuccess)
       rc = cuda_fail(e, "TV denoising");
     if (rc == RTKB_OK && prm->soft_threshold_on_image)

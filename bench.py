@@ -762,6 +762,24 @@ def profile_fdk():
     return 0
 
 
+def profile_tv():
+    """TV denoising (BPDQ, gamma 5e-5, 3 iterations) of a uniform random 256^3
+    volume, run twice: one first-iteration, two fused-iteration and one final
+    launch each, for ncu captures of the TV kernels."""
+    import torch
+
+    import rtk_b200 as rtkb
+
+    rtkb.load()
+    vd = rtkb.make_desc((256, 256, 256), (1.0, 1.0, 1.0))
+    x = torch.rand((256, 256, 256), device="cuda", generator=torch.Generator(device="cuda").manual_seed(SEED))
+    out = torch.empty_like(x)
+    for _ in range(2):
+        rtkb.ops.tv_denoising_bpdq(vd, x, 5e-5, 3, out=out)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_tv": "256^3, 3 BPDQ iterations x 2"}), flush=True)
+
+
 def use_profile_case():
     """256^3 at 0.5 mm (the benchmark's voxel size, so the same tile
     footprints and kernel configuration) from 360 of the 1024x768 projections:
@@ -787,6 +805,8 @@ def main():
                          "start + 2 eager iterations, one U-Net forward on the volume, one training step on 4 x 64^3")
     ap.add_argument("--profile-fdk", action="store_true",
                     help="FDK preprocessing (weights + Hann ramp filter) of the 720 x 1024x768 stack, twice, for ncu")
+    ap.add_argument("--profile-tv", action="store_true",
+                    help="TV denoising (BPDQ) of a uniform random 256^3 volume, 3 iterations, twice, for ncu")
     ap.add_argument("--profile-case", action="store_true",
                     help="small case for ncu captures: 256^3 @1mm from 360 projections, device-timed region only")
     args = ap.parse_args()
@@ -794,6 +814,8 @@ def main():
         return profile_cg()
     if args.profile_fdk:
         return profile_fdk()
+    if args.profile_tv:
+        return profile_tv()
     args.warmup = max(args.warmup, 3)
     if args.profile_case:
         use_profile_case()

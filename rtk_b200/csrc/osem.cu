@@ -128,19 +128,79 @@ voxel_grid(const rtkb_image_desc & v)
               (unsigned)std::min(v.size[2], 65535));
 }
 
-// OSEM update: x_out = DivideOrZeroOut(B x, R).  x_out may equal x when the
-// neighbourhood term is off (beta = 0).
-template <bool kStencil>
+// OSEM update without the neighbourhood term (beta = 0), in place:
+// x = DivideOrZeroOut(B x, R), R = (N + sqrt(N N + 0)) / 2.
 __global__ void __launch_bounds__(128)
-osem_update_kernel(const float * x, const float * __restrict__ B, const float * __restrict__ N, float * x_out,
-                   int nx, int ny, int nz, float beta, float c2)
+osem_update_kernel(float * x, const float * __restrict__ B, const float * __restrict__ N, int nx, int ny, int nz,
+                   float beta, float c2)
 {
   FOR_EACH_VOXEL(nx, ny, nz)
   {
     const long long i = ((long long)iz * ny + iy) * nx + ix;
     const float     m = B[i] * x[i];
-    const float     r = de_pierro_factor<kStencil>(x, ix, iy, iz, nx, ny, nz, N[i], m, beta, c2);
-    x_out[i] = fabsf(r) < kDivideThreshold ? 0.f : m / r;
+    const float     r = de_pierro_factor<false>(x, ix, iy, iz, nx, ny, nz, N[i], m, beta, c2);
+    x[i] = fabsf(r) < kDivideThreshold ? 0.f : m / r;
+  }
+}
+
+// OSEM update with the neighbourhood term, marching along z: a thread owns one
+// (x, y) column over a chunk of slices and slides three 3x3 in-plane sums of x
+// (slices z-1, z, z+1) through registers, so each slice's sum is loaded once
+// and used three times.  K = (3x3x3 box sum) + 25 x_c, summed in double; a
+// double sum of at most 27 floats whose magnitudes lie within 2^24 of one
+// another is exact, so K equals the filter's raster-order double inner
+// product, rounded to float, for such volumes.
+__device__ __forceinline__ double
+plane_sum3(const float * __restrict__ x, int ix, int iy, int z, int nx, int ny, int nz)
+{
+  if (z < 0 || z >= nz)
+    return 0.;
+  const float * slice = x + (long long)z * nx * ny;
+  double        s = 0.;
+#pragma unroll
+  for (int dy = -1; dy <= 1; dy++)
+  {
+    const int y = iy + dy;
+    if (y < 0 || y >= ny)
+      continue;
+    const float * row = slice + (long long)y * nx;
+#pragma unroll
+    for (int dx = -1; dx <= 1; dx++)
+    {
+      const int xx = ix + dx;
+      if (xx >= 0 && xx < nx)
+        s += (double)__ldg(row + xx);
+    }
+  }
+  return s;
+}
+
+constexpr int kZChunk = 16;
+
+__global__ void __launch_bounds__(128)
+osem_update_stencil_kernel(const float * __restrict__ x, const float * __restrict__ B, const float * __restrict__ N,
+                           float * __restrict__ x_out, int nx, int ny, int nz, float beta, float c2)
+{
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ix >= nx)
+    return;
+  const int z0 = blockIdx.z * kZChunk, z1 = min(nz, z0 + kZChunk);
+  for (int iy = blockIdx.y; iy < ny; iy += gridDim.y)
+  {
+    double sm = plane_sum3(x, ix, iy, z0 - 1, nx, ny, nz), s0 = plane_sum3(x, ix, iy, z0, nx, ny, nz);
+    for (int iz = z0; iz < z1; iz++)
+    {
+      const double    sp = plane_sum3(x, ix, iy, iz + 1, nx, ny, nz);
+      const long long i = ((long long)iz * ny + iy) * nx + ix;
+      const float     xc = x[i];
+      const float     m = B[i] * xc;
+      const double    k = sm + s0 + sp + 25. * (double)xc;
+      const float     a = N[i] - (float)k * beta;
+      const float     r = (a + sqrtf(a * a + m * c2)) / 2.f;
+      x_out[i] = fabsf(r) < kDivideThreshold ? 0.f : m / r;
+      sm = s0;
+      s0 = sp;
+    }
   }
 }
 
@@ -364,11 +424,13 @@ rtkb_osem(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image
         if (stencil)
         {
           float * xo = (x == d_x) ? xalt : d_x;
-          osem_update_kernel<true><<<voxel_grid(*vol), 128, 0, st>>>(x, B, N, xo, nx, ny, nz, fb, c2);
+          const dim3 sg((unsigned)((nx + 127) / 128), (unsigned)std::min(ny, 65535),
+                        (unsigned)((nz + kZChunk - 1) / kZChunk));
+          osem_update_stencil_kernel<<<sg, 128, 0, st>>>(x, B, N, xo, nx, ny, nz, fb, c2);
           x = xo;
         }
         else
-          osem_update_kernel<false><<<voxel_grid(*vol), 128, 0, st>>>(x, B, N, x, nx, ny, nz, fb, c2);
+          osem_update_kernel<<<voxel_grid(*vol), 128, 0, st>>>(x, B, N, nx, ny, nz, fb, c2);
         cuda_step(cudaGetLastError(), "OSEM update");
       }
     if (rc == RTKB_OK && x != d_x)

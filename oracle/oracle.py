@@ -98,6 +98,7 @@ def lib():
             "orc_sart": (None, [G, IM, IM, D, D, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_double,
                                 C.POINTER(C.c_int), C.c_int]),
             "orc_de_pierro": (None, [IM, D, D, D, C.c_double, D]),
+            "orc_geometry_set_radius_cylindrical": (None, [G, C.c_double]),
             "orc_tv_denoising_bpdq": (None, [IM, D, D, C.c_double, C.c_int, C.POINTER(C.c_int)]),
             "orc_total_variation": (C.c_double, [IM, D]),
             "orc_regularized_cg": (None, [G, IM, IM, D, D, D, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int,
@@ -163,6 +164,9 @@ class Geometry:
                 self._g = None
         except Exception:
             pass
+
+    def set_radius_cylindrical(self, radius):
+        lib().orc_geometry_set_radius_cylindrical(self._g, float(radius))
 
     def add_projection(self, sid, sdd, gantry_deg, pox=0.0, poy=0.0, oop_deg=0.0, ip_deg=0.0, sox=0.0, soy=0.0):
         rc = lib().orc_geometry_add_projection(self._g, sid, sdd, gantry_deg, pox, poy, oop_deg, ip_deg, sox, soy)

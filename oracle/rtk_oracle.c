@@ -87,6 +87,7 @@ convert_0_2pi(double a)
 /* ------------------------------------------------------------------------ */
 struct orc_geometry
 {
+  double   radius_cyl; /* SetRadiusCylindricalDetector; 0: flat panel */
   int      n, cap;
   double * par; /* 10 per projection: sid sdd ga pox poy oop ip sox soy srcangle */
   double * rot; /* 16 */
@@ -115,6 +116,12 @@ orc_geometry_new(void)
 {
   orc_geometry * g = (orc_geometry *)calloc(1, sizeof(orc_geometry));
   return g;
+}
+
+void
+orc_geometry_set_radius_cylindrical(orc_geometry * g, double radius)
+{
+  g->radius_cyl = radius;
 }
 
 void
@@ -290,6 +297,40 @@ orc_geometry_proj_coords_to_fixed(const orc_geometry * g, int i, double m[16])
   d[10] = 0.;
   rotation_inverse(g->rot + 16 * i, inv);
   mat_mul(inv, d, m, 4, 4, 4);
+}
+
+/* Cylindrical panel (ProjectionsRegionConstIteratorRayBasedWithCylindricalPanel,
+ * include/rtkProjectionsRegionConstIteratorRayBasedWithCylindricalPanel.hxx):
+ * idx2det = GetProjectionCoordinatesToDetectorSystemMatrix(i) x the stack's
+ * index-to-physical matrix; inv = the inverse rotation (detector -> fixed). */
+static void
+cyl_matrices(const orc_geometry * g, int i, const double * pi2pp, double * idx2det, double * inv)
+{
+  const double * p = g->par + 10 * i;
+  double         d[16];
+  mat4_identity(d);
+  d[3] = p[P_POX];
+  d[7] = p[P_POY];
+  d[11] = (p[P_SDD] == 0.) ? -p[P_SID] : p[P_SID] - p[P_SDD];
+  d[10] = 0.;
+  mat_mul(d, pi2pp, idx2det, 4, 4, 4);
+  rotation_inverse(g->rot + 16 * i, inv);
+}
+
+/* NewPixel of the same iterator: the flat-panel u is an arc length on the
+ * cylinder of radius R; its angle a = u / R gives u' = R sin a and
+ * w' = w + R (1 - cos a); out = M x (u', v, w', 1) */
+static void
+cyl_pixel(const double * idx2det, const double * M, double radius, double iu, double iv, double ik, double * out)
+{
+  double pos[3];
+  for (int a = 0; a < 3; a++)
+    pos[a] = idx2det[a * 4 + 0] * iu + idx2det[a * 4 + 1] * iv + idx2det[a * 4 + 2] * ik + idx2det[a * 4 + 3];
+  const double ang = pos[0] / radius;
+  pos[0] = sin(ang) * radius;
+  pos[2] += (1. - cos(ang)) * radius;
+  for (int a = 0; a < 3; a++)
+    out[a] = M[a * 4 + 3] + M[a * 4 + 0] * pos[0] + M[a * 4 + 1] * pos[1] + M[a * 4 + 2] * pos[2];
 }
 
 void
@@ -620,6 +661,9 @@ typedef struct
 {
   double pix2vol[16]; /* projection index -> volume index (homogeneous) */
   double src[3];      /* source in volume index coordinates */
+  double radius;      /* cylindrical panel radius, 0: flat */
+  double idx2det[16]; /* cylindrical: projection index -> flat detector coordinates */
+  double det2vol[16]; /* cylindrical: detector coordinates -> volume index */
 } joseph_proj_t;
 
 static void
@@ -638,6 +682,18 @@ joseph_setup(const orc_geometry * g, const orc_image * vol, const orc_image * pr
   jp->src[0] = sv[0];
   jp->src[1] = sv[1];
   jp->src[2] = sv[2];
+  /* ProjectionsRegionConstIteratorRayBasedWithCylindricalPanel::NewProjection
+   * (include/rtkProjectionsRegionConstIteratorRayBasedWithCylindricalPanel.hxx):
+   * index -> detector system (GetProjectionCoordinatesToDetectorSystemMatrix x
+   * the stack's index-to-physical matrix), detector -> volume index (the
+   * volume's physical-to-index matrix x the inverse rotation) */
+  jp->radius = g->radius_cyl;
+  if (jp->radius != 0.)
+  {
+    double inv[16];
+    cyl_matrices(g, i, pi2pp, jp->idx2det, inv);
+    mat_mul(vpp2i, inv, jp->det2vol, 4, 4, 4);
+  }
 }
 
 typedef struct
@@ -661,9 +717,12 @@ joseph_ray(const orc_image * vol, const joseph_proj_t * jp, double iu, double iv
            joseph_ray_t * r)
 {
   double pix[3], dir[3], bmin[3], bmax[3];
-  for (int a = 0; a < 3; a++)
-    pix[a] = jp->pix2vol[a * 4 + 0] * iu + jp->pix2vol[a * 4 + 1] * iv + jp->pix2vol[a * 4 + 2] * ik +
-             jp->pix2vol[a * 4 + 3];
+  if (jp->radius != 0.)
+    cyl_pixel(jp->idx2det, jp->det2vol, jp->radius, iu, iv, ik, pix);
+  else
+    for (int a = 0; a < 3; a++)
+      pix[a] = jp->pix2vol[a * 4 + 0] * iu + jp->pix2vol[a * 4 + 1] * iv + jp->pix2vol[a * 4 + 2] * ik +
+               jp->pix2vol[a * 4 + 3];
   for (int a = 0; a < 3; a++)
     dir[a] = -(pix[a] - jp->src[a]);
   int mainDir = 0;
@@ -1533,21 +1592,25 @@ orc_project_ellipsoids(const orc_geometry * g, const orc_image * proj, int n_ell
   for (int s = 0; s < np; s++)
   {
     const int k = proj->index[2] + s;
-    double    p2f[16], T[16], src[4];
+    double    p2f[16], T[16], src[4], idx2det[16], inv[16];
     orc_geometry_proj_coords_to_fixed(g, k, p2f);
     mat_mul(p2f, pi2pp, T, 4, 4, 4);
     orc_geometry_source_position(g, k, src);
+    if (g->radius_cyl != 0.)
+      cyl_matrices(g, k, pi2pp, idx2det, inv);
 #pragma omp parallel for num_threads(nthreads) schedule(dynamic, 4)
     for (int j = 0; j < nv; j++)
       for (int i = 0; i < nu; i++)
       {
         const double ii = i + proj->index[0], jj = j + proj->index[1], kk = k;
         double       pix[3], d[3];
+        if (g->radius_cyl != 0.)
+          cyl_pixel(idx2det, inv, g->radius_cyl, ii, jj, kk, pix);
+        else
+          for (int a = 0; a < 3; a++)
+            pix[a] = T[a * 4 + 0] * ii + T[a * 4 + 1] * jj + T[a * 4 + 2] * kk + T[a * 4 + 3];
         for (int a = 0; a < 3; a++)
-        {
-          pix[a] = T[a * 4 + 0] * ii + T[a * 4 + 1] * jj + T[a * 4 + 2] * kk + T[a * 4 + 3];
           d[a] = pix[a] - src[a];
-        }
         const double len = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
         double       acc = 0.;
         for (int e = 0; e < n_ell; e++)

@@ -38,6 +38,8 @@ typedef struct orc_geometry orc_geometry;
 
 /* ---- geometry (src/rtkThreeDCircularProjectionGeometry.cxx) ---- */
 orc_geometry * orc_geometry_new(void);
+/* SetRadiusCylindricalDetector (0: flat panel) */
+void orc_geometry_set_radius_cylindrical(orc_geometry * g, double radius);
 void           orc_geometry_free(orc_geometry * g);
 int            orc_geometry_add_projection(orc_geometry * g, double sid, double sdd, double gantry_deg,
                                            double proj_offset_x, double proj_offset_y, double out_of_plane_deg,

@@ -569,14 +569,15 @@ rtkb_cg_create(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_
     c->nvox = num_pixels(*vol);
     c->npix = num_pixels(*proj);
     std::vector<RayProj> tab;
-    rc = joseph_tables(g->g, *vol, *proj, tab);
+    std::vector<CylProj> cyl;
+    rc = joseph_tables(g->g, *vol, *proj, tab, &cyl);
     if (rc != RTKB_OK)
     {
       release(c);
       return rc;
     }
     auto         up = [](size_t b) { return (b + 255) & ~size_t(255); };
-    const size_t tb = up(tab.size() * sizeof(RayProj)), pb = up((size_t)c->npix * 4), vb = up((size_t)c->nvox * 4);
+    const size_t tb = joseph_table_bytes(tab, cyl), pb = up((size_t)c->npix * 4), vb = up((size_t)c->nvox * 4);
     const size_t sb = up(8 * sizeof(double)), rb = up(kRedBlocks * sizeof(double));
     const size_t fb = up(std::max(joseph_forward_scratch_bytes(c->nvox), joseph_back_scratch_bytes(c->nvox)));
     const size_t total = tb + 2 * pb + 3 * vb + sb + rb + fb;
@@ -606,7 +607,8 @@ rtkb_cg_create(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_
     c->partial = reinterpret_cast<double *>(m);
     m += rb;
     c->scratch = m;
-    e = cudaMemcpy(c->tab, tab.data(), tab.size() * sizeof(RayProj), cudaMemcpyHostToDevice);
+    joseph_args(c->args, *vol, *proj, nullptr);
+    e = joseph_upload_tables(tab, cyl, g->g.radius_cylindrical, c->tab, c->args, nullptr);
     if (e == cudaSuccess)
       e = cudaMemset(c->scal, 0, sb);
     if (e == cudaSuccess)
@@ -619,7 +621,6 @@ rtkb_cg_create(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_
       release(c);
       return cuda_fail(e, "CG plan upload");
     }
-    joseph_args(c->args, *vol, *proj, c->tab);
     *out = c;
     return RTKB_OK;
   }

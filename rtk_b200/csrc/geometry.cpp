@@ -273,15 +273,28 @@ Geometry::source_position(int i, double out[4]) const
 }
 
 void
+Geometry::proj_coords_to_detector(int i, double out[16]) const
+{
+  // GetProjectionCoordinatesToDetectorSystemMatrix, :611-625
+  mat4_identity(out);
+  out[3] = p[i].pox;
+  out[7] = p[i].poy;
+  out[11] = (p[i].sdd == 0.) ? -p[i].sid : p[i].sid - p[i].sdd;
+  out[10] = 0.;
+}
+
+void
+Geometry::inverse_rotation(int i, double out[16]) const
+{
+  rotation_inverse(p[i].rot, out);
+}
+
+void
 Geometry::proj_coords_to_fixed(int i, double out[16]) const
 {
-  // GetProjectionCoordinatesTo{Detector,Fixed}SystemMatrix, :611-637
+  // GetProjectionCoordinatesToFixedSystemMatrix, :627-637
   double d[16], inv[16];
-  mat4_identity(d);
-  d[3] = p[i].pox;
-  d[7] = p[i].poy;
-  d[11] = (p[i].sdd == 0.) ? -p[i].sid : p[i].sid - p[i].sdd;
-  d[10] = 0.;
+  proj_coords_to_detector(i, d);
   rotation_inverse(p[i].rot, inv);
   mat_mul(inv, d, out, 4, 4, 4);
 }

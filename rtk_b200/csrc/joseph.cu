@@ -34,6 +34,7 @@ using rtkb::JosephArgs;
 using rtkb::ld_elem;
 using rtkb::st_elem;
 using rtkb::RayProj;
+using rtkb::CylProj;
 
 struct Ray
 {
@@ -49,12 +50,33 @@ setup_ray(const JosephArgs & a, const RayProj & P, int u, int v, int s, bool for
 {
   const double iu = u + a.pidx0, iv = v + a.pidx1, ik = s + a.pidx2;
   double       pix[3], dir[3];
+  if (a.C)
+  {
+    // ProjectionsRegionConstIteratorRayBasedWithCylindricalPanel::NewPixel: the
+    // flat-panel u is an arc length on the cylinder; its angle gives
+    // u' = R sin(u / R), w' = w + R (1 - cos(u / R))
+    const CylProj & C = a.C[s];
+    double          pos[3];
+#pragma unroll
+    for (int q = 0; q < 3; q++)
+      pos[q] = C.idx2det[q * 4 + 0] * iu + C.idx2det[q * 4 + 1] * iv + C.idx2det[q * 4 + 2] * ik + C.idx2det[q * 4 + 3];
+    const double ang = (1. / a.radius) * pos[0];
+    pos[0] = sin(ang) * a.radius;
+    pos[2] += (1. - cos(ang)) * a.radius;
+#pragma unroll
+    for (int q = 0; q < 3; q++)
+      pix[q] = C.det2vol[q * 4 + 3] + C.det2vol[q * 4 + 0] * pos[0] + C.det2vol[q * 4 + 1] * pos[1] +
+               C.det2vol[q * 4 + 2] * pos[2];
+  }
+  else
+  {
+#pragma unroll
+    for (int q = 0; q < 3; q++)
+      pix[q] = P.pix2vol[q * 4 + 0] * iu + P.pix2vol[q * 4 + 1] * iv + P.pix2vol[q * 4 + 2] * ik + P.pix2vol[q * 4 + 3];
+  }
 #pragma unroll
   for (int q = 0; q < 3; q++)
-  {
-    pix[q] = P.pix2vol[q * 4 + 0] * iu + P.pix2vol[q * 4 + 1] * iv + P.pix2vol[q * 4 + 2] * ik + P.pix2vol[q * 4 + 3];
     dir[q] = -(pix[q] - P.src[q]);
-  }
   int mainDir = 0;
   if (fabs(dir[1]) > fabs(dir[mainDir]))
     mainDir = 1;
@@ -562,7 +584,8 @@ namespace rtkb
 // Per-projection ray set-up tables (ProjectionsRegionConstIteratorRayBasedWithFlatPanel::NewProjection,
 // include/rtkProjectionsRegionConstIteratorRayBasedWithFlatPanel.hxx:39-71).
 int
-joseph_tables(const Geometry & g, const rtkb_image_desc & vol, const rtkb_image_desc & proj, std::vector<RayProj> & out)
+joseph_tables(const Geometry & g, const rtkb_image_desc & vol, const rtkb_image_desc & proj, std::vector<RayProj> & out,
+              std::vector<CylProj> * cyl)
 {
   double vpp2i[16], pi2pp[16];
   if (!physical_to_index(vol, vpp2i))
@@ -585,13 +608,61 @@ joseph_tables(const Geometry & g, const rtkb_image_desc & vol, const rtkb_image_
     r.src[2] = sv[2];
     r.pad = 0.;
   }
+  if (cyl)
+  {
+    cyl->clear();
+    if (g.radius_cylindrical != 0.)
+    {
+      // ...WithCylindricalPanel::NewProjection: index -> detector system
+      // (GetProjectionCoordinatesToDetectorSystemMatrix x the stack's
+      // index-to-physical matrix), detector -> volume index (the volume's
+      // physical-to-index matrix x the inverse rotation)
+      cyl->resize(proj.size[2]);
+      for (int s = 0; s < proj.size[2]; s++)
+      {
+        const int k = proj.index[2] + s;
+        double    det[16], inv[16], i2d[16], d2v[16];
+        g.proj_coords_to_detector(k, det);
+        g.inverse_rotation(k, inv);
+        mat_mul(det, pi2pp, i2d, 4, 4, 4);
+        mat_mul(vpp2i, inv, d2v, 4, 4, 4);
+        std::memcpy((*cyl)[s].idx2det, i2d, 12 * sizeof(double));
+        std::memcpy((*cyl)[s].det2vol, d2v, 12 * sizeof(double));
+      }
+    }
+  }
   return RTKB_OK;
+}
+
+size_t
+joseph_table_bytes(const std::vector<RayProj> & tab, const std::vector<CylProj> & cyl)
+{
+  auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
+  return up(tab.size() * sizeof(RayProj)) + up(cyl.size() * sizeof(CylProj));
+}
+
+cudaError_t
+joseph_upload_tables(const std::vector<RayProj> & tab, const std::vector<CylProj> & cyl, double radius, void * d_mem,
+                     JosephArgs & a, cudaStream_t st)
+{
+  const size_t tb = (tab.size() * sizeof(RayProj) + 255) & ~size_t(255);
+  RayProj *    d_tab = static_cast<RayProj *>(d_mem);
+  CylProj *    d_cyl = cyl.empty() ? nullptr : reinterpret_cast<CylProj *>(static_cast<char *>(d_mem) + tb);
+  cudaError_t  e = cudaMemcpyAsync(d_tab, tab.data(), tab.size() * sizeof(RayProj), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && d_cyl)
+    e = cudaMemcpyAsync(d_cyl, cyl.data(), cyl.size() * sizeof(CylProj), cudaMemcpyHostToDevice, st);
+  a.P = d_tab;
+  a.C = d_cyl;
+  a.radius = d_cyl ? radius : 0.;
+  return e;
 }
 
 void
 joseph_args(JosephArgs & a, const rtkb_image_desc & vol, const rtkb_image_desc & proj, const RayProj * d_tab)
 {
   a.P = d_tab;
+  a.C = nullptr;
+  a.radius = 0.;
   a.nu = proj.size[0];
   a.nv = proj.size[1];
   a.np = proj.size[2];
@@ -762,8 +833,6 @@ joseph_check(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_im
     return fail(RTKB_ERR_INVALID_ARGUMENT, "Geometry has not been set.");
   if (!desc_valid(vol, why) || !desc_valid(proj, why))
     return fail(RTKB_ERR_INVALID_ARGUMENT, why);
-  if (g->g.radius_cylindrical != 0.)
-    return fail(RTKB_ERR_UNSUPPORTED, "cylindrical detectors are not supported by this projector");
   if (proj->index[2] < 0 || (long long)proj->index[2] + proj->size[2] > (long long)g->g.p.size())
     return fail(RTKB_ERR_INVALID_ARGUMENT, "Mismatch between the number of projections and the geometry entries.");
   if (proj->size[1] > 65535 * 8 || proj->size[2] > 65535 || vol->size[1] > 65535)
@@ -786,22 +855,20 @@ rtkb_joseph_forward_project(const rtkb_geometry * g, const rtkb_image_desc * vol
     if (!d_vol || !d_proj_in || !d_proj_out)
       return fail(RTKB_ERR_INVALID_ARGUMENT, "null buffer");
     std::vector<RayProj> tab;
-    rc = joseph_tables(g->g, *vol, *proj, tab);
+    std::vector<CylProj> cyl;
+    rc = joseph_tables(g->g, *vol, *proj, tab, &cyl);
     if (rc != RTKB_OK)
       return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const size_t tbytes = (tab.size() * sizeof(RayProj) + 255) & ~size_t(255);
+    const size_t tbytes = joseph_table_bytes(tab, cyl);
     void *       scratch = nullptr;
     RTKB_CUDA_TRY(rtkb::scratch_malloc(&scratch, tbytes + joseph_forward_scratch_bytes(num_pixels(*vol)), st));
-    RayProj *   d_tab = static_cast<RayProj *>(scratch);
-    void *      d_vt = static_cast<char *>(scratch) + tbytes;
-    cudaError_t e = cudaMemcpyAsync(d_tab, tab.data(), tab.size() * sizeof(RayProj), cudaMemcpyHostToDevice, st);
+    void *     d_vt = static_cast<char *>(scratch) + tbytes;
+    JosephArgs a;
+    joseph_args(a, *vol, *proj, nullptr);
+    cudaError_t e = joseph_upload_tables(tab, cyl, g->g.radius_cylindrical, scratch, a, st);
     if (e == cudaSuccess)
-    {
-      JosephArgs a;
-      joseph_args(a, *vol, *proj, d_tab);
       e = joseph_forward_launch(a, d_vol, d_vt, d_proj_in, d_proj_out, nullptr, st);
-    }
     rc = (e == cudaSuccess) ? RTKB_OK : cuda_fail(e, "joseph forward");
     cudaError_t fe = rtkb::scratch_free(scratch, st);
     if (rc == RTKB_OK && fe != cudaSuccess)
@@ -827,23 +894,21 @@ rtkb_joseph_back_project(const rtkb_geometry * g, const rtkb_image_desc * vol, c
     if (!d_proj || !d_vol_in || !d_vol_out)
       return fail(RTKB_ERR_INVALID_ARGUMENT, "null buffer");
     std::vector<RayProj> tab;
-    rc = joseph_tables(g->g, *vol, *proj, tab);
+    std::vector<CylProj> cyl;
+    rc = joseph_tables(g->g, *vol, *proj, tab, &cyl);
     if (rc != RTKB_OK)
       return rc;
     cudaStream_t    st = static_cast<cudaStream_t>(stream);
     const long long nvox = num_pixels(*vol);
-    const size_t    tbytes = (tab.size() * sizeof(RayProj) + 255) & ~size_t(255);
+    const size_t    tbytes = joseph_table_bytes(tab, cyl);
     void *          scratch = nullptr;
     RTKB_CUDA_TRY(rtkb::scratch_malloc(&scratch, tbytes + joseph_back_scratch_bytes(nvox), st));
-    RayProj *   d_tab = static_cast<RayProj *>(scratch);
-    void *      d_a = static_cast<char *>(scratch) + tbytes;
-    cudaError_t e = cudaMemcpyAsync(d_tab, tab.data(), tab.size() * sizeof(RayProj), cudaMemcpyHostToDevice, st);
+    void *     d_a = static_cast<char *>(scratch) + tbytes;
+    JosephArgs a;
+    joseph_args(a, *vol, *proj, nullptr);
+    cudaError_t e = joseph_upload_tables(tab, cyl, g->g.radius_cylindrical, scratch, a, st);
     if (e == cudaSuccess)
-    {
-      JosephArgs a;
-      joseph_args(a, *vol, *proj, d_tab);
       e = joseph_back_launch(a, d_proj, d_a, d_vol_in, d_vol_out, nullptr, 0.f, st);
-    }
     rc = (e == cudaSuccess) ? RTKB_OK : cuda_fail(e, "joseph back projection");
     cudaError_t fe = rtkb::scratch_free(scratch, st);
     if (rc == RTKB_OK && fe != cudaSuccess)
@@ -869,23 +934,23 @@ rtkb_joseph_sample_count(const rtkb_geometry * g, const rtkb_image_desc * vol, c
     if (!count)
       return fail(RTKB_ERR_INVALID_ARGUMENT, "null count");
     std::vector<RayProj> tab;
-    rc = joseph_tables(g->g, *vol, *proj, tab);
+    std::vector<CylProj> cyl;
+    rc = joseph_tables(g->g, *vol, *proj, tab, &cyl);
     if (rc != RTKB_OK)
       return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const size_t tbytes = (tab.size() * sizeof(RayProj) + 255) & ~size_t(255);
+    const size_t tbytes = joseph_table_bytes(tab, cyl);
     void *       scratch = nullptr;
     RTKB_CUDA_TRY(rtkb::scratch_malloc(&scratch, tbytes + sizeof(unsigned long long), st));
-    RayProj *            d_tab = static_cast<RayProj *>(scratch);
     unsigned long long * d_n = reinterpret_cast<unsigned long long *>(static_cast<char *>(scratch) + tbytes);
     unsigned long long   h = 0;
-    cudaError_t e = cudaMemcpyAsync(d_tab, tab.data(), tab.size() * sizeof(RayProj), cudaMemcpyHostToDevice, st);
+    JosephArgs           a;
+    joseph_args(a, *vol, *proj, nullptr);
+    cudaError_t e = joseph_upload_tables(tab, cyl, g->g.radius_cylindrical, scratch, a, st);
     if (e == cudaSuccess)
       e = cudaMemsetAsync(d_n, 0, sizeof(unsigned long long), st);
     if (e == cudaSuccess)
     {
-      JosephArgs a;
-      joseph_args(a, *vol, *proj, d_tab);
       const dim3 grid((unsigned)((a.nu + 31) / 32), (unsigned)((a.nv + 7) / 8), (unsigned)a.np);
       joseph_count_kernel<<<grid, 256, 0, st>>>(a, d_n);
       e = cudaGetLastError();

@@ -81,6 +81,8 @@ rtkb_project_ellipsoids(const rtkb_geometry * g, const rtkb_image_desc * proj, i
     return fail(RTKB_ERR_INVALID_ARGUMENT, "Mismatch between the number of projections and the geometry entries.");
   if (proj->size[1] > 65535 * 8 || proj->size[2] > 65535)
     return fail(RTKB_ERR_UNSUPPORTED, "projection stack too large for one launch");
+  if (g->g.radius_cylindrical != 0.)
+    return fail(RTKB_ERR_UNSUPPORTED, "the phantom projector models flat panels only");
   try
   {
     std::vector<PixProj> tab(proj->size[2]);

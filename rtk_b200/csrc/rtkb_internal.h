@@ -66,6 +66,8 @@ struct Geometry
                           double sox, double soy);
   void source_position(int i, double out[4]) const;
   void proj_coords_to_fixed(int i, double out[16]) const;
+  void proj_coords_to_detector(int i, double out[16]) const; // GetProjectionCoordinatesToDetectorSystemMatrix
+  void inverse_rotation(int i, double out[16]) const;        // GetRotationMatrices()[i] inverse
   void source_angles(std::vector<double> & out) const;
   void gantry_angles(std::vector<double> & out) const;
   void tilt_angles(std::vector<double> & out) const;

@@ -14,9 +14,20 @@ struct RayProj
   double pad;
 };
 
+// Cylindrical panel (ProjectionsRegionConstIteratorRayBasedWithCylindricalPanel):
+// projection index -> flat detector coordinates (u along the arc, v, w), and
+// detector coordinates -> volume index, rows 0-2 of each.
+struct CylProj
+{
+  double idx2det[12];
+  double det2vol[12];
+};
+
 struct JosephArgs
 {
   const RayProj * P;
+  const CylProj * C;      // per-projection cylindrical tables, nullptr for a flat panel
+  double          radius; // cylindrical panel radius (with C)
   int             nu, nv, np;
   int             pidx0, pidx1, pidx2; // absolute index of buffer pixel (0, 0, 0)
   int             n[3];                // volume size
@@ -27,8 +38,14 @@ struct JosephArgs
 
 
 // Per-projection ray tables of a stack (host side).
+// (cyl: filled for a cylindrical panel, left empty for a flat one)
 int  joseph_tables(const Geometry & g, const rtkb_image_desc & vol, const rtkb_image_desc & proj,
-                   std::vector<RayProj> & out);
+                   std::vector<RayProj> & out, std::vector<CylProj> * cyl = nullptr);
+// Device bytes of both tables, each 256-byte aligned.
+size_t joseph_table_bytes(const std::vector<RayProj> & tab, const std::vector<CylProj> & cyl);
+// Copies both tables to d_mem (joseph_table_bytes bytes) on st and points a's tables there.
+cudaError_t joseph_upload_tables(const std::vector<RayProj> & tab, const std::vector<CylProj> & cyl, double radius,
+                                 void * d_mem, JosephArgs & a, cudaStream_t st);
 void joseph_args(JosephArgs & a, const rtkb_image_desc & vol, const rtkb_image_desc & proj, const RayProj * d_tab);
 
 int joseph_check(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj);

@@ -133,6 +133,8 @@ ray_box_lengths(const rtkb_geometry * g, const rtkb_image_desc & vol, const rtkb
                 cudaStream_t st)
 {
   using namespace rtkb;
+  if (g->g.radius_cylindrical != 0.)
+    return fail(RTKB_ERR_UNSUPPORTED, "ray-box lengths are computed for flat panels only");
   std::vector<RayTab> tab(proj.size[2]);
   double              pi2pp[16];
   index_to_physical(proj, pi2pp);

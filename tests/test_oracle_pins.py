@@ -4,6 +4,8 @@ ITK is absent, so RTK's filters cannot run here; these are the reference's
 known-answer checks restated on the oracle:
   * test/rtkfdktest.cxx:30-120      FDK of the Shepp-Logan phantom (err/px < 0.03, PSNR > 26)
   * test/rtkforwardprojectiontest.cxx:29-130  Joseph FP of a box vs ray-box lengths (1.28 / 44 dB on 255)
+  * test/rtkforwardprojectiontest.cxx:158-193 Joseph FP of the Shepp-Logan phantom vs its analytic projections,
+                                              flat and cylindrical (radius 600) detector (1.28 / 44 dB on 255)
   * test/rtkadjointoperatorstest.cxx  Joseph FP/BP adjointness (|ratio - 1| < 1e-3; FP64 gives ~1e-13)
 plus algebraic properties of the weighting filters that RTK's formulas imply.
 """
@@ -73,6 +75,46 @@ def test_joseph_box_like_rtkforwardprojectiontest(oracle):
         fp = O.joseph_forward(g, vol, ones, proj)
         err, psnr, ok = phantoms.check_image_quality(fp, ref, 1.28, 44.0, 255.0)
         assert ok, (q, err, psnr)
+
+
+@pytest.mark.parametrize("radius", [0.0, 600.0])
+def test_joseph_shepp_logan_like_rtkforwardprojectiontest(oracle, radius):
+    """Cases 3 (flat) and 4 (cylindrical detector): 45 projections (SID 500, SDD 1000, 8 deg steps) of a 128^3
+    Shepp-Logan at 2 mm (RTK's default phantom scale 128) against the analytic projections."""
+    O = oracle
+    n = 45
+    g = O.Geometry()
+    for i in range(n):
+        g.add_projection(500.0, 1000.0, i * 8.0)
+    g.set_radius_cylindrical(radius)
+    vol = O.image((128, 128, 128), (2.0, 2.0, 2.0), origin=(-127.0, -127.0, -127.0))
+    proj = O.image((64, 64, n), (4.0, 4.0, 4.0), origin=(-126.0, -126.0, -126.0))
+    sl = phantoms.shepp_logan(128.0)
+    ref = O.project_ellipsoids(g, proj, sl)
+    fp = O.joseph_forward(g, vol, O.draw_ellipsoids(vol, sl), proj)
+    err, psnr, ok = phantoms.check_image_quality(fp, ref, 1.28, 44.0, 255.0)
+    assert ok, (radius, err, psnr)
+
+
+@pytest.mark.parametrize("radius,expected", [(0.0, 200.0), (1000.0, 1000.0 * np.arctan(0.2))])
+def test_cylindrical_panel_arc_length(oracle, radius, expected):
+    """A cylinder centred on the source (R = SDD) records a ray at angle theta from the central ray at arc length
+    R theta: a 1 mm sphere at x = 100 mm seen from SID 500 projects to u = 1000 atan(0.2) = 197.40 mm, against
+    SDD x / SID = 200 mm on a flat panel (centroid of the analytic line integrals along u)."""
+    O = oracle
+    g = O.Geometry()
+    g.add_projection(500.0, 1000.0, 0.0)
+    g.set_radius_cylindrical(radius)
+    proj = O.image((400, 1, 1), (0.025, 0.025, 1.0), origin=(195.0, 0.0, 0.0))
+    sphere = np.zeros(16)
+    sphere[0] = 100.0
+    sphere[3:6] = 1.0
+    sphere[6:15] = np.eye(3).reshape(9)
+    sphere[15] = 1.0
+    p = O.project_ellipsoids(g, proj, sphere[None])[0, 0]
+    u = 195.0 + 0.025 * np.arange(400)
+    assert p.sum() > 0
+    assert abs((p * u).sum() / p.sum() - expected) < 0.02, (p * u).sum() / p.sum()
 
 
 @pytest.mark.parametrize("sdd", [1200.0, 0.0])

@@ -556,6 +556,45 @@ orc_backproject(const orc_geometry * g, const orc_image * vol, const orc_image *
   const long nvox = npix(vol);
   if (vol_out != vol_in)
     memcpy(vol_out, vol_in, sizeof(double) * nvox);
+  if (!fdk && g->radius_cyl != 0.)
+  {
+    /* CylindricalDetectorCenteredOnSourceBackprojection
+     * (include/rtkBackProjectionImageFilter.hxx:283-345) with the matrices of
+     * :551-595: (a, b, c) = Mag Src Rot I2P_vol x, u = a/c, v = b/c,
+     * u' = R atan2(u, R), v' = v R / sqrt(R^2 + u^2), index = P2I_proj ProjT (u', v'),
+     * clamp-to-edge bilinear inside [-0.5, N - 0.5) */
+    const double R = g->radius_cyl;
+    double       i2p[16], p2i[16];
+    orc_index_to_physical(vol, i2p);
+    orc_physical_to_index(proj, p2i);
+    for (int s = 0; s < np; s++)
+    {
+      const int      k = proj->index[2] + s;
+      double         t1[12], t2[12], A[12], B[9];
+      const double   m[9] = { p2i[0], p2i[1], p2i[3], p2i[4], p2i[5], p2i[7], 0., 0., 1. };
+      const double * p = proj_data + (long)s * nu * nv;
+      mat_mul(g->mag + 12 * k, g->srt + 16 * k, t1, 3, 4, 4);
+      mat_mul(t1, g->rot + 16 * k, t2, 3, 4, 4);
+      mat_mul(t2, i2p, A, 3, 4, 4);
+      mat_mul(m, g->prt + 9 * k, B, 3, 3, 3);
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 1)
+      for (int kz = 0; kz < nz; kz++)
+        for (int j = 0; j < ny; j++)
+          for (int i = 0; i < nx; i++)
+          {
+            const double x = i + vol->index[0], y = j + vol->index[1], z = kz + vol->index[2];
+            const double c = A[8] * x + A[9] * y + A[10] * z + A[11];
+            const double u = (A[0] * x + A[1] * y + A[2] * z + A[3]) / c;
+            const double v = (A[4] * x + A[5] * y + A[6] * z + A[7]) / c;
+            const double u2 = R * atan2(u, R), v2 = v * R / sqrt(R * R + u * u);
+            const double ci = B[0] * u2 + B[1] * v2 + B[2] - proj->index[0];
+            const double cj = B[3] * u2 + B[4] * v2 + B[5] - proj->index[1];
+            if (ci >= -0.5 && ci < nu - 0.5 && cj >= -0.5 && cj < nv - 0.5)
+              vol_out[((long)kz * ny + j) * nx + i] += interp_clamped(p, nu, nv, ci, cj);
+          }
+    }
+    return;
+  }
   double * mats = (double *)malloc(sizeof(double) * 12 * (np > 0 ? np : 1));
   int *    modes = (int *)malloc(sizeof(int) * (np > 0 ? np : 1));
   for (int s = 0; s < np; s++)

@@ -32,6 +32,7 @@
 #include <algorithm>
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 
 namespace rtkb
 {
@@ -1020,12 +1021,21 @@ backproject_geometry(const rtkb_geometry * g, const rtkb_image_desc * vol, const
     return fail(RTKB_ERR_INVALID_ARGUMENT, "Geometry has not been set.");
   if (!desc_valid(vol, why) || !desc_valid(proj, why))
     return fail(RTKB_ERR_INVALID_ARGUMENT, why);
-  if (g->g.radius_cylindrical != 0.)
-    return fail(RTKB_ERR_UNSUPPORTED,
-                "Voxel-based FDK back projector can currently not handle cylindrical detectors");
   const int nproj = proj->size[2];
   if (proj->index[2] < 0 || (long long)proj->index[2] + nproj > (long long)g->g.p.size())
     return fail(RTKB_ERR_INVALID_ARGUMENT, "Mismatch between the number of projections and the geometry entries.");
+  if (g->g.radius_cylindrical != 0.)
+  {
+    // RTK's FDK back projector refuses cylindrical detectors; its voxel-based
+    // one handles a cylinder centred on the source (float stacks here)
+    if (fdk || fixed_scratch)
+      return fail(RTKB_ERR_UNSUPPORTED,
+                  "Voxel-based FDK back projector can currently not handle cylindrical detectors");
+    if constexpr (!std::is_same<T, float>::value)
+      return fail(RTKB_ERR_UNSUPPORTED, "cylindrical detectors need a float32 projection stack");
+    else
+      return cylindrical_backproject(g, *vol, *proj, d_proj, d_vin, d_vout, static_cast<cudaStream_t>(stream));
+  }
   std::vector<double> mats(12 * (size_t)nproj);
   std::vector<int>    modes(nproj);
   for (int s = 0; s < nproj; s++)

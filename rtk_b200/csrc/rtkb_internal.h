@@ -103,6 +103,11 @@ cudaError_t scratch_free(void * p, cudaStream_t st);
 int cg_rhs(rtkb_cg * c, const float * d_proj, const float * d_weights, int displaced_detector, float * d_b,
            cudaStream_t st);
 
+// The voxel-based back projector for a cylindrical detector centred on the
+// source (float32 stack): d_vout = d_vin + BP(d_proj).
+int cylindrical_backproject(const rtkb_geometry * g, const rtkb_image_desc & vol, const rtkb_image_desc & proj,
+                            const float * d_proj, const float * d_vin, float * d_vout, cudaStream_t st);
+
 // Projection processing order of the iterative solvers when the caller gives
 // none: 0..n-1 shuffled by Fisher-Yates driven by SplitMix64(seed).
 void seeded_order(int n, unsigned long long seed, std::vector<int> & order);

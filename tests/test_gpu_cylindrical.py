@@ -2,7 +2,8 @@
 pair and the CG plan, against the FP64 oracle restating
 include/rtkProjectionsRegionConstIteratorRayBasedWithCylindricalPanel.hxx;
 adjointness; RTK's cylindrical forward-projection test
-(test/rtkforwardprojectiontest.cxx case 4) on the GPU; and the entry points
+(test/rtkforwardprojectiontest.cxx case 4) on the GPU; the voxel-based back
+projector's path for a cylinder centred on the source; and the entry points
 that model flat panels only refusing the geometry."""
 import numpy as np
 import pytest
@@ -97,5 +98,31 @@ def test_flat_panel_only_entry_points_refuse(rtkb, oracle):
         rtkb.ops.ray_box_lengths(gl, vd, pd)
     with pytest.raises(rtkb.RtkbError, match="flat panels only"):
         rtkb.ops.project_ellipsoids(gl, pd, phantoms.shepp_logan(10.0))
-    with pytest.raises(rtkb.RtkbError, match="cylindrical"):
+
+
+@pytest.mark.parametrize("params,radius", [
+    ([(800.0, 1200.0, i * 360.0 / 24) for i in range(24)], 1200.0),
+    ([(700.0, 1100.0, i * 360.0 / 24 + 3.0, 12.0, -7.0, 8.0, 4.0, 5.0, -3.0) for i in range(24)], 1100.0),
+])
+def test_cylindrical_voxel_backprojection_matches_oracle(rtkb, oracle, params, radius):
+    """BackProjectionImageFilter's path for a cylinder centred on the source (radius = SDD)."""
+    gl, go = pair_geometry(rtkb, oracle, params + [(700.0, 1100.0, 0.0)] * 2)
+    gl.SetRadiusCylindricalDetector(radius)
+    go.set_radius_cylindrical(radius)
+    vd, vo = pair_image(rtkb, oracle, (36, 32, 40), (4.0, 4.5, 3.5), index=(2, -3, 1))
+    pd, po = pair_image(rtkb, oracle, (64, 56, 24), (5.0, 5.0, 1.0), index=(-4, 3, 1))
+    rng = np.random.default_rng(7)
+    vol = rng.uniform(0.0, 1.0, size=oracle.shape_of(vo)).astype(np.float32).astype(np.float64)
+    pr = rng.uniform(0.0, 1.0, size=oracle.shape_of(po)).astype(np.float32).astype(np.float64)
+    ref = oracle.backproject(go, vo, po, pr, vol, fdk=False)
+    got = to_np(rtkb.ops.voxel_backproject(gl, vd, pd, to_gpu(pr), to_gpu(vol)))
+    assert rel_l2(got, ref) < REL_L2_TOL, rel_l2(got, ref)
+
+
+def test_cylindrical_voxel_backprojection_refusals(rtkb, oracle):
+    gl, go, vd, vo, pd, po, vol, pr = _case(rtkb, oracle, "radius_600", 4, (16, 16, 16), (24, 20, 4), (5.0, 5.0, 1.0))
+    with pytest.raises(rtkb.RtkbError, match="centered on the source"):
         rtkb.ops.voxel_backproject(gl, vd, pd, to_gpu(pr), to_gpu(vol))
+    gl.SetRadiusCylindricalDetector(1200.0)
+    with pytest.raises(rtkb.RtkbError, match="FDK back projector"):
+        rtkb.ops.fdk_backproject(gl, vd, pd, to_gpu(pr), to_gpu(vol))

@@ -117,6 +117,28 @@ def test_cylindrical_panel_arc_length(oracle, radius, expected):
     assert abs((p * u).sum() / p.sum() - expected) < 0.02, (p * u).sum() / p.sum()
 
 
+@pytest.mark.parametrize("radius", [0.0, 1000.0])
+def test_voxel_backprojection_lands_on_the_panel(oracle, radius):
+    """Back projecting one projection whose pixels hold their own physical u coordinate gives every voxel the u at
+    which its ray meets the panel (bilinear interpolation is exact on a ramp): SDD X / (SID - Z) on a flat panel,
+    SDD atan(X / (SID - Z)) on a cylinder centred on the source (BackProjectionImageFilter's cylindrical path)."""
+    O = oracle
+    g = O.Geometry()
+    g.add_projection(500.0, 1000.0, 0.0)
+    g.set_radius_cylindrical(radius)
+    proj = O.image((200, 20, 1), (2.0, 2.0, 1.0), origin=(-199.0, -19.0, 0.0))
+    vol = O.image((16, 16, 16), (10.0, 10.0, 10.0))
+    p = np.broadcast_to(-199.0 + 2.0 * np.arange(200), (1, 20, 200)).copy()
+    bp = O.backproject(g, vol, proj, p, fdk=False)
+    z, y, x = np.meshgrid(*[vol.origin[a] + vol.spacing[a] * np.arange(16) for a in (2, 1, 0)], indexing="ij")
+    t = x / (500.0 - z)
+    want = 1000.0 * (np.arctan(t) if radius else t)
+    v = y * 1000.0 / (500.0 - z)  # flat-panel v; inside the 40 mm rows on both panels for |v| < 15
+    inside = (np.abs(want) < 190.0) & (np.abs(v) < 15.0)
+    assert inside.sum() > 100
+    np.testing.assert_allclose(bp[inside], want[inside], rtol=0, atol=1e-9)
+
+
 @pytest.mark.parametrize("sdd", [1200.0, 0.0])
 def test_joseph_adjoint(oracle, sdd):
     O = oracle

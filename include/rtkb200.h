@@ -238,6 +238,31 @@ int rtkb_backproject_matrices(const int vol_size[3], const int proj_size[3], int
                               const int * modes, int weighting, const float * d_proj, const float * d_vol_in,
                               float * d_vol_out, void * stream);
 
+/* ---- raw projections to line integrals ----
+ * rtk::I0EstimationProjectionFilter (include/rtkI0EstimationProjectionFilter.hxx):
+ * the unattenuated intensity I0 of a 16-bit raw image (any region the caller
+ * passes: one projection or a stack) as the mode of the histogram of
+ * raw >> bit_shift in the upper quarter of its dynamic range; the range ends
+ * are the outermost bins holding more than dyn_threshold counts.  RTK's
+ * defaults: bit_shift 2, dyn_threshold 20.  All values in raw units; waits
+ * for `stream`. */
+typedef struct rtkb_i0_estimate
+{
+  double i0;         /* GetI0() */
+  double i0_fwhm;    /* GetI0fwhm(): width of the mode at half its count */
+  double imin, imax; /* the consistent dynamic range (GetImin, GetImax) */
+  double low_bound, high_bound;
+} rtkb_i0_estimate;
+int rtkb_i0_estimation(const rtkb_image_desc * desc, const unsigned short * d_raw, int bit_shift,
+                       unsigned int dyn_threshold, rtkb_i0_estimate * out, void * stream);
+/* rtk::LUTbasedVariableI0RawToAttenuationImageFilter
+ * (include/rtkLUTbasedVariableI0RawToAttenuationImageFilter.hxx): d_out =
+ * log(max(I0 - IDark, 1)) - log(max(raw - IDark, 1)) through RTK's float
+ * lookup table (RTK's defaults: I0 = 65535, IDark = 0).  d_out float32 of
+ * the same size as d_raw. */
+int rtkb_raw_to_attenuation(const rtkb_image_desc * desc, const unsigned short * d_raw, double i0, double idark,
+                            float * d_out, void * stream);
+
 /* ---- Joseph projector pair ----
  * rtk::JosephForwardProjectionImageFilter
  * (include/rtkJosephForwardProjectionImageFilter.hxx:182-427):

@@ -98,6 +98,8 @@ def lib():
             "orc_sart": (None, [G, IM, IM, D, D, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_double,
                                 C.POINTER(C.c_int), C.c_int]),
             "orc_de_pierro": (None, [IM, D, D, D, C.c_double, D]),
+            "orc_i0_estimation": (None, [C.POINTER(C.c_ushort), C.c_long, C.c_int, C.c_uint, D]),
+            "orc_raw_to_attenuation": (None, [C.POINTER(C.c_ushort), C.c_long, C.c_double, C.c_double, C.POINTER(C.c_float)]),
             "orc_geometry_set_radius_cylindrical": (None, [G, C.c_double]),
             "orc_tv_denoising_bpdq": (None, [IM, D, D, C.c_double, C.c_int, C.POINTER(C.c_int)]),
             "orc_total_variation": (C.c_double, [IM, D]),
@@ -380,6 +382,24 @@ def regularized_cg(g, vol, proj, proj_data, x0, main_iterations=10, cg_iteration
                              float(gamma_tv), int(tv_iterations), _dims(tv_dims), int(soft_threshold),
                              float(soft_threshold_value), threads or nthreads())
     return x
+
+
+def i0_estimation(raw, bit_shift=2, dyn_threshold=20):
+    """I0EstimationProjectionFilter on a uint16 array: dict of i0, i0_fwhm, imin, imax, low_bound, high_bound."""
+    r = np.ascontiguousarray(raw, dtype=np.uint16)
+    out = np.zeros(6)
+    lib().orc_i0_estimation(r.ctypes.data_as(C.POINTER(C.c_ushort)), r.size, int(bit_shift), int(dyn_threshold),
+                            _d(out))
+    return dict(zip(("i0", "i0_fwhm", "imin", "imax", "low_bound", "high_bound"), out.tolist()))
+
+
+def raw_to_attenuation(raw, i0=65535.0, idark=0.0):
+    """LUTbasedVariableI0RawToAttenuationImageFilter (float32 out)."""
+    r = np.ascontiguousarray(raw, dtype=np.uint16)
+    out = np.empty(r.shape, dtype=np.float32)
+    lib().orc_raw_to_attenuation(r.ctypes.data_as(C.POINTER(C.c_ushort)), r.size, float(i0), float(idark),
+                                 out.ctypes.data_as(C.POINTER(C.c_float)))
+    return out
 
 
 def cg_joseph(g, vol, proj, proj_data, niter, x0=None, weights=None, tikhonov=0.0, gamma=0.0, threads=None):

@@ -2247,3 +2247,78 @@ orc_regularized_cg(const orc_geometry * g, const orc_image * vol, const orc_imag
   }
   free(t);
 }
+
+/* ------------------------------------------------------------------------ */
+/* raw projections to line integrals                                        */
+/* ------------------------------------------------------------------------ */
+void
+orc_i0_estimation(const unsigned short * raw, long n, int shift, unsigned int dyn_threshold, double out[6])
+{
+  /* I0EstimationProjectionFilter (include/rtkI0EstimationProjectionFilter.hxx):
+   * histogram of raw >> shift over 65536 >> shift bins; Imax = the last bin
+   * holding more than dyn_threshold counts (then back to a non-empty bin), Imin
+   * the first such bin below it (then back to a non-empty bin); I0 = the last
+   * highest bin in [3 Imax / 4, Imax) of pixel values; the FWHM bounds walk out
+   * from it while a bin holds more than half the mode's count.  Imin, Imax, I0,
+   * the mode's count and the half count have the 16-bit pixel type, as the
+   * filter declares them. */
+  const long      nbins = 65536L >> shift;
+  unsigned int *  h = (unsigned int *)calloc((size_t)nbins, sizeof(unsigned int));
+  for (long i = 0; i < n; i++)
+    h[raw[i] >> shift]++;
+  long imax = nbins - 1;
+  while (h[imax] <= dyn_threshold && imax > 0)
+    imax--;
+  while (h[imax] == 0 && imax < nbins - 1)
+    imax++;
+  long imin = 0;
+  while (h[imin] <= dyn_threshold && imin < imax)
+    imin++;
+  while (h[imin] == 0 && imin > 0)
+    imin--;
+  const unsigned short Imin = (unsigned short)(imin << shift), Imax = (unsigned short)(imax << shift);
+  const unsigned int   start = (3u * (unsigned int)(Imax >> 2)) >> shift;
+  unsigned int         id = start, maxid = start;
+  unsigned short       maxval = (unsigned short)h[start];
+  for (; id < (unsigned int)(Imax >> shift); id++)
+    if (h[id] >= maxval)
+    {
+      maxval = (unsigned short)h[id];
+      maxid = id;
+    }
+  const unsigned short half = (unsigned short)(float)(maxval >> 1);
+  unsigned int         lo = maxid, hi = maxid;
+  while (h[lo] > half && lo > 0)
+    lo--;
+  while (h[hi] > half && hi < Imax && hi < (unsigned int)nbins - 1)
+    hi++;
+  out[0] = (unsigned short)(maxid << shift);
+  out[1] = (unsigned short)((hi - lo) << shift);
+  out[2] = Imin;
+  out[3] = Imax;
+  out[4] = lo << shift;
+  out[5] = hi << shift;
+  free(h);
+}
+
+void
+orc_raw_to_attenuation(const unsigned short * raw, long n, double i0, double idark, float * out)
+{
+  /* LUTbasedVariableI0RawToAttenuationImageFilter
+   * (include/rtkLUTbasedVariableI0RawToAttenuationImageFilter.hxx): the float
+   * ramp 0..65535 minus float(IDark), values below 1 set to 1 (ThresholdBelow),
+   * log in double rounded to float (itk::LogImageFilter), subtracted from
+   * float(log(max(I0 - IDark, 1))); out = lut[raw] */
+  float *     lut = (float *)malloc(sizeof(float) * 65536);
+  const float c = (float)log(i0 - idark > 1. ? i0 - idark : 1.);
+  for (long r = 0; r < 65536; r++)
+  {
+    float v = (float)r - (float)idark;
+    if (v < 1.f)
+      v = 1.f;
+    lut[r] = c - (float)log((double)v);
+  }
+  for (long i = 0; i < n; i++)
+    out[i] = lut[raw[i]];
+  free(lut);
+}

@@ -149,6 +149,10 @@ void orc_regularized_cg(const orc_geometry * g, const orc_image * vol, const orc
                         const double * weights, double * x, int main_iterations, int cg_iterations, double tikhonov,
                         double gamma, int positivity, int tv, double gamma_tv, int tv_iterations, const int tv_dims[3],
                         int soft_threshold, double soft_threshold_value, int nthreads);
+/* I0EstimationProjectionFilter on n 16-bit pixels: out = I0, I0 FWHM, Imin, Imax, low bound, high bound */
+void orc_i0_estimation(const unsigned short * raw, long n, int shift, unsigned int dyn_threshold, double out[6]);
+/* LUTbasedVariableI0RawToAttenuationImageFilter: out = lut[raw] */
+void orc_raw_to_attenuation(const unsigned short * raw, long n, double i0, double idark, float * out);
 /* RTK's LaplacianImageFilter (Neumann boundary, spacing-scaled): out = Laplacian(x) */
 void orc_laplacian(const orc_image * vol, const double * x, double * out);
 

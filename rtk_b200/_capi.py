@@ -169,6 +169,8 @@ SIGNATURES.update({
     "rtkb_ray_box_lengths": (C.c_int, [_G, _IM, _IM, _V, _V]),
     "rtkb_sart": (C.c_int, [_G, _IM, _IM, _V, _V, C.c_void_p, _V]),
     "rtkb_osem": (C.c_int, [_G, _IM, _IM, _V, _V, C.c_void_p, _V]),
+    "rtkb_i0_estimation": (C.c_int, [_IM, _V, C.c_int, C.c_uint, C.c_void_p, _V]),
+    "rtkb_raw_to_attenuation": (C.c_int, [_IM, _V, C.c_double, C.c_double, _V, _V]),
     "rtkb_regularized_cg": (C.c_int, [_G, _IM, _IM, _V, _V, _V, C.c_void_p, _V]),
     "rtkb_tv_denoising_bpdq": (C.c_int, [_IM, _V, _V, C.c_double, C.c_int, C.POINTER(C.c_int), _V]),
     "rtkb_total_variation": (C.c_int, [_IM, _V, C.POINTER(C.c_double), _V]),
@@ -262,3 +264,10 @@ class RegularizedCgParams(C.Structure):
                 ("tv_iterations", C.c_int), ("tv_dimensions", C.POINTER(C.c_int)),
                 ("soft_threshold_on_image", C.c_int), ("soft_threshold", C.c_double),
                 ("disable_displaced_detector", C.c_int)]
+
+
+class I0Estimate(C.Structure):
+    """rtkb_i0_estimate."""
+
+    _fields_ = [("i0", C.c_double), ("i0_fwhm", C.c_double), ("imin", C.c_double), ("imax", C.c_double),
+                ("low_bound", C.c_double), ("high_bound", C.c_double)]

@@ -1,0 +1,248 @@
+// preprocess.cu -- raw detector counts to line integrals, upstream of the
+// projectors: rtk::I0EstimationProjectionFilter
+// (include/rtkI0EstimationProjectionFilter.hxx) and
+// rtk::LUTbasedVariableI0RawToAttenuationImageFilter
+// (include/rtkLUTbasedVariableI0RawToAttenuationImageFilter.hxx), the two
+// filters rtk::ProjectionsReader chains for 16-bit raw projections.
+//
+// I0 estimation: a histogram of raw >> bitShift (16-bit input: 65536 >>
+// bitShift bins) is built on the GPU, each CTA counting into its own copy in
+// shared memory and adding it to the global histogram once; RTK's integer
+// search for the dynamic range and the background mode then runs on the host
+// on the 64 KB histogram, step for step (including the 16-bit type of the
+// mode's count and of the bounds, as the filter declares them).
+//
+// Conversion: RTK builds a 65536-entry float lookup table
+//   lut[r] = float(log(max(I0 - IDark, 1))) - float(log(double(max(float(r) - float(IDark), 1.f))))
+// (ITK's subtract, threshold-below-1 and log image filters applied to the ramp
+// 0..65535); the table is built the same way on the host and the GPU gathers
+// from it (256 KB, resident in L2): 2 bytes read and 4 written per pixel.
+#include "rtkb200.h"
+#include "rtkb_internal.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <vector>
+
+namespace
+{
+using rtkb::fail;
+
+constexpr int kLutSize = 65536;
+
+// Histogram of (raw >> shift) into hist (nbins <= 16384 with shift >= 2);
+// per-CTA copy in shared memory.
+__global__ void __launch_bounds__(512)
+raw_histogram_kernel(const uint16_t * __restrict__ raw, long long n, int shift, int nbins,
+                     unsigned int * __restrict__ hist)
+{
+  extern __shared__ unsigned int h[];
+  for (int b = threadIdx.x; b < nbins; b += blockDim.x)
+    h[b] = 0u;
+  __syncthreads();
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    atomicAdd(&h[raw[i] >> shift], 1u);
+  __syncthreads();
+  for (int b = threadIdx.x; b < nbins; b += blockDim.x)
+    if (h[b])
+      atomicAdd(&hist[b], h[b]);
+}
+
+// The same without a shared-memory copy (bit shifts below 2: up to 65536 bins)
+__global__ void __launch_bounds__(256)
+raw_histogram_global_kernel(const uint16_t * __restrict__ raw, long long n, int shift, unsigned int * __restrict__ hist)
+{
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    atomicAdd(&hist[raw[i] >> shift], 1u);
+}
+
+// out = lut[raw], eight pixels per 16-byte load where the buffers allow it
+__global__ void __launch_bounds__(256)
+raw_lut_kernel(const uint16_t * __restrict__ raw, long long n, const float * __restrict__ lut, float * __restrict__ out)
+{
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const bool      vec = ((reinterpret_cast<uintptr_t>(raw) | reinterpret_cast<uintptr_t>(out)) & 15) == 0;
+  const long long n8 = vec ? n / 8 : 0;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n8; q += stride)
+  {
+    const uint4 r = reinterpret_cast<const uint4 *>(raw)[q];
+    float4      a, b;
+    a.x = __ldg(lut + (r.x & 0xffffu));
+    a.y = __ldg(lut + (r.x >> 16));
+    a.z = __ldg(lut + (r.y & 0xffffu));
+    a.w = __ldg(lut + (r.y >> 16));
+    b.x = __ldg(lut + (r.z & 0xffffu));
+    b.y = __ldg(lut + (r.z >> 16));
+    b.z = __ldg(lut + (r.w & 0xffffu));
+    b.w = __ldg(lut + (r.w >> 16));
+    reinterpret_cast<float4 *>(out)[2 * q] = a;
+    reinterpret_cast<float4 *>(out)[2 * q + 1] = b;
+  }
+  for (long long i = n8 * 8 + blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += stride)
+    out[i] = __ldg(lut + raw[i]);
+}
+
+unsigned
+grid_of(long long n)
+{
+  return (unsigned)std::max<long long>(1, std::min<long long>((n + 255) / 256, 148LL * 8));
+}
+} // namespace
+
+namespace rtkb
+{
+// RTK's search on the histogram (ThreadedGenerateData's last-thread block and
+// AfterThreadedGenerateData), with the filter's types: Imin, Imax, I0, the
+// mode's count and the half-maximum are of the 16-bit pixel type.
+void
+i0_search(const std::vector<unsigned int> & hist, int shift, unsigned int dyn_threshold, rtkb_i0_estimate & out)
+{
+  const size_t nbins = hist.size();
+  size_t       imax = nbins - 1;
+  while (hist[imax] <= dyn_threshold && imax > 0)
+    --imax;
+  while (hist[imax] == 0 && imax + 1 < nbins) // back to a non-empty bin (RTK's loop can run past the end)
+    ++imax;
+  size_t imin = 0;
+  while (hist[imin] <= dyn_threshold && imin < imax)
+    ++imin;
+  while (hist[imin] == 0 && imin > 0)
+    --imin;
+  const uint16_t Imin = (uint16_t)(imin << shift), Imax = (uint16_t)(imax << shift);
+  const unsigned start = (3u * (unsigned)(Imax >> 2)) >> shift;
+  unsigned       idx = start, max_id = start;
+  uint16_t       max_val = (uint16_t)hist[start];
+  while (idx < (unsigned)(Imax >> shift))
+  {
+    if (hist[idx] >= max_val)
+    {
+      max_val = (uint16_t)hist[idx];
+      max_id = idx;
+    }
+    ++idx;
+  }
+  const uint16_t I0 = (uint16_t)(max_id << shift);
+  const uint16_t width = (uint16_t)(float)(max_val >> 1);
+  unsigned       low = max_id;
+  while (hist[low] > width && low > 0)
+    --low;
+  unsigned high = max_id;
+  while (hist[high] > width && high < Imax && high + 1 < nbins)
+    ++high;
+  out.i0 = I0;
+  out.i0_fwhm = (uint16_t)((high - low) << shift);
+  out.imin = Imin;
+  out.imax = Imax;
+  out.low_bound = low << shift;
+  out.high_bound = high << shift;
+}
+
+// lut[r] as RTK's LUT pipeline computes it (float ramp minus float(IDark),
+// values below 1 set to 1, log in double rounded to float, subtracted from
+// float(log(max(I0 - IDark, 1))))
+void
+raw_to_attenuation_lut(double i0, double idark, std::vector<float> & lut)
+{
+  lut.resize(kLutSize);
+  const float c = (float)std::log(std::max(i0 - idark, 1.));
+  const float d = (float)idark;
+  for (int r = 0; r < kLutSize; r++)
+  {
+    float v = (float)r - d;
+    if (v < 1.f)
+      v = 1.f;
+    lut[r] = c - (float)std::log((double)v);
+  }
+}
+} // namespace rtkb
+
+extern "C" int
+rtkb_i0_estimation(const rtkb_image_desc * desc, const unsigned short * d_raw, int bit_shift,
+                   unsigned int dyn_threshold, rtkb_i0_estimate * out, void * stream)
+{
+  using namespace rtkb;
+  std::string why;
+  if (!desc || !d_raw || !out)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "null argument");
+  if (!desc_valid(desc, why))
+    return fail(RTKB_ERR_INVALID_ARGUMENT, why);
+  if (bit_shift < 0 || bit_shift > 8)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "bit shift must lie in 0..8");
+  try
+  {
+    cudaStream_t    st = static_cast<cudaStream_t>(stream);
+    const long long n = num_pixels(*desc);
+    const int       nbins = kLutSize >> bit_shift;
+    unsigned int *  d_hist = nullptr;
+    RTKB_CUDA_TRY(scratch_malloc(&d_hist, (size_t)nbins * 4, st));
+    cudaError_t e = cudaMemsetAsync(d_hist, 0, (size_t)nbins * 4, st);
+    if (e == cudaSuccess && n > 0)
+    {
+      if (bit_shift >= 2)
+      {
+        const size_t smem = (size_t)nbins * 4;
+        static_cast<void>(cudaFuncSetAttribute(raw_histogram_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)smem));
+        const unsigned blocks = (unsigned)std::max<long long>(1, std::min<long long>((n + 511) / 512, 148LL * 2));
+        raw_histogram_kernel<<<blocks, 512, smem, st>>>(d_raw, n, bit_shift, nbins, d_hist);
+      }
+      else
+        raw_histogram_global_kernel<<<grid_of(n), 256, 0, st>>>(d_raw, n, bit_shift, d_hist);
+      e = cudaGetLastError();
+    }
+    std::vector<unsigned int> hist(nbins);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(hist.data(), d_hist, (size_t)nbins * 4, cudaMemcpyDeviceToHost, st);
+    const cudaError_t fe = scratch_free(d_hist, st);
+    if (e == cudaSuccess)
+      e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess)
+      return cuda_fail(e, "I0 estimation");
+    if (fe != cudaSuccess)
+      return cuda_fail(fe, "cudaFreeAsync");
+    i0_search(hist, bit_shift, dyn_threshold, *out);
+    return RTKB_OK;
+  }
+  catch (...)
+  {
+    return fail(RTKB_ERR_OUT_OF_MEMORY, "host allocation failed");
+  }
+}
+
+extern "C" int
+rtkb_raw_to_attenuation(const rtkb_image_desc * desc, const unsigned short * d_raw, double i0, double idark,
+                        float * d_out, void * stream)
+{
+  using namespace rtkb;
+  std::string why;
+  if (!desc || !d_raw || !d_out)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "null argument");
+  if (!desc_valid(desc, why))
+    return fail(RTKB_ERR_INVALID_ARGUMENT, why);
+  if (!std::isfinite(i0) || !std::isfinite(idark))
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "I0 and IDark must be finite");
+  try
+  {
+    std::vector<float> lut;
+    raw_to_attenuation_lut(i0, idark, lut);
+    cudaStream_t    st = static_cast<cudaStream_t>(stream);
+    const long long n = num_pixels(*desc);
+    float *         d_lut = nullptr;
+    RTKB_CUDA_TRY(scratch_malloc(&d_lut, (size_t)kLutSize * 4, st));
+    cudaError_t e = cudaMemcpyAsync(d_lut, lut.data(), (size_t)kLutSize * 4, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && n > 0)
+    {
+      raw_lut_kernel<<<grid_of((n + 7) / 8), 256, 0, st>>>(d_raw, n, d_lut, d_out);
+      e = cudaGetLastError();
+    }
+    const cudaError_t fe = scratch_free(d_lut, st);
+    if (e != cudaSuccess)
+      return cuda_fail(e, "raw to attenuation");
+    return fe == cudaSuccess ? RTKB_OK : cuda_fail(fe, "cudaFreeAsync");
+  }
+  catch (...)
+  {
+    return fail(RTKB_ERR_OUT_OF_MEMORY, "host allocation failed");
+  }
+}

@@ -378,6 +378,39 @@ def total_variation(vol_desc, x, stream=None) -> float:
     return v.value
 
 
+def _ptr_u16(t):
+    torch = _torch()
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError("expected a CUDA tensor (there is no CPU path)")
+    if t.dtype not in (torch.uint16, torch.int16) or not t.is_contiguous():
+        raise TypeError("expected a contiguous 16-bit tensor of raw counts")
+    return C.c_void_p(t.data_ptr())
+
+
+def i0_estimation(desc, raw, bit_shift=2, dyn_threshold=20, stream=None):
+    """rtk::I0EstimationProjectionFilter on a 16-bit raw image (uint16 CUDA
+    tensor): returns a dict with i0, i0_fwhm, imin, imax, low_bound, high_bound."""
+    from ._capi import I0Estimate
+
+    _check_shape(raw, desc, "raw image")
+    r = I0Estimate()
+    check(load().rtkb_i0_estimation(C.byref(desc), _ptr_u16(raw), int(bit_shift), int(dyn_threshold), C.byref(r),
+                                    _stream(stream)))
+    return {k: getattr(r, k) for k, _ in r._fields_}
+
+
+def raw_to_attenuation(desc, raw, i0=65535.0, idark=0.0, out=None, stream=None):
+    """rtk::LUTbasedVariableI0RawToAttenuationImageFilter: line integrals
+    log(I0 - IDark) - log(raw - IDark) of a uint16 CUDA tensor (float32 out)."""
+    _check_shape(raw, desc, "raw image")
+    if out is None:
+        out = _torch().empty(tuple(raw.shape), device="cuda", dtype=_torch().float32)
+    _check_shape(out, desc, "output")
+    check(load().rtkb_raw_to_attenuation(C.byref(desc), _ptr_u16(raw), float(i0), float(idark), _ptr(out),
+                                         _stream(stream)))
+    return out
+
+
 def _storage_code(storage):
     codes = {"fp32": 0, "bf16": 1}
     if storage not in codes:

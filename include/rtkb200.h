@@ -325,6 +325,17 @@ int  rtkb_cg_start(rtkb_cg * plan, const float * d_proj, const float * d_weights
  * learned preconditioner). */
 int  rtkb_cg_start_rhs(rtkb_cg * plan, const float * d_b, float * d_x, void * stream);
 int  rtkb_cg_iterate(rtkb_cg * plan, int n, void * stream);
+/* Support mask (ConjugateGradientConeBeamReconstructionFilter::SetSupportMask,
+ * include/rtkConjugateGradientConeBeamReconstructionFilter.hxx:246-258 and
+ * include/rtkReconstructionConjugateGradientOperator.hxx:203-262): with a
+ * volume M, b = M .* BP(W .* p) and A x = M .* (BP(W .* FP(M .* x)) + gamma
+ * (-Laplacian(M .* x)) + tikhonov M .* x); rtkb_cg_finish multiplies the
+ * iterate by M, the filter's output multiplication.  d_mask is the caller's
+ * device volume (NULL removes the mask), read until the plan is destroyed or
+ * the mask changes; set it before rtkb_cg_start.  FP32 plans without a
+ * learned preconditioner.  rtkb_cg_finish does nothing without a mask. */
+int  rtkb_cg_set_support_mask(rtkb_cg * plan, const float * d_mask);
+int  rtkb_cg_finish(rtkb_cg * plan, void * stream);
 /* Waits for `stream`; *rr = ||r_k||^2 of the normal equations, *rr0 = ||r_0||^2. */
 int  rtkb_cg_residual(rtkb_cg * plan, double * rr, double * rr0, int * iterations, void * stream);
 void rtkb_cg_destroy(rtkb_cg * plan);
@@ -421,7 +432,7 @@ int rtkb_osem(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_i
  * waits for `stream` before returning.  Defaults in RTK: 10 main iterations,
  * 4 CG iterations, positivity and TV on (gamma_tv 5e-5, 10 iterations, all
  * dimensions), soft threshold off (0.001).  RTK's wavelets denoising step
- * (Daubechies) and support mask are not provided. */
+ * (Daubechies) is not provided. */
 typedef struct rtkb_regularized_cg_params
 {
   int         main_loop_iterations;
@@ -436,6 +447,7 @@ typedef struct rtkb_regularized_cg_params
   int         soft_threshold_on_image;
   double      soft_threshold;
   int         disable_displaced_detector;
+  const float * support_mask; /* NULL: none (the CG's SetSupportMask, its output multiplied by it) */
 } rtkb_regularized_cg_params;
 int rtkb_regularized_cg(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
                         const float * d_proj, const float * d_weights, float * d_x,

@@ -92,7 +92,7 @@ def lib():
             "orc_ramp_padded_size": (C.c_int, [C.c_int, C.POINTER(OrcRampParams)]),
             "orc_ramp_kernel": (None, [C.c_int, C.c_double, C.POINTER(OrcRampParams), D]),
             "orc_ramp_filter": (None, [IM, C.POINTER(OrcRampParams), D, D, C.c_int]),
-            "orc_cg_joseph": (None, [G, IM, IM, D, D, C.c_double, C.c_double, C.c_int, D, D, C.c_int]),
+            "orc_cg_joseph": (None, [G, IM, IM, D, D, D, C.c_double, C.c_double, C.c_int, D, D, C.c_int]),
             "orc_laplacian": (None, [IM, D, D]),
             "orc_ray_box": (None, [G, IM, IM, D, C.c_int]),
             "orc_sart": (None, [G, IM, IM, D, D, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_double,
@@ -103,7 +103,7 @@ def lib():
             "orc_geometry_set_radius_cylindrical": (None, [G, C.c_double]),
             "orc_tv_denoising_bpdq": (None, [IM, D, D, C.c_double, C.c_int, C.POINTER(C.c_int)]),
             "orc_total_variation": (C.c_double, [IM, D]),
-            "orc_regularized_cg": (None, [G, IM, IM, D, D, D, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int,
+            "orc_regularized_cg": (None, [G, IM, IM, D, D, D, D, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int,
                                           C.c_int, C.c_double, C.c_int, C.POINTER(C.c_int), C.c_int, C.c_double, C.c_int]),
             "orc_osem": (None, [G, IM, IM, D, D, C.c_int, C.c_int, C.c_double, C.c_int, C.POINTER(C.c_int), C.c_int]),
             "orc_project_ellipsoids": (None, [G, IM, C.c_int, D, D, C.c_int]),
@@ -372,12 +372,13 @@ def total_variation(vol, x):
 
 def regularized_cg(g, vol, proj, proj_data, x0, main_iterations=10, cg_iterations=4, weights=None, tikhonov=0.0,
                    gamma=0.0, positivity=True, tv=True, gamma_tv=5e-5, tv_iterations=10, tv_dims=(True, True, True),
-                   soft_threshold=False, soft_threshold_value=1e-3, threads=None):
+                   soft_threshold=False, soft_threshold_value=1e-3, mask=None, threads=None):
     """RegularizedConjugateGradientConeBeamReconstructionFilter (Joseph pair)."""
     p = np.ascontiguousarray(proj_data, dtype=np.float64)
     w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
     x = np.array(x0, dtype=np.float64, copy=True, order="C")
-    lib().orc_regularized_cg(g._g, C.byref(vol), C.byref(proj), _d(p), _d(w), _d(x), int(main_iterations),
+    m = None if mask is None else np.ascontiguousarray(mask, dtype=np.float64)
+    lib().orc_regularized_cg(g._g, C.byref(vol), C.byref(proj), _d(p), _d(w), _d(m), _d(x), int(main_iterations),
                              int(cg_iterations), float(tikhonov), float(gamma), int(positivity), int(tv),
                              float(gamma_tv), int(tv_iterations), _dims(tv_dims), int(soft_threshold),
                              float(soft_threshold_value), threads or nthreads())
@@ -402,12 +403,15 @@ def raw_to_attenuation(raw, i0=65535.0, idark=0.0):
     return out
 
 
-def cg_joseph(g, vol, proj, proj_data, niter, x0=None, weights=None, tikhonov=0.0, gamma=0.0, threads=None):
+def cg_joseph(g, vol, proj, proj_data, niter, x0=None, weights=None, tikhonov=0.0, gamma=0.0, mask=None,
+              threads=None):
     p = np.ascontiguousarray(proj_data, dtype=np.float64)
     w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+    m = None if mask is None else np.ascontiguousarray(mask, dtype=np.float64)
     x = np.zeros(shape_of(vol)) if x0 is None else np.array(x0, dtype=np.float64, copy=True, order="C")
     res = np.zeros(niter + 1)
-    lib().orc_cg_joseph(g._g, C.byref(vol), C.byref(proj), _d(p), _d(w), tikhonov, gamma, niter, _d(x), _d(res),
+    lib().orc_cg_joseph(g._g, C.byref(vol), C.byref(proj), _d(p), _d(w), _d(m), tikhonov, gamma, niter, _d(x),
+                        _d(res),
                         threads or nthreads())
     return x, res
 

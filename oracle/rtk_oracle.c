@@ -1527,12 +1527,23 @@ orc_laplacian(const orc_image * vol, const double * x, double * out)
 
 static void
 cg_apply_A(const orc_geometry * g, const orc_image * vol, const orc_image * proj, const double * weights,
-           double tikhonov, double gamma, const double * x, double * out, double * ptmp, int nthreads)
+           const double * mask, double tikhonov, double gamma, const double * x_in, double * out, double * ptmp,
+           int nthreads)
 {
   /* ReconstructionConjugateGradientOperator::GenerateData,
    * include/rtkReconstructionConjugateGradientOperator.hxx:192-311:
-   * BP(W .* FP(x)), then + gamma * (-Laplacian(x)), then + tikhonov * x */
+   * BP(W .* FP(x)), then + gamma * (-Laplacian(x)), then + tikhonov * x; with a
+   * support mask M, x is M .* x_in and the result is multiplied by M */
   const long np = npix(proj), nvx = npix(vol);
+  double *   xm = NULL;
+  const double * x = x_in;
+  if (mask)
+  {
+    xm = (double *)malloc(sizeof(double) * nvx);
+    for (long q = 0; q < nvx; q++)
+      xm[q] = mask[q] * x_in[q];
+    x = xm;
+  }
   memset(ptmp, 0, sizeof(double) * np);
   orc_joseph_forward(g, vol, x, proj, ptmp, ptmp, nthreads);
   if (weights)
@@ -1551,13 +1562,23 @@ cg_apply_A(const orc_geometry * g, const orc_image * vol, const orc_image * proj
   if (tikhonov != 0.)
     for (long q = 0; q < nvx; q++)
       out[q] += tikhonov * x[q];
+  if (mask)
+  {
+    for (long q = 0; q < nvx; q++)
+      out[q] *= mask[q];
+    free(xm);
+  }
 }
 
 void
 orc_cg_joseph(const orc_geometry * g, const orc_image * vol, const orc_image * proj, const double * proj_data,
-              const double * weights, double tikhonov, double gamma, int niter, double * x, double * residuals,
-              int nthreads)
+              const double * weights, const double * mask, double tikhonov, double gamma, int niter, double * x,
+              double * residuals, int nthreads)
 {
+  /* with a support mask M (ConjugateGradientConeBeamReconstructionFilter,
+   * include/rtkConjugateGradientConeBeamReconstructionFilter.hxx:246-258): b is
+   * multiplied by M, the operator masks its input and output, and the result
+   * x is multiplied by M at the end */
   /* ConjugateGradientImageFilter::GenerateData,
    * include/rtkConjugateGradientImageFilter.hxx:108-258, with FP64
    * accumulators; b from ConjugateGradientConeBeamReconstructionFilter
@@ -1571,7 +1592,10 @@ orc_cg_joseph(const orc_geometry * g, const orc_image * vol, const orc_image * p
   for (long q = 0; q < np; q++)
     ptmp[q] = proj_data[q] * (weights ? weights[q] : 1.);
   orc_joseph_back(g, vol, b, b, proj, ptmp);
-  cg_apply_A(g, vol, proj, weights, tikhonov, gamma, x, AP, ptmp, nthreads);
+  if (mask)
+    for (long q = 0; q < nvx; q++)
+      b[q] *= mask[q];
+  cg_apply_A(g, vol, proj, weights, mask, tikhonov, gamma, x, AP, ptmp, nthreads);
   for (long q = 0; q < nvx; q++)
   {
     R[q] = b[q] - AP[q];
@@ -1585,7 +1609,7 @@ orc_cg_joseph(const orc_geometry * g, const orc_image * vol, const orc_image * p
     residuals[0] = rr;
   for (int it = 0; it < niter; it++)
   {
-    cg_apply_A(g, vol, proj, weights, tikhonov, gamma, P, AP, ptmp, nthreads);
+    cg_apply_A(g, vol, proj, weights, mask, tikhonov, gamma, P, AP, ptmp, nthreads);
     double num = 0., den = 0.;
     for (long q = 0; q < nvx; q++)
     {
@@ -1608,6 +1632,9 @@ orc_cg_joseph(const orc_geometry * g, const orc_image * vol, const orc_image * p
     if (residuals)
       residuals[it + 1] = num;
   }
+  if (mask)
+    for (long q = 0; q < nvx; q++)
+      x[q] *= mask[q];
   free(ptmp);
   free(b);
   free(R);
@@ -2214,7 +2241,7 @@ orc_total_variation(const orc_image * vol, const double * x)
 
 void
 orc_regularized_cg(const orc_geometry * g, const orc_image * vol, const orc_image * proj, const double * proj_data,
-                   const double * weights, double * x, int main_iterations, int cg_iterations, double tikhonov,
+                   const double * weights, const double * mask, double * x, int main_iterations, int cg_iterations, double tikhonov,
                    double gamma, int positivity, int tv, double gamma_tv, int tv_iterations, const int tv_dims[3],
                    int soft_threshold, double soft_threshold_value, int nthreads)
 {
@@ -2228,7 +2255,7 @@ orc_regularized_cg(const orc_geometry * g, const orc_image * vol, const orc_imag
   double *   t = (double *)malloc(sizeof(double) * nvx);
   for (int m = 0; m < main_iterations; m++)
   {
-    orc_cg_joseph(g, vol, proj, proj_data, weights, tikhonov, gamma, cg_iterations, x, NULL, nthreads);
+    orc_cg_joseph(g, vol, proj, proj_data, weights, mask, tikhonov, gamma, cg_iterations, x, NULL, nthreads);
     if (positivity)
       for (long i = 0; i < nvx; i++)
         if (x[i] < 0.)

@@ -122,8 +122,8 @@ void orc_ramp_filter(const orc_image * proj, const orc_ramp_params * p, const do
  * Runs niter iterations from x (in/out).  residuals[k] = ||r_k||^2 for
  * k = 0..niter (may be NULL).  weights may be NULL (all ones). */
 void orc_cg_joseph(const orc_geometry * g, const orc_image * vol, const orc_image * proj, const double * proj_data,
-                   const double * weights, double tikhonov, double gamma, int niter, double * x, double * residuals,
-                   int nthreads);
+                   const double * weights, const double * mask, double tikhonov, double gamma, int niter, double * x,
+                   double * residuals, int nthreads);
 /* RayBoxIntersectionImageFilter with SetBoxFromImage(vol, false): per-pixel length (mm) of the ray in the box */
 void orc_ray_box(const orc_geometry * g, const orc_image * vol, const orc_image * proj, double * out, int nthreads);
 /* SARTConeBeamReconstructionFilter with the Joseph forward and voxel-based back projectors, in place on x */
@@ -146,7 +146,7 @@ double orc_total_variation(const orc_image * vol, const double * x);
 /* RegularizedConjugateGradientConeBeamReconstructionFilter with the Joseph pair (CG, positivity, TV, soft
  * threshold on the image), in place on x; weights = the CG's W or NULL */
 void orc_regularized_cg(const orc_geometry * g, const orc_image * vol, const orc_image * proj, const double * proj_data,
-                        const double * weights, double * x, int main_iterations, int cg_iterations, double tikhonov,
+                        const double * weights, const double * mask, double * x, int main_iterations, int cg_iterations, double tikhonov,
                         double gamma, int positivity, int tv, double gamma_tv, int tv_iterations, const int tv_dims[3],
                         int soft_threshold, double soft_threshold_value, int nthreads);
 /* I0EstimationProjectionFilter on n 16-bit pixels: out = I0, I0 FWHM, Imin, Imax, low bound, high bound */

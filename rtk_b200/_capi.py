@@ -169,6 +169,8 @@ SIGNATURES.update({
     "rtkb_ray_box_lengths": (C.c_int, [_G, _IM, _IM, _V, _V]),
     "rtkb_sart": (C.c_int, [_G, _IM, _IM, _V, _V, C.c_void_p, _V]),
     "rtkb_osem": (C.c_int, [_G, _IM, _IM, _V, _V, C.c_void_p, _V]),
+    "rtkb_cg_set_support_mask": (C.c_int, [C.c_void_p, _V]),
+    "rtkb_cg_finish": (C.c_int, [C.c_void_p, _V]),
     "rtkb_i0_estimation": (C.c_int, [_IM, _V, C.c_int, C.c_uint, C.c_void_p, _V]),
     "rtkb_raw_to_attenuation": (C.c_int, [_IM, _V, C.c_double, C.c_double, _V, _V]),
     "rtkb_regularized_cg": (C.c_int, [_G, _IM, _IM, _V, _V, _V, C.c_void_p, _V]),
@@ -263,7 +265,7 @@ class RegularizedCgParams(C.Structure):
                 ("gamma", C.c_double), ("positivity", C.c_int), ("tv", C.c_int), ("gamma_tv", C.c_double),
                 ("tv_iterations", C.c_int), ("tv_dimensions", C.POINTER(C.c_int)),
                 ("soft_threshold_on_image", C.c_int), ("soft_threshold", C.c_double),
-                ("disable_displaced_detector", C.c_int)]
+                ("disable_displaced_detector", C.c_int), ("support_mask", C.c_void_p)]
 
 
 class I0Estimate(C.Structure):

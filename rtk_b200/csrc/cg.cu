@@ -63,6 +63,9 @@ struct rtkb_cg
   int                      stall = 0;
   cudaGraph_t              graph_p = nullptr;
   cudaGraphExec_t          exec_p = nullptr;
+  // support mask (SetSupportMask): caller's volume, and the masked operator input
+  const float *            mask = nullptr;
+  float *                  Mx = nullptr;
 };
 
 namespace rtkb
@@ -221,6 +224,14 @@ mul_kernel(TO * __restrict__ out, const float * __restrict__ a, const float * __
 {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     st_elem(out, i, b ? a[i] * b[i] : a[i]);
+}
+
+// x = x .* m, in place
+__global__ void __launch_bounds__(256)
+mask_inplace_kernel(float * x, const float * __restrict__ m, long long n)
+{
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    x[i] = x[i] * m[i];
 }
 
 __global__ void __launch_bounds__(256)
@@ -423,18 +434,42 @@ as(float * p)
   return reinterpret_cast<S *>(p);
 }
 
+cudaError_t add_laplacian(rtkb_cg * c, const void * in, Elem ie, void * out, Elem oe, cudaStream_t st);
+
 // out = A in (uses tmp and the projector scratch); in and out have storage
 // ie and oe, tmp the plan's storage
 cudaError_t
 apply_A(rtkb_cg * c, const void * in, Elem ie, void * out, Elem oe, cudaStream_t st)
 {
+  if (c->mask)
+  {
+    // with a support mask M (FP32 plans): A x = M .* (BP(W .* FP(M .* x)) + gamma (-Laplacian(M .* x)) + tau M .* x)
+    // (ReconstructionConjugateGradientOperator, include/rtkReconstructionConjugateGradientOperator.hxx:203-262)
+    mul_kernel<float><<<grid_for(c->nvox), 256, 0, st>>>(c->Mx, static_cast<const float *>(in), c->mask, c->nvox);
+    in = c->Mx;
+    ie = Elem::F32;
+  }
   cudaError_t e = rtkb::joseph_forward_launch(c->args, in, ie, c->scratch, nullptr, c->tmp, storage(c), c->W, st);
   if (e != cudaSuccess)
     return e;
   e = rtkb::joseph_back_launch(c->args, c->tmp, storage(c), c->scratch, nullptr, out, oe,
                                c->tikhonov != 0.f ? in : nullptr, ie, c->tikhonov, st);
-  if (e != cudaSuccess || c->gamma == 0.f)
+  if (e != cudaSuccess)
     return e;
+  if (c->gamma != 0.f)
+    e = add_laplacian(c, in, ie, out, oe, st);
+  if (e == cudaSuccess && c->mask)
+  {
+    mask_inplace_kernel<<<grid_for(c->nvox), 256, 0, st>>>(static_cast<float *>(out), c->mask, c->nvox);
+    e = cudaGetLastError();
+  }
+  return e;
+}
+
+// out += gamma * (-Laplacian(in))
+cudaError_t
+add_laplacian(rtkb_cg * c, const void * in, Elem ie, void * out, Elem oe, cudaStream_t st)
+{
   // + gamma * (-Laplacian(in)) (ReconstructionConjugateGradientOperator, include/rtkReconstructionConjugateGradientOperator.hxx:294-311)
   using B = __nv_bfloat16;
   if (ie == Elem::BF16)
@@ -532,6 +567,8 @@ release(rtkb_cg * c)
   if (!c)
     return;
   drop_graphs(c);
+  if (c->Mx)
+    cudaFree(c->Mx);
   if (c->pmem)
     cudaFree(c->pmem);
   if (c->mem)
@@ -720,8 +757,14 @@ weights_and_rhs(rtkb_cg * c, const float * d_proj, const float * d_weights, int 
     mul_kernel<__nv_bfloat16><<<grid_for(c->npix), 256, 0, st>>>(as<__nv_bfloat16>(c->tmp), d_proj, c->W, c->npix);
   else
     mul_kernel<float><<<grid_for(c->npix), 256, 0, st>>>(c->tmp, d_proj, c->W, c->npix);
-  const cudaError_t e =
+  cudaError_t e =
     joseph_back_launch(c->args, c->tmp, storage(c), c->scratch, nullptr, out, oe, nullptr, Elem::F32, 0.f, st);
+  if (e == cudaSuccess && c->mask)
+  {
+    // b = M .* BP(W .* p) (ConjugateGradientConeBeamReconstructionFilter with a support mask)
+    mask_inplace_kernel<<<grid_for(c->nvox), 256, 0, st>>>(static_cast<float *>(out), c->mask, c->nvox);
+    e = cudaGetLastError();
+  }
   return e == cudaSuccess ? RTKB_OK : cuda_fail(e, "CG right-hand side");
 }
 } // namespace
@@ -835,6 +878,37 @@ extern "C" void
 rtkb_cg_destroy(rtkb_cg * c)
 {
   release(c);
+}
+
+extern "C" int
+rtkb_cg_set_support_mask(rtkb_cg * c, const float * d_mask)
+{
+  using namespace rtkb;
+  if (!c)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "null plan");
+  if (d_mask && c->bf16)
+    return fail(RTKB_ERR_UNSUPPORTED, "support masks need an FP32 plan");
+  if (d_mask && c->net)
+    return fail(RTKB_ERR_UNSUPPORTED, "support masks and the learned preconditioner do not combine");
+  if (d_mask && !c->Mx)
+    RTKB_CUDA_TRY(cudaMalloc(&c->Mx, (size_t)c->nvox * 4));
+  c->mask = d_mask;
+  drop_graphs(c); // the next start captures the masked operator
+  c->x = nullptr; // a run must start again
+  return RTKB_OK;
+}
+
+extern "C" int
+rtkb_cg_finish(rtkb_cg * c, void * stream)
+{
+  using namespace rtkb;
+  if (!c || !c->x)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "CG plan not started");
+  if (!c->mask)
+    return RTKB_OK;
+  mask_inplace_kernel<<<grid_for(c->nvox), 256, 0, static_cast<cudaStream_t>(stream)>>>(c->x, c->mask, c->nvox);
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? RTKB_OK : cuda_fail(e, "CG support mask");
 }
 
 extern "C" int

@@ -516,6 +516,11 @@ rtkb_regularized_cg(const rtkb_geometry * g, const rtkb_image_desc * vol, const 
   int       rc = rtkb_cg_create(g, vol, proj, &cp, &plan);
   if (rc != RTKB_OK)
     return rc;
+  if (prm->support_mask && (rc = rtkb_cg_set_support_mask(plan, prm->support_mask)) != RTKB_OK)
+  {
+    rtkb_cg_destroy(plan);
+    return rc;
+  }
   const size_t vb = up256((size_t)nvox * 4);
   void *       mem = nullptr;
   cudaError_t  e = scratch_malloc(&mem, vb + (prm->tv ? (size_t)6 * nvox * 4 : 0), st);
@@ -537,6 +542,8 @@ rtkb_regularized_cg(const rtkb_geometry * g, const rtkb_image_desc * vol, const 
     rc = rtkb_cg_start_rhs(plan, b, d_x, stream);
     if (rc == RTKB_OK)
       rc = rtkb_cg_iterate(plan, prm->cg_iterations, stream);
+    if (rc == RTKB_OK)
+      rc = rtkb_cg_finish(plan, stream); // the CG filter's output times the support mask
     if (rc != RTKB_OK)
       break;
     if (prm->positivity)

@@ -336,7 +336,7 @@ def _dims3(dims):
 def regularized_cg(geometry, vol_desc, proj_desc, proj, x, weights=None, main_loop_iterations=10, cg_iterations=4,
                    tikhonov=0.0, gamma=0.0, positivity=True, tv=True, gamma_tv=5e-5, tv_iterations=10,
                    tv_dimensions=(True, True, True), soft_threshold_on_image=False, soft_threshold=1e-3,
-                   displaced_detector=True, stream=None):
+                   displaced_detector=True, support_mask=None, stream=None):
     """rtk::RegularizedConjugateGradientConeBeamReconstructionFilter (Joseph
     pair; CG, positivity, TV denoising, soft threshold), in place on x."""
     from ._capi import RegularizedCgParams
@@ -353,6 +353,9 @@ def regularized_cg(geometry, vol_desc, proj_desc, proj, x, weights=None, main_lo
     p.tv_dimensions = C.cast(dims, C.POINTER(C.c_int))
     p.soft_threshold_on_image, p.soft_threshold = int(soft_threshold_on_image), float(soft_threshold)
     p.disable_displaced_detector = int(not displaced_detector)
+    if support_mask is not None:
+        _check_shape(support_mask, vol_desc, "support mask")
+        p.support_mask = _ptr(support_mask).value
     check(load().rtkb_regularized_cg(geometry.handle, C.byref(vol_desc), C.byref(proj_desc), _ptr(proj),
                                      None if weights is None else _ptr(weights), _ptr(x), C.byref(p),
                                      _stream(stream)))
@@ -449,6 +452,18 @@ class ConjugateGradient:
         check(self._lib.rtkb_cg_start(self._h, _ptr(proj), _ptr(weights) if weights is not None else None,
                                       int(displaced_detector), _ptr(x), _stream(stream)))
         return self
+
+    def set_support_mask(self, mask):
+        """ConjugateGradientConeBeamReconstructionFilter::SetSupportMask (a
+        float32 volume, kept referenced; None removes it); before start."""
+        if mask is not None:
+            _check_shape(mask, self.vol_desc, "support mask")
+        check(self._lib.rtkb_cg_set_support_mask(self._h, None if mask is None else _ptr(mask)))
+        self._mask = mask
+
+    def finish(self, stream=None):
+        """The filter's output multiplication by the support mask (no-op without one)."""
+        check(self._lib.rtkb_cg_finish(self._h, _stream(stream)))
 
     def start_rhs(self, b, x, stream=None):
         """Start CG on A x = b for a given right-hand side volume b."""

@@ -269,3 +269,31 @@ def test_cg_laplacian_regularisation_matches_oracle(rtkb, oracle):
     plain, _ = oracle.cg_joseph(go, vo, po, p, 5, tikhonov=0.3)
     assert rel_l2(plain, ref_x) > 1e-3
     assert rtkb.ops.device_status() == 0
+
+
+@pytest.mark.parametrize("kind", ["binary", "fractional"])
+def test_cg_support_mask_matches_oracle(rtkb, oracle, kind):
+    """SetSupportMask: b, the operator's input and output, and the result multiplied by the mask."""
+    import torch
+
+    n = 20
+    gl, go = pair_geometry(rtkb, oracle, [(600.0, 900.0, i * 360.0 / n, 15.0, 0.0) for i in range(n)])
+    vd, vo = pair_image(rtkb, oracle, (24, 20, 22), (6.0,) * 3)
+    pd, po = pair_image(rtkb, oracle, (48, 40, n), (4.0, 4.0, 1.0))
+    rng = np.random.default_rng(11)
+    truth = rng.uniform(0.0, 1.0, size=oracle.shape_of(vo))
+    p = oracle.joseph_forward(go, vo, truth, po).astype(np.float32).astype(np.float64)
+    mask = np.zeros(oracle.shape_of(vo))
+    mask[3:19, 2:18, 4:20] = 1.0
+    if kind == "fractional":
+        mask *= rng.uniform(0.5, 1.0, size=mask.shape)
+    mask = mask.astype(np.float32).astype(np.float64)
+    ref, _ = oracle.cg_joseph(go, vo, po, p, 4, tikhonov=5.0, gamma=2.0, mask=mask)
+    x = torch.zeros(oracle.shape_of(vo), device="cuda")
+    cg = rtkb.ops.ConjugateGradient(gl, vd, pd, tikhonov=5.0, gamma=2.0)
+    cg.set_support_mask(to_gpu(mask))
+    cg.start(to_gpu(p), x, displaced_detector=False)
+    cg.iterate(4)
+    cg.finish()
+    assert rel_l2(to_np(x), ref) < 1e-4, rel_l2(to_np(x), ref)
+    assert np.all(to_np(x)[mask == 0] == 0.0)

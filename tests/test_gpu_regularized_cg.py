@@ -116,3 +116,16 @@ def test_rtk_regularized_cg_case_1_on_gpu(rtkb, oracle):
     want = oracle.regularized_cg(g, vol, proj, pf, np.zeros(oracle.shape_of(vol)), main_iterations=2,
                                  cg_iterations=4, gamma_tv=1.0, tv_iterations=3)
     assert rel_l2(got, want) < 2e-4, rel_l2(got, want)
+
+
+def test_regularized_cg_support_mask_matches_oracle(rtkb, oracle):
+    gl, go, vd, vo, pd, po, p = _problem(rtkb, oracle, seed=6)
+    mask = np.zeros(oracle.shape_of(vo))
+    mask[2:20, 3:17, 2:22] = 1.0
+    x0 = np.zeros(oracle.shape_of(vo))
+    ref = oracle.regularized_cg(go, vo, po, p, x0, main_iterations=2, cg_iterations=3, gamma_tv=0.05, tv_iterations=3,
+                                mask=mask)
+    x = to_gpu(x0)
+    rtkb.ops.regularized_cg(gl, vd, pd, to_gpu(p), x, main_loop_iterations=2, cg_iterations=3, gamma_tv=0.05,
+                            tv_iterations=3, support_mask=to_gpu(mask))
+    assert rel_l2(to_np(x), ref) < 2e-4, rel_l2(to_np(x), ref)

@@ -65,3 +65,25 @@ def test_oracle_regularized_cg_passes_rtk_case_1():
     x1 = O.regularized_cg(g, vol, proj, p, np.zeros(O.shape_of(vol)), main_iterations=1, cg_iterations=1,
                           gamma_tv=1.0, tv_iterations=3)
     assert _quality(x1, ref)[0] > 0.05
+
+
+def test_cg_support_mask_identities():
+    """ConjugateGradientConeBeamReconstructionFilter::SetSupportMask: a mask of ones changes nothing (bit for bit); a
+    binary mask confines the solution to its support and still reduces the masked normal-equation residual."""
+    O.build()
+    n = 16
+    g = O.Geometry()
+    for i in range(n):
+        g.add_projection(600.0, 900.0, i * 360.0 / n)
+    vol = O.image((20, 18, 16), (6.0,) * 3)
+    proj = O.image((40, 32, n), (4.0, 4.0, 1.0))
+    truth = np.random.default_rng(0).uniform(0.0, 1.0, O.shape_of(vol))
+    p = O.joseph_forward(g, vol, truth, proj)
+    x, res = O.cg_joseph(g, vol, proj, p, 3)
+    x1, res1 = O.cg_joseph(g, vol, proj, p, 3, mask=np.ones(O.shape_of(vol)))
+    assert np.array_equal(x, x1) and np.array_equal(res, res1)
+    m = np.zeros(O.shape_of(vol))
+    m[3:13, 4:14, 5:15] = 1.0
+    xm, resm = O.cg_joseph(g, vol, proj, p, 3, mask=m)
+    assert np.all(xm[m == 0] == 0.0) and np.abs(xm[m == 1]).max() > 0
+    assert resm[-1] < 0.5 * resm[0]

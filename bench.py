@@ -503,6 +503,41 @@ def regularized_cg_leg(torch, rtkb, stream, main_iterations=3):
                                           "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"}}}
 
 
+def preprocess_leg(torch, rtkb, stream, reps=5):
+    """Raw 16-bit counts to line integrals for a stack the size of the
+    backprojection configuration's (720 x 768 x 1024): I0 estimation over the
+    stack, then the lookup-table conversion, against the HBM roofline (the
+    conversion moves 6 bytes per pixel: 2 in, 4 out; the estimation reads 2)."""
+    n = 720 * 768 * 1024
+    gen = torch.Generator(device="cuda").manual_seed(SEED + 4)
+    raw = torch.randint(-32768, 32768, (720, 768, 1024), device="cuda", dtype=torch.int32, generator=gen)
+    raw = raw.to(torch.int16).view(torch.uint16)
+    desc = rtkb.make_desc((1024, 768, 720))
+    out = torch.empty((720, 768, 1024), device="cuda", dtype=torch.float32)
+    est = rtkb.ops.i0_estimation(desc, raw, stream=stream)
+    rtkb.ops.raw_to_attenuation(desc, raw, est["i0"], out=out, stream=stream)
+    torch.cuda.synchronize()
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record(stream)
+    for _ in range(reps):
+        rtkb.ops.raw_to_attenuation(desc, raw, est["i0"], out=out, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_conv = e0.elapsed_time(e1) / 1e3 / reps
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        rtkb.ops.i0_estimation(desc, raw, stream=stream)  # waits for its histogram on the host
+    t_est = (time.perf_counter() - t0) / reps
+    hbm = peaks().get("hbm_gbs")
+    gbs = 6 * n / t_conv / 1e9
+    return {"workload": "720 x 768 x 1024 uniform random 16-bit counts", "i0_estimate": est["i0"],
+            "conversion_ms": t_conv * 1e3,
+            "conversion_roofline": {"bound": "hbm", "algorithmic_bytes": 6 * n, "achieved_gbs": gbs, "peak_gbs": hbm,
+                                    "frac": gbs / hbm if hbm else None,
+                                    "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+            "i0_estimation_ms_wall": t_est * 1e3}
+
+
 def cg_seconds_to_residual(torch, rtkb, stream, tol=1e-3, max_iter=300, learned_pcg=True):
     """CG configuration: 256^3 at 1 mm, 360 projections of 512x384 at 0.8 mm
     (SID 1000, SDD 1536) of 20 seeded random ellipsoids with pre-log Poisson
@@ -946,6 +981,7 @@ def main():
         line["sart"] = sart_leg(torch, rtkb, stream)
         line["osem"] = osem_leg(torch, rtkb, stream)
         line["regularized_cg"] = regularized_cg_leg(torch, rtkb, stream)
+        line["preprocess"] = preprocess_leg(torch, rtkb, stream)
         line["cg"] = cg_seconds_to_residual(torch, rtkb, stream)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:

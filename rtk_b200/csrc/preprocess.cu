@@ -16,7 +16,8 @@
 //   lut[r] = float(log(max(I0 - IDark, 1))) - float(log(double(max(float(r) - float(IDark), 1.f))))
 // (ITK's subtract, threshold-below-1 and log image filters applied to the ramp
 // 0..65535); the table is built the same way on the host and the GPU gathers
-// from it (256 KB, resident in L2): 2 bytes read and 4 written per pixel.
+// from it (the first 224 KB staged in each CTA's shared memory, the rest read
+// from L2): 2 bytes read and 4 written per pixel.
 #include "rtkb200.h"
 #include "rtkb_internal.h"
 
@@ -57,10 +58,28 @@ raw_histogram_global_kernel(const uint16_t * __restrict__ raw, long long n, int 
     atomicAdd(&hist[raw[i] >> shift], 1u);
 }
 
-// out = lut[raw], eight pixels per 16-byte load where the buffers allow it
-__global__ void __launch_bounds__(256)
+// out = lut[raw], eight pixels per 16-byte load where the buffers allow it.
+// Random 4-byte gathers from a 256 KB table in L2 move a 32-byte sector each;
+// so each CTA (one per SM) first copies the table's first kSmemLut entries
+// into shared memory and gathers from there, and only larger raw values read
+// the table in global memory.
+constexpr int kSmemLut = 57344; // 224 KB of the 227 KB a CTA may have
+
+__device__ __forceinline__ float
+lut_at(const float * __restrict__ s, const float * __restrict__ lut, unsigned r)
+{
+  return r < (unsigned)kSmemLut ? s[r] : __ldg(lut + r);
+}
+
+__global__ void __launch_bounds__(1024)
 raw_lut_kernel(const uint16_t * __restrict__ raw, long long n, const float * __restrict__ lut, float * __restrict__ out)
 {
+  extern __shared__ float4 s4[];
+  const float4 * g4 = reinterpret_cast<const float4 *>(lut);
+  for (int k = threadIdx.x; k < kSmemLut / 4; k += blockDim.x)
+    s4[k] = g4[k];
+  __syncthreads();
+  const float *   s = reinterpret_cast<const float *>(s4);
   const long long stride = (long long)gridDim.x * blockDim.x;
   const bool      vec = ((reinterpret_cast<uintptr_t>(raw) | reinterpret_cast<uintptr_t>(out)) & 15) == 0;
   const long long n8 = vec ? n / 8 : 0;
@@ -68,19 +87,19 @@ raw_lut_kernel(const uint16_t * __restrict__ raw, long long n, const float * __r
   {
     const uint4 r = reinterpret_cast<const uint4 *>(raw)[q];
     float4      a, b;
-    a.x = __ldg(lut + (r.x & 0xffffu));
-    a.y = __ldg(lut + (r.x >> 16));
-    a.z = __ldg(lut + (r.y & 0xffffu));
-    a.w = __ldg(lut + (r.y >> 16));
-    b.x = __ldg(lut + (r.z & 0xffffu));
-    b.y = __ldg(lut + (r.z >> 16));
-    b.z = __ldg(lut + (r.w & 0xffffu));
-    b.w = __ldg(lut + (r.w >> 16));
+    a.x = lut_at(s, lut, r.x & 0xffffu);
+    a.y = lut_at(s, lut, r.x >> 16);
+    a.z = lut_at(s, lut, r.y & 0xffffu);
+    a.w = lut_at(s, lut, r.y >> 16);
+    b.x = lut_at(s, lut, r.z & 0xffffu);
+    b.y = lut_at(s, lut, r.z >> 16);
+    b.z = lut_at(s, lut, r.w & 0xffffu);
+    b.w = lut_at(s, lut, r.w >> 16);
     reinterpret_cast<float4 *>(out)[2 * q] = a;
     reinterpret_cast<float4 *>(out)[2 * q + 1] = b;
   }
   for (long long i = n8 * 8 + blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += stride)
-    out[i] = __ldg(lut + raw[i]);
+    out[i] = lut_at(s, lut, raw[i]);
 }
 
 unsigned
@@ -233,8 +252,14 @@ rtkb_raw_to_attenuation(const rtkb_image_desc * desc, const unsigned short * d_r
     cudaError_t e = cudaMemcpyAsync(d_lut, lut.data(), (size_t)kLutSize * 4, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess && n > 0)
     {
-      raw_lut_kernel<<<grid_of((n + 7) / 8), 256, 0, st>>>(d_raw, n, d_lut, d_out);
-      e = cudaGetLastError();
+      const size_t smem = (size_t)kSmemLut * 4;
+      e = cudaFuncSetAttribute(raw_lut_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e == cudaSuccess)
+      {
+        const unsigned blocks = (unsigned)std::max<long long>(1, std::min<long long>((n + 8191) / 8192, 148));
+        raw_lut_kernel<<<blocks, 1024, smem, st>>>(d_raw, n, d_lut, d_out);
+        e = cudaGetLastError();
+      }
     }
     const cudaError_t fe = scratch_free(d_lut, st);
     if (e != cudaSuccess)

@@ -797,6 +797,31 @@ def profile_fdk():
     return 0
 
 
+def profile_osem():
+    """OSEM (10 projections per subset, beta 0.01) on the CG configuration's
+    problem: 256^3 at 1 mm from 360 projections of 512x384; one warm-up
+    iteration, then one iteration (36 subsets), for ncu launch lists."""
+    import torch
+
+    import rtk_b200 as rtkb
+    from tests import phantoms
+
+    rtkb.load()
+    n = 360
+    g = rtkb.geometry.circular(n, SID, SDD)
+    vd = rtkb.make_desc((256, 256, 256), (1.0, 1.0, 1.0))
+    pd = rtkb.make_desc((512, 384, n), (0.8, 0.8, 1.0))
+    ell = phantoms.random_ellipsoids(20, SEED + 2, centre_radius=60.0, axis_range=(5.0, 60.0))
+    ell[:, 15] *= 0.02
+    p = rtkb.ops.project_ellipsoids(g, pd, ell)
+    x = torch.full((256, 256, 256), 0.01, device="cuda")
+    for _ in range(2):
+        rtkb.ops.osem(g, vd, pd, p, x, niter=1, subset=10, beta=0.01, seed=1)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_osem": "256^3 <- 360 x 512x384, 10 per subset, beta 0.01, 2 x 1 iteration"}),
+          flush=True)
+
+
 def profile_tv():
     """TV denoising (BPDQ, gamma 5e-5, 3 iterations) of a uniform random 256^3
     volume, run twice: one first-iteration, two fused-iteration and one final
@@ -840,6 +865,9 @@ def main():
                          "start + 2 eager iterations, one U-Net forward on the volume, one training step on 4 x 64^3")
     ap.add_argument("--profile-fdk", action="store_true",
                     help="FDK preprocessing (weights + Hann ramp filter) of the 720 x 1024x768 stack, twice, for ncu")
+    ap.add_argument("--profile-osem", action="store_true",
+                    help="OSEM on the CG configuration's problem (10 projections per subset, beta 0.01): one warm-up "
+                         "iteration, then one iteration, for ncu launch lists")
     ap.add_argument("--profile-tv", action="store_true",
                     help="TV denoising (BPDQ) of a uniform random 256^3 volume, 3 iterations, twice, for ncu")
     ap.add_argument("--profile-case", action="store_true",
@@ -851,6 +879,8 @@ def main():
         return profile_fdk()
     if args.profile_tv:
         return profile_tv()
+    if args.profile_osem:
+        return profile_osem()
     args.warmup = max(args.warmup, 3)
     if args.profile_case:
         use_profile_case()

@@ -599,6 +599,24 @@ typedef struct rtkb_fdk_preprocess_params
 } rtkb_fdk_preprocess_params;
 int rtkb_fdk_preprocess(const rtkb_geometry * g, const rtkb_image_desc * proj, const rtkb_fdk_preprocess_params * p,
                         rtkb_image_desc * out, const float * d_in, float * d_out, void * stream);
+/* rtk::IterativeFDKConeBeamReconstructionFilter
+ * (include/rtkIterativeFDKConeBeamReconstructionFilter.hxx:171-218): d_x (x0 in,
+ * result out) += FDK(p), then niter - 1 times += FDK(lambda (p - JosephFP(x)) /
+ * raybox), where raybox is the ray length (mm) in the box from the volume's
+ * origin to origin + size x spacing (0 below 1e-5); with positivity every result
+ * is thresholded below 0.  FDK = rtkb_fdk_preprocess(fdk) then the FDK back
+ * projector.  Defaults in RTK: niter 3, lambda 0.3, no positivity, displaced
+ * detector on with padding on the truncated side, Parker short-scan weighting,
+ * ramp without truncation correction or Hann window. */
+typedef struct rtkb_iterative_fdk_params
+{
+  int                        niter;
+  double                     lambda;
+  int                        positivity;
+  rtkb_fdk_preprocess_params fdk;
+} rtkb_iterative_fdk_params;
+int rtkb_iterative_fdk(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
+                       const float * d_proj, float * d_x, const rtkb_iterative_fdk_params * params, void * stream);
 
 /* ---- phantoms ----
  * Analytic line integrals of ellipsoids (rtk::ProjectGeometricPhantomImageFilter

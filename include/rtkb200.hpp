@@ -332,6 +332,38 @@ private:
   std::vector<int> m_Order;
 };
 
+/* rtk::IterativeFDKConeBeamReconstructionFilter (RTK's defaults), in place on the volume output buffer */
+class IterativeFDKConeBeamReconstructionFilter : public ProjectorBase
+{
+public:
+  IterativeFDKConeBeamReconstructionFilter()
+  {
+    m_P = {};
+    m_P.niter = 3;
+    m_P.lambda = 0.3;
+    m_P.fdk.displaced_detector = 1;
+    m_P.fdk.pad_on_truncated_side = 1;
+    m_P.fdk.short_scan = 1;
+    m_P.fdk.angular_gap_threshold = 3.14159265358979323846 / 9.;
+    m_P.fdk.ramp = { 0., 0., 0., 0., 0., 0., 2, 2 }; // no window, no truncation correction; powers of 2, zero pad x2
+  }
+  void SetNumberOfIterations(int n) { m_P.niter = n; }
+  void SetLambda(double l) { m_P.lambda = l; }
+  void SetEnforcePositivity(bool b) { m_P.positivity = b ? 1 : 0; }
+  void SetDisableDisplacedDetectorFilter(bool d) { m_P.fdk.displaced_detector = d ? 0 : 1; }
+  void SetTruncationCorrection(double t) { m_P.fdk.ramp.truncation_correction = t; }
+  void SetHannCutFrequency(double h) { m_P.fdk.ramp.hann_cut = h; }
+  void
+  Update()
+  {
+    Check(rtkb_iterative_fdk(m_Geometry, &m_Vol, &m_Proj, m_ProjIn, m_VolOut, &m_P, m_Stream),
+          "IterativeFDKConeBeamReconstructionFilter");
+  }
+
+private:
+  rtkb_iterative_fdk_params m_P;
+};
+
 /* rtk::RegularizedConjugateGradientConeBeamReconstructionFilter (RTK's defaults; no wavelets step),
  * in place on the volume output buffer; Update() waits for the stream */
 class RegularizedConjugateGradientConeBeamReconstructionFilter : public ProjectorBase

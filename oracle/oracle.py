@@ -98,6 +98,7 @@ def lib():
             "orc_sart": (None, [G, IM, IM, D, D, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_double,
                                 C.POINTER(C.c_int), C.c_int]),
             "orc_de_pierro": (None, [IM, D, D, D, C.c_double, D]),
+            "orc_ray_box_corners": (None, [G, IM, D, D, D, C.c_int]),
             "orc_i0_estimation": (None, [C.POINTER(C.c_ushort), C.c_long, C.c_int, C.c_uint, D]),
             "orc_raw_to_attenuation": (None, [C.POINTER(C.c_ushort), C.c_long, C.c_double, C.c_double, C.POINTER(C.c_float)]),
             "orc_geometry_set_radius_cylindrical": (None, [G, C.c_double]),
@@ -401,6 +402,52 @@ def raw_to_attenuation(raw, i0=65535.0, idark=0.0):
     lib().orc_raw_to_attenuation(r.ctypes.data_as(C.POINTER(C.c_ushort)), r.size, float(i0), float(idark),
                                  out.ctypes.data_as(C.POINTER(C.c_float)))
     return out
+
+
+def ray_box_corners(g, proj, bmin, bmax, threads=None):
+    """RayBoxIntersectionImageFilter with SetBoxMin / SetBoxMax."""
+    out = np.empty(shape_of(proj))
+    lo = np.ascontiguousarray(bmin, dtype=np.float64)
+    hi = np.ascontiguousarray(bmax, dtype=np.float64)
+    lib().orc_ray_box_corners(g._g, C.byref(proj), _d(lo), _d(hi), _d(out), threads or nthreads())
+    return out
+
+
+def iterative_fdk(g, vol, proj, proj_data, x0, niter=3, lam=0.3, positivity=False, ramp=None, displaced=True,
+                  short_scan=True, threshold=np.pi / 9):
+    """IterativeFDKConeBeamReconstructionFilter::GenerateData
+    (include/rtkIterativeFDKConeBeamReconstructionFilter.hxx:171-218), composed from the oracle's
+    filters: x += FDK(p), then niter - 1 times x += FDK(lambda (p - JosephFP(x)) / raybox) with the
+    ray box from the volume's origin to origin + size x spacing (0 below 1e-5); FDK = displaced
+    detector (padded on the truncated side), Parker, FDK weights, ramp, FDK back projection."""
+    params = ramp or ramp_params()
+
+    def fdk(q):
+        qo = proj
+        if displaced:
+            q, i0, s0 = displaced_detector(g, proj, q)
+            qo = image((s0, proj.size[1], proj.size[2]), tuple(proj.spacing), origin=tuple(proj.origin),
+                       index=(i0, proj.index[1], proj.index[2]), direction=np.asarray(proj.direction).reshape(3, 3))
+        if short_scan:
+            q, _ = parker_weight(g, qo, q, threshold)
+        q = fdk_weight(g, qo, q)
+        q = ramp_filter(qo, q, params)
+        return backproject(g, vol, qo, q, fdk=True)
+
+    p = np.ascontiguousarray(proj_data, dtype=np.float64)
+    origin = np.asarray(vol.origin)
+    rb = ray_box_corners(g, proj, origin, origin + np.asarray(vol.size) * np.asarray(vol.spacing))
+    x = np.array(x0, dtype=np.float64, copy=True) + fdk(p)
+    if positivity:
+        x = np.maximum(x, 0.0)
+    for _ in range(1, niter):
+        fp = joseph_forward(g, vol, x, proj)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            e = np.where(rb < 1e-5, 0.0, lam * (p - fp) / rb)
+        x = x + fdk(e)
+        if positivity:
+            x = np.maximum(x, 0.0)
+    return x
 
 
 def cg_joseph(g, vol, proj, proj_data, niter, x0=None, weights=None, tikhonov=0.0, gamma=0.0, mask=None,

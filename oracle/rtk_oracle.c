@@ -1842,38 +1842,11 @@ orc_fdk_backproject_f32_rtk(const orc_geometry * g, const orc_image * vol, const
 /* ------------------------------------------------------------------------ */
 /* SART: SARTConeBeamReconstructionFilter (include/rtkSARTConeBeamReconstructionFilter.hxx) */
 
-void
-orc_ray_box(const orc_geometry * g, const orc_image * vol, const orc_image * proj, double * out, int nthreads)
+static void
+ray_box_impl(const orc_geometry * g, const orc_image * proj, const double * D, const double * mn, const double * mx,
+             double * out, int nthreads)
 {
-  /* RayBoxIntersectionImageFilter: RayConvexIntersectionImageFilter
-   * (include/rtkRayConvexIntersectionImageFilter.hxx:57-84) with density 1
-   * and the BoxShape of BoxShape::SetBoxFromImage(volume, false)
-   * (src/rtkBoxShape.cxx:141-160: from the origin to origin + D (spacing x
-   * (size - 1))), intersected as BoxShape::IsIntersectedByRay
-   * (src/rtkBoxShape.cxx:47-97) along the normalised source-to-pixel
-   * direction: out = supDist - infDist in mm, 0 without intersection. */
   const int nu = proj->size[0], nv = proj->size[1], np = proj->size[2];
-  const double * D = vol->direction;
-  double         bmin[3], bmax[3], ext[3];
-  for (int a = 0; a < 3; a++)
-    ext[a] = vol->spacing[a] * (vol->size[a] - 1);
-  for (int r = 0; r < 3; r++)
-  {
-    bmin[r] = vol->origin[r];
-    bmax[r] = vol->origin[r] + D[3 * r + 0] * ext[0] + D[3 * r + 1] * ext[1] + D[3 * r + 2] * ext[2];
-  }
-  double mn[3], mx[3];
-  for (int a = 0; a < 3; a++) /* D^T applied to the corners */
-  {
-    mn[a] = D[0 * 3 + a] * bmin[0] + D[1 * 3 + a] * bmin[1] + D[2 * 3 + a] * bmin[2];
-    mx[a] = D[0 * 3 + a] * bmax[0] + D[1 * 3 + a] * bmax[1] + D[2 * 3 + a] * bmax[2];
-    if (mn[a] > mx[a])
-    {
-      const double t = mn[a];
-      mn[a] = mx[a];
-      mx[a] = t;
-    }
-  }
   double pi2pp[16];
   orc_index_to_physical(proj, pi2pp);
   for (int s = 0; s < np; s++)
@@ -1923,6 +1896,55 @@ orc_ray_box(const orc_geometry * g, const orc_image * vol, const orc_image * pro
         out[((long)s * nv + j) * nu + i] = hit ? sup - inf : 0.;
       }
   }
+}
+
+void
+orc_ray_box(const orc_geometry * g, const orc_image * vol, const orc_image * proj, double * out, int nthreads)
+{
+  /* RayBoxIntersectionImageFilter: RayConvexIntersectionImageFilter
+   * (include/rtkRayConvexIntersectionImageFilter.hxx:57-84) with density 1
+   * and the BoxShape of BoxShape::SetBoxFromImage(volume, false)
+   * (src/rtkBoxShape.cxx:141-160: from the origin to origin + D (spacing x
+   * (size - 1))), intersected as BoxShape::IsIntersectedByRay
+   * (src/rtkBoxShape.cxx:47-97) along the normalised source-to-pixel
+   * direction: out = supDist - infDist in mm, 0 without intersection. */
+  const double * D = vol->direction;
+  double         bmin[3], bmax[3], ext[3];
+  for (int a = 0; a < 3; a++)
+    ext[a] = vol->spacing[a] * (vol->size[a] - 1);
+  for (int r = 0; r < 3; r++)
+  {
+    bmin[r] = vol->origin[r];
+    bmax[r] = vol->origin[r] + D[3 * r + 0] * ext[0] + D[3 * r + 1] * ext[1] + D[3 * r + 2] * ext[2];
+  }
+  double mn[3], mx[3];
+  for (int a = 0; a < 3; a++) /* D^T applied to the corners */
+  {
+    mn[a] = D[0 * 3 + a] * bmin[0] + D[1 * 3 + a] * bmin[1] + D[2 * 3 + a] * bmin[2];
+    mx[a] = D[0 * 3 + a] * bmax[0] + D[1 * 3 + a] * bmax[1] + D[2 * 3 + a] * bmax[2];
+    if (mn[a] > mx[a])
+    {
+      const double t = mn[a];
+      mn[a] = mx[a];
+      mx[a] = t;
+    }
+  }
+  ray_box_impl(g, proj, D, mn, mx, out, nthreads);
+}
+
+void
+orc_ray_box_corners(const orc_geometry * g, const orc_image * proj, const double * bmin, const double * bmax,
+                    double * out, int nthreads)
+{
+  /* RayBoxIntersectionImageFilter with SetBoxMin / SetBoxMax (identity direction) */
+  static const double I[9] = { 1., 0., 0., 0., 1., 0., 0., 0., 1. };
+  double              mn[3], mx[3];
+  for (int a = 0; a < 3; a++)
+  {
+    mn[a] = bmin[a] < bmax[a] ? bmin[a] : bmax[a];
+    mx[a] = bmin[a] < bmax[a] ? bmax[a] : bmin[a];
+  }
+  ray_box_impl(g, proj, I, mn, mx, out, nthreads);
 }
 
 void

@@ -126,6 +126,9 @@ void orc_cg_joseph(const orc_geometry * g, const orc_image * vol, const orc_imag
                    double * residuals, int nthreads);
 /* RayBoxIntersectionImageFilter with SetBoxFromImage(vol, false): per-pixel length (mm) of the ray in the box */
 void orc_ray_box(const orc_geometry * g, const orc_image * vol, const orc_image * proj, double * out, int nthreads);
+/* the same for the box between two corners (SetBoxMin / SetBoxMax) */
+void orc_ray_box_corners(const orc_geometry * g, const orc_image * proj, const double * bmin, const double * bmax,
+                         double * out, int nthreads);
 /* SARTConeBeamReconstructionFilter with the Joseph forward and voxel-based back projectors, in place on x */
 void orc_sart(const orc_geometry * g, const orc_image * vol, const orc_image * proj, const double * proj_data, double * x,
               int niter, double lambda, int positivity, int projections_per_subset, int displaced_detector,

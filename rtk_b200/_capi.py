@@ -169,6 +169,7 @@ SIGNATURES.update({
     "rtkb_ray_box_lengths": (C.c_int, [_G, _IM, _IM, _V, _V]),
     "rtkb_sart": (C.c_int, [_G, _IM, _IM, _V, _V, C.c_void_p, _V]),
     "rtkb_osem": (C.c_int, [_G, _IM, _IM, _V, _V, C.c_void_p, _V]),
+    "rtkb_iterative_fdk": (C.c_int, [_G, _IM, _IM, _V, _V, C.c_void_p, _V]),
     "rtkb_cg_set_support_mask": (C.c_int, [C.c_void_p, _V]),
     "rtkb_cg_finish": (C.c_int, [C.c_void_p, _V]),
     "rtkb_i0_estimation": (C.c_int, [_IM, _V, C.c_int, C.c_uint, C.c_void_p, _V]),
@@ -273,3 +274,9 @@ class I0Estimate(C.Structure):
 
     _fields_ = [("i0", C.c_double), ("i0_fwhm", C.c_double), ("imin", C.c_double), ("imax", C.c_double),
                 ("low_bound", C.c_double), ("high_bound", C.c_double)]
+
+
+class IterativeFdkParams(C.Structure):
+    """rtkb_iterative_fdk_params."""
+
+    _fields_ = [("niter", C.c_int), ("lam", C.c_double), ("positivity", C.c_int), ("fdk", FdkPreprocessParams)]

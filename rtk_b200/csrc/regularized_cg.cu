@@ -369,7 +369,7 @@ flat_grid(long long n)
   return (unsigned)std::min<long long>((n + 255) / 256, 148LL * 16);
 }
 
-bool
+void
 tv_dims(const rtkb_image_desc & v, const int * dims, TvDims & t, double & min_spacing)
 {
   t.nd = 0;
@@ -385,7 +385,6 @@ tv_dims(const rtkb_image_desc & v, const int * dims, TvDims & t, double & min_sp
       min_spacing = std::min(min_spacing, v.spacing[d]);
     }
   }
-  return true;
 }
 
 // BPDQ TV denoising of f into out (out may equal f); Z: two buffers of three

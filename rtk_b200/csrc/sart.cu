@@ -114,6 +114,15 @@ sart_update_kernel(float * __restrict__ x, const float * __restrict__ B, const f
   }
 }
 
+// ThresholdBelow(0) with outside value 0
+__global__ void __launch_bounds__(256)
+positivity_kernel(float * __restrict__ x, long long n)
+{
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    if (x[i] < 0.f)
+      x[i] = 0.f;
+}
+
 __global__ void __launch_bounds__(256)
 fill_value_kernel(float * __restrict__ out, float v, long long n)
 {
@@ -130,7 +139,7 @@ grid_of(long long n)
 
 int
 ray_box_lengths(const rtkb_geometry * g, const rtkb_image_desc & vol, const rtkb_image_desc & proj, float * d_out,
-                cudaStream_t st)
+                cudaStream_t st, const double * corners = nullptr)
 {
   using namespace rtkb;
   if (g->g.radius_cylindrical != 0.)
@@ -150,10 +159,22 @@ ray_box_lengths(const rtkb_geometry * g, const rtkb_image_desc & vol, const rtkb
     tab[s].src[2] = src[2];
     tab[s].pad = 0.;
   }
-  Box          b;
+  Box b;
+  if (corners)
+  {
+    // SetBoxMin / SetBoxMax: identity direction, the two corners ordered
+    const double I[9] = { 1., 0., 0., 0., 1., 0., 0., 0., 1. };
+    std::memcpy(b.D, I, sizeof(b.D));
+    for (int a = 0; a < 3; a++)
+    {
+      b.mn[a] = std::min(corners[a], corners[3 + a]);
+      b.mx[a] = std::max(corners[a], corners[3 + a]);
+    }
+  }
   const double * D = vol.direction;
   double       ext[3], bmin[3], bmax[3];
-  std::memcpy(b.D, D, sizeof(b.D));
+  if (!corners)
+    std::memcpy(b.D, D, sizeof(b.D));
   for (int a = 0; a < 3; a++)
     ext[a] = vol.spacing[a] * (vol.size[a] - 1);
   for (int r = 0; r < 3; r++)
@@ -161,7 +182,7 @@ ray_box_lengths(const rtkb_geometry * g, const rtkb_image_desc & vol, const rtkb
     bmin[r] = vol.origin[r];
     bmax[r] = vol.origin[r] + D[3 * r + 0] * ext[0] + D[3 * r + 1] * ext[1] + D[3 * r + 2] * ext[2];
   }
-  for (int a = 0; a < 3; a++)
+  for (int a = 0; a < 3 && !corners; a++)
   {
     b.mn[a] = D[0 * 3 + a] * bmin[0] + D[1 * 3 + a] * bmin[1] + D[2 * 3 + a] * bmin[2];
     b.mx[a] = D[0 * 3 + a] * bmax[0] + D[1 * 3 + a] * bmax[1] + D[2 * 3 + a] * bmax[2];
@@ -344,6 +365,102 @@ rtkb_sart(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image
       }
     }
     cudaError_t fe = rtkb::scratch_free(mem, st);
+    if (rc == RTKB_OK && fe != cudaSuccess)
+      rc = cuda_fail(fe, "cudaFreeAsync");
+    return rc;
+  }
+  catch (...)
+  {
+    return fail(RTKB_ERR_OUT_OF_MEMORY, "host allocation failed");
+  }
+}
+
+extern "C" int
+rtkb_iterative_fdk(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
+                   const float * d_proj, float * d_x, const rtkb_iterative_fdk_params * prm, void * stream)
+{
+  // IterativeFDKConeBeamReconstructionFilter::GenerateData
+  // (include/rtkIterativeFDKConeBeamReconstructionFilter.hxx:171-218):
+  // x += FDK(p); then niter - 1 times x += FDK(lambda (p - JosephFP(x)) / raybox)
+  // (DivideOrZeroOut below 1e-5, the box from the volume's origin to origin +
+  // size x spacing), each result thresholded below 0 with positivity.  FDK is
+  // the displaced-detector, Parker, weighting and ramp chain, then the FDK
+  // back projector, adding to x.
+  using namespace rtkb;
+  std::string why;
+  if (!g || !vol || !proj || !d_proj || !d_x || !prm)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "null argument");
+  if (!desc_valid(vol, why) || !desc_valid(proj, why))
+    return fail(RTKB_ERR_INVALID_ARGUMENT, why);
+  if (prm->niter < 1 || !std::isfinite(prm->lambda))
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "invalid iterative FDK parameters");
+  if (proj->index[2] < 0 || (long long)proj->index[2] + proj->size[2] > (long long)g->g.p.size())
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "Mismatch between the number of projections and the geometry entries.");
+  try
+  {
+    cudaStream_t    st = static_cast<cudaStream_t>(stream);
+    rtkb_image_desc cd = *proj; // the filtered stack (padded on the truncated side when the detector is displaced)
+    int             rc = RTKB_OK;
+    if (prm->fdk.displaced_detector)
+    {
+      int weighted = 0;
+      rc = rtkb_displaced_detector_region(g, proj, prm->fdk.pad_on_truncated_side, &cd, &weighted);
+      if (rc != RTKB_OK)
+        return rc;
+    }
+    const long long n = num_pixels(*proj), nc = num_pixels(cd), nvox = num_pixels(*vol);
+    const size_t    pb = ((size_t)n * 4 + 255) & ~size_t(255), cb = ((size_t)nc * 4 + 255) & ~size_t(255);
+    void *          mem = nullptr;
+    RTKB_CUDA_TRY(rtkb::scratch_malloc(&mem, 3 * pb + cb, st));
+    char *  m = static_cast<char *>(mem);
+    float * rb = reinterpret_cast<float *>(m);
+    float * fp = reinterpret_cast<float *>(m + pb);
+    float * e = reinterpret_cast<float *>(m + 2 * pb);
+    float * c = reinterpret_cast<float *>(m + 3 * pb);
+    double  corners[6];
+    for (int a = 0; a < 3; a++)
+    {
+      corners[a] = vol->origin[a];
+      corners[3 + a] = vol->origin[a] + vol->size[a] * vol->spacing[a];
+    }
+    auto fdk_add = [&](const float * stack) {
+      rtkb_image_desc od{};
+      int             r = rtkb_fdk_preprocess(g, proj, &prm->fdk, &od, stack, c, stream);
+      if (r == RTKB_OK)
+        r = rtkb_fdk_backproject(g, vol, &od, c, d_x, d_x, stream);
+      if (r == RTKB_OK && prm->positivity)
+      {
+        positivity_kernel<<<grid_of(nvox), 256, 0, st>>>(d_x, nvox);
+        const cudaError_t ce = cudaGetLastError();
+        if (ce != cudaSuccess)
+          r = cuda_fail(ce, "positivity");
+      }
+      return r;
+    };
+    if (prm->niter > 1)
+      rc = ray_box_lengths(g, *vol, *proj, rb, st, corners);
+    if (rc == RTKB_OK)
+      rc = fdk_add(d_proj);
+    for (int it = 1; it < prm->niter && rc == RTKB_OK; it++)
+    {
+      cudaError_t ce = cudaMemsetAsync(fp, 0, (size_t)n * 4, st);
+      if (ce != cudaSuccess)
+      {
+        rc = cuda_fail(ce, "cudaMemsetAsync");
+        break;
+      }
+      rc = rtkb_joseph_forward_project(g, vol, proj, d_x, fp, fp, stream);
+      if (rc != RTKB_OK)
+        break;
+      sart_error_kernel<<<grid_of(n), 256, 0, st>>>(d_proj, fp, rb, e, n, (float)prm->lambda, 1e-5f);
+      if ((ce = cudaGetLastError()) != cudaSuccess)
+      {
+        rc = cuda_fail(ce, "iterative FDK correction");
+        break;
+      }
+      rc = fdk_add(e);
+    }
+    const cudaError_t fe = rtkb::scratch_free(mem, st);
     if (rc == RTKB_OK && fe != cudaSuccess)
       rc = cuda_fail(fe, "cudaFreeAsync");
     return rc;

@@ -414,6 +414,24 @@ def raw_to_attenuation(desc, raw, i0=65535.0, idark=0.0, out=None, stream=None):
     return out
 
 
+def iterative_fdk(geometry, vol_desc, proj_desc, proj, x, niter=3, lam=0.3, positivity=False, ramp=None,
+                  displaced=True, pad=True, short_scan=True, threshold=3.141592653589793 / 9, stream=None):
+    """rtk::IterativeFDKConeBeamReconstructionFilter (Joseph forward projection),
+    in place on x (x0 in, result out)."""
+    from ._capi import IterativeFdkParams
+
+    _check_shape(proj, proj_desc, "projections")
+    _check_shape(x, vol_desc, "volume")
+    p = IterativeFdkParams()
+    p.niter, p.lam, p.positivity = int(niter), float(lam), int(positivity)
+    p.fdk.displaced_detector, p.fdk.pad_on_truncated_side, p.fdk.short_scan = int(displaced), int(pad), int(short_scan)
+    p.fdk.angular_gap_threshold = threshold
+    p.fdk.ramp = ramp or ramp_params()
+    check(load().rtkb_iterative_fdk(geometry.handle, C.byref(vol_desc), C.byref(proj_desc), _ptr(proj), _ptr(x),
+                                    C.byref(p), _stream(stream)))
+    return x
+
+
 def _storage_code(storage):
     codes = {"fp32": 0, "bf16": 1}
     if storage not in codes:

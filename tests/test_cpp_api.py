@@ -63,6 +63,18 @@ int main(int, char ** argv)
     f.SetProjections(rtkb::MakeImageDescription(ps, sp, o), nullptr);
     f.Update();
   }, "null argument");
+  bad += expect_throw("iterative fdk without buffers", [] {
+    rtkb::ThreeDCircularProjectionGeometry h;
+    h.AddProjection(1000., 1500., 0.);
+    const int sz[3] = { 8, 8, 8 }, ps[3] = { 8, 8, 1 };
+    const double sp[3] = { 1., 1., 1. }, o[3] = { 0., 0., 0. };
+    rtkb::IterativeFDKConeBeamReconstructionFilter f;
+    f.SetGeometry(h);
+    f.SetHannCutFrequency(0.5);
+    f.SetVolume(rtkb::MakeImageDescription(sz, sp, o), nullptr, nullptr);
+    f.SetProjections(rtkb::MakeImageDescription(ps, sp, o), nullptr);
+    f.Update();
+  }, "null argument");
   bad += expect_throw("mixed geometry", [] {
     rtkb::ThreeDCircularProjectionGeometry h;
     h.AddProjection(1000., 1500., 0.);

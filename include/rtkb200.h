@@ -262,6 +262,12 @@ int rtkb_i0_estimation(const rtkb_image_desc * desc, const unsigned short * d_ra
  * the same size as d_raw. */
 int rtkb_raw_to_attenuation(const rtkb_image_desc * desc, const unsigned short * d_raw, double i0, double idark,
                             float * d_out, void * stream);
+/* rtk::WaterPrecorrectionImageFilter (include/rtkWaterPrecorrectionImageFilter.hxx):
+ * d_out = c0 + c1 v + c2 v^2 + ... of the line integrals v (at most 16
+ * coefficients; RTK's default (0, 1) and a single 0 pass v through).  d_out may
+ * equal d_in. */
+int rtkb_water_precorrection(const rtkb_image_desc * desc, const float * d_in, float * d_out,
+                             const double * coefficients, int n_coefficients, void * stream);
 
 /* ---- Joseph projector pair ----
  * rtk::JosephForwardProjectionImageFilter

@@ -450,6 +450,27 @@ def iterative_fdk(g, vol, proj, proj_data, x0, niter=3, lam=0.3, positivity=Fals
     return x
 
 
+def water_precorrection(data, coefficients):
+    """WaterPrecorrectionImageFilter::DynamicThreadedGenerateData
+    (include/rtkWaterPrecorrectionImageFilter.hxx:14-62) on float32 data: with at least 3
+    coefficients out = float(c0 + c1 v), then out = float(out + c_j v^j) with v^j in float; with
+    two (not the identity) float(c0 + c1 v); one non-zero: c0; otherwise the input (in place)."""
+    v = np.asarray(data, dtype=np.float32)
+    c = [float(x) for x in coefficients]
+    if len(c) >= 3:
+        out = (c[0] + c[1] * v.astype(np.float64)).astype(np.float32)
+        bpow = (v * v).astype(np.float32)
+        for cj in c[2:]:
+            out = (out.astype(np.float64) + cj * bpow.astype(np.float64)).astype(np.float32)
+            bpow = (bpow * v).astype(np.float32)
+        return out
+    if len(c) == 2 and (c[0] != 0.0 or c[1] != 1.0):
+        return (c[0] + c[1] * v.astype(np.float64)).astype(np.float32)
+    if len(c) == 1 and c[0] != 0.0:
+        return np.full(v.shape, np.float32(c[0]))
+    return v.copy()
+
+
 def cg_joseph(g, vol, proj, proj_data, niter, x0=None, weights=None, tikhonov=0.0, gamma=0.0, mask=None,
               threads=None):
     p = np.ascontiguousarray(proj_data, dtype=np.float64)

@@ -169,6 +169,7 @@ SIGNATURES.update({
     "rtkb_ray_box_lengths": (C.c_int, [_G, _IM, _IM, _V, _V]),
     "rtkb_sart": (C.c_int, [_G, _IM, _IM, _V, _V, C.c_void_p, _V]),
     "rtkb_osem": (C.c_int, [_G, _IM, _IM, _V, _V, C.c_void_p, _V]),
+    "rtkb_water_precorrection": (C.c_int, [_IM, _V, _V, C.POINTER(C.c_double), C.c_int, _V]),
     "rtkb_iterative_fdk": (C.c_int, [_G, _IM, _IM, _V, _V, C.c_void_p, _V]),
     "rtkb_cg_set_support_mask": (C.c_int, [C.c_void_p, _V]),
     "rtkb_cg_finish": (C.c_int, [C.c_void_p, _V]),

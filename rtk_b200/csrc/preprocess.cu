@@ -102,6 +102,42 @@ raw_lut_kernel(const uint16_t * __restrict__ raw, long long n, const float * __r
     out[i] = lut_at(s, lut, raw[i]);
 }
 
+// Water precorrection with at least 3 coefficients, in RTK's arithmetic: the
+// products of the double coefficients and the float powers in double, the
+// running sum rounded to float after each term, powers of v in float.  No
+// fused multiply-adds, as an x86 build of the filter computes it.
+constexpr int kMaxWaterCoefficients = 16;
+struct WaterCoeffs
+{
+  double c[kMaxWaterCoefficients];
+  int    n;
+};
+
+__global__ void __launch_bounds__(256)
+water_precorrection_kernel(const float * in, float * out, long long n, WaterCoeffs k)
+{
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+  {
+    const float v = in[i];
+    float       o = (float)__dadd_rn(k.c[0], __dmul_rn(k.c[1], (double)v));
+    float       bpow = __fmul_rn(v, v);
+    for (int j = 2; j < k.n; j++)
+    {
+      o = (float)__dadd_rn((double)o, __dmul_rn(k.c[j], (double)bpow));
+      bpow = __fmul_rn(bpow, v);
+    }
+    out[i] = o;
+  }
+}
+
+// two coefficients (not the identity): out = float(c0 + c1 v); one non-zero coefficient: out = c0
+__global__ void __launch_bounds__(256)
+water_affine_kernel(const float * in, float * out, long long n, double c0, double c1, bool constant)
+{
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = constant ? (float)c0 : (float)__dadd_rn(c0, __dmul_rn(c1, (double)in[i]));
+}
+
 unsigned
 grid_of(long long n)
 {
@@ -270,4 +306,48 @@ rtkb_raw_to_attenuation(const rtkb_image_desc * desc, const unsigned short * d_r
   {
     return fail(RTKB_ERR_OUT_OF_MEMORY, "host allocation failed");
   }
+}
+
+extern "C" int
+rtkb_water_precorrection(const rtkb_image_desc * desc, const float * d_in, float * d_out, const double * coefficients,
+                         int n_coefficients, void * stream)
+{
+  // WaterPrecorrectionImageFilter::DynamicThreadedGenerateData
+  // (include/rtkWaterPrecorrectionImageFilter.hxx:14-62), an in-place filter:
+  // the cases it leaves untouched (no coefficients, the identity (0, 1), a
+  // single zero) pass the input through.
+  using namespace rtkb;
+  std::string why;
+  if (!desc || !d_in || !d_out || (n_coefficients > 0 && !coefficients))
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "null argument");
+  if (!desc_valid(desc, why))
+    return fail(RTKB_ERR_INVALID_ARGUMENT, why);
+  if (n_coefficients < 0 || n_coefficients > kMaxWaterCoefficients)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "water precorrection takes at most 16 coefficients");
+  cudaStream_t    st = static_cast<cudaStream_t>(stream);
+  const long long n = num_pixels(*desc);
+  const double *  c = coefficients;
+  cudaError_t     e = cudaSuccess;
+  if (n_coefficients >= 3)
+  {
+    WaterCoeffs k{};
+    for (int j = 0; j < n_coefficients; j++)
+      k.c[j] = c[j];
+    k.n = n_coefficients;
+    water_precorrection_kernel<<<grid_of(n), 256, 0, st>>>(d_in, d_out, n, k);
+    e = cudaGetLastError();
+  }
+  else if (n_coefficients == 2 && (c[0] != 0. || c[1] != 1.))
+  {
+    water_affine_kernel<<<grid_of(n), 256, 0, st>>>(d_in, d_out, n, c[0], c[1], false);
+    e = cudaGetLastError();
+  }
+  else if (n_coefficients == 1 && c[0] != 0.)
+  {
+    water_affine_kernel<<<grid_of(n), 256, 0, st>>>(d_in, d_out, n, c[0], 0., true);
+    e = cudaGetLastError();
+  }
+  else if (d_out != d_in)
+    e = cudaMemcpyAsync(d_out, d_in, (size_t)n * 4, cudaMemcpyDeviceToDevice, st);
+  return e == cudaSuccess ? RTKB_OK : cuda_fail(e, "water precorrection");
 }

@@ -432,6 +432,18 @@ def iterative_fdk(geometry, vol_desc, proj_desc, proj, x, niter=3, lam=0.3, posi
     return x
 
 
+def water_precorrection(desc, proj, coefficients, out=None, stream=None):
+    """rtk::WaterPrecorrectionImageFilter: out = sum_j c_j proj^j (out may be proj)."""
+    _check_shape(proj, desc, "projections")
+    if out is None:
+        out = _torch().empty_like(proj)
+    _check_shape(out, desc, "output")
+    c = (C.c_double * max(1, len(coefficients)))(*[float(v) for v in coefficients])
+    check(load().rtkb_water_precorrection(C.byref(desc), _ptr(proj), _ptr(out), c, len(coefficients),
+                                          _stream(stream)))
+    return out
+
+
 def _storage_code(storage):
     codes = {"fp32": 0, "bf16": 1}
     if storage not in codes:

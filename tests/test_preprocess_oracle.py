@@ -62,3 +62,17 @@ def test_i0_estimation_like_rtkI0estimationtest():
         est = O.i0_estimation(img, bit_shift=3, dyn_threshold=20)
         assert 3 * est["imax"] // 4 - 8 <= est["i0"] <= hi
         assert est["imin"] <= 3200 + 8 and est["imax"] >= hi - 16
+
+
+@pytest.mark.parametrize("c", [[2.0, 2.0], [0.05, 0.3, 2.0], [0.0687, 2.5, 0.6, -0.2, 0.1]])
+def test_water_precorrection_like_rtkwaterprecorrectiontest(c):
+    """test/rtkwaterprecorrectiontest.cxx: orders 2, 3 and 5 map a constant 1.5 to 5."""
+    out = O.water_precorrection(np.full((16, 16), 1.5, dtype=np.float32), c)
+    np.testing.assert_allclose(out, 5.0, atol=1e-4)
+
+
+def test_water_precorrection_pass_through():
+    v = np.random.default_rng(0).normal(size=(3, 5)).astype(np.float32)
+    for c in ([], [0.0, 1.0], [0.0]):
+        assert np.array_equal(O.water_precorrection(v, c), v)
+    assert np.all(O.water_precorrection(v, [2.5]) == np.float32(2.5))

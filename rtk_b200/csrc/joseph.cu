@@ -346,15 +346,22 @@ joseph_forward_kernel(JosephArgs a, const float * __restrict__ V, const float * 
 // f_n + f.  inf_fast: the first in-plane axis a is f (natural volume, a = x,
 // b = y); else a is m and b is f (transposed copy T[x][y][z], a = y, b = z).
 __global__ void __launch_bounds__(256)
-quad_kernel(const float * __restrict__ src, float4 * __restrict__ dst, int fn, int mn, long long n, bool inf_fast)
+quad_kernel(const float * __restrict__ src, float4 * __restrict__ dst, int fn, int mn, int outer, bool inf_fast)
 {
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
-  {
-    const int       f = (int)(e % fn), m = (int)((e / fn) % mn);
-    const long long df = (f + 1 < fn) ? 1 : 0, dm = (m + 1 < mn) ? fn : 0;
-    const long long da = inf_fast ? df : dm, db = inf_fast ? dm : df;
-    dst[e] = make_float4(__ldg(src + e), __ldg(src + e + db), __ldg(src + e + da), __ldg(src + e + da + db));
-  }
+  // threads along the fast axis f, blocks over rows m and planes o (striding
+  // past the grid's limits): no per-element division
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= fn)
+    return;
+  const long long df = (f + 1 < fn) ? 1 : 0;
+  for (int o = blockIdx.z; o < outer; o += gridDim.z)
+    for (int m = blockIdx.y; m < mn; m += gridDim.y)
+    {
+      const long long e = ((long long)o * mn + m) * fn + f;
+      const long long dm = (m + 1 < mn) ? fn : 0;
+      const long long da = inf_fast ? df : dm, db = inf_fast ? dm : df;
+      dst[e] = make_float4(__ldg(src + e), __ldg(src + e + db), __ldg(src + e + da), __ldg(src + e + da + db));
+    }
 }
 
 __device__ __forceinline__ void
@@ -722,9 +729,10 @@ forward_launch(const JosephArgs & a, const float * V, float * Vt, float4 * QN, f
   transpose_zx_kernel<<<tg, 256, 0, st>>>(V, Vt, nx, ny, nz);
   if (quads)
   {
-    const unsigned qg = (unsigned)std::min<long long>((nvox + 255) / 256, 148LL * 32);
-    quad_kernel<<<qg, 256, 0, st>>>(V, QN, nx, ny, nvox, true);  // a = x, b = y
-    quad_kernel<<<qg, 256, 0, st>>>(Vt, QT, nz, ny, nvox, false); // a = y, b = z
+    const dim3 qn((unsigned)((nx + 127) / 128), (unsigned)std::min(ny, 65535), (unsigned)std::min(nz, 65535));
+    const dim3 qt((unsigned)((nz + 127) / 128), (unsigned)std::min(ny, 65535), (unsigned)std::min(nx, 65535));
+    quad_kernel<<<qn, 128, 0, st>>>(V, QN, nx, ny, nz, true);  // a = x, b = y
+    quad_kernel<<<qt, 128, 0, st>>>(Vt, QT, nz, ny, nx, false); // a = y, b = z
   }
   const dim3 grid((unsigned)((a.nu + 31) / 32), (unsigned)a.np, (unsigned)((a.nv + 7) / 8));
   const bool small = nvox < (1ll << 31);

@@ -382,40 +382,47 @@ grid_for(long long n)
 // Neumann boundary, spacing-scaled): per axis, the sum over the existing
 // neighbours of (x_nb - x_i) * w_axis with w = 1 / spacing^2.
 // out = scale * Laplacian(x), or out += scale * Laplacian(x) when add.
+// Threads along x, blocks over (x tiles, y, z), striding past the grid's
+// limits: no per-voxel division.
 template <typename TI, typename TO>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(128)
 laplacian_kernel(const TI * __restrict__ x, TO * out, int nx, int ny, int nz, float wx, float wy, float wz,
                  float scale, bool add)
 {
-  const long long n = (long long)nx * ny * nz, sxy = (long long)nx * ny;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-  {
-    const int   ix = (int)(i % nx), iy = (int)((i / nx) % ny), iz = (int)(i / sxy);
-    const float c = ld_elem(x, i);
-    float       lx = 0.f, ly = 0.f, lz = 0.f;
-    if (ix + 1 < nx)
-      lx += ld_elem(x, i + 1) - c;
-    if (ix > 0)
-      lx += ld_elem(x, i - 1) - c;
-    if (iy + 1 < ny)
-      ly += ld_elem(x, i + nx) - c;
-    if (iy > 0)
-      ly += ld_elem(x, i - nx) - c;
-    if (iz + 1 < nz)
-      lz += ld_elem(x, i + sxy) - c;
-    if (iz > 0)
-      lz += ld_elem(x, i - sxy) - c;
-    const float l = fmaf(lx, wx, fmaf(ly, wy, lz * wz));
-    st_elem(out, i, add ? fmaf(scale, l, ld_elem(out, i)) : scale * l);
-  }
+  const long long sxy = (long long)nx * ny;
+  const int       ix = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ix >= nx)
+    return;
+  for (int iz = blockIdx.z; iz < nz; iz += gridDim.z)
+    for (int iy = blockIdx.y; iy < ny; iy += gridDim.y)
+    {
+      const long long i = (long long)iz * sxy + (long long)iy * nx + ix;
+      const float c = ld_elem(x, i);
+      float       lx = 0.f, ly = 0.f, lz = 0.f;
+      if (ix + 1 < nx)
+        lx += ld_elem(x, i + 1) - c;
+      if (ix > 0)
+        lx += ld_elem(x, i - 1) - c;
+      if (iy + 1 < ny)
+        ly += ld_elem(x, i + nx) - c;
+      if (iy > 0)
+        ly += ld_elem(x, i - nx) - c;
+      if (iz + 1 < nz)
+        lz += ld_elem(x, i + sxy) - c;
+      if (iz > 0)
+        lz += ld_elem(x, i - sxy) - c;
+      const float l = fmaf(lx, wx, fmaf(ly, wy, lz * wz));
+      st_elem(out, i, add ? fmaf(scale, l, ld_elem(out, i)) : scale * l);
+    }
 }
 
 template <typename TI, typename TO>
 cudaError_t
 laplacian_launch(const rtkb_image_desc & v, const TI * x, TO * out, float scale, bool add, cudaStream_t st)
 {
-  const long long n = (long long)v.size[0] * v.size[1] * v.size[2];
-  laplacian_kernel<TI, TO><<<(unsigned)std::min<long long>((n + 255) / 256, 148LL * 16), 256, 0, st>>>(
+  const dim3 grid((unsigned)((v.size[0] + 127) / 128), (unsigned)std::min(v.size[1], 65535),
+                  (unsigned)std::min(v.size[2], 65535));
+  laplacian_kernel<TI, TO><<<grid, 128, 0, st>>>(
     x, out, v.size[0], v.size[1], v.size[2], (float)(1. / (v.spacing[0] * v.spacing[0])),
     (float)(1. / (v.spacing[1] * v.spacing[1])), (float)(1. / (v.spacing[2] * v.spacing[2])), scale, add);
   return cudaGetLastError();

@@ -406,6 +406,112 @@ private:
   const float *              m_Weights = nullptr;
 };
 
+/* rtk::TotalVariationDenoisingBPDQImageFilter on a device volume (out may equal in) */
+class TotalVariationDenoisingBPDQImageFilter
+{
+public:
+  void SetInput(const rtkb_image_desc & d, const float * in) { m_Desc = d; m_In = in; }
+  void SetOutput(float * out) { m_Out = out; }
+  void SetGamma(double g) { m_Gamma = g; }
+  void SetNumberOfIterations(int n) { m_Iterations = n; }
+  void
+  SetDimensionsProcessed(const bool dims[3])
+  {
+    for (int d = 0; d < 3; d++)
+      m_Dims[d] = dims[d] ? 1 : 0;
+  }
+  void SetStream(void * s) { m_Stream = s; }
+  void
+  Update()
+  {
+    Check(rtkb_tv_denoising_bpdq(&m_Desc, m_In, m_Out, m_Gamma, m_Iterations, m_Dims, m_Stream),
+          "TotalVariationDenoisingBPDQImageFilter");
+  }
+
+private:
+  rtkb_image_desc m_Desc{};
+  const float *   m_In = nullptr;
+  float *         m_Out = nullptr;
+  double          m_Gamma = 1.;
+  int             m_Iterations = 1;
+  int             m_Dims[3] = { 1, 1, 1 };
+  void *          m_Stream = nullptr;
+};
+
+/* rtk::I0EstimationProjectionFilter on a device 16-bit raw image (waits for the stream) */
+class I0EstimationProjectionFilter
+{
+public:
+  void SetInput(const rtkb_image_desc & d, const unsigned short * raw) { m_Desc = d; m_Raw = raw; }
+  void SetBitShift(int b) { m_Shift = b; }
+  void SetDynThreshold(unsigned int t) { m_Threshold = t; }
+  void SetStream(void * s) { m_Stream = s; }
+  void
+  Update()
+  {
+    Check(rtkb_i0_estimation(&m_Desc, m_Raw, m_Shift, m_Threshold, &m_Estimate, m_Stream),
+          "I0EstimationProjectionFilter");
+  }
+  double GetI0() const { return m_Estimate.i0; }
+  double GetI0fwhm() const { return m_Estimate.i0_fwhm; }
+  const rtkb_i0_estimate & GetEstimate() const { return m_Estimate; }
+
+private:
+  rtkb_image_desc        m_Desc{};
+  const unsigned short * m_Raw = nullptr;
+  int                    m_Shift = 2;
+  unsigned int           m_Threshold = 20;
+  rtkb_i0_estimate       m_Estimate{};
+  void *                 m_Stream = nullptr;
+};
+
+/* rtk::LUTbasedVariableI0RawToAttenuationImageFilter: device 16-bit raw in, float line integrals out */
+class LUTbasedVariableI0RawToAttenuationImageFilter
+{
+public:
+  void SetInput(const rtkb_image_desc & d, const unsigned short * raw) { m_Desc = d; m_Raw = raw; }
+  void SetOutput(float * out) { m_Out = out; }
+  void SetI0(double i0) { m_I0 = i0; }
+  void SetIDark(double d) { m_IDark = d; }
+  void SetStream(void * s) { m_Stream = s; }
+  void
+  Update()
+  {
+    Check(rtkb_raw_to_attenuation(&m_Desc, m_Raw, m_I0, m_IDark, m_Out, m_Stream),
+          "LUTbasedVariableI0RawToAttenuationImageFilter");
+  }
+
+private:
+  rtkb_image_desc        m_Desc{};
+  const unsigned short * m_Raw = nullptr;
+  float *                m_Out = nullptr;
+  double                 m_I0 = 65535., m_IDark = 0.;
+  void *                 m_Stream = nullptr;
+};
+
+/* rtk::WaterPrecorrectionImageFilter on device line integrals (out may equal in) */
+class WaterPrecorrectionImageFilter
+{
+public:
+  void SetInput(const rtkb_image_desc & d, const float * in) { m_Desc = d; m_In = in; }
+  void SetOutput(float * out) { m_Out = out; }
+  void SetCoefficients(std::vector<double> c) { m_C = std::move(c); }
+  void SetStream(void * s) { m_Stream = s; }
+  void
+  Update()
+  {
+    Check(rtkb_water_precorrection(&m_Desc, m_In, m_Out, m_C.data(), (int)m_C.size(), m_Stream),
+          "WaterPrecorrectionImageFilter");
+  }
+
+private:
+  rtkb_image_desc     m_Desc{};
+  const float *       m_In = nullptr;
+  float *             m_Out = nullptr;
+  std::vector<double> m_C{ 0., 1. };
+  void *              m_Stream = nullptr;
+};
+
 } // namespace rtkb
 
 #endif

@@ -75,6 +75,44 @@ int main(int, char ** argv)
     f.SetProjections(rtkb::MakeImageDescription(ps, sp, o), nullptr);
     f.Update();
   }, "null argument");
+  bad += expect_throw("water precorrection without buffers", [] {
+    const int sz[3] = { 4, 4, 2 };
+    const double sp[3] = { 1., 1., 1. }, o[3] = { 0., 0., 0. };
+    rtkb::WaterPrecorrectionImageFilter f;
+    f.SetInput(rtkb::MakeImageDescription(sz, sp, o), nullptr);
+    f.SetCoefficients({ 0.05, 0.3, 2.0 });
+    f.Update();
+  }, "null argument");
+  bad += expect_throw("TV with no iterations", [] {
+    const int sz[3] = { 4, 4, 2 };
+    const double sp[3] = { 1., 1., 1. }, o[3] = { 0., 0., 0. };
+    static float dummy[1];
+    rtkb::TotalVariationDenoisingBPDQImageFilter f;
+    f.SetInput(rtkb::MakeImageDescription(sz, sp, o), dummy);
+    f.SetOutput(dummy);
+    f.SetNumberOfIterations(0);
+    f.Update();
+  }, "niter >= 1");
+  bad += expect_throw("I0 estimation with a bad bit shift", [] {
+    const int sz[3] = { 4, 4, 1 };
+    const double sp[3] = { 1., 1., 1. }, o[3] = { 0., 0., 0. };
+    static unsigned short dummy[1];
+    rtkb::I0EstimationProjectionFilter f;
+    f.SetInput(rtkb::MakeImageDescription(sz, sp, o), dummy);
+    f.SetBitShift(12);
+    f.Update();
+  }, "bit shift");
+  bad += expect_throw("raw conversion with a non-finite I0", [] {
+    const int sz[3] = { 4, 4, 1 };
+    const double sp[3] = { 1., 1., 1. }, o[3] = { 0., 0., 0. };
+    static unsigned short dummy[1];
+    static float out[1];
+    rtkb::LUTbasedVariableI0RawToAttenuationImageFilter f;
+    f.SetInput(rtkb::MakeImageDescription(sz, sp, o), dummy);
+    f.SetOutput(out);
+    f.SetI0(1.0 / 0.0);
+    f.Update();
+  }, "finite");
   bad += expect_throw("mixed geometry", [] {
     rtkb::ThreeDCircularProjectionGeometry h;
     h.AddProjection(1000., 1500., 0.);

@@ -223,8 +223,10 @@ int rtkb_convert_to_bf16(const float * d_in, void * d_out, long long n, void * s
  * GPU that loads the library until the process exits); larger stacks are
  * rejected with RTKB_ERR_INVALID_ARGUMENT.  It calls no cudaMalloc, cudaFree
  * or allocating library routine.  The first call on a device looks up the
- * array's device address (cudaGetSymbolAddress) with that device current;
- * make that first call before any stream capture.  All calls share the array
+ * array's device address (cudaGetSymbolAddress) with that device current,
+ * and so does the first call after the device's context changed (after a
+ * cudaDeviceReset the array lives at a new address); make that first call
+ * before any stream capture.  All calls share the array
  * and it keeps the last call's contents: calls whose GPU work overlaps (other
  * streams, other host threads) race on it and must be serialised by the
  * caller. */

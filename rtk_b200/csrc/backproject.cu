@@ -1727,10 +1727,33 @@ static __device__ __align__(256) unsigned char g_bp_static_scratch[kStaticMaxPro
 
 std::mutex g_static_mutex;
 void *     g_static_address[256] = {}; // per device ordinal
+void *     g_static_context[256] = {}; // the context each address belongs to
 
-// Device address of g_bp_static_scratch on the current device, looked up once
-// per device with that device current.  In host code the array's name is only
-// a stand-in for the symbol, never a device address.
+// The driver's cuCtxGetCurrent, reached through the runtime (the library does
+// not link libcuda).  Null if the driver does not export it.
+using CtxGetCurrentFn = int (*)(void **);
+CtxGetCurrentFn
+ctx_get_current()
+{
+  static std::once_flag  once;
+  static CtxGetCurrentFn fn = nullptr;
+  std::call_once(once, [] {
+    void *                          ptr = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<CtxGetCurrentFn>(ptr);
+    else
+      cudaGetLastError();
+  });
+  return fn;
+}
+
+// Device address of g_bp_static_scratch on the current device, looked up with
+// that device current the first time the entry point runs there, and again
+// whenever the device's context has changed since (after cudaDeviceReset the
+// module, and so the array, is loaded anew at another address).  In host code
+// the array's name is only a stand-in for the symbol, never a device address.
 int
 static_scratch_address(void ** out)
 {
@@ -1738,14 +1761,21 @@ static_scratch_address(void ** out)
   RTKB_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 256)
     return rtkb::fail(RTKB_ERR_UNSUPPORTED, "device ordinal out of range");
+  void *          ctx = nullptr;
+  CtxGetCurrentFn get = ctx_get_current();
+  if (get && get(&ctx) != 0)
+    ctx = nullptr;
   std::lock_guard<std::mutex> lock(g_static_mutex);
-  if (!g_static_address[dev])
+  if (!g_static_address[dev] || !ctx || g_static_context[dev] != ctx)
   {
     void *      p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_bp_static_scratch);
+    cudaError_t e = cudaGetSymbolAddress(&p, g_bp_static_scratch); // makes the primary context current
     if (e != cudaSuccess)
       return rtkb::cuda_fail(e, "cudaGetSymbolAddress(g_bp_static_scratch)");
+    if (get && get(&ctx) != 0)
+      ctx = nullptr;
     g_static_address[dev] = p;
+    g_static_context[dev] = ctx;
   }
   *out = g_static_address[dev];
   return RTKB_OK;

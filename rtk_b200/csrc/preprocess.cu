@@ -157,7 +157,10 @@ i0_search(const std::vector<unsigned int> & hist, int shift, unsigned int dyn_th
   size_t       imax = nbins - 1;
   while (hist[imax] <= dyn_threshold && imax > 0)
     --imax;
-  while (hist[imax] == 0 && imax + 1 < nbins) // back to a non-empty bin (RTK's loop can run past the end)
+  // back to a non-empty bin.  RTK's loop runs past the end only when every bin
+  // is empty, i.e. for an empty image, which the entry point refuses (image
+  // sizes must be positive); for every other histogram the bound never binds.
+  while (hist[imax] == 0 && imax + 1 < nbins)
     ++imax;
   size_t imin = 0;
   while (hist[imin] <= dyn_threshold && imin < imax)

@@ -39,7 +39,9 @@ def geometry_md_xml(path: str) -> str:
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <path of an RTK source tree>")
+    ref = sys.argv[1]
     here = os.path.dirname(os.path.abspath(__file__))
     md = os.path.join(ref, "documentation", "docs", "Geometry.md")
     kat = parse_geometry_md(md)

@@ -71,3 +71,15 @@ def test_ops_refuse_cpu_tensors(rtkb):
     pd = rtkb.make_desc((16, 16, 4))
     with pytest.raises(TypeError, match="CUDA"):
         rtkb.ops.fdk_backproject(g, vd, pd, torch.zeros(4, 16, 16), torch.zeros(8, 8, 8))
+
+
+def test_i0_estimation_refuses_an_empty_image(rtkb):
+    """RTK's histogram search reads past the histogram only when every bin is
+    empty, i.e. for an image without pixels; the entry point refuses those
+    before any device work."""
+    lib = rtkb.load()
+    empty = rtkb.make_desc((0, 16, 1))
+    out = rtkb._capi.I0Estimate()
+    rc = lib.rtkb_i0_estimation(C.byref(empty), C.c_void_p(16), 2, 20, C.byref(out), None)
+    assert rc == rtkb._capi.RTKB_ERR_INVALID_ARGUMENT
+    assert b"positive" in lib.rtkb_last_error()

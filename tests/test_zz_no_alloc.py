@@ -1,15 +1,22 @@
 """The allocation-free FDK backprojection entry point
 (rtkb_fdk_backproject_static_scratch), for callers that cannot allocate
-device memory during a reconstruction.  Called through the C ABI and checked
-against rtkb_fdk_backproject on two calls in a row (the second with a shorter
-stack, so stale scratch from the first call must not leak into it).  Collected
-last, so a run that stops at the first failure has run every other test."""
+device memory during a reconstruction: applications whose device memory is
+reserved up front by their own allocator, and on-line loops that cannot take
+cudaMalloc's implicit device synchronisation.
+
+Called through the C ABI on two calls in a row (the second with a shorter
+stack, so stale scratch from the first call must not leak into it) and
+checked three ways: bit-identical to rtkb_fdk_backproject (the same kernels
+run), within the FP32 tolerance of the FP64 oracle, and without growing the
+library's device memory pool.  A tilted detector takes the generic per-voxel
+path, whose path modes also live in the static array.  Collected last, so a
+run that stops at the first failure has run every other test."""
 import ctypes as C
 
 import numpy as np
 import pytest
 
-from tests.gpu_util import REL_L2_TOL, rel_l2, to_np
+from tests.gpu_util import REL_L2_TOL, pair_geometry, pair_image, rel_l2, to_np
 
 pytestmark = pytest.mark.gpu
 
@@ -24,21 +31,34 @@ def _call(lib, fn, g, vd, pd, p, v0):
     return out
 
 
-def test_static_scratch_matches_allocating_entry_point(rtkb):
+def _params(n, oop=0.0):
+    return [(1000.0, 1536.0, i * 360.0 / n, 4.0, -2.0, oop) for i in range(n)]
+
+
+@pytest.mark.parametrize("oop", [0.0, 7.0], ids=["circular", "tilted"])
+def test_static_scratch_matches_allocating_entry_point(rtkb, oracle, oop):
     import torch
 
     lib = rtkb.load()
-    gen = torch.Generator(device="cuda").manual_seed(7)
+    rng = np.random.default_rng(7)
     cases = [(120, (96, 80, 88), (160, 128)), (40, (64, 72, 56), (128, 120))]  # second call: shorter stack
     for nproj, vsize, (nu, nv) in cases:
-        g = rtkb.geometry.circular(nproj, 1000.0, 1536.0, projOffsetX=4.0, projOffsetY=-2.0)
-        vd = rtkb.make_desc(vsize, (1.5, 1.5, 1.5))
-        pd = rtkb.make_desc((nu, nv, nproj), (1.0, 1.0, 1.0))
-        p = torch.rand((nproj, nv, nu), device="cuda", generator=gen) * 2 - 1
-        v0 = torch.rand((vsize[2], vsize[1], vsize[0]), device="cuda", generator=gen)
-        ref = _call(lib, lib.rtkb_fdk_backproject, g, vd, pd, p, v0)
-        got = _call(lib, lib.rtkb_fdk_backproject_static_scratch, g, vd, pd, p, v0)
-        assert rel_l2(to_np(got), to_np(ref)) < REL_L2_TOL
+        gl, go = pair_geometry(rtkb, oracle, _params(nproj, oop))
+        vd, vo = pair_image(rtkb, oracle, vsize, (1.5, 1.5, 1.5))
+        pd, po = pair_image(rtkb, oracle, (nu, nv, nproj), (1.0, 1.0, 1.0))
+        p_np = rng.uniform(-1, 1, size=(nproj, nv, nu)).astype(np.float32)
+        v_np = rng.uniform(0, 1, size=(vsize[2], vsize[1], vsize[0])).astype(np.float32)
+        p, v0 = torch.from_numpy(p_np).cuda(), torch.from_numpy(v_np).cuda()
+        ref = _call(lib, lib.rtkb_fdk_backproject, gl, vd, pd, p, v0)
+        torch.cuda.synchronize()
+        rtkb.ops.trim_memory_pool()
+        reserved_before = rtkb.ops.memory_pool_reserved()
+        got = _call(lib, lib.rtkb_fdk_backproject_static_scratch, gl, vd, pd, p, v0)
+        torch.cuda.synchronize()
+        assert rtkb.ops.memory_pool_reserved() == reserved_before
+        assert torch.equal(got, ref)
+        want = oracle.backproject(go, vo, po, p_np.astype(np.float64), v_np.astype(np.float64), fdk=True)
+        assert rel_l2(to_np(got), want) < REL_L2_TOL
     assert rtkb.ops.device_status() == 0
 
 

@@ -37,9 +37,11 @@ PIX = 0.388
 SID, SDD = 1000.0, 1536.0
 SEED = 20261203 + 1
 L1_BYTES_PER_UPDATE = 16  # four 4-byte taps of one bilinear interpolation
-# DRAM bytes (read + write) of one backprojection launch of this workload, from the 1-pass ncu capture
-# summarised in profiles/bp_tiled_kernel_512cube_720proj_traffic.md (69.86 GB read + 0.651 GB written).
+# DRAM bytes (read + write) of one backprojection launch of this workload, recorded from a 1-pass ncu
+# capture (dram__bytes_read.sum + dram__bytes_write.sum) of the kernel as of BP_TRAFFIC_COMMIT; a
+# recorded figure, not a measurement of the build that runs.
 BP_LAUNCH_DRAM_BYTES = 69.86e9 + 0.6506e9
+BP_TRAFFIC_COMMIT = "aff05f8"
 WORKLOAD = {"workload": "FDK backprojection 512^3 @0.5mm <- 720 x 1024x768 @0.388mm, SID 1000, SDD 1536, 360 deg",
             "volume": [NX, NY, NZ], "projections": [NU, NV, NP], "dtype_storage": "float32",
             "l2_policy": "inputs larger than L2 (2.26 GB projection stack, 0.54 GB volume)"}
@@ -562,9 +564,9 @@ def cg_seconds_to_residual(torch, rtkb, stream, tol=1e-3, max_iter=300, learned_
     counts = torch.poisson(i0 * torch.exp(-clean), generator=gen).clamp_(min=1.0)
     p = (-torch.log(counts / i0)).contiguous()
 
-    def solve(net, storage="fp32", max_it=max_iter):
+    def solve(net, storage="fp32", max_it=max_iter, backprojector="joseph"):
         x = torch.zeros((256, 256, 256), device="cuda")
-        cg = rtkb.ops.ConjugateGradient(g, vd, pd, storage=storage)
+        cg = rtkb.ops.ConjugateGradient(g, vd, pd, storage=storage, backprojector=backprojector)
         if net is not None:
             cg.set_preconditioner(net, history=8)
         torch.cuda.synchronize()
@@ -592,6 +594,12 @@ def cg_seconds_to_residual(torch, rtkb, stream, tol=1e-3, max_iter=300, learned_
            "config": "256^3 @1mm <- 360 x 512x384 @0.8mm, SID 1000, SDD 1536, 20 random ellipsoids, "
                      "Poisson I0=5e4, Joseph pair, FP32 vectors / FP64 scalars, CUDA graph per iteration",
            "learned_pcg": None}
+    # RTK's default projector choice: Joseph forward, voxel-based back projector
+    # (not the forward projector's adjoint, so CG solves a non-symmetric system)
+    vsecs, vit, vrel, vper, _, x_vox = solve(None, backprojector="voxel", max_it=100)
+    out["voxel_backprojector"] = {"seconds_to_rel_residual_1e-3": vsecs, "iterations": vit, "relative_residual": vrel,
+                                  "seconds_per_iteration": vper, "residual_history": solve.hist}
+    del x_vox
 
     # precision study: 30 iterations in one graph replay loop per storage
     # variant (FP32, or BF16 r, p, A p and projection temporary), and each
@@ -689,6 +697,66 @@ def cpu_baseline_gups(g_oracle_factory, n_proj_sample: int, threads: int):
     O.fdk_backproject_f32_rtk(go, vo, po, p, vol, threads=threads)
     dt = time.perf_counter() - t0
     return float(NX) * NY * NZ * n_proj_sample / dt / 1e9, dt
+
+
+def oracle_slab_error(torch, proj, vol, y0=250, ny=4, r0=360, nr=40, threads=None) -> dict:
+    """The checker on the timed output: relative L2 error of the volume's
+    y-slab [y0, y0 + ny) against the FP64 oracle's FDK backprojection of the
+    same stack.  The slab projects onto detector rows ~370-392 of every
+    projection; the oracle reads rows [r0, r0 + nr) of the stack (with margin)
+    and never the rest."""
+    import numpy as np
+
+    from oracle import oracle as O
+
+    O.build()
+    go = oracle_geometry()
+    po = O.image((NU, NV, NP), (PIX, PIX, 1.0))
+    rows = O.image((NU, nr, NP), (PIX, PIX, 1.0), origin=tuple(po.origin), index=(0, r0, 0))
+    vfull = O.image((NX, NY, NZ), (VOX,) * 3)
+    slab = O.image((NX, ny, NZ), (VOX,) * 3, origin=tuple(vfull.origin), index=(0, y0, 0))
+    t0 = time.perf_counter()
+    ref = O.backproject(go, slab, rows, proj[:, r0:r0 + nr, :].cpu().numpy().astype(np.float64), fdk=True,
+                        threads=threads)
+    got = vol[:, y0:y0 + ny, :].cpu().numpy().astype(np.float64)
+    err = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+    return {"oracle_rel_l2": err, "region": f"y-slab {y0}..{y0 + ny - 1} of the last timed step's volume",
+            "oracle": "FP64 CPU restatement, ray/detector-plane voxel map", "seconds": time.perf_counter() - t0}
+
+
+def legs_summary(legs: dict) -> dict:
+    """The headline's compact copy of the extra legs: their numeric fields (one
+    nesting level deep, 4 significant digits); the full records are the 'leg'
+    lines printed before the headline."""
+    def num(v):
+        return isinstance(v, (int, float)) and not isinstance(v, bool)
+
+    out = {}
+    for name, d in legs.items():
+        if num(d):
+            out[name] = float(f"{d:.4g}")
+            continue
+        if not isinstance(d, dict):
+            continue
+        flat = {}
+        for k, v in d.items():
+            if num(v):
+                flat[k] = float(f"{v:.4g}")
+            elif isinstance(v, dict):
+                for k2, v2 in v.items():
+                    if num(v2):
+                        flat[f"{k}.{k2}"] = float(f"{v2:.4g}")
+            elif k == "error":
+                flat[k] = str(v)[:120]
+        out[name] = flat
+    return out
+
+
+def emit_leg(name: str, data) -> None:
+    """One extra measurement as its own line, 'leg <name> <json>', printed as
+    soon as it is measured (not a JSON line, so the headline stays the only
+    one)."""
+    print(f"leg {name} " + json.dumps(data, separators=(",", ":")), flush=True)
 
 
 def oracle_geometry():
@@ -973,7 +1041,8 @@ def main():
     roofline = {"bound": "l1", "achieved": achieved, "peak": peak_smem, "unit": "GB/s",
                 "frac": achieved / peak_smem if peak_smem else None,
                 "traffic": BP_LAUNCH_DRAM_BYTES if NX == 512 else None,
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one full-size launch",
+                "traffic_source": "recorded constant: ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                  f"full-size launch of the kernel at commit {BP_TRAFFIC_COMMIT}",
                 "peak_source": "measured in this run: shared-memory bilinear-gather probe (rtkb_probe_smem_gather)",
                 "per_launch_updates": updates_per_step(), "bytes_per_update": L1_BYTES_PER_UPDATE,
                 "hbm": {"algorithmic_bytes_per_launch": hbm_bytes,
@@ -993,6 +1062,7 @@ def main():
             "gpu_launches_note": "one rtkb backprojection kernel per step (plus one matrix upload copy)",
             "autotune": tuned}
 
+    legs = {}
     if world == 1 and not args.no_extra_legs:
         # the project's autotuner on this workload (every configuration timed on
         # the real stack, after the timed region): which configuration it picks
@@ -1002,17 +1072,35 @@ def main():
         line["autotune"] = {"config": best, "heuristic_config": heuristic_cfg,
                             "ms_per_config": [round(t, 2) for t in times]}
         rtkb.ops.fdk_backproject(g, vd, pd, proj, zero, out=vol, stream=stream)
-        line["bf16_storage"] = bf16_storage_leg(torch, rtkb, g, vd, pd, proj, vol, stream, peak_smem)
-        line["fdk_pipeline_ms"] = fdk_pipeline_ms(torch, rtkb, g, vd, pd, proj, stream)
+
+    # the checker on the last timed output (outside every timed region)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and NX == 512:
+        try:
+            line["oracle_check"] = oracle_slab_error(torch, proj, vol)
+        except Exception as ex:  # the check is reported; a failure to run it is reported too
+            line["oracle_check"] = {"oracle_rel_l2": None, "error": str(ex)}
+
+    if world == 1 and not args.no_extra_legs:
+        def leg(name, fn, *a, **kw):
+            try:
+                legs[name] = fn(*a, **kw)
+            except Exception as ex:
+                legs[name] = {"error": str(ex)}
+            if rank == 0:
+                emit_leg(name, legs[name])
+
+        leg("bf16_storage", bf16_storage_leg, torch, rtkb, g, vd, pd, proj, vol, stream, peak_smem)
+        leg("fdk_pipeline_ms", fdk_pipeline_ms, torch, rtkb, g, vd, pd, proj, stream)
         del proj
-        line["joseph_forward"] = joseph_forward_leg(torch, rtkb, lib, stream)
-        line["batched"] = batch_leg(torch, rtkb, stream)
-        line["batched_cg"] = batch_cg_leg(torch, rtkb, stream)
-        line["sart"] = sart_leg(torch, rtkb, stream)
-        line["osem"] = osem_leg(torch, rtkb, stream)
-        line["regularized_cg"] = regularized_cg_leg(torch, rtkb, stream)
-        line["preprocess"] = preprocess_leg(torch, rtkb, stream)
-        line["cg"] = cg_seconds_to_residual(torch, rtkb, stream)
+        leg("joseph_forward", joseph_forward_leg, torch, rtkb, lib, stream)
+        leg("batched", batch_leg, torch, rtkb, stream)
+        leg("batched_cg", batch_cg_leg, torch, rtkb, stream)
+        leg("sart", sart_leg, torch, rtkb, stream)
+        leg("osem", osem_leg, torch, rtkb, stream)
+        leg("regularized_cg", regularized_cg_leg, torch, rtkb, stream)
+        leg("preprocess", preprocess_leg, torch, rtkb, stream)
+        leg("cg", cg_seconds_to_residual, torch, rtkb, stream)
+        line["legs"] = legs_summary(legs)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             threads = os.cpu_count() or 1

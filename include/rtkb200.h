@@ -313,6 +313,14 @@ typedef struct rtkb_cg_params
                             (no counterpart in the reference; the iterate stays in the caller's FP32
                             buffer; no learned preconditioner) */
   double gamma;          /* Laplacian regularisation weight (RTK's SetGamma): A x += gamma * (-Laplacian(x)) */
+  int    backprojector;  /* IterativeConeBeamReconstructionFilter's BackProjectionType
+                            (include/rtkIterativeConeBeamReconstructionFilter.h:80-88, .hxx:33-103), the back
+                            projector of b = BP(W .* p) and of A x = BP(W .* FP(x)), with RTK's values:
+                            0 = BP_VOXELBASED (RTK's default, and so that of zero-initialised parameters; FP32
+                            storage and flat panels; not the exact adjoint of the forward projector),
+                            1 = BP_JOSEPH (the Joseph forward projector's exact adjoint), 2 = BP_CUDAVOXELBASED
+                            (the same voxel-based back projector here).  The forward projector is Joseph
+                            (FP_JOSEPH) either way. */
 } rtkb_cg_params;
 /* rtk::LaplacianImageFilter / CudaLaplacianImageFilter (include/rtkLaplacianImageFilter.hxx;
  * src/rtkCudaLaplacianImageFilter.cu): d_out = Laplacian(d_in), the

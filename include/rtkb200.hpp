@@ -242,6 +242,14 @@ public:
   {
     m_Params.gamma = g;
   }
+  /* IterativeConeBeamReconstructionFilter::SetBackProjectionFilter with RTK's
+   * BackProjectionType values: 0 BP_VOXELBASED (default), 1 BP_JOSEPH,
+   * 2 BP_CUDAVOXELBASED; the forward projector is Joseph. */
+  void
+  SetBackProjectionFilter(int bptype)
+  {
+    m_Params.backprojector = bptype;
+  }
   void
   SetInputWeights(const float * w)
   {
@@ -274,7 +282,7 @@ public:
 
 private:
   rtkb_cg *      m_Plan = nullptr;
-  rtkb_cg_params m_Params{ 0., 1, 0, 0. };
+  rtkb_cg_params m_Params{ 0., 1, 0, 0., 0 };
   int            m_Iterations = 3;
   const float *  m_Weights = nullptr;
   const float *  m_Mask = nullptr;

@@ -81,6 +81,7 @@ def lib():
             "orc_index_to_physical": (None, [IM, D]),
             "orc_physical_to_index": (None, [IM, D]),
             "orc_bp_matrix": (C.c_int, [G, IM, IM, C.c_int, C.c_int, D]),
+            "orc_bp_project": (C.c_int, [G, IM, IM, C.c_int, C.c_int, D, D]),
             "orc_backproject": (None, [G, IM, IM, D, D, D, C.c_int, C.c_int]),
             "orc_joseph_forward": (None, [G, IM, D, IM, D, D, C.c_int]),
             "orc_joseph_back": (None, [G, IM, D, D, IM, D]),
@@ -93,6 +94,8 @@ def lib():
             "orc_ramp_kernel": (None, [C.c_int, C.c_double, C.POINTER(OrcRampParams), D]),
             "orc_ramp_filter": (None, [IM, C.POINTER(OrcRampParams), D, D, C.c_int]),
             "orc_cg_joseph": (None, [G, IM, IM, D, D, D, C.c_double, C.c_double, C.c_int, D, D, C.c_int]),
+            "orc_cg": (None, [G, IM, IM, D, D, D, C.c_double, C.c_double, C.c_int, D, D, C.c_int, C.c_int]),
+            "orc_joseph_back_mt": (None, [G, IM, D, D, IM, D, C.c_int]),
             "orc_laplacian": (None, [IM, D, D]),
             "orc_ray_box": (None, [G, IM, IM, D, C.c_int]),
             "orc_sart": (None, [G, IM, IM, D, D, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_double,
@@ -224,6 +227,15 @@ def bp_matrix(g: Geometry, vol: OrcImage, proj: OrcImage, i: int, fdk: bool):
     return m.reshape(3, 4), mode
 
 
+def bp_project(g: Geometry, vol: OrcImage, proj: OrcImage, k: int, fdk: bool, physical):
+    """(u, v, weight) of a physical point in projection k by the oracle's own
+    ray/detector-plane derivation, and RTK's path mode."""
+    x = np.ascontiguousarray(physical, dtype=np.float64)
+    out = np.zeros(3)
+    mode = lib().orc_bp_project(g._g, C.byref(vol), C.byref(proj), k, int(fdk), _d(x), _d(out))
+    return out, mode
+
+
 def backproject(g, vol, proj, proj_data, vol_in=None, fdk=True, threads=None):
     p = np.ascontiguousarray(proj_data, dtype=np.float64)
     vin = np.zeros(shape_of(vol)) if vol_in is None else np.ascontiguousarray(vol_in, dtype=np.float64)
@@ -241,11 +253,16 @@ def joseph_forward(g, vol, vol_data, proj, proj_in=None, threads=None):
     return out
 
 
-def joseph_back(g, vol, proj, proj_data, vol_in=None):
+def joseph_back(g, vol, proj, proj_data, vol_in=None, threads=1):
+    """RTK's single-threaded Joseph back projection (threads > 1: the same sum
+    split over threads by projection)."""
     p = np.ascontiguousarray(proj_data, dtype=np.float64)
     vin = np.zeros(shape_of(vol)) if vol_in is None else np.ascontiguousarray(vol_in, dtype=np.float64)
     out = np.empty(shape_of(vol))
-    lib().orc_joseph_back(g._g, C.byref(vol), _d(vin), _d(out), C.byref(proj), _d(p))
+    if threads == 1:
+        lib().orc_joseph_back(g._g, C.byref(vol), _d(vin), _d(out), C.byref(proj), _d(p))
+    else:
+        lib().orc_joseph_back_mt(g._g, C.byref(vol), _d(vin), _d(out), C.byref(proj), _d(p), threads or nthreads())
     return out
 
 
@@ -472,15 +489,17 @@ def water_precorrection(data, coefficients):
 
 
 def cg_joseph(g, vol, proj, proj_data, niter, x0=None, weights=None, tikhonov=0.0, gamma=0.0, mask=None,
-              threads=None):
+              threads=None, backprojector="joseph"):
+    """RTK's CG reconstruction with the Joseph forward projector and the
+    chosen back projector ("joseph", or "voxel" for the voxel-based one)."""
     p = np.ascontiguousarray(proj_data, dtype=np.float64)
     w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
     m = None if mask is None else np.ascontiguousarray(mask, dtype=np.float64)
     x = np.zeros(shape_of(vol)) if x0 is None else np.array(x0, dtype=np.float64, copy=True, order="C")
     res = np.zeros(niter + 1)
-    lib().orc_cg_joseph(g._g, C.byref(vol), C.byref(proj), _d(p), _d(w), _d(m), tikhonov, gamma, niter, _d(x),
-                        _d(res),
-                        threads or nthreads())
+    bp = {"joseph": 0, "voxel": 1}[backprojector]
+    lib().orc_cg(g._g, C.byref(vol), C.byref(proj), _d(p), _d(w), _d(m), tikhonov, gamma, niter, _d(x), _d(res), bp,
+                 threads or nthreads())
     return x, res
 
 

@@ -333,6 +333,22 @@ cyl_pixel(const double * idx2det, const double * M, double radius, double iu, do
     out[a] = M[a * 4 + 3] + M[a * 4 + 0] * pos[0] + M[a * 4 + 1] * pos[1] + M[a * 4 + 2] * pos[2];
 }
 
+/* Parallel beam (SDD 0): ProjectionsRegionConstIteratorRayBasedParallel
+ * (include/rtkProjectionsRegionConstIteratorRayBasedParallel.hxx:40-75) with
+ * the identity post-matrix (RayConvexIntersectionImageFilter): pixel - source
+ * = -2 SID x row 2 of the rotation matrix, in mm.  Returns 1 for a parallel
+ * projection, 0 (s2p untouched) otherwise. */
+static int
+parallel_source_to_pixel(const orc_geometry * g, int i, double s2p[3])
+{
+  if (g->par[10 * i + P_SDD] != 0.)
+    return 0;
+  const double * R = g->rot + 16 * i + 8;
+  for (int a = 0; a < 3; a++)
+    s2p[a] = -2. * g->par[10 * i + P_SID] * R[a];
+  return 1;
+}
+
 void
 orc_geometry_source_angles(const orc_geometry * g, double * out)
 {
@@ -478,6 +494,13 @@ npix(const orc_image * im)
 /* ------------------------------------------------------------------------ */
 /* voxel-based and FDK backprojection                                       */
 /* ------------------------------------------------------------------------ */
+typedef struct
+{
+  double S[3], O[3], eu[3], ev[3], n[3];
+  double a[3], b[3];     /* stack physical (u, v, 1) -> absolute index */
+  double h, c0, su, sv;  /* (O - S).n, (0 - S).n, (S - O).eu, (S - O).ev */
+  int    parallel, fdk, mode;
+} bp_frame_t;
 int
 orc_bp_matrix(const orc_geometry * g, const orc_image * vol, const orc_image * proj, int i, int fdk, double m[12])
 {
@@ -524,6 +547,143 @@ orc_bp_matrix(const orc_geometry * g, const orc_image * vol, const orc_image * p
   return 0;
 }
 
+/* The detector frame of one projection in the fixed (physical) system:
+ * source S (GetSourcePosition, src/rtkThreeDCircularProjectionGeometry.cxx:597-608),
+ * detector origin O and unit axes eu, ev (the columns of
+ * GetProjectionCoordinatesToFixedSystemMatrix, :611-637), normal n = eu x ev
+ * (pointing at the source), and the stack's physical -> index map restricted
+ * to u, v (ci = a . (pu, pv, 1), cj = b . (pu, pv, 1)), as RTK restricts it. */
+static void
+bp_frame(const orc_geometry * g, const orc_image * vol, const orc_image * proj, int k, int fdk, bp_frame_t * f)
+{
+  double m[16], s4[4], p2i[16];
+  orc_geometry_proj_coords_to_fixed(g, k, m);
+  orc_geometry_source_position(g, k, s4);
+  orc_physical_to_index(proj, p2i);
+  for (int a = 0; a < 3; a++)
+  {
+    f->S[a] = s4[a];
+    f->eu[a] = m[a * 4 + 0];
+    f->ev[a] = m[a * 4 + 1];
+    f->O[a] = m[a * 4 + 3];
+  }
+  f->n[0] = f->eu[1] * f->ev[2] - f->eu[2] * f->ev[1];
+  f->n[1] = f->eu[2] * f->ev[0] - f->eu[0] * f->ev[2];
+  f->n[2] = f->eu[0] * f->ev[1] - f->eu[1] * f->ev[0];
+  f->a[0] = p2i[0];
+  f->a[1] = p2i[1];
+  f->a[2] = p2i[3];
+  f->b[0] = p2i[4];
+  f->b[1] = p2i[5];
+  f->b[2] = p2i[7];
+  f->parallel = g->par[10 * k + P_SDD] == 0.;
+  f->fdk = fdk;
+  double SO[3], Sn = 0., h = 0.;
+  for (int a = 0; a < 3; a++)
+  {
+    SO[a] = f->S[a] - f->O[a];
+    Sn += f->S[a] * f->n[a];
+    h -= SO[a] * f->n[a];
+  }
+  f->h = h;         /* (O - S) . n */
+  f->c0 = -Sn;      /* (X - S) . n at the physical origin (RTK's rotation centre) */
+  f->su = SO[0] * f->eu[0] + SO[1] * f->eu[1] + SO[2] * f->eu[2];
+  f->sv = SO[0] * f->ev[0] + SO[1] * f->ev[1] + SO[2] * f->ev[2];
+  /* RTK's choice between its optimised and generic paths
+   * (include/rtkFDKBackProjectionImageFilter.hxx:106-116,
+   * include/rtkBackProjectionImageFilter.hxx:220-230): the optimised Y (X)
+   * path when the homogeneous u numerator and w do not change along the
+   * volume's y (x) index, both below 1e-10 in RTK's scaling (w = (X - S).n,
+   * divided by its value at the rotation centre for FDK; w = 1 for a
+   * parallel beam).  Their rates along an index axis with physical step
+   * delta: du = K (delta.n) + h (a0 delta.eu + a1 delta.ev), dw = delta.n, K the
+   * u index of the point where the detector plane is met by the ray through
+   * S parallel to it (a0 su + a1 sv + a2); parallel beam: du = a0 delta.eu +
+   * a1 delta.ev, dw = 0. */
+  double rate_u[2], rate_w[2];
+  for (int ax = 0; ax < 2; ax++)
+  {
+    double d[3], dn = 0., de = 0., dv = 0.;
+    for (int a = 0; a < 3; a++)
+    {
+      d[a] = vol->direction[a * 3 + ax] * vol->spacing[ax];
+      dn += d[a] * f->n[a];
+      de += d[a] * f->eu[a];
+      dv += d[a] * f->ev[a];
+    }
+    if (f->parallel)
+    {
+      rate_u[ax] = f->a[0] * de + f->a[1] * dv;
+      rate_w[ax] = 0.;
+    }
+    else
+    {
+      const double K = f->a[0] * f->su + f->a[1] * f->sv + f->a[2];
+      rate_u[ax] = K * dn + h * (f->a[0] * de + f->a[1] * dv);
+      rate_w[ax] = dn;
+      if (fdk)
+      {
+        rate_u[ax] /= f->c0;
+        rate_w[ax] /= f->c0;
+      }
+    }
+  }
+  if (fabs(rate_u[0]) < 1e-10 && fabs(rate_w[0]) < 1e-10)
+    f->mode = 1;
+  else if (fabs(rate_u[1]) < 1e-10 && fabs(rate_w[1]) < 1e-10)
+    f->mode = 2;
+  else
+    f->mode = 0;
+}
+
+/* Continuous projection index (absolute) of the physical point X and the FDK
+ * weight: cone beam, the detector-plane point P = S + t (X - S) with
+ * t = ((O - S).n) / ((X - S).n), (pu, pv) = ((P - O).eu, (P - O).ev), weight
+ * (w0 / w)^2 with w = (X - S).n, w0 its value at the rotation centre (the
+ * distance ratio along the normal; 1 without FDK); parallel beam, P the
+ * orthogonal projection of X, weight 1. */
+static void
+bp_frame_map(const bp_frame_t * f, const double * X, double * u, double * v, double * wt)
+{
+  double pu, pv;
+  *wt = 1.;
+  if (f->parallel)
+  {
+    double XO[3];
+    for (int a = 0; a < 3; a++)
+      XO[a] = X[a] - f->O[a];
+    pu = XO[0] * f->eu[0] + XO[1] * f->eu[1] + XO[2] * f->eu[2];
+    pv = XO[0] * f->ev[0] + XO[1] * f->ev[1] + XO[2] * f->ev[2];
+  }
+  else
+  {
+    double d[3];
+    for (int a = 0; a < 3; a++)
+      d[a] = X[a] - f->S[a];
+    const double dn = d[0] * f->n[0] + d[1] * f->n[1] + d[2] * f->n[2];
+    const double t = f->h / dn;
+    pu = f->su + t * (d[0] * f->eu[0] + d[1] * f->eu[1] + d[2] * f->eu[2]);
+    pv = f->sv + t * (d[0] * f->ev[0] + d[1] * f->ev[1] + d[2] * f->ev[2]);
+    if (f->fdk)
+    {
+      const double r = f->c0 / dn;
+      *wt = r * r;
+    }
+  }
+  *u = f->a[0] * pu + f->a[1] * pv + f->a[2];
+  *v = f->b[0] * pu + f->b[1] * pv + f->b[2];
+}
+
+int
+orc_bp_project(const orc_geometry * g, const orc_image * vol, const orc_image * proj, int k, int fdk,
+               const double * physical, double out[3])
+{
+  bp_frame_t f;
+  bp_frame(g, vol, proj, k, fdk, &f);
+  bp_frame_map(&f, physical, out, out + 1, out + 2);
+  return f.mode;
+}
+
 static double
 interp_clamped(const double * p, int nu, int nv, double u, double v)
 {
@@ -547,10 +707,12 @@ orc_backproject(const orc_geometry * g, const orc_image * vol, const orc_image *
    * (include/rtkBackProjectionImageFilter.hxx:185-279) and
    * FDKBackProjectionImageFilter::DynamicThreadedGenerateData
    * (include/rtkFDKBackProjectionImageFilter.hxx:52-148) with their optimised
-   * paths (:152-306 and :352-475): u = (M0.x)/(M2.x), v = (M1.x)/(M2.x);
+   * paths (:152-306 and :352-475): RTK's u = (M0.x)/(M2.x), v = (M1.x)/(M2.x)
+   * and weight (1/(M2.x))^2 after normalisation at the rotation centre are
+   * computed here by bp_frame_map (the same quantities, derived from the
+   * source and the detector frame instead of RTK's composed matrix);
    * optimised paths accept 0 <= floor(u) < Nu-1 and 0 <= floor(v) < Nv-1,
-   * the generic path accepts [-0.5, N-0.5) with clamp-to-edge interpolation;
-   * FDK weights each sample by (1/(M2.x))^2 after normalisation. */
+   * the generic path accepts [-0.5, N-0.5) with clamp-to-edge interpolation. */
   const int  nx = vol->size[0], ny = vol->size[1], nz = vol->size[2];
   const int  nu = proj->size[0], nv = proj->size[1], np = proj->size[2];
   const long nvox = npix(vol);
@@ -595,42 +757,34 @@ orc_backproject(const orc_geometry * g, const orc_image * vol, const orc_image *
     }
     return;
   }
-  double * mats = (double *)malloc(sizeof(double) * 12 * (np > 0 ? np : 1));
-  int *    modes = (int *)malloc(sizeof(int) * (np > 0 ? np : 1));
+  /* Flat panels.  The voxel -> pixel map is derived here from the geometry's
+   * frame, not from RTK's composed index-to-index matrix (orc_bp_matrix, kept
+   * as a separate restatement and checked against this derivation): the ray
+   * from the source through the voxel centre meets the detector plane. */
+  bp_frame_t * fr = (bp_frame_t *)malloc(sizeof(bp_frame_t) * (np > 0 ? np : 1));
   for (int s = 0; s < np; s++)
-  {
-    modes[s] = orc_bp_matrix(g, vol, proj, proj->index[2] + s, fdk, mats + 12 * s);
-    double * m = mats + 12 * s;
-    if (modes[s] == 1)
-    {
-      m[0] = 0.;
-      m[8] = 0.;
-    }
-    else if (modes[s] == 2)
-    {
-      m[1] = 0.;
-      m[9] = 0.;
-    }
-  }
-  const double pi0 = proj->index[0], pi1 = proj->index[1];
+    bp_frame(g, vol, proj, proj->index[2] + s, fdk, fr + s);
+  double i2p[16];
+  orc_index_to_physical(vol, i2p);
 #pragma omp parallel for num_threads(nthreads) schedule(dynamic, 1)
   for (int k = 0; k < nz; k++)
   {
     for (int s = 0; s < np; s++)
     {
-      const double * m = mats + 12 * s;
-      const double * p = proj_data + (long)s * nu * nv;
+      const bp_frame_t * f = fr + s;
+      const double *     p = proj_data + (long)s * nu * nv;
       for (int j = 0; j < ny; j++)
         for (int i = 0; i < nx; i++)
         {
-          const double x = i + vol->index[0], y = j + vol->index[1], z = k + vol->index[2];
-          const double w = m[8] * x + m[9] * y + m[10] * z + m[11];
-          const double rw = 1. / w;
-          const double u = (m[0] * x + m[1] * y + m[2] * z + m[3]) * rw - pi0;
-          const double v = (m[4] * x + m[5] * y + m[6] * z + m[7]) * rw - pi1;
-          const long   o = ((long)k * ny + j) * nx + i;
-          const double wt = fdk ? rw * rw : 1.;
-          if (modes[s])
+          const double idx[3] = { i + vol->index[0], j + vol->index[1], k + vol->index[2] };
+          double       X[3], u, v, wt;
+          for (int a = 0; a < 3; a++)
+            X[a] = i2p[a * 4 + 0] * idx[0] + i2p[a * 4 + 1] * idx[1] + i2p[a * 4 + 2] * idx[2] + i2p[a * 4 + 3];
+          bp_frame_map(f, X, &u, &v, &wt);
+          u -= proj->index[0];
+          v -= proj->index[1];
+          const long o = ((long)k * ny + j) * nx + i;
+          if (f->mode)
           {
             const int iu = (int)floor(u), iv = (int)floor(v);
             if (iu >= 0 && iu < nu - 1 && iv >= 0 && iv < nv - 1)
@@ -645,8 +799,7 @@ orc_backproject(const orc_geometry * g, const orc_image * vol, const orc_image *
         }
     }
   }
-  free(mats);
-  free(modes);
+  free(fr);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -700,6 +853,8 @@ typedef struct
 {
   double pix2vol[16]; /* projection index -> volume index (homogeneous) */
   double src[3];      /* source in volume index coordinates */
+  int    parallel;    /* parallel beam: every pixel has its own source */
+  double s2p[3];      /* parallel beam: pixel - source, volume index coordinates */
   double radius;      /* cylindrical panel radius, 0: flat */
   double idx2det[16]; /* cylindrical: projection index -> flat detector coordinates */
   double det2vol[16]; /* cylindrical: detector coordinates -> volume index */
@@ -721,6 +876,20 @@ joseph_setup(const orc_geometry * g, const orc_image * vol, const orc_image * pr
   jp->src[0] = sv[0];
   jp->src[1] = sv[1];
   jp->src[2] = sv[2];
+  /* ProjectionsRegionConstIteratorRayBased::New picks the parallel iterator
+   * when the SDD is 0 (include/rtkProjectionsRegionConstIteratorRayBased.hxx:86-98).
+   * ...Parallel::NewProjection (include/rtkProjectionsRegionConstIteratorRayBasedParallel.hxx:40-60):
+   * SourceToPixel = -2 SID x (row 2 of the rotation matrix), mapped by the
+   * 3x3 part of the volume's physical-to-index matrix; NewPixel puts the
+   * source at pixel - SourceToPixel, so every ray is parallel to that row. */
+  jp->parallel = g->par[10 * i + P_SDD] == 0.;
+  if (jp->parallel)
+  {
+    const double * R = g->rot + 16 * i + 8;
+    const double   sid = g->par[10 * i + P_SID];
+    for (int a = 0; a < 3; a++)
+      jp->s2p[a] = -2. * sid * (vpp2i[a * 4 + 0] * R[0] + vpp2i[a * 4 + 1] * R[1] + vpp2i[a * 4 + 2] * R[2]);
+  }
   /* ProjectionsRegionConstIteratorRayBasedWithCylindricalPanel::NewProjection
    * (include/rtkProjectionsRegionConstIteratorRayBasedWithCylindricalPanel.hxx):
    * index -> detector system (GetProjectionCoordinatesToDetectorSystemMatrix x
@@ -762,8 +931,8 @@ joseph_ray(const orc_image * vol, const joseph_proj_t * jp, double iu, double iv
     for (int a = 0; a < 3; a++)
       pix[a] = jp->pix2vol[a * 4 + 0] * iu + jp->pix2vol[a * 4 + 1] * iv + jp->pix2vol[a * 4 + 2] * ik +
                jp->pix2vol[a * 4 + 3];
-  for (int a = 0; a < 3; a++)
-    dir[a] = -(pix[a] - jp->src[a]);
+  for (int a = 0; a < 3; a++) /* dirVox = -SourceToPixel */
+    dir[a] = jp->parallel ? -jp->s2p[a] : -(pix[a] - jp->src[a]);
   int mainDir = 0;
   for (int a = 0; a < 3; a++)
     if (fabs(dir[a]) > fabs(dir[mainDir]))
@@ -952,16 +1121,13 @@ orc_joseph_forward(const orc_geometry * g, const orc_image * vol, const double *
   }
 }
 
-void
-orc_joseph_back(const orc_geometry * g, const orc_image * vol, const double * vol_in, double * vol_out,
-                const orc_image * proj, const double * proj_data)
+/* Joseph back projection of stack slices [s0, s1) added into vol_out. */
+static void
+joseph_back_slices(const orc_geometry * g, const orc_image * vol, double * vol_out, const orc_image * proj,
+                   const double * proj_data, int s0, int s1)
 {
-  /* JosephBackProjectionImageFilter::GenerateData,
-   * include/rtkJosephBackProjectionImageFilter.hxx:57-323 (single-threaded) */
-  const int nu = proj->size[0], nv = proj->size[1], np = proj->size[2];
-  if (vol_out != vol_in)
-    memcpy(vol_out, vol_in, sizeof(double) * npix(vol));
-  for (int s = 0; s < np; s++)
+  const int nu = proj->size[0], nv = proj->size[1];
+  for (int s = s0; s < s1; s++)
   {
     joseph_proj_t jp;
     joseph_setup(g, vol, proj, proj->index[2] + s, &jp);
@@ -1011,6 +1177,61 @@ orc_joseph_back(const orc_geometry * g, const orc_image * vol, const double * vo
         }
       }
   }
+}
+
+void
+orc_joseph_back(const orc_geometry * g, const orc_image * vol, const double * vol_in, double * vol_out,
+                const orc_image * proj, const double * proj_data)
+{
+  /* JosephBackProjectionImageFilter::GenerateData,
+   * include/rtkJosephBackProjectionImageFilter.hxx:57-323 (single-threaded) */
+  if (vol_out != vol_in)
+    memcpy(vol_out, vol_in, sizeof(double) * npix(vol));
+  joseph_back_slices(g, vol, vol_out, proj, proj_data, 0, proj->size[2]);
+}
+
+void
+orc_joseph_back_mt(const orc_geometry * g, const orc_image * vol, const double * vol_in, double * vol_out,
+                   const orc_image * proj, const double * proj_data, int nthreads)
+{
+  /* the same sum split over threads by projection, each into its own FP64
+   * volume, added together at the end (RTK's filter is single-threaded; only
+   * the FP64 summation order differs) */
+  const long nvx = npix(vol);
+  const int  np = proj->size[2];
+  if (vol_out != vol_in)
+    memcpy(vol_out, vol_in, sizeof(double) * nvx);
+  if (nthreads > np)
+    nthreads = np;
+  if (nthreads <= 1)
+  {
+    joseph_back_slices(g, vol, vol_out, proj, proj_data, 0, np);
+    return;
+  }
+  double ** part = (double **)calloc(nthreads, sizeof(double *));
+#pragma omp parallel num_threads(nthreads)
+  {
+#ifdef _OPENMP
+    const int t = omp_get_thread_num(), nt = omp_get_num_threads();
+#else
+    const int t = 0, nt = 1;
+#endif
+    double * acc = (double *)calloc(nvx, sizeof(double));
+    part[t] = acc;
+    joseph_back_slices(g, vol, acc, proj, proj_data, (int)((long)np * t / nt), (int)((long)np * (t + 1) / nt));
+  }
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+  for (long q = 0; q < nvx; q++)
+  {
+    double v = vol_out[q];
+    for (int t = 0; t < nthreads; t++)
+      if (part[t])
+        v += part[t][q];
+    vol_out[q] = v;
+  }
+  for (int t = 0; t < nthreads; t++)
+    free(part[t]);
+  free(part);
 }
 
 double
@@ -1525,10 +1746,24 @@ orc_laplacian(const orc_image * vol, const double * x, double * out)
       }
 }
 
+/* The CG's back projector (IterativeConeBeamReconstructionFilter's
+ * InstantiateBackProjectionFilter, include/rtkIterativeConeBeamReconstructionFilter.hxx:33-103):
+ * 0 Joseph (BP_JOSEPH), 1 voxel-based (BP_VOXELBASED, rtkconjugategradient's
+ * default); out += BP(p). */
+static void
+cg_backproject(const orc_geometry * g, const orc_image * vol, const orc_image * proj, const double * p, double * out,
+               int backprojector, int nthreads)
+{
+  if (backprojector == 1)
+    orc_backproject(g, vol, proj, p, out, out, 0, nthreads);
+  else
+    orc_joseph_back_mt(g, vol, out, out, proj, p, nthreads);
+}
+
 static void
 cg_apply_A(const orc_geometry * g, const orc_image * vol, const orc_image * proj, const double * weights,
            const double * mask, double tikhonov, double gamma, const double * x_in, double * out, double * ptmp,
-           int nthreads)
+           int backprojector, int nthreads)
 {
   /* ReconstructionConjugateGradientOperator::GenerateData,
    * include/rtkReconstructionConjugateGradientOperator.hxx:192-311:
@@ -1550,7 +1785,7 @@ cg_apply_A(const orc_geometry * g, const orc_image * vol, const orc_image * proj
     for (long q = 0; q < np; q++)
       ptmp[q] *= weights[q];
   memset(out, 0, sizeof(double) * nvx);
-  orc_joseph_back(g, vol, out, out, proj, ptmp);
+  cg_backproject(g, vol, proj, ptmp, out, backprojector, nthreads);
   if (gamma != 0.)
   {
     double * lap = (double *)malloc(sizeof(double) * nvx);
@@ -1571,9 +1806,9 @@ cg_apply_A(const orc_geometry * g, const orc_image * vol, const orc_image * proj
 }
 
 void
-orc_cg_joseph(const orc_geometry * g, const orc_image * vol, const orc_image * proj, const double * proj_data,
-              const double * weights, const double * mask, double tikhonov, double gamma, int niter, double * x,
-              double * residuals, int nthreads)
+orc_cg(const orc_geometry * g, const orc_image * vol, const orc_image * proj, const double * proj_data,
+       const double * weights, const double * mask, double tikhonov, double gamma, int niter, double * x,
+       double * residuals, int backprojector, int nthreads)
 {
   /* with a support mask M (ConjugateGradientConeBeamReconstructionFilter,
    * include/rtkConjugateGradientConeBeamReconstructionFilter.hxx:246-258): b is
@@ -1591,11 +1826,11 @@ orc_cg_joseph(const orc_geometry * g, const orc_image * vol, const orc_image * p
   double *   AP = (double *)malloc(sizeof(double) * nvx);
   for (long q = 0; q < np; q++)
     ptmp[q] = proj_data[q] * (weights ? weights[q] : 1.);
-  orc_joseph_back(g, vol, b, b, proj, ptmp);
+  cg_backproject(g, vol, proj, ptmp, b, backprojector, nthreads);
   if (mask)
     for (long q = 0; q < nvx; q++)
       b[q] *= mask[q];
-  cg_apply_A(g, vol, proj, weights, mask, tikhonov, gamma, x, AP, ptmp, nthreads);
+  cg_apply_A(g, vol, proj, weights, mask, tikhonov, gamma, x, AP, ptmp, backprojector, nthreads);
   for (long q = 0; q < nvx; q++)
   {
     R[q] = b[q] - AP[q];
@@ -1609,7 +1844,7 @@ orc_cg_joseph(const orc_geometry * g, const orc_image * vol, const orc_image * p
     residuals[0] = rr;
   for (int it = 0; it < niter; it++)
   {
-    cg_apply_A(g, vol, proj, weights, mask, tikhonov, gamma, P, AP, ptmp, nthreads);
+    cg_apply_A(g, vol, proj, weights, mask, tikhonov, gamma, P, AP, ptmp, backprojector, nthreads);
     double num = 0., den = 0.;
     for (long q = 0; q < nvx; q++)
     {
@@ -1642,6 +1877,14 @@ orc_cg_joseph(const orc_geometry * g, const orc_image * vol, const orc_image * p
   free(AP);
 }
 
+void
+orc_cg_joseph(const orc_geometry * g, const orc_image * vol, const orc_image * proj, const double * proj_data,
+              const double * weights, const double * mask, double tikhonov, double gamma, int niter, double * x,
+              double * residuals, int nthreads)
+{
+  orc_cg(g, vol, proj, proj_data, weights, mask, tikhonov, gamma, niter, x, residuals, 0, nthreads);
+}
+
 /* ------------------------------------------------------------------------ */
 /* phantoms                                                                 */
 /* ------------------------------------------------------------------------ */
@@ -1664,26 +1907,31 @@ orc_project_ellipsoids(const orc_geometry * g, const orc_image * proj, int n_ell
     orc_geometry_source_position(g, k, src);
     if (g->radius_cyl != 0.)
       cyl_matrices(g, k, pi2pp, idx2det, inv);
+    double s2p[3];
+    const int parallel = parallel_source_to_pixel(g, k, s2p);
 #pragma omp parallel for num_threads(nthreads) schedule(dynamic, 4)
     for (int j = 0; j < nv; j++)
       for (int i = 0; i < nu; i++)
       {
         const double ii = i + proj->index[0], jj = j + proj->index[1], kk = k;
-        double       pix[3], d[3];
+        double       pix[3], d[3], srcp[3];
         if (g->radius_cyl != 0.)
           cyl_pixel(idx2det, inv, g->radius_cyl, ii, jj, kk, pix);
         else
           for (int a = 0; a < 3; a++)
             pix[a] = T[a * 4 + 0] * ii + T[a * 4 + 1] * jj + T[a * 4 + 2] * kk + T[a * 4 + 3];
         for (int a = 0; a < 3; a++)
-          d[a] = pix[a] - src[a];
+        {
+          srcp[a] = parallel ? pix[a] - s2p[a] : src[a];
+          d[a] = pix[a] - srcp[a];
+        }
         const double len = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
         double       acc = 0.;
         for (int e = 0; e < n_ell; e++)
         {
           const double * E = ell + 16 * e;
           const double * R = E + 6;
-          double         o[3], dd[3], rel[3] = { src[0] - E[0], src[1] - E[1], src[2] - E[2] };
+          double         o[3], dd[3], rel[3] = { srcp[0] - E[0], srcp[1] - E[1], srcp[2] - E[2] };
           for (int a = 0; a < 3; a++)
           {
             /* local = R^T (world - c), scaled by 1/axis */
@@ -1856,19 +2104,25 @@ ray_box_impl(const orc_geometry * g, const orc_image * proj, const double * D, c
     orc_geometry_proj_coords_to_fixed(g, k, p2f);
     mat_mul(p2f, pi2pp, T, 4, 4, 4);
     orc_geometry_source_position(g, k, src);
+    double    s2p[3];
+    const int parallel = parallel_source_to_pixel(g, k, s2p);
 #pragma omp parallel for num_threads(nthreads) schedule(dynamic, 4)
     for (int j = 0; j < nv; j++)
       for (int i = 0; i < nu; i++)
       {
         const double ii = i + proj->index[0], jj = j + proj->index[1], kk = k;
-        double       d[3];
+        double       d[3], srcp[3];
         for (int a = 0; a < 3; a++)
-          d[a] = T[a * 4 + 0] * ii + T[a * 4 + 1] * jj + T[a * 4 + 2] * kk + T[a * 4 + 3] - src[a];
+        {
+          const double pix = T[a * 4 + 0] * ii + T[a * 4 + 1] * jj + T[a * 4 + 2] * kk + T[a * 4 + 3];
+          srcp[a] = parallel ? pix - s2p[a] : src[a];
+          d[a] = pix - srcp[a];
+        }
         const double len = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
         double       org[3], dir[3];
         for (int a = 0; a < 3; a++)
         {
-          org[a] = D[0 * 3 + a] * src[0] + D[1 * 3 + a] * src[1] + D[2 * 3 + a] * src[2];
+          org[a] = D[0 * 3 + a] * srcp[0] + D[1 * 3 + a] * srcp[1] + D[2 * 3 + a] * srcp[2];
           dir[a] = (D[0 * 3 + a] * d[0] + D[1 * 3 + a] * d[1] + D[2 * 3 + a] * d[2]) / len;
         }
         double inf = -DBL_MAX, sup = DBL_MAX;

@@ -70,6 +70,13 @@ void orc_physical_to_index(const orc_image * im, double m[16]);
  * 1 = optimised X, 2 = optimised Y, 0 = generic interpolator path. */
 int  orc_bp_matrix(const orc_geometry * g, const orc_image * vol, const orc_image * proj, int i, int fdk,
                    double m[12]);
+/* Independent voxel -> pixel map (the ray from the source through the
+ * physical point meets the detector plane, from the source position and the
+ * detector frame): out = (u, v) absolute continuous projection index of
+ * projection k, and the FDK weight (1 when fdk == 0); returns the path mode as
+ * orc_bp_matrix does.  orc_backproject uses this map for flat panels. */
+int  orc_bp_project(const orc_geometry * g, const orc_image * vol, const orc_image * proj, int k, int fdk,
+                    const double * physical, double out[3]);
 /* vol_out = vol_in + sum over projections.  proj data = stack buffer; stack
  * slice s is geometry projection proj->index[2] + s. */
 void orc_backproject(const orc_geometry * g, const orc_image * vol, const orc_image * proj, const double * proj_data,
@@ -81,6 +88,9 @@ void   orc_joseph_forward(const orc_geometry * g, const orc_image * vol, const d
                           const orc_image * proj, const double * proj_in, double * proj_out, int nthreads);
 void   orc_joseph_back(const orc_geometry * g, const orc_image * vol, const double * vol_in, double * vol_out,
                        const orc_image * proj, const double * proj_data);
+/* the same back projection split over nthreads (FP64 partial volumes) */
+void   orc_joseph_back_mt(const orc_geometry * g, const orc_image * vol, const double * vol_in, double * vol_out,
+                          const orc_image * proj, const double * proj_data, int nthreads);
 /* Number of bilinear samples the Joseph forward projector takes (work count). */
 double orc_joseph_sample_count(const orc_geometry * g, const orc_image * vol, const orc_image * proj, int nthreads);
 
@@ -121,6 +131,12 @@ void orc_ramp_filter(const orc_image * proj, const orc_ramp_params * p, const do
 /* A x = BP(W .* FP(x)) + tikhonov * x with the Joseph pair; b = BP(W .* p).
  * Runs niter iterations from x (in/out).  residuals[k] = ||r_k||^2 for
  * k = 0..niter (may be NULL).  weights may be NULL (all ones). */
+/* orc_cg_joseph with the back projector chosen as RTK's iterative filters
+ * choose it: backprojector 0 = Joseph, 1 = voxel-based (not the exact adjoint
+ * of the Joseph forward projector; RTK's rtkconjugategradient default). */
+void orc_cg(const orc_geometry * g, const orc_image * vol, const orc_image * proj, const double * proj_data,
+            const double * weights, const double * mask, double tikhonov, double gamma, int niter, double * x,
+            double * residuals, int backprojector, int nthreads);
 void orc_cg_joseph(const orc_geometry * g, const orc_image * vol, const orc_image * proj, const double * proj_data,
                    const double * weights, const double * mask, double tikhonov, double gamma, int niter, double * x,
                    double * residuals, int nthreads);

@@ -142,7 +142,8 @@ def check(code: int) -> None:
 class CgParams(C.Structure):
     """rtkb_cg_params."""
 
-    _fields_ = [("tikhonov", C.c_double), ("use_cuda_graph", C.c_int), ("storage", C.c_int), ("gamma", C.c_double)]
+    _fields_ = [("tikhonov", C.c_double), ("use_cuda_graph", C.c_int), ("storage", C.c_int), ("gamma", C.c_double),
+                ("backprojector", C.c_int)]
 
 
 SIGNATURES.update({

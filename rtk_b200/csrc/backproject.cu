@@ -24,6 +24,7 @@
 //    accuracy; a tile whose footprint does not fit the box (or whose corners
 //    are not all in front of the source) falls back to an FP64 global-memory
 //    path for that projection.
+#include "rtkb_backproject.h"
 #include "rtkb_internal.h"
 #include "rtkb_ptx.cuh"
 
@@ -894,11 +895,15 @@ to_buffer_matrix(const rtkb_image_desc & vol, const rtkb_image_desc & proj, int 
   std::memcpy(out, m, sizeof(m));
 }
 
+// Host half of a backprojection: argument checks, RTK's path per projection
+// (the tiled kernel needs optimised-Y everywhere), the tile configuration from
+// footprints probed on the host, and the TMA descriptor of the stack.  No
+// device work: the launch half (bp_launch) can run later, and inside a stream
+// capture, as long as d_proj keeps its address.
 template <typename T>
 int
-backproject_buffer(const int vol_size[3], const int proj_size[3], int nproj, const double * mats, const int * modes,
-                   bool fdk, const T * d_proj, const float * d_vin, float * d_vout, cudaStream_t st,
-                   void * fixed_scratch = nullptr)
+bp_prepare(const int vol_size[3], const int proj_size[3], int nproj, const double * mats, const int * modes, bool fdk,
+           const T * d_proj, BpPrepared & out)
 {
   constexpr bool    kBf16 = sizeof(T) == 2;
   const BpConfig *  configs = kBf16 ? kBpConfigsBf16 : kBpConfigs;
@@ -907,15 +912,17 @@ backproject_buffer(const int vol_size[3], const int proj_size[3], int nproj, con
   const int nu = proj_size[0], nv = proj_size[1];
   if (nx <= 0 || ny <= 0 || nz <= 0 || nu <= 0 || nv <= 0 || nproj < 0 || proj_size[2] < nproj)
     return fail(RTKB_ERR_INVALID_ARGUMENT, "invalid sizes");
-  if (!d_vin || !d_vout || (nproj > 0 && !d_proj) || (nproj > 0 && (!mats || !modes)))
+  if (nproj > 0 && (!d_proj || !mats || !modes))
     return fail(RTKB_ERR_INVALID_ARGUMENT, "null buffer");
-  const long long nvox = (long long)nx * ny * nz;
-  if (nproj == 0)
-  {
-    if (d_vout != d_vin)
-      RTKB_CUDA_TRY(cudaMemcpyAsync(d_vout, d_vin, nvox * sizeof(float), cudaMemcpyDeviceToDevice, st));
-    return RTKB_OK;
-  }
+  out = BpPrepared{};
+  out.nproj = nproj;
+  out.nu = nu;
+  out.nv = nv;
+  out.np_total = proj_size[2];
+  out.nx = nx;
+  out.ny = ny;
+  out.nz = nz;
+  out.fdk = fdk;
   bool all_opt_y = true;
   for (int p = 0; p < nproj; p++)
   {
@@ -925,82 +932,109 @@ backproject_buffer(const int vol_size[3], const int proj_size[3], int nproj, con
     if (modes[p] != 2)
       all_opt_y = false;
   }
+  if (nproj == 0)
+    return RTKB_OK;
+  if (!all_opt_y)
+  {
+    out.generic = true;
+    return RTKB_OK;
+  }
+  // first configuration whose box holds the footprints probed on the host
+  std::vector<double> mv(mats, mats + 12 * (size_t)nproj);
+  double              fw[3], fh[3]; // columns of 8, 16, 24 voxels
+  for (int q = 0; q < 3; q++)
+    estimate_footprint(mv, nproj, nx, ny, nz, 8 * (q + 1), fw[q], fh[q]);
+  int cfg = kNumBpConfigs - 1;
+  for (int c = 0; c < kNumBpConfigs; c++)
+  {
+    const int q = configs[c].nyt / 8 - 1;
+    if (fw[q] + kSlack < configs[c].bw - 1 && fh[q] + 0.2 < configs[c].bh - 1)
+    {
+      cfg = c;
+      break;
+    }
+  }
+  if (g_bp_forced_config >= 0)
+    cfg = g_bp_forced_config; // a box too small for some tiles only sends them to the FP64 path
+  g_bp_last_config = cfg;
+  out.cfg = cfg;
+  // TMA needs 16-byte aligned rows and base address
+  std::memset(&out.tmap, 0, sizeof(out.tmap));
+  EncodeTiledFn            enc = tensor_map_encoder();
+  const long long          np_total = proj_size[2];
+  const unsigned long long esz = sizeof(T);
+  if (enc && ((unsigned long long)nu * esz) % 16 == 0 && (reinterpret_cast<uintptr_t>(d_proj) % 16) == 0 &&
+      np_total <= 0x7fffffffLL)
+  {
+    const unsigned long long dims[3] = { (unsigned long long)nu, (unsigned long long)nv, (unsigned long long)np_total };
+    const unsigned long long strides[2] = { (unsigned long long)nu * esz, (unsigned long long)nu * nv * esz };
+    const unsigned           box[3] = { (unsigned)configs[cfg].bw, (unsigned)configs[cfg].bh, 1u };
+    const unsigned           estr[3] = { 1u, 1u, 1u };
+    const int r = enc(&out.tmap, kBf16 ? (int)CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : (int)CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                      3u, const_cast<T *>(d_proj), dims, strides, box, estr, (int)CU_TENSOR_MAP_INTERLEAVE_NONE,
+                      (int)CU_TENSOR_MAP_SWIZZLE_NONE, (int)CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                      (int)CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    out.use_tma = (r == 0);
+  }
+  return RTKB_OK;
+}
+
+// Device half: d_vout = d_vin + BP(d_proj) with the matrices and modes already
+// in device memory (d_vin may equal d_vout).  Stream-ordered launches only.
+template <typename T>
+int
+bp_launch(const BpPrepared & b, const T * d_proj, const double * d_mats, const int * d_modes, const float * d_vin,
+          float * d_vout, cudaStream_t st)
+{
+  const long long nvox = (long long)b.nx * b.ny * b.nz;
+  if (b.nproj == 0)
+  {
+    if (d_vout != d_vin)
+      RTKB_CUDA_TRY(cudaMemcpyAsync(d_vout, d_vin, nvox * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    return RTKB_OK;
+  }
+  if (b.generic)
+  {
+    const long long blocks = std::min<long long>((nvox + 255) / 256, 148LL * 64);
+    if (b.fdk)
+      bp_generic_kernel<true, T><<<(unsigned)blocks, 256, 0, st>>>(d_proj, d_mats, d_modes, b.nproj, b.nu, b.nv, b.nx,
+                                                                   b.ny, b.nz, d_vin, d_vout);
+    else
+      bp_generic_kernel<false, T><<<(unsigned)blocks, 256, 0, st>>>(d_proj, d_mats, d_modes, b.nproj, b.nu, b.nv, b.nx,
+                                                                    b.ny, b.nz, d_vin, d_vout);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? RTKB_OK : cuda_fail(e, "bp_generic_kernel launch");
+  }
+  return b.fdk ? dispatch_tiled<true>(b.cfg, b.tmap, b.use_tma, d_proj, d_mats, b.nproj, b.nu, b.nv, b.nx, b.ny, b.nz,
+                                      d_vin, d_vout, st)
+               : dispatch_tiled<false>(b.cfg, b.tmap, b.use_tma, d_proj, d_mats, b.nproj, b.nu, b.nv, b.nx, b.ny, b.nz,
+                                       d_vin, d_vout, st);
+}
+
+template <typename T>
+int
+backproject_buffer(const int vol_size[3], const int proj_size[3], int nproj, const double * mats, const int * modes,
+                   bool fdk, const T * d_proj, const float * d_vin, float * d_vout, cudaStream_t st,
+                   void * fixed_scratch = nullptr)
+{
+  if (!d_vin || !d_vout)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "null buffer");
+  BpPrepared b;
+  int        rc = bp_prepare(vol_size, proj_size, nproj, mats, modes, fdk, d_proj, b);
+  if (rc != RTKB_OK || nproj == 0)
+    return rc != RTKB_OK ? rc : bp_launch<T>(b, d_proj, nullptr, nullptr, d_vin, d_vout, st);
   // matrices and modes in one scratch block: the caller's when given, else a
   // stream-ordered allocation
   const size_t mbytes = sizeof(double) * 12 * (size_t)nproj;
   void *       scratch = fixed_scratch;
   if (!scratch)
     RTKB_CUDA_TRY(rtkb::scratch_malloc(&scratch, mbytes + sizeof(int) * nproj, st));
-  double * d_mats = static_cast<double *>(scratch);
-  int *    d_modes = reinterpret_cast<int *>(static_cast<char *>(scratch) + mbytes);
-  int      rc = RTKB_OK;
-  do
-  {
-    cudaError_t e = cudaMemcpyAsync(d_mats, mats, mbytes, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(d_modes, modes, sizeof(int) * nproj, cudaMemcpyHostToDevice, st);
-    if (e != cudaSuccess)
-    {
-      rc = cuda_fail(e, "cudaMemcpyAsync");
-      break;
-    }
-    if (!all_opt_y)
-    {
-      const long long blocks = std::min<long long>((nvox + 255) / 256, 148LL * 64);
-      if (fdk)
-        bp_generic_kernel<true, T><<<(unsigned)blocks, 256, 0, st>>>(d_proj, d_mats, d_modes, nproj, nu, nv, nx, ny,
-                                                                     nz, d_vin, d_vout);
-      else
-        bp_generic_kernel<false, T><<<(unsigned)blocks, 256, 0, st>>>(d_proj, d_mats, d_modes, nproj, nu, nv, nx, ny,
-                                                                      nz, d_vin, d_vout);
-      e = cudaGetLastError();
-      if (e != cudaSuccess)
-        rc = cuda_fail(e, "bp_generic_kernel launch");
-      break;
-    }
-    // first configuration whose box holds the footprints probed on the host
-    std::vector<double> mv(mats, mats + 12 * (size_t)nproj);
-    double              fw[3], fh[3]; // columns of 8, 16, 24 voxels
-    for (int q = 0; q < 3; q++)
-      estimate_footprint(mv, nproj, nx, ny, nz, 8 * (q + 1), fw[q], fh[q]);
-    int cfg = kNumBpConfigs - 1;
-    for (int c = 0; c < kNumBpConfigs; c++)
-    {
-      const int q = configs[c].nyt / 8 - 1;
-      if (fw[q] + kSlack < configs[c].bw - 1 && fh[q] + 0.2 < configs[c].bh - 1)
-      {
-        cfg = c;
-        break;
-      }
-    }
-    if (g_bp_forced_config >= 0)
-      cfg = g_bp_forced_config; // a box too small for some tiles only sends them to the FP64 path
-    g_bp_last_config = cfg;
-    // TMA needs 16-byte aligned rows and base address
-    CUtensorMap tmap;
-    std::memset(&tmap, 0, sizeof(tmap));
-    bool              use_tma = false;
-    EncodeTiledFn     enc = tensor_map_encoder();
-    const long long   np_total = proj_size[2];
-    const unsigned long long esz = sizeof(T);
-    if (enc && ((unsigned long long)nu * esz) % 16 == 0 && (reinterpret_cast<uintptr_t>(d_proj) % 16) == 0 &&
-        np_total <= 0x7fffffffLL)
-    {
-      const unsigned long long dims[3] = { (unsigned long long)nu, (unsigned long long)nv,
-                                           (unsigned long long)np_total };
-      const unsigned long long strides[2] = { (unsigned long long)nu * esz, (unsigned long long)nu * nv * esz };
-      const unsigned           box[3] = { (unsigned)configs[cfg].bw, (unsigned)configs[cfg].bh, 1u };
-      const unsigned           estr[3] = { 1u, 1u, 1u };
-      const int r = enc(&tmap, kBf16 ? (int)CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : (int)CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
-                        3u, const_cast<T *>(d_proj), dims, strides,
-                        box, estr, (int)CU_TENSOR_MAP_INTERLEAVE_NONE, (int)CU_TENSOR_MAP_SWIZZLE_NONE,
-                        (int)CU_TENSOR_MAP_L2_PROMOTION_L2_128B, (int)CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-      use_tma = (r == 0);
-    }
-    rc = fdk ? dispatch_tiled<true>(cfg, tmap, use_tma, d_proj, d_mats, nproj, nu, nv, nx, ny, nz, d_vin, d_vout, st)
-             : dispatch_tiled<false>(cfg, tmap, use_tma, d_proj, d_mats, nproj, nu, nv, nx, ny, nz, d_vin, d_vout,
-                                     st);
-  } while (0);
+  double *    d_mats = static_cast<double *>(scratch);
+  int *       d_modes = reinterpret_cast<int *>(static_cast<char *>(scratch) + mbytes);
+  cudaError_t e = cudaMemcpyAsync(d_mats, mats, mbytes, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_modes, modes, sizeof(int) * nproj, cudaMemcpyHostToDevice, st);
+  rc = e == cudaSuccess ? bp_launch<T>(b, d_proj, d_mats, d_modes, d_vin, d_vout, st) : cuda_fail(e, "cudaMemcpyAsync");
   if (!fixed_scratch)
   {
     cudaError_t fe = rtkb::scratch_free(scratch, st);
@@ -1008,6 +1042,47 @@ backproject_buffer(const int vol_size[3], const int proj_size[3], int nproj, con
       rc = cuda_fail(fe, "cudaFreeAsync");
   }
   return rc;
+}
+
+// The voxel-based back projector as a reusable object (the CG plan's
+// BP_VOXELBASED choice): matrices and modes uploaded once at creation into
+// device memory the caller owns, launches replayable inside a CUDA graph.
+size_t
+voxel_backprojector_bytes(int nproj)
+{
+  return ((sizeof(double) * 12 + sizeof(int)) * (size_t)std::max(nproj, 1) + 255) & ~size_t(255);
+}
+
+int
+voxel_backprojector_create(const rtkb_geometry * g, const rtkb_image_desc & vol, const rtkb_image_desc & proj,
+                           const float * d_proj, void * d_mem, VoxelBackprojector & out)
+{
+  if (g->g.radius_cylindrical != 0.)
+    return fail(RTKB_ERR_UNSUPPORTED, "the reusable voxel-based back projector models flat panels only");
+  const int           nproj = proj.size[2];
+  std::vector<double> mats(12 * (size_t)std::max(nproj, 1));
+  std::vector<int>    modes(std::max(nproj, 1));
+  for (int s = 0; s < nproj; s++)
+  {
+    double m[12];
+    modes[s] = bp_matrix(g->g, vol, proj, proj.index[2] + s, false, m);
+    to_buffer_matrix(vol, proj, modes[s], m, mats.data() + 12 * s);
+  }
+  int rc = bp_prepare<float>(vol.size, proj.size, nproj, mats.data(), modes.data(), false, d_proj, out.prep);
+  if (rc != RTKB_OK)
+    return rc;
+  out.d_proj = d_proj;
+  out.d_mats = static_cast<double *>(d_mem);
+  out.d_modes = reinterpret_cast<int *>(static_cast<char *>(d_mem) + sizeof(double) * 12 * (size_t)std::max(nproj, 1));
+  RTKB_CUDA_TRY(cudaMemcpy(out.d_mats, mats.data(), sizeof(double) * mats.size(), cudaMemcpyHostToDevice));
+  RTKB_CUDA_TRY(cudaMemcpy(out.d_modes, modes.data(), sizeof(int) * modes.size(), cudaMemcpyHostToDevice));
+  return RTKB_OK;
+}
+
+int
+voxel_backprojector_launch(const VoxelBackprojector & b, const float * d_vin, float * d_vout, cudaStream_t st)
+{
+  return bp_launch<float>(b.prep, b.d_proj, b.d_mats, b.d_modes, d_vin, d_vout, st);
 }
 
 template <typename T>

@@ -18,6 +18,8 @@
 #include "rtkb_elem.cuh"
 #include "rtkb_joseph.h"
 
+#include "rtkb_backproject.h"
+
 #include <cfloat>
 #include <cstring>
 #include <vector>
@@ -66,6 +68,9 @@ struct rtkb_cg
   // support mask (SetSupportMask): caller's volume, and the masked operator input
   const float *            mask = nullptr;
   float *                  Mx = nullptr;
+  // voxel-based back projector (BP_VOXELBASED) reading tmp, instead of Joseph's
+  bool                     voxel_bp = false;
+  rtkb::VoxelBackprojector vbp{};
 };
 
 namespace rtkb
@@ -443,6 +448,29 @@ as(float * p)
 
 cudaError_t add_laplacian(rtkb_cg * c, const void * in, Elem ie, void * out, Elem oe, cudaStream_t st);
 
+__global__ void
+scale_kernel(float * __restrict__ out, const float * __restrict__ in, float s, long long n)
+{
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = s * in[i];
+}
+
+// out = BP_voxel(tmp) + tikhonov * x (x may be null: no Tikhonov term); FP32 plans
+cudaError_t
+voxel_bp_into(rtkb_cg * c, const float * x, float * out, cudaStream_t st)
+{
+  if (x)
+    scale_kernel<<<grid_for(c->nvox), 256, 0, st>>>(out, x, c->tikhonov, c->nvox);
+  else
+  {
+    const cudaError_t e = cudaMemsetAsync(out, 0, (size_t)c->nvox * sizeof(float), st);
+    if (e != cudaSuccess)
+      return e;
+  }
+  const int rc = rtkb::voxel_backprojector_launch(c->vbp, out, out, st);
+  return rc == RTKB_OK ? cudaGetLastError() : cudaErrorLaunchFailure;
+}
+
 // out = A in (uses tmp and the projector scratch); in and out have storage
 // ie and oe, tmp the plan's storage
 cudaError_t
@@ -459,8 +487,11 @@ apply_A(rtkb_cg * c, const void * in, Elem ie, void * out, Elem oe, cudaStream_t
   cudaError_t e = rtkb::joseph_forward_launch(c->args, in, ie, c->scratch, nullptr, c->tmp, storage(c), c->W, st);
   if (e != cudaSuccess)
     return e;
-  e = rtkb::joseph_back_launch(c->args, c->tmp, storage(c), c->scratch, nullptr, out, oe,
-                               c->tikhonov != 0.f ? in : nullptr, ie, c->tikhonov, st);
+  if (c->voxel_bp)
+    e = voxel_bp_into(c, c->tikhonov != 0.f ? static_cast<const float *>(in) : nullptr, static_cast<float *>(out), st);
+  else
+    e = rtkb::joseph_back_launch(c->args, c->tmp, storage(c), c->scratch, nullptr, out, oe,
+                                 c->tikhonov != 0.f ? in : nullptr, ie, c->tikhonov, st);
   if (e != cudaSuccess)
     return e;
   if (c->gamma != 0.f)
@@ -610,6 +641,19 @@ rtkb_cg_create(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_
     c->gamma = params ? (float)params->gamma : 0.f;
     c->use_graph = params ? params->use_cuda_graph != 0 : true;
     c->bf16 = params ? params->storage == 1 : false;
+    // RTK's BackProjectionType: BP_VOXELBASED 0 (its default), BP_JOSEPH 1, BP_CUDAVOXELBASED 2
+    const int bpt = params ? params->backprojector : 0;
+    if (bpt < 0 || bpt > 2)
+    {
+      release(c);
+      return fail(RTKB_ERR_UNSUPPORTED, "back projector: BP_VOXELBASED (0), BP_JOSEPH (1) or BP_CUDAVOXELBASED (2)");
+    }
+    c->voxel_bp = bpt != 1;
+    if (c->voxel_bp && (c->bf16 || g->g.radius_cylindrical != 0.))
+    {
+      release(c);
+      return fail(RTKB_ERR_UNSUPPORTED, "the voxel-based back projector in CG needs FP32 storage and a flat panel");
+    }
     c->nvox = num_pixels(*vol);
     c->npix = num_pixels(*proj);
     std::vector<RayProj> tab;
@@ -624,7 +668,8 @@ rtkb_cg_create(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_
     const size_t tb = joseph_table_bytes(tab, cyl), pb = up((size_t)c->npix * 4), vb = up((size_t)c->nvox * 4);
     const size_t sb = up(8 * sizeof(double)), rb = up(kRedBlocks * sizeof(double));
     const size_t fb = up(std::max(joseph_forward_scratch_bytes(c->nvox), joseph_back_scratch_bytes(c->nvox)));
-    const size_t total = tb + 2 * pb + 3 * vb + sb + rb + fb;
+    const size_t xb = c->voxel_bp ? voxel_backprojector_bytes(proj->size[2]) : 0;
+    const size_t total = tb + 2 * pb + 3 * vb + sb + rb + fb + xb;
     cudaError_t  e = cudaMalloc(&c->mem, total);
     if (e == cudaSuccess && c->use_graph)
       e = cudaStreamCreateWithFlags(&c->cap, cudaStreamNonBlocking);
@@ -651,6 +696,16 @@ rtkb_cg_create(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_
     c->partial = reinterpret_cast<double *>(m);
     m += rb;
     c->scratch = m;
+    m += fb;
+    if (c->voxel_bp)
+    {
+      rc = voxel_backprojector_create(g, *vol, *proj, c->tmp, m, c->vbp);
+      if (rc != RTKB_OK)
+      {
+        release(c);
+        return rc;
+      }
+    }
     joseph_args(c->args, *vol, *proj, nullptr);
     e = joseph_upload_tables(tab, cyl, g->g.radius_cylindrical, c->tab, c->args, nullptr);
     if (e == cudaSuccess)
@@ -764,8 +819,9 @@ weights_and_rhs(rtkb_cg * c, const float * d_proj, const float * d_weights, int 
     mul_kernel<__nv_bfloat16><<<grid_for(c->npix), 256, 0, st>>>(as<__nv_bfloat16>(c->tmp), d_proj, c->W, c->npix);
   else
     mul_kernel<float><<<grid_for(c->npix), 256, 0, st>>>(c->tmp, d_proj, c->W, c->npix);
-  cudaError_t e =
-    joseph_back_launch(c->args, c->tmp, storage(c), c->scratch, nullptr, out, oe, nullptr, Elem::F32, 0.f, st);
+  cudaError_t e = c->voxel_bp ? voxel_bp_into(c, nullptr, static_cast<float *>(out), st)
+                              : joseph_back_launch(c->args, c->tmp, storage(c), c->scratch, nullptr, out, oe, nullptr,
+                                                   Elem::F32, 0.f, st);
   if (e == cudaSuccess && c->mask)
   {
     // b = M .* BP(W .* p) (ConjugateGradientConeBeamReconstructionFilter with a support mask)

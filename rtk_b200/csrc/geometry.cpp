@@ -289,6 +289,21 @@ Geometry::inverse_rotation(int i, double out[16]) const
   rotation_inverse(p[i].rot, out);
 }
 
+// ProjectionsRegionConstIteratorRayBasedParallel::NewProjection
+// (include/rtkProjectionsRegionConstIteratorRayBasedParallel.hxx:40-60): with
+// no source-to-detector distance every pixel gets its own source, 2 SID along
+// the detector normal, so all rays of a projection are parallel.
+bool
+Geometry::parallel_source_to_pixel(int i, double out[3]) const
+{
+  const Proj & q = p[i];
+  if (q.sdd != 0.)
+    return false;
+  for (int a = 0; a < 3; a++)
+    out[a] = -2. * q.sid * q.rot[8 + a];
+  return true;
+}
+
 void
 Geometry::proj_coords_to_fixed(int i, double out[16]) const
 {

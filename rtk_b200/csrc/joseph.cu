@@ -74,9 +74,11 @@ setup_ray(const JosephArgs & a, const RayProj & P, int u, int v, int s, bool for
     for (int q = 0; q < 3; q++)
       pix[q] = P.pix2vol[q * 4 + 0] * iu + P.pix2vol[q * 4 + 1] * iv + P.pix2vol[q * 4 + 2] * ik + P.pix2vol[q * 4 + 3];
   }
+  // dirVox = -SourceToPixel; a parallel beam's source moves with the pixel
+  const bool par = P.parallel != 0.;
 #pragma unroll
   for (int q = 0; q < 3; q++)
-    dir[q] = -(pix[q] - P.src[q]);
+    dir[q] = par ? -P.src[q] : -(pix[q] - P.src[q]);
   int mainDir = 0;
   if (fabs(dir[1]) > fabs(dir[mainDir]))
     mainDir = 1;
@@ -613,7 +615,16 @@ joseph_tables(const Geometry & g, const rtkb_image_desc & vol, const rtkb_image_
     r.src[0] = sv[0];
     r.src[1] = sv[1];
     r.src[2] = sv[2];
-    r.pad = 0.;
+    r.parallel = 0.;
+    double s2p[3];
+    if (g.parallel_source_to_pixel(k, s2p))
+    {
+      // ...Parallel::NewProjection maps SourceToPixel by the 3x3 part of the
+      // volume's physical-to-index matrix
+      for (int a = 0; a < 3; a++)
+        r.src[a] = vpp2i[a * 4 + 0] * s2p[0] + vpp2i[a * 4 + 1] * s2p[1] + vpp2i[a * 4 + 2] * s2p[2];
+      r.parallel = 1.;
+    }
   }
   if (cyl)
   {
@@ -845,6 +856,9 @@ joseph_check(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_im
     return fail(RTKB_ERR_INVALID_ARGUMENT, "Mismatch between the number of projections and the geometry entries.");
   if (proj->size[1] > 65535 * 8 || proj->size[2] > 65535 || vol->size[1] > 65535)
     return fail(RTKB_ERR_UNSUPPORTED, "image too large for one launch");
+  // ProjectionsRegionConstIteratorRayBased::New (include/rtkProjectionsRegionConstIteratorRayBased.hxx:90-95)
+  if (!g->g.p.empty() && g->g.p[0].sdd == 0. && g->g.radius_cylindrical != 0.)
+    return fail(RTKB_ERR_UNSUPPORTED, "Parallel geometry assumes a flat panel detector.");
   return RTKB_OK;
 }
 

@@ -16,8 +16,8 @@ namespace
 struct PixProj
 {
   double m[12];  // projection index -> world (rows 0-2)
-  double src[3]; // source position (world)
-  double pad;
+  double src[3];   // source position (world); parallel beam: pixel - source
+  double parallel; // 1: parallel beam (the source moves with the pixel, RTK's parallel ray iterator)
 };
 
 struct Ell
@@ -34,17 +34,21 @@ project_ellipsoids_kernel(const PixProj * __restrict__ P, const Ell * __restrict
     return;
   const PixProj & q = P[s];
   const double    iu = u + pidx0, iv = v + pidx1, ik = s + pidx2;
-  double          d[3];
+  double          d[3], src[3];
 #pragma unroll
   for (int a = 0; a < 3; a++)
-    d[a] = q.m[a * 4 + 0] * iu + q.m[a * 4 + 1] * iv + q.m[a * 4 + 2] * ik + q.m[a * 4 + 3] - q.src[a];
+  {
+    const double pix = q.m[a * 4 + 0] * iu + q.m[a * 4 + 1] * iv + q.m[a * 4 + 2] * ik + q.m[a * 4 + 3];
+    src[a] = q.parallel != 0. ? pix - q.src[a] : q.src[a];
+    d[a] = pix - src[a];
+  }
   const double len = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
   double       acc = 0.;
   for (int e = 0; e < ne; e++)
   {
     const Ell & el = E[e];
     double      o[3], dd[3];
-    const double rel[3] = { q.src[0] - el.c[0], q.src[1] - el.c[1], q.src[2] - el.c[2] };
+    const double rel[3] = { src[0] - el.c[0], src[1] - el.c[1], src[2] - el.c[2] };
 #pragma unroll
     for (int a = 0; a < 3; a++)
     {
@@ -98,7 +102,7 @@ rtkb_project_ellipsoids(const rtkb_geometry * g, const rtkb_image_desc * proj, i
       tab[s].src[0] = src[0];
       tab[s].src[1] = src[1];
       tab[s].src[2] = src[2];
-      tab[s].pad = 0.;
+      tab[s].parallel = g->g.parallel_source_to_pixel(proj->index[2] + s, tab[s].src) ? 1. : 0.;
     }
     std::vector<Ell> ell(n_ellipsoids > 0 ? n_ellipsoids : 1);
     for (int e = 0; e < n_ellipsoids; e++)

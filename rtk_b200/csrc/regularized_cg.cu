@@ -511,6 +511,7 @@ rtkb_regularized_cg(const rtkb_geometry * g, const rtkb_image_desc * vol, const 
   cp.use_cuda_graph = 1;
   cp.storage = 0;
   cp.gamma = prm->gamma;
+  cp.backprojector = 1; // BP_JOSEPH: the regularised CG runs on the Joseph pair
   rtkb_cg * plan = nullptr;
   int       rc = rtkb_cg_create(g, vol, proj, &cp, &plan);
   if (rc != RTKB_OK)

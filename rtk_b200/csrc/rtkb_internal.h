@@ -68,6 +68,9 @@ struct Geometry
   void proj_coords_to_fixed(int i, double out[16]) const;
   void proj_coords_to_detector(int i, double out[16]) const; // GetProjectionCoordinatesToDetectorSystemMatrix
   void inverse_rotation(int i, double out[16]) const;        // GetRotationMatrices()[i] inverse
+  // Parallel beam (SDD 0): pixel - source of RTK's parallel ray iterator, in
+  // mm (-2 SID x row 2 of the rotation matrix); false for a divergent beam.
+  bool parallel_source_to_pixel(int i, double out[3]) const;
   void source_angles(std::vector<double> & out) const;
   void gantry_angles(std::vector<double> & out) const;
   void tilt_angles(std::vector<double> & out) const;

@@ -10,8 +10,8 @@ namespace rtkb
 struct RayProj
 {
   double pix2vol[12]; // rows 0-2 of the projection-index -> volume-index matrix
-  double src[3];      // source in volume index coordinates
-  double pad;
+  double src[3];      // source in volume index coordinates; parallel beam: pixel - source (volume index units)
+  double parallel;    // 1: parallel beam (every pixel has its own source, RTK's parallel ray iterator)
 };
 
 // Cylindrical panel (ProjectionsRegionConstIteratorRayBasedWithCylindricalPanel):

@@ -33,8 +33,8 @@ using rtkb::fail;
 struct RayTab
 {
   double m[12];  // projection index -> world (rows 0-2)
-  double src[3]; // source position (world)
-  double pad;
+  double src[3];   // source position (world); parallel beam: pixel - source
+  double parallel; // 1: parallel beam (the source moves with the pixel, RTK's parallel ray iterator)
 };
 
 struct Box
@@ -53,17 +53,21 @@ ray_box_kernel(const RayTab * __restrict__ P, Box b, int nu, int nv, int pidx0, 
     return;
   const RayTab & q = P[s];
   const double   iu = u + pidx0, iv = v + pidx1, ik = s + pidx2;
-  double         d[3];
+  double         d[3], src[3];
 #pragma unroll
   for (int a = 0; a < 3; a++)
-    d[a] = q.m[a * 4 + 0] * iu + q.m[a * 4 + 1] * iv + q.m[a * 4 + 2] * ik + q.m[a * 4 + 3] - q.src[a];
+  {
+    const double pix = q.m[a * 4 + 0] * iu + q.m[a * 4 + 1] * iv + q.m[a * 4 + 2] * ik + q.m[a * 4 + 3];
+    src[a] = q.parallel != 0. ? pix - q.src[a] : q.src[a];
+    d[a] = pix - src[a];
+  }
   const double len = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
   double       inf = -DBL_MAX, sup = DBL_MAX;
   bool         hit = true;
 #pragma unroll
   for (int a = 0; a < 3; a++)
   {
-    const double org = b.D[0 * 3 + a] * q.src[0] + b.D[1 * 3 + a] * q.src[1] + b.D[2 * 3 + a] * q.src[2];
+    const double org = b.D[0 * 3 + a] * src[0] + b.D[1 * 3 + a] * src[1] + b.D[2 * 3 + a] * src[2];
     const double dir = (b.D[0 * 3 + a] * d[0] + b.D[1 * 3 + a] * d[1] + b.D[2 * 3 + a] * d[2]) / len;
     if (!hit)
       continue;
@@ -157,7 +161,7 @@ ray_box_lengths(const rtkb_geometry * g, const rtkb_image_desc & vol, const rtkb
     tab[s].src[0] = src[0];
     tab[s].src[1] = src[1];
     tab[s].src[2] = src[2];
-    tab[s].pad = 0.;
+    tab[s].parallel = g->g.parallel_source_to_pixel(proj.index[2] + s, tab[s].src) ? 1. : 0.;
   }
   Box b;
   if (corners)

@@ -444,6 +444,15 @@ def water_precorrection(desc, proj, coefficients, out=None, stream=None):
     return out
 
 
+def _backprojector_code(bp):
+    """RTK's back projector choice of its iterative filters: "joseph"
+    (BP_JOSEPH) or "voxel" (BP_VOXELBASED, rtkconjugategradient's default)."""
+    codes = {"voxel": 0, "voxelbased": 0, "joseph": 1}  # RTK's BackProjectionType values
+    if bp not in codes:
+        raise ValueError(f"backprojector must be one of {sorted(codes)}")
+    return codes[bp]
+
+
 def _storage_code(storage):
     codes = {"fp32": 0, "bf16": 1}
     if storage not in codes:
@@ -452,13 +461,15 @@ def _storage_code(storage):
 
 
 class ConjugateGradient:
-    """Plan of rtk::ConjugateGradientConeBeamReconstructionFilter (Joseph pair,
-    FP64 scalars on the device, one CUDA graph per iteration).  storage="bf16"
-    stores the normal-equation vectors and the projection-domain temporary
-    as bfloat16 (FP32 arithmetic, FP64 dots and step sizes)."""
+    """Plan of rtk::ConjugateGradientConeBeamReconstructionFilter (Joseph
+    forward projector; Joseph or voxel-based back projector, RTK's SetBackProjectionFilter
+    choice; FP64 scalars on the device, one CUDA graph per iteration).
+    storage="bf16" stores the normal-equation vectors and the
+    projection-domain temporary as bfloat16 (FP32 arithmetic, FP64 dots and
+    step sizes; Joseph back projector)."""
 
     def __init__(self, geometry, vol_desc, proj_desc, tikhonov=0.0, use_cuda_graph=True, storage="fp32",
-                 gamma=0.0):
+                 gamma=0.0, backprojector="joseph"):
         from ._capi import CgParams
 
         self._lib = load()
@@ -467,6 +478,7 @@ class ConjugateGradient:
         p = CgParams()
         p.tikhonov, p.use_cuda_graph, p.storage = tikhonov, int(use_cuda_graph), _storage_code(storage)
         p.gamma = gamma
+        p.backprojector = _backprojector_code(backprojector)
         h = C.c_void_p()
         check(self._lib.rtkb_cg_create(geometry.handle, C.byref(vol_desc), C.byref(proj_desc), C.byref(p),
                                        C.byref(h)))
@@ -550,7 +562,7 @@ class ConjugateGradientBatch:
     (geometry, vol_desc, proj_desc, proj, x[, weights[, displaced_detector]]);
     iterate(n) runs n iterations of every problem as one CUDA graph launch."""
 
-    def __init__(self, problems, tikhonov=0.0, storage="fp32", gamma=0.0):
+    def __init__(self, problems, tikhonov=0.0, storage="fp32", gamma=0.0, backprojector="joseph"):
         from ._capi import CgBatchProblem, CgParams
 
         self._lib = load()
@@ -572,6 +584,7 @@ class ConjugateGradientBatch:
         self._arr = arr
         p = CgParams()
         p.tikhonov, p.use_cuda_graph, p.storage, p.gamma = tikhonov, 0, _storage_code(storage), gamma
+        p.backprojector = _backprojector_code(backprojector)
         h = C.c_void_p()
         check(self._lib.rtkb_cg_batch_create(arr, len(problems), C.byref(p), C.byref(h)))
         self._h = h
@@ -607,13 +620,14 @@ class ConjugateGradientBatch:
 
 def conjugate_gradient(geometry, vol_desc, proj_desc, proj, x, niter, rel_residual=0.0, weights=None,
                        displaced_detector=True, tikhonov=0.0, use_cuda_graph=True, stream=None, storage="fp32",
-                       gamma=0.0):
+                       gamma=0.0, backprojector="joseph"):
     """Whole CG reconstruction in place on x; returns (iterations, relative residual)."""
     from ._capi import CgParams
 
     p = CgParams()
     p.tikhonov, p.use_cuda_graph, p.storage = tikhonov, int(use_cuda_graph), _storage_code(storage)
     p.gamma = gamma
+    p.backprojector = _backprojector_code(backprojector)
     it, rel = C.c_int(), C.c_double()
     check(load().rtkb_conjugate_gradient(geometry.handle, C.byref(vol_desc), C.byref(proj_desc), C.byref(p),
                                          _ptr(proj), _ptr(weights) if weights is not None else None,

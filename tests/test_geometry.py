@@ -82,20 +82,42 @@ def test_parallel_divergent_mix_is_rejected(rtkb):
         g.AddProjection(1000.0, 0.0, 10.0)
 
 
+def _eval(m, x):
+    h = m @ np.append(x, 1.0)
+    return h[0] / h[2], h[1] / h[2], 1.0 / (h[2] * h[2])
+
+
+@pytest.mark.parametrize("kind", ["irregular", "circular", "parallel"])
 @pytest.mark.parametrize("direction", ["identity", "perpendicular", "oblique"])
-def test_backprojection_matrices_match_oracle(rtkb, oracle, direction):
+def test_backprojection_matrices_against_ray_plane_intersection(rtkb, oracle, direction, kind):
+    """RTK's composed volume-index -> projection-index matrix
+    (include/rtkBackProjectionImageFilter.hxx:535-595, FDK normalisation
+    include/rtkFDKBackProjectionImageFilter.hxx:80-104), as the product builds
+    it and as the oracle restates it, evaluated at voxel indices, against the
+    oracle's independent derivation: the ray from the source through the
+    voxel's physical position meets the detector plane (source position and
+    detector frame), then the stack's physical-to-index map.  Volume and
+    stack regions start at non-zero indices; directions are non-trivial."""
     import ctypes as C
 
     rng = np.random.default_rng(7)
     gl = rtkb.ThreeDCircularProjectionGeometry()
     go = oracle.Geometry()
-    _irregular(rng, 12, gl, go)
+    if kind == "irregular":
+        _irregular(rng, 12, gl, go)
+    else:
+        for i in range(12):
+            p = (1000.0, 0.0 if kind == "parallel" else 1536.0, i * 30.0 + 3.0, 12.0, -7.0, 0.0, 0.0, 5.0, -3.0)
+            gl.AddProjection(*p)
+            go.add_projection(*p)
     d = {"identity": np.eye(3), "perpendicular": np.array([[0, 1, 0], [-1, 0, 0], [0, 0, 1.0]]),
          "oblique": np.array([[np.cos(0.7), -np.sin(0.7), 0], [np.sin(0.7), np.cos(0.7), 0], [0, 0, 1.0]])}[direction]
     vd = rtkb.make_desc((20, 18, 16), (1.5, 1.2, 1.1), origin=(-13.0, -9.0, -8.0), index=(3, -2, 5), direction=d)
     pd = rtkb.make_desc((40, 30, 12), (1.3, 1.1, 1.0), origin=(-25.0, -16.0, 0.0), index=(-7, 4, 0))
     vo = oracle.image((20, 18, 16), (1.5, 1.2, 1.1), origin=(-13.0, -9.0, -8.0), index=(3, -2, 5), direction=d)
     po = oracle.image((40, 30, 12), (1.3, 1.1, 1.0), origin=(-25.0, -16.0, 0.0), index=(-7, 4, 0))
+    i2p = oracle.index_to_physical(vo)
+    idx = [np.array(v, dtype=np.float64) for v in ((3, -2, 5), (22, 15, 20), (10, 4, 11), (3, 15, 5))]
     for fdk in (0, 1):
         out = np.zeros(12 * 12)
         modes = np.zeros(12, dtype=np.int32)
@@ -103,6 +125,16 @@ def test_backprojection_matrices_match_oracle(rtkb, oracle, direction):
             gl.handle, C.byref(vd), C.byref(pd), 0, 12, fdk, out.ctypes.data_as(C.POINTER(C.c_double)),
             modes.ctypes.data_as(C.POINTER(C.c_int))))
         for i in range(12):
-            m, mode = oracle.bp_matrix(go, vo, po, i, bool(fdk))
-            np.testing.assert_allclose(out[12 * i:12 * i + 12].reshape(3, 4), m, rtol=1e-12, atol=1e-12)
-            assert modes[i] == mode
+            m_orc, mode_orc = oracle.bp_matrix(go, vo, po, i, bool(fdk))
+            m_prod = out[12 * i:12 * i + 12].reshape(3, 4)
+            for x in idx:
+                phys = (i2p @ np.append(x, 1.0))[:3]
+                want, mode = oracle.bp_project(go, vo, po, i, bool(fdk), phys)
+                for m in (m_prod, m_orc):
+                    u, v, w2 = _eval(m, x)
+                    assert abs(u - want[0]) < 1e-9 and abs(v - want[1]) < 1e-9, (u, v, want)
+                    if fdk:
+                        assert abs(w2 - want[2]) < 1e-12 * max(1.0, want[2]), (w2, want[2])
+            assert modes[i] == mode and mode_orc == mode
+            if kind != "irregular" and direction != "oblique":
+                assert mode != 0  # circular and parallel stacks take RTK's optimised paths

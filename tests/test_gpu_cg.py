@@ -102,9 +102,37 @@ def test_cg_early_stop_on_relative_residual(rtkb, oracle):
     assert rel <= 1e-2 and it < 200
 
 
-def test_cg_sphere_like_rtkconjugategradientreconstructiontest(rtkb, oracle):
+@pytest.mark.parametrize("tikhonov,offset", [(0.0, 0.0), (0.3, 40.0)])
+def test_cg_voxel_backprojector_matches_oracle(rtkb, oracle, tikhonov, offset):
+    """RTK's default projector choice (Joseph forward, voxel-based back
+    projector, include/rtkIterativeConeBeamReconstructionFilter.hxx:33-103):
+    b = BP_voxel(W p), A = BP_voxel W FP_Joseph (+ tikhonov), iterates and
+    residuals against the oracle's CG with the same back projector."""
+    import torch
+
+    gl, go, vd, vo, pd, po, p = _problem(rtkb, oracle, offset=offset, seed=4)
+    niter = 6
+    w = oracle.displaced_detector(go, po, np.ones(oracle.shape_of(po)), pad=False)[0] if offset else None
+    ref_x, ref_res = oracle.cg_joseph(go, vo, po, p, niter, weights=w, tikhonov=tikhonov, backprojector="voxel")
+    x = torch.zeros(oracle.shape_of(vo), device="cuda")
+    cg = rtkb.ops.ConjugateGradient(gl, vd, pd, tikhonov=tikhonov, backprojector="voxel")
+    cg.start(to_gpu(p), x, displaced_detector=bool(offset))
+    res = [cg.residual()[0]]
+    for _ in range(niter):
+        cg.iterate(1)
+        res.append(cg.residual()[0])
+    cg.close()
+    assert rel_l2(to_np(x), ref_x) < CG_TOL
+    np.testing.assert_allclose(res, ref_res, rtol=CG_TOL)
+    assert rtkb.ops.device_status() == 0
+
+
+@pytest.mark.parametrize("backprojector", ["voxel", "joseph"])
+def test_cg_sphere_like_rtkconjugategradientreconstructiontest(rtkb, oracle, backprojector):
     """Sphere of radius 90 mm, 64^3 at 4 mm, 180 projections, 5 iterations
-    (RTK's test, Joseph back projector case)."""
+    (RTK's test: case 1 with the voxel-based back projector, uniform input
+    weights; the Joseph back projector as in its case 2 without the
+    regularisation weights)."""
     n = 180
     params = [(600.0, 1200.0, i * 360.0 / n) for i in range(n)]
     gl, go = pair_geometry(rtkb, oracle, params)
@@ -116,9 +144,11 @@ def test_cg_sphere_like_rtkconjugategradientreconstructiontest(rtkb, oracle):
     import torch
 
     x = torch.zeros((64, 64, 64), device="cuda")
-    rtkb.ops.conjugate_gradient(gl, vd, pd, to_gpu(p), x, 5, displaced_detector=True)
+    rtkb.ops.conjugate_gradient(gl, vd, pd, to_gpu(p), x, 5, displaced_detector=True, backprojector=backprojector)
     err, psnr, ok = phantoms.check_image_quality(to_np(x), ref, 0.08, 23.0, 2.0)
     assert ok, (err, psnr)
+    ref_x, _ = oracle.cg_joseph(go, vo, po, p, 5, backprojector=backprojector)
+    assert rel_l2(to_np(x), ref_x) < CG_TOL
 
 
 # BF16 storage of r, p, A p and the projection temporary rounds each stored

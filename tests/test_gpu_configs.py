@@ -1,0 +1,138 @@
+"""Parity at the benchmark configurations, through the C ABI, against the
+FP64 oracle (its voxel -> pixel map derived independently of the product's
+matrices):
+
+  * C1 end to end: noisy Shepp-Logan projections, FDK weighting + Hann ramp +
+    backprojection, 128^3 from 180 x 256^2, within 1e-5 of the oracle FDK,
+    and RTK's rtkfdktest thresholds (test/rtkfdktest.cxx:117: error per
+    pixel < 0.03, PSNR > 26 dB on 2.0) inside the region the truncated data
+    reconstruct (a 60 mm cylinder: C1's field of view at the isocentre is
+    85 mm, smaller than the phantom, and its edge carries truncation
+    artefacts in any FDK);
+  * C2's displaced-detector (80 mm) and 200 deg Parker short-scan variants at
+    full size (512^3 from 720 x 1024 x 768): preprocessing and
+    backprojection of the whole stack on the GPU, a y-slab of the volume
+    against the oracle fed the detector rows that slab projects onto;
+  * parallel beams: RTK's rtkfbpparalleltest on the GPU, and the Joseph
+    projection of a box against analytic chord lengths of parallel rays.
+"""
+import numpy as np
+import pytest
+
+from tests import phantoms
+from tests import workloads as W
+from tests.gpu_util import REL_L2_TOL, pair_geometry, pair_image, rel_l2, to_gpu, to_np
+from tests.test_oracle_pins import _ray_box_lengths
+
+pytestmark = pytest.mark.gpu
+
+
+def _inner_cylinder(vol_size, vox, radius):
+    nz, ny, nx = vol_size[2], vol_size[1], vol_size[0]
+    zz, yy, xx = np.meshgrid(*(np.arange(n) * vox - 0.5 * vox * (n - 1) for n in (nz, ny, nx)), indexing="ij")
+    return (xx * xx + zz * zz < radius * radius) & (np.abs(yy) < radius)
+
+
+def test_c1_fdk_end_to_end(rtkb, oracle):
+    import torch
+
+    c = W.C1
+    gl, go = pair_geometry(rtkb, oracle, W.circular_params(c["n"], c["sid"], c["sdd"]))
+    vd, vo = pair_image(rtkb, oracle, c["vol"], (c["vox"],) * 3)
+    pd, po = pair_image(rtkb, oracle, (*c["det"], c["n"]), (c["pix"], c["pix"], 1.0))
+    p, sl = W.c1_projections(oracle, go, po)
+    ramp_o = oracle.ramp_params(hann=1.0)
+    ref = oracle.backproject(go, vo, po, oracle.ramp_filter(po, oracle.fdk_weight(go, po, p), ramp_o), fdk=True)
+    f, _ = rtkb.ops.fdk_preprocess(gl, pd, to_gpu(p), rtkb.ops.ramp_params(hann=1.0))
+    rec = to_np(rtkb.ops.fdk_backproject(gl, vd, pd, f, torch.zeros(oracle.shape_of(vo), device="cuda")))
+    assert rtkb.ops.device_status() == 0
+    assert rel_l2(rec, ref) < REL_L2_TOL
+    inner = _inner_cylinder(c["vol"], c["vox"], 60.0) & phantoms.fov_mask(go, vo, po)
+    err, psnr, ok = phantoms.check_image_quality(rec[inner], oracle.draw_ellipsoids(vo, sl)[inner], 0.03, 26.0, 2.0)
+    assert ok, (err, psnr)
+
+
+@pytest.mark.parametrize("variant", ["displaced", "short_scan"])
+def test_c2_variants_full_size_slab(rtkb, oracle, variant):
+    import torch
+
+    c = W.C2
+    displaced = variant == "displaced"
+    arc = 360.0 if displaced else c["short_arc"]
+    params = W.circular_params(c["n"], c["sid"], c["sdd"], arc=arc, pox=c["displaced_offset"] if displaced else 0.0)
+    gl, go = pair_geometry(rtkb, oracle, params)
+    vd = rtkb.make_desc(c["vol"], (c["vox"],) * 3)
+    pd, po = pair_image(rtkb, oracle, (*c["det"], c["n"]), (c["pix"], c["pix"], 1.0))
+    p = rtkb.ops.project_ellipsoids(gl, pd, W.c2_ellipsoids())
+    f, od = rtkb.ops.fdk_preprocess(gl, pd, p, displaced=displaced, short_scan=not displaced)
+    vol = rtkb.ops.fdk_backproject(gl, vd, od, f, torch.zeros(tuple(reversed(c["vol"])), device="cuda"))
+    assert rtkb.ops.device_status() == 0
+    # y-slab 250..253 (y from -2.75 to -1.25 mm) projects onto detector rows
+    # ~370-392; the oracle filters rows 360..399 (the ramp filter and the
+    # weights act within a row) and backprojects the slab from them
+    r0, nr = 360, 40
+    rows = p[:, r0:r0 + nr, :].cpu().numpy().astype(np.float64)
+    po_rows = oracle.image((c["det"][0], nr, c["n"]), (c["pix"], c["pix"], 1.0), origin=tuple(po.origin),
+                           index=(0, r0, 0))
+    q, qo = rows, po_rows
+    if displaced:
+        q, i0, s0 = oracle.displaced_detector(go, po_rows, q)
+        qo = oracle.image((s0, nr, c["n"]), (c["pix"], c["pix"], 1.0), origin=tuple(po.origin), index=(i0, r0, 0))
+        assert (od.index[0], od.size[0]) == (i0, s0)
+    else:
+        q, short = oracle.parker_weight(go, qo, q)
+        assert short
+    q = oracle.ramp_filter(qo, oracle.fdk_weight(go, qo, q), oracle.ramp_params())
+    vo_slab = oracle.image((c["vol"][0], 4, c["vol"][2]), (c["vox"],) * 3, origin=tuple(vd.origin), index=(0, 250, 0))
+    ref = oracle.backproject(go, vo_slab, qo, q, fdk=True)
+    got = vol[:, 250:254, :].cpu().numpy()
+    assert rel_l2(got, ref) < REL_L2_TOL, rel_l2(got, ref)
+
+
+def test_fdk_parallel_like_rtkfbpparalleltest(rtkb, oracle):
+    """test/rtkfbpparalleltest.cxx on the GPU: parallel projections (SDD 0,
+    source offsets 20 / 15 mm) of the Shepp-Logan phantom by the GPU's
+    analytic projector, FDK on the GPU, against the oracle at each stage and
+    the phantom at RTK's thresholds."""
+    import torch
+
+    n = 180
+    params = [(600.0, 0.0, i * 360.0 / n, 0, 0, 0, 0, 20, 15) for i in range(n)]
+    gl, go = pair_geometry(rtkb, oracle, params)
+    vd, vo = pair_image(rtkb, oracle, (128, 128, 128), (2.0,) * 3, origin=(-127.0,) * 3)
+    pd, po = pair_image(rtkb, oracle, (128, 128, n), (2.0,) * 3, origin=(-127.0,) * 3)
+    sl = phantoms.shepp_logan(116.0)
+    p_ref = oracle.project_ellipsoids(go, po, sl)
+    p = rtkb.ops.project_ellipsoids(gl, pd, sl)
+    assert rel_l2(to_np(p), p_ref) < 1e-6
+    p64 = to_np(p)
+    ref = oracle.backproject(go, vo, po, oracle.ramp_filter(po, oracle.fdk_weight(go, po, p64), oracle.ramp_params()),
+                             fdk=True)
+    f, _ = rtkb.ops.fdk_preprocess(gl, pd, p)
+    rec = to_np(rtkb.ops.fdk_backproject(gl, vd, pd, f, torch.zeros((128, 128, 128), device="cuda")))
+    assert rel_l2(rec, ref) < REL_L2_TOL
+    err, psnr, ok = phantoms.check_image_quality(rec * phantoms.fov_mask(go, vo, po), oracle.draw_ellipsoids(vo, sl),
+                                                 0.03, 26.0, 2.0)
+    assert ok, (err, psnr)
+
+
+def test_joseph_parallel_box(rtkb, oracle):
+    """The Joseph forward projection of a box of ones in parallel geometry
+    against the analytic chord lengths of parallel rays (RTK's thresholds)
+    and the oracle; the ray-box lengths of the same geometry against both."""
+    import torch
+
+    n = 45
+    params = [(1000.0, 0.0, -45.0 + i * 2.0, 0.0, 0.0, 0.0, 0.0, 10.0, -6.0) for i in range(n)]
+    gl, go = pair_geometry(rtkb, oracle, params)
+    vd, vo = pair_image(rtkb, oracle, (64, 64, 64), (4.0,) * 3, origin=(-126.0,) * 3)
+    pd, po = pair_image(rtkb, oracle, (64, 64, n), (4.0,) * 3, origin=(-126.0, -124.0, -126.0))
+    ones = torch.ones((64, 64, 64), device="cuda")
+    fp = to_np(rtkb.ops.joseph_forward_project(gl, vd, pd, ones, torch.zeros((n, 64, 64), device="cuda")))
+    assert rel_l2(fp, oracle.joseph_forward(go, vo, np.ones((64, 64, 64)), po)) < REL_L2_TOL
+    chords = _ray_box_lengths(oracle, go, po, (-126.0,) * 3, (126.0,) * 3, parallel=True)
+    err, psnr, ok = phantoms.check_image_quality(fp, chords, 1.28, 44.0, 255.0)
+    assert ok, (err, psnr)
+    rb = to_np(rtkb.ops.ray_box_lengths(gl, vd, pd))
+    assert rel_l2(rb, oracle.ray_box(go, vo, po)) < 1e-6
+    assert rtkb.ops.device_status() == 0

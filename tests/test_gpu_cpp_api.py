@@ -109,7 +109,7 @@ def test_cpp_layer_on_gpu_matches_python_binding(rtkb, tmp_path):
     fp = to_np(rtkb.ops.joseph_forward_project(g, vd, pd, to_gpu(vol), torch.zeros(proj.shape, device="cuda")))
     assert np.array_equal(fp_cpp, fp.astype(np.float32))
     x = torch.zeros(vol.shape, device="cuda")
-    cg = rtkb.ops.ConjugateGradient(g, vd, pd)
+    cg = rtkb.ops.ConjugateGradient(g, vd, pd, backprojector="voxel")  # the C++ filter's default, as RTK's
     cg.start(to_gpu(proj), x, displaced_detector=False)
     cg.iterate(3)
     assert rel_l2(x_cpp, to_np(x)) < 1e-5, rel_l2(x_cpp, to_np(x))

@@ -8,6 +8,8 @@ known-answer checks restated on the oracle:
                                               flat and cylindrical (radius 600) detector (1.28 / 44 dB on 255)
   * test/rtkiterativefdktest.cxx              3 iterations of iterative FDK (0.027 / 27 dB in the field of view)
   * test/rtkadjointoperatorstest.cxx  Joseph FP/BP adjointness (|ratio - 1| < 1e-3; FP64 gives ~1e-13)
+  * test/rtkfbpparalleltest.cxx       FDK in parallel geometry (SDD 0, source offsets 20 / 15 mm) of the
+                                      Shepp-Logan phantom (err/px < 0.03, PSNR > 26 in the field of view)
 plus algebraic properties of the weighting filters that RTK's formulas imply.
 """
 import numpy as np
@@ -39,16 +41,23 @@ def test_fdk_shepp_logan_like_rtkfdktest(oracle):
     assert ok, (err, psnr)
 
 
-def _ray_box_lengths(O, g, proj, bmin, bmax):
-    """Analytic length of each source-to-pixel segment inside a box (mm)."""
+def _ray_box_lengths(O, g, proj, bmin, bmax, parallel=False):
+    """Analytic length of each source-to-pixel segment inside a box (mm).  A
+    parallel beam's source moves with the pixel, 2 SID along the detector
+    normal (RTK's parallel ray iterator)."""
     nz, nv, nu = O.shape_of(proj)
     out = np.zeros((nz, nv, nu))
     i2p = O.index_to_physical(proj)
     jj, ii = np.meshgrid(np.arange(nv), np.arange(nu), indexing="ij")
     for k in range(nz):
-        T = g.proj_coords_to_fixed(k) @ i2p
+        P = g.proj_coords_to_fixed(k)
+        T = P @ i2p
         pix = (T @ np.stack([ii.ravel(), jj.ravel(), np.full(ii.size, k), np.ones(ii.size)]))[:3].T
-        s = g.source_position(k)[:3]
+        if parallel:
+            n = np.cross(P[:3, 0], P[:3, 1])
+            s = pix + 2.0 * 1000.0 * n
+        else:
+            s = g.source_position(k)[:3]
         d = pix - s
         with np.errstate(divide="ignore", invalid="ignore"):
             t1 = (np.asarray(bmin) - s) / d
@@ -76,6 +85,47 @@ def test_joseph_box_like_rtkforwardprojectiontest(oracle):
         fp = O.joseph_forward(g, vol, ones, proj)
         err, psnr, ok = phantoms.check_image_quality(fp, ref, 1.28, 44.0, 255.0)
         assert ok, (q, err, psnr)
+
+
+def test_joseph_box_parallel_beam(oracle):
+    """Known answer in the spirit of rtkforwardprojectiontest case 1 for a
+    parallel beam (SDD 0, SID 1000): the Joseph projection of a box of ones
+    against the analytic chord lengths of parallel rays along the detector
+    normal, at RTK's thresholds.  A cone of rays converging on the source
+    point fails it by far."""
+    O = oracle
+    n = 45
+    vol = O.image((64, 64, 64), (4.0, 4.0, 4.0), origin=(-126.0, -126.0, -126.0))
+    # detector rows 2 mm off the box's faces (a ray along a face has no defined chord)
+    proj = O.image((64, 64, n), (4.0, 4.0, 4.0), origin=(-126.0, -124.0, -126.0))
+    g = O.Geometry()
+    for i in range(n):
+        g.add_projection(1000.0, 0.0, -45.0 + i * 2.0, 0.0, 0.0, 0.0, 0.0, 10.0, -6.0)
+    ref = _ray_box_lengths(O, g, proj, (-126.0, -126.0, -126.0), (126.0, 126.0, 126.0), parallel=True)
+    fp = O.joseph_forward(g, vol, np.ones(O.shape_of(vol)), proj)
+    err, psnr, ok = phantoms.check_image_quality(fp, ref, 1.28, 44.0, 255.0)
+    assert ok, (err, psnr)
+    cone = _ray_box_lengths(O, g, proj, (-126.0, -126.0, -126.0), (126.0, 126.0, 126.0), parallel=False)
+    assert not phantoms.check_image_quality(fp, cone, 1.28, 44.0, 255.0)[2]
+
+
+def test_fdk_parallel_shepp_logan_like_rtkfbpparalleltest(oracle):
+    """test/rtkfbpparalleltest.cxx: 180 parallel projections (SID 600, SDD 0, source offsets 20 / 15 mm) of the
+    Shepp-Logan phantom scaled 116, 128^3 at 2 mm from 128^2 at 2 mm, FDK, field-of-view mask."""
+    O = oracle
+    n = 180
+    g = O.Geometry()
+    for i in range(n):
+        g.add_projection(600.0, 0.0, i * 360.0 / n, 0, 0, 0, 0, 20, 15)
+    vol = O.image((128, 128, 128), (2.0, 2.0, 2.0), origin=(-127.0, -127.0, -127.0))
+    proj = O.image((128, 128, n), (2.0, 2.0, 2.0), origin=(-127.0, -127.0, -127.0))
+    sl = phantoms.shepp_logan(116.0)
+    p = O.project_ellipsoids(g, proj, sl)
+    ref = O.draw_ellipsoids(vol, sl)
+    rec = fdk_oracle(O, g, vol, proj, p)
+    rec *= phantoms.fov_mask(g, vol, proj)
+    err, psnr, ok = phantoms.check_image_quality(rec, ref, 0.03, 26.0, 2.0)
+    assert ok, (err, psnr)
 
 
 @pytest.mark.parametrize("radius", [0.0, 600.0])
@@ -224,3 +274,18 @@ def test_iterative_fdk_like_rtkiterativefdktest(oracle):
     one = O.iterative_fdk(g, vol, proj, p, np.zeros(O.shape_of(vol)), niter=1)
     err1, psnr1, _ = phantoms.check_image_quality(one * fov, ref, 0.027, 27.0, 2.0)
     assert err < err1 and psnr > psnr1, (err, err1, psnr, psnr1)
+
+
+def test_threaded_joseph_back_equals_single_threaded(oracle):
+    """The oracle's threaded Joseph back projection (used at large sizes) sums
+    the same terms as RTK's single-threaded filter."""
+    O = oracle
+    g = O.Geometry()
+    for i in range(23):
+        g.add_projection(700.0, 1100.0, i * 15.7, 3.0, -2.0, 4.0, 1.0, 2.0, 1.0)
+    vol = O.image((30, 26, 28), (2.0, 2.0, 2.0), index=(1, -2, 3))
+    proj = O.image((48, 40, 23), (2.5, 2.5, 1.0))
+    p = np.random.default_rng(3).uniform(-1, 1, size=O.shape_of(proj))
+    a = O.joseph_back(g, vol, proj, p)
+    b = O.joseph_back(g, vol, proj, p, threads=5)
+    assert np.linalg.norm(a - b) <= 1e-13 * np.linalg.norm(a)

@@ -62,8 +62,9 @@ const char * rtkb_last_error(void);
 /* Library version string. */
 const char * rtkb_version(void);
 /* Waits for `stream`, then reads and clears the device-side status word that
- * kernels set when a bounded wait gives up (RTKB_ERR_TIMEOUT) or an internal
- * check fails.  *status receives 0 when no kernel reported a problem. */
+ * kernels set when a bounded wait gives up or an internal check fails.
+ * *status receives 0 when no kernel reported a problem, RTKB_ERR_TIMEOUT when a
+ * wait gave up, RTKB_ERR_CUDA for a failed internal check. */
 int rtkb_device_status(void * stream, int * status);
 /* Temporary device memory of every entry point comes from one stream-ordered
  * memory pool per device that the library owns; memory freed there stays
@@ -74,6 +75,23 @@ int rtkb_device_status(void * stream, int * status);
  * No reference counterpart (ITK's CUDA images allocate per image). */
 int rtkb_trim_memory_pool(long long * reserved_after);
 int rtkb_memory_pool_reserved(long long * reserved);
+
+/* ---- failure detection (testing aids; no counterpart in the reference, whose
+ * CUDA_CHECK_ERROR, include/rtkCudaUtilities.hcu:30-35, only reports launch
+ * errors) ----
+ * rtkb_device_status reports RTKB_ERR_TIMEOUT when a bounded device-side wait
+ * gave up.  rtkb_set_wait_limit sets how many polls such a wait makes before
+ * it gives up (default 4194304, about a second or more; current device;
+ * *previous may be NULL).  rtkb_wait_self_test launches one CTA whose bounded
+ * wait is on an mbarrier that nobody arrives at: it gives up after the limit,
+ * records the timeout and returns, leaving the context usable.
+ * rtkb_inject_allocation_failures makes the library's next `count` scratch
+ * allocations fail as if the device were out of memory, which exercises the
+ * pool's trim-and-retry path (a failed retry is returned to the caller as an
+ * error before any of the call's kernels is enqueued). */
+int rtkb_set_wait_limit(unsigned int polls, unsigned int * previous);
+int rtkb_wait_self_test(void * stream);
+int rtkb_inject_allocation_failures(int count);
 
 /* ---- geometry: rtk::ThreeDCircularProjectionGeometry, FP64 ----
  * src/rtkThreeDCircularProjectionGeometry.cxx:56-153 (AddProjection),

@@ -180,6 +180,9 @@ SIGNATURES.update({
     "rtkb_tv_denoising_bpdq": (C.c_int, [_IM, _V, _V, C.c_double, C.c_int, C.POINTER(C.c_int), _V]),
     "rtkb_total_variation": (C.c_int, [_IM, _V, C.POINTER(C.c_double), _V]),
     "rtkb_trim_memory_pool": (C.c_int, [C.POINTER(C.c_longlong)]),
+    "rtkb_set_wait_limit": (C.c_int, [C.c_uint, C.POINTER(C.c_uint)]),
+    "rtkb_wait_self_test": (C.c_int, [_V]),
+    "rtkb_inject_allocation_failures": (C.c_int, [C.c_int]),
     "rtkb_memory_pool_reserved": (C.c_int, [C.POINTER(C.c_longlong)]),
     "rtkb_de_pierro_regularization": (C.c_int, [_IM, _V, _V, _V, C.c_double, _V, _V]),
     "rtkb_image_write_mha": (C.c_int, [C.c_char_p, _IM, _V, C.c_int]),

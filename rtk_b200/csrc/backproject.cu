@@ -40,6 +40,7 @@ namespace rtkb
 namespace dev
 {
 __device__ unsigned int g_device_status = 0;
+__device__ unsigned int g_wait_limit = kDefaultWaitLimit;
 }
 struct BatchProblemHandle; // device-side problem table of a prepared batch
 } // namespace rtkb
@@ -1767,7 +1768,52 @@ rtkb_device_status(void * stream, int * status)
   RTKB_CUDA_TRY(cudaMemcpyToSymbolAsync(rtkb::dev::g_device_status, &zero, sizeof(zero), 0, cudaMemcpyHostToDevice,
                                         st));
   RTKB_CUDA_TRY(cudaStreamSynchronize(st));
-  *status = (int)v;
+  // a wait that gave up, else another failed device-side check (a tile whose
+  // footprint left its staged box)
+  *status = v == 0 ? RTKB_OK : (v & RTKB_STATUS_TIMEOUT) ? RTKB_ERR_TIMEOUT : RTKB_ERR_CUDA;
+  return RTKB_OK;
+}
+
+// ---- failure detection without a GPU fault --------------------------------------
+namespace
+{
+// One CTA waits, with the library's bounded wait, on an mbarrier that expects
+// one arrival nobody makes; the wait gives up after g_wait_limit polls,
+// records the timeout and the kernel returns.
+__global__ void
+wait_self_test_kernel()
+{
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0)
+  {
+    rtkb::dev::mbar_init(&bar, 1);
+    rtkb::dev::fence_barrier_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0)
+    rtkb::dev::mbar_wait(&bar, 0);
+  __syncthreads();
+}
+} // namespace
+
+extern "C" int
+rtkb_set_wait_limit(unsigned int polls, unsigned int * previous)
+{
+  if (polls == 0)
+    return rtkb::fail(RTKB_ERR_INVALID_ARGUMENT, "the wait limit must be at least one poll");
+  unsigned int old = 0;
+  RTKB_CUDA_TRY(cudaMemcpyFromSymbol(&old, rtkb::dev::g_wait_limit, sizeof(old)));
+  RTKB_CUDA_TRY(cudaMemcpyToSymbol(rtkb::dev::g_wait_limit, &polls, sizeof(polls)));
+  if (previous)
+    *previous = old;
+  return RTKB_OK;
+}
+
+extern "C" int
+rtkb_wait_self_test(void * stream)
+{
+  wait_self_test_kernel<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>();
+  RTKB_CUDA_TRY(cudaGetLastError());
   return RTKB_OK;
 }
 

@@ -13,6 +13,7 @@
 #include "rtkb200.h"
 #include "rtkb_internal.h"
 
+#include <atomic>
 #include <cstdint>
 #include <mutex>
 
@@ -21,6 +22,18 @@ namespace
 constexpr int    kMaxDevices = 64;
 std::mutex       g_pool_mutex;
 cudaMemPool_t    g_pools[kMaxDevices] = {};
+std::atomic<int> g_injected_failures{ 0 }; // allocations still to fail (rtkb_inject_allocation_failures)
+
+// the pool allocation, or an injected out-of-memory failure
+cudaError_t
+pool_alloc(void ** p, size_t bytes, cudaMemPool_t pool, cudaStream_t st)
+{
+  int left = g_injected_failures.load();
+  while (left > 0)
+    if (g_injected_failures.compare_exchange_weak(left, left - 1))
+      return cudaErrorMemoryAllocation;
+  return cudaMallocFromPoolAsync(p, bytes, pool, st);
+}
 
 cudaError_t
 pool_for(int dev, cudaMemPool_t * out)
@@ -65,7 +78,7 @@ scratch_malloc(void ** p, size_t bytes, cudaStream_t st)
     e = pool_for(dev, &pool);
   if (e != cudaSuccess)
     return e;
-  e = cudaMallocFromPoolAsync(p, bytes, pool, st);
+  e = pool_alloc(p, bytes, pool, st);
   if (e == cudaErrorMemoryAllocation)
   {
     cudaGetLastError();
@@ -74,7 +87,7 @@ scratch_malloc(void ** p, size_t bytes, cudaStream_t st)
     if (e == cudaSuccess)
       e = cudaMemPoolTrimTo(pool, 0);
     if (e == cudaSuccess)
-      e = cudaMallocFromPoolAsync(p, bytes, pool, st);
+      e = pool_alloc(p, bytes, pool, st);
   }
   return e;
 }
@@ -124,5 +137,14 @@ rtkb_memory_pool_reserved(long long * reserved)
   if (e != cudaSuccess)
     return cuda_fail(e, "rtkb_memory_pool_reserved");
   *reserved = (long long)r;
+  return RTKB_OK;
+}
+
+extern "C" int
+rtkb_inject_allocation_failures(int count)
+{
+  if (count < 0)
+    return rtkb::fail(RTKB_ERR_INVALID_ARGUMENT, "count must not be negative");
+  g_injected_failures.store(count);
   return RTKB_OK;
 }

@@ -1,7 +1,7 @@
 // rtkb_ptx.cuh -- hand-written PTX wrappers for sm_100a (mbarrier, TMA) with
-// bounded waits.  Every wait gives up after a fixed number of polls, records
-// RTKB_STATUS_TIMEOUT in the device status word and returns false, so a
-// kernel can never spin forever.
+// bounded waits.  Every wait gives up after g_wait_limit polls (4 M unless
+// rtkb_set_wait_limit changed it), records RTKB_STATUS_TIMEOUT in the device
+// status word and returns false, so a kernel can never spin forever.
 #pragma once
 
 #include <cstdint>
@@ -16,9 +16,11 @@ namespace dev
 {
 
 extern __device__ unsigned int g_device_status;
+// polls of try_wait (each suspends for a bounded, hardware-defined time)
+// before a bounded wait gives up; set from the host (rtkb_set_wait_limit)
+extern __device__ unsigned int g_wait_limit;
 
-// ~4 M polls of try_wait (each suspends for a bounded, hardware-defined time)
-constexpr uint32_t kWaitLimit = 1u << 22;
+constexpr uint32_t kDefaultWaitLimit = 1u << 22;
 
 __device__ __forceinline__ uint32_t
 smem_u32(const void * p)
@@ -66,11 +68,15 @@ mbar_try_wait(uint64_t * bar, uint32_t parity)
   return ok != 0;
 }
 
-// Bounded wait for the phase with the given parity to complete.
+// Bounded wait for the phase with the given parity to complete (the limit is
+// read only when the first poll fails).
 __device__ __forceinline__ bool
 mbar_wait(uint64_t * bar, uint32_t parity)
 {
-  for (uint32_t it = 0; it < kWaitLimit; ++it)
+  if (mbar_try_wait(bar, parity))
+    return true;
+  const uint32_t limit = *static_cast<volatile unsigned int *>(&g_wait_limit);
+  for (uint32_t it = 1; it < limit; ++it)
     if (mbar_try_wait(bar, parity))
       return true;
   atomicOr(&g_device_status, RTKB_STATUS_TIMEOUT);

@@ -112,3 +112,27 @@ def check_image_quality(recon: np.ndarray, ref: np.ndarray, err_tol: float, psnr
     mse = (d * d).mean()
     psnr = 20 * np.log10(ref_value) - 10 * np.log10(mse)
     return err, psnr, bool(err < err_tol and psnr > psnr_tol)
+
+
+def acceptance_ties(g, vol, proj, tol=1e-6) -> np.ndarray:
+    """Voxels that some projection maps within tol pixels of RTK's acceptance
+    bounds of its optimised paths (u or v at 0 or N - 1, the ends of
+    0 <= floor(u) < N - 1).  On exactly symmetric geometries (pixel and voxel
+    centres aligned, angles in exact steps) such ties are frequent, and
+    whether the sample counts depends on the last bit of the map's rounding,
+    which differs between any two correct implementations."""
+    from oracle import oracle as O
+
+    nz, ny, nx = O.shape_of(vol)
+    z, y, x = np.meshgrid(np.arange(nz) + vol.index[2], np.arange(ny) + vol.index[1], np.arange(nx) + vol.index[0],
+                          indexing="ij")
+    X = np.stack([x.ravel(), y.ravel(), z.ravel(), np.ones(x.size)]).astype(np.float64)
+    tie = np.zeros(X.shape[1], dtype=bool)
+    for i in range(proj.size[2]):
+        m, _ = O.bp_matrix(g, vol, proj, proj.index[2] + i, False)
+        w = m[2] @ X
+        u = (m[0] @ X) / w - proj.index[0]
+        v = (m[1] @ X) / w - proj.index[1]
+        for c, n in ((u, proj.size[0]), (v, proj.size[1])):
+            tie |= (np.abs(c) < tol) | (np.abs(c - (n - 1)) < tol)
+    return tie.reshape(nz, ny, nx)

@@ -26,7 +26,6 @@
 
 #include <algorithm>
 #include <cfloat>
-#include <climits>
 #include <cstring>
 
 namespace
@@ -183,14 +182,12 @@ struct View
 };
 
 __device__ __forceinline__ View
-view_of_main(const JosephArgs & a, int main)
+view_for(const JosephArgs & a, const Ray & r)
 {
   View      w;
   const int nx = a.n[0], ny = a.n[1], nz = a.n[2];
-  // in-plane axes in increasing order (RTK's dinf < dsup)
-  const int di = main == 0 ? 1 : 0, ds = main == 2 ? 1 : 2;
-  w.transposed = (main == 0);
-  if (main == 0)
+  w.transposed = (r.main == 0);
+  if (r.main == 0)
   {
     // transposed copy T[x][y][z]: y stride nz, z stride 1, x stride ny*nz
     w.ox = nz;
@@ -200,23 +197,17 @@ view_of_main(const JosephArgs & a, int main)
   else
   {
     const long long st[3] = { 1, nx, (long long)nx * ny };
-    w.ox = st[di];
-    w.oy = st[ds];
-    w.oz = st[main];
+    w.ox = st[r.dinf];
+    w.oy = st[r.dsup];
+    w.oz = st[r.main];
   }
-  w.nxp = a.n[di];
-  w.nyp = a.n[ds];
-  w.nzp = a.n[main];
-  w.bx = a.vidx[di];
-  w.by = a.vidx[ds];
-  w.bz = a.vidx[main];
+  w.nxp = a.n[r.dinf];
+  w.nyp = a.n[r.dsup];
+  w.nzp = a.n[r.main];
+  w.bx = a.vidx[r.dinf];
+  w.by = a.vidx[r.dsup];
+  w.bz = a.vidx[r.main];
   return w;
-}
-
-__device__ __forceinline__ View
-view_for(const JosephArgs & a, const Ray & r)
-{
-  return view_of_main(a, r.main);
 }
 
 // Border step (BilinearInterpolationOnBorders / BilinearSplatOnBorders): FP64
@@ -388,232 +379,107 @@ red_add4(float4 * p, float4 v)
                : "memory");
 }
 
-// Back projector.  The border steps splat into the scalar accumulators A (or
-// At, the z<->x transposed accumulator of main-x rays) with global reductions.
-// The middle steps of main-z (main-x) rays go through a shared-memory window:
-// the 256 rays of a CTA (32 x 8 neighbouring detector pixels of one
-// projection) march the slices in lockstep; at each slice their four bilinear
-// weights are added into a window covering that slice's footprint of the CTA
-// (shared-memory atomics), and the window of the previous slice is then added
-// to the accumulator with one reduction per touched voxel, the contiguous axis
-// fastest, instead of one per sample and tap (a warp's samples are about 0.5
-// voxel apart, so its scattered reductions touched ~20 sectors).  The
-// positions are those of the forward projector (x0 + i * step in FP32), so the
-// pair stays adjoint.  The window follows two lines that bound the CTA's
-// samples from below (their minima at the first and last slice), one voxel of
-// slack on each side; a sample outside it, rays whose main direction or
-// marching sense differs from the CTA's majority, and rays with main
-// direction y take scalar global reductions.
-constexpr int kWinCells = 1024; // floats per window buffer (two buffers)
-
-__device__ __forceinline__ float
-block_reduce(float v, bool take_max, float * scratch)
-{
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1)
-  {
-    const float w = __shfl_xor_sync(0xffffffffu, v, o);
-    v = take_max ? fmaxf(v, w) : fminf(v, w);
-  }
-  const int warp = threadIdx.x >> 5;
-  __syncthreads();
-  if ((threadIdx.x & 31) == 0)
-    scratch[warp] = v;
-  __syncthreads();
-  float r = scratch[0];
-  for (int q = 1; q < (int)(blockDim.x >> 5); q++)
-    r = take_max ? fmaxf(r, scratch[q]) : fminf(r, scratch[q]);
-  return r;
-}
-
-template <typename Off>
-__device__ __forceinline__ void
-splat_global(float * slice, const Off ox1, const Off oy1, Off o, float cy0, float cy1, float lx)
-{
-  red_add(slice + o, cy0 * (1.f - lx));
-  red_add(slice + o + ox1, cy0 * lx);
-  red_add(slice + o + oy1, cy1 * (1.f - lx));
-  red_add(slice + o + ox1 + oy1, cy1 * lx);
-}
-
+// Back projector: the border steps splat into the scalar accumulators A (or
+// At, transposed); the middle steps of main-z (main-x) rays add their four
+// weights with one 16-byte vector reduction into the quad accumulator QAN
+// (QAT), laid out as the forward projector's quad copies: element e collects
+// the contributions to (f(a,b), f(a,b+1), f(a+1,b), f(a+1,b+1)) of the 2 x 2
+// neighbourhood at e.  The fold kernel adds each voxel's four quad entries.
+// Rays with main direction y keep four scalar reductions into A.  64
+// registers (4 CTAs per SM) keep more reductions in flight.
 template <typename Off, typename TP>
 __global__ void __launch_bounds__(256, 4)
-joseph_back_kernel(JosephArgs a, const TP * __restrict__ proj, float * A, float * At)
+joseph_back_kernel(JosephArgs a, const TP * __restrict__ proj, float * A, float * At, float4 * QAN, float4 * QAT)
 {
-  __shared__ float win[2][kWinCells];
-  __shared__ float red_scratch[8];
-  __shared__ int   s_key;
-  const int        u = blockIdx.x * 32 + (threadIdx.x & 31);
-  const int        v = blockIdx.z * 8 + (threadIdx.x >> 5);
-  const int        s = blockIdx.y;
-  const bool       valid = u < a.nu && v < a.nv;
-  if (threadIdx.x == 0)
-    s_key = -1;
-  const float val = valid ? ld_elem(proj, ((long long)s * a.nv + v) * a.nu + u) : 0.f;
+  const int u = blockIdx.x * 32 + (threadIdx.x & 31);
+  const int v = blockIdx.z * 8 + (threadIdx.x >> 5);
+  const int s = blockIdx.y;
+  if (u >= a.nu || v >= a.nv)
+    return;
+  const float val = ld_elem(proj, ((long long)s * a.nv + v) * a.nu + u);
   Ray         r;
-  const bool  ok = valid && setup_ray(a, a.P[s], u, v, s, false, r);
-  int         nmid = 0, key = -1;
-  View        w{};
-  float       cf = 0.f;
-  float *     vol = A;
-  if (ok)
+  if (!setup_ray(a, a.P[s], u, v, s, false, r))
+    return;
+  const View   w = view_for(a, r);
+  float *      vol = w.transposed ? At : A;
+  const double c = (double)val * r.norm;
+  long long    o[4];
+  double       wt[4];
+  if (r.fs == r.ns)
   {
-    w = view_for(a, r);
-    vol = w.transposed ? At : A;
-    const double c = (double)val * r.norm;
-    cf = (float)c;
-    long long    o[4];
-    double       wt[4];
-    if (r.fs == r.ns)
-    {
-      border_taps(a, r, w, r.ns, r.curx, r.cury, o, wt);
-      const double f = c * r.len0;
+    border_taps(a, r, w, r.ns, r.curx, r.cury, o, wt);
+    const double f = c * r.len0;
 #pragma unroll
-      for (int q = 0; q < 4; q++)
-        red_add(vol + o[q], (float)(f * wt[q]));
-    }
-    else
-    {
-      border_taps(a, r, w, r.ns, r.curx, r.cury, o, wt);
-      double f = c * (r.resB + 0.5);
-#pragma unroll
-      for (int q = 0; q < 4; q++)
-        red_add(vol + o[q], (float)(f * wt[q]));
-      nmid = abs(r.fs - r.ns) - 1;
-      const int last = r.ns + r.dz * (nmid + 1);
-      border_taps(a, r, w, last, r.curx + (nmid + 1) * r.stepx, r.cury + (nmid + 1) * r.stepy, o, wt);
-      f = c * (r.resE + 0.5);
-#pragma unroll
-      for (int q = 0; q < 4; q++)
-        red_add(vol + o[q], (float)(f * wt[q]));
-    }
-    if (nmid > 0 && r.main != 1)
-      key = r.main * 2 + (r.dz > 0 ? 1 : 0);
+    for (int q = 0; q < 4; q++)
+      red_add(vol + o[q], (float)(f * wt[q]));
+    return;
   }
-  // middle-step geometry (buffer coordinates of the ray's view): the sample
-  // of slice c is x0 + i * sx with i = dz * (c - c0)
-  const float x0 = ok ? (float)(r.curx + r.stepx - w.bx) : 0.f, y0 = ok ? (float)(r.cury + r.stepy - w.by) : 0.f;
-  const float sx = ok ? (float)r.stepx : 0.f, sy = ok ? (float)r.stepy : 0.f;
-  const int   dz = ok ? r.dz : 1;
-  const int   c0 = ok ? r.ns + r.dz - w.bz : 0; // first middle slice
-  const int   c1 = c0 + dz * (nmid - 1);         // last middle slice
-  const int   xmax = max(w.nxp - 2, 0), ymax = max(w.nyp - 2, 0);
-  const Off   ox = (Off)w.ox, oy = (Off)w.oy;
-  const Off   ox1 = (w.nxp > 1) ? ox : 0, oy1 = (w.nyp > 1) ? oy : 0;
-  __syncthreads();
-  if (key >= 0)
-    atomicCAS(&s_key, -1, key);
-  __syncthreads();
-  const int  dom = s_key;
-  const bool in_win = key >= 0 && key == dom;
-  // rays outside the window scheme: scalar global reductions per sample
-  if (nmid > 0 && !in_win)
+  border_taps(a, r, w, r.ns, r.curx, r.cury, o, wt);
+  double f = c * (r.resB + 0.5);
+#pragma unroll
+  for (int q = 0; q < 4; q++)
+    red_add(vol + o[q], (float)(f * wt[q]));
+  const int nmid = abs(r.fs - r.ns) - 1;
+  // the last border step goes first, so the FP64 ray state is dead in the loop
+  const int last = r.ns + r.dz * (nmid + 1);
+  border_taps(a, r, w, last, r.curx + (nmid + 1) * r.stepx, r.cury + (nmid + 1) * r.stepy, o, wt);
+  f = c * (r.resE + 0.5);
+#pragma unroll
+  for (int q = 0; q < 4; q++)
+    red_add(vol + o[q], (float)(f * wt[q]));
+  const float     x0 = (float)(r.curx + r.stepx - w.bx), y0 = (float)(r.cury + r.stepy - w.by);
+  const float     sx = (float)r.stepx, sy = (float)r.stepy, cf = (float)c;
+  const int       xmax = max(w.nxp - 2, 0), ymax = max(w.nyp - 2, 0);
+  const Off       ox = (Off)w.ox, oy = (Off)w.oy;
+  const long long first = (long long)(r.ns + r.dz - w.bz) * w.oz, dslice = r.dz * w.oz;
+  if (r.main != 1)
   {
-    for (int i = 0; i < nmid; i++)
+    // one-voxel in-plane axes: the "+1" neighbour is the voxel itself
+    const bool ca = w.nxp == 1, cb = w.nyp == 1;
+    float4 *   slice = (w.transposed ? QAT : QAN) + first;
+    for (int i = 0; i < nmid; i++, slice += dslice)
     {
       const float x = fmaf((float)i, sx, x0), y = fmaf((float)i, sy, y0);
       const int   ix = min(max((int)floorf(x), 0), xmax), iy = min(max((int)floorf(y), 0), ymax);
       const float lx = x - ix, ly = y - iy;
-      float *     slice = vol + (long long)(c0 + dz * i) * w.oz;
-      splat_global<Off>(slice, ox1, oy1, (Off)ix * ox + (Off)iy * oy, cf * (1.f - ly), cf * ly, lx);
+      const float cy0 = cf * (1.f - ly), cy1 = cf * ly;
+      float4      q = make_float4(cy0 * (1.f - lx), cy1 * (1.f - lx), cy0 * lx, cy1 * lx);
+      if (ca)
+        q = make_float4(q.x + q.z, q.y + q.w, 0.f, 0.f);
+      if (cb)
+        q = make_float4(q.x + q.y, 0.f, q.z + q.w, 0.f);
+      float4 *       dst = slice + ((Off)ix * ox + (Off)iy * oy);
+      // lanes 2k and 2k+1 (neighbouring pixels of one row) often hit the same
+      // quad: the even lane then adds both, the odd lane sends nothing
+      const unsigned act = __activemask();
+      const int      lane = threadIdx.x & 31;
+      const bool     pa = (act >> (lane ^ 1)) & 1u;
+      const unsigned long long pk = __shfl_xor_sync(act, (unsigned long long)dst, 1);
+      const float4   pq = make_float4(__shfl_xor_sync(act, q.x, 1), __shfl_xor_sync(act, q.y, 1),
+                                      __shfl_xor_sync(act, q.z, 1), __shfl_xor_sync(act, q.w, 1));
+      const bool     same = pa && pk == (unsigned long long)dst;
+      if (same && (lane & 1))
+        continue;
+      if (same)
+        q = make_float4(q.x + pq.x, q.y + pq.y, q.z + pq.z, q.w + pq.w);
+      red_add4(dst, q);
     }
   }
-  if (dom < 0)
-    return; // block-uniform: no ray of this CTA uses the window
-  // slice range and bounding lines of the window rays (block reductions)
-  const int   lo = in_win ? min(c0, c1) : INT_MAX, hi = in_win ? max(c0, c1) : INT_MIN;
-  const float cmin_f = block_reduce(in_win ? (float)lo : 3.0e38f, false, red_scratch);
-  const float cmax_f = block_reduce(in_win ? (float)hi : -3.0e38f, true, red_scratch);
-  const int   cmin = (int)cmin_f, cmax = (int)cmax_f;
-  const float ia = (float)(dz * (cmin - c0)), ib = (float)(dz * (cmax - c0));
-  const float xa = fmaf(ia, sx, x0), xb = fmaf(ib, sx, x0), ya = fmaf(ia, sy, y0), yb = fmaf(ib, sy, y0);
-  const float big = 3.0e38f;
-  const float xlo0 = block_reduce(in_win ? xa : big, false, red_scratch);
-  const float xlo1 = block_reduce(in_win ? xb : big, false, red_scratch);
-  const float xhi0 = block_reduce(in_win ? xa : -big, true, red_scratch);
-  const float xhi1 = block_reduce(in_win ? xb : -big, true, red_scratch);
-  const float ylo0 = block_reduce(in_win ? ya : big, false, red_scratch);
-  const float ylo1 = block_reduce(in_win ? yb : big, false, red_scratch);
-  const float yhi0 = block_reduce(in_win ? ya : -big, true, red_scratch);
-  const float yhi1 = block_reduce(in_win ? yb : -big, true, red_scratch);
-  // a window Wa x Wb anchored at floor(lower line) - 1 holds every tap
-  const int   Wa = (int)ceilf(fmaxf(xhi0 - xlo0, xhi1 - xlo1)) + 4;
-  const int   Wb = (int)ceilf(fmaxf(yhi0 - ylo0, yhi1 - ylo1)) + 4;
-  const bool  fits = (long long)Wa * Wb <= kWinCells;
-  const float span = (float)max(cmax - cmin, 1);
-  const float dxl = (xlo1 - xlo0) / span, dyl = (ylo1 - ylo0) / span;
-  const int   ncell = Wa * Wb;
-  if (fits)
-    for (int q = threadIdx.x; q < 2 * kWinCells; q += blockDim.x)
-      (&win[0][0])[q] = 0.f;
-  __syncthreads();
-  // the window rays' view, block-uniform (main direction from the majority key)
-  const View      bw = view_of_main(a, dom >> 1);
-  const long long boz = bw.oz;
-  const Off       box = (Off)bw.ox, boy = (Off)bw.oy;
-  const bool      bafast = bw.ox == 1;
-  float *         bvol = bw.transposed ? At : A;
-  int             pa = 0, pb = 0; // window origin of the previous slice
-  for (int c = cmin; c <= cmax; c++)
+  else
   {
-    const int   k = c - cmin;
-    float *     cur = win[k & 1];
-    const int   wa0 = max((int)floorf(fmaf((float)k, dxl, xlo0)) - 1, 0);
-    const int   wb0 = max((int)floorf(fmaf((float)k, dyl, ylo0)) - 1, 0);
-    if (in_win && c >= lo && c <= hi)
+    const Off ox1 = (w.nxp > 1) ? ox : 0, oy1 = (w.nyp > 1) ? oy : 0;
+    float *   slice = vol + first;
+    for (int i = 0; i < nmid; i++, slice += dslice)
     {
-      const float i = (float)(dz * (c - c0));
-      const float x = fmaf(i, sx, x0), y = fmaf(i, sy, y0);
+      const float x = fmaf((float)i, sx, x0), y = fmaf((float)i, sy, y0);
       const int   ix = min(max((int)floorf(x), 0), xmax), iy = min(max((int)floorf(y), 0), ymax);
       const float lx = x - ix, ly = y - iy;
+      float *     q = slice + ((Off)ix * ox + (Off)iy * oy);
       const float cy0 = cf * (1.f - ly), cy1 = cf * ly;
-      const int   qa = ix - wa0, qb = iy - wb0;
-      const int   da = ox1 != 0 ? 1 : 0, db = oy1 != 0 ? 1 : 0;
-      if (fits && qa >= 0 && qb >= 0 && qa + 1 < Wa && qb + 1 < Wb)
-      {
-        // the window's contiguous axis is the accumulator's (a = x natural, b = z transposed)
-        const int sa = bafast ? 1 : Wb, sb = bafast ? Wa : 1;
-        float *   cell = cur + qa * sa + qb * sb;
-        atomicAdd(cell, cy0 * (1.f - lx));
-        atomicAdd(cell + da * sa, cy0 * lx);
-        atomicAdd(cell + db * sb, cy1 * (1.f - lx));
-        atomicAdd(cell + da * sa + db * sb, cy1 * lx);
-      }
-      else
-        splat_global<Off>(vol + (long long)c * w.oz, ox1, oy1, (Off)ix * ox + (Off)iy * oy, cy0, cy1, lx);
-    }
-    if (k > 0 && fits)
-    {
-      // flush the previous slice's window (complete since the last barrier)
-      float *   prev = win[(k - 1) & 1];
-      float *   pslice = bvol + (long long)(c - 1) * boz;
-      for (int q = threadIdx.x; q < ncell; q += blockDim.x)
-      {
-        const float val2 = prev[q];
-        if (val2 != 0.f)
-        {
-          const int qa2 = bafast ? q % Wa : q / Wb, qb2 = bafast ? q / Wa : q % Wb;
-          red_add(pslice + ((Off)(pa + qa2) * box + (Off)(pb + qb2) * boy), val2);
-          prev[q] = 0.f;
-        }
-      }
-    }
-    pa = wa0;
-    pb = wb0;
-    __syncthreads();
-  }
-  if (fits)
-  {
-    float * prev = win[(cmax - cmin) & 1];
-    float * pslice = bvol + (long long)cmax * boz;
-    for (int q = threadIdx.x; q < ncell; q += blockDim.x)
-    {
-      const float val2 = prev[q];
-      if (val2 != 0.f)
-      {
-        const int qa2 = bafast ? q % Wa : q / Wb, qb2 = bafast ? q / Wa : q % Wb;
-        red_add(pslice + ((Off)(pa + qa2) * box + (Off)(pb + qb2) * boy), val2);
-      }
+      red_add(q, cy0 * (1.f - lx));
+      red_add(q + ox1, cy0 * lx);
+      red_add(q + oy1, cy1 * (1.f - lx));
+      red_add(q + ox1 + oy1, cy1 * lx);
     }
   }
 }
@@ -645,8 +511,9 @@ transpose_zx_kernel(const float * __restrict__ V, float * __restrict__ T, int nx
 // in and x may be null.
 template <typename TV, typename TX>
 __global__ void __launch_bounds__(256)
-fold_transposed_kernel(const TV * in, const float * __restrict__ A, const float * __restrict__ At, TV * out, int nx,
-                       int ny, int nz, const TX * __restrict__ xv, float tau)
+fold_transposed_kernel(const TV * in, const float * __restrict__ A, const float * __restrict__ At,
+                       const float4 * __restrict__ QAN, const float4 * __restrict__ QAT, TV * out, int nx, int ny,
+                       int nz, const TX * __restrict__ xv, float tau)
 {
   __shared__ float tile[32][33];
   const int        y = blockIdx.y;
@@ -656,7 +523,20 @@ fold_transposed_kernel(const TV * in, const float * __restrict__ A, const float 
   {
     const int x = x0 + k, z = z0 + tx;
     if (x < nx && z < nz)
-      tile[k][tx] = At[((long long)x * ny + y) * nz + z];
+    {
+      // transposed quads: a = y (stride nz), b = z (stride 1)
+      const long long t = ((long long)x * ny + y) * nz + z;
+      float           r = At[t] + QAT[t].x;
+      if (z > 0)
+        r += QAT[t - 1].y;
+      if (y > 0)
+      {
+        r += QAT[t - nz].z;
+        if (z > 0)
+          r += QAT[t - nz - 1].w;
+      }
+      tile[k][tx] = r;
+    }
   }
   __syncthreads();
   for (int k = ty; k < 32; k += 8)
@@ -664,8 +544,18 @@ fold_transposed_kernel(const TV * in, const float * __restrict__ A, const float 
     const int z = z0 + k, x = x0 + tx;
     if (z < nz && x < nx)
     {
+      // natural quads: a = x (stride 1), b = y (stride nx)
       const long long o = ((long long)z * ny + y) * nx + x;
-      float           r = A[o] + tile[tx][k];
+      float           r = A[o] + QAN[o].x;
+      if (y > 0)
+        r += QAN[o - nx].y;
+      if (x > 0)
+      {
+        r += QAN[o - 1].z;
+        if (y > 0)
+          r += QAN[o - nx - 1].w;
+      }
+      r += tile[tx][k];
       if (in)
         r += ld_elem(in, o);
       if (xv)
@@ -821,7 +711,7 @@ joseph_forward_scratch_bytes(long long nvox)
 size_t
 joseph_back_scratch_bytes(long long nvox)
 {
-  return 2 * (((size_t)nvox * sizeof(float) + 255) / 256 * 256);
+  return joseph_forward_scratch_bytes(nvox);
 }
 
 namespace
@@ -879,16 +769,18 @@ back_launch(const JosephArgs & a, const TP * proj, void * scratch, const TV * vi
   char *          m = static_cast<char *>(scratch);
   float *         A = reinterpret_cast<float *>(m);
   float *         At = reinterpret_cast<float *>(m + vb);
+  float4 *        QAN = reinterpret_cast<float4 *>(m + 2 * vb);
+  float4 *        QAT = QAN + nvox;
   cudaError_t     e = cudaMemsetAsync(scratch, 0, joseph_back_scratch_bytes(nvox), st);
   if (e != cudaSuccess)
     return e;
   const dim3 grid((unsigned)((a.nu + 31) / 32), (unsigned)a.np, (unsigned)((a.nv + 7) / 8));
   if (nvox < (1ll << 31))
-    joseph_back_kernel<int, TP><<<grid, 256, 0, st>>>(a, proj, A, At);
+    joseph_back_kernel<int, TP><<<grid, 256, 0, st>>>(a, proj, A, At, QAN, QAT);
   else
-    joseph_back_kernel<long long, TP><<<grid, 256, 0, st>>>(a, proj, A, At);
+    joseph_back_kernel<long long, TP><<<grid, 256, 0, st>>>(a, proj, A, At, QAN, QAT);
   const dim3 tg((unsigned)(((nx + 31) / 32) * ((nz + 31) / 32)), (unsigned)ny);
-  fold_transposed_kernel<TV, TX><<<tg, 256, 0, st>>>(vin, A, At, vout, nx, ny, nz, x, tau);
+  fold_transposed_kernel<TV, TX><<<tg, 256, 0, st>>>(vin, A, At, QAN, QAT, vout, nx, ny, nz, x, tau);
   return cudaGetLastError();
 }
 } // namespace

@@ -752,6 +752,46 @@ def legs_summary(legs: dict) -> dict:
     return out
 
 
+def rtk_cuda_leg(torch, proj, product_ms, reps=3) -> dict:
+    """RTK's own CUDA FDK back projector on the same stack: CUDA_reconstruct_conebeam
+    (src/rtkCudaFDKBackProjectionImageFilter.cu, compiled unchanged from RTK's
+    sources into oracle/_ref) driven in 16-projection slabs as
+    CudaFDKBackProjectionImageFilter runs it, each slab copying its projections
+    into a layered texture array.  Device time per backprojection, GUPS, and
+    its error against the oracle on the same y-slab as the headline's check.
+    The reference's GPU kernel, timed beside the product; never the product."""
+    from oracle import oracle as O
+    from oracle import rtk_cuda
+
+    if not rtk_cuda.available():
+        return {"unavailable": "RTK's CUDA back projector was not built (no RTK source tree where the library was built)"}
+    go = oracle_geometry()
+    vo = O.image((NX, NY, NZ), (VOX,) * 3)
+    po = O.image((NU, NV, NP), (PIX, PIX, 1.0))
+    mats = rtk_cuda.filter_matrices(O, go, vo, po)
+    vin = torch.zeros((NZ, NY, NX), device="cuda")
+    vout = torch.empty_like(vin)
+
+    def run():
+        rtk_cuda.fdk_backproject((NU, NV, NP), (NX, NY, NZ), mats, vin.data_ptr(), vout.data_ptr(), proj.data_ptr())
+
+    torch.cuda.synchronize()
+    run()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        run()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    check = oracle_slab_error(torch, proj, vout)
+    return {"ms_per_backprojection": ms, "gups": updates_per_step() / (ms / 1e3) / 1e9,
+            "product_speedup": ms / product_ms, "oracle_rel_l2": check["oracle_rel_l2"],
+            "kernel": "RTK kernel_fdk_3Dgrid, SLAB_SIZE 16, layered-texture bilinear (8-bit weight fractions)"}
+
+
 def emit_leg(name: str, data) -> None:
     """One extra measurement as its own line, 'leg <name> <json>', printed as
     soon as it is measured (not a JSON line, so the headline stays the only
@@ -1073,12 +1113,17 @@ def main():
                             "ms_per_config": [round(t, 2) for t in times]}
         rtkb.ops.fdk_backproject(g, vd, pd, proj, zero, out=vol, stream=stream)
 
-    # the checker on the last timed output (outside every timed region)
+    # the checker on the last timed output (outside every timed region), and
+    # the reference's own CUDA back projector on the same stack
     if rank == 0 and world == 1 and not args.no_cpu_baseline and NX == 512:
         try:
             line["oracle_check"] = oracle_slab_error(torch, proj, vol)
         except Exception as ex:  # the check is reported; a failure to run it is reported too
             line["oracle_check"] = {"oracle_rel_l2": None, "error": str(ex)}
+        try:
+            line["rtk_cuda_reference"] = rtk_cuda_leg(torch, proj, ms_per_step)
+        except Exception as ex:
+            line["rtk_cuda_reference"] = {"error": str(ex)}
 
     if world == 1 and not args.no_extra_legs:
         def leg(name, fn, *a, **kw):

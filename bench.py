@@ -550,19 +550,20 @@ def cg_seconds_to_residual(torch, rtkb, stream, tol=1e-3, max_iter=300, learned_
     (training pairs from the plan's own normal operator, hand-written
     forward/backward kernels, Adam) and solves the same problem with
     flexible PCG; training time is reported separately."""
-    from tests import phantoms
+    import numpy as np
 
-    n = 360
-    g = rtkb.geometry.circular(n, SID, SDD)
-    vd = rtkb.make_desc((256, 256, 256), (1.0, 1.0, 1.0))
-    pd = rtkb.make_desc((512, 384, n), (0.8, 0.8, 1.0))
-    ell = phantoms.random_ellipsoids(20, SEED + 2, centre_radius=60.0, axis_range=(5.0, 60.0))
-    ell[:, 15] *= 0.02  # attenuation in 1/mm: densities 0.002-0.02
-    clean = rtkb.ops.project_ellipsoids(g, pd, ell, stream=stream)
-    i0 = 5e4
-    gen = torch.Generator(device="cuda").manual_seed(SEED + 3)
-    counts = torch.poisson(i0 * torch.exp(-clean), generator=gen).clamp_(min=1.0)
-    p = (-torch.log(counts / i0)).contiguous()
+    from tests import workloads as W
+
+    c = W.C3
+    n = c["n"]
+    g = rtkb.geometry.circular(n, c["sid"], c["sdd"])
+    vd = rtkb.make_desc(c["vol"], (c["vox"],) * 3)
+    pd = rtkb.make_desc((*c["det"], n), (c["pix"], c["pix"], 1.0))
+    # the CG configuration's inputs (tests/workloads.py): analytic projections
+    # of its ellipsoids (on the GPU), seeded pre-log Poisson noise at I0 = 5e4
+    clean = rtkb.ops.project_ellipsoids(g, pd, W.c3_ellipsoids(), stream=stream)
+    p = torch.from_numpy(W.c3_noise(clean.double().cpu().numpy())).cuda()
+    del clean
 
     def solve(net, storage="fp32", max_it=max_iter, backprojector="joseph"):
         x = torch.zeros((256, 256, 256), device="cuda")
@@ -620,16 +621,37 @@ def cg_seconds_to_residual(torch, rtkb, stream, tol=1e-3, max_iter=300, learned_
 
     study = {"iterations": 30}
     t32, r32, x32 = fixed("fp32")
-    t16, r16, x16 = fixed("bf16")
-    bsecs, bit, brel, bper, _, _ = solve(None, storage="bf16", max_it=100)
     study["fp32"] = {"seconds": t32, "relative_residual": r32}
-    study["bf16"] = {"seconds": t16, "relative_residual": r16,
-                     "rel_diff_to_fp32": float((x16 - x32).double().norm() / x32.double().norm()),
-                     "seconds_to_rel_residual_1e-3": bsecs, "iterations_to_1e-3": bit if bsecs else None,
-                     "residual_history": solve.hist}
-    study["oracle_error"] = ("per-variant error against the FP64 oracle's CG: "
-                             "tests/test_gpu_cg.py::test_cg_bf16_storage_precision_against_oracle")
-    del x32, x16
+    for variant in ("bf16", "bf16_direction"):
+        tv, rv, xv = fixed(variant)
+        bsecs, bit, brel, bper, _, _ = solve(None, storage=variant, max_it=100)
+        study[variant] = {"seconds": tv, "relative_residual": rv,
+                          "rel_diff_to_fp32": float((xv - x32).double().norm() / x32.double().norm()),
+                          "seconds_to_rel_residual_1e-3": bsecs, "iterations_to_1e-3": bit if bsecs else None,
+                          "residual_history": solve.hist}
+        del xv
+    del x32
+    study["storage"] = {"bf16": "r, p, A p and the projection temporary in BF16",
+                        "bf16_direction": "p and the projection temporary in BF16; r, A p and x in FP32"}
+    # each variant after 3 iterations against the FP64 oracle's CG of the same
+    # problem (a committed fixture: every 8th voxel of its iterate)
+    try:
+        fx = np.load(os.path.join(ROOT, "tests", "golden", "cg_c3_oracle.npz"))
+        k, stride = int(fx["iterations"]), int(fx["stride"])
+        ref = fx["x_sample"].astype(np.float64)
+        errs = {}
+        for variant in ("fp32", "bf16", "bf16_direction"):
+            x = torch.zeros((256, 256, 256), device="cuda")
+            cg = rtkb.ops.ConjugateGradient(g, vd, pd, storage=variant)
+            cg.start(p, x, stream=stream)
+            cg.iterate(k, stream)
+            torch.cuda.synchronize()
+            cg.close()
+            got = x[::stride, ::stride, ::stride].double().cpu().numpy()
+            errs[variant] = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+        study["oracle_rel_l2_after_3_iterations"] = errs
+    except Exception as ex:
+        study["oracle_rel_l2_after_3_iterations"] = {"error": str(ex)}
     out["precision_study"] = study
     if not learned_pcg:
         return out

@@ -326,10 +326,13 @@ typedef struct rtkb_cg_params
 {
   double tikhonov;       /* Tikhonov weight (RTK's SetTikhonov), 0 = none */
   int    use_cuda_graph; /* 1: replay a captured iteration graph */
-  int    storage;        /* 0: FP32; 1: BF16 storage of the normal-equation vectors (r, p, A p) and of the
-                            projection-domain temporary, FP32 arithmetic and FP64 dots, alpha and beta
-                            (no counterpart in the reference; the iterate stays in the caller's FP32
-                            buffer; no learned preconditioner) */
+  int    storage;        /* precision study (no counterpart in the reference, whose images are float):
+                            0: FP32; 1: BF16 storage of the normal-equation vectors (r, p, A p) and of the
+                            projection-domain temporary; 2: BF16 storage of the direction p and of the
+                            projection-domain temporary, r, A p and the iterate FP32 (the residual
+                            recurrence stays in FP32).  FP32 arithmetic and FP64 dots, alpha and beta in
+                            all; the iterate stays in the caller's FP32 buffer; FP32 plans only for the
+                            learned preconditioner, the support mask and the voxel-based back projector */
   double gamma;          /* Laplacian regularisation weight (RTK's SetGamma): A x += gamma * (-Laplacian(x)) */
   int    backprojector;  /* IterativeConeBeamReconstructionFilter's BackProjectionType
                             (include/rtkIterativeConeBeamReconstructionFilter.h:80-88, .hxx:33-103), the back

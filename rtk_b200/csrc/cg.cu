@@ -32,7 +32,8 @@ struct rtkb_cg
   float                    tikhonov = 0.f;
   float                    gamma = 0.f; // Laplacian regularisation weight (RTK's SetGamma)
   bool                     use_graph = true;
-  bool                     bf16 = false; // R, P, AP and tmp stored as bfloat16 (FP32 arithmetic)
+  bool                     bf16 = false;  // R, P, AP and tmp stored as bfloat16 (FP32 arithmetic)
+  bool                     bf16p = false; // P and tmp stored as bfloat16; R, AP and x FP32
   long long                nvox = 0, npix = 0;
   void *                   mem = nullptr; // one device allocation for everything below
   rtkb::RayProj *          tab = nullptr;
@@ -117,9 +118,9 @@ block_sum(double v)
 }
 
 // partial[b] = sum over block b's fixed slice of a[i] * b[i] (FP64)
-template <typename S>
+template <typename SA, typename SB = SA>
 __global__ void __launch_bounds__(kRedThreads)
-dot_partial_kernel(const S * __restrict__ a, const S * __restrict__ b, long long n, double * partial)
+dot_partial_kernel(const SA * __restrict__ a, const SB * __restrict__ b, long long n, double * partial)
 {
   double s = 0.;
   for (long long i = blockIdx.x * (long long)kRedThreads + threadIdx.x; i < n; i += (long long)kRedBlocks * kRedThreads)
@@ -129,10 +130,11 @@ dot_partial_kernel(const S * __restrict__ a, const S * __restrict__ b, long long
     partial[blockIdx.x] = s;
 }
 
-// x += alpha p; r -= alpha ap; partial of <r, r> (of r as stored)
-template <typename S>
+// x += alpha p; r -= alpha ap; partial of <r, r> (of r as stored); r and ap
+// stored as SR, p as SP
+template <typename SR, typename SP = SR>
 __global__ void __launch_bounds__(kRedThreads)
-update_xr_kernel(float * __restrict__ x, S * __restrict__ r, const S * __restrict__ p, const S * __restrict__ ap,
+update_xr_kernel(float * __restrict__ x, SR * __restrict__ r, const SP * __restrict__ p, const SR * __restrict__ ap,
                  long long n, const double * __restrict__ scal, double * partial)
 {
   const double alpha = scal[S_ALPHA];
@@ -200,9 +202,9 @@ finalize_start_kernel(const double * partial, double * scal)
 }
 
 // p = r + beta p
-template <typename S>
+template <typename SP, typename SR = SP>
 __global__ void __launch_bounds__(256)
-update_p_kernel(S * __restrict__ p, const S * __restrict__ r, long long n, const double * __restrict__ scal)
+update_p_kernel(SP * __restrict__ p, const SR * __restrict__ r, long long n, const double * __restrict__ scal)
 {
   const float beta = (float)scal[S_BETA];
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
@@ -210,9 +212,9 @@ update_p_kernel(S * __restrict__ p, const S * __restrict__ r, long long n, const
 }
 
 // r = r - ap; p = r (start: R0 = B - A x0)
-template <typename S>
+template <typename SR, typename SP = SR>
 __global__ void __launch_bounds__(256)
-start_rp_kernel(S * __restrict__ r, S * __restrict__ p, const S * __restrict__ ap, long long n)
+start_rp_kernel(SR * __restrict__ r, SP * __restrict__ p, const SR * __restrict__ ap, long long n)
 {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
   {
@@ -433,8 +435,23 @@ laplacian_launch(const rtkb_image_desc & v, const TI * x, TO * out, float scale,
   return cudaGetLastError();
 }
 
+// storage of the projection-domain temporary (tmp), of the direction P, and
+// of R and AP: all FP32 (storage 0); all BF16 (storage 1); P and tmp BF16
+// with R, AP and the iterate FP32 (storage 2)
 Elem
 storage(const rtkb_cg * c)
+{
+  return (c->bf16 || c->bf16p) ? Elem::BF16 : Elem::F32;
+}
+
+Elem
+pstore(const rtkb_cg * c)
+{
+  return (c->bf16 || c->bf16p) ? Elem::BF16 : Elem::F32;
+}
+
+Elem
+rstore(const rtkb_cg * c)
 {
   return c->bf16 ? Elem::BF16 : Elem::F32;
 }
@@ -517,28 +534,31 @@ add_laplacian(rtkb_cg * c, const void * in, Elem ie, void * out, Elem oe, cudaSt
                           : laplacian_launch(c->vol, static_cast<const float *>(in), static_cast<float *>(out), -c->gamma, true, st);
 }
 
-template <typename S>
+template <typename SR, typename SP>
 cudaError_t
 enqueue_iteration_t(rtkb_cg * c, cudaStream_t st)
 {
-  S *         P = as<S>(c->P);
-  S *         AP = as<S>(c->AP);
-  S *         R = as<S>(c->R);
-  cudaError_t e = apply_A(c, P, storage(c), AP, storage(c), st);
+  SP *        P = as<SP>(c->P);
+  SR *        AP = as<SR>(c->AP);
+  SR *        R = as<SR>(c->R);
+  cudaError_t e = apply_A(c, P, pstore(c), AP, rstore(c), st);
   if (e != cudaSuccess)
     return e;
-  dot_partial_kernel<S><<<kRedBlocks, kRedThreads, 0, st>>>(P, AP, c->nvox, c->partial);
+  dot_partial_kernel<SP, SR><<<kRedBlocks, kRedThreads, 0, st>>>(P, AP, c->nvox, c->partial);
   finalize_alpha_kernel<<<1, 32, 0, st>>>(c->partial, c->scal);
-  update_xr_kernel<S><<<kRedBlocks, kRedThreads, 0, st>>>(c->x, R, P, AP, c->nvox, c->scal, c->partial);
+  update_xr_kernel<SR, SP><<<kRedBlocks, kRedThreads, 0, st>>>(c->x, R, P, AP, c->nvox, c->scal, c->partial);
   finalize_beta_kernel<<<1, 32, 0, st>>>(c->partial, c->scal);
-  update_p_kernel<S><<<grid_for(c->nvox), 256, 0, st>>>(P, R, c->nvox, c->scal);
+  update_p_kernel<SP, SR><<<grid_for(c->nvox), 256, 0, st>>>(P, R, c->nvox, c->scal);
   return cudaGetLastError();
 }
 
 cudaError_t
 enqueue_iteration(rtkb_cg * c, cudaStream_t st)
 {
-  return c->bf16 ? enqueue_iteration_t<__nv_bfloat16>(c, st) : enqueue_iteration_t<float>(c, st);
+  using B = __nv_bfloat16;
+  if (c->bf16)
+    return enqueue_iteration_t<B, B>(c, st);
+  return c->bf16p ? enqueue_iteration_t<float, B>(c, st) : enqueue_iteration_t<float, float>(c, st);
 }
 
 // One truncated flexible-PCG iteration: Ap; alpha = <p,r>/<p,Ap>;
@@ -641,6 +661,12 @@ rtkb_cg_create(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_
     c->gamma = params ? (float)params->gamma : 0.f;
     c->use_graph = params ? params->use_cuda_graph != 0 : true;
     c->bf16 = params ? params->storage == 1 : false;
+    c->bf16p = params ? params->storage == 2 : false;
+    if (params && (params->storage < 0 || params->storage > 2))
+    {
+      release(c);
+      return fail(RTKB_ERR_INVALID_ARGUMENT, "storage must be 0 (FP32), 1 or 2 (BF16 variants)");
+    }
     // RTK's BackProjectionType: BP_VOXELBASED 0 (its default), BP_JOSEPH 1, BP_CUDAVOXELBASED 2
     const int bpt = params ? params->backprojector : 0;
     if (bpt < 0 || bpt > 2)
@@ -649,7 +675,7 @@ rtkb_cg_create(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_
       return fail(RTKB_ERR_UNSUPPORTED, "back projector: BP_VOXELBASED (0), BP_JOSEPH (1) or BP_CUDAVOXELBASED (2)");
     }
     c->voxel_bp = bpt != 1;
-    if (c->voxel_bp && (c->bf16 || g->g.radius_cylindrical != 0.))
+    if (c->voxel_bp && (c->bf16 || c->bf16p || g->g.radius_cylindrical != 0.))
     {
       release(c);
       return fail(RTKB_ERR_UNSUPPORTED, "the voxel-based back projector in CG needs FP32 storage and a flat panel");
@@ -738,7 +764,7 @@ int
 start_from_rhs(rtkb_cg * c, cudaStream_t st)
 {
   using namespace rtkb;
-  cudaError_t e = apply_A(c, c->x, Elem::F32, c->AP, storage(c), st);
+  cudaError_t e = apply_A(c, c->x, Elem::F32, c->AP, rstore(c), st);
   if (e != cudaSuccess)
     return cuda_fail(e, "CG start");
   if (c->bf16)
@@ -746,6 +772,12 @@ start_from_rhs(rtkb_cg * c, cudaStream_t st)
     using B = __nv_bfloat16;
     start_rp_kernel<B><<<grid_for(c->nvox), 256, 0, st>>>(as<B>(c->R), as<B>(c->P), as<B>(c->AP), c->nvox);
     dot_partial_kernel<B><<<kRedBlocks, kRedThreads, 0, st>>>(as<B>(c->R), as<B>(c->R), c->nvox, c->partial);
+  }
+  else if (c->bf16p)
+  {
+    using B = __nv_bfloat16;
+    start_rp_kernel<float, B><<<grid_for(c->nvox), 256, 0, st>>>(c->R, as<B>(c->P), c->AP, c->nvox);
+    dot_partial_kernel<float><<<kRedBlocks, kRedThreads, 0, st>>>(c->R, c->R, c->nvox, c->partial);
   }
   else
   {
@@ -815,7 +847,7 @@ weights_and_rhs(rtkb_cg * c, const float * d_proj, const float * d_weights, int 
   else
     fill_kernel<<<grid_for(c->npix), 256, 0, st>>>(c->W, 1.f, c->npix);
   // tmp = W .* p in the plan's storage
-  if (c->bf16)
+  if (storage(c) == Elem::BF16)
     mul_kernel<__nv_bfloat16><<<grid_for(c->npix), 256, 0, st>>>(as<__nv_bfloat16>(c->tmp), d_proj, c->W, c->npix);
   else
     mul_kernel<float><<<grid_for(c->npix), 256, 0, st>>>(c->tmp, d_proj, c->W, c->npix);
@@ -854,7 +886,7 @@ rtkb_cg_start(rtkb_cg * c, const float * d_proj, const float * d_weights, int di
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   reset_run(c, d_x);
   // R = b = BP(W .* p)
-  const int rc = weights_and_rhs(c, d_proj, d_weights, displaced_detector, c->R, storage(c), st);
+  const int rc = weights_and_rhs(c, d_proj, d_weights, displaced_detector, c->R, rstore(c), st);
   if (rc != RTKB_OK)
     return rc;
   return start_from_rhs(c, st);
@@ -949,7 +981,7 @@ rtkb_cg_set_support_mask(rtkb_cg * c, const float * d_mask)
   using namespace rtkb;
   if (!c)
     return fail(RTKB_ERR_INVALID_ARGUMENT, "null plan");
-  if (d_mask && c->bf16)
+  if (d_mask && (c->bf16 || c->bf16p))
     return fail(RTKB_ERR_UNSUPPORTED, "support masks need an FP32 plan");
   if (d_mask && c->net)
     return fail(RTKB_ERR_UNSUPPORTED, "support masks and the learned preconditioner do not combine");
@@ -1016,7 +1048,7 @@ rtkb_cg_set_preconditioner(rtkb_cg * c, rtkb_unet * net, int history)
     return fail(RTKB_ERR_INVALID_ARGUMENT, "null plan");
   if (net && (history < 1 || history > kMaxHistory))
     return fail(RTKB_ERR_INVALID_ARGUMENT, "history must be in 1..16");
-  if (net && c->bf16)
+  if (net && (c->bf16 || c->bf16p))
     return fail(RTKB_ERR_UNSUPPORTED, "the learned preconditioner runs on FP32 plans only");
   drop_graphs(c);
   c->x = nullptr; // must be started again

@@ -454,7 +454,9 @@ def _backprojector_code(bp):
 
 
 def _storage_code(storage):
-    codes = {"fp32": 0, "bf16": 1}
+    # "bf16": r, p, A p and the projection temporary stored as BF16;
+    # "bf16_direction": p and the projection temporary BF16, r and A p FP32
+    codes = {"fp32": 0, "bf16": 1, "bf16_direction": 2}
     if storage not in codes:
         raise ValueError(f"storage must be one of {sorted(codes)}")
     return codes[storage]

@@ -168,7 +168,7 @@ def test_cg_bf16_storage_precision_against_oracle(rtkb, oracle):
     niter = 6
     ref_x, ref_res = oracle.cg_joseph(go, vo, po, p, niter)
     errs = {}
-    for storage, graph in (("fp32", True), ("bf16", True), ("bf16", False)):
+    for storage, graph in (("fp32", True), ("bf16", True), ("bf16", False), ("bf16_direction", True)):
         x = torch.zeros(oracle.shape_of(vo), device="cuda")
         cg = rtkb.ops.ConjugateGradient(gl, vd, pd, storage=storage, use_cuda_graph=graph)
         cg.start(to_gpu(p), x, displaced_detector=False)
@@ -187,6 +187,10 @@ def test_cg_bf16_storage_precision_against_oracle(rtkb, oracle):
     # BF16 storage really rounds (error well above FP32's) and stays bounded
     for graph in (True, False):
         assert 10 * errs[("fp32", True)] < errs[("bf16", graph)] < BF16_CG_TOL, errs
+    # a BF16 direction with an FP32 residual recurrence: converges as FP32 does
+    # and stays closer to the exact iterates than all-BF16 storage
+    assert errs[("bf16_direction", True, "residual")] < 2 * errs[("fp32", True, "residual")], errs
+    assert errs[("bf16_direction", True)] < errs[("bf16", True)], errs
 
 
 def test_cg_bf16_operator_and_preconditioner_refusal(rtkb, oracle):

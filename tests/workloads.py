@@ -59,14 +59,19 @@ def c3_ellipsoids():
     return ell
 
 
-def c3_projections(O, g, proj):
-    """C3's noisy line integrals (attenuation units) as float32 values in an
-    FP64 array: the oracle's analytic projection of c3_ellipsoids, counts
-    Poisson(I0 exp(-p)) at I0 = 5e4 clamped to >= 1, p' = -log(counts / I0)."""
-    clean = O.project_ellipsoids(g, proj, c3_ellipsoids())
+def c3_noise(clean):
+    """C3's pre-log Poisson noise on analytic line integrals (attenuation
+    units): counts Poisson(I0 exp(-p)) at I0 = 5e4 clamped to >= 1,
+    p' = -log(counts / I0), as float32."""
     rng = np.random.default_rng(SEED + 3)
-    counts = np.maximum(rng.poisson(C3["i0"] * np.exp(-clean)), 1)
-    return (-np.log(counts / C3["i0"])).astype(np.float32).astype(np.float64)
+    counts = np.maximum(rng.poisson(C3["i0"] * np.exp(-np.asarray(clean, dtype=np.float64))), 1)
+    return (-np.log(counts / C3["i0"])).astype(np.float32)
+
+
+def c3_projections(O, g, proj):
+    """C3's noisy projections (float32 values in an FP64 array) from the
+    oracle's analytic projection of c3_ellipsoids."""
+    return c3_noise(O.project_ellipsoids(g, proj, c3_ellipsoids())).astype(np.float64)
 
 
 def c3_oracle_problem(O):

@@ -774,7 +774,7 @@ def legs_summary(legs: dict) -> dict:
     return out
 
 
-def rtk_cuda_leg(torch, proj, product_ms, reps=3) -> dict:
+def rtk_cuda_leg(torch, proj, product_ms, reps=5) -> dict:
     """RTK's own CUDA FDK back projector on the same stack: CUDA_reconstruct_conebeam
     (src/rtkCudaFDKBackProjectionImageFilter.cu, compiled unchanged from RTK's
     sources into oracle/_ref) driven in 16-projection slabs as
@@ -801,15 +801,18 @@ def rtk_cuda_leg(torch, proj, product_ms, reps=3) -> dict:
     run()
     torch.cuda.synchronize()
     stream = torch.cuda.current_stream()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
+    times = []
     for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
         run()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / reps
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    ms = statistics.median(times)
     check = oracle_slab_error(torch, proj, vout)
-    return {"ms_per_backprojection": ms, "gups": updates_per_step() / (ms / 1e3) / 1e9,
+    return {"ms_per_backprojection": ms, "ms_each": [round(t, 1) for t in times],
+            "gups": updates_per_step() / (ms / 1e3) / 1e9,
             "product_speedup": ms / product_ms, "oracle_rel_l2": check["oracle_rel_l2"],
             "kernel": "RTK kernel_fdk_3Dgrid, SLAB_SIZE 16, layered-texture bilinear (8-bit weight fractions)"}
 

@@ -70,8 +70,10 @@ def c3_noise(clean):
 
 def c3_projections(O, g, proj):
     """C3's noisy projections (float32 values in an FP64 array) from the
-    oracle's analytic projection of c3_ellipsoids."""
-    return c3_noise(O.project_ellipsoids(g, proj, c3_ellipsoids())).astype(np.float64)
+    oracle's analytic projection of c3_ellipsoids, rounded to float32 before
+    the noise (as the GPU's analytic projector stores it, so both give the
+    same noisy stack)."""
+    return c3_noise(O.project_ellipsoids(g, proj, c3_ellipsoids()).astype(np.float32)).astype(np.float64)
 
 
 def c3_oracle_problem(O):

@@ -543,6 +543,12 @@ int       rtkb_unet_train_step(rtkb_unet * net, int batch, int nx, int ny, int n
                                const float * d_target, int loss_margin, double learning_rate, int update,
                                double * loss, void * stream);
 void      rtkb_unet_destroy(rtkb_unet * net);
+/* Selects the forward / data-gradient convolution kernel (process-wide; no counterpart in the
+ * reference): 1 (default) = halo and weights of each input-channel chunk loaded by TMA into one
+ * shared-memory stage; 2 = the same with two stages, the next chunk's loads overlapping the current
+ * chunk's tcgen05 MMAs (one stage where two do not fit); 0 = halo gathered by the threads.  All
+ * compute the same MMAs in the same order; kept to compare them. */
+int       rtkb_unet_set_conv_pipeline(int enable);
 
 /* Flexible PCG: with a network set (before rtkb_cg_start; NULL removes it) each
  * iteration preconditions the residual, z = s N(r / s), steps with

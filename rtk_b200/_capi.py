@@ -227,6 +227,7 @@ SIGNATURES.update({
     "rtkb_unet_train_step": (C.c_int, [_V, C.c_int, C.c_int, C.c_int, C.c_int, _V, _V, C.c_int, C.c_double,
                                        C.c_int, _D, _V]),
     "rtkb_unet_destroy": (None, [_V]),
+    "rtkb_unet_set_conv_pipeline": (C.c_int, [C.c_int]),
 })
 
 

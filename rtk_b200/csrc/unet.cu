@@ -375,6 +375,274 @@ conv_fwd_tc_kernel(ConvIn in, const bf16 * __restrict__ wpack, TcDims d, bf16 * 
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)kCols));
 }
 
+// ---- the same convolution, pipelined: TMA halo loads overlapped with the MMAs ----------------------
+// Two stages of [halo | weights].  While the MMAs of chunk c read stage c & 1,
+// stage (c + 1) & 1 is filled with chunk c + 1 once the MMAs of chunk c - 1
+// (its previous reader) have completed.  A full-resolution source is loaded
+// by TMA: two boxes of 8 channels x 10 x 18 x 6 voxels (5-D tensor map over
+// [batch][z][y][x][channel]), which land exactly in the [k-half][voxel][16 B]
+// layout the A descriptors read, zero-filled outside the volume; the chunk's
+// weights [27][2][N][8] come by one bulk copy.  A half-resolution source
+// (nearest up-sampling, decoder inputs) is gathered by the threads into the
+// same layout, still overlapped with the previous chunk's MMAs.  Every wait is
+// bounded; a wait that gives up ends the chunk loop on every thread.
+__device__ __forceinline__ void
+tma_load_5d(void * dst, const CUtensorMap * map, int c0, int c1, int c2, int c3, int c4, uint64_t * bar)
+{
+  asm volatile("cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+               " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(rtkb::dev::smem_u32(dst)),
+               "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4),
+               "r"(rtkb::dev::smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void
+bulk_load(void * dst, const void * src, uint32_t bytes, uint64_t * bar)
+{
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                 rtkb::dev::smem_u32(dst)),
+               "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(rtkb::dev::smem_u32(bar))
+               : "memory");
+}
+
+template <int N, int NS>
+struct PipeLayout
+{
+  static constexpr int kW = 27 * 2 * N * 16;            // weight bytes per chunk
+  static constexpr int kStage = kCHaloBytes + kW;        // one stage (multiple of 128 bytes)
+  static constexpr int kBars = NS * kStage;              // full[2], done[2], TMEM slot
+  static constexpr int kTotal = kBars + 64 + 128;        // + alignment slack of the dynamic base
+  static_assert(kCHaloBytes % 128 == 0 && kW % 128 == 0, "TMA destinations need 128-byte alignment");
+};
+
+template <int N, int NS>
+__global__ void __launch_bounds__(128, 1)
+conv_fwd_pipe_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b, int tma_a,
+                     int tma_b, ConvIn in, const bf16 * __restrict__ wpack, TcDims d, bf16 * __restrict__ out,
+                     const bf16 * __restrict__ mask, int relu)
+{
+  using L = PipeLayout<N, NS>;
+  constexpr int      kCols = (kCZ * N <= 32) ? 32 : (kCZ * N <= 64) ? 64 : (kCZ * N <= 128) ? 128 : (kCZ * N <= 256) ? 256 : 512;
+  constexpr uint32_t kIdesc = umma_idesc_bf16<N>();
+  extern __shared__ __align__(128) char smem_raw[];
+  char * smem = reinterpret_cast<char *>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+  uint64_t *         full = reinterpret_cast<uint64_t *>(smem + L::kBars);
+  uint64_t *         done = full + 2;
+  uint32_t *         tmem_slot = reinterpret_cast<uint32_t *>(done + 2);
+  __shared__ int     s_ok;
+  const int          warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  long long          tile = blockIdx.x;
+  const int          tx = (int)(tile % d.tx);
+  tile /= d.tx;
+  const int ty = (int)(tile % d.ty);
+  tile /= d.ty;
+  const int tz = (int)(tile % d.tz);
+  const int n = (int)(tile / d.tz);
+  const int x0 = tx * kCX, y0 = ty * kCY, z0 = tz * kCZ;
+
+  if (warp == 0)
+  {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(rtkb::dev::smem_u32(tmem_slot)),
+                 "r"((uint32_t)kCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (threadIdx.x == 0)
+  {
+    for (int q = 0; q < 2; q++)
+    {
+      rtkb::dev::mbar_init(&full[q], 1);
+      rtkb::dev::mbar_init(&done[q], 1);
+    }
+    rtkb::dev::fence_barrier_init();
+    s_ok = 1;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = *tmem_slot;
+  const int      nchunks = (in.ca + in.cb) / 16;
+
+  // fill stage st with chunk c (block-uniform branch)
+  auto load_chunk = [&](int c, int st) {
+    char *       halo = smem + st * L::kStage;
+    char *       wsm = halo + kCHaloBytes;
+    const bool   from_a = c * 16 < in.ca;
+    const int    c0 = from_a ? c * 16 : c * 16 - in.ca;
+    const bool   tma = from_a ? tma_a != 0 : tma_b != 0;
+    const bf16 * wsrc = wpack + (size_t)c * 27 * 2 * N * 8;
+    if (tma)
+    {
+      if (threadIdx.x == 0)
+      {
+        const CUtensorMap * map = from_a ? &map_a : &map_b;
+        rtkb::dev::mbar_arrive_expect_tx(&full[st], (uint32_t)(kCHaloBytes + L::kW));
+        tma_load_5d(halo, map, c0, x0 - 1, y0 - 1, z0 - 1, n, &full[st]);
+        tma_load_5d(halo + kCHalo * 16, map, c0 + 8, x0 - 1, y0 - 1, z0 - 1, n, &full[st]);
+        bulk_load(wsm, wsrc, (uint32_t)L::kW, &full[st]);
+      }
+      return;
+    }
+    const int    cs = from_a ? in.ca : in.cb;
+    const bf16 * src = from_a ? in.a : in.b;
+    const bool   half = from_a && in.a_half;
+    const int    snx = half ? d.nx >> 1 : d.nx, sny = half ? d.ny >> 1 : d.ny, snz = half ? d.nz >> 1 : d.nz;
+    for (int i = threadIdx.x; i < kCHalo * 2; i += 128)
+    {
+      const int hv = i >> 1, h = i & 1;
+      const int hx = hv % kCHX, hy = (hv / kCHX) % kCHY, hz = hv / (kCHX * kCHY);
+      const int gx = x0 - 1 + hx, gy = y0 - 1 + hy, gz = z0 - 1 + hz;
+      uint4     v = make_uint4(0u, 0u, 0u, 0u);
+      if (gx >= 0 && gx < d.nx && gy >= 0 && gy < d.ny && gz >= 0 && gz < d.nz)
+      {
+        const int sx = half ? gx >> 1 : gx, sy = half ? gy >> 1 : gy, sz = half ? gz >> 1 : gz;
+        v = *reinterpret_cast<const uint4 *>(src + ((((long long)n * snz + sz) * sny + sy) * snx + sx) * cs + c0 + h * 8);
+      }
+      *reinterpret_cast<uint4 *>(halo + (h * kCHalo + hv) * 16) = v;
+    }
+    const uint4 * w4 = reinterpret_cast<const uint4 *>(wsrc);
+    uint4 *       wdst = reinterpret_cast<uint4 *>(wsm);
+    for (int i = threadIdx.x; i < 27 * 2 * N; i += 128)
+      wdst[i] = w4[i];
+    // the tensor cores read this stage through the async proxy
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0)
+      rtkb::dev::mbar_arrive(&full[st]);
+  };
+
+  // thread 0's count of fills / commits issued and seen complete per stage (to
+  // drain in-flight copies and MMAs if a wait gives up)
+  int fill_issued[2] = { 0, 0 }, fill_seen[2] = { 0, 0 }, commit_issued[2] = { 0, 0 }, commit_seen[2] = { 0, 0 };
+  if (nchunks > 0)
+  {
+    load_chunk(0, 0);
+    fill_issued[0]++;
+  }
+  bool ok = true;
+  for (int c = 0; c < nchunks && ok; c++)
+  {
+    const int      st = c % NS;
+    const uint32_t par = (uint32_t)((c / NS) & 1);
+    if (threadIdx.x == 0)
+    {
+      if (rtkb::dev::mbar_wait(&full[st], par))
+      {
+        fill_seen[st]++;
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        const uint32_t halo_s = rtkb::dev::smem_u32(smem + st * L::kStage);
+        const uint32_t w_s = halo_s + (uint32_t)kCHaloBytes;
+#pragma unroll 1
+        for (int t = 0; t < 27; t++)
+        {
+          const int      dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
+          const uint64_t db = umma_desc(w_s + (uint32_t)(t * 2 * N * 16), (uint32_t)(N * 16), 128u);
+#pragma unroll
+          for (int zl = 0; zl < kCZ; zl++)
+          {
+            const int      hv0 = ((zl + dz) * kCHY + dy) * kCHX + dx;
+            const uint64_t da = umma_desc(halo_s + (uint32_t)(hv0 * 16), (uint32_t)(kCHalo * 16), (uint32_t)(kCHX * 16));
+            umma_bf16(tmem + (uint32_t)(zl * N), da, db, kIdesc, (c > 0 || t > 0) ? 1u : 0u);
+          }
+        }
+        umma_commit(&done[st]);
+        commit_issued[st]++;
+      }
+      else
+        s_ok = 0;
+    }
+    if (c + 1 < nchunks)
+    {
+      // chunk c + 1's stage is free once its previous reader, chunk c + 1 - NS,
+      // has completed its MMAs
+      const int nx_st = (c + 1) % NS, prev = c + 1 - NS;
+      bool      free_ok = true;
+      if (prev >= 0)
+      {
+        free_ok = __syncthreads_and(s_ok ? 1 : 0) != 0 && rtkb::dev::mbar_wait(&done[nx_st], (uint32_t)((prev / NS) & 1));
+        if (free_ok && threadIdx.x == 0)
+          commit_seen[nx_st]++;
+      }
+      free_ok = __syncthreads_and(free_ok && s_ok ? 1 : 0) != 0;
+      if (free_ok)
+      {
+        load_chunk(c + 1, nx_st);
+        fill_issued[nx_st]++;
+      }
+      ok = free_ok;
+    }
+    ok = __syncthreads_and(ok && s_ok ? 1 : 0) != 0;
+  }
+  // the last chunk's MMAs
+  if (ok && nchunks > 0)
+  {
+    const int  sl = (nchunks - 1) % NS;
+    const bool got = rtkb::dev::mbar_wait(&done[sl], (uint32_t)(((nchunks - 1) / NS) & 1));
+    if (got && threadIdx.x == 0)
+      commit_seen[sl]++;
+    ok = __syncthreads_and(got ? 1 : 0) != 0;
+  }
+  if (!ok && threadIdx.x == 0)
+  {
+    // a wait gave up: let this CTA's own copies and MMAs finish (bounded)
+    // before its shared memory and tensor memory are released
+    for (int q = 0; q < NS; q++)
+    {
+      if (fill_issued[q] > fill_seen[q])
+        rtkb::dev::mbar_wait(&full[q], (uint32_t)(fill_seen[q] & 1));
+      if (commit_issued[q] > commit_seen[q])
+        rtkb::dev::mbar_wait(&done[q], (uint32_t)(commit_seen[q] & 1));
+    }
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;");
+
+  if (ok)
+  {
+    const int m = warp * 32 + lane;
+    const int x = x0 + (m & 7), y = y0 + (m >> 3);
+#pragma unroll 1
+    for (int zl = 0; zl < kCZ; zl++)
+    {
+      const int       z = z0 + zl;
+      const bool      inside = x < d.nx && y < d.ny && z < d.nz;
+      const long long vbase = ((((long long)n * d.nz + z) * d.ny + y) * d.nx + x) * N;
+#pragma unroll
+      for (int cb = 0; cb < N; cb += 16)
+      {
+        uint32_t r[16];
+        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(zl * N + cb), r);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (!inside)
+          continue;
+        unsigned o[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++)
+        {
+          float v0 = __uint_as_float(r[2 * q]), v1 = __uint_as_float(r[2 * q + 1]);
+          if (relu)
+          {
+            v0 = fmaxf(v0, 0.f);
+            v1 = fmaxf(v1, 0.f);
+          }
+          if (mask)
+          {
+            const float2 mk = unpack_bf16x2(*reinterpret_cast<const unsigned *>(mask + vbase + cb + 2 * q));
+            v0 = mk.x > 0.f ? v0 : 0.f;
+            v1 = mk.y > 0.f ? v1 : 0.f;
+          }
+          o[q] = pack_bf16x2(v0, v1);
+        }
+        uint4 * dst = reinterpret_cast<uint4 *>(out + vbase + cb);
+        dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
+        dst[1] = make_uint4(o[4], o[5], o[6], o[7]);
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)kCols));
+}
+
 // ---- weight gradient --------------------------------------------------------------------------------
 // dW[t][ci][co] += sum_v in[v + t - 1][ci] * g[v][co] for the 16 input channels
 // of chunk blockIdx.y; CTAs stride over voxel tiles and flush once with
@@ -895,10 +1163,61 @@ tmem_bounded_smem(int need, int cols)
   return std::max(need, floor_bytes);
 }
 
+// Convolution kernel (rtkb_unet_set_conv_pipeline): 0 = thread-loaded halo,
+// one stage; 1 = TMA-loaded halo, one stage (default); 2 = TMA-loaded halo,
+// two stages (the widest data-gradient layers, whose two stages do not fit in
+// shared memory, use one).
+int g_conv_pipeline = 1;
+
 constexpr int
 tmem_cols(int n)
 {
   return (n <= 32) ? 32 : (n <= 64) ? 64 : (n <= 128) ? 128 : (n <= 256) ? 256 : 512;
+}
+
+// 5-D TMA descriptor of an activation [batch][z][y][x][c] at full resolution,
+// box 8 channels x the 10 x 18 x 6 halo; false if it cannot be encoded.
+bool
+encode_activation_map(CUtensorMap & map, const bf16 * base, int c, int nx, int ny, int nz, int batch)
+{
+  std::memset(&map, 0, sizeof(map));
+  rtkb::EncodeTiledFn enc = rtkb::tensor_map_encoder();
+  if (!enc || !base || (reinterpret_cast<uintptr_t>(base) % 16) != 0 || (c * 2) % 16 != 0)
+    return false;
+  const unsigned long long e = 2;
+  const unsigned long long dims[5] = { (unsigned long long)c, (unsigned long long)nx, (unsigned long long)ny,
+                                       (unsigned long long)nz, (unsigned long long)batch };
+  const unsigned long long strides[4] = { c * e, c * e * nx, c * e * nx * ny, c * e * nx * ny * nz };
+  const unsigned           box[5] = { 8u, (unsigned)kCHX, (unsigned)kCHY, (unsigned)kCHZ, 1u };
+  const unsigned           estr[5] = { 1u, 1u, 1u, 1u, 1u };
+  return enc(&map, (int)CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5u, const_cast<bf16 *>(base), dims, strides, box, estr,
+             (int)CU_TENSOR_MAP_INTERLEAVE_NONE, (int)CU_TENSOR_MAP_SWIZZLE_NONE, (int)CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             (int)CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == 0;
+}
+
+template <int N, int NS>
+void
+conv_fwd_pipe_launch(const ConvIn & in, const bf16 * wp, const Dims & d0, bf16 * out, const bf16 * mask, int relu,
+                     cudaStream_t st)
+{
+  using L = PipeLayout<N, NS>;
+  const int   smem = tmem_bounded_smem(L::kTotal, tmem_cols(kCZ * N));
+  static bool configured = false; // attribute set once per process (same value on every device)
+  if (!configured)
+  {
+    cudaFuncSetAttribute(conv_fwd_pipe_kernel<N, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    configured = true;
+  }
+  CUtensorMap ma, mb;
+  const int   ta = (in.ca > 0 && !in.a_half) ? (encode_activation_map(ma, in.a, in.ca, d0.nx, d0.ny, d0.nz, d0.batch) ? 1 : 0) : 0;
+  const int   tb = in.cb > 0 ? (encode_activation_map(mb, in.b, in.cb, d0.nx, d0.ny, d0.nz, d0.batch) ? 1 : 0) : 0;
+  if (!ta)
+    std::memset(&ma, 0, sizeof(ma));
+  if (!tb)
+    std::memset(&mb, 0, sizeof(mb));
+  const TcDims    d = make_tc_dims(d0.nx, d0.ny, d0.nz, d0.batch);
+  const long long tiles = (long long)d.tx * d.ty * d.tz * d.batch;
+  conv_fwd_pipe_kernel<N, NS><<<(unsigned)tiles, 128, smem, st>>>(ma, mb, ta, tb, in, wp, d, out, mask, relu);
 }
 
 template <int N>
@@ -906,6 +1225,19 @@ void
 conv_fwd_tc_launch(const ConvIn & in, const bf16 * wp, const Dims & d0, bf16 * out, const bf16 * mask, int relu,
                    cudaStream_t st)
 {
+  if (g_conv_pipeline == 1)
+  {
+    conv_fwd_pipe_launch<N, 1>(in, wp, d0, out, mask, relu, st);
+    return;
+  }
+  if constexpr (PipeLayout<N, 2>::kTotal <= 227 * 1024)
+  {
+    if (g_conv_pipeline == 2)
+    {
+      conv_fwd_pipe_launch<N, 2>(in, wp, d0, out, mask, relu, st);
+      return;
+    }
+  }
   const int smem = tmem_bounded_smem(kCHaloBytes + 27 * 2 * N * 16 + 16, tmem_cols(kCZ * N));
   static bool configured = false; // attribute set once per process (same value on every device)
   if (!configured)
@@ -1307,6 +1639,15 @@ rtkb_unet_reserve(rtkb_unet * u, int batch, int nx, int ny, int nz)
     return fail(RTKB_ERR_INVALID_ARGUMENT, "null network");
   const int rc = check_dims(batch, nx, ny, nz);
   return rc != RTKB_OK ? rc : reserve_forward(u, batch, nx, ny, nz);
+}
+
+extern "C" int
+rtkb_unet_set_conv_pipeline(int enable)
+{
+  if (enable < 0 || enable > 2)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "convolution kernel: 0, 1 or 2");
+  g_conv_pipeline = enable;
+  return RTKB_OK;
 }
 
 extern "C" int

@@ -122,3 +122,32 @@ def test_unet_rejects_sizes_not_multiple_of_4(rtkb):
     with pytest.raises(rtkb.RtkbError):
         net.forward(to_gpu(np.zeros((1, 10, 16, 16), np.float32)))
     net.close()
+
+
+@pytest.mark.parametrize("shape", [(2, 12, 20, 24), (1, 32, 32, 32)])
+def test_unet_pipelined_convolution_equals_single_stage(rtkb, shape):
+    """The convolution kernels with TMA halo and weight loads (one stage, the
+    default, and two stages; zero fill outside the volume by the TMA unit,
+    thread gathers for the up-sampled decoder inputs) issue the same MMAs in
+    the same order as the thread-loaded kernel: the forward pass is
+    bit-identical, and the training gradients (which add FP32 atomics in the
+    weight gradient) agree to rounding."""
+    lib = rtkb.load()
+    net = _net(13)
+    rng = np.random.default_rng(sum(shape) + 1)
+    x = rng.standard_normal(shape).astype(np.float32)
+    t = rng.standard_normal(shape).astype(np.float32) * 0.2
+    out, grads = {}, {}
+    try:
+        for pipe in (1, 2, 0):
+            assert lib.rtkb_unet_set_conv_pipeline(pipe) == 0
+            out[pipe] = to_np(net.forward(to_gpu(x), normalize=False))
+            net.train_step(to_gpu(x), to_gpu(t), update=False)
+            grads[pipe] = net.get_gradients()
+    finally:
+        lib.rtkb_unet_set_conv_pipeline(1)
+    for pipe in (1, 2):
+        assert np.array_equal(out[0], out[pipe])
+        assert rel_l2(grads[pipe], grads[0]) < 1e-5
+    assert rtkb.ops.device_status() == 0
+    net.close()

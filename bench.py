@@ -40,8 +40,8 @@ L1_BYTES_PER_UPDATE = 16  # four 4-byte taps of one bilinear interpolation
 # DRAM bytes (read + write) of one backprojection launch of this workload, recorded from a 1-pass ncu
 # capture (dram__bytes_read.sum + dram__bytes_write.sum) of the kernel as of BP_TRAFFIC_COMMIT; a
 # recorded figure, not a measurement of the build that runs.
-BP_LAUNCH_DRAM_BYTES = 69.86e9 + 0.6506e9
-BP_TRAFFIC_COMMIT = "aff05f8"
+BP_LAUNCH_DRAM_BYTES = 69.3747e9 + 0.5982e9
+BP_TRAFFIC_COMMIT = "0d49521"
 WORKLOAD = {"workload": "FDK backprojection 512^3 @0.5mm <- 720 x 1024x768 @0.388mm, SID 1000, SDD 1536, 360 deg",
             "volume": [NX, NY, NZ], "projections": [NU, NV, NP], "dtype_storage": "float32",
             "l2_policy": "inputs larger than L2 (2.26 GB projection stack, 0.54 GB volume)"}
@@ -332,59 +332,116 @@ def batch_leg(torch, rtkb, stream, n=64, reps=3):
             "note": "FDK backprojection part of the batched configuration; its CG part is the batched_cg entry"}
 
 
-def batch_cg_leg(torch, rtkb, stream, n=64, niter=10):
-    """CG half of the batched configuration: n seeded problems (volumes
-    64^3-256^3, 90-360 projections, detectors 128^2-512^2, SID 800-1200 mm),
-    niter CG iterations each with the Joseph pair.  Batched: one CUDA graph
-    launch runs every problem's iterations, each problem on its own branch;
-    against the same plans iterated one problem after another."""
+def c4_leg(torch, rtkb, stream, n=64, niter=10):
+    """The batched configuration end to end: n seeded problems (volumes
+    64^3-256^3, 90-360 projections, detectors 128^2-512^2, SID 800-1200 mm) of
+    random-ellipsoid phantoms, each reconstructed by FDK (weights + Hann ramp,
+    then backprojection) followed by niter CG iterations (Joseph pair) started
+    from the FDK volume.  Batched: the preprocessing of every stack in stream
+    order, every backprojection in one persistent launch (autotuned
+    configuration), every problem's CG start and iterations in one CUDA graph
+    launch (a branch per problem).  Against the same work problem after problem
+    (the same CG plans, one after another).  Plans and the backprojection batch
+    are prepared outside both timed regions.  The two smallest problems' FDK
+    volumes are checked against the FP64 oracle's FDK."""
     import numpy as np
 
     from rtk_b200._capi import check
+    from tests import phantoms
 
     rng = np.random.default_rng(SEED + 8)
     probs = []
-    samples = 0.0
     for _ in range(n):
         nv_ = int(rng.integers(64, 257))
         npj = int(rng.integers(90, 361))
         nu = int(rng.integers(32, 129)) * 4
         nvd = int(rng.integers(128, 513))
         sid = float(rng.uniform(800, 1200))
-        g = rtkb.geometry.circular(npj, sid, 1.5 * sid)
         vsp = min(1.0, 0.9 * nu / (nv_ * 1.5))
-        vd = rtkb.make_desc((nv_, nv_, nv_), (vsp,) * 3)
-        pd = rtkb.make_desc((nu, nvd, npj), (1.0, 1.0, 1.0))
-        probs.append((g, vd, pd, torch.rand((npj, nvd, nu), device="cuda"),
-                      torch.zeros((nv_, nv_, nv_), device="cuda"), None, False))
-    batch = rtkb.ops.ConjugateGradientBatch(probs)
-    batch.start(stream)
-    batch.iterate(niter, stream)  # capture and a first replay
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    batch.iterate(niter, stream)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    t_batch = e0.elapsed_time(e1)
-    lib = rtkb.load()
-    e0.record(stream)
-    for i in range(n):
-        plan = lib.rtkb_cg_batch_plan(batch._h, i)
-        check(lib.rtkb_cg_iterate(plan, niter, stream.cuda_stream))
-    e1.record(stream)
-    torch.cuda.synchronize()
-    t_seq = e0.elapsed_time(e1)
-    assert rtkb.ops.device_status(stream) == 0
-    batch.close()
-    del probs
-    return {"workload": f"{n} CG problems x {niter} iterations (Joseph pair), volumes 64^3-256^3, 90-360 "
-                        "projections, detectors 128^2-512^2, SID 800-1200 mm (seeded)",
-            "batched_graph_ms": t_batch, "one_problem_after_another_ms": t_seq,
-            "speedup": t_seq / t_batch if t_batch else None,
-            "note": "one CUDA graph launch with a branch per problem; the Joseph pair is not a persistent "
-                    "multi-problem kernel"}
+        P = {"nv": nv_, "np": npj, "nu": nu, "nvd": nvd, "sid": sid, "vsp": vsp,
+             "ell": phantoms.random_ellipsoids(8, int(rng.integers(1 << 30)), axis_range=(0.05 * nv_ * vsp, 0.25 * nv_ * vsp),
+                                               centre_radius=0.2 * nv_ * vsp, density_range=(0.002, 0.02))}
+        P["g"] = rtkb.geometry.circular(npj, sid, 1.5 * sid)
+        P["vd"] = rtkb.make_desc((nv_,) * 3, (vsp,) * 3)
+        P["pd"] = rtkb.make_desc((nu, nvd, npj), (1.0, 1.0, 1.0))
+        P["p"] = rtkb.ops.project_ellipsoids(P["g"], P["pd"], P["ell"], stream=stream)
+        P["f"] = torch.empty_like(P["p"])
+        P["zero"] = torch.zeros((nv_,) * 3, device="cuda")
+        P["x"] = torch.zeros_like(P["zero"])
+        probs.append(P)
+    ramp = rtkb.ops.ramp_params(hann=1.0)
 
+    def preprocess(P):
+        rtkb.ops.fdk_preprocess(P["g"], P["pd"], P["p"], ramp, stream=stream, out=P["f"])
+
+    for P in probs:
+        preprocess(P)
+    bp_args = [(P["g"], P["vd"], P["pd"], P["f"], P["zero"], P["x"]) for P in probs]
+    best, _, _ = rtkb.ops.backproject_autotune(bp_args, repeats=1, stream=stream)
+    bpb = rtkb.ops.BackprojectionBatch(bp_args, config=best)
+    cgb = rtkb.ops.ConjugateGradientBatch([(P["g"], P["vd"], P["pd"], P["p"], P["x"], None, False) for P in probs])
+    lib = rtkb.load()
+    plans = [lib.rtkb_cg_batch_plan(cgb._h, i) for i in range(n)]
+
+    def batched():
+        for P in probs:
+            preprocess(P)
+        bpb.execute(stream)
+        cgb.start(stream)
+        cgb.iterate(niter, stream)
+
+    def one_after_another():
+        for P, plan in zip(probs, plans):
+            preprocess(P)
+            rtkb.ops.fdk_backproject(P["g"], P["vd"], P["pd"], P["f"], P["zero"], out=P["x"], stream=stream)
+            check(lib.rtkb_cg_start(plan, rtkb.ops._ptr(P["p"]), None, 0, rtkb.ops._ptr(P["x"]), stream.cuda_stream))
+            check(lib.rtkb_cg_iterate(plan, niter, stream.cuda_stream))
+
+    batched()  # captures the CG graph
+    torch.cuda.synchronize()
+    times = {}
+    for name, fn in (("batched", batched), ("one_after_another", one_after_another)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times[name] = e0.elapsed_time(e1)
+    assert rtkb.ops.device_status(stream) == 0
+    # the FP64 oracle's FDK of the two smallest problems (the batched backprojection's volumes)
+    errs = {}
+    try:
+        from oracle import oracle as O
+
+        bpb.execute(stream)
+        torch.cuda.synchronize()
+        order = sorted(range(n), key=lambda i: probs[i]["nv"] ** 3 * probs[i]["np"])[:2]
+        for i in order:
+            P = probs[i]
+            go = O.Geometry()
+            for k in range(P["np"]):
+                go.add_projection(P["sid"], 1.5 * P["sid"], k * 360.0 / P["np"])
+            vo = O.image((P["nv"],) * 3, (P["vsp"],) * 3)
+            po = O.image((P["nu"], P["nvd"], P["np"]), (1.0, 1.0, 1.0))
+            pr = P["p"].double().cpu().numpy()
+            ref = O.backproject(go, vo, po, O.ramp_filter(po, O.fdk_weight(go, po, pr), O.ramp_params(hann=1.0)),
+                                fdk=True)
+            got = P["x"].double().cpu().numpy()
+            errs[f"problem_{i}_{P['nv']}^3_{P['np']}x{P['nu']}x{P['nvd']}"] = float(
+                np.linalg.norm(got - ref) / np.linalg.norm(ref))
+    except Exception as ex:
+        errs = {"error": str(ex)}
+    bpb.close()
+    cgb.close()
+    return {"workload": f"{n} problems: FDK (weights + Hann ramp + backprojection) then {niter} CG iterations "
+                        "(Joseph pair) from the FDK volume; volumes 64^3-256^3, 90-360 projections, detectors "
+                        "128^2-512^2, SID 800-1200 mm (seeded ellipsoid phantoms)",
+            "batched_ms": times["batched"], "one_problem_after_another_ms": times["one_after_another"],
+            "speedup": times["one_after_another"] / times["batched"],
+            "autotuned_config": best,
+            "fdk_oracle_rel_l2": errs,
+            "launches_batched": "preprocessing per problem, one persistent backprojection launch, one CUDA graph "
+                                "launch for every problem's CG start and iterations"}
 
 def sart_leg(torch, rtkb, stream, niter=1):
     """SART (RTK's defaults: lambda 0.3, one projection per subset, Joseph
@@ -1164,7 +1221,7 @@ def main():
         del proj
         leg("joseph_forward", joseph_forward_leg, torch, rtkb, lib, stream)
         leg("batched", batch_leg, torch, rtkb, stream)
-        leg("batched_cg", batch_cg_leg, torch, rtkb, stream)
+        leg("batched_fdk_cg", c4_leg, torch, rtkb, stream)
         leg("sart", sart_leg, torch, rtkb, stream)
         leg("osem", osem_leg, torch, rtkb, stream)
         leg("regularized_cg", regularized_cg_leg, torch, rtkb, stream)

@@ -167,7 +167,7 @@ def displaced_detector_region(geometry, proj_desc, pad=True):
 def displaced_detector(geometry, proj_desc, proj, pad=True, stream=None):
     """rtk::DisplacedDetectorImageFilter; returns (out, out_desc)."""
     od, _ = displaced_detector_region(geometry, proj_desc, pad)
-    out = _unary(None, proj_desc, proj, None, shape_of(od))
+    out = _unary(None, proj_desc, proj, out, shape_of(od))
     check(load().rtkb_displaced_detector(geometry.handle, C.byref(proj_desc), int(pad), _ptr(proj), _ptr(out),
                                          _stream(stream)))
     return out, od
@@ -193,7 +193,7 @@ def ramp_filter(proj_desc, proj, params=None, out=None, stream=None):
 
 
 def fdk_preprocess(geometry, proj_desc, proj, ramp=None, displaced=False, pad=True, short_scan=False,
-                   threshold=3.141592653589793 / 9, stream=None):
+                   threshold=3.141592653589793 / 9, stream=None, out=None):
     """Displaced detector + Parker + FDK weighting + ramp in one pass.
     Returns (filtered stack, its description)."""
     from ._capi import FdkPreprocessParams
@@ -205,7 +205,7 @@ def fdk_preprocess(geometry, proj_desc, proj, ramp=None, displaced=False, pad=Tr
     od = proj_desc
     if displaced:
         od, _ = displaced_detector_region(geometry, proj_desc, pad)
-    out = _unary(None, proj_desc, proj, None, shape_of(od))
+    out = _unary(None, proj_desc, proj, out, shape_of(od))
     from ._capi import ImageDesc
 
     got = ImageDesc()

@@ -94,6 +94,7 @@ def lib():
             "orc_ramp_kernel": (None, [C.c_int, C.c_double, C.POINTER(OrcRampParams), D]),
             "orc_ramp_filter": (None, [IM, C.POINTER(OrcRampParams), D, D, C.c_int]),
             "orc_cg_joseph": (None, [G, IM, IM, D, D, D, C.c_double, C.c_double, C.c_int, D, D, C.c_int]),
+            "orc_parker_params": (C.c_int, [G, C.c_double, D, D]),
             "orc_cg": (None, [G, IM, IM, D, D, D, C.c_double, C.c_double, C.c_int, D, D, C.c_int, C.c_int]),
             "orc_joseph_back_mt": (None, [G, IM, D, D, IM, D, C.c_int]),
             "orc_laplacian": (None, [IM, D, D]),
@@ -192,6 +193,12 @@ class Geometry:
         lib().orc_geometry_source_position(self._g, i, _d(s))
         return s
 
+    def parameters(self, i):
+        """(sid, sdd, gantry, pox, poy, oop, ip, sox, soy, source angle) of projection i."""
+        p = np.zeros(10)
+        lib().orc_geometry_parameters(self._g, i, _d(p))
+        return p
+
     def proj_coords_to_fixed(self, i):
         m = np.zeros(16)
         lib().orc_geometry_proj_coords_to_fixed(self._g, i, _d(m))
@@ -282,6 +289,13 @@ def parker_weight(g, proj, data, threshold=np.pi / 9):
     out = np.empty_like(d)
     short = lib().orc_parker_weight(g._g, C.byref(proj), threshold, _d(d), _d(out))
     return out, bool(short)
+
+
+def parker_params(g, threshold=np.pi / 9):
+    """(short scan?, delta, first angle) of ParkerShortScanImageFilter."""
+    d, f = C.c_double(), C.c_double()
+    short = lib().orc_parker_params(g._g, threshold, C.byref(d), C.byref(f))
+    return bool(short), d.value, f.value
 
 
 def displaced_detector_region(g, proj, pad=True):

@@ -58,3 +58,85 @@ rtkcuda_fdk_backproject(const int proj_size[3], const int vol_size[3], const flo
     return -1;
   }
 }
+
+// ---- RTK's CUDA projection weighting filters (compiled unchanged), on whole
+// images (requested region = buffered region).  The scalar state that their
+// ITK filters compute on the host (angular-gap factors, Parker's delta and
+// first angle, the displaced detector's corners) is passed in by the caller.
+
+#include "rtkCudaDisplacedDetectorImageFilter.hcu"
+#include "rtkCudaFDKWeightProjectionFilter.hcu"
+#include "rtkCudaParkerShortScanImageFilter.hcu"
+
+// CudaFDKWeightProjectionFilter::GPUGenerateData
+// (src/rtkCudaFDKWeightProjectionFilter.cxx:31-124): geometry = 7 floats per
+// projection (sdd, sid, projection offset x, y, source offset y, weight
+// factor, tilt angle).
+extern "C" int
+rtkcuda_fdk_weight(const int proj_idx[2], const int proj_size[3], float * dev_in, float * dev_out, const float * geometry,
+                   const float proj_orig[2], const float proj_row[2], const float proj_col[2])
+{
+  try
+  {
+    int   idx[2] = { proj_idx[0], proj_idx[1] }, size[3] = { proj_size[0], proj_size[1], proj_size[2] };
+    int   buf[2] = { proj_size[0], proj_size[1] };
+    float o[2] = { proj_orig[0], proj_orig[1] }, r[2] = { proj_row[0], proj_row[1] }, c[2] = { proj_col[0], proj_col[1] };
+    CUDA_weight_projection(idx, size, buf, buf, dev_in, dev_out, const_cast<float *>(geometry), o, r, c);
+    return 0;
+  }
+  catch (const std::exception & e)
+  {
+    g_error = e.what();
+    return -1;
+  }
+}
+
+// CudaParkerShortScanImageFilter::GPUGenerateData
+// (src/rtkCudaParkerShortScanImageFilter.cxx:30-120), short-scan branch:
+// geometry = 5 floats per projection (sdd, source offset x, projection offset
+// x, sid, gantry angle).
+extern "C" int
+rtkcuda_parker_weight(const int proj_idx[2], const int proj_size[3], float * dev_in, float * dev_out,
+                      const float * geometry, float delta, float first_angle, float proj_orig, float proj_row,
+                      float proj_col)
+{
+  try
+  {
+    int idx[2] = { proj_idx[0], proj_idx[1] }, size[3] = { proj_size[0], proj_size[1], proj_size[2] };
+    int buf[2] = { proj_size[0], proj_size[1] };
+    CUDA_parker_weight(idx, size, buf, buf, dev_in, dev_out, const_cast<float *>(geometry), delta, first_angle,
+                       proj_orig, proj_row, proj_col);
+    return 0;
+  }
+  catch (const std::exception & e)
+  {
+    g_error = e.what();
+    return -1;
+  }
+}
+
+// CudaDisplacedDetectorImageFilter::GPUGenerateData
+// (src/rtkCudaDisplacedDetectorImageFilter.cxx:30-140): input stack region
+// (idx_in, size_in), output region (idx_out, size_out, padded on the
+// truncated side), geometry = 4 floats per projection (sdd, source offset x,
+// projection offset x, sid), theta = min(-inferior corner, superior corner).
+extern "C" int
+rtkcuda_displaced_weight(const int idx_in[3], const int size_in[3], const int idx_out[3], const int size_out[3],
+                         float * dev_in, float * dev_out, const float * geometry, float theta, int positive_case,
+                         float proj_orig, float proj_row, float proj_col)
+{
+  try
+  {
+    int ii[3] = { idx_in[0], idx_in[1], idx_in[2] }, si[3] = { size_in[0], size_in[1], size_in[2] };
+    int io[3] = { idx_out[0], idx_out[1], idx_out[2] }, so[3] = { size_out[0], size_out[1], size_out[2] };
+    int bi[2] = { size_in[0], size_in[1] }, bo[2] = { size_out[0], size_out[1] };
+    CUDA_displaced_weight(ii, si, bi, io, so, bo, dev_in, dev_out, const_cast<float *>(geometry), theta,
+                          positive_case != 0, proj_orig, proj_row, proj_col);
+    return 0;
+  }
+  catch (const std::exception & e)
+  {
+    g_error = e.what();
+    return -1;
+  }
+}

@@ -1331,6 +1331,52 @@ orc_fdk_weight(const orc_geometry * g, const orc_image * proj, const double * in
 /* ------------------------------------------------------------------------ */
 /* Parker short scan (include/rtkParkerShortScanImageFilter.hxx:41-209)      */
 /* ------------------------------------------------------------------------ */
+
+/* ParkerShortScanImageFilter::GenerateInputRequestedRegion's short-scan
+ * detection and angles (include/rtkParkerShortScanImageFilter.hxx:41-110):
+ * returns 1 for a short scan (largest gap between consecutive gantry angles
+ * above threshold, divergent geometry) with delta and the first angle. */
+int
+orc_parker_params(const orc_geometry * g, double threshold, double * delta_out, double * first_out)
+{
+  const int n = g->n;
+  double *  ga = (double *)malloc(sizeof(double) * (n > 0 ? n : 1));
+  double *  gaps = (double *)malloc(sizeof(double) * (n > 0 ? n : 1));
+  orc_geometry_gantry_angles(g, ga);
+  orc_geometry_angular_gaps_with_next(g, ga, gaps);
+  int maxpos = 0;
+  for (int k = 1; k < n; k++)
+    if (gaps[k] > gaps[maxpos])
+      maxpos = k;
+  if (n < 1 || g->par[P_SDD] == 0. || gaps[maxpos] < threshold)
+  {
+    free(ga);
+    free(gaps);
+    return 0;
+  }
+  angle_idx * s = sorted_angles(ga, n);
+  int         nu_ = 0;
+  for (int k = 0; k < n; k++)
+    if (nu_ == 0 || s[k].a != s[nu_ - 1].a)
+      s[nu_++] = s[k];
+  int last = 0;
+  for (int k = 0; k < nu_; k++)
+    if (s[k].a == ga[maxpos])
+      last = k;
+  const int first = (last + 1 == nu_) ? 0 : last + 1;
+  double    firstAngle = s[first].a, lastAngle = s[last].a;
+  if (lastAngle < firstAngle)
+    lastAngle += 2 * ORC_PI;
+  double delta = 0.5 * (lastAngle - firstAngle - ORC_PI);
+  delta = delta - 2 * ORC_PI * floor(delta / (2 * ORC_PI));
+  free(s);
+  free(ga);
+  free(gaps);
+  *delta_out = delta;
+  *first_out = firstAngle;
+  return 1;
+}
+
 int
 orc_parker_weight(const orc_geometry * g, const orc_image * proj, double threshold, const double * in, double * out)
 {

@@ -97,6 +97,8 @@ double orc_joseph_sample_count(const orc_geometry * g, const orc_image * vol, co
 /* ---- projection weighting ---- */
 void orc_fdk_weight(const orc_geometry * g, const orc_image * proj, const double * in, double * out);
 /* returns 1 when the scan is a short scan (weights applied), 0 otherwise */
+/* Parker's short-scan detection, delta and first gantry angle (returns 1 for a short scan) */
+int    orc_parker_params(const orc_geometry * g, double threshold, double * delta, double * first_angle);
 int  orc_parker_weight(const orc_geometry * g, const orc_image * proj, double angular_gap_threshold,
                        const double * in, double * out);
 /* Computes the displaced-detector output region. out_index0/out_size0 receive the

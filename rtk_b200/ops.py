@@ -164,7 +164,7 @@ def displaced_detector_region(geometry, proj_desc, pad=True):
     return out, bool(w.value)
 
 
-def displaced_detector(geometry, proj_desc, proj, pad=True, stream=None):
+def displaced_detector(geometry, proj_desc, proj, pad=True, stream=None, out=None):
     """rtk::DisplacedDetectorImageFilter; returns (out, out_desc)."""
     od, _ = displaced_detector_region(geometry, proj_desc, pad)
     out = _unary(None, proj_desc, proj, out, shape_of(od))

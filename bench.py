@@ -241,11 +241,101 @@ def joseph_forward_leg(torch, rtkb, lib, stream, reps=2):
     t = e0.elapsed_time(e1) / 1e3 / reps
     peak = smem_peak_gbs(torch, lib, stream)
     achieved = n * 16 / t / 1e9
-    return {"workload": "Joseph forward projection 512^3 @0.5mm -> 720 x 1024x768 @0.388mm, 20 random ellipsoids",
-            "samples_per_launch": n, "ms_per_launch": t * 1e3, "gsamples_per_s": n / t / 1e9,
-            "roofline": {"bound": "l1", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "bytes_per_sample": 16,
-                         "peak_source": "shared-memory bilinear-gather probe (the taps are L1-cached global loads)"}}
+    out_leg = {"workload": "Joseph forward projection 512^3 @0.5mm -> 720 x 1024x768 @0.388mm, 20 random ellipsoids",
+               "samples_per_launch": n, "ms_per_launch": t * 1e3, "gsamples_per_s": n / t / 1e9,
+               "roofline": {"bound": "l1", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                            "frac": achieved / peak, "bytes_per_sample": 16,
+                            "peak_source": "shared-memory bilinear-gather probe (the taps are L1-cached global loads)"}}
+    out_leg["rtk_cuda_reference"] = rtk_cuda_forward_leg(torch, vol, out, t * 1e3)
+    return out_leg
+
+
+def _event_median_ms(torch, run, reps):
+    """Median device time of run() over reps calls (one warm-up call first);
+    run() may issue work on the legacy default stream, so each call is
+    bracketed by events on the current stream and a synchronise."""
+    torch.cuda.synchronize()
+    run()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    times = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    return statistics.median(times), times
+
+
+def rtk_cuda_forward_leg(torch, vol, product_out, product_ms, reps=3) -> dict:
+    """RTK's own CUDA forward projector (kernel_forwardProject of
+    src/rtkCudaForwardProjectionImageFilter.cu, compiled unchanged into
+    oracle/_ref) on the same volume and geometry, driven in 16-projection slabs
+    as CudaForwardProjectionImageFilter runs it (each slab copies the volume
+    into a 3-D texture array; trilinear samples every 0.5 mm along the ray).
+    A different quadrature of the same line integrals than Joseph's: its
+    relative L2 distance to the product's projections is reported, not a
+    parity figure.  The reference's GPU code, timed beside the product."""
+    from oracle import oracle as O
+    from oracle import rtk_cuda
+
+    if not rtk_cuda.iter_available():
+        return {"unavailable": "RTK's CUDA projectors were not built (no RTK source tree where the library was built)"}
+    go = oracle_geometry()
+    vo = O.image((NX, NY, NZ), (VOX,) * 3)
+    po = O.image((NU, NV, NP), (PIX, PIX, 1.0))
+    zero = torch.zeros((NP, NV, NU), device="cuda")
+    res = torch.empty_like(zero)
+
+    def run():
+        rtk_cuda.forward_project(O, go, vo, po, vol.data_ptr(), zero.data_ptr(), res.data_ptr())
+
+    ms, times = _event_median_ms(torch, run, reps)
+    d = (res - product_out).double().norm() / product_out.double().norm()
+    return {"ms_per_projection": ms, "ms_each": [round(x, 1) for x in times], "product_speedup": ms / product_ms,
+            "rel_l2_to_product_joseph": float(d),
+            "kernel": "RTK kernel_forwardProject, SLAB_SIZE 16, 3-D texture trilinear samples every 0.5 mm"}
+
+
+def voxel_bp_leg(torch, rtkb, g, vd, pd, proj, stream, reps=3) -> dict:
+    """Voxel-based back projection (rtk::BackProjectionImageFilter, RTK's
+    default back projector of its iterative filters) of the headline's stack
+    into the 512^3 volume: the product's kernel against RTK's own CUDA back
+    projector (kernel_backProject of src/rtkCudaBackProjectionImageFilter.cu,
+    compiled unchanged, 16-projection layered-texture slabs), device time with
+    inputs resident, and the two outputs' relative L2 distance."""
+    from oracle import oracle as O
+    from oracle import rtk_cuda
+
+    zero = torch.zeros((NZ, NY, NX), device="cuda")
+    out = torch.empty_like(zero)
+
+    def run_product():
+        rtkb.ops.voxel_backproject(g, vd, pd, proj, zero, out=out, stream=stream)
+
+    ms, times = _event_median_ms(torch, run_product, reps)
+    leg = {"workload": "voxel-based back projection 720 x 1024x768 @0.388mm -> 512^3 @0.5mm",
+           "updates": updates_per_step(), "ms_per_backprojection": ms, "gups": updates_per_step() / ms / 1e6}
+    if not rtk_cuda.iter_available():
+        leg["rtk_cuda_reference"] = {"unavailable": "RTK's CUDA back projector was not built"}
+        return leg
+    go = oracle_geometry()
+    vo = O.image((NX, NY, NZ), (VOX,) * 3)
+    po = O.image((NU, NV, NP), (PIX, PIX, 1.0))
+    res = torch.empty_like(zero)
+
+    def run_rtk():
+        rtk_cuda.back_project(O, go, vo, po, zero.data_ptr(), res.data_ptr(), proj.data_ptr())
+
+    rms, rtimes = _event_median_ms(torch, run_rtk, reps)
+    d = (res - out).double().norm() / out.double().norm()
+    leg["rtk_cuda_reference"] = {"ms_per_backprojection": rms, "ms_each": [round(x, 1) for x in rtimes],
+                                 "gups": updates_per_step() / rms / 1e6, "product_speedup": rms / ms,
+                                 "rel_l2_to_product": float(d),
+                                 "kernel": "RTK kernel_backProject, SLAB_SIZE 16, layered-texture bilinear"}
+    return leg
 
 
 def bf16_storage_leg(torch, rtkb, g, vd, pd, proj, vol_fp32, stream, peak_smem, reps=5):
@@ -733,8 +823,9 @@ def cg_seconds_to_residual(torch, rtkb, stream, tol=1e-3, max_iter=300, learned_
         "residual_history": solve.hist,
         "training": {"pairs": 32, "pairs_seconds": t_pairs, "steps": 3000, "batch": 4, "crop": 64,
                      "train_seconds": t_train, "final_loss": hist[-1][1] if hist else None},
-        "method": "flexible PCG, history 8, 3-level 3D U-Net 16/32/64 (BF16 mma.sync convolutions, FP32 "
-                  "accumulation), fallback to plain CG after 2 non-improving iterations"}
+        "method": "flexible PCG, history 8, 3-level 3D U-Net 16/32/64 (BF16 convolutions: tcgen05 forward "
+                  "and data gradient, mma.sync weight gradient; FP32 accumulation), fallback to plain CG after 2 "
+                  "non-improving iterations"}
     return out
 
 
@@ -1218,6 +1309,7 @@ def main():
 
         leg("bf16_storage", bf16_storage_leg, torch, rtkb, g, vd, pd, proj, vol, stream, peak_smem)
         leg("fdk_pipeline_ms", fdk_pipeline_ms, torch, rtkb, g, vd, pd, proj, stream)
+        leg("voxel_backprojection", voxel_bp_leg, torch, rtkb, g, vd, pd, proj, stream)
         del proj
         leg("joseph_forward", joseph_forward_leg, torch, rtkb, lib, stream)
         leg("batched", batch_leg, torch, rtkb, stream)

@@ -1,11 +1,15 @@
-"""RTK's own CUDA FDK back projector (CUDA_reconstruct_conebeam from
-src/rtkCudaFDKBackProjectionImageFilter.cu), built from an RTK source tree by
-oracle/rtk_cuda/Makefile into oracle/_ref/librtkcudafdk.so.
+"""RTK's own CUDA code, built unchanged from an RTK source tree by
+oracle/rtk_cuda/Makefile: the FDK back projector (CUDA_reconstruct_conebeam,
+src/rtkCudaFDKBackProjectionImageFilter.cu) and the projection weighting
+filters in oracle/_ref/librtkcudafdk.so; the ray-casting forward projector,
+the voxel-based back projector, the Laplacian, TV denoising and the
+conjugate-gradient update in oracle/_ref/librtkcudaiter.so.
 
-TEST INFRASTRUCTURE ONLY: the reference's CUDA kernel is timed beside the
-product and checked against the FP64 oracle (a pin of the half-pixel,
-normalisation and weighting conventions, at the precision of its
-texture-filtered interpolation).  The product never loads it.
+TEST INFRASTRUCTURE ONLY: the reference's CUDA kernels are timed beside the
+product and checked against the FP64 oracle (pins of the half-pixel,
+normalisation and weighting conventions, at the precision of their
+texture-filtered interpolation where they use textures).  The product never
+loads them.
 """
 from __future__ import annotations
 
@@ -17,7 +21,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_ref", "librtkcudafdk.so")
+ITER_LIB_PATH = os.path.join(HERE, "_ref", "librtkcudaiter.so")
 _lib = None
+_ilib = None
 
 
 def build(rtk_src: str | None = None) -> str | None:
@@ -32,6 +38,10 @@ def build(rtk_src: str | None = None) -> str | None:
 
 def available() -> bool:
     return os.path.exists(LIB_PATH)
+
+
+def iter_available() -> bool:
+    return os.path.exists(ITER_LIB_PATH)
 
 
 def lib():
@@ -188,3 +198,125 @@ def displaced_weight(O, g, proj, d_in: int, d_out: int, pad=True):
                                           theta, int(sup + inf > 0.0), proj.origin[0], D[0, 0] * proj.spacing[0],
                                           D[0, 1] * proj.spacing[1]))
     return i0, s0
+
+
+# ---- librtkcudaiter.so: projectors, Laplacian, TV denoising, CG update
+
+
+def ilib():
+    global _ilib
+    if _ilib is None:
+        L = C.CDLL(ITER_LIB_PATH)
+        I3 = C.POINTER(C.c_int)
+        F = C.POINTER(C.c_float)
+        V = C.c_void_p
+        L.rtkcuda_forward_project.restype = C.c_int
+        L.rtkcuda_forward_project.argtypes = [I3, I3, F, F, V, V, V, C.c_float, F, F, F]
+        L.rtkcuda_back_project.restype = C.c_int
+        L.rtkcuda_back_project.argtypes = [I3, I3, F, V, V, V]
+        L.rtkcuda_laplacian.restype = C.c_int
+        L.rtkcuda_laplacian.argtypes = [I3, F, V, V]
+        L.rtkcuda_total_variation.restype = C.c_int
+        L.rtkcuda_total_variation.argtypes = [I3, F, V, V, C.c_float, C.c_float, C.c_int]
+        for name in ("rtkcuda_cg_copy", "rtkcuda_cg_subtract"):
+            getattr(L, name).restype = C.c_int
+            getattr(L, name).argtypes = [C.c_size_t, V, V]
+        L.rtkcuda_cg_update.restype = C.c_int
+        L.rtkcuda_cg_update.argtypes = [C.c_size_t, V, V, V, V]
+        L.rtkcuda_iter_last_error.restype = C.c_char_p
+        _ilib = L
+    return _ilib
+
+
+def _icheck(rc):
+    if rc != 0:
+        raise RuntimeError("RTK CUDA: " + ilib().rtkcuda_iter_last_error().decode())
+
+
+def forward_matrices(O, g, vol, proj):
+    """What CudaForwardProjectionImageFilter::GPUGenerateData passes for a
+    flat panel (include/rtkCudaForwardProjectionImageFilter.hxx:60-167):
+    per projection, detector index -> volume texture coordinates (the
+    volume's physical-to-index matrix shifted by 0.5 to the texel-corner
+    convention, times the oracle's projection-coordinates-to-fixed-system
+    matrix and the stack's index-to-physical matrix), the source in the same
+    coordinates, the box from the first to the last voxel centre, the spacing
+    and the default step (the smallest spacing).  Volume and stack regions
+    start at index 0 here."""
+    if any(vol.index) or any(proj.index[:2]):
+        raise ValueError("regions starting at index 0 only")
+    pp2i = np.linalg.inv(O.index_to_physical(vol))
+    pp2i[:3, 3] += 0.5
+    i2p = O.index_to_physical(proj)
+    n = proj.size[2]
+    mats = np.zeros((n, 12), dtype=np.float32)
+    src = np.zeros((n, 3), dtype=np.float32)
+    for s in range(n):
+        k = proj.index[2] + s
+        mats[s] = (pp2i @ g.proj_coords_to_fixed(k) @ i2p)[:3].reshape(12)
+        src[s] = (pp2i @ g.source_position(k))[:3]
+    bmin = [0.5, 0.5, 0.5]
+    bmax = [0.5 + vol.size[i] - 1.0 for i in range(3)]
+    return mats, src, bmin, bmax, list(vol.spacing), float(min(vol.spacing))
+
+
+def forward_project(O, g, vol, proj, d_vol: int, d_proj_in: int, d_proj_out: int, t_step=None) -> None:
+    """RTK's CUDA ray-casting forward projection (kernel_forwardProject:
+    trilinear texture samples every t_step mm between the box faces) of the
+    FP32 volume at d_vol, added to d_proj_in, into d_proj_out; the filter's
+    slab loop over CUDA_forward_project."""
+    mats, src, bmin, bmax, sp, step = forward_matrices(O, g, vol, proj)
+    m, mp = _f(mats)
+    s, sp_ = _f(src)
+    a, ap = _f(bmin)
+    b, bp = _f(bmax)
+    c, cp = _f(sp)
+    _icheck(ilib().rtkcuda_forward_project(_i(proj.size), _i(vol.size), mp, sp_, C.c_void_p(d_proj_in),
+                                           C.c_void_p(d_proj_out), C.c_void_p(d_vol),
+                                           float(step if t_step is None else t_step), ap, bp, cp))
+
+
+def back_project(O, g, vol, proj, d_vol_in: int, d_vol_out: int, d_proj: int) -> None:
+    """RTK's CUDA voxel-based back projection (kernel_backProject: bilinear
+    texture reads at each voxel's projection, no distance weight) with the
+    filter's matrices (include/rtkCudaBackProjectionImageFilter.hxx:51-134:
+    the same texel-centred, rotation-centre-normalised index-to-index
+    matrices as the FDK filter's)."""
+    m, mp = _f(filter_matrices(O, g, vol, proj))
+    _icheck(ilib().rtkcuda_back_project(_i(proj.size), _i(vol.size), mp, C.c_void_p(d_vol_in), C.c_void_p(d_vol_out),
+                                        C.c_void_p(d_proj)))
+
+
+def laplacian(vol, d_in: int, d_out: int) -> None:
+    """CUDA_laplacian (src/rtkCudaLaplacianImageFilter.cu): gradient then
+    divergence kernels of src/rtkCudaFirstOrderKernels.cu."""
+    sp, spp = _f(vol.spacing)
+    _icheck(ilib().rtkcuda_laplacian(_i(vol.size), spp, C.c_void_p(d_in), C.c_void_p(d_out)))
+
+
+def total_variation_denoising(vol, d_in: int, d_out: int, gamma: float, niter: int) -> None:
+    """CUDA_total_variation (src/rtkCudaTotalVariationDenoisingBPDQImageFilter.cu)
+    on all three dimensions, with beta = 0.9 / 2^3 x the smallest spacing as
+    DenoisingBPDQImageFilter::GenerateOutputInformation sets it
+    (include/rtkDenoisingBPDQImageFilter.hxx:69-86)."""
+    sp, spp = _f(vol.spacing)
+    beta = 0.9 / 8.0 * min(vol.spacing)
+    _icheck(ilib().rtkcuda_total_variation(_i(vol.size), spp, C.c_void_p(d_in), C.c_void_p(d_out), float(gamma),
+                                           float(beta), int(niter)))
+
+
+def conjugate_gradient(n: int, apply_operator, d_b: int, d_x: int, d_r: int, d_p: int, d_ap: int, niter: int) -> None:
+    """CudaConjugateGradientImageFilter::GPUGenerateData
+    (include/rtkCudaConjugateGradientImageFilter.hxx:58-105) on FP32 device
+    vectors of n elements: x holds X0 on entry and the iterate on return;
+    apply_operator(src, dst) computes dst = A src (device pointers) and must
+    have finished when it returns (RTK's update runs on the legacy default
+    stream)."""
+    L = ilib()
+    apply_operator(d_x, d_ap)
+    _icheck(L.rtkcuda_cg_copy(n, C.c_void_p(d_b), C.c_void_p(d_r)))
+    _icheck(L.rtkcuda_cg_subtract(n, C.c_void_p(d_r), C.c_void_p(d_ap)))
+    _icheck(L.rtkcuda_cg_copy(n, C.c_void_p(d_r), C.c_void_p(d_p)))
+    for _ in range(niter):
+        apply_operator(d_p, d_ap)
+        _icheck(L.rtkcuda_cg_update(n, C.c_void_p(d_x), C.c_void_p(d_r), C.c_void_p(d_p), C.c_void_p(d_ap)))

@@ -14,7 +14,7 @@ using SizeValueType = unsigned long;
 #define itkGenericExceptionMacro(x)                                                                                    \
   {                                                                                                                    \
     std::ostringstream rtkb_message;                                                                                   \
-    rtkb_message x;                                                                                                    \
+    rtkb_message << "RTK CUDA error: " x;                                                                              \
     throw std::runtime_error(rtkb_message.str());                                                                      \
   }
 #endif

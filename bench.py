@@ -37,11 +37,11 @@ PIX = 0.388
 SID, SDD = 1000.0, 1536.0
 SEED = 20261203 + 1
 L1_BYTES_PER_UPDATE = 16  # four 4-byte taps of one bilinear interpolation
-# DRAM bytes (read + write) of one backprojection launch of this workload, recorded from a 1-pass ncu
-# capture (dram__bytes_read.sum + dram__bytes_write.sum) of the kernel as of BP_TRAFFIC_COMMIT; a
-# recorded figure, not a measurement of the build that runs.
-BP_LAUNCH_DRAM_BYTES = 69.3747e9 + 0.5982e9
-BP_TRAFFIC_COMMIT = "0d49521"
+# DRAM bytes (read + write) of one backprojection launch of this workload under each tile schedule,
+# recorded from a 1-pass ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of the kernel as of
+# BP_TRAFFIC_COMMIT; recorded figures, not measurements of the build that runs.
+BP_DRAM_BYTES_BY_SCHEDULE = {0: 69.3747e9 + 0.5982e9, 1: 13.2181e9 + 0.5855e9}
+BP_TRAFFIC_COMMIT = "0d49521 (schedule 0), sweep build (schedule 1)"
 WORKLOAD = {"workload": "FDK backprojection 512^3 @0.5mm <- 720 x 1024x768 @0.388mm, SID 1000, SDD 1536, 360 deg",
             "volume": [NX, NY, NZ], "projections": [NU, NV, NP], "dtype_storage": "float32",
             "l2_policy": "inputs larger than L2 (2.26 GB projection stack, 0.54 GB volume)"}
@@ -297,6 +297,29 @@ def rtk_cuda_forward_leg(torch, vol, product_out, product_ms, reps=3) -> dict:
     return {"ms_per_projection": ms, "ms_each": [round(x, 1) for x in times], "product_speedup": ms / product_ms,
             "rel_l2_to_product_joseph": float(d),
             "kernel": "RTK kernel_forwardProject, SLAB_SIZE 16, 3-D texture trilinear samples every 0.5 mm"}
+
+
+def sweep_leg(torch, rtkb, g, vd, pd, proj, vol_ref, stream, schedule_timed, reps=5) -> dict:
+    """The headline backprojection under the other tile schedule: the
+    projection sweep (schedule 1: tiles start where the resident CTAs are in
+    the stack and wrap around, so the tiles in flight share projections in L2)
+    against every tile from projection 0 (schedule 0).  Median device time of
+    `reps` steps, its relative L2 distance to the timed output (summation
+    order only), and the DRAM bytes of one launch recorded from a 1-pass ncu
+    capture of each schedule."""
+    other = 1 - schedule_timed
+    zero = torch.zeros((NZ, NY, NX), device="cuda")
+    out = torch.empty_like(zero)
+    rtkb.ops.backproject_schedule(other)
+    try:
+        ms, times = _event_median_ms(
+            torch, lambda: rtkb.ops.fdk_backproject(g, vd, pd, proj, zero, out=out, stream=stream), reps)
+    finally:
+        rtkb.ops.backproject_schedule(schedule_timed)
+    d = float((out - vol_ref).double().norm() / vol_ref.double().norm())
+    return {"schedule": other, "ms_per_backprojection": ms, "gups": updates_per_step() / ms / 1e6,
+            "rel_l2_to_timed_output": d, "dram_bytes_per_launch_recorded": BP_DRAM_BYTES_BY_SCHEDULE[other],
+            "dram_bytes_commit": BP_TRAFFIC_COMMIT}
 
 
 def voxel_bp_leg(torch, rtkb, g, vd, pd, proj, stream, reps=3) -> dict:
@@ -1141,6 +1164,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra-legs", action="store_true",
                     help="skip the FDK pipeline and CG seconds-to-residual legs")
+    ap.add_argument("--bp-schedule", type=int, default=0, choices=[0, 1],
+                    help="tile schedule of the timed backprojections (rtkb_bp_set_schedule): 0 every tile from "
+                         "projection 0 (default), 1 the projection sweep")
     ap.add_argument("--profile-cg", action="store_true",
                     help="run the CG configuration's kernels once each for ncu captures (256^3, 360 x 512x384): CG "
                          "start + 2 eager iterations, one U-Net forward on the volume, one training step on 4 x 64^3")
@@ -1195,6 +1221,7 @@ def main():
         rtkb.ops.fdk_backproject(g, vd, pd, proj, zero, out=vol, stream=stream)
 
     tuned = None
+    rtkb.ops.backproject_schedule(args.bp_schedule)
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -1253,7 +1280,7 @@ def main():
     hbm_bytes = (NX * NY * NZ * 4 * 2) + (NP * NV * NU * 4)
     roofline = {"bound": "l1", "achieved": achieved, "peak": peak_smem, "unit": "GB/s",
                 "frac": achieved / peak_smem if peak_smem else None,
-                "traffic": BP_LAUNCH_DRAM_BYTES if NX == 512 else None,
+                "traffic": BP_DRAM_BYTES_BY_SCHEDULE[args.bp_schedule] if NX == 512 else None,
                 "traffic_source": "recorded constant: ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
                                   f"full-size launch of the kernel at commit {BP_TRAFFIC_COMMIT}",
                 "peak_source": "measured in this run: shared-memory bilinear-gather probe (rtkb_probe_smem_gather)",
@@ -1310,6 +1337,7 @@ def main():
         leg("bf16_storage", bf16_storage_leg, torch, rtkb, g, vd, pd, proj, vol, stream, peak_smem)
         leg("fdk_pipeline_ms", fdk_pipeline_ms, torch, rtkb, g, vd, pd, proj, stream)
         leg("voxel_backprojection", voxel_bp_leg, torch, rtkb, g, vd, pd, proj, stream)
+        leg("projection_sweep", sweep_leg, torch, rtkb, g, vd, pd, proj, vol, stream, args.bp_schedule)
         del proj
         leg("joseph_forward", joseph_forward_leg, torch, rtkb, lib, stream)
         leg("batched", batch_leg, torch, rtkb, stream)

@@ -96,6 +96,7 @@ SIGNATURES = {
     "rtkb_backproject_matrices": (C.c_int, [_I, _I, C.c_int, _D, _I, C.c_int, _V, _V, _V, _V]),
     "rtkb_probe_smem_gather": (C.c_int, [C.c_int, C.c_int, _V, _V]),
     "rtkb_backproject_config": (C.c_int, [C.c_int, _I, _I]),
+    "rtkb_bp_set_schedule": (C.c_int, [C.c_int, C.c_int]),
     "rtkb_joseph_forward_project": (C.c_int, [_G, _IM, _IM, _V, _V, _V, _V]),
     "rtkb_joseph_back_project": (C.c_int, [_G, _IM, _IM, _V, _V, _V, _V]),
     "rtkb_fdk_weight": (C.c_int, [_G, _IM, _V, _V, _V]),

@@ -28,9 +28,11 @@ struct VoxelBackprojector
   const float * d_proj = nullptr; // the stack it reads (fixed address)
   double *      d_mats = nullptr; // buffer-index matrices, uploaded at creation
   int *         d_modes = nullptr;
+  unsigned *    d_progress = nullptr; // the tile schedule's sweep counter
 };
 
-// Device bytes of the matrix and mode tables of nproj projections.
+// Device bytes of the matrix and mode tables of nproj projections and the
+// tile schedule's sweep counter.
 size_t voxel_backprojector_bytes(int nproj);
 // Builds RTK's voxel-based (non-FDK) back projector of the stack d_proj
 // (description proj) into volumes described by vol; uploads its tables into

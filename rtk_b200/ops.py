@@ -773,3 +773,11 @@ def backproject_config(force=-1):
     last, count = C.c_int(), C.c_int()
     check(load().rtkb_backproject_config(int(force), C.byref(last), C.byref(count)))
     return last.value, count.value
+
+
+def backproject_schedule(schedule, sweep_shift=4):
+    """Tile schedule of the tiled backprojector (rtkb_bp_set_schedule): 0 every
+    tile walks the stack from projection 0 (run-to-run identical sums), 1 the
+    projection sweep (chunks of 2^sweep_shift projections; tiles in flight
+    share projections in L2, summation order varies at FP32 rounding)."""
+    check(load().rtkb_bp_set_schedule(int(schedule), int(sweep_shift)))

@@ -178,3 +178,36 @@ def test_fdk_bp_host_rejects_device_tensors(rtkb, oracle):
     pd, po = pair_image(rtkb, oracle, (16, 16, 4), (1.0,) * 3)
     with pytest.raises(TypeError):
         rtkb.ops.fdk_backproject_host(gl, vd, pd, torch.zeros((4, 16, 16), device="cuda"))
+
+
+@pytest.mark.parametrize("fdk", [True, False])
+def test_bp_projection_sweep_schedule(rtkb, oracle, fdk):
+    """Tile schedule 1 (the projection sweep: tiles start at the projection the
+    resident CTAs have reached and wrap around the stack) sums the same terms
+    in another order: within FP32 rounding of schedule 0, and both within the
+    oracle's tolerance.  Schedule 0 is identical from run to run."""
+    import torch
+
+    params = _circular(240, 1000.0, 1536.0, pox=7.0, sox=3.0)
+    gl, go = pair_geometry(rtkb, oracle, params)
+    vd, vo = pair_image(rtkb, oracle, (160, 144, 128), (1.0,) * 3, index=(2, -3, 1))
+    pd, po = pair_image(rtkb, oracle, (256, 192, 240), (1.2, 1.2, 1.0))
+    p = np.random.default_rng(3).uniform(-1.0, 1.0, size=oracle.shape_of(po)).astype(np.float32)
+    dp = torch.from_numpy(p).cuda()
+    zero = torch.zeros(oracle.shape_of(vo), device="cuda")
+    fn = rtkb.ops.fdk_backproject if fdk else rtkb.ops.voxel_backproject
+    outs = {}
+    try:
+        for sched in (0, 1, 0):
+            rtkb.ops.backproject_schedule(sched, 2)
+            outs.setdefault(sched, []).append(to_np(fn(gl, vd, pd, dp, zero)))
+    finally:
+        rtkb.ops.backproject_schedule(0)
+    assert rtkb.ops.device_status() == 0
+    a, b = outs[0]
+    assert np.array_equal(a, b)
+    assert rel_l2(outs[1][0], a) < 1e-6
+    ref = oracle.backproject(go, vo, po, p.astype(np.float64), fdk=fdk)
+    assert rel_l2(outs[1][0], ref) < REL_L2_TOL
+    with pytest.raises(rtkb.RtkbError):
+        rtkb.ops.backproject_schedule(2)

@@ -456,7 +456,8 @@ def c4_leg(torch, rtkb, stream, n=64, niter=10):
     launch (a branch per problem).  Against the same work problem after problem
     (the same CG plans, one after another).  Plans and the backprojection batch
     are prepared outside both timed regions.  The two smallest problems' FDK
-    volumes are checked against the FP64 oracle's FDK."""
+    volumes are checked against the FP64 oracle's FDK, and their CG results
+    (from that FDK volume) against the oracle's CG from the same start."""
     import numpy as np
 
     from rtk_b200._capi import check
@@ -521,8 +522,9 @@ def c4_leg(torch, rtkb, stream, n=64, niter=10):
         torch.cuda.synchronize()
         times[name] = e0.elapsed_time(e1)
     assert rtkb.ops.device_status(stream) == 0
-    # the FP64 oracle's FDK of the two smallest problems (the batched backprojection's volumes)
-    errs = {}
+    # the FP64 oracle's FDK of the two smallest problems (the batched backprojection's volumes), then
+    # its CG from that volume
+    errs, cg_errs = {}, {}
     try:
         from oracle import oracle as O
 
@@ -542,6 +544,15 @@ def c4_leg(torch, rtkb, stream, n=64, niter=10):
             got = P["x"].double().cpu().numpy()
             errs[f"problem_{i}_{P['nv']}^3_{P['np']}x{P['nu']}x{P['nvd']}"] = float(
                 np.linalg.norm(got - ref) / np.linalg.norm(ref))
+            # the problem's CG from its FDK volume, on the GPU (its batch plan)
+            # and in the oracle (FP64 CG, Joseph pair) from the same FP32 start
+            check(lib.rtkb_cg_start(plans[i], rtkb.ops._ptr(P["p"]), None, 0, rtkb.ops._ptr(P["x"]),
+                                    stream.cuda_stream))
+            check(lib.rtkb_cg_iterate(plans[i], niter, stream.cuda_stream))
+            torch.cuda.synchronize()
+            ref_cg, _ = O.cg_joseph(go, vo, po, pr, niter, x0=got)
+            got_cg = P["x"].double().cpu().numpy()
+            cg_errs[f"problem_{i}"] = float(np.linalg.norm(got_cg - ref_cg) / np.linalg.norm(ref_cg))
     except Exception as ex:
         errs = {"error": str(ex)}
     bpb.close()
@@ -553,6 +564,7 @@ def c4_leg(torch, rtkb, stream, n=64, niter=10):
             "speedup": times["one_after_another"] / times["batched"],
             "autotuned_config": best,
             "fdk_oracle_rel_l2": errs,
+            f"cg_{niter}_iterations_oracle_rel_l2": cg_errs,
             "launches_batched": "preprocessing per problem, one persistent backprojection launch, one CUDA graph "
                                 "launch for every problem's CG start and iterations"}
 

@@ -1186,6 +1186,9 @@ def main():
     ap.add_argument("--profile-cg", action="store_true",
                     help="run the CG configuration's kernels once each for ncu captures (256^3, 360 x 512x384): CG "
                          "start + 2 eager iterations, one U-Net forward on the volume, one training step on 4 x 64^3")
+    ap.add_argument("--unet-wgrad-kernel", type=int, default=0, choices=[0, 1, 2],
+                    help="weight-gradient kernel of the U-Net's training (rtkb_unet_set_wgrad_kernel): 0 mma.sync "
+                         "(default), 1 tcgen05 M = 64, 2 tcgen05 M = 128")
     ap.add_argument("--profile-fdk", action="store_true",
                     help="FDK preprocessing (weights + Hann ramp filter) of the 720 x 1024x768 stack, twice, for ncu")
     ap.add_argument("--profile-osem", action="store_true",
@@ -1196,6 +1199,12 @@ def main():
     ap.add_argument("--profile-case", action="store_true",
                     help="small case for ncu captures: 256^3 @1mm from 360 projections, device-timed region only")
     args = ap.parse_args()
+    if args.unet_wgrad_kernel:
+        import rtk_b200 as rtkb_w
+        from rtk_b200 import build as rbuild_w
+
+        rbuild_w.build()
+        rtkb_w.ops.check(rtkb_w.load().rtkb_unet_set_wgrad_kernel(args.unet_wgrad_kernel))
     if args.profile_cg:
         return profile_cg()
     if args.profile_fdk:

@@ -549,6 +549,12 @@ void      rtkb_unet_destroy(rtkb_unet * net);
  * chunk's tcgen05 MMAs (one stage where two do not fit); 0 = halo gathered by the threads.  All
  * compute the same MMAs in the same order; kept to compare them. */
 int       rtkb_unet_set_conv_pipeline(int enable);
+/* Weight-gradient kernel of the U-Net's convolutions, for later training
+ * steps in this process: 0 warp-level mma.sync (default, fastest for these
+ * layer widths); 1 tcgen05 with the output channels as M = 64 (tiles of
+ * 8 x 16 x 4 voxels); 2 tcgen05 with M = 128 (tiles of 8 x 16 x 2 voxels).
+ * All three give the same gradients up to FP32 summation order. */
+int       rtkb_unet_set_wgrad_kernel(int kernel);
 
 /* Flexible PCG: with a network set (before rtkb_cg_start; NULL removes it) each
  * iteration preconditions the residual, z = s N(r / s), steps with

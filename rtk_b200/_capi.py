@@ -229,6 +229,7 @@ SIGNATURES.update({
                                        C.c_int, _D, _V]),
     "rtkb_unet_destroy": (None, [_V]),
     "rtkb_unet_set_conv_pipeline": (C.c_int, [C.c_int]),
+    "rtkb_unet_set_wgrad_kernel": (C.c_int, [C.c_int]),
 })
 
 

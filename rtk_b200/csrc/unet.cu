@@ -738,6 +738,178 @@ conv_wgrad_kernel(ConvIn in, const bf16 * __restrict__ g, Dims d, float * __rest
   }
 }
 
+// ---- weight gradient on the 5th-generation tensor cores -----------------------------------------------
+// dW[t][ci][co] += sum_v in[v + t - 1][ci] * g[v][co] as 27 GEMMs per 16-channel input chunk:
+// D_t (M rows = output channels, zero-padded to M; N = 16 input channels) += A B_t^T with A = g^T
+// (output channels x voxels) and B_t = the chunk's inputs shifted by tap t (input channels x
+// voxels), K = the voxels of an 8 x 16 x KZ tile.  Both operands are MN-major in shared memory
+// (8 channels contiguous in 16 bytes, voxels 16 bytes apart): the halo in its [k-half][voxel][8
+// channels] layout serves every tap -- tap t is a descriptor offset of one halo voxel step in x,
+// one halo row in y, one halo plane in z, with the K step of 8 voxels one halo row (160 bytes) --
+// and the gradient tile is stored [channel group][voxel][8 channels].  The 27 accumulators (27 x 16
+// FP32 columns of tensor memory) stay in tensor memory across the CTA's tiles and are added to dW
+// with atomics once, at the end.  A CTA owns an SM (512 tensor-memory columns); one thread issues the
+// 27 x (K / 16) MMAs of a tile and commits them to an mbarrier, waited on with a bound before the
+// next tile overwrites the operands.
+template <int M>
+struct WgradTcLayout
+{
+  static constexpr int kKZ = (M == 64) ? 4 : 2;                // tile depth
+  static constexpr int kKV = kCX * kCY * kKZ;                   // voxels per tile (K)
+  static constexpr int kHZ = kKZ + 2;
+  static constexpr int kHV = kCHX * kCHY * kHZ;                 // halo voxels
+  static constexpr int kA = (M / 8) * kKV * 16;                 // A bytes
+  static constexpr int kHalo = kHV * 32;                        // two k-halves
+  static constexpr int kTotal = kA + kHalo + 16;                // + mbarrier and TMEM slot
+};
+
+template <int M>
+__device__ __forceinline__ constexpr uint32_t
+umma_idesc_bf16_mn16()
+{
+  // FP32 accumulator, BF16 A and B, both MN-major (bits 15, 16), N = 16, M
+  return (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | ((uint32_t)(16 >> 3) << 17) |
+         ((uint32_t)(M >> 4) << 24);
+}
+
+template <int COUT, int M>
+__global__ void __launch_bounds__(128, 1)
+conv_wgrad_tc_kernel(ConvIn in, const bf16 * __restrict__ g, Dims d, float * __restrict__ dW, int cin_total)
+{
+  using L = WgradTcLayout<M>;
+  static_assert(COUT <= M && COUT % 8 == 0, "output channels must fit the MMA's M");
+  constexpr uint32_t kCols = 512;
+  constexpr uint32_t kIdesc = umma_idesc_bf16_mn16<M>();
+  extern __shared__ __align__(128) char smem[];
+  char *     asm_a = smem;                                   // [M / 8][KV][16 B]
+  char *     halo = smem + L::kA;                            // [2][HV][16 B]
+  uint64_t * bar = reinterpret_cast<uint64_t *>(halo + L::kHalo);
+  uint32_t * tmem_slot = reinterpret_cast<uint32_t *>(bar + 1);
+  const int  warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int  chunk = blockIdx.y;
+  const int  tx = (d.nx + kCX - 1) / kCX, ty = (d.ny + kCY - 1) / kCY, tz = (d.nz + L::kKZ - 1) / L::kKZ;
+  const long long ntiles = (long long)tx * ty * tz * d.batch;
+
+  if (warp == 0)
+  {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(rtkb::dev::smem_u32(tmem_slot)),
+                 "r"(kCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (threadIdx.x == 0)
+  {
+    rtkb::dev::mbar_init(bar, 1);
+    rtkb::dev::fence_barrier_init();
+  }
+  // the A rows of padding channels (COUT..M-1) stay zero
+  for (int i = (COUT / 8) * L::kKV + threadIdx.x; i < (M / 8) * L::kKV; i += 128)
+    *reinterpret_cast<uint4 *>(asm_a + i * 16) = make_uint4(0u, 0u, 0u, 0u);
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t a_s = rtkb::dev::smem_u32(asm_a), halo_s = rtkb::dev::smem_u32(halo);
+  const bool     from_a = chunk * 16 < in.ca;
+  const int      cs = from_a ? in.ca : in.cb;
+  const int      c0 = from_a ? chunk * 16 : chunk * 16 - in.ca;
+  const bf16 *   src = from_a ? in.a : in.b;
+  const bool     half = from_a && in.a_half;
+  const int      snx = half ? d.nx >> 1 : d.nx, sny = half ? d.ny >> 1 : d.ny, snz = half ? d.nz >> 1 : d.nz;
+  // descriptor offsets: A = (K step 128 B, channel groups KV x 16 B), B = (K step one halo row, k-halves)
+  const uint32_t a_k = 128u, a_m = (uint32_t)(L::kKV * 16), b_k = (uint32_t)(kCHX * 16), b_n = (uint32_t)(L::kHV * 16);
+  bool           ok = true;
+  int            it = 0;
+  for (long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, it++)
+  {
+    long long r = tile;
+    const int bx = (int)(r % tx);
+    r /= tx;
+    const int by = (int)(r % ty);
+    r /= ty;
+    const int bz = (int)(r % tz);
+    const int n = (int)(r / tz);
+    const int x0 = bx * kCX, y0 = by * kCY, z0 = bz * L::kKZ;
+    // the previous tile's MMAs read the operands asynchronously
+    if (it > 0)
+    {
+      ok = __syncthreads_and(rtkb::dev::mbar_wait(bar, (uint32_t)((it - 1) & 1)) ? 1 : 0) != 0;
+      if (!ok)
+        break;
+    }
+    for (int i = threadIdx.x; i < L::kHV * 2; i += 128)
+    {
+      const int hv = i >> 1, h = i & 1;
+      const int hx = hv % kCHX, hy = (hv / kCHX) % kCHY, hz = hv / (kCHX * kCHY);
+      const int gx = x0 - 1 + hx, gy = y0 - 1 + hy, gz = z0 - 1 + hz;
+      uint4     v = make_uint4(0u, 0u, 0u, 0u);
+      if (gx >= 0 && gx < d.nx && gy >= 0 && gy < d.ny && gz >= 0 && gz < d.nz)
+      {
+        const int sx = half ? gx >> 1 : gx, sy = half ? gy >> 1 : gy, sz = half ? gz >> 1 : gz;
+        v = *reinterpret_cast<const uint4 *>(src + ((((long long)n * snz + sz) * sny + sy) * snx + sx) * cs + c0 + h * 8);
+      }
+      *reinterpret_cast<uint4 *>(halo + (h * L::kHV + hv) * 16) = v;
+    }
+    for (int i = threadIdx.x; i < L::kKV * (COUT / 8); i += 128)
+    {
+      const int v = i / (COUT / 8), cg = i % (COUT / 8);
+      const int x = x0 + (v & 7), y = y0 + ((v >> 3) & 15), z = z0 + (v >> 7);
+      uint4     val = make_uint4(0u, 0u, 0u, 0u);
+      if (x < d.nx && y < d.ny && z < d.nz)
+        val = *reinterpret_cast<const uint4 *>(g + ((((long long)n * d.nz + z) * d.ny + y) * d.nx + x) * COUT + cg * 8);
+      *reinterpret_cast<uint4 *>(asm_a + (cg * L::kKV + v) * 16) = val;
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+      asm volatile("tcgen05.fence::after_thread_sync;");
+#pragma unroll 1
+      for (int t = 0; t < 27; t++)
+      {
+        const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
+#pragma unroll 1
+        for (int zl = 0; zl < L::kKZ; zl++)
+#pragma unroll
+          for (int yp = 0; yp < kCY / 2; yp++)
+          {
+            const int      kv0 = (zl * kCY + 2 * yp) * kCX;
+            const int      hv0 = ((zl + dz) * kCHY + 2 * yp + dy) * kCHX + dx;
+            // MN-major, no swizzle: leading offset = the K step between 8-voxel core matrices,
+            // stride offset = the step between 8-channel groups
+            const uint64_t da = umma_desc(a_s + (uint32_t)(kv0 * 16), a_k, a_m);
+            const uint64_t db = umma_desc(halo_s + (uint32_t)(hv0 * 16), b_k, b_n);
+            umma_bf16(tmem + (uint32_t)(t * 16), da, db, kIdesc, (it > 0 || zl > 0 || yp > 0) ? 1u : 0u);
+          }
+      }
+      umma_commit(bar);
+    }
+  }
+  if (ok && it > 0)
+    ok = __syncthreads_and(rtkb::dev::mbar_wait(bar, (uint32_t)((it - 1) & 1)) ? 1 : 0) != 0;
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  // epilogue: row m of D is output channel m; with M = 128 row m sits in TMEM lane m, with M = 64
+  // rows 16w..16w+15 sit in lanes 32w..32w+15
+  if (ok && it > 0)
+  {
+    const int co = (M == 128) ? warp * 32 + lane : (lane < 16 ? warp * 16 + lane : COUT);
+#pragma unroll 1
+    for (int t = 0; t < 27; t++)
+    {
+      uint32_t r[16];
+      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(t * 16), r);
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (co < COUT)
+#pragma unroll
+        for (int c = 0; c < 16; c++)
+          atomicAdd(dW + ((size_t)t * cin_total + chunk * 16 + c) * COUT + co, __uint_as_float(r[c]));
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols));
+}
+
 // ---- first layer (1 -> 16, CUDA cores) ----------------------------------------------------------------
 // out[v][co] = relu( sum_t x[v + t - 1] * inv_s * W1[t][co] )
 __global__ void __launch_bounds__(256)
@@ -1281,14 +1453,52 @@ conv_fwd(int cout, const ConvIn & in, const bf16 * wp, const Dims & d, bf16 * ou
   }
 }
 
+// Weight-gradient kernel (rtkb_unet_set_wgrad_kernel): 0 = warp-level mma.sync; 1 = tcgen05 with
+// M = 64 (tiles of 8 x 16 x 4 voxels); 2 = tcgen05 with M = 128 (tiles of 8 x 16 x 2 voxels).
+int g_wgrad_kernel = 0;
+
+template <int COUT, int M>
+void
+conv_wgrad_tc_launch(const ConvIn & in, const bf16 * g, const Dims & d, float * dW, cudaStream_t st)
+{
+  using L = WgradTcLayout<M>;
+  const int   smem = tmem_bounded_smem(L::kTotal, 512);
+  static bool configured = false;
+  if (!configured)
+  {
+    cudaFuncSetAttribute(conv_wgrad_tc_kernel<COUT, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    configured = true;
+  }
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess)
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int       nchunks = (in.ca + in.cb) / 16;
+  const long long tiles = (long long)((d.nx + kCX - 1) / kCX) * ((d.ny + kCY - 1) / kCY) *
+                          ((d.nz + L::kKZ - 1) / L::kKZ) * d.batch;
+  const unsigned  gx = (unsigned)std::max<long long>(1, std::min<long long>(tiles, std::max(1, sms / nchunks)));
+  conv_wgrad_tc_kernel<COUT, M><<<dim3(gx, (unsigned)nchunks), 128, smem, st>>>(in, g, d, dW, in.ca + in.cb);
+}
+
+template <int COUT>
+void
+conv_wgrad_dispatch(const ConvIn & in, const bf16 * g, const Dims & d, float * dW, cudaStream_t st)
+{
+  if (g_wgrad_kernel == 1)
+    conv_wgrad_tc_launch<COUT, 64>(in, g, d, dW, st);
+  else if (g_wgrad_kernel == 2)
+    conv_wgrad_tc_launch<COUT, 128>(in, g, d, dW, st);
+  else
+    conv_wgrad_launch<COUT / 8>(in, g, d, dW, st);
+}
+
 void
 conv_wgrad(int cout, const ConvIn & in, const bf16 * g, const Dims & d, float * dW, cudaStream_t st)
 {
   switch (cout)
   {
-  case 16: conv_wgrad_launch<2>(in, g, d, dW, st); break;
-  case 32: conv_wgrad_launch<4>(in, g, d, dW, st); break;
-  default: conv_wgrad_launch<8>(in, g, d, dW, st); break;
+  case 16: conv_wgrad_dispatch<16>(in, g, d, dW, st); break;
+  case 32: conv_wgrad_dispatch<32>(in, g, d, dW, st); break;
+  default: conv_wgrad_dispatch<64>(in, g, d, dW, st); break;
   }
 }
 
@@ -1639,6 +1849,15 @@ rtkb_unet_reserve(rtkb_unet * u, int batch, int nx, int ny, int nz)
     return fail(RTKB_ERR_INVALID_ARGUMENT, "null network");
   const int rc = check_dims(batch, nx, ny, nz);
   return rc != RTKB_OK ? rc : reserve_forward(u, batch, nx, ny, nz);
+}
+
+extern "C" int
+rtkb_unet_set_wgrad_kernel(int kernel)
+{
+  if (kernel < 0 || kernel > 2)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "weight-gradient kernel: 0, 1 or 2");
+  g_wgrad_kernel = kernel;
+  return RTKB_OK;
 }
 
 extern "C" int

@@ -151,3 +151,40 @@ def test_unet_pipelined_convolution_equals_single_stage(rtkb, shape):
         assert rel_l2(grads[pipe], grads[0]) < 1e-5
     assert rtkb.ops.device_status() == 0
     net.close()
+
+
+@pytest.mark.parametrize("kernel", [1, 2])
+def test_unet_tcgen05_weight_gradient(rtkb, kernel):
+    """The tcgen05 weight-gradient kernels (MN-major shared-memory operands:
+    the halo's [k-half][voxel][8 channels] layout and the gradient tile as
+    [channel group][voxel][8 channels]; output channels as M = 64 or 128,
+    27 tap accumulators resident in tensor memory) give the warp-level
+    kernel's gradients up to FP32 summation order, and the oracle's within
+    the gradient bound."""
+    from oracle import unet_ref
+
+    lib = rtkb.load()
+    net = _net(7)
+    rng = np.random.default_rng(5)
+    shape = (2, 16, 12, 20)
+    x = rng.standard_normal(shape).astype(np.float32)
+    t = rng.standard_normal(shape).astype(np.float32) * 0.3
+    params = net.get_parameters()
+    grads = {}
+    try:
+        for k in (0, kernel):
+            assert lib.rtkb_unet_set_wgrad_kernel(k) == 0
+            net.train_step(to_gpu(x), to_gpu(t), update=False)
+            grads[k] = net.split(net.get_gradients())
+    finally:
+        lib.rtkb_unet_set_wgrad_kernel(0)
+    assert rtkb.ops.device_status() == 0
+    _, ref_g, _ = unet_ref.loss_and_gradients(x.astype(np.float64), t.astype(np.float64), params)
+    for k, (a, b, r) in enumerate(zip(grads[kernel], grads[0], net.split(ref_g))):
+        assert rel_l2(a, b) < 1e-5, (k, rel_l2(a, b))
+        assert rel_l2(a, r) < GRAD_TOL, (k, rel_l2(a, r))
+    with pytest.raises(rtkb.RtkbError):
+        from rtk_b200._capi import check
+
+        check(lib.rtkb_unet_set_wgrad_kernel(3))
+    net.close()

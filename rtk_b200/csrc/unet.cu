@@ -29,7 +29,8 @@
 // M = voxels of an 8x16x4 output tile as four M = 128 accumulators in tensor
 // memory, N = output channels, K = 27 taps x 16-channel input chunks, operands
 // from shared-memory descriptors); the weight gradient uses mma.sync m16n8k16
-// with ldmatrix gathers.  Up-sampling and concatenation of the decoder inputs
+// with ldmatrix gathers by default, or a tcgen05 kernel with MN-major operands
+// (rtkb_unet_set_wgrad_kernel; slower for these layer widths).  Up-sampling and concatenation of the decoder inputs
 // are folded into the halo loaders, the ReLU-derivative mask into the
 // data-gradient epilogue.
 #include "rtkb_internal.h"

@@ -776,8 +776,26 @@ def cg_seconds_to_residual(torch, rtkb, stream, tol=1e-3, max_iter=300, learned_
 
     secs, it, rel, per_it, _, x_cg = solve(None)
     cg_hist = solve.hist
+    # roofline of one iteration, the sum of its components' bounds (they run one after another): the
+    # Joseph forward and back projections at the measured shared-memory gather peak (16 B per bilinear
+    # sample, gathered or scattered), and the HBM traffic they cannot avoid (the volume read and the
+    # projections written by the forward projector, the projections read and the volume written by
+    # the back projector) plus the vector updates (about 10 volume reads and writes) at the HBM peak
+    ns = rtkb.ops.joseph_sample_count(g, vd, pd, stream=stream)
+    l1_peak = smem_peak_gbs(torch, rtkb.load(), stream)
+    hbm_peak = peaks().get("hbm_gbs")
+    nvox, npix = 256 ** 3, n * c["det"][0] * c["det"][1]
+    hbm_bytes = 2 * npix * 4 + 12 * nvox * 4
+    t_l1 = 2 * ns * 16 / (l1_peak * 1e9)
+    t_hbm = hbm_bytes / (hbm_peak * 1e9) if hbm_peak else 0.0
+    roofline = {"samples_per_projection": ns, "l1_bytes_per_iteration": 2 * ns * 16, "l1_peak_gbs": l1_peak,
+                "hbm_bytes_per_iteration": hbm_bytes, "hbm_peak_gbs": hbm_peak,
+                "seconds_per_iteration_bound": t_l1 + t_hbm,
+                "seconds_to_rel_residual_1e-3_bound": (t_l1 + t_hbm) * it,
+                "frac": (t_l1 + t_hbm) / per_it if per_it else None,
+                "peak_source": "shared-memory gather probe of this run; MEASURED_PEAKS.json hbm_gbs (of measured)"}
     out = {"seconds_to_rel_residual_1e-3": secs, "iterations": it, "relative_residual": rel,
-           "seconds_per_iteration": per_it, "residual_history": cg_hist,
+           "seconds_per_iteration": per_it, "roofline": roofline, "residual_history": cg_hist,
            "config": "256^3 @1mm <- 360 x 512x384 @0.8mm, SID 1000, SDD 1536, 20 random ellipsoids, "
                      "Poisson I0=5e4, Joseph pair, FP32 vectors / FP64 scalars, CUDA graph per iteration",
            "learned_pcg": None}

@@ -376,6 +376,20 @@ int  rtkb_cg_finish(rtkb_cg * plan, void * stream);
 /* Waits for `stream`; *rr = ||r_k||^2 of the normal equations, *rr0 = ||r_0||^2. */
 int  rtkb_cg_residual(rtkb_cg * plan, double * rr, double * rr0, int * iterations, void * stream);
 void rtkb_cg_destroy(rtkb_cg * plan);
+/* Checkpoint / resume of a CG plan between iterations (no reference
+ * counterpart: RTK resumes only by a warm start from a saved iterate, which
+ * restarts the Krylov recurrence).  rtkb_cg_state_bytes gives the size of the
+ * state -- a 64-byte header, the FP64 scalars (rr, rr0, alpha, beta, pAp), the
+ * residual and direction vectors in the plan's storage types, and the
+ * iteration count.  rtkb_cg_save_state writes it to `buffer` (device or host
+ * memory; waits for `stream`).  rtkb_cg_load_state restores it into a plan of
+ * the same volume size and storage that was started (rtkb_cg_start or
+ * rtkb_cg_start_rhs) on the saved iterate; the next rtkb_cg_iterate then
+ * continues the saved recurrence.  The iterate itself is the caller's
+ * buffer.  Plans with a learned preconditioner are refused (UNSUPPORTED). */
+int  rtkb_cg_state_bytes(const rtkb_cg * plan, long long * bytes);
+int  rtkb_cg_save_state(rtkb_cg * plan, void * buffer, void * stream);
+int  rtkb_cg_load_state(rtkb_cg * plan, const void * buffer, void * stream);
 /* Whole reconstruction: at most max_iterations iterations, stopping early when
  * ||r_k|| <= relative_residual * ||r_0|| (relative_residual <= 0: never). */
 int  rtkb_conjugate_gradient(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,

@@ -211,6 +211,9 @@ SIGNATURES.update({
 
 SIGNATURES.update({
     "rtkb_cg_apply_operator": (C.c_int, [_V, _V, _V, _V]),
+    "rtkb_cg_state_bytes": (C.c_int, [_V, C.POINTER(C.c_longlong)]),
+    "rtkb_cg_save_state": (C.c_int, [_V, _V, _V]),
+    "rtkb_cg_load_state": (C.c_int, [_V, _V, _V]),
     "rtkb_cg_start_rhs": (C.c_int, [_V, _V, _V, _V]),
     "rtkb_joseph_sample_count": (C.c_int, [_G, _IM, _IM, _D, _V]),
     "rtkb_fdk_backproject_bf16": (C.c_int, [_G, _IM, _IM, _V, _V, _V, _V]),

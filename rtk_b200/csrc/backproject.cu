@@ -1426,6 +1426,7 @@ extern "C" int
 rtkb_fdk_backproject(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
                      const float * d_proj, const float * d_vol_in, float * d_vol_out, void * stream)
 {
+  RTKB_TRACE();
   try
   {
     return rtkb::backproject_geometry(g, vol, proj, d_proj, d_vol_in, d_vol_out, stream, true);
@@ -1605,6 +1606,7 @@ extern "C" int
 rtkb_fdk_backproject_host(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
                           const float * h_proj, const float * h_vol_in, float * h_vol_out, int chunk, void * stream)
 {
+  RTKB_TRACE();
   try
   {
     return rtkb::fdk_backproject_host(g, vol, proj, h_proj, h_vol_in, h_vol_out, chunk,
@@ -1620,6 +1622,7 @@ extern "C" int
 rtkb_voxel_backproject(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
                        const float * d_proj, const float * d_vol_in, float * d_vol_out, void * stream)
 {
+  RTKB_TRACE();
   try
   {
     return rtkb::backproject_geometry(g, vol, proj, d_proj, d_vol_in, d_vol_out, stream, false);
@@ -1634,6 +1637,7 @@ extern "C" int
 rtkb_fdk_backproject_bf16(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
                           const void * d_proj_bf16, const float * d_vol_in, float * d_vol_out, void * stream)
 {
+  RTKB_TRACE();
   try
   {
     return rtkb::backproject_geometry(g, vol, proj, static_cast<const __nv_bfloat16 *>(d_proj_bf16), d_vol_in,
@@ -1649,6 +1653,7 @@ extern "C" int
 rtkb_voxel_backproject_bf16(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
                             const void * d_proj_bf16, const float * d_vol_in, float * d_vol_out, void * stream)
 {
+  RTKB_TRACE();
   try
   {
     return rtkb::backproject_geometry(g, vol, proj, static_cast<const __nv_bfloat16 *>(d_proj_bf16), d_vol_in,
@@ -1663,6 +1668,7 @@ rtkb_voxel_backproject_bf16(const rtkb_geometry * g, const rtkb_image_desc * vol
 extern "C" int
 rtkb_fdk_backproject_batch(const rtkb_bp_problem * problems, int n, int config, int * used_config, void * stream)
 {
+  RTKB_TRACE();
   try
   {
     return rtkb::backproject_batch(problems, n, true, config, used_config, static_cast<cudaStream_t>(stream));
@@ -1676,6 +1682,7 @@ rtkb_fdk_backproject_batch(const rtkb_bp_problem * problems, int n, int config, 
 extern "C" int
 rtkb_voxel_backproject_batch(const rtkb_bp_problem * problems, int n, int config, int * used_config, void * stream)
 {
+  RTKB_TRACE();
   try
   {
     return rtkb::backproject_batch(problems, n, false, config, used_config, static_cast<cudaStream_t>(stream));
@@ -1689,6 +1696,7 @@ rtkb_voxel_backproject_batch(const rtkb_bp_problem * problems, int n, int config
 extern "C" int
 rtkb_bp_batch_create(const rtkb_bp_problem * problems, int n, int fdk, int config, rtkb_bp_batch ** batch)
 {
+  RTKB_TRACE();
   try
   {
     return rtkb::create_batch(problems, n, fdk != 0, config, batch);
@@ -1702,6 +1710,7 @@ rtkb_bp_batch_create(const rtkb_bp_problem * problems, int n, int fdk, int confi
 extern "C" int
 rtkb_bp_batch_execute(rtkb_bp_batch * batch, void * stream)
 {
+  RTKB_TRACE();
   return rtkb::execute_batch(batch, static_cast<cudaStream_t>(stream));
 }
 
@@ -1721,6 +1730,7 @@ extern "C" int
 rtkb_backproject_autotune(const rtkb_bp_problem * problems, int n, int fdk, int repeats, int * best_config,
                           double * best_ms, double * config_ms, void * stream)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   if (!problems || n <= 0 || !best_config)
     return fail(RTKB_ERR_INVALID_ARGUMENT, "null argument");
@@ -1789,6 +1799,7 @@ rtkb_backproject_autotune(const rtkb_bp_problem * problems, int n, int fdk, int 
 extern "C" int
 rtkb_convert_to_bf16(const float * d_in, void * d_out, long long n, void * stream)
 {
+  RTKB_TRACE();
   if ((!d_in || !d_out) && n > 0)
     return rtkb::fail(RTKB_ERR_INVALID_ARGUMENT, "null buffer");
   if (n <= 0)
@@ -1805,6 +1816,7 @@ rtkb_backproject_matrices(const int vol_size[3], const int proj_size[3], int n_p
                           const int * modes, int weighting, const float * d_proj, const float * d_vol_in,
                           float * d_vol_out, void * stream)
 {
+  RTKB_TRACE();
   if (!vol_size || !proj_size)
     return rtkb::fail(RTKB_ERR_INVALID_ARGUMENT, "null size");
   try
@@ -1874,6 +1886,7 @@ rtkb_set_wait_limit(unsigned int polls, unsigned int * previous)
 extern "C" int
 rtkb_wait_self_test(void * stream)
 {
+  RTKB_TRACE();
   wait_self_test_kernel<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>();
   RTKB_CUDA_TRY(cudaGetLastError());
   return RTKB_OK;
@@ -1981,6 +1994,7 @@ rtkb_fdk_backproject_static_scratch(const rtkb_geometry * g, const rtkb_image_de
                                     const rtkb_image_desc * proj, const float * d_proj, const float * d_vol_in,
                                     float * d_vol_out, void * stream)
 {
+  RTKB_TRACE();
   if (proj && proj->size[2] > kStaticMaxProjections)
     return rtkb::fail(RTKB_ERR_INVALID_ARGUMENT,
                       "rtkb_fdk_backproject_static_scratch: the stack has more than 2048 projections, the size of "

@@ -643,6 +643,7 @@ extern "C" int
 rtkb_cg_create(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
                const rtkb_cg_params * params, rtkb_cg ** out)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   if (!out)
     return fail(RTKB_ERR_INVALID_ARGUMENT, "null plan pointer");
@@ -880,6 +881,7 @@ extern "C" int
 rtkb_cg_start(rtkb_cg * c, const float * d_proj, const float * d_weights, int displaced_detector, float * d_x,
               void * stream)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   if (!c || !d_proj || !d_x)
     return fail(RTKB_ERR_INVALID_ARGUMENT, "null argument");
@@ -895,6 +897,7 @@ rtkb_cg_start(rtkb_cg * c, const float * d_proj, const float * d_weights, int di
 extern "C" int
 rtkb_cg_start_rhs(rtkb_cg * c, const float * d_b, float * d_x, void * stream)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   if (!c || !d_b || !d_x)
     return fail(RTKB_ERR_INVALID_ARGUMENT, "null argument");
@@ -911,6 +914,7 @@ rtkb_cg_start_rhs(rtkb_cg * c, const float * d_b, float * d_x, void * stream)
 extern "C" int
 rtkb_cg_iterate(rtkb_cg * c, int n, void * stream)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   if (!c || !c->x || n < 0)
     return fail(RTKB_ERR_INVALID_ARGUMENT, "CG plan not started");
@@ -969,6 +973,120 @@ rtkb_cg_residual(rtkb_cg * c, double * rr, double * rr0, int * iterations, void 
   return RTKB_OK;
 }
 
+// ---- checkpoint of a CG plan between iterations --------------------------------------------------
+// Layout: a 64-byte header (magic, version, voxels, storage, iterations), the five FP64 scalars
+// (rr, rr0, alpha, beta, pAp), R and P in the plan's storage types.
+namespace
+{
+constexpr unsigned long long kStateMagic = 0x3174617453474342ull; // "BCGStat1" in little-endian bytes
+struct StateHeader
+{
+  unsigned long long magic;
+  long long          nvox;
+  int                version, storage, iterations, pad;
+  char               reserved[32];
+};
+static_assert(sizeof(StateHeader) == 64, "state header size");
+
+int
+plan_storage(const rtkb_cg * c)
+{
+  return c->bf16 ? 1 : (c->bf16p ? 2 : 0);
+}
+
+size_t
+r_bytes(const rtkb_cg * c)
+{
+  return (size_t)c->nvox * (c->bf16 ? 2 : 4);
+}
+
+size_t
+p_bytes(const rtkb_cg * c)
+{
+  return (size_t)c->nvox * ((c->bf16 || c->bf16p) ? 2 : 4);
+}
+
+int
+state_check(const rtkb_cg * c)
+{
+  if (!c)
+    return rtkb::fail(RTKB_ERR_INVALID_ARGUMENT, "null plan");
+  if (c->net)
+    return rtkb::fail(RTKB_ERR_UNSUPPORTED, "the state of a plan with a learned preconditioner is not saved");
+  return RTKB_OK;
+}
+} // namespace
+
+extern "C" int
+rtkb_cg_state_bytes(const rtkb_cg * c, long long * bytes)
+{
+  int rc = state_check(c);
+  if (rc != RTKB_OK)
+    return rc;
+  if (!bytes)
+    return rtkb::fail(RTKB_ERR_INVALID_ARGUMENT, "null argument");
+  *bytes = (long long)(sizeof(StateHeader) + 5 * sizeof(double) + r_bytes(c) + p_bytes(c));
+  return RTKB_OK;
+}
+
+extern "C" int
+rtkb_cg_save_state(rtkb_cg * c, void * buffer, void * stream)
+{
+  RTKB_TRACE();
+  using namespace rtkb;
+  int rc = state_check(c);
+  if (rc != RTKB_OK)
+    return rc;
+  if (!buffer)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "null buffer");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  StateHeader  h{};
+  h.magic = kStateMagic;
+  h.nvox = c->nvox;
+  h.version = 1;
+  h.storage = plan_storage(c);
+  h.iterations = c->iterations;
+  char * b = static_cast<char *>(buffer);
+  RTKB_CUDA_TRY(cudaMemcpyAsync(b + sizeof(h), c->scal, 5 * sizeof(double), cudaMemcpyDefault, st));
+  RTKB_CUDA_TRY(cudaMemcpyAsync(b + sizeof(h) + 5 * sizeof(double), c->R, r_bytes(c), cudaMemcpyDefault, st));
+  RTKB_CUDA_TRY(
+    cudaMemcpyAsync(b + sizeof(h) + 5 * sizeof(double) + r_bytes(c), c->P, p_bytes(c), cudaMemcpyDefault, st));
+  // the header last, from this frame: synchronous with respect to the host for pageable memory, so
+  // wait for the stream before h goes out of scope
+  RTKB_CUDA_TRY(cudaMemcpyAsync(b, &h, sizeof(h), cudaMemcpyDefault, st));
+  RTKB_CUDA_TRY(cudaStreamSynchronize(st));
+  return RTKB_OK;
+}
+
+extern "C" int
+rtkb_cg_load_state(rtkb_cg * c, const void * buffer, void * stream)
+{
+  RTKB_TRACE();
+  using namespace rtkb;
+  int rc = state_check(c);
+  if (rc != RTKB_OK)
+    return rc;
+  if (!buffer)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "null buffer");
+  if (!c->x)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "start the plan (rtkb_cg_start) with the saved iterate first");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  StateHeader  h{};
+  RTKB_CUDA_TRY(cudaStreamSynchronize(st));
+  RTKB_CUDA_TRY(cudaMemcpy(&h, buffer, sizeof(h), cudaMemcpyDefault));
+  if (h.magic != kStateMagic || h.version != 1)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "not a CG state");
+  if (h.nvox != c->nvox || h.storage != plan_storage(c) || h.iterations < 0)
+    return fail(RTKB_ERR_INVALID_ARGUMENT, "the state belongs to a plan of another size or storage");
+  const char * b = static_cast<const char *>(buffer);
+  RTKB_CUDA_TRY(cudaMemcpyAsync(c->scal, b + sizeof(h), 5 * sizeof(double), cudaMemcpyDefault, st));
+  RTKB_CUDA_TRY(cudaMemcpyAsync(c->R, b + sizeof(h) + 5 * sizeof(double), r_bytes(c), cudaMemcpyDefault, st));
+  RTKB_CUDA_TRY(
+    cudaMemcpyAsync(c->P, b + sizeof(h) + 5 * sizeof(double) + r_bytes(c), p_bytes(c), cudaMemcpyDefault, st));
+  c->iterations = h.iterations;
+  return RTKB_OK;
+}
+
 extern "C" void
 rtkb_cg_destroy(rtkb_cg * c)
 {
@@ -978,6 +1096,7 @@ rtkb_cg_destroy(rtkb_cg * c)
 extern "C" int
 rtkb_cg_set_support_mask(rtkb_cg * c, const float * d_mask)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   if (!c)
     return fail(RTKB_ERR_INVALID_ARGUMENT, "null plan");
@@ -996,6 +1115,7 @@ rtkb_cg_set_support_mask(rtkb_cg * c, const float * d_mask)
 extern "C" int
 rtkb_cg_finish(rtkb_cg * c, void * stream)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   if (!c || !c->x)
     return fail(RTKB_ERR_INVALID_ARGUMENT, "CG plan not started");
@@ -1012,6 +1132,7 @@ rtkb_conjugate_gradient(const rtkb_geometry * g, const rtkb_image_desc * vol, co
                         int displaced_detector, float * d_x, int max_iterations, double relative_residual,
                         int * iterations, double * final_relative_residual, void * stream)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   rtkb_cg * c = nullptr;
   int       rc = rtkb_cg_create(g, vol, proj, params, &c);
@@ -1043,6 +1164,7 @@ rtkb_conjugate_gradient(const rtkb_geometry * g, const rtkb_image_desc * vol, co
 extern "C" int
 rtkb_cg_set_preconditioner(rtkb_cg * c, rtkb_unet * net, int history)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   if (!c)
     return fail(RTKB_ERR_INVALID_ARGUMENT, "null plan");
@@ -1107,6 +1229,7 @@ rtkb_cg_preconditioner_status(const rtkb_cg * c, int * active, int * fallback_it
 extern "C" int
 rtkb_cg_apply_operator(rtkb_cg * c, const float * d_in, float * d_out, void * stream)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   if (!c || !d_in || !d_out || d_in == d_out)
     return fail(RTKB_ERR_INVALID_ARGUMENT, "null or aliased argument");
@@ -1200,6 +1323,7 @@ extern "C" int
 rtkb_cg_batch_create(const rtkb_cg_batch_problem * problems, int n, const rtkb_cg_params * params,
                      rtkb_cg_batch ** out)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   if (!out || !problems || n <= 0)
     return fail(RTKB_ERR_INVALID_ARGUMENT, "null argument or empty batch");
@@ -1262,6 +1386,7 @@ rtkb_cg_batch_create(const rtkb_cg_batch_problem * problems, int n, const rtkb_c
 extern "C" int
 rtkb_cg_batch_start(rtkb_cg_batch * b, const rtkb_cg_batch_problem * problems, void * stream)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   if (!b || !problems)
     return fail(RTKB_ERR_INVALID_ARGUMENT, "null argument");
@@ -1280,6 +1405,7 @@ rtkb_cg_batch_start(rtkb_cg_batch * b, const rtkb_cg_batch_problem * problems, v
 extern "C" int
 rtkb_cg_batch_iterate(rtkb_cg_batch * b, int niter, void * stream)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   if (!b || !b->started || niter < 0)
     return fail(RTKB_ERR_INVALID_ARGUMENT, "batch not started");
@@ -1318,6 +1444,7 @@ rtkb_cg_batch_destroy(rtkb_cg_batch * b)
 extern "C" int
 rtkb_laplacian(const rtkb_image_desc * vol, const float * d_in, float * d_out, void * stream)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   std::string why;
   if (!vol || !d_in || !d_out || d_in == d_out)

@@ -654,6 +654,7 @@ extern "C" int
 rtkb_fdk_weight(const rtkb_geometry * g, const rtkb_image_desc * proj, const float * d_in, float * d_out,
                 void * stream)
 {
+  RTKB_TRACE();
   return guarded([&] {
     Options o;
     o.fdk = true;
@@ -665,6 +666,7 @@ extern "C" int
 rtkb_parker_short_scan(const rtkb_geometry * g, const rtkb_image_desc * proj, double threshold, const float * d_in,
                        float * d_out, void * stream, int * is_short_scan)
 {
+  RTKB_TRACE();
   return guarded([&] {
     if (!std::isfinite(threshold))
       return rtkb::fail(RTKB_ERR_INVALID_ARGUMENT, "invalid angular gap threshold");
@@ -679,6 +681,7 @@ extern "C" int
 rtkb_displaced_detector_region(const rtkb_geometry * g, const rtkb_image_desc * proj, int pad, rtkb_image_desc * out,
                                int * weighted)
 {
+  RTKB_TRACE();
   return guarded([&] {
     std::string why;
     if (!g || !out)
@@ -700,6 +703,7 @@ extern "C" int
 rtkb_displaced_detector(const rtkb_geometry * g, const rtkb_image_desc * proj, int pad, const float * d_in,
                         float * d_out, void * stream)
 {
+  RTKB_TRACE();
   return guarded([&] {
     Options o;
     o.displaced = true;
@@ -711,6 +715,7 @@ rtkb_displaced_detector(const rtkb_geometry * g, const rtkb_image_desc * proj, i
 extern "C" int
 rtkb_ramp_kernel(int nu, double spacing, const rtkb_ramp_params * p, int * padded, double * kernel)
 {
+  RTKB_TRACE();
   return guarded([&] {
     if (nu <= 0 || !p || !padded || !std::isfinite(spacing) || spacing == 0.)
       return rtkb::fail(RTKB_ERR_INVALID_ARGUMENT, "invalid ramp kernel arguments");
@@ -732,6 +737,7 @@ extern "C" int
 rtkb_ramp_filter(const rtkb_image_desc * proj, const rtkb_ramp_params * p, const float * d_in, float * d_out,
                  void * stream)
 {
+  RTKB_TRACE();
   return guarded([&] {
     if (!p)
       return rtkb::fail(RTKB_ERR_INVALID_ARGUMENT, "null ramp parameters");
@@ -755,6 +761,7 @@ extern "C" int
 rtkb_fdk_preprocess(const rtkb_geometry * g, const rtkb_image_desc * proj, const rtkb_fdk_preprocess_params * p,
                     rtkb_image_desc * out, const float * d_in, float * d_out, void * stream)
 {
+  RTKB_TRACE();
   return guarded([&] {
     if (!p)
       return rtkb::fail(RTKB_ERR_INVALID_ARGUMENT, "null preprocessing parameters");

@@ -868,6 +868,7 @@ extern "C" int
 rtkb_joseph_forward_project(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
                             const float * d_vol, const float * d_proj_in, float * d_proj_out, void * stream)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   try
   {
@@ -907,6 +908,7 @@ extern "C" int
 rtkb_joseph_back_project(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
                          const float * d_proj, const float * d_vol_in, float * d_vol_out, void * stream)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   try
   {
@@ -947,6 +949,7 @@ extern "C" int
 rtkb_joseph_sample_count(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
                          double * count, void * stream)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   try
   {

@@ -245,6 +245,7 @@ extern "C" int
 rtkb_de_pierro_regularization(const rtkb_image_desc * vol, const float * d_xk, const float * d_update,
                               const float * d_norm, double beta, float * d_out, void * stream)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   std::string why;
   if (!vol || !d_xk || !d_update || !d_out)
@@ -274,6 +275,7 @@ extern "C" int
 rtkb_osem(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj, const float * d_proj,
           float * d_x, const rtkb_osem_params * prm, void * stream)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   std::string why;
   if (!g || !vol || !proj || !d_proj || !d_x || !prm)

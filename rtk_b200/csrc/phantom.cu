@@ -75,6 +75,7 @@ extern "C" int
 rtkb_project_ellipsoids(const rtkb_geometry * g, const rtkb_image_desc * proj, int n_ellipsoids,
                         const double * ellipsoids, float * d_out, void * stream)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   std::string why;
   if (!g || !d_out || n_ellipsoids < 0 || (n_ellipsoids > 0 && !ellipsoids))

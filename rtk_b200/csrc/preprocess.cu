@@ -219,6 +219,7 @@ extern "C" int
 rtkb_i0_estimation(const rtkb_image_desc * desc, const unsigned short * d_raw, int bit_shift,
                    unsigned int dyn_threshold, rtkb_i0_estimate * out, void * stream)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   std::string why;
   if (!desc || !d_raw || !out)
@@ -272,6 +273,7 @@ extern "C" int
 rtkb_raw_to_attenuation(const rtkb_image_desc * desc, const unsigned short * d_raw, double i0, double idark,
                         float * d_out, void * stream)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   std::string why;
   if (!desc || !d_raw || !d_out)
@@ -315,6 +317,7 @@ extern "C" int
 rtkb_water_precorrection(const rtkb_image_desc * desc, const float * d_in, float * d_out, const double * coefficients,
                          int n_coefficients, void * stream)
 {
+  RTKB_TRACE();
   // WaterPrecorrectionImageFilter::DynamicThreadedGenerateData
   // (include/rtkWaterPrecorrectionImageFilter.hxx:14-62), an in-place filter:
   // the cases it leaves untouched (no coefficients, the identity (0, 1), a

@@ -433,6 +433,7 @@ extern "C" int
 rtkb_tv_denoising_bpdq(const rtkb_image_desc * vol, const float * d_in, float * d_out, double gamma, int niter,
                        const int dims_processed[3], void * stream)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   std::string why;
   if (!vol || !d_in || !d_out)
@@ -459,6 +460,7 @@ rtkb_tv_denoising_bpdq(const rtkb_image_desc * vol, const float * d_in, float * 
 extern "C" int
 rtkb_total_variation(const rtkb_image_desc * vol, const float * d_in, double * tv, void * stream)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   std::string why;
   if (!vol || !d_in || !tv)
@@ -492,6 +494,7 @@ rtkb_regularized_cg(const rtkb_geometry * g, const rtkb_image_desc * vol, const 
                     const float * d_proj, const float * d_weights, float * d_x,
                     const rtkb_regularized_cg_params * prm, void * stream)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   std::string why;
   if (!g || !vol || !proj || !d_proj || !d_x || !prm)

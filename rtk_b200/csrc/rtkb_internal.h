@@ -9,9 +9,22 @@
 #include <vector>
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 namespace rtkb
 {
+
+// NVTX range around a C-ABI entry point (header-only NVTX 3): a push and a pop
+// that cost nothing without a tool attached, and name each call on an ncu or
+// Nsight timeline (ncu --nvtx --nvtx-include "rtkb_fdk_backproject/").
+struct TraceRange
+{
+  explicit TraceRange(const char * name) { nvtxRangePushA(name); }
+  ~TraceRange() { nvtxRangePop(); }
+  TraceRange(const TraceRange &) = delete;
+  TraceRange & operator=(const TraceRange &) = delete;
+};
+
 
 // ---- error reporting -------------------------------------------------------
 void         set_error(const std::string & msg);
@@ -121,3 +134,5 @@ struct rtkb_geometry
 {
   rtkb::Geometry g;
 };
+
+#define RTKB_TRACE() rtkb::TraceRange rtkb_trace_range_(__func__)

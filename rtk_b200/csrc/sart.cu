@@ -238,6 +238,7 @@ extern "C" int
 rtkb_ray_box_lengths(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj, float * d_out,
                      void * stream)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   std::string why;
   if (!g || !vol || !proj || !d_out)
@@ -262,6 +263,7 @@ extern "C" int
 rtkb_sart(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj, const float * d_proj,
           float * d_x, const rtkb_sart_params * prm, void * stream)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   std::string why;
   if (!g || !vol || !proj || !d_proj || !d_x || !prm)
@@ -383,6 +385,7 @@ extern "C" int
 rtkb_iterative_fdk(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
                    const float * d_proj, float * d_x, const rtkb_iterative_fdk_params * prm, void * stream)
 {
+  RTKB_TRACE();
   // IterativeFDKConeBeamReconstructionFilter::GenerateData
   // (include/rtkIterativeFDKConeBeamReconstructionFilter.hxx:171-218):
   // x += FDK(p); then niter - 1 times x += FDK(lambda (p - JosephFP(x)) / raybox)

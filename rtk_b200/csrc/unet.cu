@@ -1722,6 +1722,7 @@ backward(rtkb_unet * u, const float * x, const float * tgt, int margin, cudaStre
 extern "C" int
 rtkb_unet_create(unsigned long long seed, rtkb_unet ** out)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   if (!out)
     return fail(RTKB_ERR_INVALID_ARGUMENT, "null network pointer");
@@ -1807,6 +1808,7 @@ rtkb_unet_num_parameters(const rtkb_unet * u)
 extern "C" int
 rtkb_unet_get_parameters(const rtkb_unet * u, float * host, long long n)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   if (!u || !host || n != u->nparams)
     return fail(RTKB_ERR_INVALID_ARGUMENT, "parameter count mismatch");
@@ -1834,6 +1836,7 @@ rtkb_unet_set_parameters(rtkb_unet * u, const float * host, long long n)
 extern "C" int
 rtkb_unet_get_gradients(const rtkb_unet * u, float * host, long long n)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   if (!u || !host || n != u->nparams)
     return fail(RTKB_ERR_INVALID_ARGUMENT, "parameter count mismatch");
@@ -1845,6 +1848,7 @@ rtkb_unet_get_gradients(const rtkb_unet * u, float * host, long long n)
 extern "C" int
 rtkb_unet_reserve(rtkb_unet * u, int batch, int nx, int ny, int nz)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   if (!u)
     return fail(RTKB_ERR_INVALID_ARGUMENT, "null network");
@@ -1874,6 +1878,7 @@ extern "C" int
 rtkb_unet_forward(rtkb_unet * u, int batch, int nx, int ny, int nz, const float * d_in, float * d_out, int normalize,
                   void * stream)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   if (!u || !d_in || !d_out)
     return fail(RTKB_ERR_INVALID_ARGUMENT, "null argument");
@@ -1890,6 +1895,7 @@ extern "C" int
 rtkb_unet_train_step(rtkb_unet * u, int batch, int nx, int ny, int nz, const float * d_in, const float * d_target,
                      int loss_margin, double learning_rate, int update, double * loss, void * stream)
 {
+  RTKB_TRACE();
   using namespace rtkb;
   if (!u || !d_in || !d_target)
     return fail(RTKB_ERR_INVALID_ARGUMENT, "null argument");

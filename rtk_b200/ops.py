@@ -7,6 +7,8 @@ returns without synchronising.  Errors raise ``RtkbError``.
 from __future__ import annotations
 
 import ctypes as C
+import json
+import os
 
 from ._capi import check, load
 from .image import shape_of
@@ -541,6 +543,23 @@ class ConjugateGradient:
         check(self._lib.rtkb_cg_apply_operator(self._h, _ptr(x), _ptr(out), _stream(stream)))
         return out
 
+    def save_state(self, stream=None, device="cuda"):
+        """Checkpoint of the recurrence (rtkb_cg_save_state): a uint8 tensor on
+        `device` holding the scalars, R, P and the iteration count; the iterate
+        x is the caller's tensor and is saved by the caller."""
+        n = C.c_longlong()
+        check(self._lib.rtkb_cg_state_bytes(self._h, C.byref(n)))
+        buf = _torch().empty(n.value, dtype=_torch().uint8, device=device)
+        check(self._lib.rtkb_cg_save_state(self._h, C.c_void_p(buf.data_ptr()), _stream(stream)))
+        return buf
+
+    def load_state(self, buf, stream=None):
+        """Resume from save_state()'s checkpoint (rtkb_cg_load_state); call
+        after start() on the saved iterate."""
+        if buf.dtype != _torch().uint8 or not buf.is_contiguous():
+            raise TypeError("expected the contiguous uint8 tensor save_state() returned")
+        check(self._lib.rtkb_cg_load_state(self._h, C.c_void_p(buf.data_ptr()), _stream(stream)))
+
     def residual(self, stream=None):
         """(||r_k||^2, ||r_0||^2, k) -- synchronises the stream."""
         rr, rr0, it = C.c_double(), C.c_double(), C.c_int()
@@ -724,15 +743,57 @@ def backproject_batch(problems, fdk=True, config=-1, stream=None):
     return used.value
 
 
-def backproject_autotune(problems, fdk=True, repeats=2, stream=None):
+def _tune_key(problems, fdk, device_name):
+    """Autotuner cache key: the kernel, the device and every problem's volume
+    and stack sizes (the tile configuration depends on nothing else)."""
+    shapes = sorted((tuple(int(v) for v in p[1].size), tuple(int(v) for v in p[2].size)) for p in problems)
+    return json.dumps({"kernel": "fdk_backproject" if fdk else "voxel_backproject", "device": device_name,
+                       "problems": shapes}, sort_keys=True)
+
+
+def _cache_get(path, key):
+    try:
+        with open(path) as f:
+            return json.load(f).get(key)
+    except (OSError, ValueError):
+        return None
+
+
+def _cache_put(path, key, value):
+    """Adds one entry to the JSON cache file (written to a temporary file and
+    renamed, so a reader never sees a partial file)."""
+    try:
+        with open(path) as f:
+            data = json.load(f)
+    except (OSError, ValueError):
+        data = {}
+    data[key] = value
+    tmp = f"{path}.{os.getpid()}.tmp"
+    with open(tmp, "w") as f:
+        json.dump(data, f, indent=1, sort_keys=True)
+    os.replace(tmp, path)
+
+
+def backproject_autotune(problems, fdk=True, repeats=2, stream=None, cache=None):
     """The project's autotuner: times every backprojector configuration on the
-    batch and returns (best configuration, its ms, [ms per configuration])."""
+    batch and returns (best configuration, its ms, [ms per configuration]).
+    cache: path of a JSON file of earlier results keyed by kernel, device and
+    problem sizes; a hit returns the stored result without timing anything."""
+    key = None
+    if cache is not None:
+        key = _tune_key(problems, fdk, _torch().cuda.get_device_name())
+        hit = _cache_get(cache, key)
+        if hit is not None:
+            return hit["config"], hit["ms"], hit["ms_per_config"]
     arr, _ = _problem_array(problems)
     times = (C.c_double * 16)(*([-1.0] * 16))  # one entry per configuration (fewer than 16)
     best, best_ms = C.c_int(), C.c_double()
     check(load().rtkb_backproject_autotune(arr, len(problems), int(fdk), int(repeats), C.byref(best),
                                            C.byref(best_ms), times, _stream(stream)))
-    return best.value, best_ms.value, [t for t in times if t >= 0.0]
+    result = (best.value, best_ms.value, [t for t in times if t >= 0.0])
+    if cache is not None:
+        _cache_put(cache, key, {"config": result[0], "ms": result[1], "ms_per_config": result[2]})
+    return result
 
 
 class BackprojectionBatch:

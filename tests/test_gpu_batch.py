@@ -112,3 +112,23 @@ def test_single_problem_autotune_and_forced_configuration(rtkb, oracle):
         rtkb.ops.backproject_config(-1)
     assert count == 6 and last in (best, -1)
     assert rel_l2(got, oracle.backproject(go, vo, po, p, v0)) < REL_L2_TOL
+
+
+def test_autotune_cache_hit_returns_the_stored_result(rtkb, oracle, tmp_path):
+    """With a cache file, the first call times the configurations and stores
+    the result under (kernel, device, problem sizes); the second call returns
+    it without timing (identical per-configuration times), another kernel
+    choice misses."""
+    probs = _problems(rtkb, oracle, n=3, seed=8)
+    args = [(gl, vd, pd, to_gpu(p), to_gpu(v0), to_gpu(np.zeros(oracle.shape_of(vo))))
+            for (gl, go, vd, vo, pd, po, p, v0) in probs]
+    path = str(tmp_path / "autotune.json")
+    first = rtkb.ops.backproject_autotune(args, repeats=1, cache=path)
+    second = rtkb.ops.backproject_autotune(args, repeats=1, cache=path)
+    assert second == first
+    other = rtkb.ops.backproject_autotune(args, fdk=False, repeats=1, cache=path)
+    assert len(other[2]) == 6
+    import json
+
+    with open(path) as f:
+        assert len(json.load(f)) == 2

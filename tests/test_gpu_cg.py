@@ -331,3 +331,51 @@ def test_cg_support_mask_matches_oracle(rtkb, oracle, kind):
     cg.finish()
     assert rel_l2(to_np(x), ref) < 1e-4, rel_l2(to_np(x), ref)
     assert np.all(to_np(x)[mask == 0] == 0.0)
+
+
+@pytest.mark.parametrize("storage,where", [("fp32", "cuda"), ("bf16_direction", "cpu")])
+def test_cg_checkpoint_resume(rtkb, oracle, storage, where):
+    """rtkb_cg_save_state after 3 iterations, a new plan started on the saved
+    iterate and loaded from the checkpoint, 3 more iterations: the iterate and
+    residuals of 6 uninterrupted iterations (the back projector's atomics
+    reorder FP32 sums, hence a tolerance), unlike a warm start from the saved
+    iterate, which restarts the recurrence; foreign checkpoints are refused."""
+    import torch
+
+    gl, go, vd, vo, pd, po, p = _problem(rtkb, oracle, seed=4)
+    dp = to_gpu(p)
+
+    def plan():
+        return rtkb.ops.ConjugateGradient(gl, vd, pd, storage=storage)
+
+    x = torch.zeros(oracle.shape_of(vo), device="cuda")
+    a = plan().start(dp, x, displaced_detector=False)
+    a.iterate(3)
+    x3 = x.clone()
+    state = a.save_state(device=where)
+    rr3 = a.residual()
+    a.iterate(3)
+    rr6 = a.residual()
+    x6 = to_np(x)
+
+    xb = x3.clone()
+    b = plan().start(dp, xb, displaced_detector=False)
+    b.load_state(state)
+    assert b.residual() == rr3
+    b.iterate(3)
+    rb = b.residual()
+    assert rb[2] == 6 and abs(rb[0] - rr6[0]) <= 1e-4 * rr6[0]
+    assert rel_l2(to_np(xb), x6) < 1e-5
+
+    xc = x3.clone()
+    c = plan().start(dp, xc, displaced_detector=False)  # warm start: a new recurrence
+    c.iterate(3)
+    assert rel_l2(to_np(xc), x6) > 10 * rel_l2(to_np(xb), x6)
+
+    other = rtkb.ops.ConjugateGradient(gl, vd, pd, storage="bf16" if storage == "fp32" else "fp32")
+    other.start(dp, torch.zeros_like(x), displaced_detector=False)
+    with pytest.raises(rtkb.RtkbError):
+        other.load_state(state)
+    for q in (a, b, c, other):
+        q.close()
+    assert rtkb.ops.device_status() == 0

@@ -164,14 +164,16 @@ int rtkb_fdk_backproject(const rtkb_geometry * g, const rtkb_image_desc * vol, c
 int rtkb_voxel_backproject(const rtkb_geometry * g, const rtkb_image_desc * vol, const rtkb_image_desc * proj,
                            const float * d_proj, const float * d_vol_in, float * d_vol_out, void * stream);
 /* rtk::FDKBackProjectionImageFilter on host buffers, as RTK's CUDA pipeline
- * runs it from CPU images: the stack is streamed to the device in subsets of
- * `chunk` projections (include/rtkFDKConeBeamReconstructionFilter.hxx:116-157;
- * chunk <= 0: an eighth of the stack), each copied on an internal stream into
- * one of two device staging buffers while the previous one is backprojected
- * into a device copy of the volume (the first chunk, whose copy nothing
- * overlaps, is a quarter of the others); the last chunk is backprojected in
- * eight z-slabs, each copied back while the next is computed (the host<->device
- * transfers ITK's CudaDataManager makes around
+ * runs it from CPU images: the stack is streamed to the device in projection
+ * subsets (include/rtkFDKConeBeamReconstructionFilter.hxx:116-157), each
+ * copied on an internal stream into one of two device staging buffers while
+ * the previous one is backprojected into a device copy of the volume.  The
+ * subsets grow geometrically (x1.5) from chunk/12 to `chunk` projections
+ * (chunk <= 0: a quarter of the stack), so that each copy hides behind the
+ * previous subset's backprojection from the first, short one on; the last
+ * subset takes the remainder (up to 1.5 chunk) and is backprojected in
+ * sixteen z-slabs, each copied back while the next is computed (the
+ * host<->device transfers ITK's CudaDataManager makes around
  * rtkCudaFDKBackProjectionImageFilter.cxx:34-125, overlapped).  h_vol_in may
  * be NULL (zero volume).  Asynchronous on `stream`
  * like cudaMemcpyAsync: h_vol_out is written when the stream reaches the end

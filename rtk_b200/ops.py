@@ -668,11 +668,11 @@ def _host_ptr(t, what):
 
 def fdk_backproject_host(geometry, vol_desc, proj_desc, proj, vol_in=None, out=None, chunk=0, stream=None):
     """rtkb_fdk_backproject_host: FDK backprojection of a host (CPU) stack into a
-    host volume, the stack streamed to the GPU in chunks of `chunk`
-    projections (0: an eighth of the stack) whose copies overlap the
-    backprojection of the previous chunk (the first chunk is a quarter of the
-    others); the volume comes back slab by slab while the last chunk is
-    backprojected.  vol_in None means a zero volume.
+    host volume, the stack streamed to the GPU in subsets growing from
+    chunk / 12 to `chunk` projections (0: a quarter of the stack), each copy
+    overlapping the backprojection of the previous subset; the volume comes
+    back slab by slab while the last subset is backprojected.  vol_in None
+    means a zero volume.
     Asynchronous on `stream`: synchronise it before reading `out`.  Pinned
     tensors (pin_memory=True) give full copy bandwidth and overlap."""
     torch = _torch()

@@ -1338,9 +1338,9 @@ def main():
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h_proj.numel() * 4,
                     "d2h_bytes_per_step": h_vol.numel() * 4,
                     "path": "rtkb_fdk_backproject_host via ctypes: pinned host stack in, pinned host volume out, "
-                            "the stack's copy (a short first chunk, then chunks of 90 projections) and the volume's copy "
-                            "back (8 slabs) overlapped with the "
-                            "backprojection, all inside the timed region"},
+                            "the stack's copy (subsets growing x1.5 from 15 to 180 projections, the last one the "
+                            "remainder) and the volume's copy back (16 slabs) overlapped with the backprojection, all "
+                            "inside the timed region"},
             "roofline": roofline, "clocks": clocks, "gpu_launches": args.steps,
             "gpu_launches_note": "one rtkb backprojection kernel per step (plus one matrix upload copy)",
             "autotune": tuned}

@@ -496,6 +496,10 @@ def c4_leg(torch, rtkb, stream, n=64, niter=10):
     bp_args = [(P["g"], P["vd"], P["pd"], P["f"], P["zero"], P["x"]) for P in probs]
     best, _, _ = rtkb.ops.backproject_autotune(bp_args, repeats=1, stream=stream)
     bpb = rtkb.ops.BackprojectionBatch(bp_args, config=best)
+    # the Joseph pair's band heights from the autotuner, timed on the largest problem
+    big = max(probs, key=lambda P: P["nv"] ** 3 * P["np"])
+    bands = rtkb.ops.joseph_autotune(big["g"], big["vd"], big["pd"], torch.ones_like(big["zero"]), big["p"],
+                                     repeats=1, stream=stream)
     cgb = rtkb.ops.ConjugateGradientBatch([(P["g"], P["vd"], P["pd"], P["p"], P["x"], None, False) for P in probs])
     lib = rtkb.load()
     plans = [lib.rtkb_cg_batch_plan(cgb._h, i) for i in range(n)]
@@ -558,6 +562,7 @@ def c4_leg(torch, rtkb, stream, n=64, niter=10):
             cg_errs[f"problem_{i}"] = float(np.linalg.norm(got_cg - ref_cg) / np.linalg.norm(ref_cg))
     except Exception as ex:
         errs = {"error": str(ex)}
+    rtkb.ops.joseph_band_rows(8, 8)
     bpb.close()
     cgb.close()
     return {"workload": f"{n} problems: FDK (weights + Hann ramp + backprojection) then {niter} CG iterations "
@@ -565,7 +570,7 @@ def c4_leg(torch, rtkb, stream, n=64, niter=10):
                         "128^2-512^2, SID 800-1200 mm (seeded ellipsoid phantoms)",
             "batched_ms": times["batched"], "one_problem_after_another_ms": times["one_after_another"],
             "speedup": times["one_after_another"] / times["batched"],
-            "autotuned_config": best,
+            "autotuned_config": best, "joseph_band_rows": {"forward": bands["forward"], "back": bands["back"]},
             "fdk_oracle_rel_l2": errs,
             f"cg_{niter}_iterations_oracle_rel_l2": cg_errs,
             "launches_batched": "preprocessing per problem, one persistent backprojection launch, one CUDA graph "
@@ -774,6 +779,9 @@ def cg_seconds_to_residual(torch, rtkb, stream, tol=1e-3, max_iter=300, learned_
         solve.hist = hist
         return (secs if rr <= tol * tol * rr0 else None), it, (rr / rr0) ** 0.5, secs / max(it, 1), status, x
 
+    # the Joseph pair's band heights from the autotuner, timed on this problem
+    bands = rtkb.ops.joseph_autotune(g, vd, pd, torch.zeros((256, 256, 256), device="cuda").add_(0.01), p,
+                                     repeats=2, stream=stream)
     secs, it, rel, per_it, _, x_cg = solve(None)
     cg_hist = solve.hist
     # roofline of one iteration, the sum of its components' bounds (they run one after another): the
@@ -795,7 +803,8 @@ def cg_seconds_to_residual(torch, rtkb, stream, tol=1e-3, max_iter=300, learned_
                 "frac": (t_l1 + t_hbm) / per_it if per_it else None,
                 "peak_source": "shared-memory gather probe of this run; MEASURED_PEAKS.json hbm_gbs (of measured)"}
     out = {"seconds_to_rel_residual_1e-3": secs, "iterations": it, "relative_residual": rel,
-           "seconds_per_iteration": per_it, "roofline": roofline, "residual_history": cg_hist,
+           "seconds_per_iteration": per_it, "roofline": roofline, "joseph_band_rows": bands,
+           "residual_history": cg_hist,
            "config": "256^3 @1mm <- 360 x 512x384 @0.8mm, SID 1000, SDD 1536, 20 random ellipsoids, "
                      "Poisson I0=5e4, Joseph pair, FP32 vectors / FP64 scalars, CUDA graph per iteration",
            "learned_pcg": None}
@@ -883,6 +892,7 @@ def cg_seconds_to_residual(torch, rtkb, stream, tol=1e-3, max_iter=300, learned_
         "method": "flexible PCG, history 8, 3-level 3D U-Net 16/32/64 (BF16 convolutions: tcgen05 forward "
                   "and data gradient, mma.sync weight gradient; FP32 accumulation), fallback to plain CG after 2 "
                   "non-improving iterations"}
+    rtkb.ops.joseph_band_rows(8, 8)
     return out
 
 

@@ -605,6 +605,16 @@ int rtkb_backproject_config(int force, int * last_used, int * count);
  * projections are then summed in an order that varies from run to run (FP32
  * rounding differences, ~5e-7 relative).  sweep_shift in 0..10. */
 int rtkb_bp_set_schedule(int schedule, int sweep_shift);
+/* Detector rows per band of the Joseph projectors' grids (no reference
+ * counterpart), for later calls in this process: every projection of a band
+ * runs before the next band, so the blocks in flight touch one y-slab of the
+ * volume's copies and accumulators, which stays in L2.  8, 16, 32 or 64 rows
+ * for the forward and the back projector (default 8 and 8); the forward
+ * projection is identical whatever the band, the back projection up to FP32
+ * summation order.  rtk_b200.ops.joseph_autotune times the choices on the
+ * caller's problem.  rtkb_joseph_get_band_rows reads the current values. */
+int rtkb_joseph_set_band_rows(int forward_rows, int back_rows);
+int rtkb_joseph_get_band_rows(int * forward_rows, int * back_rows);
 
 /* ---- projection weighting and ramp filtering ----
  * All take a projection stack description `proj` (slice s = geometry

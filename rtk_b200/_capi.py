@@ -97,6 +97,8 @@ SIGNATURES = {
     "rtkb_probe_smem_gather": (C.c_int, [C.c_int, C.c_int, _V, _V]),
     "rtkb_backproject_config": (C.c_int, [C.c_int, _I, _I]),
     "rtkb_bp_set_schedule": (C.c_int, [C.c_int, C.c_int]),
+    "rtkb_joseph_set_band_rows": (C.c_int, [C.c_int, C.c_int]),
+    "rtkb_joseph_get_band_rows": (C.c_int, [_I, _I]),
     "rtkb_joseph_forward_project": (C.c_int, [_G, _IM, _IM, _V, _V, _V, _V]),
     "rtkb_joseph_back_project": (C.c_int, [_G, _IM, _IM, _V, _V, _V, _V]),
     "rtkb_fdk_weight": (C.c_int, [_G, _IM, _V, _V, _V]),

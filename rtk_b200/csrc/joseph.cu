@@ -8,8 +8,9 @@
 // use fixed-step trilinear texture sampling instead of Joseph's scheme.
 //
 // One thread per detector pixel.  Both projectors' grids run every
-// projection of a band of 8 detector rows before the next band (blockIdx.y =
-// projection, blockIdx.z = row band): detector rows run along the volume's y
+// projection of a band of detector rows (8 by default, tunable) before the
+// next band (blockIdx.y = projection, blockIdx.z = row band): detector rows
+// run along the volume's y
 // axis, so the blocks in flight touch one y-slab of the volume, which stays
 // in L2 across projections (the quad copies and quad accumulators are 4x the
 // volume).  The ray set-up
@@ -262,10 +263,11 @@ template <typename Off, typename TP, bool kQuads>
 __global__ void __launch_bounds__(256, 4)
 joseph_forward_kernel(JosephArgs a, const float * __restrict__ V, const float * __restrict__ Vt,
                       const float4 * __restrict__ QN, const float4 * __restrict__ QT, const TP * pin, TP * pout,
-                      const float * __restrict__ weights)
+                      const float * __restrict__ weights, int rb)
 {
-  const int u = blockIdx.x * 32 + (threadIdx.x & 31);
-  const int v = blockIdx.z * 8 + (threadIdx.x >> 5);
+  const int nub = (a.nu + 31) / 32;
+  const int u = (int)(blockIdx.x % nub) * 32 + (threadIdx.x & 31);
+  const int v = ((int)blockIdx.z * rb + (int)(blockIdx.x / nub)) * 8 + (threadIdx.x >> 5);
   const int s = blockIdx.y;
   if (u >= a.nu || v >= a.nv)
     return;
@@ -389,10 +391,12 @@ red_add4(float4 * p, float4 v)
 // registers (4 CTAs per SM) keep more reductions in flight.
 template <typename Off, typename TP>
 __global__ void __launch_bounds__(256, 4)
-joseph_back_kernel(JosephArgs a, const TP * __restrict__ proj, float * A, float * At, float4 * QAN, float4 * QAT)
+joseph_back_kernel(JosephArgs a, const TP * __restrict__ proj, float * A, float * At, float4 * QAN, float4 * QAT,
+                   int rb)
 {
-  const int u = blockIdx.x * 32 + (threadIdx.x & 31);
-  const int v = blockIdx.z * 8 + (threadIdx.x >> 5);
+  const int nub = (a.nu + 31) / 32;
+  const int u = (int)(blockIdx.x % nub) * 32 + (threadIdx.x & 31);
+  const int v = ((int)blockIdx.z * rb + (int)(blockIdx.x / nub)) * 8 + (threadIdx.x >> 5);
   const int s = blockIdx.y;
   if (u >= a.nu || v >= a.nv)
     return;
@@ -728,6 +732,22 @@ widen_kernel(const __nv_bfloat16 * __restrict__ in, float * __restrict__ out, lo
 // the four-tap loop directly.
 constexpr int kQuadMinProjections = 4;
 
+// Detector rows per band of the projectors' grids (rtkb_joseph_set_band_rows):
+// [0] forward, [1] back; multiples of 8 (one CTA covers 32 x 8 pixels).
+int g_joseph_band_rows[2] = { 8, 8 };
+
+// Grid of one projector launch: x = the band's 32 x 8-pixel blocks (detector
+// columns fastest), y = projection, z = band, so every projection of a band
+// runs before the next band.
+dim3
+band_grid(const JosephArgs & a, int rb)
+{
+  const unsigned nub = (unsigned)((a.nu + 31) / 32);
+  const unsigned nrb = (unsigned)((a.nv + 7) / 8);
+  const unsigned rbu = (unsigned)std::max(1, std::min(rb, (int)nrb));
+  return dim3(nub * rbu, (unsigned)a.np, (nrb + rbu - 1) / rbu);
+}
+
 template <typename TP>
 cudaError_t
 forward_launch(const JosephArgs & a, const float * V, float * Vt, float4 * QN, float4 * QT, const TP * pin, TP * pout,
@@ -745,16 +765,17 @@ forward_launch(const JosephArgs & a, const float * V, float * Vt, float4 * QN, f
     quad_kernel<<<qn, 128, 0, st>>>(V, QN, nx, ny, nz, true);  // a = x, b = y
     quad_kernel<<<qt, 128, 0, st>>>(Vt, QT, nz, ny, nx, false); // a = y, b = z
   }
-  const dim3 grid((unsigned)((a.nu + 31) / 32), (unsigned)a.np, (unsigned)((a.nv + 7) / 8));
+  const int  rb = g_joseph_band_rows[0] / 8;
+  const dim3 grid(band_grid(a, rb));
   const bool small = nvox < (1ll << 31);
   if (quads && small)
-    joseph_forward_kernel<int, TP, true><<<grid, 256, 0, st>>>(a, V, Vt, QN, QT, pin, pout, w);
+    joseph_forward_kernel<int, TP, true><<<grid, 256, 0, st>>>(a, V, Vt, QN, QT, pin, pout, w, rb);
   else if (quads)
-    joseph_forward_kernel<long long, TP, true><<<grid, 256, 0, st>>>(a, V, Vt, QN, QT, pin, pout, w);
+    joseph_forward_kernel<long long, TP, true><<<grid, 256, 0, st>>>(a, V, Vt, QN, QT, pin, pout, w, rb);
   else if (small)
-    joseph_forward_kernel<int, TP, false><<<grid, 256, 0, st>>>(a, V, Vt, QN, QT, pin, pout, w);
+    joseph_forward_kernel<int, TP, false><<<grid, 256, 0, st>>>(a, V, Vt, QN, QT, pin, pout, w, rb);
   else
-    joseph_forward_kernel<long long, TP, false><<<grid, 256, 0, st>>>(a, V, Vt, QN, QT, pin, pout, w);
+    joseph_forward_kernel<long long, TP, false><<<grid, 256, 0, st>>>(a, V, Vt, QN, QT, pin, pout, w, rb);
   return cudaGetLastError();
 }
 
@@ -774,11 +795,12 @@ back_launch(const JosephArgs & a, const TP * proj, void * scratch, const TV * vi
   cudaError_t     e = cudaMemsetAsync(scratch, 0, joseph_back_scratch_bytes(nvox), st);
   if (e != cudaSuccess)
     return e;
-  const dim3 grid((unsigned)((a.nu + 31) / 32), (unsigned)a.np, (unsigned)((a.nv + 7) / 8));
+  const int  rb = g_joseph_band_rows[1] / 8;
+  const dim3 grid(band_grid(a, rb));
   if (nvox < (1ll << 31))
-    joseph_back_kernel<int, TP><<<grid, 256, 0, st>>>(a, proj, A, At, QAN, QAT);
+    joseph_back_kernel<int, TP><<<grid, 256, 0, st>>>(a, proj, A, At, QAN, QAT, rb);
   else
-    joseph_back_kernel<long long, TP><<<grid, 256, 0, st>>>(a, proj, A, At, QAN, QAT);
+    joseph_back_kernel<long long, TP><<<grid, 256, 0, st>>>(a, proj, A, At, QAN, QAT, rb);
   const dim3 tg((unsigned)(((nx + 31) / 32) * ((nz + 31) / 32)), (unsigned)ny);
   fold_transposed_kernel<TV, TX><<<tg, 256, 0, st>>>(vin, A, At, QAN, QAT, vout, nx, ny, nz, x, tau);
   return cudaGetLastError();
@@ -995,4 +1017,25 @@ rtkb_joseph_sample_count(const rtkb_geometry * g, const rtkb_image_desc * vol, c
   {
     return fail(RTKB_ERR_OUT_OF_MEMORY, "host allocation failed");
   }
+}
+
+extern "C" int
+rtkb_joseph_set_band_rows(int forward_rows, int back_rows)
+{
+  auto ok = [](int r) { return r == 8 || r == 16 || r == 32 || r == 64; };
+  if (!ok(forward_rows) || !ok(back_rows))
+    return rtkb::fail(RTKB_ERR_INVALID_ARGUMENT, "band rows must be 8, 16, 32 or 64");
+  rtkb::g_joseph_band_rows[0] = forward_rows;
+  rtkb::g_joseph_band_rows[1] = back_rows;
+  return RTKB_OK;
+}
+
+extern "C" int
+rtkb_joseph_get_band_rows(int * forward_rows, int * back_rows)
+{
+  if (forward_rows)
+    *forward_rows = rtkb::g_joseph_band_rows[0];
+  if (back_rows)
+    *back_rows = rtkb::g_joseph_band_rows[1];
+  return RTKB_OK;
 }

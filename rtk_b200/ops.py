@@ -796,6 +796,79 @@ def backproject_autotune(problems, fdk=True, repeats=2, stream=None, cache=None)
     return result
 
 
+JOSEPH_BAND_ROWS = (8, 16, 32, 64)
+
+
+def joseph_band_rows(forward=None, back=None):
+    """Current detector rows per band of the Joseph projectors' grids; sets
+    them first when given (rtkb_joseph_set_band_rows)."""
+    f, b = C.c_int(), C.c_int()
+    check(load().rtkb_joseph_get_band_rows(C.byref(f), C.byref(b)))
+    if forward is not None or back is not None:
+        f.value, b.value = forward or f.value, back or b.value
+        check(load().rtkb_joseph_set_band_rows(f.value, b.value))
+    return f.value, b.value
+
+
+def joseph_autotune(geometry, vol_desc, proj_desc, vol, proj, repeats=2, stream=None, cache=None, apply=True):
+    """Autotuner of the Joseph pair's band height: times the forward projection
+    of `vol` and the back projection of `proj` (neither is modified; outputs go
+    to scratch tensors) for every band of JOSEPH_BAND_ROWS with CUDA events,
+    and returns {"forward": rows, "back": rows, "forward_ms": [...],
+    "back_ms": [...]}, applied with rtkb_joseph_set_band_rows unless
+    apply=False.  cache: JSON file keyed by kernel, device and sizes, as for
+    backproject_autotune."""
+    torch = _torch()
+    key = None
+    if cache is not None:
+        shapes = [tuple(int(v) for v in vol_desc.size), tuple(int(v) for v in proj_desc.size)]
+        key = json.dumps({"kernel": "joseph_pair", "device": torch.cuda.get_device_name(), "problems": [shapes]},
+                         sort_keys=True)
+        hit = _cache_get(cache, key)
+        if hit is not None:
+            if apply:
+                joseph_band_rows(hit["forward"], hit["back"])
+            return hit
+    saved = joseph_band_rows()
+    st = stream if stream is not None else torch.cuda.current_stream()
+    pout = torch.empty_like(proj)
+    pzero = torch.zeros_like(proj)
+    vout = torch.empty_like(vol)
+    vzero = torch.zeros_like(vol)
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        best = None
+        for _ in range(max(1, repeats)):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            fn()
+            e1.record(st)
+            torch.cuda.synchronize()
+            t = e0.elapsed_time(e1)
+            best = t if best is None else min(best, t)
+        return best
+
+    fwd_ms, back_ms = [], []
+    try:
+        for rows in JOSEPH_BAND_ROWS:
+            joseph_band_rows(rows, rows)
+            fwd_ms.append(timed(lambda: joseph_forward_project(geometry, vol_desc, proj_desc, vol, pzero, out=pout,
+                                                               stream=st)))
+            back_ms.append(timed(lambda: joseph_back_project(geometry, vol_desc, proj_desc, proj, vzero, out=vout,
+                                                             stream=st)))
+    finally:
+        joseph_band_rows(*saved)
+    res = {"forward": JOSEPH_BAND_ROWS[fwd_ms.index(min(fwd_ms))], "back": JOSEPH_BAND_ROWS[back_ms.index(min(back_ms))],
+           "forward_ms": fwd_ms, "back_ms": back_ms}
+    if apply:
+        joseph_band_rows(res["forward"], res["back"])
+    if cache is not None:
+        _cache_put(cache, key, res)
+    return res
+
+
 class BackprojectionBatch:
     """Prepared batch (rtkb_bp_batch_*): host work done once, each execute()
     is one persistent launch over all problems.  The tensors of `problems`

@@ -133,3 +133,41 @@ def test_joseph_forward_short_stack_without_quads(rtkb, oracle):
     got = to_np(rtkb.ops.joseph_forward_project(gl, vd, pd, to_gpu(vol), to_gpu(pr)))
     assert rtkb.ops.device_status() == 0
     assert rel_l2(got, ref) < REL_L2_TOL, rel_l2(got, ref)
+
+
+def test_joseph_band_rows_and_autotune(rtkb, oracle, tmp_path):
+    """Bands of 16, 32 and 64 detector rows regroup the projectors' blocks
+    only: the forward projection is bit-identical to 8-row bands (each ray is
+    one thread), the back projection equal up to the FP32 order of its
+    reductions, both within the oracle's tolerance on a ragged detector
+    (rows not a multiple of the band); the autotuner restores the setting it
+    found when apply=False and caches its result."""
+    import torch
+
+    gl, go, vd, vo, pd, po, vol, pr = _case(rtkb, oracle, GEOMS["offsets_tilts"](30), (40, 36, 44), (4.0, 4.5, 3.5),
+                                            (72, 100, 30), (5.0, 5.0, 1.0), vindex=(2, -3, 1), pindex=(-4, 3, 0))
+    dv, dp = to_gpu(vol), to_gpu(pr)
+    zp, zv = torch.zeros(pr.shape, device="cuda"), torch.zeros(vol.shape, device="cuda")
+    out = {}
+    try:
+        for rows in (8, 16, 32, 64):
+            assert rtkb.ops.joseph_band_rows(rows, rows) == (rows, rows)
+            out[rows] = (to_np(rtkb.ops.joseph_forward_project(gl, vd, pd, dv, zp)),
+                         to_np(rtkb.ops.joseph_back_project(gl, vd, pd, dp, zv)))
+    finally:
+        rtkb.ops.joseph_band_rows(8, 8)
+    for rows in (16, 32, 64):
+        assert np.array_equal(out[rows][0], out[8][0])
+        assert rel_l2(out[rows][1], out[8][1]) < 1e-6
+    assert rel_l2(out[64][0], oracle.joseph_forward(go, vo, vol, po)) < REL_L2_TOL
+    assert rel_l2(out[64][1], oracle.joseph_back(go, vo, po, pr)) < REL_L2_TOL
+    with pytest.raises(rtkb.RtkbError):
+        rtkb.ops.joseph_band_rows(12, 8)
+    path = str(tmp_path / "tune.json")
+    res = rtkb.ops.joseph_autotune(gl, vd, pd, dv, dp, repeats=1, cache=path, apply=False)
+    assert res["forward"] in (8, 16, 32, 64) and res["back"] in (8, 16, 32, 64)
+    assert len(res["forward_ms"]) == 4 and len(res["back_ms"]) == 4
+    assert rtkb.ops.joseph_band_rows() == (8, 8)
+    assert rtkb.ops.joseph_autotune(gl, vd, pd, dv, dp, cache=path, apply=False) == res
+    assert np.array_equal(to_np(dv), vol.astype(np.float32)) and np.array_equal(to_np(dp), pr.astype(np.float32))
+    assert rtkb.ops.device_status() == 0

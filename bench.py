@@ -453,8 +453,8 @@ def c4_leg(torch, rtkb, stream, n=64, niter=10):
     64^3-256^3, 90-360 projections, detectors 128^2-512^2, SID 800-1200 mm) of
     random-ellipsoid phantoms, each reconstructed by FDK (weights + Hann ramp,
     then backprojection) followed by niter CG iterations (Joseph pair) started
-    from the FDK volume.  Batched: the preprocessing of every stack in stream
-    order, every backprojection in one persistent launch (autotuned
+    from the FDK volume.  Batched: the preprocessing of every stack in one
+    launch per padded row length, every backprojection in one persistent launch (autotuned
     configuration), every problem's CG start and iterations in one CUDA graph
     launch (a branch per problem).  Against the same work problem after problem
     (the same CG plans, one after another).  Plans and the backprojection batch
@@ -504,9 +504,10 @@ def c4_leg(torch, rtkb, stream, n=64, niter=10):
     lib = rtkb.load()
     plans = [lib.rtkb_cg_batch_plan(cgb._h, i) for i in range(n)]
 
+    pre_batch = [(P["g"], P["pd"], P["p"], P["f"]) for P in probs]
+
     def batched():
-        for P in probs:
-            preprocess(P)
+        rtkb.ops.fdk_preprocess_batch(pre_batch, ramp, stream=stream)
         bpb.execute(stream)
         cgb.start(stream)
         cgb.iterate(niter, stream)
@@ -573,8 +574,8 @@ def c4_leg(torch, rtkb, stream, n=64, niter=10):
             "autotuned_config": best, "joseph_band_rows": {"forward": bands["forward"], "back": bands["back"]},
             "fdk_oracle_rel_l2": errs,
             f"cg_{niter}_iterations_oracle_rel_l2": cg_errs,
-            "launches_batched": "preprocessing per problem, one persistent backprojection launch, one CUDA graph "
-                                "launch for every problem's CG start and iterations"}
+            "launches_batched": "one preprocessing launch per padded row length, one persistent backprojection "
+                                "launch, one CUDA graph launch for every problem's CG start and iterations"}
 
 def sart_leg(torch, rtkb, stream, niter=1):
     """SART (RTK's defaults: lambda 0.3, one projection per subset, Joseph

@@ -685,6 +685,23 @@ typedef struct rtkb_fdk_preprocess_params
 } rtkb_fdk_preprocess_params;
 int rtkb_fdk_preprocess(const rtkb_geometry * g, const rtkb_image_desc * proj, const rtkb_fdk_preprocess_params * p,
                         rtkb_image_desc * out, const float * d_in, float * d_out, void * stream);
+/* Batched preprocessing (no counterpart in the reference): rtkb_fdk_preprocess
+ * of many independent stacks (own geometry, description and buffers each)
+ * with the same parameters, in one launch per padded row length: the ramp
+ * kernel's CTAs take row pairs of every stack of that length.  Each problem's
+ * output description is written to its `out`.  Results are those of one
+ * rtkb_fdk_preprocess call per stack, bit for bit.  Nothing is launched unless
+ * every problem is valid. */
+typedef struct rtkb_fdk_preprocess_problem
+{
+  const rtkb_geometry * geometry;
+  rtkb_image_desc       proj;
+  const float *         d_in;
+  float *               d_out;
+  rtkb_image_desc       out; /* written */
+} rtkb_fdk_preprocess_problem;
+int rtkb_fdk_preprocess_batch(rtkb_fdk_preprocess_problem * problems, int n, const rtkb_fdk_preprocess_params * p,
+                              void * stream);
 /* rtk::IterativeFDKConeBeamReconstructionFilter
  * (include/rtkIterativeFDKConeBeamReconstructionFilter.hxx:171-218): d_x (x0 in,
  * result out) += FDK(p), then niter - 1 times += FDK(lambda (p - JosephFP(x)) /

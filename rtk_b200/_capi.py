@@ -48,6 +48,13 @@ class RampParams(C.Structure):
     ]
 
 
+class FdkPreprocessProblem(C.Structure):
+    """rtkb_fdk_preprocess_problem."""
+
+    _fields_ = [("geometry", C.c_void_p), ("proj", ImageDesc), ("d_in", C.c_void_p), ("d_out", C.c_void_p),
+                ("out", ImageDesc)]
+
+
 class FdkPreprocessParams(C.Structure):
     """rtkb_fdk_preprocess_params."""
 
@@ -108,6 +115,8 @@ SIGNATURES = {
     "rtkb_ramp_kernel": (C.c_int, [C.c_int, C.c_double, C.POINTER(RampParams), _I, _D]),
     "rtkb_ramp_filter": (C.c_int, [_IM, C.POINTER(RampParams), _V, _V, _V]),
     "rtkb_fdk_preprocess": (C.c_int, [_G, _IM, C.POINTER(FdkPreprocessParams), _IM, _V, _V, _V]),
+    "rtkb_fdk_preprocess_batch": (C.c_int, [C.POINTER(FdkPreprocessProblem), C.c_int, C.POINTER(FdkPreprocessParams),
+                                            _V]),
 }
 
 _lib = None

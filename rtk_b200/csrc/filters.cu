@@ -21,6 +21,7 @@
 // weights from FP64 host tables; the stack is read once and written once.
 #include "rtkb_filters.h"
 
+#include <algorithm>
 #include <cstring>
 
 namespace
@@ -305,33 +306,40 @@ fft_chain(float2 * src, float2 * dst, const float2 * tw)
   }
 }
 
-// Ramp filter of the stack, persistent: each CTA loads the pass twiddles and
-// the ramp kernel into shared memory once, then filters row pairs (two real
-// rows as one complex sequence) until the stack is done.
+// Ramp filter of one or more stacks, persistent: each CTA loads the pass
+// twiddles (shared by every stack of padded length N) into shared memory once
+// and the ramp kernel of the stack it is working on whenever that changes,
+// then filters row pairs (two real rows as one complex sequence) until every
+// stack is done.  probs[q] describes stack q, whose row pairs are the global
+// pair indices [pair_begin[q], pair_begin[q + 1]); a CTA's pairs increase, so
+// it finds each pair's stack by walking forward from the previous one.
 // 128 registers per thread at most: (threads x 128) x (512 / threads) = 64 K
 template <int N>
 __global__ void __launch_bounds__(N / 16 > 64 ? N / 16 : 64, 512 / (N / 16 > 64 ? N / 16 : 64))
-ramp_fft_kernel(FilterArgs a, int tw_len)
+ramp_fft_kernel(const FilterArgs * __restrict__ probs, const long long * __restrict__ pair_begin,
+                long long total, const float2 * __restrict__ tw, int tw_len)
 {
   constexpr int T = N / 16 > 64 ? N / 16 : 64; // threads; 16 columns per thread cover the row
   constexpr int P = pidx(N);
   extern __shared__ float2 sbuf[];
-  const int nu = a.nu_out;
   float2 *  b0 = sbuf;
   float2 *  b1 = sbuf + P;
   float2 *  tws = sbuf + 2 * P;
   float *   Ks = reinterpret_cast<float *>(tws + tw_len);
   for (int i = threadIdx.x; i < tw_len; i += blockDim.x)
-    tws[i] = a.tw[i];
-  for (int i = threadIdx.x; i <= N / 2; i += blockDim.x)
-    Ks[i] = a.K[i];
-  const long long rows = (long long)a.nv * a.np, pairs = (rows + 1) / 2;
-  const float     inv = 1.f / (float)N;
+    tws[i] = tw[i];
+  const float inv = 1.f / (float)N;
+  auto        locate = [&](long long pr, int q) {
+    while (pr >= pair_begin[q + 1])
+      q++;
+    return q;
+  };
   // the next pair's raw pixels are prefetched into registers while the
   // current pair is transformed (columns threadIdx.x + i * blockDim.x;
   // blockDim.x >= N / 16, so 16 columns per thread cover the row)
   float pa[16], pb[16];
-  auto  prefetch = [&](long long pr) {
+  auto  prefetch = [&](const FilterArgs & a, long long pr) {
+    const long long rows = (long long)a.nv * a.np;
     const long long ra = 2 * pr, rb = ra + 1;
     const int       sa = (int)(ra / a.nv), rra = (int)(ra % a.nv);
     const bool      hb = rb < rows;
@@ -340,21 +348,36 @@ ramp_fft_kernel(FilterArgs a, int tw_len)
     for (int i = 0; i < 16; i++)
     {
       const int c = threadIdx.x + i * T;
-      pa[i] = (c < nu) ? raw_pixel(a, sa, rra, c) : 0.f;
-      pb[i] = (c < nu && hb) ? raw_pixel(a, sb, rrb, c) : 0.f;
+      pa[i] = (c < a.nu_out) ? raw_pixel(a, sa, rra, c) : 0.f;
+      pb[i] = (c < a.nu_out && hb) ? raw_pixel(a, sb, rrb, c) : 0.f;
     }
   };
-  if (blockIdx.x < pairs)
-    prefetch(blockIdx.x);
-  for (long long pr = blockIdx.x; pr < pairs; pr += gridDim.x)
+  int q = 0, kq = -1;
+  if (blockIdx.x < total)
   {
-    const long long ra = 2 * pr, rb = ra + 1;
-    const bool      hb = rb < rows;
-    const int       sa = (int)(ra / a.nv), rra = (int)(ra % a.nv);
-    const int       sb = hb ? (int)(rb / a.nv) : sa, rrb = hb ? (int)(rb % a.nv) : rra;
-    const RowWeight wa = row_weight(a, sa, rra);
-    const RowWeight wb = row_weight(a, sb, rrb);
+    q = locate(blockIdx.x, 0);
+    prefetch(probs[q], blockIdx.x - pair_begin[q]);
+  }
+  for (long long gpr = blockIdx.x; gpr < total; gpr += gridDim.x)
+  {
+    q = locate(gpr, q);
+    const FilterArgs & a = probs[q];
+    const long long    pr = gpr - pair_begin[q];
+    const int          nu = a.nu_out;
+    const long long    rows = (long long)a.nv * a.np;
+    const long long    ra = 2 * pr, rb = ra + 1;
+    const bool         hb = rb < rows;
+    const int          sa = (int)(ra / a.nv), rra = (int)(ra % a.nv);
+    const int          sb = hb ? (int)(rb / a.nv) : sa, rrb = hb ? (int)(rb % a.nv) : rra;
+    const RowWeight    wa = row_weight(a, sa, rra);
+    const RowWeight    wb = row_weight(a, sb, rrb);
     __syncthreads(); // the previous pair's results have been stored
+    if (q != kq)
+    {
+      for (int i = threadIdx.x; i <= N / 2; i += blockDim.x)
+        Ks[i] = a.K[i];
+      kq = q; // read after the barriers below, before the multiplication
+    }
 #pragma unroll
     for (int i = 0; i < 16; i++)
     {
@@ -366,8 +389,11 @@ ramp_fft_kernel(FilterArgs a, int tw_len)
         b0[pidx(c)] = make_float2(x, y);
       }
     }
-    if (pr + gridDim.x < pairs)
-      prefetch(pr + gridDim.x);
+    if (gpr + gridDim.x < total)
+    {
+      const int qn = locate(gpr + gridDim.x, q);
+      prefetch(probs[qn], gpr + gridDim.x - pair_begin[qn]);
+    }
     __syncthreads();
     if (a.next > 0)
     {
@@ -433,7 +459,8 @@ pass_twiddles(int N, std::vector<float> & tw)
 
 template <int N>
 static cudaError_t
-launch_ramp(const FilterArgs & a, int tw_len, long long pairs, cudaStream_t st)
+launch_ramp(const FilterArgs * d_probs, const long long * d_begin, long long pairs, const float2 * d_tw, int tw_len,
+            cudaStream_t st)
 {
   constexpr int threads = N / 16 > 64 ? N / 16 : 64;
   const size_t  smem = (2 * (size_t)pidx(N) + tw_len) * sizeof(float2) + ((size_t)N / 2 + 1) * sizeof(float);
@@ -448,10 +475,32 @@ launch_ramp(const FilterArgs & a, int tw_len, long long pairs, cudaStream_t st)
   if (e == cudaSuccess && pairs > 0)
   {
     const long long grid = std::min<long long>(pairs, (long long)sms * std::max(per_sm, 1));
-    ramp_fft_kernel<N><<<(unsigned)grid, threads, smem, st>>>(a, tw_len);
+    ramp_fft_kernel<N><<<(unsigned)grid, threads, smem, st>>>(d_probs, d_begin, pairs, d_tw, tw_len);
     e = cudaGetLastError();
   }
   return e;
+}
+
+static cudaError_t
+launch_ramp_n(int N, const FilterArgs * d_probs, const long long * d_begin, long long pairs, const float2 * d_tw,
+              int tw_len, cudaStream_t st)
+{
+  switch (N)
+  {
+    case 2: return launch_ramp<2>(d_probs, d_begin, pairs, d_tw, tw_len, st);
+    case 4: return launch_ramp<4>(d_probs, d_begin, pairs, d_tw, tw_len, st);
+    case 8: return launch_ramp<8>(d_probs, d_begin, pairs, d_tw, tw_len, st);
+    case 16: return launch_ramp<16>(d_probs, d_begin, pairs, d_tw, tw_len, st);
+    case 32: return launch_ramp<32>(d_probs, d_begin, pairs, d_tw, tw_len, st);
+    case 64: return launch_ramp<64>(d_probs, d_begin, pairs, d_tw, tw_len, st);
+    case 128: return launch_ramp<128>(d_probs, d_begin, pairs, d_tw, tw_len, st);
+    case 256: return launch_ramp<256>(d_probs, d_begin, pairs, d_tw, tw_len, st);
+    case 512: return launch_ramp<512>(d_probs, d_begin, pairs, d_tw, tw_len, st);
+    case 1024: return launch_ramp<1024>(d_probs, d_begin, pairs, d_tw, tw_len, st);
+    case 2048: return launch_ramp<2048>(d_probs, d_begin, pairs, d_tw, tw_len, st);
+    case 4096: return launch_ramp<4096>(d_probs, d_begin, pairs, d_tw, tw_len, st);
+    default: return launch_ramp<8192>(d_probs, d_begin, pairs, d_tw, tw_len, st);
+  }
 }
 
 struct Options
@@ -472,9 +521,24 @@ append(std::vector<unsigned char> & blob, const std::vector<T> & v)
   return off;
 }
 
+// Host half of the weighting and ramp filters of one stack: argument checks,
+// the output region, the FP64 weight tables, the ramp kernel, the twiddles and
+// the truncation weights, gathered into P.blob for one upload; P.a holds the
+// sizes and, after bind_filters, the device pointers.
+struct Prepared
+{
+  FilterArgs                 a{};
+  std::vector<unsigned char> blob;
+  size_t                     o_fdk = 0, o_colw = 0, o_K = 0, o_tw = 0, o_mw = 0;
+  bool                       h_fdk = false, h_colw = false, h_K = false, h_tw = false, h_mw = false;
+  int                        tw_len = 0;
+  long long                  pairs = 0;
+  bool                       ramp = false;
+};
+
 int
-run_filters(const rtkb_geometry * g, const rtkb_image_desc * in, const Options & o, rtkb_image_desc * out_desc,
-            const float * d_in, float * d_out, cudaStream_t st, int * is_short)
+prepare_filters(const rtkb_geometry * g, const rtkb_image_desc * in, const Options & o, rtkb_image_desc * out_desc,
+                const float * d_in, float * d_out, int * is_short, Prepared & P)
 {
   using namespace rtkb;
   std::string why;
@@ -564,73 +628,84 @@ run_filters(const rtkb_geometry * g, const rtkb_image_desc * in, const Options &
     a.N = N;
     a.next = next;
   }
-  std::vector<unsigned char> blob;
-  const size_t               o_fdk = append(blob, fdkp), o_colw = append(blob, colw), o_K = append(blob, K),
-               o_tw = append(blob, tw), o_mw = append(blob, mw);
-  void * scratch = nullptr;
-  if (!blob.empty())
-    RTKB_CUDA_TRY(rtkb::scratch_malloc(&scratch, blob.size(), st));
-  int rc = RTKB_OK;
-  do
+  P.blob.clear();
+  P.o_fdk = append(P.blob, fdkp);
+  P.o_colw = append(P.blob, colw);
+  P.o_K = append(P.blob, K);
+  P.o_tw = append(P.blob, tw);
+  P.o_mw = append(P.blob, mw);
+  P.h_fdk = !fdkp.empty();
+  P.h_colw = !colw.empty();
+  P.h_K = !K.empty();
+  P.h_tw = !tw.empty();
+  P.h_mw = !mw.empty();
+  P.tw_len = (int)(tw.size() / 2);
+  P.pairs = ((long long)nv * np + 1) / 2;
+  P.ramp = o.ramp;
+  a.in = d_in;
+  a.out = d_out;
+  P.a = a;
+  return RTKB_OK;
+}
+
+// Points P.a's tables at the device copy of P.blob that starts at base.
+void
+bind_filters(Prepared & P, char * base)
+{
+  P.a.fdkp = P.h_fdk ? reinterpret_cast<const double *>(base + P.o_fdk) : nullptr;
+  P.a.colw = P.h_colw ? reinterpret_cast<const float *>(base + P.o_colw) : nullptr;
+  P.a.K = P.h_K ? reinterpret_cast<const float *>(base + P.o_K) : nullptr;
+  P.a.tw = P.h_tw ? reinterpret_cast<const float2 *>(base + P.o_tw) : nullptr;
+  P.a.mw = P.h_mw ? reinterpret_cast<const float *>(base + P.o_mw) : nullptr;
+}
+
+size_t
+align256(size_t x)
+{
+  return (x + 255) & ~size_t(255);
+}
+
+int
+run_filters(const rtkb_geometry * g, const rtkb_image_desc * in, const Options & o, rtkb_image_desc * out_desc,
+            const float * d_in, float * d_out, cudaStream_t st, int * is_short)
+{
+  using namespace rtkb;
+  Prepared P;
+  int      rc = prepare_filters(g, in, o, out_desc, d_in, d_out, is_short, P);
+  if (rc != RTKB_OK)
+    return rc;
+  // one upload: the tables, then (ramp) the problem table and its pair range
+  const size_t o_args = align256(P.blob.size()), o_begin = align256(o_args + sizeof(FilterArgs));
+  const size_t bytes = o_begin + 2 * sizeof(long long);
+  void *       scratch = nullptr;
+  RTKB_CUDA_TRY(rtkb::scratch_malloc(&scratch, bytes, st));
+  char * base = static_cast<char *>(scratch);
+  bind_filters(P, base);
+  P.blob.resize(bytes, 0);
+  std::memcpy(P.blob.data() + o_args, &P.a, sizeof(FilterArgs));
+  const long long begin[2] = { 0, P.pairs };
+  std::memcpy(P.blob.data() + o_begin, begin, sizeof(begin));
+  cudaError_t e = cudaMemcpyAsync(scratch, P.blob.data(), bytes, cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess)
+    rc = cuda_fail(e, "cudaMemcpyAsync");
+  else if (P.ramp)
   {
-    if (scratch)
-    {
-      cudaError_t e = cudaMemcpyAsync(scratch, blob.data(), blob.size(), cudaMemcpyHostToDevice, st);
-      if (e != cudaSuccess)
-      {
-        rc = cuda_fail(e, "cudaMemcpyAsync");
-        break;
-      }
-    }
-    auto at = [&](size_t off, bool present) -> const void * {
-      return present ? static_cast<const void *>(static_cast<char *>(scratch) + off) : nullptr;
-    };
-    a.in = d_in;
-    a.out = d_out;
-    a.fdkp = static_cast<const double *>(at(o_fdk, !fdkp.empty()));
-    a.colw = static_cast<const float *>(at(o_colw, !colw.empty()));
-    a.K = static_cast<const float *>(at(o_K, !K.empty()));
-    a.tw = static_cast<const float2 *>(at(o_tw, !tw.empty()));
-    a.mw = static_cast<const float *>(at(o_mw, !mw.empty()));
-    if (o.ramp)
-    {
-      const long long pairs = ((long long)nv * np + 1) / 2;
-      const int    tw_len = (int)(tw.size() / 2);
-      cudaError_t  e = cudaSuccess;
-      switch (a.N)
-      {
-        case 2: e = launch_ramp<2>(a, tw_len, pairs, st); break;
-        case 4: e = launch_ramp<4>(a, tw_len, pairs, st); break;
-        case 8: e = launch_ramp<8>(a, tw_len, pairs, st); break;
-        case 16: e = launch_ramp<16>(a, tw_len, pairs, st); break;
-        case 32: e = launch_ramp<32>(a, tw_len, pairs, st); break;
-        case 64: e = launch_ramp<64>(a, tw_len, pairs, st); break;
-        case 128: e = launch_ramp<128>(a, tw_len, pairs, st); break;
-        case 256: e = launch_ramp<256>(a, tw_len, pairs, st); break;
-        case 512: e = launch_ramp<512>(a, tw_len, pairs, st); break;
-        case 1024: e = launch_ramp<1024>(a, tw_len, pairs, st); break;
-        case 2048: e = launch_ramp<2048>(a, tw_len, pairs, st); break;
-        case 4096: e = launch_ramp<4096>(a, tw_len, pairs, st); break;
-        default: e = launch_ramp<8192>(a, tw_len, pairs, st); break;
-      }
-      if (e != cudaSuccess)
-        rc = cuda_fail(e, "ramp_fft_kernel launch");
-    }
-    else
-    {
-      const dim3 grid((unsigned)((nu_out + 255) / 256), (unsigned)nv, (unsigned)np);
-      weight_kernel<<<grid, 256, 0, st>>>(a);
-      cudaError_t e = cudaGetLastError();
-      if (e != cudaSuccess)
-        rc = cuda_fail(e, "weight_kernel launch");
-    }
-  } while (0);
-  if (scratch)
-  {
-    cudaError_t fe = rtkb::scratch_free(scratch, st);
-    if (rc == RTKB_OK && fe != cudaSuccess)
-      rc = cuda_fail(fe, "cudaFreeAsync");
+    e = launch_ramp_n(P.a.N, reinterpret_cast<const FilterArgs *>(base + o_args),
+                      reinterpret_cast<const long long *>(base + o_begin), P.pairs, P.a.tw, P.tw_len, st);
+    if (e != cudaSuccess)
+      rc = cuda_fail(e, "ramp_fft_kernel launch");
   }
+  else
+  {
+    const dim3 grid((unsigned)((P.a.nu_out + 255) / 256), (unsigned)P.a.nv, (unsigned)P.a.np);
+    weight_kernel<<<grid, 256, 0, st>>>(P.a);
+    e = cudaGetLastError();
+    if (e != cudaSuccess)
+      rc = cuda_fail(e, "weight_kernel launch");
+  }
+  cudaError_t fe = rtkb::scratch_free(scratch, st);
+  if (rc == RTKB_OK && fe != cudaSuccess)
+    rc = cuda_fail(fe, "cudaFreeAsync");
   return rc;
 }
 
@@ -774,5 +849,113 @@ rtkb_fdk_preprocess(const rtkb_geometry * g, const rtkb_image_desc * proj, const
     o.ramp = true;
     o.rp = p->ramp;
     return run_filters(g, proj, o, out, d_in, d_out, static_cast<cudaStream_t>(stream), nullptr);
+  });
+}
+
+extern "C" int
+rtkb_fdk_preprocess_batch(rtkb_fdk_preprocess_problem * problems, int n, const rtkb_fdk_preprocess_params * p,
+                          void * stream)
+{
+  RTKB_TRACE();
+  return guarded([&] {
+    using namespace rtkb;
+    if (!p)
+      return fail(RTKB_ERR_INVALID_ARGUMENT, "null preprocessing parameters");
+    if (n < 0 || (n > 0 && !problems))
+      return fail(RTKB_ERR_INVALID_ARGUMENT, "invalid problem list");
+    Options o;
+    o.displaced = p->displaced_detector != 0;
+    o.pad = p->pad_on_truncated_side != 0;
+    o.parker = p->short_scan != 0;
+    o.threshold = p->angular_gap_threshold > 0. ? p->angular_gap_threshold : 3.14159265358979323846 / 9;
+    o.fdk = true;
+    o.ramp = true;
+    o.rp = p->ramp;
+    // every problem's host half first: nothing is launched unless all are valid
+    std::vector<Prepared> P(n);
+    for (int i = 0; i < n; i++)
+    {
+      const rtkb_fdk_preprocess_problem & q = problems[i];
+      const int rc = prepare_filters(q.geometry, &q.proj, o, &problems[i].out, q.d_in, q.d_out, nullptr, P[i]);
+      if (rc != RTKB_OK)
+        return rc;
+    }
+    if (n == 0)
+      return (int)RTKB_OK;
+    // one device block: every problem's tables, then per padded length N a
+    // problem table and its pair ranges (one launch per N)
+    struct Group
+    {
+      int              N;
+      std::vector<int> idx;
+      size_t           o_args = 0, o_begin = 0;
+      long long        pairs = 0;
+    };
+    std::vector<Group> groups;
+    for (int i = 0; i < n; i++)
+    {
+      auto it = std::find_if(groups.begin(), groups.end(), [&](const Group & gr) { return gr.N == P[i].a.N; });
+      if (it == groups.end())
+      {
+        groups.push_back(Group{ P[i].a.N, {} });
+        it = groups.end() - 1;
+      }
+      it->idx.push_back(i);
+    }
+    std::vector<size_t> offs(n);
+    size_t              off = 0;
+    for (int i = 0; i < n; i++)
+    {
+      offs[i] = off;
+      off = align256(off + P[i].blob.size());
+    }
+    for (Group & gr : groups)
+    {
+      gr.o_args = off;
+      off = align256(off + gr.idx.size() * sizeof(FilterArgs));
+      gr.o_begin = off;
+      off = align256(off + (gr.idx.size() + 1) * sizeof(long long));
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    void *       scratch = nullptr;
+    RTKB_CUDA_TRY(rtkb::scratch_malloc(&scratch, off, st));
+    char *                     base = static_cast<char *>(scratch);
+    std::vector<unsigned char> host(off, 0);
+    for (int i = 0; i < n; i++)
+    {
+      if (!P[i].blob.empty())
+        std::memcpy(host.data() + offs[i], P[i].blob.data(), P[i].blob.size());
+      bind_filters(P[i], base + offs[i]);
+    }
+    for (Group & gr : groups)
+    {
+      long long acc = 0;
+      for (size_t k = 0; k < gr.idx.size(); k++)
+      {
+        std::memcpy(host.data() + gr.o_args + k * sizeof(FilterArgs), &P[gr.idx[k]].a, sizeof(FilterArgs));
+        std::memcpy(host.data() + gr.o_begin + k * sizeof(long long), &acc, sizeof(long long));
+        acc += P[gr.idx[k]].pairs;
+      }
+      std::memcpy(host.data() + gr.o_begin + gr.idx.size() * sizeof(long long), &acc, sizeof(long long));
+      gr.pairs = acc;
+    }
+    int         rc = RTKB_OK;
+    cudaError_t e = cudaMemcpyAsync(scratch, host.data(), off, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess)
+      rc = cuda_fail(e, "cudaMemcpyAsync");
+    for (size_t k = 0; k < groups.size() && rc == RTKB_OK; k++)
+    {
+      const Group &    gr = groups[k];
+      const Prepared & f = P[gr.idx[0]]; // the group's pass twiddles (one set per N)
+      e = launch_ramp_n(gr.N, reinterpret_cast<const FilterArgs *>(base + gr.o_args),
+                        reinterpret_cast<const long long *>(base + gr.o_begin), gr.pairs, f.a.tw, f.tw_len, st);
+      if (e != cudaSuccess)
+        rc = cuda_fail(e, "ramp_fft_kernel launch");
+    }
+    // (a copy from pageable memory returns once its source has been staged)
+    cudaError_t fe = rtkb::scratch_free(scratch, st);
+    if (rc == RTKB_OK && fe != cudaSuccess)
+      rc = cuda_fail(fe, "cudaFreeAsync");
+    return rc;
   });
 }

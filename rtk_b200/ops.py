@@ -216,6 +216,31 @@ def fdk_preprocess(geometry, proj_desc, proj, ramp=None, displaced=False, pad=Tr
     return out, got
 
 
+def fdk_preprocess_batch(problems, ramp=None, displaced=False, pad=True, short_scan=False,
+                         threshold=3.141592653589793 / 9, stream=None):
+    """rtkb_fdk_preprocess_batch: fdk_preprocess of every (geometry,
+    proj_desc, proj, out) in `problems` (out None: allocated) in one launch per
+    padded row length.  Returns [(filtered stack, its description)]."""
+    from ._capi import FdkPreprocessParams, FdkPreprocessProblem
+
+    p = FdkPreprocessParams()
+    p.displaced_detector, p.pad_on_truncated_side, p.short_scan = int(displaced), int(pad), int(short_scan)
+    p.angular_gap_threshold = threshold
+    p.ramp = ramp or ramp_params()
+    arr = (FdkPreprocessProblem * max(1, len(problems)))()
+    outs = []
+    for k, (geometry, proj_desc, proj, out) in enumerate(problems):
+        od = proj_desc
+        if displaced:
+            od, _ = displaced_detector_region(geometry, proj_desc, pad)
+        out = _unary(None, proj_desc, proj, out, shape_of(od))
+        arr[k].geometry, arr[k].proj = geometry.handle, proj_desc
+        arr[k].d_in, arr[k].d_out = _ptr(proj), _ptr(out)
+        outs.append(out)
+    check(load().rtkb_fdk_preprocess_batch(arr, len(problems), C.byref(p), _stream(stream)))
+    return [(o, arr[k].out) for k, o in enumerate(outs)]
+
+
 def trim_memory_pool() -> int:
     """Return the library's unused reserved scratch memory (current device) to
     the driver; returns the bytes still reserved."""

@@ -170,3 +170,42 @@ def test_project_ellipsoids_matches_oracle(rtkb, oracle):
     ref = oracle.project_ellipsoids(go, po, ell)
     got = to_np(rtkb.ops.project_ellipsoids(gl, pd, ell))
     assert rel_l2(got, ref) < 1e-6
+
+
+@pytest.mark.parametrize("displaced", [False, True])
+def test_fdk_preprocess_batch_equals_one_call_per_stack(rtkb, oracle, displaced):
+    """rtkb_fdk_preprocess_batch on stacks of different widths (three padded
+    row lengths, one of them shared by two stacks), projection counts, index
+    offsets and geometries: every output bit-identical to its own
+    rtkb_fdk_preprocess call (the same kernel over a one-stack table), one
+    within the oracle's tolerance; an invalid problem fails the whole call."""
+    rng = np.random.default_rng(21)
+    cases = []
+    for k, (nu, nv, n) in enumerate([(200, 9, 90), (120, 17, 47), (230, 5, 61), (500, 12, 33)]):
+        params = [(900.0 + 50 * k, 1400.0 + 40 * k, i * 360.0 / n, (40.0 if displaced else 0.0) + k, 1.0)
+                  for i in range(n)]
+        gl, go = pair_geometry(rtkb, oracle, params)
+        pd, po = pair_image(rtkb, oracle, (nu, nv, n), (0.8, 0.8, 1.0), index=(-k, k, 0))
+        p = rng.uniform(0, 1, size=oracle.shape_of(po)).astype(np.float32)
+        cases.append((gl, go, pd, po, p))
+    ramp = rtkb.ops.ramp_params(hann=0.7)
+    batch = rtkb.ops.fdk_preprocess_batch([(gl, pd, to_gpu(p), None) for gl, go, pd, po, p in cases], ramp,
+                                          displaced=displaced)
+    for (gl, go, pd, po, p), (got, od) in zip(cases, batch):
+        one, od1 = rtkb.ops.fdk_preprocess(gl, pd, to_gpu(p), ramp, displaced=displaced)
+        assert (od.index[0], od.size[0]) == (od1.index[0], od1.size[0])
+        assert np.array_equal(to_np(got), to_np(one))
+    gl, go, pd, po, p = cases[1]
+    q, qo = p.astype(np.float64), po
+    if displaced:
+        q, i0, s0 = oracle.displaced_detector(go, po, q)
+        qo = oracle.image((s0, po.size[1], po.size[2]), (0.8, 0.8, 1.0), origin=tuple(po.origin),
+                          index=(i0, po.index[1], 0))
+    ref = oracle.ramp_filter(qo, oracle.fdk_weight(go, qo, q), oracle.ramp_params(hann=0.7))
+    assert rel_l2(to_np(batch[1][0]), ref) < REL_L2_TOL
+    bad = rtkb.make_desc((120, 17, 500), (0.8, 0.8, 1.0))  # more projections than the geometry has
+    with pytest.raises(rtkb.RtkbError):
+        rtkb.ops.fdk_preprocess_batch([(cases[0][0], cases[0][2], to_gpu(cases[0][4]), None),
+                                       (cases[1][0], bad, to_gpu(np.zeros((500, 17, 120), np.float32)), None)],
+                                      ramp)
+    assert rtkb.ops.device_status() == 0

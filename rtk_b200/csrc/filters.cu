@@ -352,7 +352,10 @@ ramp_fft_kernel(const FilterArgs * __restrict__ probs, const long long * __restr
       pb[i] = (c < a.nu_out && hb) ? raw_pixel(a, sb, rrb, c) : 0.f;
     }
   };
-  int q = 0, kq = -1;
+  // the current stack's description, in shared memory: read there, its fields
+  // cannot alias the output the loop stores to global memory
+  __shared__ FilterArgs cur;
+  int                   q = 0, kq = -1;
   if (blockIdx.x < total)
   {
     q = locate(blockIdx.x, 0);
@@ -361,7 +364,17 @@ ramp_fft_kernel(const FilterArgs * __restrict__ probs, const long long * __restr
   for (long long gpr = blockIdx.x; gpr < total; gpr += gridDim.x)
   {
     q = locate(gpr, q);
-    const FilterArgs & a = probs[q];
+    __syncthreads(); // the previous pair's results have been stored
+    if (q != kq)
+    {
+      if (threadIdx.x == 0)
+        cur = probs[q];
+      for (int i = threadIdx.x; i <= N / 2; i += blockDim.x)
+        Ks[i] = probs[q].K[i];
+      kq = q;
+      __syncthreads();
+    }
+    const FilterArgs & a = cur;
     const long long    pr = gpr - pair_begin[q];
     const int          nu = a.nu_out;
     const long long    rows = (long long)a.nv * a.np;
@@ -371,13 +384,6 @@ ramp_fft_kernel(const FilterArgs * __restrict__ probs, const long long * __restr
     const int          sb = hb ? (int)(rb / a.nv) : sa, rrb = hb ? (int)(rb % a.nv) : rra;
     const RowWeight    wa = row_weight(a, sa, rra);
     const RowWeight    wb = row_weight(a, sb, rrb);
-    __syncthreads(); // the previous pair's results have been stored
-    if (q != kq)
-    {
-      for (int i = threadIdx.x; i <= N / 2; i += blockDim.x)
-        Ks[i] = a.K[i];
-      kq = q; // read after the barriers below, before the multiplication
-    }
 #pragma unroll
     for (int i = 0; i < 16; i++)
     {
@@ -392,7 +398,10 @@ ramp_fft_kernel(const FilterArgs * __restrict__ probs, const long long * __restr
     if (gpr + gridDim.x < total)
     {
       const int qn = locate(gpr + gridDim.x, q);
-      prefetch(probs[qn], gpr + gridDim.x - pair_begin[qn]);
+      if (qn == q)
+        prefetch(a, gpr + gridDim.x - pair_begin[qn]);
+      else
+        prefetch(probs[qn], gpr + gridDim.x - pair_begin[qn]);
     }
     __syncthreads();
     if (a.next > 0)

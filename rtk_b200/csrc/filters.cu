@@ -306,40 +306,27 @@ fft_chain(float2 * src, float2 * dst, const float2 * tw)
   }
 }
 
-// Ramp filter of one or more stacks, persistent: each CTA loads the pass
-// twiddles (shared by every stack of padded length N) into shared memory once
-// and the ramp kernel of the stack it is working on whenever that changes,
-// then filters row pairs (two real rows as one complex sequence) until every
-// stack is done.  probs[q] describes stack q, whose row pairs are the global
-// pair indices [pair_begin[q], pair_begin[q + 1]); a CTA's pairs increase, so
-// it finds each pair's stack by walking forward from the previous one.
-// 128 registers per thread at most: (threads x 128) x (512 / threads) = 64 K
+// Threads of the ramp kernels: 16 columns per thread cover a row of N.
 template <int N>
-__global__ void __launch_bounds__(N / 16 > 64 ? N / 16 : 64, 512 / (N / 16 > 64 ? N / 16 : 64))
-ramp_fft_kernel(const FilterArgs * __restrict__ probs, const long long * __restrict__ pair_begin,
-                long long total, const float2 * __restrict__ tw, int tw_len)
+constexpr int kRampThreads = N / 16 > 64 ? N / 16 : 64;
+
+// Ramp filter of the row pairs first, first + stride, ... < pairs of one stack
+// (two real rows as one complex sequence); the pass twiddles and the stack's
+// ramp kernel are in shared memory already.  The next pair's raw pixels are
+// prefetched into registers while the current pair is transformed.
+template <int N>
+__device__ __forceinline__ void
+ramp_pairs(const FilterArgs & a, long long first, long long pairs, long long stride, float2 * b0, float2 * b1,
+           const float2 * tws, const float * Ks)
 {
-  constexpr int T = N / 16 > 64 ? N / 16 : 64; // threads; 16 columns per thread cover the row
-  constexpr int P = pidx(N);
-  extern __shared__ float2 sbuf[];
-  float2 *  b0 = sbuf;
-  float2 *  b1 = sbuf + P;
-  float2 *  tws = sbuf + 2 * P;
-  float *   Ks = reinterpret_cast<float *>(tws + tw_len);
-  for (int i = threadIdx.x; i < tw_len; i += blockDim.x)
-    tws[i] = tw[i];
-  const float inv = 1.f / (float)N;
-  auto        locate = [&](long long pr, int q) {
-    while (pr >= pair_begin[q + 1])
-      q++;
-    return q;
-  };
-  // the next pair's raw pixels are prefetched into registers while the
-  // current pair is transformed (columns threadIdx.x + i * blockDim.x;
-  // blockDim.x >= N / 16, so 16 columns per thread cover the row)
+  constexpr int   T = kRampThreads<N>;
+  const int       nu = a.nu_out;
+  const long long rows = (long long)a.nv * a.np;
+  const float     inv = 1.f / (float)N;
+  // columns threadIdx.x + i * blockDim.x; blockDim.x >= N / 16, so 16 columns
+  // per thread cover the row
   float pa[16], pb[16];
-  auto  prefetch = [&](const FilterArgs & a, long long pr) {
-    const long long rows = (long long)a.nv * a.np;
+  auto  prefetch = [&](long long pr) {
     const long long ra = 2 * pr, rb = ra + 1;
     const int       sa = (int)(ra / a.nv), rra = (int)(ra % a.nv);
     const bool      hb = rb < rows;
@@ -348,42 +335,21 @@ ramp_fft_kernel(const FilterArgs * __restrict__ probs, const long long * __restr
     for (int i = 0; i < 16; i++)
     {
       const int c = threadIdx.x + i * T;
-      pa[i] = (c < a.nu_out) ? raw_pixel(a, sa, rra, c) : 0.f;
-      pb[i] = (c < a.nu_out && hb) ? raw_pixel(a, sb, rrb, c) : 0.f;
+      pa[i] = (c < nu) ? raw_pixel(a, sa, rra, c) : 0.f;
+      pb[i] = (c < nu && hb) ? raw_pixel(a, sb, rrb, c) : 0.f;
     }
   };
-  // the current stack's description, in shared memory: read there, its fields
-  // cannot alias the output the loop stores to global memory
-  __shared__ FilterArgs cur;
-  int                   q = 0, kq = -1;
-  if (blockIdx.x < total)
+  if (first < pairs)
+    prefetch(first);
+  for (long long pr = first; pr < pairs; pr += stride)
   {
-    q = locate(blockIdx.x, 0);
-    prefetch(probs[q], blockIdx.x - pair_begin[q]);
-  }
-  for (long long gpr = blockIdx.x; gpr < total; gpr += gridDim.x)
-  {
-    q = locate(gpr, q);
+    const long long ra = 2 * pr, rb = ra + 1;
+    const bool      hb = rb < rows;
+    const int       sa = (int)(ra / a.nv), rra = (int)(ra % a.nv);
+    const int       sb = hb ? (int)(rb / a.nv) : sa, rrb = hb ? (int)(rb % a.nv) : rra;
+    const RowWeight wa = row_weight(a, sa, rra);
+    const RowWeight wb = row_weight(a, sb, rrb);
     __syncthreads(); // the previous pair's results have been stored
-    if (q != kq)
-    {
-      if (threadIdx.x == 0)
-        cur = probs[q];
-      for (int i = threadIdx.x; i <= N / 2; i += blockDim.x)
-        Ks[i] = probs[q].K[i];
-      kq = q;
-      __syncthreads();
-    }
-    const FilterArgs & a = cur;
-    const long long    pr = gpr - pair_begin[q];
-    const int          nu = a.nu_out;
-    const long long    rows = (long long)a.nv * a.np;
-    const long long    ra = 2 * pr, rb = ra + 1;
-    const bool         hb = rb < rows;
-    const int          sa = (int)(ra / a.nv), rra = (int)(ra % a.nv);
-    const int          sb = hb ? (int)(rb / a.nv) : sa, rrb = hb ? (int)(rb % a.nv) : rra;
-    const RowWeight    wa = row_weight(a, sa, rra);
-    const RowWeight    wb = row_weight(a, sb, rrb);
 #pragma unroll
     for (int i = 0; i < 16; i++)
     {
@@ -395,14 +361,8 @@ ramp_fft_kernel(const FilterArgs * __restrict__ probs, const long long * __restr
         b0[pidx(c)] = make_float2(x, y);
       }
     }
-    if (gpr + gridDim.x < total)
-    {
-      const int qn = locate(gpr + gridDim.x, q);
-      if (qn == q)
-        prefetch(a, gpr + gridDim.x - pair_begin[qn]);
-      else
-        prefetch(probs[qn], gpr + gridDim.x - pair_begin[qn]);
-    }
+    if (pr + stride < pairs)
+      prefetch(pr + stride);
     __syncthreads();
     if (a.next > 0)
     {
@@ -440,6 +400,60 @@ ramp_fft_kernel(const FilterArgs * __restrict__ probs, const long long * __restr
   }
 }
 
+// Ramp filter of one stack, persistent: each CTA loads the pass twiddles and
+// the ramp kernel into shared memory once, then filters row pairs until the
+// stack is done.  The stack's description is a kernel parameter.
+// 128 registers per thread at most: (threads x 128) x (512 / threads) = 64 K
+template <int N>
+__global__ void __launch_bounds__(kRampThreads<N>, 512 / kRampThreads<N>)
+ramp_fft_kernel(FilterArgs a, int tw_len)
+{
+  constexpr int P = pidx(N);
+  extern __shared__ float2 sbuf[];
+  float2 *      tws = sbuf + 2 * P;
+  float *       Ks = reinterpret_cast<float *>(tws + tw_len);
+  for (int i = threadIdx.x; i < tw_len; i += blockDim.x)
+    tws[i] = a.tw[i];
+  for (int i = threadIdx.x; i <= N / 2; i += blockDim.x)
+    Ks[i] = a.K[i];
+  const long long pairs = ((long long)a.nv * a.np + 1) / 2;
+  ramp_pairs<N>(a, blockIdx.x, pairs, gridDim.x, sbuf, sbuf + P, tws, Ks);
+}
+
+// Ramp filter of many stacks of one padded length N, persistent: the global
+// row-pair range of stack q is [pair_begin[q], pair_begin[q + 1]); a CTA takes
+// the pairs blockIdx.x + k gridDim.x, stack after stack, loading each stack's
+// description (into shared memory) and ramp kernel when it reaches it.  The
+// pass twiddles are shared by every stack of the launch.
+template <int N>
+__global__ void __launch_bounds__(kRampThreads<N>, 512 / kRampThreads<N>)
+ramp_fft_batch_kernel(const FilterArgs * __restrict__ probs, const long long * __restrict__ pair_begin, int nprob,
+                      const float2 * __restrict__ tw, int tw_len)
+{
+  constexpr int P = pidx(N);
+  extern __shared__ float2 sbuf[];
+  __shared__ FilterArgs cur;
+  float2 *              tws = sbuf + 2 * P;
+  float *               Ks = reinterpret_cast<float *>(tws + tw_len);
+  for (int i = threadIdx.x; i < tw_len; i += blockDim.x)
+    tws[i] = tw[i];
+  for (int q = 0; q < nprob; q++)
+  {
+    const long long lo = pair_begin[q], hi = pair_begin[q + 1];
+    // this CTA's first pair at or after lo, as an index of stack q
+    const long long first = (((long long)blockIdx.x - lo) % gridDim.x + gridDim.x) % gridDim.x;
+    if (lo + first >= hi)
+      continue;
+    __syncthreads(); // the previous stack's last pair has been stored
+    if (threadIdx.x == 0)
+      cur = probs[q];
+    for (int i = threadIdx.x; i <= N / 2; i += blockDim.x)
+      Ks[i] = probs[q].K[i];
+    __syncthreads();
+    ramp_pairs<N>(cur, first, hi - lo, gridDim.x, sbuf, sbuf + P, tws, Ks);
+  }
+}
+
 // Twiddle rows of every pass of a length-N transform, in pass order, FP64
 // values stored as float2 (see fft_pass).
 static void
@@ -466,50 +480,89 @@ pass_twiddles(int N, std::vector<float> & tw)
   }
 }
 
-template <int N>
+// Grid of a persistent ramp launch: as many CTAs as fit on the GPU, at most
+// one per row pair.
+template <typename K>
 static cudaError_t
-launch_ramp(const FilterArgs * d_probs, const long long * d_begin, long long pairs, const float2 * d_tw, int tw_len,
-            cudaStream_t st)
+ramp_grid(K kern, int threads, size_t smem, long long pairs, long long & grid)
 {
-  constexpr int threads = N / 16 > 64 ? N / 16 : 64;
-  const size_t  smem = (2 * (size_t)pidx(N) + tw_len) * sizeof(float2) + ((size_t)N / 2 + 1) * sizeof(float);
-  cudaError_t   e = cudaFuncSetAttribute(ramp_fft_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  int           dev = 0, sms = 0, per_sm = 0;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int         dev = 0, sms = 0, per_sm = 0;
   if (e == cudaSuccess)
     e = cudaGetDevice(&dev);
   if (e == cudaSuccess)
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (e == cudaSuccess)
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ramp_fft_kernel<N>, threads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+  grid = std::min<long long>(pairs, (long long)sms * std::max(per_sm, 1));
+  return e;
+}
+
+template <int N>
+static size_t
+ramp_smem(int tw_len)
+{
+  return (2 * (size_t)pidx(N) + tw_len) * sizeof(float2) + ((size_t)N / 2 + 1) * sizeof(float);
+}
+
+template <int N>
+static cudaError_t
+launch_ramp(const FilterArgs & a, int tw_len, long long pairs, cudaStream_t st)
+{
+  long long   grid = 0;
+  cudaError_t e = ramp_grid(ramp_fft_kernel<N>, kRampThreads<N>, ramp_smem<N>(tw_len), pairs, grid);
   if (e == cudaSuccess && pairs > 0)
   {
-    const long long grid = std::min<long long>(pairs, (long long)sms * std::max(per_sm, 1));
-    ramp_fft_kernel<N><<<(unsigned)grid, threads, smem, st>>>(d_probs, d_begin, pairs, d_tw, tw_len);
+    ramp_fft_kernel<N><<<(unsigned)grid, kRampThreads<N>, ramp_smem<N>(tw_len), st>>>(a, tw_len);
     e = cudaGetLastError();
   }
   return e;
 }
 
+template <int N>
 static cudaError_t
-launch_ramp_n(int N, const FilterArgs * d_probs, const long long * d_begin, long long pairs, const float2 * d_tw,
-              int tw_len, cudaStream_t st)
+launch_ramp_batch(const FilterArgs * d_probs, const long long * d_begin, int nprob, long long pairs,
+                  const float2 * d_tw, int tw_len, cudaStream_t st)
 {
+  long long   grid = 0;
+  cudaError_t e = ramp_grid(ramp_fft_batch_kernel<N>, kRampThreads<N>, ramp_smem<N>(tw_len), pairs, grid);
+  if (e == cudaSuccess && pairs > 0)
+  {
+    ramp_fft_batch_kernel<N><<<(unsigned)grid, kRampThreads<N>, ramp_smem<N>(tw_len), st>>>(d_probs, d_begin, nprob,
+                                                                                           d_tw, tw_len);
+    e = cudaGetLastError();
+  }
+  return e;
+}
+
+// One stack (d_probs == nullptr: a) or a table of nprob stacks of length N.
+static cudaError_t
+launch_ramp_n(int N, const FilterArgs & a, const FilterArgs * d_probs, const long long * d_begin, int nprob,
+              long long pairs, const float2 * d_tw, int tw_len, cudaStream_t st)
+{
+#define RTKB_RAMP_CASE(n)                                                                                              \
+  case n:                                                                                                              \
+    return d_probs ? launch_ramp_batch<n>(d_probs, d_begin, nprob, pairs, d_tw, tw_len, st)                            \
+                   : launch_ramp<n>(a, tw_len, pairs, st)
   switch (N)
   {
-    case 2: return launch_ramp<2>(d_probs, d_begin, pairs, d_tw, tw_len, st);
-    case 4: return launch_ramp<4>(d_probs, d_begin, pairs, d_tw, tw_len, st);
-    case 8: return launch_ramp<8>(d_probs, d_begin, pairs, d_tw, tw_len, st);
-    case 16: return launch_ramp<16>(d_probs, d_begin, pairs, d_tw, tw_len, st);
-    case 32: return launch_ramp<32>(d_probs, d_begin, pairs, d_tw, tw_len, st);
-    case 64: return launch_ramp<64>(d_probs, d_begin, pairs, d_tw, tw_len, st);
-    case 128: return launch_ramp<128>(d_probs, d_begin, pairs, d_tw, tw_len, st);
-    case 256: return launch_ramp<256>(d_probs, d_begin, pairs, d_tw, tw_len, st);
-    case 512: return launch_ramp<512>(d_probs, d_begin, pairs, d_tw, tw_len, st);
-    case 1024: return launch_ramp<1024>(d_probs, d_begin, pairs, d_tw, tw_len, st);
-    case 2048: return launch_ramp<2048>(d_probs, d_begin, pairs, d_tw, tw_len, st);
-    case 4096: return launch_ramp<4096>(d_probs, d_begin, pairs, d_tw, tw_len, st);
-    default: return launch_ramp<8192>(d_probs, d_begin, pairs, d_tw, tw_len, st);
+    RTKB_RAMP_CASE(2);
+    RTKB_RAMP_CASE(4);
+    RTKB_RAMP_CASE(8);
+    RTKB_RAMP_CASE(16);
+    RTKB_RAMP_CASE(32);
+    RTKB_RAMP_CASE(64);
+    RTKB_RAMP_CASE(128);
+    RTKB_RAMP_CASE(256);
+    RTKB_RAMP_CASE(512);
+    RTKB_RAMP_CASE(1024);
+    RTKB_RAMP_CASE(2048);
+    RTKB_RAMP_CASE(4096);
+    default:
+      return d_probs ? launch_ramp_batch<8192>(d_probs, d_begin, nprob, pairs, d_tw, tw_len, st)
+                     : launch_ramp<8192>(a, tw_len, pairs, st);
   }
+#undef RTKB_RAMP_CASE
 }
 
 struct Options
@@ -683,24 +736,17 @@ run_filters(const rtkb_geometry * g, const rtkb_image_desc * in, const Options &
   int      rc = prepare_filters(g, in, o, out_desc, d_in, d_out, is_short, P);
   if (rc != RTKB_OK)
     return rc;
-  // one upload: the tables, then (ramp) the problem table and its pair range
-  const size_t o_args = align256(P.blob.size()), o_begin = align256(o_args + sizeof(FilterArgs));
-  const size_t bytes = o_begin + 2 * sizeof(long long);
-  void *       scratch = nullptr;
-  RTKB_CUDA_TRY(rtkb::scratch_malloc(&scratch, bytes, st));
-  char * base = static_cast<char *>(scratch);
-  bind_filters(P, base);
-  P.blob.resize(bytes, 0);
-  std::memcpy(P.blob.data() + o_args, &P.a, sizeof(FilterArgs));
-  const long long begin[2] = { 0, P.pairs };
-  std::memcpy(P.blob.data() + o_begin, begin, sizeof(begin));
-  cudaError_t e = cudaMemcpyAsync(scratch, P.blob.data(), bytes, cudaMemcpyHostToDevice, st);
+  void * scratch = nullptr;
+  if (!P.blob.empty())
+    RTKB_CUDA_TRY(rtkb::scratch_malloc(&scratch, P.blob.size(), st));
+  bind_filters(P, static_cast<char *>(scratch));
+  cudaError_t e = scratch ? cudaMemcpyAsync(scratch, P.blob.data(), P.blob.size(), cudaMemcpyHostToDevice, st)
+                          : cudaSuccess;
   if (e != cudaSuccess)
     rc = cuda_fail(e, "cudaMemcpyAsync");
   else if (P.ramp)
   {
-    e = launch_ramp_n(P.a.N, reinterpret_cast<const FilterArgs *>(base + o_args),
-                      reinterpret_cast<const long long *>(base + o_begin), P.pairs, P.a.tw, P.tw_len, st);
+    e = launch_ramp_n(P.a.N, P.a, nullptr, nullptr, 1, P.pairs, P.a.tw, P.tw_len, st);
     if (e != cudaSuccess)
       rc = cuda_fail(e, "ramp_fft_kernel launch");
   }
@@ -712,9 +758,12 @@ run_filters(const rtkb_geometry * g, const rtkb_image_desc * in, const Options &
     if (e != cudaSuccess)
       rc = cuda_fail(e, "weight_kernel launch");
   }
-  cudaError_t fe = rtkb::scratch_free(scratch, st);
-  if (rc == RTKB_OK && fe != cudaSuccess)
-    rc = cuda_fail(fe, "cudaFreeAsync");
+  if (scratch)
+  {
+    cudaError_t fe = rtkb::scratch_free(scratch, st);
+    if (rc == RTKB_OK && fe != cudaSuccess)
+      rc = cuda_fail(fe, "cudaFreeAsync");
+  }
   return rc;
 }
 
@@ -956,8 +1005,9 @@ rtkb_fdk_preprocess_batch(rtkb_fdk_preprocess_problem * problems, int n, const r
     {
       const Group &    gr = groups[k];
       const Prepared & f = P[gr.idx[0]]; // the group's pass twiddles (one set per N)
-      e = launch_ramp_n(gr.N, reinterpret_cast<const FilterArgs *>(base + gr.o_args),
-                        reinterpret_cast<const long long *>(base + gr.o_begin), gr.pairs, f.a.tw, f.tw_len, st);
+      e = launch_ramp_n(gr.N, f.a, reinterpret_cast<const FilterArgs *>(base + gr.o_args),
+                        reinterpret_cast<const long long *>(base + gr.o_begin), (int)gr.idx.size(), gr.pairs, f.a.tw,
+                        f.tw_len, st);
       if (e != cudaSuccess)
         rc = cuda_fail(e, "ramp_fft_kernel launch");
     }

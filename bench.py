@@ -797,7 +797,7 @@ def cg_seconds_to_residual(torch, rtkb, stream, tol=1e-3, max_iter=300, learned_
     hbm_bytes = 2 * npix * 4 + 12 * nvox * 4
     t_l1 = 2 * ns * 16 / (l1_peak * 1e9)
     t_hbm = hbm_bytes / (hbm_peak * 1e9) if hbm_peak else 0.0
-    roofline = {"samples_per_projection": ns, "l1_bytes_per_iteration": 2 * ns * 16, "l1_peak_gbs": l1_peak,
+    roofline = {"samples_per_projector_call": ns, "l1_bytes_per_iteration": 2 * ns * 16, "l1_peak_gbs": l1_peak,
                 "hbm_bytes_per_iteration": hbm_bytes, "hbm_peak_gbs": hbm_peak,
                 "seconds_per_iteration_bound": t_l1 + t_hbm,
                 "seconds_to_rel_residual_1e-3_bound": (t_l1 + t_hbm) * it,

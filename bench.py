@@ -1079,7 +1079,10 @@ def run_reference(args, world, rank):
 
 def profile_cg():
     """CG configuration kernels, each launched a few times outside any graph
-    (targets for ncu --set full captures; prints a JSON line of device times)."""
+    (targets for ncu --set full captures; prints a JSON line of device times).
+    The Joseph band heights are autotuned first, as in the CG leg; the CG
+    iterations run inside the NVTX range "rtkb_cg_iterate" (ncu --nvtx
+    --nvtx-include "rtkb_cg_iterate/" selects exactly their kernels)."""
     import torch
 
     import rtk_b200 as rtkb
@@ -1095,6 +1098,8 @@ def profile_cg():
     ell[:, 15] *= 0.02
     p = rtkb.ops.project_ellipsoids(g, pd, ell)
     x = torch.zeros((256, 256, 256), device="cuda")
+    # the Joseph pair's band heights from the autotuner, as the CG leg runs it
+    bands = rtkb.ops.joseph_autotune(g, vd, pd, torch.full_like(x, 0.01), p, repeats=1)
     cg = rtkb.ops.ConjugateGradient(g, vd, pd, use_cuda_graph=False)
     cg.start(p, x)
     torch.cuda.synchronize()
@@ -1117,7 +1122,9 @@ def profile_cg():
     xb = torch.randn((4, 64, 64, 64), device="cuda")
     net.train_step(xb, xb, lr=1e-3, margin=16)
     net.close()
+    rtkb.ops.joseph_band_rows(8, 8)
     print(json.dumps({"profile_cg": {"cg_iteration_ms": t_it, "unet_forward_ms_256": t_fwd,
+                                     "joseph_band_rows": [bands["forward"], bands["back"]],
                                      "workload": "256^3 @1mm <- 360 x 512x384 @0.8mm"}}), flush=True)
     return 0
 

@@ -185,6 +185,142 @@ public:
   }
 };
 
+/* rtk::FDKWeightProjectionFilter: projections out = FDK-weighted projections in (out may equal in) */
+class FDKWeightProjectionFilter : public ProjectorBase
+{
+public:
+  void
+  Update()
+  {
+    Check(rtkb_fdk_weight(m_Geometry, &m_Proj, m_ProjIn, m_ProjOut, m_Stream), "FDKWeightProjectionFilter");
+  }
+};
+
+/* rtk::ParkerShortScanImageFilter; a full scan copies the projections */
+class ParkerShortScanImageFilter : public ProjectorBase
+{
+public:
+  void
+  SetAngularGapThreshold(double radians)
+  {
+    m_Threshold = radians;
+  }
+  void
+  Update()
+  {
+    int s = 0;
+    Check(rtkb_parker_short_scan(m_Geometry, &m_Proj, m_Threshold, m_ProjIn, m_ProjOut, m_Stream, &s),
+          "ParkerShortScanImageFilter");
+    m_Short = s != 0;
+  }
+  /* after Update: whether the scan was short (weights applied) */
+  bool
+  GetIsShortScan() const
+  {
+    return m_Short;
+  }
+
+private:
+  double m_Threshold = 3.14159265358979323846 / 9;
+  bool   m_Short = false;
+};
+
+/* rtk::DisplacedDetectorImageFilter; the output may be wider than the input
+ * (padded on the truncated side): size its buffer from GetOutputRegion(). */
+class DisplacedDetectorImageFilter : public ProjectorBase
+{
+public:
+  void
+  SetPadOnTruncatedSide(bool pad)
+  {
+    m_Pad = pad;
+  }
+  rtkb_image_desc
+  GetOutputRegion() const
+  {
+    rtkb_image_desc out{};
+    int             weighted = 0;
+    Check(rtkb_displaced_detector_region(m_Geometry, &m_Proj, m_Pad ? 1 : 0, &out, &weighted),
+          "DisplacedDetectorImageFilter");
+    return out;
+  }
+  void
+  Update()
+  {
+    Check(rtkb_displaced_detector(m_Geometry, &m_Proj, m_Pad ? 1 : 0, m_ProjIn, m_ProjOut, m_Stream),
+          "DisplacedDetectorImageFilter");
+  }
+
+private:
+  bool m_Pad = true;
+};
+
+/* rtk::FFTRampImageFilter (no geometry): window cut frequencies as RTK's setters */
+class FFTRampImageFilter : public ProjectorBase
+{
+public:
+  FFTRampImageFilter() { m_R = rtkb_ramp_params{ 0., 0., 0., 0., 0., 0., 2, 2 }; }
+  void SetHannCutFrequency(double f) { m_R.hann_cut = f; }
+  void SetCosineCutFrequency(double f) { m_R.cosine_cut = f; }
+  void SetHammingFrequency(double f) { m_R.hamming = f; }
+  void SetRamLakCutFrequency(double f) { m_R.ramlak_cut = f; }
+  void SetSheppLoganCutFrequency(double f) { m_R.shepplogan_cut = f; }
+  void SetTruncationCorrection(double t) { m_R.truncation_correction = t; }
+  void SetZeroPadFactor(int z) { m_R.zero_pad_factor = z; }
+  void
+  Update()
+  {
+    Check(rtkb_ramp_filter(&m_Proj, &m_R, m_ProjIn, m_ProjOut, m_Stream), "FFTRampImageFilter");
+  }
+
+protected:
+  rtkb_ramp_params m_R;
+};
+
+/* rtk::FDKConeBeamReconstructionFilter: weighting and ramp filtering of the
+ * projections (in one pass; optionally the displaced-detector and Parker
+ * weights of the filters rtkfdk chains before it) into a caller-provided
+ * buffer, then the FDK backprojection into the volume.  The filtered buffer
+ * holds GetFilteredRegion()'s pixels. */
+class FDKConeBeamReconstructionFilter : public FFTRampImageFilter
+{
+public:
+  void SetDisplacedDetector(bool on) { m_Displaced = on; }
+  void SetShortScan(bool on) { m_Short = on; }
+  void SetFilteredProjectionsBuffer(float * d) { m_Filtered = d; }
+  rtkb_image_desc
+  GetFilteredRegion() const
+  {
+    if (!m_Displaced)
+      return m_Proj;
+    rtkb_image_desc out{};
+    int             weighted = 0;
+    Check(rtkb_displaced_detector_region(m_Geometry, &m_Proj, 1, &out, &weighted), "FDKConeBeamReconstructionFilter");
+    return out;
+  }
+  void
+  Update()
+  {
+    if (!m_Filtered)
+      throw Exception("FDKConeBeamReconstructionFilter: no buffer for the filtered projections");
+    rtkb_fdk_preprocess_params p{};
+    p.displaced_detector = m_Displaced ? 1 : 0;
+    p.pad_on_truncated_side = 1;
+    p.short_scan = m_Short ? 1 : 0;
+    p.angular_gap_threshold = 0.;
+    p.ramp = m_R;
+    rtkb_image_desc f{};
+    Check(rtkb_fdk_preprocess(m_Geometry, &m_Proj, &p, &f, m_ProjIn, m_Filtered, m_Stream),
+          "FDKConeBeamReconstructionFilter");
+    Check(rtkb_fdk_backproject(m_Geometry, &m_Vol, &f, m_Filtered, m_VolIn, m_VolOut, m_Stream),
+          "FDKConeBeamReconstructionFilter");
+  }
+
+private:
+  bool    m_Displaced = false, m_Short = false;
+  float * m_Filtered = nullptr;
+};
+
 /* rtk::BackProjectionImageFilter (voxel-based) */
 class BackProjectionImageFilter : public ProjectorBase
 {

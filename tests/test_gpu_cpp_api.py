@@ -1,7 +1,8 @@
 """The header-only C++ layer (include/rtkb200.hpp) on a GPU: a C++ program
-runs JosephForwardProjectionImageFilter and ConjugateGradientConeBeamReconstructionFilter
-on device buffers it allocates itself; the results equal those of the same
-entry points called through the Python binding."""
+runs JosephForwardProjectionImageFilter, ConjugateGradientConeBeamReconstructionFilter,
+FDKConeBeamReconstructionFilter and the FDKWeightProjectionFilter ->
+FFTRampImageFilter chain on device buffers it allocates itself; the results
+equal those of the same entry points called through the Python binding."""
 import os
 import shutil
 import subprocess
@@ -38,9 +39,11 @@ int main(int, char ** argv)
   const double vsp[3] = { 6., 6., 6. }, psp[3] = { 4., 4., 1. };
   const double vo[3] = { -69., -57., -63. }, po[3] = { -78., -62., -7.5 };
   const rtkb_image_desc vd = rtkb::MakeImageDescription(vs, vsp, vo), pd = rtkb::MakeImageDescription(ps, psp, po);
-  float *d_vol, *d_proj, *d_out, *d_x;
-  if (cudaMalloc(&d_vol, nv * 4) || cudaMalloc(&d_proj, np * 4) || cudaMalloc(&d_out, np * 4) || cudaMalloc(&d_x, nv * 4))
+  float *d_vol, *d_proj, *d_out, *d_x, *d_fdk, *d_filt, *d_w;
+  if (cudaMalloc(&d_vol, nv * 4) || cudaMalloc(&d_proj, np * 4) || cudaMalloc(&d_out, np * 4) || cudaMalloc(&d_x, nv * 4) ||
+      cudaMalloc(&d_fdk, nv * 4) || cudaMalloc(&d_filt, np * 4) || cudaMalloc(&d_w, np * 4))
     return 3;
+  cudaMemset(d_fdk, 0, nv * 4);
   cudaMemcpy(d_vol, vol.data(), nv * 4, cudaMemcpyHostToDevice);
   cudaMemcpy(d_proj, proj.data(), np * 4, cudaMemcpyHostToDevice);
   cudaMemset(d_out, 0, np * 4);
@@ -59,6 +62,21 @@ int main(int, char ** argv)
     cg.SetNumberOfIterations(3);
     cg.SetDisableDisplacedDetectorFilter(true);
     cg.Update();
+    rtkb::FDKConeBeamReconstructionFilter fdk;
+    fdk.SetGeometry(g);
+    fdk.SetVolume(vd, d_fdk, d_fdk);
+    fdk.SetProjections(pd, d_proj);
+    fdk.SetHannCutFrequency(0.8);
+    fdk.SetFilteredProjectionsBuffer(d_filt);
+    fdk.Update();
+    rtkb::FDKWeightProjectionFilter w;
+    w.SetGeometry(g);
+    w.SetProjections(pd, d_proj, d_w);
+    w.Update();
+    rtkb::FFTRampImageFilter ramp;
+    ramp.SetProjections(pd, d_w, d_w);
+    ramp.SetHannCutFrequency(0.8);
+    ramp.Update();
   }
   catch (const rtkb::Exception & e)
   {
@@ -69,9 +87,14 @@ int main(int, char ** argv)
     return 5;
   cudaMemcpy(out.data(), d_out, np * 4, cudaMemcpyDeviceToHost);
   cudaMemcpy(x.data(), d_x, nv * 4, cudaMemcpyDeviceToHost);
+  std::vector<float> fdkv(nv), chain(np);
+  cudaMemcpy(fdkv.data(), d_fdk, nv * 4, cudaMemcpyDeviceToHost);
+  cudaMemcpy(chain.data(), d_w, np * 4, cudaMemcpyDeviceToHost);
   f = std::fopen(argv[2], "wb");
   std::fwrite(out.data(), 4, np, f);
   std::fwrite(x.data(), 4, nv, f);
+  std::fwrite(fdkv.data(), 4, nv, f);
+  std::fwrite(chain.data(), 4, np, f);
   std::fclose(f);
   return 0;
 }
@@ -99,7 +122,9 @@ def test_cpp_layer_on_gpu_matches_python_binding(rtkb, tmp_path):
                          text=True, timeout=120, env=env)
     assert run.returncode == 0, run.stdout + run.stderr
     data = np.frombuffer((tmp_path / "out.bin").read_bytes(), dtype=np.float32)
-    fp_cpp, x_cpp = data[:proj.size].reshape(proj.shape), data[proj.size:].reshape(vol.shape)
+    fp_cpp, x_cpp = data[:proj.size].reshape(proj.shape), data[proj.size:proj.size + vol.size].reshape(vol.shape)
+    fdk_cpp = data[proj.size + vol.size:proj.size + 2 * vol.size].reshape(vol.shape)
+    chain_cpp = data[proj.size + 2 * vol.size:].reshape(proj.shape)
 
     g = rtkb.ThreeDCircularProjectionGeometry()
     for i in range(16):
@@ -113,3 +138,9 @@ def test_cpp_layer_on_gpu_matches_python_binding(rtkb, tmp_path):
     cg.start(to_gpu(proj), x, displaced_detector=False)
     cg.iterate(3)
     assert rel_l2(x_cpp, to_np(x)) < 1e-5, rel_l2(x_cpp, to_np(x))
+    ramp = rtkb.ops.ramp_params(hann=0.8)
+    f, fd = rtkb.ops.fdk_preprocess(g, pd, to_gpu(proj), ramp)
+    fdk = to_np(rtkb.ops.fdk_backproject(g, vd, fd, f, torch.zeros(vol.shape, device="cuda")))
+    assert np.array_equal(fdk_cpp, fdk.astype(np.float32))
+    chain = to_np(rtkb.ops.ramp_filter(pd, rtkb.ops.fdk_weight(g, pd, to_gpu(proj)), ramp))
+    assert np.array_equal(chain_cpp, chain.astype(np.float32))

@@ -1,7 +1,8 @@
 """RTK's own CUDA code, built unchanged from an RTK source tree by
 oracle/rtk_cuda/Makefile: the FDK back projector (CUDA_reconstruct_conebeam,
-src/rtkCudaFDKBackProjectionImageFilter.cu) and the projection weighting
-filters in oracle/_ref/librtkcudafdk.so; the ray-casting forward projector,
+src/rtkCudaFDKBackProjectionImageFilter.cu), the projection weighting
+filters and the ramp filter (CUDA_padding, CUDA_fft_convolution) in
+oracle/_ref/librtkcudafdk.so; the ray-casting forward projector,
 the voxel-based back projector, the Laplacian, TV denoising and the
 conjugate-gradient update in oracle/_ref/librtkcudaiter.so.
 
@@ -61,6 +62,8 @@ def lib():
         L.rtkcuda_displaced_weight.restype = C.c_int
         L.rtkcuda_displaced_weight.argtypes = [I3, I3, I3, I3, C.c_void_p, C.c_void_p, F, C.c_float, C.c_int,
                                                C.c_float, C.c_float, C.c_float]
+        L.rtkcuda_fft_ramp.restype = C.c_int
+        L.rtkcuda_fft_ramp.argtypes = [I3, C.c_int, F, F, C.c_int, C.c_void_p, C.c_void_p]
         L.rtkcuda_last_error.restype = C.c_char_p
         L.rtkcuda_slab_size.restype = C.c_int
         _lib = L
@@ -198,6 +201,31 @@ def displaced_weight(O, g, proj, d_in: int, d_out: int, pad=True):
                                           theta, int(sup + inf > 0.0), proj.origin[0], D[0, 0] * proj.spacing[0],
                                           D[0, 1] * proj.spacing[1]))
     return i0, s0
+
+
+def fft_ramp(O, proj, params, d_in: int, d_out: int) -> int:
+    """RTK's CUDA ramp filter (CudaFFTRampImageFilter, whose GPUGenerateData
+    is CudaFFTProjectionsConvolutionImageFilter's) on a whole stack: the
+    padded width from the oracle's restatement of GetPaddedImageRegion, the
+    kernel spectrum from the oracle's restatement of
+    FFTRampImageFilter::UpdateFFTProjectionsConvolutionKernel (real: the
+    spatial kernel is even) scaled by 1 / (padded pixel count) as the CUDA
+    filter does, and the mirror weights as UpdateTruncationMirrorWeights
+    computes them (include/rtkFFTProjectionsConvolutionImageFilter.hxx:345-355,
+    float, from the extent floor(t * nu)).  Returns the padded width."""
+    nu, nv, n = proj.size
+    padded = O.ramp_padded_size(nu, params)
+    K = O.ramp_kernel(padded, proj.spacing[0], params) / (float(padded) * nv * n)
+    spec = np.zeros((padded // 2 + 1, 2))
+    spec[:, 0] = K
+    k, kp = _f(spec)
+    ext = int(np.floor(params.truncation_correction * nu))
+    i = np.arange(ext + 1, dtype=np.float64)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        w = np.sin((ext - i) * np.pi / (2 * ext - 2)) ** 0.75
+    mw, mwp = _f(w)
+    _check(lib().rtkcuda_fft_ramp(_i(proj.size), padded, kp, mwp, ext + 1, C.c_void_p(d_in), C.c_void_p(d_out)))
+    return padded
 
 
 # ---- librtkcudaiter.so: projectors, Laplacian, TV denoising, CG update

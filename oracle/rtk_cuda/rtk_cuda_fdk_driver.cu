@@ -1,7 +1,8 @@
-// rtk_cuda_fdk_driver.cu -- C entry point around RTK's own CUDA FDK back
-// projector (CUDA_reconstruct_conebeam, compiled unchanged from the RTK
-// sources), so that tests and bench.py can time it and compare it with the
-// oracle.  TEST INFRASTRUCTURE ONLY: never part of the product.
+// rtk_cuda_fdk_driver.cu -- C entry points around RTK's own CUDA FDK back
+// projector (CUDA_reconstruct_conebeam), its CUDA projection weighting filters
+// and its CUDA ramp filter (CUDA_padding, CUDA_fft_convolution), compiled
+// unchanged from the RTK sources, so that tests and bench.py can time them and
+// compare them with the oracle.  TEST INFRASTRUCTURE ONLY: never part of the product.
 //
 // rtkcuda_fdk_backproject runs the slab loop of
 // CudaFDKBackProjectionImageFilter::GPUGenerateData
@@ -12,11 +13,15 @@
 // centre, :74-97), computed by the caller.  Returns 0, or -1 with the message
 // of the exception RTK's error macro threw (rtkcuda_last_error).
 #include "rtkCudaFDKBackProjectionImageFilter.hcu"
+#include "rtkCudaFFTProjectionsConvolutionImageFilter.hcu"
 #include "rtkConfiguration.h"
 
 #include <cstring>
 #include <exception>
+#include <stdexcept>
 #include <string>
+#include <utility>
+#include <vector>
 
 static std::string g_error;
 
@@ -139,4 +144,53 @@ rtkcuda_displaced_weight(const int idx_in[3], const int size_in[3], const int id
     g_error = e.what();
     return -1;
   }
+}
+
+// CudaFFTProjectionsConvolutionImageFilter::GPUGenerateData
+// (include/rtkCudaFFTProjectionsConvolutionImageFilter.hxx) for the ramp
+// filter of a whole stack (requested region = buffered region, index 0):
+// PadInputImageRegion's CUDA_padding into a stack of `padded` columns with
+// the input at column (padded - nu) / 2 and the Ohnesorge mirror weights
+// `mirror_weights` (n_weights = truncation extent + 1, as
+// UpdateTruncationMirrorWeights sizes them), CUDA_fft_convolution with the
+// 1-D kernel spectrum `kernel_fft` (padded / 2 + 1 complex values, already
+// scaled by 1 / (padded * nv * np) as the filter does for cuFFT), then the crop
+// back to nu columns (CudaCropImageFilter's copy) into dev_out.
+extern "C" int
+rtkcuda_fft_ramp(const int proj_size[3], int padded, const float * kernel_fft, const float * mirror_weights,
+                 int n_weights, float * dev_in, float * dev_out)
+{
+  float *  d_pad = nullptr;
+  float2 * d_kernel = nullptr;
+  int      rc = 0;
+  try
+  {
+    const int nu = proj_size[0], nv = proj_size[1], np = proj_size[2];
+    const int zeroext = (padded - nu) / 2;
+    if (cudaMalloc((void **)&d_pad, sizeof(float) * (size_t)padded * nv * np) != cudaSuccess ||
+        cudaMalloc((void **)&d_kernel, sizeof(float2) * (size_t)(padded / 2 + 1)) != cudaSuccess)
+      throw std::runtime_error("cudaMalloc failed");
+    cudaMemcpy(d_kernel, kernel_fft, sizeof(float2) * (size_t)(padded / 2 + 1), cudaMemcpyHostToDevice);
+    int3               idx = { zeroext, 0, 0 };
+    uint3              sz = { (unsigned)padded, (unsigned)nv, (unsigned)np };
+    uint3              sz_i = { (unsigned)nu, (unsigned)nv, (unsigned)np };
+    std::vector<float> mw(mirror_weights, mirror_weights + n_weights);
+    CUDA_padding(idx, sz, sz_i, dev_in, d_pad, mw);
+    int3 dim = { padded, nv, np };
+    if (dim.y == 1 && dim.z > 1)
+      std::swap(dim.y, dim.z);
+    int2 kdim = { padded / 2 + 1, 1 };
+    CUDA_fft_convolution(dim, kdim, d_pad, d_kernel);
+    if (cudaMemcpy2D(dev_out, sizeof(float) * nu, d_pad + zeroext, sizeof(float) * padded, sizeof(float) * nu,
+                     (size_t)nv * np, cudaMemcpyDeviceToDevice) != cudaSuccess)
+      throw std::runtime_error("crop copy failed");
+  }
+  catch (const std::exception & e)
+  {
+    g_error = e.what();
+    rc = -1;
+  }
+  cudaFree(d_pad);
+  cudaFree(d_kernel);
+  return rc;
 }

@@ -1712,12 +1712,14 @@ orc_ramp_filter(const orc_image * proj, const orc_ramp_params * p, const double 
   const int nu = proj->size[0], nv = proj->size[1], np = proj->size[2];
   const int padded = orc_ramp_padded_size(nu, p);
   const int zeroext = (padded - nu) / 2;
-  int       next = (int)floor(p->truncation_correction * nu);
-  if (next > zeroext)
-    next = zeroext;
-  double * mw = (double *)malloc(sizeof(double) * (next + 1));
-  for (int i = 0; i < next + 1; i++)
-    mw[i] = pow(sin((next - i) * ORC_PI / (2 * next - 2)), 0.75);
+  /* the weights follow the full extent floor(t * nu)
+   * (UpdateTruncationMirrorWeights :345-355, GetTruncationCorrectionExtent
+   * :78-81); the mirror covers at most the zero padding (:215-216) */
+  const int extent = (int)floor(p->truncation_correction * nu);
+  const int next = extent < zeroext ? extent : zeroext;
+  double *  mw = (double *)malloc(sizeof(double) * (extent + 1));
+  for (int i = 0; i < extent + 1; i++)
+    mw[i] = pow(sin((extent - i) * ORC_PI / (2 * extent - 2)), 0.75);
   double * K = (double *)malloc(sizeof(double) * (padded / 2 + 1));
   orc_ramp_kernel(padded, proj->spacing[0], p, K);
 #pragma omp parallel for num_threads(nthreads) schedule(dynamic, 8)

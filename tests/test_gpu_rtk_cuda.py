@@ -134,3 +134,51 @@ def test_rtk_cuda_displaced_detector_agrees_with_oracle(rtkb, oracle, offset):
     torch.cuda.synchronize()
     assert rel_l2(to_np(d_out), ref) < WEIGHT_TOL
     assert rel_l2(to_np(rtkb.ops.displaced_detector(gl, pd, d_in)[0]), ref) < WEIGHT_TOL
+
+
+# FP32 cuFFT against the FP64 oracle: measured ~1e-7 on these stacks
+RAMP_TOL = 1e-5
+
+
+@pytest.mark.parametrize("size,kw", [((128, 24, 8), {}), ((128, 24, 8), {"hann": 0.8, "truncation": 0.1}),
+                                     ((128, 16, 6), {"truncation": 0.6}), ((96, 1, 6), {"shepplogan": 0.9}),
+                                     ((100, 12, 5), {"cosine": 0.7, "truncation": 0.25, "pad": 1})])
+def test_rtk_cuda_ramp_filter_agrees_with_oracle(rtkb, oracle, size, kw):
+    """RTK's CUDA ramp filter (CUDA_padding + CUDA_fft_convolution: a 3-D
+    cuFFT of the padded stack times the 1-D kernel spectrum) against the
+    oracle and the product.  With truncation 0.6 the extent floor(0.6 * 128)
+    = 76 exceeds the 64 columns of zero padding: RTK mirrors 64 columns with
+    the weights of extent 76, and the case measures the margin by running
+    RTK's kernels with the weights of extent 64 instead."""
+    import torch
+
+    from oracle import rtk_cuda
+
+    _need_rtk()
+    nu, nv, n = size
+    pd, po = pair_image(rtkb, oracle, size, (0.8, 0.8, 1.0), origin=(-0.4 * (nu - 1), -0.4 * (nv - 1), 0.0))
+    rng = np.random.default_rng(nu + nv)
+    u = np.linspace(-1.0, 1.0, nu)
+    p = (30.0 + 20.0 * np.cos(1.3 * u)[None, None, :] + rng.uniform(0.0, 5.0, size=(n, nv, nu))).astype(np.float32)
+    params = oracle.ramp_params(**kw)
+    ref = oracle.ramp_filter(po, p.astype(np.float64), params)
+    d_in = torch.from_numpy(p).cuda()
+    d_out = torch.empty_like(d_in)
+    torch.cuda.synchronize()
+    padded = rtk_cuda.fft_ramp(oracle, po, params, d_in.data_ptr(), d_out.data_ptr())
+    torch.cuda.synchronize()
+    got_rtk = to_np(d_out)
+    e_rtk = rel_l2(got_rtk, ref)
+    assert e_rtk < RAMP_TOL, e_rtk
+    got = to_np(rtkb.ops.ramp_filter(pd, d_in, rtkb.ops.ramp_params(**kw)))
+    assert rel_l2(got, ref) < RAMP_TOL
+    assert rel_l2(got, got_rtk) < RAMP_TOL
+    zeroext = (padded - nu) // 2
+    ext = int(np.floor(kw.get("truncation", 0.0) * nu))
+    if ext > zeroext:
+        clamped = oracle.ramp_params(**dict(kw, truncation=(zeroext + 0.5) / nu))
+        d_slip = torch.empty_like(d_in)
+        rtk_cuda.fft_ramp(oracle, po, clamped, d_in.data_ptr(), d_slip.data_ptr())
+        torch.cuda.synchronize()
+        e_slip = rel_l2(to_np(d_slip), ref)
+        assert e_slip > 100 * RAMP_TOL, e_slip

@@ -16,7 +16,11 @@
 // shared-memory indices; the inverse transform is a forward transform of the
 // conjugate.  CTAs are persistent: the twiddles and the ramp kernel are loaded
 // into shared memory once, and the next row pair is prefetched into registers
-// while the current one is transformed.  FDK cos(gamma) weights come from
+// while the current one is transformed.  With N/16 threads per CTA (N >= 1024)
+// a thread's 16 columns are both the inputs of its first-pass butterfly and
+// the outputs of its last-pass butterflies, so the load, the kernel product
+// and the store never touch shared memory; butterfly sums and differences use
+// packed FP32 pairs (FADD2 / FFMA2).  FDK cos(gamma) weights come from
 // FP64 per-row terms evaluated per pixel in FP32, Parker and displaced-detector
 // weights from FP64 host tables; the stack is read once and written once.
 #include "rtkb_filters.h"
@@ -127,15 +131,32 @@ cmul(float2 a, float2 b)
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
-// d * e^{-2 pi i j / L} for the constant twiddles of a size-L (2, 4, 8) DFT
+// Complex sum and difference as packed FP32 pairs (one FADD2 / FFMA2 each
+// instead of two scalar instructions; x - y = fma(y, -1, x) rounds once, so
+// both are bit-identical to the scalar forms).
 __device__ __forceinline__ float2
-rot_const(float2 d, int j, int L)
+cadd(float2 x, float2 y)
+{
+  return __fadd2_rn(x, y);
+}
+
+__device__ __forceinline__ float2
+csub(float2 x, float2 y)
+{
+  return __ffma2_rn(y, make_float2(-1.f, -1.f), x);
+}
+
+// (x - y) e^{-2 pi i j / L} for the constant twiddles of a size-L (2, 4, 8)
+// DFT; the -i rotation is formed directly from x and y.
+__device__ __forceinline__ float2
+diff_rot(float2 x, float2 y, int j, int L)
 {
   constexpr float c = 0.70710678118654752440f; // sqrt(1/2)
   if (L == 2 || j == 0)
-    return d;
+    return csub(x, y);
   if (L == 4 || j == 2)
-    return make_float2(d.y, -d.x);
+    return make_float2(x.y - y.y, y.x - x.x);
+  const float2 d = csub(x, y);
   if (j == 1)
     return make_float2(c * (d.x + d.y), c * (d.y - d.x));
   return make_float2(c * (d.y - d.x), -c * (d.x + d.y));
@@ -156,8 +177,8 @@ dft_reg(float2 (&v)[R])
       for (int j = 0; j < half; j++)
       {
         const float2 x = v[i + j], y = v[i + j + half];
-        v[i + j] = make_float2(x.x + y.x, x.y + y.y);
-        v[i + j + half] = rot_const(make_float2(x.x - y.x, x.y - y.y), j, 2 * half);
+        v[i + j] = cadd(x, y);
+        v[i + j + half] = diff_rot(x, y, j, 2 * half);
       }
     }
   }
@@ -191,9 +212,16 @@ dft16(float2 (&v)[16])
   for (int j = 0; j < 8; j++)
   {
     const float2 x = v[j], y = v[j + 8];
-    const float2 d = make_float2(x.x - y.x, x.y - y.y);
-    v[j] = make_float2(x.x + y.x, x.y + y.y);
-    v[j + 8] = make_float2(d.x * c[j] + d.y * sn[j], d.y * c[j] - d.x * sn[j]); // d * W16^j
+    v[j] = cadd(x, y);
+    if (j == 0)
+      v[j + 8] = csub(x, y);
+    else if (j == 4)
+      v[j + 8] = make_float2(x.y - y.y, y.x - x.x); // -i (x - y)
+    else
+    {
+      const float2 d = csub(x, y);
+      v[j + 8] = make_float2(d.x * c[j] + d.y * sn[j], d.y * c[j] - d.x * sn[j]); // d * W16^j
+    }
   }
 #pragma unroll
   for (int half = 4; half >= 1; half >>= 1)
@@ -205,8 +233,8 @@ dft16(float2 (&v)[16])
       for (int j = 0; j < half; j++)
       {
         const float2 x = v[i + j], y = v[i + j + half];
-        v[i + j] = make_float2(x.x + y.x, x.y + y.y);
-        v[i + j + half] = rot_const(make_float2(x.x - y.x, x.y - y.y), j, 2 * half);
+        v[i + j] = cadd(x, y);
+        v[i + j + half] = diff_rot(x, y, j, 2 * half);
       }
     }
   }
@@ -238,6 +266,41 @@ twiddle_rows()
   return R == 16 ? 4 : R == 8 ? 3 : R == 4 ? 2 : 1;
 }
 
+// v[r] *= w^r for r = 1..R-1, w = e^{-2 pi i k / (Ns R)}: the powers 1, 2, 4
+// and 8 from the pass's twiddle rows, the others as their products.
+template <int R, int Ns>
+__device__ __forceinline__ void
+twiddle(float2 (&v)[R], const float2 * __restrict__ twp, int k)
+{
+  if constexpr (Ns > 1)
+  {
+    float2 t[R];
+    t[1] = twp[k];
+    if constexpr (R > 2)
+    {
+      t[2] = twp[Ns + k];
+      t[3] = cmul(t[2], t[1]);
+    }
+    if constexpr (R > 4)
+    {
+      t[4] = twp[2 * Ns + k];
+      t[5] = cmul(t[4], t[1]);
+      t[6] = cmul(t[4], t[2]);
+      t[7] = cmul(t[4], t[3]);
+    }
+    if constexpr (R > 8)
+    {
+      t[8] = twp[3 * Ns + k];
+#pragma unroll
+      for (int q = 1; q < 8; q++)
+        t[8 + q] = cmul(t[8], t[q]);
+    }
+#pragma unroll
+    for (int r = 1; r < R; r++)
+      v[r] = cmul(v[r], t[r]);
+  }
+}
+
 // Compile-time version of the pass chain for a fixed N: every stride, radix
 // and loop trip is a constant, so index arithmetic folds into immediates.
 template <int N, int T, int Ns, int R>
@@ -256,33 +319,7 @@ fft_pass_c(const float2 * __restrict__ src, float2 * __restrict__ dst, const flo
 #pragma unroll
     for (int r = 0; r < R; r++)
       v[r] = src[pidx(j + r * nb)];
-    if constexpr (Ns > 1)
-    {
-      float2 t[R];
-      t[1] = twp[k];
-      if constexpr (R > 2)
-      {
-        t[2] = twp[Ns + k];
-        t[3] = cmul(t[2], t[1]);
-      }
-      if constexpr (R > 4)
-      {
-        t[4] = twp[2 * Ns + k];
-        t[5] = cmul(t[4], t[1]);
-        t[6] = cmul(t[4], t[2]);
-        t[7] = cmul(t[4], t[3]);
-      }
-      if constexpr (R > 8)
-      {
-        t[8] = twp[3 * Ns + k];
-#pragma unroll
-        for (int q = 1; q < 8; q++)
-          t[8 + q] = cmul(t[8], t[q]);
-      }
-#pragma unroll
-      for (int r = 1; r < R; r++)
-        v[r] = cmul(v[r], t[r]);
-    }
+    twiddle<R, Ns>(v, twp, k);
     dft_any<R>(v);
     const int d = (j - k) * R + k;
 #pragma unroll
@@ -310,94 +347,254 @@ fft_chain(float2 * src, float2 * dst, const float2 * tw)
 template <int N>
 constexpr int kRampThreads = N / 16 > 64 ? N / 16 : 64;
 
-// Ramp filter of the row pairs first, first + stride, ... < pairs of one stack
-// (two real rows as one complex sequence); the pass twiddles and the stack's
-// ramp kernel are in shared memory already.  The next pair's raw pixels are
-// prefetched into registers while the current pair is transformed.
+// First pass (Ns = 1, radix 16) from registers: v holds the columns
+// threadIdx.x + i N/16, which are exactly this thread's butterfly inputs.
 template <int N>
 __device__ __forceinline__ void
-ramp_pairs(const FilterArgs & a, long long first, long long pairs, long long stride, float2 * b0, float2 * b1,
-           const float2 * tws, const float * Ks)
+fft_first_regs(float2 (&v)[16], float2 * __restrict__ dst)
 {
-  constexpr int   T = kRampThreads<N>;
-  const int       nu = a.nu_out;
-  const long long rows = (long long)a.nv * a.np;
-  const float     inv = 1.f / (float)N;
-  // columns threadIdx.x + i * blockDim.x; blockDim.x >= N / 16, so 16 columns
-  // per thread cover the row
-  float pa[16], pb[16];
-  auto  prefetch = [&](long long pr) {
-    const long long ra = 2 * pr, rb = ra + 1;
-    const int       sa = (int)(ra / a.nv), rra = (int)(ra % a.nv);
-    const bool      hb = rb < rows;
-    const int       sb = hb ? (int)(rb / a.nv) : sa, rrb = hb ? (int)(rb % a.nv) : rra;
+  dft16(v);
+#pragma unroll
+  for (int r = 0; r < 16; r++)
+    dst[pidx(16 * threadIdx.x + r)] = v[r];
+}
+
+// Last pass (Ns R = N) into registers: with T = N/16 threads a thread does
+// 16/R butterflies j = threadIdx.x + jj T (k = j), whose outputs j + r Ns are
+// the columns threadIdx.x + m T, m = jj + r 16/R -- the same column set as
+// the first pass reads.
+template <int N, int T, int Ns, int R>
+__device__ __forceinline__ void
+fft_last_regs(const float2 * __restrict__ src, const float2 * __restrict__ twp, float2 (&out)[16])
+{
+  constexpr int per = Ns / T;
+  static_assert(Ns * R == N && per * R == 16, "last pass covers the row with 16 outputs per thread");
+#pragma unroll
+  for (int jj = 0; jj < per; jj++)
+  {
+    const int j = threadIdx.x + jj * T;
+    float2    v[R];
+#pragma unroll
+    for (int r = 0; r < R; r++)
+      v[r] = src[pidx(j + r * Ns)];
+    twiddle<R, Ns>(v, twp, j);
+    dft_any<R>(v);
+#pragma unroll
+    for (int r = 0; r < R; r++)
+      out[jj + r * per] = v[r];
+  }
+}
+
+// Passes Ns, 16 Ns, ... of a length-N transform whose first pass is done:
+// radix-16 passes through shared memory, the last one into registers.
+// `spare` receives the buffer the last pass did not read (free to write
+// without a barrier).
+template <int N, int T, int Ns>
+__device__ __forceinline__ void
+fft_rest_regs(float2 * src, float2 * dst, const float2 * tw, float2 (&out)[16], float2 *& spare)
+{
+  if constexpr (N / Ns <= 16)
+  {
+    fft_last_regs<N, T, Ns, N / Ns>(src, tw, out);
+    spare = dst;
+  }
+  else
+  {
+    fft_pass_c<N, T, Ns, 16>(src, dst, tw);
+    __syncthreads();
+    fft_rest_regs<N, T, Ns * 16>(dst, src, tw + 4 * Ns, out, spare);
+  }
+}
+
+// The two rows of row pair pr (the second absent past the last row of an odd
+// stack): projection and row indices.
+struct PairRows
+{
+  int  sa, ra, sb, rb;
+  bool hb;
+};
+
+__device__ __forceinline__ PairRows
+pair_rows(const FilterArgs & a, int pr)
+{
+  const unsigned row = 2u * (unsigned)pr, nv = (unsigned)a.nv;
+  PairRows       q;
+  q.sa = (int)(row / nv);
+  q.ra = (int)(row - (unsigned)q.sa * nv);
+  q.hb = (long long)row + 1 < (long long)a.nv * a.np;
+  q.sb = q.sa;
+  q.rb = q.ra + 1;
+  if (q.rb == a.nv)
+  {
+    q.sb = q.sa + 1;
+    q.rb = 0;
+  }
+  if (!q.hb)
+  {
+    q.sb = q.sa;
+    q.rb = q.ra;
+  }
+  return q;
+}
+
+// Ohnesorge mirror extrapolation (PadInputImageRegion :218-258) in the
+// shared row b0 (the row at columns 0..nu-1, zeros after): left values wrap
+// to the end of the circular buffer.
+__device__ __forceinline__ void
+mirror_pad(const FilterArgs & a, float2 * b0, int nu, int N)
+{
+  const float2 SA = b0[pidx(1)], SE = b0[pidx(nu - 1)];
+  for (int bq = 1 + threadIdx.x; bq <= a.next; bq += blockDim.x)
+  {
+    const float  w = __ldg(a.mw + bq);
+    const float2 l = b0[pidx(bq)], r = b0[pidx(nu - 1 - bq)];
+    b0[pidx(N - bq)] = make_float2(w * (2.f * SA.x - l.x), w * (2.f * SA.y - l.y));
+    b0[pidx(nu - 1 + bq)] = make_float2(w * (2.f * SE.x - r.x), w * (2.f * SE.y - r.y));
+  }
+}
+
+// Ramp filter of the row pairs first, first + stride, ... < pairs of one stack
+// (two real rows as one complex sequence); the pass twiddles and the stack's
+// ramp kernel, pre-scaled by 1/N (a power of two: exact), are in shared
+// memory already.  The next pair's raw pixels are prefetched into registers
+// while the current pair is transformed.  With N/16 threads (N >= 1024) the
+// row pair stays in registers from the load to the first pass, from the last
+// forward pass through the kernel product to the first inverse pass, and from
+// the last inverse pass to the store.
+template <int N>
+__device__ __forceinline__ void
+ramp_pairs(const FilterArgs & a, int first, int pairs, int stride, float2 * b0, float2 * b1, const float2 * tws,
+           const float * Ks)
+{
+  constexpr int  T = kRampThreads<N>;
+  constexpr bool kRegs = (T == N / 16);
+  const int      nu = a.nu_out;
+  // columns threadIdx.x + i T; T >= N / 16, so 16 columns per thread cover the row
+  float          pa[16], pb[16];
+  auto           prefetch = [&](const PairRows & q) {
 #pragma unroll
     for (int i = 0; i < 16; i++)
     {
       const int c = threadIdx.x + i * T;
-      pa[i] = (c < nu) ? raw_pixel(a, sa, rra, c) : 0.f;
-      pb[i] = (c < nu && hb) ? raw_pixel(a, sb, rrb, c) : 0.f;
+      pa[i] = (c < nu) ? raw_pixel(a, q.sa, q.ra, c) : 0.f;
+      pb[i] = (c < nu && q.hb) ? raw_pixel(a, q.sb, q.rb, c) : 0.f;
     }
   };
+  PairRows q{};
   if (first < pairs)
-    prefetch(first);
-  for (long long pr = first; pr < pairs; pr += stride)
   {
-    const long long ra = 2 * pr, rb = ra + 1;
-    const bool      hb = rb < rows;
-    const int       sa = (int)(ra / a.nv), rra = (int)(ra % a.nv);
-    const int       sb = hb ? (int)(rb / a.nv) : sa, rrb = hb ? (int)(rb % a.nv) : rra;
-    const RowWeight wa = row_weight(a, sa, rra);
-    const RowWeight wb = row_weight(a, sb, rrb);
-    __syncthreads(); // the previous pair's results have been stored
+    q = pair_rows(a, first);
+    prefetch(q);
+  }
+  for (int pr = first; pr < pairs; pr += stride)
+  {
+    const PairRows  cur = q;
+    const RowWeight wa = row_weight(a, cur.sa, cur.ra);
+    const RowWeight wb = row_weight(a, cur.sb, cur.rb);
+    float2          v[16];
 #pragma unroll
     for (int i = 0; i < 16; i++)
     {
       const int c = threadIdx.x + i * T;
-      if (c < N)
-      {
-        const float x = (c < nu) ? apply_weights(a, wa, sa, c, pa[i]) : 0.f;
-        const float y = (c < nu && hb) ? apply_weights(a, wb, sb, c, pb[i]) : 0.f;
-        b0[pidx(c)] = make_float2(x, y);
-      }
+      v[i] = make_float2((c < nu) ? apply_weights(a, wa, cur.sa, c, pa[i]) : 0.f,
+                         (c < nu && cur.hb) ? apply_weights(a, wb, cur.sb, c, pb[i]) : 0.f);
     }
     if (pr + stride < pairs)
-      prefetch(pr + stride);
-    __syncthreads();
-    if (a.next > 0)
     {
-      // Ohnesorge mirror extrapolation (PadInputImageRegion :218-258): left
-      // values wrap to the end of the circular buffer.
-      const float2 SA = b0[pidx(1)], SE = b0[pidx(nu - 1)];
-      for (int bq = 1 + threadIdx.x; bq <= a.next; bq += blockDim.x)
+      q = pair_rows(a, pr + stride);
+      prefetch(q);
+    }
+    float * oa = a.out + ((long long)cur.sa * a.nv + cur.ra) * nu;
+    float * ob = a.out + ((long long)cur.sb * a.nv + cur.rb) * nu;
+    __syncthreads(); // the previous pair's last pass has read the shared buffers
+    if constexpr (kRegs)
+    {
+      if (a.next > 0)
       {
-        const float  w = __ldg(a.mw + bq);
-        const float2 l = b0[pidx(bq)], r = b0[pidx(nu - 1 - bq)];
-        b0[pidx(N - bq)] = make_float2(w * (2.f * SA.x - l.x), w * (2.f * SA.y - l.y));
-        b0[pidx(nu - 1 + bq)] = make_float2(w * (2.f * SE.x - r.x), w * (2.f * SE.y - r.y));
+#pragma unroll
+        for (int i = 0; i < 16; i++)
+          b0[pidx(threadIdx.x + i * T)] = v[i];
+        __syncthreads();
+        mirror_pad(a, b0, nu, N);
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < 16; i++)
+          v[i] = b0[pidx(threadIdx.x + i * T)];
+        __syncthreads();
+      }
+      fft_first_regs<N>(v, b0);
+      __syncthreads();
+      float2 * spare;
+      fft_rest_regs<N, T, 16>(b0, b1, tws, v, spare);
+      // times the real, even kernel, conjugated: the inverse transform is
+      // conj(FFT(conj(K X))) (the 1/N is in K)
+#pragma unroll
+      for (int m = 0; m < 16; m++)
+      {
+        const int   f = threadIdx.x + m * T;
+        const float k = Ks[min(f, N - f)];
+        v[m] = make_float2(v[m].x * k, -v[m].y * k);
+      }
+      fft_first_regs<N>(v, spare);
+      __syncthreads();
+      float2 * unused;
+      fft_rest_regs<N, T, 16>(spare, spare == b0 ? b1 : b0, tws, v, unused);
+#pragma unroll
+      for (int m = 0; m < 16; m++)
+      {
+        const int c = threadIdx.x + m * T;
+        if (c < nu)
+        {
+          oa[c] = v[m].x;
+          if (cur.hb)
+            ob[c] = -v[m].y;
+        }
+      }
+    }
+    else
+    {
+#pragma unroll
+      for (int i = 0; i < 16; i++)
+      {
+        const int c = threadIdx.x + i * T;
+        if (c < N)
+          b0[pidx(c)] = v[i];
       }
       __syncthreads();
-    }
-    float2 * X = fft_chain<N, T, 1>(b0, b1, tws);
-    float2 * other = (X == b0) ? b1 : b0;
-    // multiply by the real, even kernel and conjugate: the inverse transform is
-    // conj(FFT(conj(K X))) / N
-    for (int f = threadIdx.x; f < N; f += blockDim.x)
-    {
-      const float  k = Ks[min(f, N - f)];
-      const float2 z = X[pidx(f)];
-      X[pidx(f)] = make_float2(z.x * k, -z.y * k);
-    }
-    __syncthreads();
-    float2 * W = fft_chain<N, T, 1>(X, other, tws);
-    for (int c = threadIdx.x; c < nu; c += blockDim.x)
-    {
-      const float2 z = W[pidx(c)];
-      a.out[ra * nu + c] = z.x * inv;
-      if (hb)
-        a.out[rb * nu + c] = -z.y * inv;
+      if (a.next > 0)
+      {
+        mirror_pad(a, b0, nu, N);
+        __syncthreads();
+      }
+      float2 * X = fft_chain<N, T, 1>(b0, b1, tws);
+      float2 * other = (X == b0) ? b1 : b0;
+      for (int f = threadIdx.x; f < N; f += blockDim.x)
+      {
+        const float  k = Ks[min(f, N - f)];
+        const float2 z = X[pidx(f)];
+        X[pidx(f)] = make_float2(z.x * k, -z.y * k);
+      }
+      __syncthreads();
+      float2 * W = fft_chain<N, T, 1>(X, other, tws);
+      for (int c = threadIdx.x; c < nu; c += blockDim.x)
+      {
+        const float2 z = W[pidx(c)];
+        oa[c] = z.x;
+        if (cur.hb)
+          ob[c] = -z.y;
+      }
     }
   }
+}
+
+// Shared-memory ramp kernel of one stack, times 1/N (exact: N is a power of two)
+template <int N>
+__device__ __forceinline__ void
+load_kernel(const float * __restrict__ K, float * Ks)
+{
+  constexpr float inv = 1.f / (float)N;
+  for (int i = threadIdx.x; i <= N / 2; i += blockDim.x)
+    Ks[i] = K[i] * inv;
 }
 
 // Ramp filter of one stack, persistent: each CTA loads the pass twiddles and
@@ -414,9 +611,8 @@ ramp_fft_kernel(FilterArgs a, int tw_len)
   float *       Ks = reinterpret_cast<float *>(tws + tw_len);
   for (int i = threadIdx.x; i < tw_len; i += blockDim.x)
     tws[i] = a.tw[i];
-  for (int i = threadIdx.x; i <= N / 2; i += blockDim.x)
-    Ks[i] = a.K[i];
-  const long long pairs = ((long long)a.nv * a.np + 1) / 2;
+  load_kernel<N>(a.K, Ks);
+  const int pairs = (a.nv * a.np + 1) / 2;
   ramp_pairs<N>(a, blockIdx.x, pairs, gridDim.x, sbuf, sbuf + P, tws, Ks);
 }
 
@@ -447,10 +643,9 @@ ramp_fft_batch_kernel(const FilterArgs * __restrict__ probs, const long long * _
     __syncthreads(); // the previous stack's last pair has been stored
     if (threadIdx.x == 0)
       cur = probs[q];
-    for (int i = threadIdx.x; i <= N / 2; i += blockDim.x)
-      Ks[i] = probs[q].K[i];
+    load_kernel<N>(probs[q].K, Ks);
     __syncthreads();
-    ramp_pairs<N>(cur, first, hi - lo, gridDim.x, sbuf, sbuf + P, tws, Ks);
+    ramp_pairs<N>(cur, (int)first, (int)(hi - lo), gridDim.x, sbuf, sbuf + P, tws, Ks);
   }
 }
 
@@ -677,16 +872,20 @@ prepare_filters(const rtkb_geometry * g, const rtkb_image_desc * in, const Optio
     const int N = ramp_padded_size(nu_out, o.rp);
     if ((N & (N - 1)) != 0 || N > kMaxFFT || N < 2)
       return fail(RTKB_ERR_UNSUPPORTED, "padded row length must be a power of two <= 8192");
+    if ((long long)nv * np > 0x7ffffffe)
+      return fail(RTKB_ERR_UNSUPPORTED, "the ramp filter indexes rows in 32 bits: nv * np must be < 2^31");
     std::vector<double> Kd;
     ramp_kernel(N, out.spacing[0], o.rp, Kd);
     K.assign(Kd.begin(), Kd.end());
     pass_twiddles(N, tw);
-    int next = (int)std::floor(o.rp.truncation_correction * nu_out);
-    next = std::min(next, (N - nu_out) / 2);
-    if (next == 1)
+    // the weights follow the full extent floor(t * nu) (UpdateTruncationMirrorWeights
+    // :345-355); the mirror covers at most the zero padding (PadInputImageRegion :215-216)
+    const int extent = (int)std::floor(o.rp.truncation_correction * nu_out);
+    const int next = std::min(extent, (N - nu_out) / 2);
+    if (next > 0 && extent == 1)
       return fail(RTKB_ERR_INVALID_ARGUMENT, "truncation correction extent of one pixel is undefined");
     if (next > 0)
-      truncation_mirror_weights(next, mw);
+      truncation_mirror_weights(extent, mw);
     a.N = N;
     a.next = next;
   }

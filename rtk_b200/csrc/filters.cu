@@ -199,30 +199,21 @@ dft_reg(float2 (&v)[R])
   }
 }
 
-// In-register forward DFT of size 16 (radix-2 decimation in frequency with the
-// W16^j = e^{-2 pi i j/16} constants, then the 4-bit reversal).
-__device__ __forceinline__ void
-dft16(float2 (&v)[16])
+// W16^j = e^{-2 pi i j/16}, j = 0..7
+__device__ __forceinline__ float2
+w16(float2 d, int j)
 {
   constexpr float c[8] = { 1.f, 0.92387953251128675613f, 0.70710678118654752440f, 0.38268343236508977173f,
                            0.f, -0.38268343236508977173f, -0.70710678118654752440f, -0.92387953251128675613f };
   constexpr float sn[8] = { 0.f, 0.38268343236508977173f, 0.70710678118654752440f, 0.92387953251128675613f,
                             1.f, 0.92387953251128675613f, 0.70710678118654752440f, 0.38268343236508977173f };
-#pragma unroll
-  for (int j = 0; j < 8; j++)
-  {
-    const float2 x = v[j], y = v[j + 8];
-    v[j] = cadd(x, y);
-    if (j == 0)
-      v[j + 8] = csub(x, y);
-    else if (j == 4)
-      v[j + 8] = make_float2(x.y - y.y, y.x - x.x); // -i (x - y)
-    else
-    {
-      const float2 d = csub(x, y);
-      v[j + 8] = make_float2(d.x * c[j] + d.y * sn[j], d.y * c[j] - d.x * sn[j]); // d * W16^j
-    }
-  }
+  return make_float2(d.x * c[j] + d.y * sn[j], d.y * c[j] - d.x * sn[j]);
+}
+
+// Stages 2-4 of the 16-point DFT (three radix-2 levels) and the 4-bit reversal.
+__device__ __forceinline__ void
+dft16_tail(float2 (&v)[16])
+{
 #pragma unroll
   for (int half = 4; half >= 1; half >>= 1)
   {
@@ -245,6 +236,45 @@ dft16(float2 (&v)[16])
 #pragma unroll
   for (int k = 0; k < 16; k++)
     v[k] = t[k];
+}
+
+// In-register forward DFT of size 16 (radix-2 decimation in frequency with the
+// W16^j constants, then the 4-bit reversal).
+__device__ __forceinline__ void
+dft16(float2 (&v)[16])
+{
+#pragma unroll
+  for (int j = 0; j < 8; j++)
+  {
+    const float2 x = v[j], y = v[j + 8];
+    v[j] = cadd(x, y);
+    if (j == 0)
+      v[j + 8] = csub(x, y);
+    else if (j == 4)
+      v[j + 8] = make_float2(x.y - y.y, y.x - x.x); // -i (x - y)
+    else
+      v[j + 8] = w16(csub(x, y), j);
+  }
+  dft16_tail(v);
+}
+
+// The same DFT of an input whose upper half v[8..15] is zero: the first
+// stage's sums are the inputs themselves (bit-identical: x + 0 = x).
+__device__ __forceinline__ void
+dft16_upper_zero(float2 (&v)[16])
+{
+#pragma unroll
+  for (int j = 0; j < 8; j++)
+  {
+    const float2 x = v[j];
+    if (j == 0)
+      v[j + 8] = x;
+    else if (j == 4)
+      v[j + 8] = make_float2(x.y, -x.x);
+    else
+      v[j + 8] = w16(x, j);
+  }
+  dft16_tail(v);
 }
 
 template <int R>
@@ -349,11 +379,14 @@ constexpr int kRampThreads = N / 16 > 64 ? N / 16 : 64;
 
 // First pass (Ns = 1, radix 16) from registers: v holds the columns
 // threadIdx.x + i N/16, which are exactly this thread's butterfly inputs.
-template <int N>
+template <int N, bool UPPER_ZERO = false>
 __device__ __forceinline__ void
 fft_first_regs(float2 (&v)[16], float2 * __restrict__ dst)
 {
-  dft16(v);
+  if constexpr (UPPER_ZERO)
+    dft16_upper_zero(v);
+  else
+    dft16(v);
 #pragma unroll
   for (int r = 0; r < 16; r++)
     dst[pidx(16 * threadIdx.x + r)] = v[r];
@@ -460,20 +493,24 @@ mirror_pad(const FilterArgs & a, float2 * b0, int nu, int N)
 // while the current pair is transformed.  With N/16 threads (N >= 1024) the
 // row pair stays in registers from the load to the first pass, from the last
 // forward pass through the kernel product to the first inverse pass, and from
-// the last inverse pass to the store.
-template <int N>
+// the last inverse pass to the store.  UZ (upper zero): the row occupies at
+// most the lower half of the padded buffer and nothing is mirrored, so the
+// upper 8 of a thread's 16 columns are zero on input and unused on output.
+template <int N, bool UZ>
 __device__ __forceinline__ void
 ramp_pairs(const FilterArgs & a, int first, int pairs, int stride, float2 * b0, float2 * b1, const float2 * tws,
            const float * Ks)
 {
   constexpr int  T = kRampThreads<N>;
   constexpr bool kRegs = (T == N / 16);
+  static_assert(kRegs || !UZ, "the upper-zero form needs N/16 threads");
+  constexpr int  kCols = UZ ? 8 : 16;
   const int      nu = a.nu_out;
   // columns threadIdx.x + i T; T >= N / 16, so 16 columns per thread cover the row
-  float          pa[16], pb[16];
+  float          pa[kCols], pb[kCols];
   auto           prefetch = [&](const PairRows & q) {
 #pragma unroll
-    for (int i = 0; i < 16; i++)
+    for (int i = 0; i < kCols; i++)
     {
       const int c = threadIdx.x + i * T;
       pa[i] = (c < nu) ? raw_pixel(a, q.sa, q.ra, c) : 0.f;
@@ -493,7 +530,7 @@ ramp_pairs(const FilterArgs & a, int first, int pairs, int stride, float2 * b0, 
     const RowWeight wb = row_weight(a, cur.sb, cur.rb);
     float2          v[16];
 #pragma unroll
-    for (int i = 0; i < 16; i++)
+    for (int i = 0; i < kCols; i++)
     {
       const int c = threadIdx.x + i * T;
       v[i] = make_float2((c < nu) ? apply_weights(a, wa, cur.sa, c, pa[i]) : 0.f,
@@ -509,7 +546,7 @@ ramp_pairs(const FilterArgs & a, int first, int pairs, int stride, float2 * b0, 
     __syncthreads(); // the previous pair's last pass has read the shared buffers
     if constexpr (kRegs)
     {
-      if (a.next > 0)
+      if (!UZ && a.next > 0)
       {
 #pragma unroll
         for (int i = 0; i < 16; i++)
@@ -522,7 +559,7 @@ ramp_pairs(const FilterArgs & a, int first, int pairs, int stride, float2 * b0, 
           v[i] = b0[pidx(threadIdx.x + i * T)];
         __syncthreads();
       }
-      fft_first_regs<N>(v, b0);
+      fft_first_regs<N, UZ>(v, b0);
       __syncthreads();
       float2 * spare;
       fft_rest_regs<N, T, 16>(b0, b1, tws, v, spare);
@@ -540,7 +577,7 @@ ramp_pairs(const FilterArgs & a, int first, int pairs, int stride, float2 * b0, 
       float2 * unused;
       fft_rest_regs<N, T, 16>(spare, spare == b0 ? b1 : b0, tws, v, unused);
 #pragma unroll
-      for (int m = 0; m < 16; m++)
+      for (int m = 0; m < kCols; m++)
       {
         const int c = threadIdx.x + m * T;
         if (c < nu)
@@ -601,7 +638,7 @@ load_kernel(const float * __restrict__ K, float * Ks)
 // the ramp kernel into shared memory once, then filters row pairs until the
 // stack is done.  The stack's description is a kernel parameter.
 // 128 registers per thread at most: (threads x 128) x (512 / threads) = 64 K
-template <int N>
+template <int N, bool UZ>
 __global__ void __launch_bounds__(kRampThreads<N>, 512 / kRampThreads<N>)
 ramp_fft_kernel(FilterArgs a, int tw_len)
 {
@@ -613,7 +650,7 @@ ramp_fft_kernel(FilterArgs a, int tw_len)
     tws[i] = a.tw[i];
   load_kernel<N>(a.K, Ks);
   const int pairs = (a.nv * a.np + 1) / 2;
-  ramp_pairs<N>(a, blockIdx.x, pairs, gridDim.x, sbuf, sbuf + P, tws, Ks);
+  ramp_pairs<N, UZ>(a, blockIdx.x, pairs, gridDim.x, sbuf, sbuf + P, tws, Ks);
 }
 
 // Ramp filter of many stacks of one padded length N, persistent: the global
@@ -621,7 +658,7 @@ ramp_fft_kernel(FilterArgs a, int tw_len)
 // the pairs blockIdx.x + k gridDim.x, stack after stack, loading each stack's
 // description (into shared memory) and ramp kernel when it reaches it.  The
 // pass twiddles are shared by every stack of the launch.
-template <int N>
+template <int N, bool UZ>
 __global__ void __launch_bounds__(kRampThreads<N>, 512 / kRampThreads<N>)
 ramp_fft_batch_kernel(const FilterArgs * __restrict__ probs, const long long * __restrict__ pair_begin, int nprob,
                       const float2 * __restrict__ tw, int tw_len)
@@ -645,7 +682,7 @@ ramp_fft_batch_kernel(const FilterArgs * __restrict__ probs, const long long * _
       cur = probs[q];
     load_kernel<N>(probs[q].K, Ks);
     __syncthreads();
-    ramp_pairs<N>(cur, (int)first, (int)(hi - lo), gridDim.x, sbuf, sbuf + P, tws, Ks);
+    ramp_pairs<N, UZ>(cur, (int)first, (int)(hi - lo), gridDim.x, sbuf, sbuf + P, tws, Ks);
   }
 }
 
@@ -700,15 +737,42 @@ ramp_smem(int tw_len)
   return (2 * (size_t)pidx(N) + tw_len) * sizeof(float2) + ((size_t)N / 2 + 1) * sizeof(float);
 }
 
-template <int N>
+template <int N, bool UZ>
 static cudaError_t
-launch_ramp(const FilterArgs & a, int tw_len, long long pairs, cudaStream_t st)
+launch_ramp_uz(const FilterArgs & a, int tw_len, long long pairs, cudaStream_t st)
 {
   long long   grid = 0;
-  cudaError_t e = ramp_grid(ramp_fft_kernel<N>, kRampThreads<N>, ramp_smem<N>(tw_len), pairs, grid);
+  cudaError_t e = ramp_grid(ramp_fft_kernel<N, UZ>, kRampThreads<N>, ramp_smem<N>(tw_len), pairs, grid);
   if (e == cudaSuccess && pairs > 0)
   {
-    ramp_fft_kernel<N><<<(unsigned)grid, kRampThreads<N>, ramp_smem<N>(tw_len), st>>>(a, tw_len);
+    ramp_fft_kernel<N, UZ><<<(unsigned)grid, kRampThreads<N>, ramp_smem<N>(tw_len), st>>>(a, tw_len);
+    e = cudaGetLastError();
+  }
+  return e;
+}
+
+// The upper-zero form exists for N/16-thread CTAs (N >= 1024) only.
+template <int N>
+static cudaError_t
+launch_ramp(const FilterArgs & a, int tw_len, long long pairs, bool uz, cudaStream_t st)
+{
+  if constexpr (kRampThreads<N> == N / 16)
+    if (uz)
+      return launch_ramp_uz<N, true>(a, tw_len, pairs, st);
+  return launch_ramp_uz<N, false>(a, tw_len, pairs, st);
+}
+
+template <int N, bool UZ>
+static cudaError_t
+launch_ramp_batch_uz(const FilterArgs * d_probs, const long long * d_begin, int nprob, long long pairs,
+                     const float2 * d_tw, int tw_len, cudaStream_t st)
+{
+  long long   grid = 0;
+  cudaError_t e = ramp_grid(ramp_fft_batch_kernel<N, UZ>, kRampThreads<N>, ramp_smem<N>(tw_len), pairs, grid);
+  if (e == cudaSuccess && pairs > 0)
+  {
+    ramp_fft_batch_kernel<N, UZ><<<(unsigned)grid, kRampThreads<N>, ramp_smem<N>(tw_len), st>>>(d_probs, d_begin, nprob,
+                                                                                           d_tw, tw_len);
     e = cudaGetLastError();
   }
   return e;
@@ -717,28 +781,32 @@ launch_ramp(const FilterArgs & a, int tw_len, long long pairs, cudaStream_t st)
 template <int N>
 static cudaError_t
 launch_ramp_batch(const FilterArgs * d_probs, const long long * d_begin, int nprob, long long pairs,
-                  const float2 * d_tw, int tw_len, cudaStream_t st)
+                  const float2 * d_tw, int tw_len, bool uz, cudaStream_t st)
 {
-  long long   grid = 0;
-  cudaError_t e = ramp_grid(ramp_fft_batch_kernel<N>, kRampThreads<N>, ramp_smem<N>(tw_len), pairs, grid);
-  if (e == cudaSuccess && pairs > 0)
-  {
-    ramp_fft_batch_kernel<N><<<(unsigned)grid, kRampThreads<N>, ramp_smem<N>(tw_len), st>>>(d_probs, d_begin, nprob,
-                                                                                           d_tw, tw_len);
-    e = cudaGetLastError();
-  }
-  return e;
+  if constexpr (kRampThreads<N> == N / 16)
+    if (uz)
+      return launch_ramp_batch_uz<N, true>(d_probs, d_begin, nprob, pairs, d_tw, tw_len, st);
+  return launch_ramp_batch_uz<N, false>(d_probs, d_begin, nprob, pairs, d_tw, tw_len, st);
 }
 
-// One stack (d_probs == nullptr: a) or a table of nprob stacks of length N.
+// Whether a stack's rows fit the upper-zero form: at most N/2 columns and no
+// mirror extrapolation (the N/16-thread condition is the launcher's).
+static bool
+upper_zero(const FilterArgs & a)
+{
+  return a.next == 0 && 2 * a.nu_out <= a.N;
+}
+
+// One stack (d_probs == nullptr: a) or a table of nprob stacks of length N;
+// uz: every stack has upper_zero().
 static cudaError_t
 launch_ramp_n(int N, const FilterArgs & a, const FilterArgs * d_probs, const long long * d_begin, int nprob,
-              long long pairs, const float2 * d_tw, int tw_len, cudaStream_t st)
+              long long pairs, const float2 * d_tw, int tw_len, bool uz, cudaStream_t st)
 {
 #define RTKB_RAMP_CASE(n)                                                                                              \
   case n:                                                                                                              \
-    return d_probs ? launch_ramp_batch<n>(d_probs, d_begin, nprob, pairs, d_tw, tw_len, st)                            \
-                   : launch_ramp<n>(a, tw_len, pairs, st)
+    return d_probs ? launch_ramp_batch<n>(d_probs, d_begin, nprob, pairs, d_tw, tw_len, uz, st)                        \
+                   : launch_ramp<n>(a, tw_len, pairs, uz, st)
   switch (N)
   {
     RTKB_RAMP_CASE(2);
@@ -754,8 +822,8 @@ launch_ramp_n(int N, const FilterArgs & a, const FilterArgs * d_probs, const lon
     RTKB_RAMP_CASE(2048);
     RTKB_RAMP_CASE(4096);
     default:
-      return d_probs ? launch_ramp_batch<8192>(d_probs, d_begin, nprob, pairs, d_tw, tw_len, st)
-                     : launch_ramp<8192>(a, tw_len, pairs, st);
+      return d_probs ? launch_ramp_batch<8192>(d_probs, d_begin, nprob, pairs, d_tw, tw_len, uz, st)
+                     : launch_ramp<8192>(a, tw_len, pairs, uz, st);
   }
 #undef RTKB_RAMP_CASE
 }
@@ -945,7 +1013,7 @@ run_filters(const rtkb_geometry * g, const rtkb_image_desc * in, const Options &
     rc = cuda_fail(e, "cudaMemcpyAsync");
   else if (P.ramp)
   {
-    e = launch_ramp_n(P.a.N, P.a, nullptr, nullptr, 1, P.pairs, P.a.tw, P.tw_len, st);
+    e = launch_ramp_n(P.a.N, P.a, nullptr, nullptr, 1, P.pairs, P.a.tw, P.tw_len, upper_zero(P.a), st);
     if (e != cudaSuccess)
       rc = cuda_fail(e, "ramp_fft_kernel launch");
   }
@@ -1204,9 +1272,12 @@ rtkb_fdk_preprocess_batch(rtkb_fdk_preprocess_problem * problems, int n, const r
     {
       const Group &    gr = groups[k];
       const Prepared & f = P[gr.idx[0]]; // the group's pass twiddles (one set per N)
+      bool             uz = true;
+      for (int i : gr.idx)
+        uz = uz && upper_zero(P[i].a);
       e = launch_ramp_n(gr.N, f.a, reinterpret_cast<const FilterArgs *>(base + gr.o_args),
                         reinterpret_cast<const long long *>(base + gr.o_begin), (int)gr.idx.size(), gr.pairs, f.a.tw,
-                        f.tw_len, st);
+                        f.tw_len, uz, st);
       if (e != cudaSuccess)
         rc = cuda_fail(e, "ramp_fft_kernel launch");
     }

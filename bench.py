@@ -1357,7 +1357,7 @@ def main():
                     "d2h_bytes_per_step": h_vol.numel() * 4,
                     "path": "rtkb_fdk_backproject_host via ctypes: pinned host stack in, pinned host volume out, "
                             "the stack's copy (subsets growing x1.5 from 15 to 180 projections, the last one the "
-                            "remainder) and the volume's copy back (16 slabs) overlapped with the backprojection, all "
+                            "remainder) and the volume's copy back (slabs of halving size) overlapped with the backprojection, all "
                             "inside the timed region"},
             "roofline": roofline, "clocks": clocks, "gpu_launches": args.steps,
             "gpu_launches_note": "one rtkb backprojection kernel per step (plus one matrix upload copy)",

@@ -172,7 +172,8 @@ int rtkb_voxel_backproject(const rtkb_geometry * g, const rtkb_image_desc * vol,
  * (chunk <= 0: a quarter of the stack), so that each copy hides behind the
  * previous subset's backprojection from the first, short one on; the last
  * subset takes the remainder (up to 1.5 chunk) and is backprojected in
- * sixteen z-slabs, each copied back while the next is computed (the
+ * z-slabs of whole 16-slice tile layers whose sizes halve (16, 8, 4, 2, 1, 1
+ * layers of 32), each copied back while the next ones are computed (the
  * host<->device transfers ITK's CudaDataManager makes around
  * rtkCudaFDKBackProjectionImageFilter.cxx:34-125, overlapped).  h_vol_in may
  * be NULL (zero volume).  Asynchronous on `stream`

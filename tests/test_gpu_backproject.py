@@ -141,16 +141,18 @@ def test_fdk_bp_full_size_c2_region_and_linearity(rtkb, oracle):
     assert rtkb.ops.device_status() == 0
 
 
-@pytest.mark.parametrize("chunk,vol_init", [(0, False), (7, True), (1000, True), (1, False)])
-def test_fdk_bp_host_buffers_streamed_in_chunks(rtkb, oracle, chunk, vol_init):
+@pytest.mark.parametrize("chunk,vol_init,nz", [(0, False, 44), (7, True, 44), (1000, True, 100), (1, False, 44),
+                                               (0, True, 137)])
+def test_fdk_bp_host_buffers_streamed_in_chunks(rtkb, oracle, chunk, vol_init, nz):
     """rtkb_fdk_backproject_host: host stack and volume, the stack streamed in
     chunks (ragged last chunk with 7, one chunk with 1000, one projection per
-    chunk with 1), projection indices offset as in a subset of a longer scan."""
+    chunk with 1), projection indices offset as in a subset of a longer scan;
+    the last subset's slabs of halving size over 3, 7 and 9 tile layers."""
     import torch
 
     params = _circular(50, 1000.0, 1536.0, pox=12.0)
     gl, go = pair_geometry(rtkb, oracle, params)
-    vd, vo = pair_image(rtkb, oracle, (40, 36, 44), (2.5,) * 3, index=(2, -3, 1))
+    vd, vo = pair_image(rtkb, oracle, (40, 36, nz), (2.5,) * 3, index=(2, -3, 1))
     pd, po = pair_image(rtkb, oracle, (160, 120, 45), (1.0,) * 3, index=(-80, 0, 3))
     rng = np.random.default_rng(11 + chunk)
     p = rng.uniform(-1.0, 1.0, size=oracle.shape_of(po)).astype(np.float32).astype(np.float64)

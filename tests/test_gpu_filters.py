@@ -101,8 +101,15 @@ def test_displaced_irregular_like_rtkdisplaceddetectorcompcudatest(rtkb, oracle)
 @pytest.mark.parametrize("nu,window", [(256, {}), (1024, {"hann": 1.0}), (300, {"hann": 0.8}),
                                        (128, {"cosine": 0.7}), (512, {"hamming": 0.9}),
                                        (200, {"ramlak": 0.6}), (256, {"shepplogan": 0.8}),
-                                       (256, {"truncation": 0.1}), (2048, {"hann": 0.5})])
+                                       (256, {"truncation": 0.1}), (2048, {"hann": 0.5}),
+                                       (600, {"pad": 1}), (700, {"truncation": 0.3}),
+                                       (600, {"truncation": 0.9, "pad": 1}), (4096, {"hann": 0.9})])
 def test_ramp_filter(rtkb, oracle, nu, window):
+    """Every form of the ramp kernel: shared-memory passes (N < 1024), the
+    register-resident first and last passes with the upper-zero form (row in
+    the lower half, no mirror: 300, 1024, 2048, 4096 columns), without it (600
+    columns padded to 1024 only) and with the truncation mirror (700 columns;
+    600 with an extent wider than the zero padding)."""
     pd, po = pair_image(rtkb, oracle, (nu, 7, 3), (0.5, 0.5, 1.0))
     rng = np.random.default_rng(nu)
     p = rng.uniform(0, 1, size=oracle.shape_of(po))

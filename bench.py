@@ -197,6 +197,33 @@ def fdk_pipeline_ms(torch, rtkb, g, vd, pd, proj, stream, reps=3):
     return e0.elapsed_time(e1) / reps
 
 
+def ramp_leg(torch, rtkb, g, pd, proj, reps=5) -> dict:
+    """The projection filter of the headline's stack (720 x 768 rows of 1024,
+    zero-padded to 2048): FDK weighting + Hann ramp filter in one kernel, and
+    the ramp filter alone.  Device time (median of `reps`, current stream), the
+    HBM roofline (the stack read once and written once) and the transforms'
+    arithmetic (per row pair one forward and one inverse complex FFT of the
+    padded length, 5 N log2 N flops each)."""
+    import math
+
+    rp = rtkb.ops.ramp_params(hann=1.0)
+    out = torch.empty_like(proj)
+    ms_pre, _ = _event_median_ms(torch, lambda: rtkb.ops.fdk_preprocess(g, pd, proj, rp, out=out), reps)
+    ms_ramp, _ = _event_median_ms(torch, lambda: rtkb.ops.ramp_filter(pd, proj, rp, out=out), reps)
+    n_pad = rtkb.ops.ramp_kernel(NU, PIX, rp)[0]
+    pairs = (NP * NV + 1) // 2
+    algo_bytes = 2 * proj.numel() * 4
+    flops = pairs * 2 * 5 * n_pad * math.log2(n_pad)
+    hbm = peaks().get("hbm_gbs")
+    gbs = algo_bytes / (ms_ramp * 1e-3) / 1e9
+    return {"workload": f"720 x 768 rows of {NU} columns, padded to {n_pad}; Hann ramp (cut 1.0)",
+            "weights_and_ramp_ms": ms_pre, "ramp_ms": ms_ramp,
+            "roofline": {"bound": "hbm", "algorithmic_bytes": algo_bytes, "achieved_gbs": gbs, "peak_gbs": hbm,
+                         "frac": gbs / hbm if hbm else None,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+            "fft_gflops": flops / (ms_ramp * 1e-3) / 1e9}
+
+
 def draw_ellipsoids(torch, vd, ell):
     """Voxelised ellipsoids (rtk::DrawEllipsoidImageFilter semantics: a voxel
     whose centre lies inside adds the density) on a volume description with
@@ -1397,6 +1424,7 @@ def main():
 
         leg("bf16_storage", bf16_storage_leg, torch, rtkb, g, vd, pd, proj, vol, stream, peak_smem)
         leg("fdk_pipeline_ms", fdk_pipeline_ms, torch, rtkb, g, vd, pd, proj, stream)
+        leg("ramp_filter", ramp_leg, torch, rtkb, g, pd, proj)
         leg("voxel_backprojection", voxel_bp_leg, torch, rtkb, g, vd, pd, proj, stream)
         leg("projection_sweep", sweep_leg, torch, rtkb, g, vd, pd, proj, vol, stream, args.bp_schedule)
         del proj

@@ -648,7 +648,10 @@ int rtkb_displaced_detector(const rtkb_geometry * g, const rtkb_image_desc * pro
  * and rtk::FFTProjectionsConvolutionImageFilter: window cut frequencies (0 =
  * off, first non-zero wins in this order), Ohnesorge truncation correction,
  * greatest prime factor of the padded size (2 as in RTK built without FFTW;
- * only 2 is accepted on the GPU) and zero-pad factor (2). */
+ * only 2 is accepted on the GPU) and zero-pad factor (2).  hann_cut_y is
+ * HannCutFrequencyY: > 0 makes the kernel 2-D (the 1-D kernel times a Hann
+ * window along the detector rows' frequency, rows zero-padded by
+ * zero_pad_factor_y, ZeroPadFactors[1]: 1 or 2, <= 0 meaning RTK's default 2). */
 typedef struct rtkb_ramp_params
 {
   double hann_cut;
@@ -659,6 +662,8 @@ typedef struct rtkb_ramp_params
   double truncation_correction;
   int    greatest_prime_factor;
   int    zero_pad_factor;
+  double hann_cut_y;
+  int    zero_pad_factor_y;
 } rtkb_ramp_params;
 
 /* Padded FFT length for rows of nu pixels and, when kernel != NULL, the

@@ -259,7 +259,7 @@ private:
 class FFTRampImageFilter : public ProjectorBase
 {
 public:
-  FFTRampImageFilter() { m_R = rtkb_ramp_params{ 0., 0., 0., 0., 0., 0., 2, 2 }; }
+  FFTRampImageFilter() { m_R = rtkb_ramp_params{ 0., 0., 0., 0., 0., 0., 2, 2, 0., 2 }; }
   void SetHannCutFrequency(double f) { m_R.hann_cut = f; }
   void SetCosineCutFrequency(double f) { m_R.cosine_cut = f; }
   void SetHammingFrequency(double f) { m_R.hamming = f; }
@@ -267,6 +267,14 @@ public:
   void SetSheppLoganCutFrequency(double f) { m_R.shepplogan_cut = f; }
   void SetTruncationCorrection(double t) { m_R.truncation_correction = t; }
   void SetZeroPadFactor(int z) { m_R.zero_pad_factor = z; }
+  void SetHannCutFrequencyY(double f) { m_R.hann_cut_y = f; }
+  /* ZeroPadFactors (x, y) as RTK's SetZeroPadFactors */
+  void
+  SetZeroPadFactors(int zx, int zy)
+  {
+    m_R.zero_pad_factor = zx;
+    m_R.zero_pad_factor_y = zy;
+  }
   void
   Update()
   {
@@ -489,7 +497,7 @@ public:
     m_P.fdk.pad_on_truncated_side = 1;
     m_P.fdk.short_scan = 1;
     m_P.fdk.angular_gap_threshold = 3.14159265358979323846 / 9.;
-    m_P.fdk.ramp = { 0., 0., 0., 0., 0., 0., 2, 2 }; // no window, no truncation correction; powers of 2, zero pad x2
+    m_P.fdk.ramp = { 0., 0., 0., 0., 0., 0., 2, 2, 0., 2 }; // no window, no truncation correction; powers of 2, zero pad x2
   }
   void SetNumberOfIterations(int n) { m_P.niter = n; }
   void SetLambda(double l) { m_P.lambda = l; }
@@ -497,6 +505,7 @@ public:
   void SetDisableDisplacedDetectorFilter(bool d) { m_P.fdk.displaced_detector = d ? 0 : 1; }
   void SetTruncationCorrection(double t) { m_P.fdk.ramp.truncation_correction = t; }
   void SetHannCutFrequency(double h) { m_P.fdk.ramp.hann_cut = h; }
+  void SetHannCutFrequencyY(double h) { m_P.fdk.ramp.hann_cut_y = h; }
   void
   Update()
   {

@@ -39,6 +39,8 @@ class OrcRampParams(C.Structure):
         ("truncation_correction", C.c_double),
         ("greatest_prime_factor", C.c_int),
         ("zero_pad_factor", C.c_int),
+        ("hann_cut_y", C.c_double),
+        ("zero_pad_factor_y", C.c_int),
     ]
 
 
@@ -91,6 +93,8 @@ def lib():
             "orc_displaced_detector_region": (C.c_int, [G, IM, C.c_int, I, I, D, D]),
             "orc_displaced_detector": (C.c_int, [G, IM, C.c_int, D, D]),
             "orc_ramp_padded_size": (C.c_int, [C.c_int, C.POINTER(OrcRampParams)]),
+            "orc_ramp_padded_size_y": (C.c_int, [C.c_int, C.POINTER(OrcRampParams)]),
+            "orc_ramp_window_y": (None, [C.c_int, C.POINTER(OrcRampParams), D]),
             "orc_ramp_kernel": (None, [C.c_int, C.c_double, C.POINTER(OrcRampParams), D]),
             "orc_ramp_filter": (None, [IM, C.POINTER(OrcRampParams), D, D, C.c_int]),
             "orc_cg_joseph": (None, [G, IM, IM, D, D, D, C.c_double, C.c_double, C.c_int, D, D, C.c_int]),
@@ -316,16 +320,28 @@ def displaced_detector(g, proj, data, pad=True):
     return out, i0, s0
 
 
-def ramp_params(hann=0.0, cosine=0.0, hamming=0.0, ramlak=0.0, shepplogan=0.0, truncation=0.0, gpf=2, pad=2):
+def ramp_params(hann=0.0, cosine=0.0, hamming=0.0, ramlak=0.0, shepplogan=0.0, truncation=0.0, gpf=2, pad=2,
+                hann_y=0.0, pad_y=2):
     p = OrcRampParams()
     p.hann_cut, p.cosine_cut, p.hamming = hann, cosine, hamming
     p.ramlak_cut, p.shepplogan_cut, p.truncation_correction = ramlak, shepplogan, truncation
     p.greatest_prime_factor, p.zero_pad_factor = gpf, pad
+    p.hann_cut_y, p.zero_pad_factor_y = hann_y, pad_y
     return p
 
 
 def ramp_padded_size(nu, params):
     return lib().orc_ramp_padded_size(nu, C.byref(params))
+
+
+def ramp_padded_size_y(nv, params):
+    return lib().orc_ramp_padded_size_y(nv, C.byref(params))
+
+
+def ramp_window_y(padded_y, params):
+    w = np.zeros(padded_y // 2 + 1)
+    lib().orc_ramp_window_y(padded_y, C.byref(params), _d(w))
+    return w
 
 
 def ramp_kernel(padded, spacing, params):

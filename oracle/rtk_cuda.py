@@ -63,7 +63,7 @@ def lib():
         L.rtkcuda_displaced_weight.argtypes = [I3, I3, I3, I3, C.c_void_p, C.c_void_p, F, C.c_float, C.c_int,
                                                C.c_float, C.c_float, C.c_float]
         L.rtkcuda_fft_ramp.restype = C.c_int
-        L.rtkcuda_fft_ramp.argtypes = [I3, C.c_int, F, F, C.c_int, C.c_void_p, C.c_void_p]
+        L.rtkcuda_fft_ramp.argtypes = [I3, C.c_int, C.c_int, F, C.c_int, F, C.c_int, C.c_void_p, C.c_void_p]
         L.rtkcuda_last_error.restype = C.c_char_p
         L.rtkcuda_slab_size.restype = C.c_int
         _lib = L
@@ -206,25 +206,37 @@ def displaced_weight(O, g, proj, d_in: int, d_out: int, pad=True):
 def fft_ramp(O, proj, params, d_in: int, d_out: int) -> int:
     """RTK's CUDA ramp filter (CudaFFTRampImageFilter, whose GPUGenerateData
     is CudaFFTProjectionsConvolutionImageFilter's) on a whole stack: the
-    padded width from the oracle's restatement of GetPaddedImageRegion, the
-    kernel spectrum from the oracle's restatement of
+    padded width and height from the oracle's restatement of
+    GetPaddedImageRegion, the kernel spectrum from the oracle's restatement of
     FFTRampImageFilter::UpdateFFTProjectionsConvolutionKernel (real: the
-    spatial kernel is even) scaled by 1 / (padded pixel count) as the CUDA
-    filter does, and the mirror weights as UpdateTruncationMirrorWeights
-    computes them (include/rtkFFTProjectionsConvolutionImageFilter.hxx:345-355,
-    float, from the extent floor(t * nu)).  Returns the padded width."""
+    spatial kernel is even; with HannCutFrequencyY the 1-D kernel replicated
+    over the padded height times the vertical window, the 2-D kernel) scaled by
+    1 / (padded pixel count) as the CUDA filter does, and the mirror weights as
+    UpdateTruncationMirrorWeights computes them
+    (include/rtkFFTProjectionsConvolutionImageFilter.hxx:345-355, float, from
+    the extent floor(t * nu)).  Returns the padded width."""
     nu, nv, n = proj.size
     padded = O.ramp_padded_size(nu, params)
-    K = O.ramp_kernel(padded, proj.spacing[0], params) / (float(padded) * nv * n)
-    spec = np.zeros((padded // 2 + 1, 2))
-    spec[:, 0] = K
+    K = O.ramp_kernel(padded, proj.spacing[0], params)
+    if params.hann_cut_y > 0.0:
+        H = O.ramp_padded_size_y(nv, params)
+        wy = O.ramp_window_y(H, params)
+        rows = np.array([wy[min(j, H - j)] for j in range(H)])
+        K2 = rows[:, None] * K[None, :]
+    else:
+        H = nv
+        K2 = K[None, :]
+    K2 = K2 / (float(padded) * H * n)
+    spec = np.zeros(K2.shape + (2,))
+    spec[..., 0] = K2
     k, kp = _f(spec)
     ext = int(np.floor(params.truncation_correction * nu))
     i = np.arange(ext + 1, dtype=np.float64)
     with np.errstate(divide="ignore", invalid="ignore"):
         w = np.sin((ext - i) * np.pi / (2 * ext - 2)) ** 0.75
     mw, mwp = _f(w)
-    _check(lib().rtkcuda_fft_ramp(_i(proj.size), padded, kp, mwp, ext + 1, C.c_void_p(d_in), C.c_void_p(d_out)))
+    _check(lib().rtkcuda_fft_ramp(_i(proj.size), padded, H, kp, K2.shape[0], mwp, ext + 1, C.c_void_p(d_in),
+                                  C.c_void_p(d_out)))
     return padded
 
 

@@ -150,40 +150,45 @@ rtkcuda_displaced_weight(const int idx_in[3], const int size_in[3], const int id
 // (include/rtkCudaFFTProjectionsConvolutionImageFilter.hxx) for the ramp
 // filter of a whole stack (requested region = buffered region, index 0):
 // PadInputImageRegion's CUDA_padding into a stack of `padded` columns with
-// the input at column (padded - nu) / 2 and the Ohnesorge mirror weights
-// `mirror_weights` (n_weights = truncation extent + 1, as
-// UpdateTruncationMirrorWeights sizes them), CUDA_fft_convolution with the
-// 1-D kernel spectrum `kernel_fft` (padded / 2 + 1 complex values, already
-// scaled by 1 / (padded * nv * np) as the filter does for cuFFT), then the crop
-// back to nu columns (CudaCropImageFilter's copy) into dev_out.
+// the input at column (padded - nu) / 2 and `padded_y` rows (nv, or the
+// padded height of the 2-D kernel) with the input at row 0, and the Ohnesorge
+// mirror weights `mirror_weights` (n_weights = truncation extent + 1, as
+// UpdateTruncationMirrorWeights sizes them); CUDA_fft_convolution with the
+// kernel spectrum `kernel_fft` (kernel_rows rows of padded / 2 + 1 complex
+// values: 1 row for the 1-D kernel, padded_y rows for the 2-D one, already
+// scaled by 1 / (padded * padded_y * np) as the filter does for cuFFT); then the
+// crop back to nv rows of nu columns (CudaCropImageFilter's copy) into dev_out.
 extern "C" int
-rtkcuda_fft_ramp(const int proj_size[3], int padded, const float * kernel_fft, const float * mirror_weights,
-                 int n_weights, float * dev_in, float * dev_out)
+rtkcuda_fft_ramp(const int proj_size[3], int padded, int padded_y, const float * kernel_fft, int kernel_rows,
+                 const float * mirror_weights, int n_weights, float * dev_in, float * dev_out)
 {
   float *  d_pad = nullptr;
   float2 * d_kernel = nullptr;
   int      rc = 0;
   try
   {
-    const int nu = proj_size[0], nv = proj_size[1], np = proj_size[2];
-    const int zeroext = (padded - nu) / 2;
-    if (cudaMalloc((void **)&d_pad, sizeof(float) * (size_t)padded * nv * np) != cudaSuccess ||
-        cudaMalloc((void **)&d_kernel, sizeof(float2) * (size_t)(padded / 2 + 1)) != cudaSuccess)
+    const int    nu = proj_size[0], nv = proj_size[1], np = proj_size[2];
+    const int    zeroext = (padded - nu) / 2;
+    const size_t nk = (size_t)(padded / 2 + 1) * kernel_rows;
+    if (cudaMalloc((void **)&d_pad, sizeof(float) * (size_t)padded * padded_y * np) != cudaSuccess ||
+        cudaMalloc((void **)&d_kernel, sizeof(float2) * nk) != cudaSuccess)
       throw std::runtime_error("cudaMalloc failed");
-    cudaMemcpy(d_kernel, kernel_fft, sizeof(float2) * (size_t)(padded / 2 + 1), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_kernel, kernel_fft, sizeof(float2) * nk, cudaMemcpyHostToDevice);
     int3               idx = { zeroext, 0, 0 };
-    uint3              sz = { (unsigned)padded, (unsigned)nv, (unsigned)np };
+    uint3              sz = { (unsigned)padded, (unsigned)padded_y, (unsigned)np };
     uint3              sz_i = { (unsigned)nu, (unsigned)nv, (unsigned)np };
     std::vector<float> mw(mirror_weights, mirror_weights + n_weights);
     CUDA_padding(idx, sz, sz_i, dev_in, d_pad, mw);
-    int3 dim = { padded, nv, np };
+    int3 dim = { padded, padded_y, np };
     if (dim.y == 1 && dim.z > 1)
       std::swap(dim.y, dim.z);
-    int2 kdim = { padded / 2 + 1, 1 };
+    int2 kdim = { padded / 2 + 1, kernel_rows };
     CUDA_fft_convolution(dim, kdim, d_pad, d_kernel);
-    if (cudaMemcpy2D(dev_out, sizeof(float) * nu, d_pad + zeroext, sizeof(float) * padded, sizeof(float) * nu,
-                     (size_t)nv * np, cudaMemcpyDeviceToDevice) != cudaSuccess)
-      throw std::runtime_error("crop copy failed");
+    for (int s = 0; s < np; s++)
+      if (cudaMemcpy2D(dev_out + (size_t)s * nv * nu, sizeof(float) * nu,
+                       d_pad + (size_t)s * padded_y * padded + zeroext, sizeof(float) * padded, sizeof(float) * nu,
+                       (size_t)nv, cudaMemcpyDeviceToDevice) != cudaSuccess)
+        throw std::runtime_error("crop copy failed");
   }
   catch (const std::exception & e)
   {

@@ -1583,6 +1583,38 @@ orc_ramp_padded_size(int nu, const orc_ramp_params * p)
   return x;
 }
 
+int
+orc_ramp_padded_size_y(int nv, const orc_ramp_params * p)
+{
+  /* GetPaddedImageRegion :296-301: padding along y only with the 2-D kernel
+   * (HannCutFrequencyY > 0, FFTRampImageFilter::GenerateInputRequestedRegion
+   * :41); ZeroPadFactors[1] is clamped to [1, 2] (header :108-111), default 2 */
+  if (!(p->hann_cut_y > 0.))
+    return nv;
+  int zy = p->zero_pad_factor_y <= 0 ? 2 : (p->zero_pad_factor_y > 2 ? 2 : p->zero_pad_factor_y);
+  int y = zy * nv;
+  while (greatest_prime_factor(y) > p->greatest_prime_factor)
+    y++;
+  return y;
+}
+
+void
+orc_ramp_window_y(int padded_y, const orc_ramp_params * p, double * w)
+{
+  /* UpdateFFTProjectionsConvolutionKernel :141-177: kernel rows j < ncut and
+   * padded_y - j (1 <= j < ncut) are the 1-D kernel times the Hann window
+   * 0.5 (1 + cos(pi j / ncut)), ncut = round((padded_y / 2 + 1) min(1, fy));
+   * the other rows are zero */
+  const int half = padded_y / 2;
+  for (int j = 0; j <= half; j++)
+    w[j] = 0.;
+  if (!(p->hann_cut_y > 0.))
+    return;
+  const int ncut = (int)floor((half + 1) * fmin(1.0, p->hann_cut_y) + 0.5);
+  for (int j = 0; j < ncut && j <= half; j++)
+    w[j] = 0.5 * (1 + cos(ORC_PI * j / ncut));
+}
+
 /* complex DFT of length n in place (radix-2 when n is a power of two,
  * direct O(n^2) otherwise); sign -1 forward, +1 inverse (unscaled) */
 static void
@@ -1722,6 +1754,79 @@ orc_ramp_filter(const orc_image * proj, const orc_ramp_params * p, const double 
     mw[i] = pow(sin((extent - i) * ORC_PI / (2 * extent - 2)), 0.75);
   double * K = (double *)malloc(sizeof(double) * (padded / 2 + 1));
   orc_ramp_kernel(padded, proj->spacing[0], p, K);
+  if (p->hann_cut_y > 0.)
+  {
+    /* 2-D kernel: per projection, the padded image (rows 0..nv-1 at their own
+     * index, x as for the 1-D kernel, zero rows up to the padded height)
+     * through a 2-D DFT, times K2[j][f] = wy[min(j, H - j)] K[min(f, N - f)],
+     * the inverse 2-D DFT and the crop (ThreadedGenerateData :121-198 with
+     * one projection per region, GetPaddedImageRegion :280-306) */
+    const int H = orc_ramp_padded_size_y(nv, p);
+    double *  wy = (double *)malloc(sizeof(double) * (H / 2 + 1));
+    orc_ramp_window_y(H, p, wy);
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 1)
+    for (int s = 0; s < np; s++)
+    {
+      double * re = (double *)calloc((size_t)H * padded, sizeof(double));
+      double * im = (double *)calloc((size_t)H * padded, sizeof(double));
+      double * cr = (double *)malloc(sizeof(double) * H);
+      double * ci = (double *)malloc(sizeof(double) * H);
+      for (int r = 0; r < nv; r++)
+      {
+        const double * x = in + ((long)s * nv + r) * nu;
+        double *       rr = re + (size_t)r * padded;
+        for (int i = 0; i < nu; i++)
+          rr[zeroext + i] = x[i];
+        if (next)
+        {
+          const double SA = x[1], SE = x[nu - 1];
+          for (int b = 1; b <= next; b++)
+          {
+            rr[zeroext - b] = mw[b] * (2.0 * SA - x[b]);
+            rr[zeroext + nu - 1 + b] = mw[b] * (2.0 * SE - x[nu - 1 - b]);
+          }
+        }
+        dft(rr, im + (size_t)r * padded, padded, -1);
+      }
+      for (int f = 0; f < padded; f++)
+      {
+        const double kf = K[f <= padded / 2 ? f : padded - f];
+        for (int j = 0; j < H; j++)
+        {
+          cr[j] = re[(size_t)j * padded + f];
+          ci[j] = im[(size_t)j * padded + f];
+        }
+        dft(cr, ci, H, -1);
+        for (int j = 0; j < H; j++)
+        {
+          const double k = kf * wy[j <= H / 2 ? j : H - j];
+          cr[j] *= k;
+          ci[j] *= k;
+        }
+        dft(cr, ci, H, +1);
+        for (int j = 0; j < H; j++)
+        {
+          re[(size_t)j * padded + f] = cr[j];
+          im[(size_t)j * padded + f] = ci[j];
+        }
+      }
+      for (int r = 0; r < nv; r++)
+      {
+        double * rr = re + (size_t)r * padded;
+        dft(rr, im + (size_t)r * padded, padded, +1);
+        for (int i = 0; i < nu; i++)
+          out[((long)s * nv + r) * nu + i] = rr[zeroext + i] / ((double)padded * H);
+      }
+      free(re);
+      free(im);
+      free(cr);
+      free(ci);
+    }
+    free(wy);
+    free(K);
+    free(mw);
+    return;
+  }
 #pragma omp parallel for num_threads(nthreads) schedule(dynamic, 8)
   for (long row = 0; row < (long)nv * np; row++)
   {

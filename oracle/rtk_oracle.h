@@ -121,8 +121,15 @@ typedef struct orc_ramp_params
   double truncation_correction;
   int    greatest_prime_factor; /* 2 without FFTW, 13 with */
   int    zero_pad_factor;       /* 2 */
+  double hann_cut_y;            /* HannCutFrequencyY: > 0 makes the kernel 2-D */
+  int    zero_pad_factor_y;     /* ZeroPadFactors[1], used with the 2-D kernel; <= 0 means 2 */
 } orc_ramp_params;
 int  orc_ramp_padded_size(int nu, const orc_ramp_params * p);
+/* padded height with the 2-D kernel (hann_cut_y > 0), else nv */
+int  orc_ramp_padded_size_y(int nv, const orc_ramp_params * p);
+/* vertical window of the 2-D kernel, w[j] for j = 0..padded_y/2 (row j and
+ * row padded_y - j of the kernel carry w[j]) */
+void orc_ramp_window_y(int padded_y, const orc_ramp_params * p, double * w);
 /* frequency-domain kernel, length padded/2+1, real (the spatial kernel is even) */
 void orc_ramp_kernel(int padded, double spacing, const orc_ramp_params * p, double * kernel);
 void orc_ramp_filter(const orc_image * proj, const orc_ramp_params * p, const double * in, double * out,

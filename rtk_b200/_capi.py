@@ -45,6 +45,8 @@ class RampParams(C.Structure):
         ("truncation_correction", C.c_double),
         ("greatest_prime_factor", C.c_int),
         ("zero_pad_factor", C.c_int),
+        ("hann_cut_y", C.c_double),
+        ("zero_pad_factor_y", C.c_int),
     ]
 
 

@@ -117,6 +117,30 @@ weight_kernel(FilterArgs a)
     o[c] = weighted_pixel(a, w, s, r, c);
 }
 
+// T[s][c][r] = A[s][r][c] for r < rows, c < cols: 32 x 32 tiles through shared
+// memory, so that both the reads and the writes are coalesced.
+// grid: (column tiles, row tiles, projections), block 32 x 8
+__global__ void __launch_bounds__(256)
+transpose_rc_kernel(const float * __restrict__ A, float * __restrict__ T, int rows, int cols)
+{
+  __shared__ float tile[32][33];
+  const long long base = (long long)blockIdx.z * rows * cols;
+  const int       c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+  for (int k = threadIdx.y; k < 32; k += 8)
+  {
+    const int r = r0 + k, c = c0 + threadIdx.x;
+    if (r < rows && c < cols)
+      tile[k][threadIdx.x] = A[base + (long long)r * cols + c];
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += 8)
+  {
+    const int c = c0 + k, r = r0 + threadIdx.x;
+    if (r < rows && c < cols)
+      T[base + (long long)c * rows + r] = tile[threadIdx.x][k];
+  }
+}
+
 // Shared-memory index with one pad element after every 16: the stride-16
 // writes of the first radix-16 Stockham pass then spread over all banks.
 __host__ __device__ __forceinline__ constexpr int
@@ -859,6 +883,13 @@ struct Prepared
   int                        tw_len = 0;
   long long                  pairs = 0;
   bool                       ramp = false;
+  // 2-D kernel (HannCutFrequencyY): the column pass's arguments (rows = the
+  // stack's columns, N = padded height; in/out set when it runs) and tables
+  FilterArgs                 col{};
+  size_t                     o_Ky = 0, o_twy = 0;
+  int                        tw_len_y = 0;
+  long long                  col_pairs = 0;
+  bool                       colpass = false;
 };
 
 int
@@ -957,12 +988,37 @@ prepare_filters(const rtkb_geometry * g, const rtkb_image_desc * in, const Optio
     a.N = N;
     a.next = next;
   }
+  std::vector<float> Ky, twy;
+  P.colpass = o.ramp && o.rp.hann_cut_y > 0.;
+  if (P.colpass)
+  {
+    const int H = ramp_padded_size_y(nv, o.rp);
+    if ((H & (H - 1)) != 0 || H > kMaxFFT || H < 2)
+      return fail(RTKB_ERR_UNSUPPORTED, "padded column length must be a power of two <= 8192");
+    if ((long long)nu_out * np > 0x7ffffffe)
+      return fail(RTKB_ERR_UNSUPPORTED, "the 2-D ramp kernel indexes columns in 32 bits: nu * np must be < 2^31");
+    std::vector<double> Wd;
+    ramp_window_y(H, o.rp, Wd);
+    Ky.assign(Wd.begin(), Wd.end());
+    pass_twiddles(H, twy);
+    FilterArgs c{};
+    c.nu_in = nv;
+    c.nu_out = nv;
+    c.nv = nu_out;
+    c.np = np;
+    c.N = H;
+    P.col = c;
+    P.col_pairs = ((long long)nu_out * np + 1) / 2;
+  }
   P.blob.clear();
   P.o_fdk = append(P.blob, fdkp);
   P.o_colw = append(P.blob, colw);
   P.o_K = append(P.blob, K);
   P.o_tw = append(P.blob, tw);
   P.o_mw = append(P.blob, mw);
+  P.o_Ky = append(P.blob, Ky);
+  P.o_twy = append(P.blob, twy);
+  P.tw_len_y = (int)(twy.size() / 2);
   P.h_fdk = !fdkp.empty();
   P.h_colw = !colw.empty();
   P.h_K = !K.empty();
@@ -986,6 +1042,53 @@ bind_filters(Prepared & P, char * base)
   P.a.K = P.h_K ? reinterpret_cast<const float *>(base + P.o_K) : nullptr;
   P.a.tw = P.h_tw ? reinterpret_cast<const float2 *>(base + P.o_tw) : nullptr;
   P.a.mw = P.h_mw ? reinterpret_cast<const float *>(base + P.o_mw) : nullptr;
+  if (P.colpass)
+  {
+    P.col.K = reinterpret_cast<const float *>(base + P.o_Ky);
+    P.col.tw = P.tw_len_y ? reinterpret_cast<const float2 *>(base + P.o_twy) : nullptr;
+  }
+}
+
+// The vertical part of the 2-D kernel (HannCutFrequencyY).  The kernel is the
+// 1-D ramp kernel times a window of the rows' frequency, so the 2-D
+// convolution (FFTProjectionsConvolutionImageFilter::ThreadedGenerateData with
+// the 2-D kernel, include/rtkFFTProjectionsConvolutionImageFilter.hxx:121-198)
+// is the row filter followed by a circular convolution of every column,
+// zero-padded to the padded height H, with the window's inverse transform.  The
+// columns of d_out become rows of a transposed copy, which the ramp FFT kernel
+// filters in place with the window as its (real, even) kernel, and the result
+// is transposed back into d_out.
+int
+column_pass(Prepared & P, float * d_out, cudaStream_t st)
+{
+  using namespace rtkb;
+  const int nu = P.a.nu_out, nv = P.a.nv, np = P.a.np;
+  void *    t = nullptr;
+  RTKB_CUDA_TRY(rtkb::scratch_malloc(&t, (size_t)nu * nv * np * sizeof(float), st));
+  float *     T = static_cast<float *>(t);
+  int         rc = RTKB_OK;
+  const dim3  blk(32, 8);
+  transpose_rc_kernel<<<dim3((unsigned)((nu + 31) / 32), (unsigned)((nv + 31) / 32), (unsigned)np), blk, 0, st>>>(
+    d_out, T, nv, nu);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+  {
+    P.col.in = T;
+    P.col.out = T;
+    e = launch_ramp_n(P.col.N, P.col, nullptr, nullptr, 1, P.col_pairs, P.col.tw, P.tw_len_y, upper_zero(P.col), st);
+  }
+  if (e == cudaSuccess)
+  {
+    transpose_rc_kernel<<<dim3((unsigned)((nv + 31) / 32), (unsigned)((nu + 31) / 32), (unsigned)np), blk, 0, st>>>(
+      T, d_out, nu, nv);
+    e = cudaGetLastError();
+  }
+  if (e != cudaSuccess)
+    rc = cuda_fail(e, "2-D ramp kernel column pass");
+  const cudaError_t fe = rtkb::scratch_free(t, st);
+  if (rc == RTKB_OK && fe != cudaSuccess)
+    rc = cuda_fail(fe, "cudaFreeAsync");
+  return rc;
 }
 
 size_t
@@ -1016,6 +1119,8 @@ run_filters(const rtkb_geometry * g, const rtkb_image_desc * in, const Options &
     e = launch_ramp_n(P.a.N, P.a, nullptr, nullptr, 1, P.pairs, P.a.tw, P.tw_len, upper_zero(P.a), st);
     if (e != cudaSuccess)
       rc = cuda_fail(e, "ramp_fft_kernel launch");
+    else if (P.colpass)
+      rc = column_pass(P, d_out, st);
   }
   else
   {
@@ -1281,6 +1386,9 @@ rtkb_fdk_preprocess_batch(rtkb_fdk_preprocess_problem * problems, int n, const r
       if (e != cudaSuccess)
         rc = cuda_fail(e, "ramp_fft_kernel launch");
     }
+    for (int i = 0; i < n && rc == RTKB_OK; i++)
+      if (P[i].colpass)
+        rc = column_pass(P[i], problems[i].d_out, st);
     // (a copy from pageable memory returns once its source has been staged)
     cudaError_t fe = rtkb::scratch_free(scratch, st);
     if (rc == RTKB_OK && fe != cudaSuccess)

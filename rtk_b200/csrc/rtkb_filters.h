@@ -28,6 +28,8 @@ void displaced_weights(const Geometry & g, const rtkb_image_desc & proj, const D
                        std::vector<float> & w);
 
 int  ramp_padded_size(int nu, const rtkb_ramp_params & p);
+int  ramp_padded_size_y(int nv, const rtkb_ramp_params & p); // nv without the 2-D kernel
+void ramp_window_y(int padded_y, const rtkb_ramp_params & p, std::vector<double> & w); // padded_y/2+1
 void ramp_kernel(int padded, double spacing, const rtkb_ramp_params & p, std::vector<double> & K);
 void twiddles(int n, std::vector<float> & tw);
 void truncation_mirror_weights(int next, std::vector<float> & mw);

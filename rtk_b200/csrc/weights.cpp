@@ -234,6 +234,37 @@ ramp_padded_size(int nu, const rtkb_ramp_params & p)
   return (int)x;
 }
 
+int
+ramp_padded_size_y(int nv, const rtkb_ramp_params & p)
+{
+  // GetPaddedImageRegion, :296-301: rows are padded only for the 2-D kernel
+  // (HannCutFrequencyY > 0, FFTRampImageFilter.hxx:41); ZeroPadFactors[1] is
+  // clamped to [1, 2] (FFTProjectionsConvolutionImageFilter.h:108-111)
+  if (!(p.hann_cut_y > 0.))
+    return nv;
+  const int gpf = p.greatest_prime_factor > 0 ? p.greatest_prime_factor : 2;
+  const int zy = p.zero_pad_factor_y > 0 ? std::min(p.zero_pad_factor_y, 2) : 2;
+  long long y = (long long)zy * nv;
+  while (greatest_prime_factor((int)y) > gpf)
+    y++;
+  return (int)y;
+}
+
+void
+ramp_window_y(int padded_y, const rtkb_ramp_params & p, std::vector<double> & w)
+{
+  // UpdateFFTProjectionsConvolutionKernel, include/rtkFFTRampImageFilter.hxx:141-177:
+  // rows j and padded_y - j of the 2-D kernel carry the 1-D kernel times
+  // 0.5 (1 + cos(pi j / ncut)) for j < ncut = round((padded_y/2 + 1) min(1, fy))
+  const int half = padded_y / 2;
+  w.assign((size_t)half + 1, 0.);
+  if (!(p.hann_cut_y > 0.))
+    return;
+  const int ncut = (int)std::floor((half + 1) * std::min(1.0, p.hann_cut_y) + 0.5);
+  for (int j = 0; j < ncut && j <= half; j++)
+    w[j] = 0.5 * (1 + std::cos(kPi * j / ncut));
+}
+
 static void
 fft_pow2(std::vector<std::complex<double>> & a)
 {

@@ -122,13 +122,19 @@ def joseph_sample_count(geometry, vol_desc, proj_desc, stream=None) -> float:
     return n.value
 
 
-def ramp_params(hann=0.0, cosine=0.0, hamming=0.0, ramlak=0.0, shepplogan=0.0, truncation=0.0, gpf=2, pad=2):
+def ramp_params(hann=0.0, cosine=0.0, hamming=0.0, ramlak=0.0, shepplogan=0.0, truncation=0.0, gpf=2, pad=2,
+                hann_y=0.0, pad_y=2):
+    """rtkb_ramp_params: RTK's FFTRampImageFilter windows (HannCutFrequency,
+    CosineCutFrequency, HammingFrequency, RamLakCutFrequency,
+    SheppLoganCutFrequency; HannCutFrequencyY as hann_y), TruncationCorrection,
+    GreatestPrimeFactor and ZeroPadFactors (pad, pad_y)."""
     from ._capi import RampParams
 
     p = RampParams()
     p.hann_cut, p.cosine_cut, p.hamming = hann, cosine, hamming
     p.ramlak_cut, p.shepplogan_cut, p.truncation_correction = ramlak, shepplogan, truncation
     p.greatest_prime_factor, p.zero_pad_factor = gpf, pad
+    p.hann_cut_y, p.zero_pad_factor_y = hann_y, pad_y
     return p
 
 

@@ -289,3 +289,39 @@ def test_threaded_joseph_back_equals_single_threaded(oracle):
     a = O.joseph_back(g, vol, proj, p)
     b = O.joseph_back(g, vol, proj, p, threads=5)
     assert np.linalg.norm(a - b) <= 1e-13 * np.linalg.norm(a)
+
+
+def test_ramp_2d_kernel_equals_rows_then_windowed_columns(oracle):
+    """HannCutFrequencyY (include/rtkFFTRampImageFilter.hxx:141-177): the
+    oracle's literal 2-D path (2-D DFT of the padded projection, times the 1-D
+    kernel replicated over the rows with the vertical Hann window, inverse,
+    crop) against an independent numpy computation of the same convolution as
+    the row filter followed by each column's circular convolution, zero-padded
+    to the padded height, with the window (numpy's FFT).  Also the padded
+    heights and the window's shape as RTK sizes them."""
+    O = oracle
+    assert O.ramp_padded_size_y(12, O.ramp_params()) == 12  # no 2-D kernel: no padding
+    assert O.ramp_padded_size_y(12, O.ramp_params(hann_y=0.8)) == 32
+    assert O.ramp_padded_size_y(12, O.ramp_params(hann_y=0.8, pad_y=1)) == 16
+    assert O.ramp_padded_size_y(12, O.ramp_params(hann_y=0.8, pad_y=0)) == 32  # 0: RTK's default 2
+    w = O.ramp_window_y(32, O.ramp_params(hann_y=0.8))
+    ncut = int(np.floor(17 * 0.8 + 0.5))
+    np.testing.assert_allclose(w[:ncut], 0.5 * (1 + np.cos(np.pi * np.arange(ncut) / ncut)), rtol=0, atol=1e-15)
+    assert np.all(w[ncut:] == 0.0)
+    assert np.all(O.ramp_window_y(32, O.ramp_params(hann_y=5.0)) > 0.0)  # cut >= 1: every frequency kept
+    rng = np.random.default_rng(8)
+    for nu, nv, kw in ((40, 12, {"hann": 0.7, "hann_y": 0.8}), (37, 9, {"hann_y": 0.5, "truncation": 0.2}),
+                       (24, 20, {"shepplogan": 0.9, "hann_y": 1.0, "pad_y": 1})):
+        po = O.image((nu, nv, 3), (0.8, 0.8, 1.0))
+        p = rng.uniform(0, 1, size=(3, nv, nu))
+        got = O.ramp_filter(po, p, O.ramp_params(**kw))
+        rows = O.ramp_filter(po, p, O.ramp_params(**{k: v for k, v in kw.items() if k not in ("hann_y", "pad_y")}))
+        prm = O.ramp_params(**kw)
+        H = O.ramp_padded_size_y(nv, prm)
+        wy = O.ramp_window_y(H, prm)
+        full = np.array([wy[min(j, H - j)] for j in range(H)])
+        pad = np.zeros((3, H, nu))
+        pad[:, :nv, :] = rows
+        ref = np.fft.ifft(np.fft.fft(pad, axis=1) * full[None, :, None], axis=1).real[:, :nv, :]
+        assert np.linalg.norm(got - ref) <= 1e-12 * np.linalg.norm(ref), (nu, nv, kw)
+        assert np.linalg.norm(got - rows) > 1e-3 * np.linalg.norm(rows)  # the window does act

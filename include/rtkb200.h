@@ -647,8 +647,10 @@ int rtkb_displaced_detector(const rtkb_geometry * g, const rtkb_image_desc * pro
 /* Ramp filter parameters of rtk::FFTRampImageFilter (include/rtkFFTRampImageFilter.h)
  * and rtk::FFTProjectionsConvolutionImageFilter: window cut frequencies (0 =
  * off, first non-zero wins in this order), Ohnesorge truncation correction,
- * greatest prime factor of the padded size (2 as in RTK built without FFTW;
- * only 2 is accepted on the GPU) and zero-pad factor (2).  hann_cut_y is
+ * greatest prime factor of the padded size (2 as in RTK built without FFTW, 13
+ * as with FFTW: a padded length that is not a power of two is the period of
+ * the circular convolution, run embedded in a power-of-two FFT of at least
+ * twice that length) and zero-pad factor (2).  hann_cut_y is
  * HannCutFrequencyY: > 0 makes the kernel 2-D (the 1-D kernel times a Hann
  * window along the detector rows' frequency, rows zero-padded by
  * zero_pad_factor_y, ZeroPadFactors[1]: 1 or 2, <= 0 meaning RTK's default 2). */

@@ -43,6 +43,7 @@ struct FilterArgs
   const float2 * tw;    // twiddles e^{-2 pi i m/N}
   const float *  mw;    // truncation mirror weights, next+1
   int            nu_in, nu_out, nv, np, shift, N, next;
+  int            period; // RTK's padded length: the circular convolution's period (N, or <= (N+1)/2 when embedded)
 };
 
 // Per-row part of the weights: FDK cos(gamma) terms for row r of projection s
@@ -496,16 +497,17 @@ pair_rows(const FilterArgs & a, int pr)
 
 // Ohnesorge mirror extrapolation (PadInputImageRegion :218-258) in the
 // shared row b0 (the row at columns 0..nu-1, zeros after): left values wrap
-// to the end of the circular buffer.
+// to the end of the convolution's period (the buffer's end unless the period
+// is embedded in a longer FFT).
 __device__ __forceinline__ void
-mirror_pad(const FilterArgs & a, float2 * b0, int nu, int N)
+mirror_pad(const FilterArgs & a, float2 * b0, int nu)
 {
   const float2 SA = b0[pidx(1)], SE = b0[pidx(nu - 1)];
   for (int bq = 1 + threadIdx.x; bq <= a.next; bq += blockDim.x)
   {
     const float  w = __ldg(a.mw + bq);
     const float2 l = b0[pidx(bq)], r = b0[pidx(nu - 1 - bq)];
-    b0[pidx(N - bq)] = make_float2(w * (2.f * SA.x - l.x), w * (2.f * SA.y - l.y));
+    b0[pidx(a.period - bq)] = make_float2(w * (2.f * SA.x - l.x), w * (2.f * SA.y - l.y));
     b0[pidx(nu - 1 + bq)] = make_float2(w * (2.f * SE.x - r.x), w * (2.f * SE.y - r.y));
   }
 }
@@ -576,7 +578,7 @@ ramp_pairs(const FilterArgs & a, int first, int pairs, int stride, float2 * b0, 
         for (int i = 0; i < 16; i++)
           b0[pidx(threadIdx.x + i * T)] = v[i];
         __syncthreads();
-        mirror_pad(a, b0, nu, N);
+        mirror_pad(a, b0, nu);
         __syncthreads();
 #pragma unroll
         for (int i = 0; i < 16; i++)
@@ -624,7 +626,7 @@ ramp_pairs(const FilterArgs & a, int first, int pairs, int stride, float2 * b0, 
       __syncthreads();
       if (a.next > 0)
       {
-        mirror_pad(a, b0, nu, N);
+        mirror_pad(a, b0, nu);
         __syncthreads();
       }
       float2 * X = fft_chain<N, T, 1>(b0, b1, tws);
@@ -966,26 +968,32 @@ prepare_filters(const rtkb_geometry * g, const rtkb_image_desc * in, const Optio
   std::vector<float> K, tw, mw;
   if (o.ramp)
   {
-    if (o.rp.greatest_prime_factor != 2 && o.rp.greatest_prime_factor != 0)
-      return fail(RTKB_ERR_UNSUPPORTED, "the GPU ramp filter pads to powers of two (greatest prime factor 2)");
-    const int N = ramp_padded_size(nu_out, o.rp);
-    if ((N & (N - 1)) != 0 || N > kMaxFFT || N < 2)
-      return fail(RTKB_ERR_UNSUPPORTED, "padded row length must be a power of two <= 8192");
+    // RTK's padded length P is the period of the circular convolution; a P
+    // that is not a power of two (greatest prime factor above 2, RTK built
+    // with FFTW) is embedded in a power-of-two FFT of length >= 2P - 1
+    const int P = ramp_padded_size(nu_out, o.rp);
+    const int N = P >= 1 ? fft_length_for_period(P) : 0;
+    if (P < 2 || N > kMaxFFT)
+      return fail(RTKB_ERR_UNSUPPORTED, "the ramp filter's FFT length (the padded row length, a power of two, or "
+                                        "the power of two >= twice it otherwise) must be <= 8192");
     if ((long long)nv * np > 0x7ffffffe)
       return fail(RTKB_ERR_UNSUPPORTED, "the ramp filter indexes rows in 32 bits: nv * np must be < 2^31");
-    std::vector<double> Kd;
-    ramp_kernel(N, out.spacing[0], o.rp, Kd);
-    K.assign(Kd.begin(), Kd.end());
+    std::vector<double> Kd, KM;
+    ramp_kernel(P, out.spacing[0], o.rp, Kd);
+    if (N != P)
+      embed_spectrum(P, N, Kd, KM);
+    K.assign(N != P ? KM.begin() : Kd.begin(), N != P ? KM.end() : Kd.end());
     pass_twiddles(N, tw);
     // the weights follow the full extent floor(t * nu) (UpdateTruncationMirrorWeights
     // :345-355); the mirror covers at most the zero padding (PadInputImageRegion :215-216)
     const int extent = (int)std::floor(o.rp.truncation_correction * nu_out);
-    const int next = std::min(extent, (N - nu_out) / 2);
+    const int next = std::min(extent, (P - nu_out) / 2);
     if (next > 0 && extent == 1)
       return fail(RTKB_ERR_INVALID_ARGUMENT, "truncation correction extent of one pixel is undefined");
     if (next > 0)
       truncation_mirror_weights(extent, mw);
     a.N = N;
+    a.period = P;
     a.next = next;
   }
   std::vector<float> Ky, twy;
@@ -993,20 +1001,25 @@ prepare_filters(const rtkb_geometry * g, const rtkb_image_desc * in, const Optio
   if (P.colpass)
   {
     const int H = ramp_padded_size_y(nv, o.rp);
-    if ((H & (H - 1)) != 0 || H > kMaxFFT || H < 2)
-      return fail(RTKB_ERR_UNSUPPORTED, "padded column length must be a power of two <= 8192");
+    const int M = H >= 1 ? fft_length_for_period(H) : 0;
+    if (H < 2 || M > kMaxFFT)
+      return fail(RTKB_ERR_UNSUPPORTED, "the 2-D kernel's column FFT length (the padded height, a power of two, or "
+                                        "the power of two >= twice it otherwise) must be <= 8192");
     if ((long long)nu_out * np > 0x7ffffffe)
       return fail(RTKB_ERR_UNSUPPORTED, "the 2-D ramp kernel indexes columns in 32 bits: nu * np must be < 2^31");
-    std::vector<double> Wd;
+    std::vector<double> Wd, WM;
     ramp_window_y(H, o.rp, Wd);
-    Ky.assign(Wd.begin(), Wd.end());
-    pass_twiddles(H, twy);
+    if (M != H)
+      embed_spectrum(H, M, Wd, WM);
+    Ky.assign(M != H ? WM.begin() : Wd.begin(), M != H ? WM.end() : Wd.end());
+    pass_twiddles(M, twy);
     FilterArgs c{};
     c.nu_in = nv;
     c.nu_out = nv;
     c.nv = nu_out;
     c.np = np;
-    c.N = H;
+    c.N = M;
+    c.period = H;
     P.col = c;
     P.col_pairs = ((long long)nu_out * np + 1) / 2;
   }

@@ -30,6 +30,11 @@ void displaced_weights(const Geometry & g, const rtkb_image_desc & proj, const D
 int  ramp_padded_size(int nu, const rtkb_ramp_params & p);
 int  ramp_padded_size_y(int nv, const rtkb_ramp_params & p); // nv without the 2-D kernel
 void ramp_window_y(int padded_y, const rtkb_ramp_params & p, std::vector<double> & w); // padded_y/2+1
+// FFT length for a circular convolution of period P: P itself when a power of
+// two, else the power of two >= 2P - 1 that embed_spectrum targets
+int  fft_length_for_period(int P);
+// spectrum (M/2+1) on a length-M FFT of the even period-P kernel K (P/2+1)
+void embed_spectrum(int P, int M, const std::vector<double> & K, std::vector<double> & KM);
 void ramp_kernel(int padded, double spacing, const rtkb_ramp_params & p, std::vector<double> & K);
 void twiddles(int n, std::vector<float> & tw);
 void truncation_mirror_weights(int next, std::vector<float> & mw);

@@ -306,11 +306,26 @@ ramp_kernel(int padded, double spacing, const rtkb_ramp_params & p, std::vector<
     a[ix] = v;
     a[jx] = v;
   }
-  fft_pow2(a);
   const int n = padded / 2 + 1;
   K.resize(n);
-  for (int i = 0; i < n; i++)
-    K[i] = a[i].real();
+  if ((padded & (padded - 1)) == 0)
+  {
+    fft_pow2(a);
+    for (int i = 0; i < n; i++)
+      K[i] = a[i].real();
+  }
+  else
+  {
+    // other lengths (a greatest prime factor above 2, RTK built with FFTW):
+    // the transform of the real, even kernel as cosine sums
+    for (int i = 0; i < n; i++)
+    {
+      double acc = 0.;
+      for (int k = 0; k < padded; k++)
+        acc += a[k].real() * std::cos(2. * kPi * (double)(((long long)i * k) % padded) / padded);
+      K[i] = acc;
+    }
+  }
   auto ncut_of = [n](double c) { return (int)std::floor(n * std::min(1.0, c) + 0.5); };
   int  start_zero = n;
   if (p.hann_cut > 0.)
@@ -348,6 +363,43 @@ ramp_kernel(int padded, double spacing, const rtkb_ramp_params & p, std::vector<
   }
   for (int i = start_zero; i < n; i++)
     K[i] = 0.;
+}
+
+void
+embed_spectrum(int P, int M, const std::vector<double> & K, std::vector<double> & KM)
+{
+  // h = the kernel's period-P spatial form (real and even: h[d] = h[P - d]);
+  // on an FFT of length M >= 2P - 1 it sits at offsets -(P-1)..P-1, so the
+  // length-M circular convolution of an input supported in [0, P) equals the
+  // period-P one at every output sample in [0, P).
+  std::vector<double> h((size_t)P);
+  for (int d = 0; d < P; d++)
+  {
+    double acc = 0.;
+    for (int f = 0; f < P; f++)
+      acc += K[(size_t)std::min(f, P - f)] * std::cos(2. * kPi * (double)(((long long)f * d) % P) / P);
+    h[d] = acc / P;
+  }
+  std::vector<std::complex<double>> a((size_t)M, 0.);
+  for (int d = 0; d < P; d++)
+    a[d] = h[d];
+  for (int d = 1; d < P; d++)
+    a[(size_t)M - d] = h[(size_t)P - d];
+  fft_pow2(a);
+  KM.resize((size_t)M / 2 + 1);
+  for (int i = 0; i <= M / 2; i++)
+    KM[i] = a[i].real();
+}
+
+int
+fft_length_for_period(int P)
+{
+  if ((P & (P - 1)) == 0)
+    return P;
+  int M = 1;
+  while (M < 2 * P - 1)
+    M <<= 1;
+  return M;
 }
 
 void

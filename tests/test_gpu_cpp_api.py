@@ -1,7 +1,8 @@
 """The header-only C++ layer (include/rtkb200.hpp) on a GPU: a C++ program
 runs JosephForwardProjectionImageFilter, ConjugateGradientConeBeamReconstructionFilter,
 FDKConeBeamReconstructionFilter and the FDKWeightProjectionFilter ->
-FFTRampImageFilter chain on device buffers it allocates itself; the results
+FFTRampImageFilter chain (with the 2-D kernel of SetHannCutFrequencyY) on
+device buffers it allocates itself; the results
 equal those of the same entry points called through the Python binding."""
 import os
 import shutil
@@ -76,6 +77,7 @@ int main(int, char ** argv)
     rtkb::FFTRampImageFilter ramp;
     ramp.SetProjections(pd, d_w, d_w);
     ramp.SetHannCutFrequency(0.8);
+    ramp.SetHannCutFrequencyY(0.5);
     ramp.Update();
   }
   catch (const rtkb::Exception & e)
@@ -142,5 +144,6 @@ def test_cpp_layer_on_gpu_matches_python_binding(rtkb, tmp_path):
     f, fd = rtkb.ops.fdk_preprocess(g, pd, to_gpu(proj), ramp)
     fdk = to_np(rtkb.ops.fdk_backproject(g, vd, fd, f, torch.zeros(vol.shape, device="cuda")))
     assert np.array_equal(fdk_cpp, fdk.astype(np.float32))
-    chain = to_np(rtkb.ops.ramp_filter(pd, rtkb.ops.fdk_weight(g, pd, to_gpu(proj)), ramp))
+    chain = to_np(rtkb.ops.ramp_filter(pd, rtkb.ops.fdk_weight(g, pd, to_gpu(proj)),
+                                       rtkb.ops.ramp_params(hann=0.8, hann_y=0.5)))
     assert np.array_equal(chain_cpp, chain.astype(np.float32))

@@ -103,13 +103,18 @@ def test_displaced_irregular_like_rtkdisplaceddetectorcompcudatest(rtkb, oracle)
                                        (200, {"ramlak": 0.6}), (256, {"shepplogan": 0.8}),
                                        (256, {"truncation": 0.1}), (2048, {"hann": 0.5}),
                                        (600, {"pad": 1}), (700, {"truncation": 0.3}),
-                                       (600, {"truncation": 0.9, "pad": 1}), (4096, {"hann": 0.9})])
+                                       (600, {"truncation": 0.9, "pad": 1}), (4096, {"hann": 0.9}),
+                                       (300, {"gpf": 13}), (99, {"gpf": 13, "pad": 1, "hann": 0.9}),
+                                       (700, {"gpf": 13, "truncation": 0.3}), (1000, {"gpf": 13, "cosine": 0.8})])
 def test_ramp_filter(rtkb, oracle, nu, window):
     """Every form of the ramp kernel: shared-memory passes (N < 1024), the
     register-resident first and last passes with the upper-zero form (row in
     the lower half, no mirror: 300, 1024, 2048, 4096 columns), without it (600
     columns padded to 1024 only) and with the truncation mirror (700 columns;
-    600 with an extent wider than the zero padding)."""
+    600 with an extent wider than the zero padding); with a greatest prime
+    factor of 13 (RTK built with FFTW) the padded lengths 600, 99, 1400 and
+    2000, whose period-P convolution runs embedded in a power-of-two FFT of
+    length >= 2P - 1."""
     pd, po = pair_image(rtkb, oracle, (nu, 7, 3), (0.5, 0.5, 1.0))
     rng = np.random.default_rng(nu)
     p = rng.uniform(0, 1, size=oracle.shape_of(po))
@@ -121,7 +126,8 @@ def test_ramp_filter(rtkb, oracle, nu, window):
 @pytest.mark.parametrize("nu,nv,n,window", [(300, 200, 2, {"hann_y": 0.8}), (1024, 768, 2, {"hann": 1.0, "hann_y": 0.6}),
                                             (128, 40, 3, {"hann_y": 1.0, "pad_y": 1}),
                                             (700, 33, 3, {"cosine": 0.8, "hann_y": 0.4, "truncation": 0.3}),
-                                            (57, 1, 4, {"hann_y": 0.9})])
+                                            (57, 1, 4, {"hann_y": 0.9}),
+                                            (300, 200, 2, {"hann_y": 0.8, "gpf": 13, "truncation": 0.2})])
 def test_ramp_filter_2d_kernel(rtkb, oracle, nu, nv, n, window):
     """HannCutFrequencyY: the 2-D kernel (the row filter, then every column
     zero-padded to the padded height and filtered with the vertical window by

@@ -145,12 +145,17 @@ RAMP_TOL = 1e-5
                                      ((100, 12, 5), {"cosine": 0.7, "truncation": 0.25, "pad": 1}),
                                      ((64, 20, 4), {"hann": 0.8, "hann_y": 0.8}),
                                      ((100, 13, 3), {"hann_y": 0.5, "truncation": 0.2}),
-                                     ((96, 16, 4), {"hann_y": 1.0, "pad_y": 1})])
+                                     ((96, 16, 4), {"hann_y": 1.0, "pad_y": 1}),
+                                     ((100, 12, 5), {"gpf": 13}), ((99, 8, 3), {"gpf": 13, "pad": 1, "hann": 0.9}),
+                                     ((120, 16, 4), {"gpf": 13, "truncation": 0.3}),
+                                     ((64, 20, 4), {"gpf": 13, "hann_y": 0.8})])
 def test_rtk_cuda_ramp_filter_agrees_with_oracle(rtkb, oracle, size, kw):
     """RTK's CUDA ramp filter (CUDA_padding + CUDA_fft_convolution: a 3-D
     cuFFT of the padded stack times the 1-D kernel spectrum, or the 2-D one
     of HannCutFrequencyY through multiply_kernel2D) against the oracle and
-    the product.  With truncation 0.6 the extent floor(0.6 * 128)
+    the product; with a greatest prime factor of 13 (RTK built with FFTW) on
+    padded lengths 200, 99, 240 and height 40, which cuFFT transforms as they
+    are and the product embeds in power-of-two FFTs.  With truncation 0.6 the extent floor(0.6 * 128)
     = 76 exceeds the 64 columns of zero padding: RTK mirrors 64 columns with
     the weights of extent 76, and the case measures the margin by running
     RTK's kernels with the weights of extent 64 instead."""

@@ -330,6 +330,8 @@ joseph_forward_kernel(JosephArgs a, const float * __restrict__ V, const float * 
     {
       const Off     ox1 = (w.nxp > 1) ? ox : 0, oy1 = (w.nyp > 1) ? oy : 0;
       const float * slice = vol + first;
+      // two steps' taps in flight per thread (one projection: 0.254 -> 0.242 ms at 256^3 <- 512x384)
+#pragma unroll 2
       for (int i = 0; i < nmid; i++, slice += dslice)
       {
         const float2  xy = __ffma2_rn(make_float2((float)i, (float)i), sxy, x0);

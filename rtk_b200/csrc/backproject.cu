@@ -378,6 +378,16 @@ bp_consumer(const T * __restrict__ proj, int nproj, int nu, int nv, int nx, int 
   for (int k = 0; k < NYT / 2; k++)
     acc2[k] = make_float2(0.f, 0.f);
 #define BP_ACC(j) (((j) & 1) ? acc2[(j) >> 1].y : acc2[(j) >> 1].x)
+  // the input volume is read after the last projection: start pulling it
+  // into L2 now, so that short launches (few projections per tile) do not
+  // wait on DRAM at the end of every tile
+  if (active)
+  {
+#pragma unroll
+    for (int j = 0; j < NYT; j++)
+      if (y0 + j < ny)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(vol_in + ((long long)Z * ny + y0 + j) * nx + X));
+  }
 
   for (int p = 0; p < nproj; p++)
   {

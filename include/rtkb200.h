@@ -643,6 +643,24 @@ int rtkb_displaced_detector_region(const rtkb_geometry * g, const rtkb_image_des
                                    rtkb_image_desc * out, int * weighted);
 int rtkb_displaced_detector(const rtkb_geometry * g, const rtkb_image_desc * proj, int pad_on_truncated_side,
                             const float * d_in, float * d_out, void * stream);
+/* rtk::DisplacedDetectorForOffsetFieldOfViewImageFilter
+ * (include/rtkDisplacedDetectorForOffsetFieldOfViewImageFilter.hxx), the
+ * variant RTK's CPU rtkfdk chains: the padding and the weights follow the
+ * stack's field of view (the largest disc every projection sees, below)
+ * instead of the detector corners; always padded on the truncated side. */
+int rtkb_displaced_detector_offset_fov_region(const rtkb_geometry * g, const rtkb_image_desc * proj,
+                                              rtkb_image_desc * out, int * weighted);
+int rtkb_displaced_detector_offset_fov(const rtkb_geometry * g, const rtkb_image_desc * proj, const float * d_in,
+                                       float * d_out, void * stream);
+/* rtk::FieldOfViewImageFilter::ComputeFOVRadius (include/rtkFieldOfViewImageFilter.hxx:41-187),
+ * host only: the centre (x, z) and radius r of the largest disc in the
+ * rotation plane that every projection of the geometry sees through the
+ * stack's detector; type 0 RADIUSINF (the first column's rays only), 1
+ * RADIUSSUP (the last column's), 2 RADIUSBOTH.  The linear programme RTK gives
+ * lp_solve is solved exactly (its dual, revised simplex).  RTKB_ERR_INVALID_ARGUMENT
+ * when no such disc exists. */
+int rtkb_field_of_view_radius(const rtkb_geometry * g, const rtkb_image_desc * proj, int type, double * x, double * z,
+                              double * r);
 
 /* Ramp filter parameters of rtk::FFTRampImageFilter (include/rtkFFTRampImageFilter.h)
  * and rtk::FFTProjectionsConvolutionImageFilter: window cut frequencies (0 =
@@ -685,7 +703,7 @@ int rtkb_ramp_filter(const rtkb_image_desc * proj, const rtkb_ramp_params * para
  * with rtkb_displaced_detector_region when displaced != 0). */
 typedef struct rtkb_fdk_preprocess_params
 {
-  int              displaced_detector; /* 0 off, 1 on */
+  int              displaced_detector; /* 0 off, 1 DisplacedDetectorImageFilter, 2 ...ForOffsetFieldOfView */
   int              pad_on_truncated_side;
   int              short_scan;          /* 0 off, 1 Parker weighting when the scan is short */
   double           angular_gap_threshold;

@@ -255,6 +255,28 @@ private:
   bool m_Pad = true;
 };
 
+/* rtk::DisplacedDetectorForOffsetFieldOfViewImageFilter: padding and weights
+ * from the stack's field of view (always padded on the truncated side) */
+class DisplacedDetectorForOffsetFieldOfViewImageFilter : public ProjectorBase
+{
+public:
+  rtkb_image_desc
+  GetOutputRegion() const
+  {
+    rtkb_image_desc out{};
+    int             weighted = 0;
+    Check(rtkb_displaced_detector_offset_fov_region(m_Geometry, &m_Proj, &out, &weighted),
+          "DisplacedDetectorForOffsetFieldOfViewImageFilter");
+    return out;
+  }
+  void
+  Update()
+  {
+    Check(rtkb_displaced_detector_offset_fov(m_Geometry, &m_Proj, m_ProjIn, m_ProjOut, m_Stream),
+          "DisplacedDetectorForOffsetFieldOfViewImageFilter");
+  }
+};
+
 /* rtk::FFTRampImageFilter (no geometry): window cut frequencies as RTK's setters */
 class FFTRampImageFilter : public ProjectorBase
 {

@@ -557,3 +557,112 @@ def fdk_backproject_f32_rtk(g, vol, proj, proj_data_f32, vol_inout_f32, threads=
                                            threads or nthreads())
     if rc != 0:
         raise RuntimeError("CPU baseline needs the optimised-Y path (circular geometry)")
+
+
+# ---- field of view and the offset-field-of-view displaced detector ----------
+
+
+def fov_radius(g, proj, kind):
+    """rtk::FieldOfViewImageFilter::ComputeFOVRadius
+    (include/rtkFieldOfViewImageFilter.hxx:41-187): per projection, the lines
+    from the source through the corner pixels of the first (corners 0, 1) and
+    last (2, 3) detector columns, in the rotation plane (x, z), bound
+    half-planes a x + b z <= c, oriented so that the other side's corners lie
+    inside (:110-131); the largest disc (x, z, r) at distance r inside every
+    half-plane of the kind (0 RADIUSINF: first column, 1 RADIUSSUP: last, 2
+    RADIUSBOTH) maximises r.  RTK hands the programme to lp_solve; the oracle
+    solves the same programme with scipy's HiGHS (geometries without
+    collimation jaws: AddCollimationConstraints adds nothing then).  Returns
+    (x, z, r), or None where lp_solve reports no solution."""
+    from scipy.optimize import linprog
+
+    i2p = index_to_physical(proj)
+    rows, rhs = [], []
+    for k in range(len(g)):
+        s = g.source_position(k)
+        p2f = g.proj_coords_to_fixed(k)
+        a, b, c, cor = [], [], [], []
+        for q in range(4):
+            iu = proj.index[0] + (q // 2) * (proj.size[0] - 1)
+            iv = proj.index[1] + (q % 2) * (proj.size[1] - 1)
+            pos = p2f @ (i2p @ np.array([iu, iv, k, 1.0]))
+            cor.append((pos[0], pos[2]))
+            a.append(pos[2] - s[2])
+            b.append(s[0] - pos[0])
+            c.append(s[0] * pos[2] - pos[0] * s[2])
+        if a[0] * cor[2][0] + b[0] * cor[2][1] >= c[0] and a[1] * cor[3][0] + b[1] * cor[3][1] >= c[1]:
+            flip = (0, 1)
+        elif a[2] * cor[0][0] + b[2] * cor[0][1] >= c[2] and a[3] * cor[1][0] + b[3] * cor[1][1] >= c[3]:
+            flip = (2, 3)
+        else:
+            raise ValueError("Error computing the FOV, unhandled detector rotation.")
+        for q in flip:
+            a[q], b[q], c[q] = -a[q], -b[q], -c[q]
+        for q in range(4):
+            if (q < 2 and kind != 1) or (q >= 2 and kind != 0):
+                rows.append([a[q], b[q], np.hypot(a[q], b[q])])
+                rhs.append(c[q])
+    res = linprog([0.0, 0.0, -1.0], A_ub=np.array(rows), b_ub=np.array(rhs),
+                  bounds=[(None, None), (None, None), (0, None)], method="highs")
+    if res.status != 0:
+        return None
+    return float(res.x[0]), float(res.x[1]), float(res.x[2])
+
+
+def displaced_detector_offset_fov_region(g, proj):
+    """DisplacedDetectorForOffsetFieldOfViewImageFilter::GenerateOutputInformation
+    (include/rtkDisplacedDetectorForOffsetFieldOfViewImageFilter.hxx:36-118):
+    returns (weighted, out index0, out size0, disc (x, z, r), shift)."""
+    fov = fov_radius(g, proj, 2)
+    if fov is None:
+        raise ValueError("Cannot account for too large detector displacements")
+    inf, sup = fov_radius(g, proj, 0), fov_radius(g, proj, 1)
+    ri = inf[2] if inf else float("nan")
+    rs = sup[2] if sup else float("nan")
+    nu = proj.size[0]
+    if 200.0 * abs(ri - rs) / (ri + rs) < 10.0:
+        return False, proj.index[0], nu, fov, 0
+    if rs > ri:
+        return True, proj.index[0] - nu, 2 * nu, fov, nu
+    return True, proj.index[0], 2 * nu, fov, 0
+
+
+def displaced_detector_offset_fov(g, proj, data):
+    """DisplacedDetectorForOffsetFieldOfViewImageFilter::DynamicThreadedGenerateData
+    (:122-270) on a whole stack: returns (out, out index0, out size0)."""
+    weighted, i0, s0, (cx, cz, R), shift = displaced_detector_offset_fov_region(g, proj)
+    d = np.asarray(data, dtype=np.float64)
+    if not weighted:
+        return d.copy(), i0, s0
+    n, nv, nu = d.shape
+    out = np.zeros((n, nv, s0))
+    for s in range(n):
+        k = proj.index[2] + s
+        sp = g.source_position(k)
+        opp = -1.0 / (sp[0] * sp[0] + sp[2] * sp[2])
+        scx, scz = cx - sp[0], cz - sp[2]
+        inv = 1.0 / np.sqrt(scx * scx + scz * scz)
+        ang = np.arctan2(scz * inv, scx * inv) - np.arctan2(sp[2] * opp, sp[0] * opp)
+        if ang > np.pi:
+            ang -= 2 * np.pi
+        if ang < -np.pi:
+            ang += 2 * np.pi
+        t2 = np.arcsin(R / np.sqrt((cx - sp[0]) ** 2 + (cz - sp[2]) ** 2))
+        t1 = -t2 + ang
+        t2 = t2 + ang
+        prm = g.parameters(k)
+        sid = np.sqrt(prm[0] ** 2 + prm[7] ** 2)
+        l1, l2 = np.tan(t1) * sid, np.tan(t2) * sid
+        invsid = 1.0 / sid
+        pod = np.pi / 2 * np.sqrt(scx * scx + scz * scz) / R
+        w = np.empty(nu)
+        for i in range(nu):
+            x = proj.origin[0] + proj.spacing[0] * (proj.index[0] + i)
+            l = g.to_untilted(k, x)
+            f = np.sin(np.sin(np.arctan(l * invsid) - ang) * pod)
+            if shift:
+                w[i] = 0.0 if l <= l1 else (2.0 if l >= l2 else f + 1.0)
+            else:
+                w[i] = 2.0 if l <= l1 else (0.0 if l >= l2 else 1.0 - f)
+        out[s, :, shift:shift + nu] = d[s] * w[None, :]
+    return out, i0, s0

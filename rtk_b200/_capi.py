@@ -114,6 +114,9 @@ SIGNATURES = {
     "rtkb_parker_short_scan": (C.c_int, [_G, _IM, C.c_double, _V, _V, _V, _I]),
     "rtkb_displaced_detector_region": (C.c_int, [_G, _IM, C.c_int, _IM, _I]),
     "rtkb_displaced_detector": (C.c_int, [_G, _IM, C.c_int, _V, _V, _V]),
+    "rtkb_displaced_detector_offset_fov_region": (C.c_int, [_G, _IM, _IM, _I]),
+    "rtkb_displaced_detector_offset_fov": (C.c_int, [_G, _IM, _V, _V, _V]),
+    "rtkb_field_of_view_radius": (C.c_int, [_G, _IM, C.c_int, _D, _D, _D]),
     "rtkb_ramp_kernel": (C.c_int, [C.c_int, C.c_double, C.POINTER(RampParams), _I, _D]),
     "rtkb_ramp_filter": (C.c_int, [_IM, C.POINTER(RampParams), _V, _V, _V]),
     "rtkb_fdk_preprocess": (C.c_int, [_G, _IM, C.POINTER(FdkPreprocessParams), _IM, _V, _V, _V]),

@@ -857,6 +857,7 @@ launch_ramp_n(int N, const FilterArgs & a, const FilterArgs * d_probs, const lon
 struct Options
 {
   bool             displaced = false, pad = true, parker = false, fdk = false, ramp = false;
+  bool             offset_fov = false; // DisplacedDetectorForOffsetFieldOfViewImageFilter
   double           threshold = 3.14159265358979323846 / 9;
   rtkb_ramp_params rp{};
 };
@@ -916,14 +917,17 @@ prepare_filters(const rtkb_geometry * g, const rtkb_image_desc * in, const Optio
   if (o.displaced)
   {
     DisplacedInfo info;
-    int           rc = displaced_region(G, *in, o.pad, info);
+    int           rc = o.offset_fov ? offset_fov_region(G, *in, info) : displaced_region(G, *in, o.pad, info);
     if (rc != RTKB_OK)
       return rc;
     if (info.weighted)
     {
       out = info.out;
       shift = info.shift;
-      displaced_weights(G, *in, info, wd);
+      if (o.offset_fov)
+        offset_fov_weights(G, *in, info, wd);
+      else
+        displaced_weights(G, *in, info, wd);
     }
   }
   bool short_scan = false;
@@ -1231,6 +1235,61 @@ rtkb_displaced_detector(const rtkb_geometry * g, const rtkb_image_desc * proj, i
 }
 
 extern "C" int
+rtkb_displaced_detector_offset_fov_region(const rtkb_geometry * g, const rtkb_image_desc * proj, rtkb_image_desc * out,
+                                          int * weighted)
+{
+  RTKB_TRACE();
+  return guarded([&] {
+    std::string why;
+    if (!g || !out)
+      return rtkb::fail(RTKB_ERR_INVALID_ARGUMENT, "null argument");
+    if (!rtkb::desc_valid(proj, why))
+      return rtkb::fail(RTKB_ERR_INVALID_ARGUMENT, why);
+    if (g->g.radius_cylindrical != 0. || (!g->g.p.empty() && g->g.p[0].sdd == 0.))
+      return rtkb::fail(RTKB_ERR_UNSUPPORTED, "Displaced detector cannot handle cylindrical detector or parallel geometry");
+    rtkb::DisplacedInfo info;
+    int                 rc = rtkb::offset_fov_region(g->g, *proj, info);
+    if (rc != RTKB_OK)
+      return rc;
+    *out = info.weighted ? info.out : *proj;
+    if (weighted)
+      *weighted = info.weighted ? 1 : 0;
+    return RTKB_OK;
+  });
+}
+
+extern "C" int
+rtkb_displaced_detector_offset_fov(const rtkb_geometry * g, const rtkb_image_desc * proj, const float * d_in,
+                                   float * d_out, void * stream)
+{
+  RTKB_TRACE();
+  return guarded([&] {
+    Options o;
+    o.displaced = true;
+    o.offset_fov = true;
+    return run_filters(g, proj, o, nullptr, d_in, d_out, static_cast<cudaStream_t>(stream), nullptr);
+  });
+}
+
+extern "C" int
+rtkb_field_of_view_radius(const rtkb_geometry * g, const rtkb_image_desc * proj, int type, double * x, double * z,
+                          double * r)
+{
+  RTKB_TRACE();
+  return guarded([&] {
+    std::string why;
+    if (!g || !x || !z || !r || type < 0 || type > 2)
+      return rtkb::fail(RTKB_ERR_INVALID_ARGUMENT, "invalid field-of-view arguments");
+    if (!rtkb::desc_valid(proj, why))
+      return rtkb::fail(RTKB_ERR_INVALID_ARGUMENT, why);
+    const int rc = rtkb::fov_radius(g->g, *proj, type, *x, *z, *r);
+    return rc == RTKB_OK || rc == RTKB_ERR_UNSUPPORTED
+             ? rc
+             : rtkb::fail(RTKB_ERR_INVALID_ARGUMENT, "no disc is seen by every projection (the programme has no solution)");
+  });
+}
+
+extern "C" int
 rtkb_ramp_kernel(int nu, double spacing, const rtkb_ramp_params * p, int * padded, double * kernel)
 {
   RTKB_TRACE();
@@ -1285,6 +1344,7 @@ rtkb_fdk_preprocess(const rtkb_geometry * g, const rtkb_image_desc * proj, const
       return rtkb::fail(RTKB_ERR_INVALID_ARGUMENT, "null preprocessing parameters");
     Options o;
     o.displaced = p->displaced_detector != 0;
+    o.offset_fov = p->displaced_detector == 2;
     o.pad = p->pad_on_truncated_side != 0;
     o.parker = p->short_scan != 0;
     o.threshold = p->angular_gap_threshold > 0. ? p->angular_gap_threshold : 3.14159265358979323846 / 9;
@@ -1308,6 +1368,7 @@ rtkb_fdk_preprocess_batch(rtkb_fdk_preprocess_problem * problems, int n, const r
       return fail(RTKB_ERR_INVALID_ARGUMENT, "invalid problem list");
     Options o;
     o.displaced = p->displaced_detector != 0;
+    o.offset_fov = p->displaced_detector == 2;
     o.pad = p->pad_on_truncated_side != 0;
     o.parker = p->short_scan != 0;
     o.threshold = p->angular_gap_threshold > 0. ? p->angular_gap_threshold : 3.14159265358979323846 / 9;

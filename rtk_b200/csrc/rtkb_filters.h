@@ -22,7 +22,16 @@ struct DisplacedInfo
   bool            weighted;
   int             shift; // output column of input column 0
   double          inf, sup;
+  // DisplacedDetectorForOffsetFieldOfViewImageFilter: the field of view's disc
+  bool            offset_fov = false;
+  double          fov_x = 0., fov_z = 0., fov_r = -1.;
 };
+// FieldOfViewImageFilter::ComputeFOVRadius: type 0 RADIUSINF, 1 RADIUSSUP,
+// 2 RADIUSBOTH; RTKB_OK with the disc, an error code when there is none
+int  fov_radius(const Geometry & g, const rtkb_image_desc & proj, int type, double & x, double & z, double & r);
+int  offset_fov_region(const Geometry & g, const rtkb_image_desc & proj, DisplacedInfo & info);
+void offset_fov_weights(const Geometry & g, const rtkb_image_desc & proj, const DisplacedInfo & info,
+                        std::vector<float> & w);
 int  displaced_region(const Geometry & g, const rtkb_image_desc & proj, bool pad, DisplacedInfo & info);
 void displaced_weights(const Geometry & g, const rtkb_image_desc & proj, const DisplacedInfo & info,
                        std::vector<float> & w);

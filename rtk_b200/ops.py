@@ -181,6 +181,41 @@ def displaced_detector(geometry, proj_desc, proj, pad=True, stream=None, out=Non
     return out, od
 
 
+def displaced_detector_offset_fov_region(geometry, proj_desc):
+    """Output image of rtk::DisplacedDetectorForOffsetFieldOfViewImageFilter
+    and whether it weights: (out_desc, weighted)."""
+    from ._capi import ImageDesc
+
+    out = ImageDesc()
+    w = C.c_int(0)
+    check(load().rtkb_displaced_detector_offset_fov_region(geometry.handle, C.byref(proj_desc), C.byref(out),
+                                                           C.byref(w)))
+    return out, bool(w.value)
+
+
+def displaced_detector_offset_fov(geometry, proj_desc, proj, stream=None, out=None):
+    """rtk::DisplacedDetectorForOffsetFieldOfViewImageFilter (the displaced-detector
+    weighting RTK's CPU rtkfdk chains: padding and weights from the stack's
+    field of view); returns (out, out_desc)."""
+    od, _ = displaced_detector_offset_fov_region(geometry, proj_desc)
+    out = _unary(None, proj_desc, proj, out, shape_of(od))
+    check(load().rtkb_displaced_detector_offset_fov(geometry.handle, C.byref(proj_desc), _ptr(proj), _ptr(out),
+                                                    _stream(stream)))
+    return out, od
+
+
+FOV_RADIUS_INF, FOV_RADIUS_SUP, FOV_RADIUS_BOTH = 0, 1, 2
+
+
+def field_of_view_radius(geometry, proj_desc, kind=FOV_RADIUS_BOTH):
+    """rtk::FieldOfViewImageFilter::ComputeFOVRadius (host only): (x, z, r) of
+    the largest disc in the rotation plane every projection sees."""
+    x, z, r = C.c_double(0.0), C.c_double(0.0), C.c_double(0.0)
+    check(load().rtkb_field_of_view_radius(geometry.handle, C.byref(proj_desc), int(kind), C.byref(x), C.byref(z),
+                                           C.byref(r)))
+    return x.value, z.value, r.value
+
+
 def ramp_kernel(nu, spacing, params):
     import numpy as np
 
@@ -200,19 +235,35 @@ def ramp_filter(proj_desc, proj, params=None, out=None, stream=None):
     return out
 
 
+def _displaced_mode(displaced):
+    """rtkb_fdk_preprocess_params.displaced_detector: False 0, True 1
+    (DisplacedDetectorImageFilter), "offset_fov" 2 (its ForOffsetFieldOfView
+    variant)."""
+    return 2 if displaced == "offset_fov" else int(bool(displaced))
+
+
+def _displaced_region(geometry, proj_desc, displaced, pad):
+    if _displaced_mode(displaced) == 2:
+        return displaced_detector_offset_fov_region(geometry, proj_desc)[0]
+    return displaced_detector_region(geometry, proj_desc, pad)[0]
+
+
 def fdk_preprocess(geometry, proj_desc, proj, ramp=None, displaced=False, pad=True, short_scan=False,
                    threshold=3.141592653589793 / 9, stream=None, out=None):
     """Displaced detector + Parker + FDK weighting + ramp in one pass.
-    Returns (filtered stack, its description)."""
+    displaced: False, True (DisplacedDetectorImageFilter) or "offset_fov"
+    (DisplacedDetectorForOffsetFieldOfViewImageFilter).  Returns (filtered
+    stack, its description)."""
     from ._capi import FdkPreprocessParams
 
     p = FdkPreprocessParams()
-    p.displaced_detector, p.pad_on_truncated_side, p.short_scan = int(displaced), int(pad), int(short_scan)
+    p.displaced_detector, p.pad_on_truncated_side = _displaced_mode(displaced), int(pad)
+    p.short_scan = int(short_scan)
     p.angular_gap_threshold = threshold
     p.ramp = ramp or ramp_params()
     od = proj_desc
     if displaced:
-        od, _ = displaced_detector_region(geometry, proj_desc, pad)
+        od = _displaced_region(geometry, proj_desc, displaced, pad)
     out = _unary(None, proj_desc, proj, out, shape_of(od))
     from ._capi import ImageDesc
 
@@ -230,7 +281,8 @@ def fdk_preprocess_batch(problems, ramp=None, displaced=False, pad=True, short_s
     from ._capi import FdkPreprocessParams, FdkPreprocessProblem
 
     p = FdkPreprocessParams()
-    p.displaced_detector, p.pad_on_truncated_side, p.short_scan = int(displaced), int(pad), int(short_scan)
+    p.displaced_detector, p.pad_on_truncated_side = _displaced_mode(displaced), int(pad)
+    p.short_scan = int(short_scan)
     p.angular_gap_threshold = threshold
     p.ramp = ramp or ramp_params()
     arr = (FdkPreprocessProblem * max(1, len(problems)))()
@@ -238,7 +290,7 @@ def fdk_preprocess_batch(problems, ramp=None, displaced=False, pad=True, short_s
     for k, (geometry, proj_desc, proj, out) in enumerate(problems):
         od = proj_desc
         if displaced:
-            od, _ = displaced_detector_region(geometry, proj_desc, pad)
+            od = _displaced_region(geometry, proj_desc, displaced, pad)
         out = _unary(None, proj_desc, proj, out, shape_of(od))
         arr[k].geometry, arr[k].proj = geometry.handle, proj_desc
         arr[k].d_in, arr[k].d_out = _ptr(proj), _ptr(out)

@@ -110,7 +110,7 @@ def check_image_quality(recon: np.ndarray, ref: np.ndarray, err_tol: float, psnr
     d = recon.astype(np.float64) - ref.astype(np.float64)
     err = np.abs(d).mean()
     mse = (d * d).mean()
-    psnr = 20 * np.log10(ref_value) - 10 * np.log10(mse)
+    psnr = float("inf") if mse == 0.0 else 20 * np.log10(ref_value) - 10 * np.log10(mse)
     return err, psnr, bool(err < err_tol and psnr > psnr_tol)
 
 

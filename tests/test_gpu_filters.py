@@ -98,6 +98,58 @@ def test_displaced_irregular_like_rtkdisplaceddetectorcompcudatest(rtkb, oracle)
     _rtk_cuda_cpu_check(to_np(got), ref)
 
 
+@pytest.mark.parametrize("offset,irregular", [(60.0, False), (-45.0, False), (50.0, True)])
+def test_displaced_detector_offset_fov(rtkb, oracle, offset, irregular):
+    """DisplacedDetectorForOffsetFieldOfViewImageFilter (the variant RTK's CPU
+    rtkfdk chains) on detectors displaced to either side and on an irregular
+    geometry (per-projection distances, offsets and source offsets): padded
+    region and weights (from the field of view's disc) against the oracle."""
+    if irregular:
+        params = [(900.0 + 3 * (i % 7), 1400.0 + 5 * (i % 5), i * 3.7 + 1.0, offset + (i % 3), 2.0, 0.0, 0.0, 4.0, 1.0)
+                  for i in range(97)]
+    else:
+        params = [(1000.0, 1536.0, i * 6.0, offset, 0.0) for i in range(60)]
+    gl, go = pair_geometry(rtkb, oracle, params)
+    pd, po = pair_image(rtkb, oracle, (256, 6, len(params)), (0.8, 0.8, 1.0))
+    p = np.random.default_rng(5).uniform(0, 1, size=oracle.shape_of(po))
+    ref, i0, s0 = oracle.displaced_detector_offset_fov(go, po, p)
+    got, od = rtkb.ops.displaced_detector_offset_fov(gl, pd, to_gpu(p))
+    assert (od.index[0], od.size[0]) == (i0, s0) and s0 == 512
+    assert rel_l2(to_np(got), ref) < 1e-6
+
+
+def test_offset_fov_like_rtkdisplaceddetectorcompoffsettest(rtkb, oracle):
+    """RTK's test/rtkdisplaceddetectorcompoffsettest.cxx: on its four-projection
+    geometry and Shepp-Logan stack the offset-field-of-view variant equals
+    DisplacedDetectorImageFilter (CheckImageQuality 1e-6, 100 dB, reference 1)."""
+    params = [(600., 560., 0., 3., 0., 0., 0., 2., 0.), (500., 545., 90., 2., 0., 0., 0., 4., 0.),
+              (700., 790., 180., 8., 0., 0., 0., 5., 0.), (900., 935., 270., 4., 0., 0., 0., 8., 0.)]
+    gl, go = pair_geometry(rtkb, oracle, params)
+    pd, po = pair_image(rtkb, oracle, (128, 4, 4), (8.0, 2.0, 2.0), origin=(-508.0, -3.0, 0.0))
+    p = _sl_projections(oracle, go, po).astype(np.float32)
+    a, oda = rtkb.ops.displaced_detector_offset_fov(gl, pd, to_gpu(p))
+    b, odb = rtkb.ops.displaced_detector(gl, pd, to_gpu(p))
+    assert (oda.index[0], oda.size[0]) == (odb.index[0], odb.size[0])
+    err, psnr, ok = phantoms.check_image_quality(to_np(a), to_np(b), 1e-6, 100.0, 1.0)
+    assert ok, (err, psnr)
+
+
+def test_fdk_preprocess_offset_fov(rtkb, oracle):
+    """The fused FDK preprocessing with the offset-field-of-view displaced
+    detector (rtkfdk's CPU chain: displaced detector, Parker, FDK weights,
+    ramp) against the oracle's filters in sequence."""
+    params = [(1000.0, 1536.0, i * 4.0, 70.0, 1.0) for i in range(90)]
+    gl, go = pair_geometry(rtkb, oracle, params)
+    pd, po = pair_image(rtkb, oracle, (200, 9, 90), (0.8, 0.8, 1.0))
+    p = np.random.default_rng(6).uniform(0, 1, size=oracle.shape_of(po))
+    q, i0, s0 = oracle.displaced_detector_offset_fov(go, po, p)
+    qo = oracle.image((s0, 9, 90), (0.8, 0.8, 1.0), origin=tuple(po.origin), index=(i0, 0, 0))
+    ref = oracle.ramp_filter(qo, oracle.fdk_weight(go, qo, q), oracle.ramp_params(hann=0.9))
+    got, od = rtkb.ops.fdk_preprocess(gl, pd, to_gpu(p), rtkb.ops.ramp_params(hann=0.9), displaced="offset_fov")
+    assert (od.index[0], od.size[0]) == (i0, s0)
+    assert rel_l2(to_np(got), ref) < REL_L2_TOL
+
+
 @pytest.mark.parametrize("nu,window", [(256, {}), (1024, {"hann": 1.0}), (300, {"hann": 0.8}),
                                        (128, {"cosine": 0.7}), (512, {"hamming": 0.9}),
                                        (200, {"ramlak": 0.6}), (256, {"shepplogan": 0.8}),

@@ -325,3 +325,67 @@ def test_ramp_2d_kernel_equals_rows_then_windowed_columns(oracle):
         ref = np.fft.ifft(np.fft.fft(pad, axis=1) * full[None, :, None], axis=1).real[:, :nv, :]
         assert np.linalg.norm(got - ref) <= 1e-12 * np.linalg.norm(ref), (nu, nv, kw)
         assert np.linalg.norm(got - rows) > 1e-3 * np.linalg.norm(rows)  # the window does act
+
+
+def _fov_geometries(oracle, rtkb):
+    """(name, product geometry, oracle geometry, product stack desc, oracle stack)"""
+    from tests.gpu_util import pair_geometry, pair_image
+
+    n = 90
+    cases = [("centred", [(1000.0, 1536.0, i * 4.0, 0.0, 0.0) for i in range(n)]),
+             ("displaced +60", [(1000.0, 1536.0, i * 4.0, 60.0, 0.0) for i in range(n)]),
+             ("displaced -45", [(1000.0, 1536.0, i * 4.0, -45.0, 0.0) for i in range(n)]),
+             ("irregular", [(900.0 + 3 * (i % 7), 1400.0 + 5 * (i % 5), i * 3.7 + 1.0, 50.0 + (i % 3), 2.0, 0.0, 0.0,
+                             4.0, 1.0) for i in range(97)]),
+             ("short scan", [(1000.0, 1536.0, i * 220.0 / n, 0.0, 0.0) for i in range(n)])]
+    out = []
+    for name, params in cases:
+        gl, go = pair_geometry(rtkb, oracle, params)
+        pd, po = pair_image(rtkb, oracle, (200, 20, len(params)), (1.0, 1.0, 1.0), index=(3, -2, 0))
+        out.append((name, gl, go, pd, po))
+    return out
+
+
+def test_field_of_view_radius_product_equals_oracle(oracle):
+    """FieldOfViewImageFilter::ComputeFOVRadius: the product's exact solution
+    of RTK's linear programme (its dual, revised simplex, host code) against
+    the oracle's (scipy HiGHS on the primal), for each kind of disc and five
+    geometries; and the known answer for a centred detector over 360 degrees,
+    R = SID sin(atan(half width / SDD)) with the half width to the outer
+    pixel centres."""
+    import rtk_b200 as rtkb
+
+    O = oracle
+    for name, gl, go, pd, po in _fov_geometries(O, rtkb):
+        for kind in (0, 1, 2):
+            ref = O.fov_radius(go, po, kind)
+            got = rtkb.ops.field_of_view_radius(gl, pd, kind)
+            assert ref is not None, (name, kind)
+            np.testing.assert_allclose(got, ref, rtol=0, atol=1e-7, err_msg=f"{name} kind {kind}")
+    # the centred stack's columns 3..202 at 1 mm lie at -96.5..102.5 mm: over
+    # 360 degrees the disc is bounded by the nearer edge
+    name, gl, go, pd, po = _fov_geometries(O, rtkb)[0]
+    x0, x1 = po.origin[0] + 3.0, po.origin[0] + 202.0
+    r_exact = 1000.0 * np.sin(np.arctan(min(-x0, x1) / 1536.0))
+    assert abs(O.fov_radius(go, po, 2)[2] - r_exact) < 1e-9 * r_exact
+    assert abs(rtkb.ops.field_of_view_radius(gl, pd, 2)[2] - r_exact) < 1e-7
+
+
+def test_offset_fov_displaced_detector_region_rules(oracle):
+    """DisplacedDetectorForOffsetFieldOfViewImageFilter's region rules
+    (include/rtkDisplacedDetectorForOffsetFieldOfViewImageFilter.hxx:96-117):
+    centred detector -> no padding; a detector displaced to +x (its superior
+    disc the larger) -> padded on the left; to -x -> on the right."""
+    import rtk_b200 as rtkb
+
+    O = oracle
+    geoms = {c[0]: c for c in _fov_geometries(O, rtkb)}
+    for name, left in (("centred", None), ("displaced +60", True), ("displaced -45", False)):
+        _, gl, go, pd, po = geoms[name]
+        weighted, i0, s0, _, shift = O.displaced_detector_offset_fov_region(go, po)
+        od, w = rtkb.ops.displaced_detector_offset_fov_region(gl, pd)
+        assert (weighted, i0, s0) == (w, od.index[0], od.size[0])
+        if left is None:
+            assert not weighted
+        else:
+            assert weighted and s0 == 2 * po.size[0] and (shift > 0) == left

@@ -40,8 +40,8 @@ L1_BYTES_PER_UPDATE = 16  # four 4-byte taps of one bilinear interpolation
 # DRAM bytes (read + write) of one backprojection launch of this workload under each tile schedule,
 # recorded from a 1-pass ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of the kernel as of
 # BP_TRAFFIC_COMMIT; recorded figures, not measurements of the build that runs.
-BP_DRAM_BYTES_BY_SCHEDULE = {0: 69.6170e9 + 0.5954e9, 1: 13.1531e9 + 0.5867e9}
-BP_TRAFFIC_COMMIT = "69769ba"
+BP_DRAM_BYTES_BY_SCHEDULE = {0: 70.3237e9 + 0.5960e9, 1: 13.6485e9 + 0.5856e9}
+BP_TRAFFIC_COMMIT = "e17605a"
 WORKLOAD = {"workload": "FDK backprojection 512^3 @0.5mm <- 720 x 1024x768 @0.388mm, SID 1000, SDD 1536, 360 deg",
             "volume": [NX, NY, NZ], "projections": [NU, NV, NP], "dtype_storage": "float32",
             "l2_policy": "inputs larger than L2 (2.26 GB projection stack, 0.54 GB volume)"}

@@ -277,6 +277,58 @@ def joseph_forward_leg(torch, rtkb, lib, stream, reps=2):
     return out_leg
 
 
+def joseph_back_leg(torch, rtkb, lib, stream, reps=3):
+    """Joseph back projection of the CG configuration (360 x 512x384 @0.8 mm
+    -> 256^3 @1 mm, seeded uniform projections), device time, samples per
+    second and the L1-gather roofline (one bilinear splat moves 4 taps x 4 B;
+    the kernel is bound by its atomic reductions instead), beside RTK's own
+    CUDA ray-cast back projector (kernel_ray_cast_back_project, built
+    unchanged, 16-projection slabs; steps of the smallest spacing, trilinear
+    atomic splats) on the same projections, with the two outputs' relative L2
+    distance (different discretisations of the same adjoint)."""
+    from oracle import oracle as O
+    from oracle import rtk_cuda
+    from tests import workloads as W
+
+    c = W.C3
+    n = c["n"]
+    g = rtkb.geometry.circular(n, c["sid"], c["sdd"])
+    vd = rtkb.make_desc(c["vol"], (c["vox"],) * 3)
+    pd = rtkb.make_desc((*c["det"], n), (c["pix"], c["pix"], 1.0))
+    gen = torch.Generator(device="cuda").manual_seed(SEED + 5)
+    p = torch.rand((n, c["det"][1], c["det"][0]), device="cuda", generator=gen)
+    vin = torch.zeros(tuple(reversed(c["vol"])), device="cuda")
+    vout = torch.empty_like(vin)
+    samples = rtkb.ops.joseph_sample_count(g, vd, pd, stream=stream)
+    ms, _ = _event_median_ms(torch, lambda: rtkb.ops.joseph_back_project(g, vd, pd, p, vin, out=vout), reps)
+    peak = smem_peak_gbs(torch, lib, stream)
+    achieved = samples * 16 / (ms * 1e-3) / 1e9
+    leg = {"workload": "Joseph back projection 360 x 512x384 @0.8mm -> 256^3 @1mm, seeded uniform projections",
+           "samples_per_launch": samples, "ms_per_launch": ms, "gsamples_per_s": samples / (ms * 1e-3) / 1e9,
+           "roofline": {"bound": "l1", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                        "bytes_per_sample": 16,
+                        "peak_source": "shared-memory bilinear-gather probe (the bound is the atomic reductions)"}}
+    if not rtk_cuda.iter_available():
+        leg["rtk_cuda_reference"] = {"unavailable": "RTK's CUDA projectors were not built"}
+        return leg
+    prod = vout.clone()
+    go = O.Geometry()
+    for i in range(n):
+        go.add_projection(c["sid"], c["sdd"], i * 360.0 / n)
+    vo = O.image(c["vol"], (c["vox"],) * 3)
+    po = O.image((*c["det"], n), (c["pix"], c["pix"], 1.0))
+
+    def run_rtk():
+        rtk_cuda.ray_cast_back_project(O, go, vo, po, vin.data_ptr(), vout.data_ptr(), p.data_ptr())
+
+    ms_rtk, _ = _event_median_ms(torch, run_rtk, reps)
+    leg["rtk_cuda_reference"] = {
+        "ms_per_back_projection": ms_rtk, "product_speedup": ms_rtk / ms,
+        "rel_l2_to_product": float((vout - prod).double().norm() / prod.double().norm()),
+        "kernel": "RTK kernel_ray_cast_back_project, SLAB_SIZE 16, trilinear atomic splats every smallest spacing"}
+    return leg
+
+
 def _event_median_ms(torch, run, reps):
     """Median device time of run() over reps calls (one warm-up call first);
     run() may issue work on the legacy default stream, so each call is
@@ -1429,6 +1481,7 @@ def main():
         leg("projection_sweep", sweep_leg, torch, rtkb, g, vd, pd, proj, vol, stream, args.bp_schedule)
         del proj
         leg("joseph_forward", joseph_forward_leg, torch, rtkb, lib, stream)
+        leg("joseph_back", joseph_back_leg, torch, rtkb, lib, stream)
         leg("batched", batch_leg, torch, rtkb, stream)
         leg("batched_fdk_cg", c4_leg, torch, rtkb, stream)
         leg("sart", sart_leg, torch, rtkb, stream)

@@ -254,6 +254,8 @@ def ilib():
         L.rtkcuda_forward_project.argtypes = [I3, I3, F, F, V, V, V, C.c_float, F, F, F]
         L.rtkcuda_back_project.restype = C.c_int
         L.rtkcuda_back_project.argtypes = [I3, I3, F, V, V, V]
+        L.rtkcuda_ray_cast_back_project.restype = C.c_int
+        L.rtkcuda_ray_cast_back_project.argtypes = [I3, I3, F, F, V, V, V, C.c_float, F, F, F]
         L.rtkcuda_laplacian.restype = C.c_int
         L.rtkcuda_laplacian.argtypes = [I3, F, V, V]
         L.rtkcuda_total_variation.restype = C.c_int
@@ -314,6 +316,43 @@ def forward_project(O, g, vol, proj, d_vol: int, d_proj_in: int, d_proj_out: int
     _icheck(ilib().rtkcuda_forward_project(_i(proj.size), _i(vol.size), mp, sp_, C.c_void_p(d_proj_in),
                                            C.c_void_p(d_proj_out), C.c_void_p(d_vol),
                                            float(step if t_step is None else t_step), ap, bp, cp))
+
+
+def ray_cast_back_matrices(O, g, vol, proj):
+    """What CudaRayCastBackProjectionImageFilter::GPUGenerateData passes for
+    a flat panel (src/rtkCudaRayCastBackProjectionImageFilter.cxx:57-156): per
+    projection, detector index -> volume index (voxel centres: the volume's
+    physical-to-index matrix, the oracle's projection-coordinates-to-fixed-system
+    matrix, the stack's index-to-physical matrix), the source in volume
+    indices, the box from the first to the last voxel index, the spacing and
+    the default step (the smallest spacing).  Regions start at index 0."""
+    if any(vol.index) or any(proj.index[:2]):
+        raise ValueError("regions starting at index 0 only")
+    pp2i = np.linalg.inv(O.index_to_physical(vol))
+    i2p = O.index_to_physical(proj)
+    n = proj.size[2]
+    mats = np.zeros((n, 12), dtype=np.float32)
+    src = np.zeros((n, 3), dtype=np.float32)
+    for s in range(n):
+        k = proj.index[2] + s
+        mats[s] = (pp2i @ g.proj_coords_to_fixed(k) @ i2p)[:3].reshape(12)
+        src[s] = (pp2i @ g.source_position(k))[:3]
+    return mats, src, [0.0, 0.0, 0.0], [vol.size[i] - 1.0 for i in range(3)], list(vol.spacing), \
+        float(min(vol.spacing))
+
+
+def ray_cast_back_project(O, g, vol, proj, d_vol_in: int, d_vol_out: int, d_proj: int, t_step=None) -> None:
+    """RTK's CUDA ray-cast back projector (kernel_ray_cast_back_project, the
+    adjoint of its ray-casting forward projector: steps of the smallest
+    spacing along each ray, trilinear atomic splats) over 16-projection
+    slabs."""
+    mats, src, bmin, bmax, sp, step = ray_cast_back_matrices(O, g, vol, proj)
+    m, mp = _f(mats)
+    q, qp = _f(src)
+    b0, b1, s0 = _f(bmin), _f(bmax), _f(sp)  # (array, pointer) pairs, alive for the call
+    _icheck(ilib().rtkcuda_ray_cast_back_project(_i(proj.size), _i(vol.size), mp, qp, C.c_void_p(d_vol_in),
+                                                 C.c_void_p(d_vol_out), C.c_void_p(d_proj),
+                                                 float(t_step or step), b0[1], b1[1], s0[1]))
 
 
 def back_project(O, g, vol, proj, d_vol_in: int, d_vol_out: int, d_proj: int) -> None:

@@ -1,6 +1,6 @@
 // rtk_cuda_iter_driver.cu -- C entry points around RTK's own CUDA projectors
 // and iterative-reconstruction pieces, compiled unchanged from the RTK
-// sources: the ray-casting forward projector, the voxel-based back projector,
+// sources: the ray-casting forward and back projectors, the voxel-based back projector,
 // the Laplacian, total-variation denoising (BPDQ) and the conjugate-gradient
 // vector update.  Tests and bench.py use them to pin the oracle's conventions
 // to the reference's GPU code and to time the reference beside the product.
@@ -14,6 +14,7 @@
 #include "rtkCudaConjugateGradientImageFilter.hcu"
 #include "rtkCudaForwardProjectionImageFilter.hcu"
 #include "rtkCudaLaplacianImageFilter.hcu"
+#include "rtkCudaRayCastBackProjectionImageFilter.hcu"
 #include "rtkCudaTotalVariationDenoisingBPDQImageFilter.hcu"
 
 #include <cstddef>
@@ -70,6 +71,38 @@ rtkcuda_forward_project(const int proj_size[3], const int vol_size[3], const flo
       // the volume transforms are read only for cylindrical panels
       CUDA_forward_project(ps, vs, m, m, dev_proj_in + plane * i, dev_proj_out + plane * i, dev_vol, t_step,
                            const_cast<float *>(sources) + 3 * i, 0.f, bmin, bmax, sp, 1);
+    }
+  });
+}
+
+// CudaRayCastBackProjectionImageFilter::GPUGenerateData
+// (src/rtkCudaRayCastBackProjectionImageFilter.cxx:35-186), flat panel: slabs
+// of SLAB_SIZE projections, the output of one slab the input of the next;
+// `pixel_to_volume` and `sources` as for the forward projector (the same
+// matrices, :115-156), the box from the first to the last voxel index and the
+// step the minimum spacing (:57-76), all computed by the caller.
+extern "C" int
+rtkcuda_ray_cast_back_project(const int proj_size[3], const int vol_size[3], const float * pixel_to_volume,
+                              const float * sources, float * dev_vol_in, float * dev_vol_out, float * dev_proj,
+                              float t_step, const float box_min[3], const float box_max[3], const float spacing[3])
+{
+  return guarded([&] {
+    int          ps[3] = { proj_size[0], proj_size[1], proj_size[2] };
+    int          vs[3] = { vol_size[0], vol_size[1], vol_size[2] };
+    float        bmin[3] = { box_min[0], box_min[1], box_min[2] }, bmax[3] = { box_max[0], box_max[1], box_max[2] };
+    float        sp[3] = { spacing[0], spacing[1], spacing[2] };
+    const size_t plane = (size_t)ps[0] * ps[1];
+    const int    n = proj_size[2];
+    float *      pin = dev_vol_in;
+    for (int i = 0; i < n; i += SLAB_SIZE)
+    {
+      ps[2] = (n - i < SLAB_SIZE) ? n - i : SLAB_SIZE;
+      float * m = const_cast<float *>(pixel_to_volume) + 12 * i;
+      // the filter passes its float source array through a double pointer
+      // that the kernel reads back as floats (:155, :173)
+      CUDA_ray_cast_back_project(ps, vs, m, m, pin, dev_vol_out, dev_proj + plane * i, t_step,
+                                 reinterpret_cast<double *>(const_cast<float *>(sources) + 3 * i), 0.f, bmin, bmax, sp);
+      pin = dev_vol_out;
     }
   });
 }
